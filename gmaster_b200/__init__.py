@@ -1,0 +1,25 @@
+"""gmaster_b200 -- B200-native pseudo-C_ell MASTER estimator on HEALPix maps.
+
+A drop-in for the hot path of licongxu/GMaster (NaMaster-style API):
+`NmtField` -> `NmtWorkspace.from_fields` -> `compute_coupled_cell` -> `decouple_cell`,
+plus `map2alm` / `alm2map` for spin 0 and spin 2.  Every stage runs in hand-written
+sm_100a CUDA kernels (``libgm_b200.so``, C ABI in ``include/gm_b200.h``) on one GPU;
+there is no CPU fallback.  Arrays are CUDA ``torch.Tensor``s.
+"""
+
+from ._config import (get_default_params, get_precision, nmt_params, set_n_iter_default,
+                      set_precision, set_sht_calculator, set_tol_pinv_default)
+from .bins import NmtBin
+from .field import NmtField
+from .utils import (NmtAlmInfo, NmtMapInfo, alm2map, map2alm, map2alm_pair, mask_apodization,
+                    synfast_spherical)
+from .workspaces import NmtWorkspace, compute_coupled_cell
+
+__all__ = [
+    "NmtAlmInfo", "NmtBin", "NmtField", "NmtMapInfo", "NmtWorkspace", "alm2map",
+    "compute_coupled_cell", "get_default_params", "get_precision", "map2alm", "map2alm_pair",
+    "mask_apodization", "nmt_params", "set_n_iter_default", "set_precision",
+    "set_sht_calculator", "set_tol_pinv_default", "synfast_spherical",
+]
+
+__version__ = "0.1.0"

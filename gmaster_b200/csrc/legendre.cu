@@ -1,0 +1,531 @@
+// Latitudinal (Legendre / spin-weighted Wigner-d) stage, SIMT kernels for sm_100a.
+//
+// For each order m the rows lambda^{s'}_lm(theta) = sqrt((2l+1)/4pi) d^l_{m,s'}(theta)
+// are generated on the fly by the normalised three-term recurrence in l, in double
+// precision with an explicit binary exponent per lane (values below 2^-300 are
+// carried exactly and emitted as zero), and contracted against the ring spectra.
+// Only northern lanes are marched: the hemisphere fold
+//   lambda^{s'}_lm(pi - theta) = (-1)^{l+m} lambda^{-s'}_lm(theta)
+// turns the two hemispheres into the Sum / Diff right-hand sides of `rhs`.
+//
+// The contraction is carried in T (double for GM_FP64, float for GM_MIXED); the
+// recurrence is always double.  These kernels are the plain-FP64 path and the
+// narrow-batch mixed path; the tensor-core path (legendre_tc.cu) takes wide batches.
+//
+// Replaces gmaster/_native/cuda/march_v2.cu:155-407 (march_analysis /
+// march_synthesis: float32 difference-form recurrence, SIMT FMA contraction).
+#include <math.h>
+
+#include "gm_common.cuh"
+
+namespace gm {
+
+constexpr int kThreads = 128;
+constexpr int kWarps = kThreads / 32;
+constexpr int kWindow = 32;
+constexpr double kBig = 2.037035976334486e90;     // 2^300
+constexpr double kShrink = 2.409919865102884e-181;  // 2^-600
+
+// Seed of one lane: value = sign * 2^f carried as v * 2^(600 k), k <= 0.
+__device__ __forceinline__ void seed_lane(const double *__restrict__ sd, double lsin, double lcos,
+                                          double &v, int &k)
+{
+    double f = sd[0];
+    if (sd[2] != 0.0) f += sd[2] * lcos;
+    if (sd[3] != 0.0) f += sd[3] * lsin;
+    if (!(f > -1.0e300)) {
+        v = 0.0;
+        k = 0;
+        return;
+    }
+    int kk = 0;
+    if (f < -300.0) kk = (int)floor((f + 300.0) / 600.0);
+    v = sd[1] * exp2(f - 600.0 * (double)kk);
+    k = kk;
+}
+
+__device__ __forceinline__ void rescale(double &v, double &vp, int &k)
+{
+    if (k < 0 && fabs(v) > kBig) {
+        v *= kShrink;
+        vp *= kShrink;
+        ++k;
+    }
+}
+
+// Recurrence coefficients for target degree l (lambda_l from lambda_{l-1}, lambda_{l-2}):
+//   lambda_l = alpha (x - m s'/((l-1) l)) lambda_{l-1} - beta lambda_{l-2}.
+struct Coef {
+    double alpha, beta, c0;  // c0 = 2 m / ((l-1) l) for spin 2, 0 for spin 0
+};
+
+__device__ __forceinline__ Coef make_coef(int l, int m, int s, int l0)
+{
+    Coef c;
+    double dl = (double)l, dm = (double)m, ds = (double)s;
+    double den = sqrt((dl * dl - dm * dm) * (dl * dl - ds * ds));
+    c.alpha = sqrt((2.0 * dl + 1.0) * (2.0 * dl - 1.0)) * dl / den;
+    if (l >= l0 + 2) {
+        double dl1 = dl - 1.0;
+        double num = sqrt((dl1 * dl1 - dm * dm) * (dl1 * dl1 - ds * ds));
+        c.beta = sqrt((2.0 * dl + 1.0) / (2.0 * dl - 3.0)) * dl * num / (dl1 * den);
+    } else {
+        c.beta = 0.0;
+    }
+    c.c0 = (s != 0 && l >= 2) ? 2.0 * dm / ((dl - 1.0) * dl) : 0.0;
+    return c;
+}
+
+template <typename T, int V>
+__device__ __forceinline__ T warp_reduce_scatter(T (&v)[V], int lane)
+{
+#pragma unroll
+    for (int h = V / 2; h >= 1; h >>= 1) {
+        const bool upper = (lane & h) != 0;
+#pragma unroll
+        for (int i = 0; i < h; ++i) {
+            T send = upper ? v[i] : v[i + h];
+            T keep = upper ? v[i + h] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, h);
+        }
+    }
+    T r = v[0];
+#pragma unroll
+    for (int h = V; h < 32; h <<= 1) r += __shfl_xor_sync(0xffffffffu, r, h);
+    return r;
+}
+
+__device__ __forceinline__ int64_t alm_index(int64_t lmax, int64_t l, int64_t m)
+{
+    return m * (2 * lmax + 1 - m) / 2 + l;
+}
+
+// ---------------------------------------------------------------- analysis
+
+// NC components per CTA (spin 0: NC maps; spin 2: NC = 2, one (Q, U) pair).
+// NV values per degree: spin 0: 2 NC; spin 2: 8.  LB degrees per reduce-scatter block.
+template <typename T, int SPIN, int NC, int R>
+__global__ void __launch_bounds__(kThreads) k_legendre_ana(
+    int64_t nside, int64_t lmax, int64_t ncomp, const double *__restrict__ geom,
+    const double *__restrict__ seeds, const T *__restrict__ rhs, double *__restrict__ alm,
+    double scale)
+{
+    constexpr int NV = SPIN == 0 ? 2 * NC : 8;
+    constexpr int LB = 32 / NV;
+    constexpr int NVAR = SPIN == 0 ? 1 : 2;
+    static_assert(LB * NV == 32, "reduce-scatter width");
+    __shared__ Coef coef[kWindow];
+    __shared__ double red[kWarps][kWindow * NV];
+
+    const int64_t L = lmax + 1, nlanes = 2 * nside, nelem = L * (L + 1) / 2;
+    const int m = blockIdx.y;
+    const int64_t c0 = (int64_t)blockIdx.z * NC;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int l0 = SPIN == 0 ? m : (m > 2 ? m : 2);
+    if (l0 > lmax) return;
+
+    double x[R], v[NVAR][R], vp[NVAR][R];
+    int kx[NVAR][R];
+    T rh[R][NC][4];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int64_t j = (int64_t)blockIdx.x * kThreads * R + r * kThreads + threadIdx.x;
+        const bool ok = j < nlanes;
+        x[r] = ok ? geom[j] : 0.0;
+        const double ls = ok ? geom[nlanes + j] : 0.0, lc = ok ? geom[2 * nlanes + j] : 0.0;
+#pragma unroll
+        for (int q = 0; q < NVAR; ++q) {
+            const int var = SPIN == 0 ? 0 : 1 + q;  // 1: s' = -2 (lambda+), 2: s' = +2 (lambda-)
+            if (ok) {
+                seed_lane(seeds + ((int64_t)var * L + m) * 4, ls, lc, v[q][r], kx[q][r]);
+            } else {
+                v[q][r] = 0.0;
+                kx[q][r] = 0;
+            }
+            vp[q][r] = 0.0;
+        }
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                rh[r][c][e] = (ok && c0 + c < ncomp)
+                                  ? rhs[(((int64_t)m * nlanes + j) * ncomp + c0 + c) * 4 + e]
+                                  : (T)0;
+    }
+
+    for (int lb = l0; lb < L; lb += kWindow) {
+        if (threadIdx.x < kWindow) {
+            const int l = lb + threadIdx.x;
+            coef[threadIdx.x] = make_coef(l, m, SPIN, l0);
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int i = 0; i < kWindow; i += LB) {
+            T acc[LB * NV];
+#pragma unroll
+            for (int q = 0; q < LB * NV; ++q) acc[q] = (T)0;
+#pragma unroll
+            for (int s = 0; s < LB; ++s) {
+                const int l = lb + i + s;
+                if (l < L) {
+                    if (l > l0) {
+                        const Coef cf = coef[i + s];
+#pragma unroll
+                        for (int r = 0; r < R; ++r) {
+                            if (SPIN == 0) {
+                                double nv = cf.alpha * (x[r] * v[0][r]) - cf.beta * vp[0][r];
+                                vp[0][r] = v[0][r];
+                                v[0][r] = nv;
+                                rescale(v[0][r], vp[0][r], kx[0][r]);
+                            } else {
+                                // s' = -2: x - m s'/((l-1)l) = x + c0 ; s' = +2: x - c0
+                                double nva = cf.alpha * ((x[r] + cf.c0) * v[0][r]) - cf.beta * vp[0][r];
+                                double nvb = cf.alpha * ((x[r] - cf.c0) * v[1][r]) - cf.beta * vp[1][r];
+                                vp[0][r] = v[0][r];
+                                v[0][r] = nva;
+                                vp[1][r] = v[1][r];
+                                v[1][r] = nvb;
+                                rescale(v[0][r], vp[0][r], kx[0][r]);
+                                rescale(v[1][r], vp[1][r], kx[1][r]);
+                            }
+                        }
+                    }
+                    const int par = (l + m) & 1;
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        if (SPIN == 0) {
+                            const T val = kx[0][r] == 0 ? (T)v[0][r] : (T)0;
+#pragma unroll
+                            for (int c = 0; c < NC; ++c) {
+                                const T hr = par ? rh[r][c][2] : rh[r][c][0];
+                                const T hi = par ? rh[r][c][3] : rh[r][c][1];
+                                acc[s * NV + 2 * c] += val * hr;
+                                acc[s * NV + 2 * c + 1] += val * hi;
+                            }
+                        } else {
+                            const double lp = kx[0][r] == 0 ? v[0][r] : 0.0;
+                            const double lm = kx[1][r] == 0 ? v[1][r] : 0.0;
+                            const T f1 = (T)(0.5 * (lp + lm)), f2 = (T)(0.5 * (lp - lm));
+                            // same-parity side P = Sum (even) / Diff (odd); other side D
+                            const T qpr = par ? rh[r][0][2] : rh[r][0][0];
+                            const T qpi = par ? rh[r][0][3] : rh[r][0][1];
+                            const T upr = par ? rh[r][1][2] : rh[r][1][0];
+                            const T upi = par ? rh[r][1][3] : rh[r][1][1];
+                            const T qdr = par ? rh[r][0][0] : rh[r][0][2];
+                            const T qdi = par ? rh[r][0][1] : rh[r][0][3];
+                            const T udr = par ? rh[r][1][0] : rh[r][1][2];
+                            const T udi = par ? rh[r][1][1] : rh[r][1][3];
+                            acc[s * NV + 0] += f1 * qpr;
+                            acc[s * NV + 1] += f1 * qpi;
+                            acc[s * NV + 2] += f1 * upr;
+                            acc[s * NV + 3] += f1 * upi;
+                            acc[s * NV + 4] += f2 * qdr;
+                            acc[s * NV + 5] += f2 * qdi;
+                            acc[s * NV + 6] += f2 * udr;
+                            acc[s * NV + 7] += f2 * udi;
+                        }
+                    }
+                }
+            }
+            const T tot = warp_reduce_scatter<T, LB * NV>(acc, lane);
+            red[warp][i * NV + lane] = (double)tot;
+        }
+        __syncthreads();
+        if (threadIdx.x < kWindow) {
+            const int l = lb + threadIdx.x;
+            if (l < L) {
+                double sv[NV];
+#pragma unroll
+                for (int q = 0; q < NV; ++q) {
+                    double t = 0.0;
+#pragma unroll
+                    for (int w = 0; w < kWarps; ++w) t += red[w][threadIdx.x * NV + q];
+                    sv[q] = t;
+                }
+                const int64_t idx = alm_index(lmax, l, m);
+                if (SPIN == 0) {
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) {
+                        if (c0 + c < ncomp) {
+                            double *a = alm + 2 * ((c0 + c) * nelem + idx);
+                            atomicAdd(a, scale * sv[2 * c]);
+                            atomicAdd(a + 1, scale * sv[2 * c + 1]);
+                        }
+                    }
+                } else {
+                    // E = -(a1 + i-rotated a2), B likewise (see the docstring of gm_legendre_analysis)
+                    const int64_t f = c0 / 2;
+                    double *e = alm + 2 * ((2 * f) * nelem + idx);
+                    double *b = alm + 2 * ((2 * f + 1) * nelem + idx);
+                    atomicAdd(e, -scale * (sv[0] - sv[7]));
+                    atomicAdd(e + 1, -scale * (sv[1] + sv[6]));
+                    atomicAdd(b, -scale * (sv[2] + sv[5]));
+                    atomicAdd(b + 1, -scale * (sv[3] - sv[4]));
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- synthesis
+
+template <typename T, int SPIN, int NC, int R>
+__global__ void __launch_bounds__(kThreads) k_legendre_syn(
+    int64_t nside, int64_t lmax, int64_t ncomp, const double *__restrict__ geom,
+    const double *__restrict__ seeds, const double *__restrict__ alm, T *__restrict__ syn)
+{
+    constexpr int NVAR = SPIN == 0 ? 1 : 2;
+    constexpr int NA = SPIN == 0 ? NC : 2;  // complex alm rows per degree (maps, or E and B)
+    constexpr int NACC = SPIN == 0 ? 4 * NC : 16;
+    __shared__ Coef coef[2][kWindow];
+    __shared__ T aw[2][kWindow][NA][2];
+
+    const int64_t L = lmax + 1, nlanes = 2 * nside, nelem = L * (L + 1) / 2;
+    const int m = blockIdx.y;
+    const int64_t c0 = (int64_t)blockIdx.z * NC;
+    const int l0 = SPIN == 0 ? m : (m > 2 ? m : 2);
+
+    double x[R], v[NVAR][R], vp[NVAR][R];
+    int kx[NVAR][R];
+    T acc[R][NACC];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int64_t j = (int64_t)blockIdx.x * kThreads * R + r * kThreads + threadIdx.x;
+        const bool ok = j < nlanes && l0 <= lmax;
+        x[r] = ok ? geom[j] : 0.0;
+        const double ls = ok ? geom[nlanes + j] : 0.0, lc = ok ? geom[2 * nlanes + j] : 0.0;
+#pragma unroll
+        for (int q = 0; q < NVAR; ++q) {
+            const int var = SPIN == 0 ? 0 : 1 + q;
+            if (ok) {
+                seed_lane(seeds + ((int64_t)var * L + m) * 4, ls, lc, v[q][r], kx[q][r]);
+            } else {
+                v[q][r] = 0.0;
+                kx[q][r] = 0;
+            }
+            vp[q][r] = 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < NACC; ++q) acc[r][q] = (T)0;
+    }
+
+    int buf = 0;
+    for (int lb = l0; lb < L; lb += kWindow, buf ^= 1) {
+        if (threadIdx.x < kWindow) {
+            const int l = lb + threadIdx.x;
+            coef[buf][threadIdx.x] = make_coef(l, m, SPIN, l0);
+#pragma unroll
+            for (int a = 0; a < NA; ++a) {
+                T re = 0, im = 0;
+                if (l < L) {
+                    const int64_t row = SPIN == 0 ? c0 + a : c0 + a;  // spin 2: rows E, B of field c0/2
+                    if (row < ncomp) {
+                        const double *p = alm + 2 * (row * nelem + alm_index(lmax, l, m));
+                        re = (T)p[0];
+                        im = (T)p[1];
+                    }
+                }
+                aw[buf][threadIdx.x][a][0] = re;
+                aw[buf][threadIdx.x][a][1] = im;
+            }
+        }
+        __syncthreads();
+        const int lend = (lb + kWindow < L) ? kWindow : (int)(L - lb);
+#pragma unroll 4
+        for (int s = 0; s < lend; ++s) {
+            const int l = lb + s;
+            if (l > l0) {
+                const Coef cf = coef[buf][s];
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    if (SPIN == 0) {
+                        double nv = cf.alpha * (x[r] * v[0][r]) - cf.beta * vp[0][r];
+                        vp[0][r] = v[0][r];
+                        v[0][r] = nv;
+                        rescale(v[0][r], vp[0][r], kx[0][r]);
+                    } else {
+                        double nva = cf.alpha * ((x[r] + cf.c0) * v[0][r]) - cf.beta * vp[0][r];
+                        double nvb = cf.alpha * ((x[r] - cf.c0) * v[1][r]) - cf.beta * vp[1][r];
+                        vp[0][r] = v[0][r];
+                        v[0][r] = nva;
+                        vp[1][r] = v[1][r];
+                        v[1][r] = nvb;
+                        rescale(v[0][r], vp[0][r], kx[0][r]);
+                        rescale(v[1][r], vp[1][r], kx[1][r]);
+                    }
+                }
+            }
+            const int par = (l + m) & 1;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (SPIN == 0) {
+                    const T val = kx[0][r] == 0 ? (T)v[0][r] : (T)0;
+                    const T ve = par ? (T)0 : val, vo = par ? val : (T)0;
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) {
+                        const T ar = aw[buf][s][c][0], ai = aw[buf][s][c][1];
+                        acc[r][4 * c] += ve * ar;
+                        acc[r][4 * c + 1] += ve * ai;
+                        acc[r][4 * c + 2] += vo * ar;
+                        acc[r][4 * c + 3] += vo * ai;
+                    }
+                } else {
+                    const double lp = kx[0][r] == 0 ? v[0][r] : 0.0;
+                    const double lm = kx[1][r] == 0 ? v[1][r] : 0.0;
+                    const T f1 = (T)(0.5 * (lp + lm)), f2 = (T)(0.5 * (lp - lm));
+                    const T er = aw[buf][s][0][0], ei = aw[buf][s][0][1];
+                    const T br = aw[buf][s][1][0], bi = aw[buf][s][1][1];
+                    // per parity: [S1E re, im, S1B re, im, S2E re, im, S2B re, im]
+                    const T f1e = par ? (T)0 : f1, f1o = par ? f1 : (T)0;
+                    const T f2e = par ? (T)0 : f2, f2o = par ? f2 : (T)0;
+                    acc[r][0] += f1e * er;
+                    acc[r][1] += f1e * ei;
+                    acc[r][2] += f1e * br;
+                    acc[r][3] += f1e * bi;
+                    acc[r][4] += f2e * er;
+                    acc[r][5] += f2e * ei;
+                    acc[r][6] += f2e * br;
+                    acc[r][7] += f2e * bi;
+                    acc[r][8] += f1o * er;
+                    acc[r][9] += f1o * ei;
+                    acc[r][10] += f1o * br;
+                    acc[r][11] += f1o * bi;
+                    acc[r][12] += f2o * er;
+                    acc[r][13] += f2o * ei;
+                    acc[r][14] += f2o * br;
+                    acc[r][15] += f2o * bi;
+                }
+            }
+        }
+    }
+
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int64_t j = (int64_t)blockIdx.x * kThreads * R + r * kThreads + threadIdx.x;
+        if (j >= nlanes) continue;
+        if (SPIN == 0) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                if (c0 + c >= ncomp) continue;
+                T *o = syn + (((int64_t)m * nlanes + j) * ncomp + c0 + c) * 4;
+                const T er = acc[r][4 * c], ei = acc[r][4 * c + 1];
+                const T orr = acc[r][4 * c + 2], oi = acc[r][4 * c + 3];
+                o[0] = er + orr;
+                o[1] = ei + oi;
+                o[2] = er - orr;
+                o[3] = ei - oi;
+            }
+        } else {
+            const T *e = &acc[r][0];
+            const T *od = &acc[r][8];
+            // north: sums; south: F1 -> e - o, F2 -> o - e
+            T s1e_n[2] = {e[0] + od[0], e[1] + od[1]}, s1b_n[2] = {e[2] + od[2], e[3] + od[3]};
+            T s2e_n[2] = {e[4] + od[4], e[5] + od[5]}, s2b_n[2] = {e[6] + od[6], e[7] + od[7]};
+            T s1e_s[2] = {e[0] - od[0], e[1] - od[1]}, s1b_s[2] = {e[2] - od[2], e[3] - od[3]};
+            T s2e_s[2] = {od[4] - e[4], od[5] - e[5]}, s2b_s[2] = {od[6] - e[6], od[7] - e[7]};
+            T *oq = syn + (((int64_t)m * nlanes + j) * ncomp + c0) * 4;
+            T *ou = oq + 4;
+            // Q~ = -(S1E + i S2B), U~ = -(S1B - i S2E)
+            oq[0] = -(s1e_n[0] - s2b_n[1]);
+            oq[1] = -(s1e_n[1] + s2b_n[0]);
+            oq[2] = -(s1e_s[0] - s2b_s[1]);
+            oq[3] = -(s1e_s[1] + s2b_s[0]);
+            ou[0] = -(s1b_n[0] + s2e_n[1]);
+            ou[1] = -(s1b_n[1] - s2e_n[0]);
+            ou[2] = -(s1b_s[0] + s2e_s[1]);
+            ou[3] = -(s1b_s[1] - s2e_s[0]);
+        }
+    }
+}
+
+}  // namespace gm
+
+using namespace gm;
+
+extern "C" int64_t gm_seed_table_len(int64_t L) { return 3 * 4 * L; }
+
+template <typename T, int SPIN, int NC, int R>
+static int launch_ana(int64_t nside, int64_t lmax, int64_t ncomp, const double *geom,
+                      const double *seeds, const void *rhs, double *alm, double scale,
+                      cudaStream_t s)
+{
+    const int64_t nlanes = 2 * nside;
+    dim3 grid((unsigned)((nlanes + kThreads * R - 1) / (kThreads * R)), (unsigned)(lmax + 1),
+              (unsigned)((ncomp + NC - 1) / NC));
+    k_legendre_ana<T, SPIN, NC, R><<<grid, kThreads, 0, s>>>(nside, lmax, ncomp, geom, seeds,
+                                                             (const T *)rhs, alm, scale);
+    return check_launch("gm_legendre_analysis");
+}
+
+template <typename T, int SPIN, int NC, int R>
+static int launch_syn(int64_t nside, int64_t lmax, int64_t ncomp, const double *geom,
+                      const double *seeds, const double *alm, void *syn, cudaStream_t s)
+{
+    const int64_t nlanes = 2 * nside;
+    dim3 grid((unsigned)((nlanes + kThreads * R - 1) / (kThreads * R)), (unsigned)(lmax + 1),
+              (unsigned)((ncomp + NC - 1) / NC));
+    k_legendre_syn<T, SPIN, NC, R><<<grid, kThreads, 0, s>>>(nside, lmax, ncomp, geom, seeds, alm,
+                                                             (T *)syn);
+    return check_launch("gm_legendre_synthesis");
+}
+
+template <typename T>
+static int dispatch_ana(int spin, int64_t nside, int64_t lmax, int64_t ncomp, const double *geom,
+                        const double *seeds, const void *rhs, double *alm, double scale,
+                        cudaStream_t s)
+{
+    if (spin == 0) {
+        if (ncomp == 1)
+            return launch_ana<T, 0, 1, 4>(nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s);
+        if (ncomp == 2)
+            return launch_ana<T, 0, 2, 4>(nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s);
+        return launch_ana<T, 0, 4, 2>(nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s);
+    }
+    return launch_ana<T, 2, 2, 2>(nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s);
+}
+
+template <typename T>
+static int dispatch_syn(int spin, int64_t nside, int64_t lmax, int64_t ncomp, const double *geom,
+                        const double *seeds, const double *alm, void *syn, cudaStream_t s)
+{
+    if (spin == 0) {
+        if (ncomp == 1) return launch_syn<T, 0, 1, 2>(nside, lmax, ncomp, geom, seeds, alm, syn, s);
+        if (ncomp == 2) return launch_syn<T, 0, 2, 2>(nside, lmax, ncomp, geom, seeds, alm, syn, s);
+        return launch_syn<T, 0, 4, 1>(nside, lmax, ncomp, geom, seeds, alm, syn, s);
+    }
+    return launch_syn<T, 2, 2, 2>(nside, lmax, ncomp, geom, seeds, alm, syn, s);
+}
+
+extern "C" int gm_legendre_analysis(int precision, int spin, int64_t nside, int64_t lmax,
+                                    int64_t ncomp, const double *lane_geom, const double *seeds,
+                                    const void *rhs, double *alm, double scale, void *stream)
+{
+    if (nside < 1 || lmax < 0 || lmax + 1 > 65535 || ncomp < 1 || ncomp > 65535)
+        return GM_ERR_BAD_SHAPE;
+    if (spin != 0 && spin != 2) return GM_ERR_UNSUPPORTED;
+    if (spin == 2 && (ncomp % 2)) return GM_ERR_BAD_SHAPE;
+    if (!lane_geom || !seeds || !rhs || !alm) return GM_ERR_BAD_PTR;
+    cudaStream_t s = as_stream(stream);
+    if (precision == GM_FP64)
+        return dispatch_ana<double>(spin, nside, lmax, ncomp, lane_geom, seeds, rhs, alm, scale, s);
+    if (precision == GM_MIXED)
+        return dispatch_ana<float>(spin, nside, lmax, ncomp, lane_geom, seeds, rhs, alm, scale, s);
+    return GM_ERR_UNSUPPORTED;
+}
+
+extern "C" int gm_legendre_synthesis(int precision, int spin, int64_t nside, int64_t lmax,
+                                     int64_t ncomp, const double *lane_geom, const double *seeds,
+                                     const double *alm, void *syn, void *stream)
+{
+    if (nside < 1 || lmax < 0 || lmax + 1 > 65535 || ncomp < 1 || ncomp > 65535)
+        return GM_ERR_BAD_SHAPE;
+    if (spin != 0 && spin != 2) return GM_ERR_UNSUPPORTED;
+    if (spin == 2 && (ncomp % 2)) return GM_ERR_BAD_SHAPE;
+    if (!lane_geom || !seeds || !alm || !syn) return GM_ERR_BAD_PTR;
+    cudaStream_t s = as_stream(stream);
+    if (precision == GM_FP64)
+        return dispatch_syn<double>(spin, nside, lmax, ncomp, lane_geom, seeds, alm, syn, s);
+    if (precision == GM_MIXED)
+        return dispatch_syn<float>(spin, nside, lmax, ncomp, lane_geom, seeds, alm, syn, s);
+    return GM_ERR_UNSUPPORTED;
+}

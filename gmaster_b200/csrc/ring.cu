@@ -1,0 +1,577 @@
+// Azimuthal (ring) stage of the HEALPix spherical-harmonic transforms, sm_100a.
+//
+// One CTA transforms one ring of one map component entirely in shared memory:
+// a real ring of nphi = 4i samples is packed into a complex sequence of length
+// h = nphi/2 (even samples real, odd samples imaginary), transformed by a
+// self-sorting Stockham FFT of mixed radix (4, 2, then odd primes; a generic
+// radix-p stage for large prime factors), and unpacked.  Loads and stores of
+// pixels and spectra are coalesced along the ring / along m.
+//
+// Replaces the reference's XLA-lowered ring stage (gmaster/_sht/rings.py:251-299
+// forward, :477-524 inverse: a cuFFT of the equatorial belt plus Bluestein chirp-Z
+// convolutions for the polar caps) and its ring-fold residual kernel
+// (gmaster/_native/cuda/march_v2.cu:426-493).
+#include <math.h>
+
+#include "gm_common.cuh"
+
+namespace gm {
+
+// ---------------------------------------------------------------- twiddles
+
+// tw64[i(i-1) + k] = exp(-2 pi i k / (4 i)), k < 2 i, followed by the float copy.
+__global__ void k_twiddles(int64_t nside, double2 *tw64, float2 *tw32)
+{
+    int64_t i = blockIdx.y + 1;
+    int64_t half = 2 * i;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < half;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        double s, c;
+        sincospi(-(double)k / (double)half, &s, &c);  // -2 pi k / (4 i) = -pi k / (2 i)
+        int64_t idx = i * (i - 1) + k;
+        tw64[idx] = make_double2(c, s);
+        tw32[idx] = make_float2((float)c, (float)s);
+    }
+}
+
+template <typename T2> struct TwTable;
+template <> struct TwTable<double2> {
+    static __device__ __forceinline__ const double2 *get(const void *tw, int64_t cnt)
+    {
+        return reinterpret_cast<const double2 *>(tw);
+    }
+};
+template <> struct TwTable<float2> {
+    static __device__ __forceinline__ const float2 *get(const void *tw, int64_t cnt)
+    {
+        return reinterpret_cast<const float2 *>(reinterpret_cast<const double2 *>(tw) + cnt);
+    }
+};
+
+// omega_h^e for a ring of half-length h (n = 2h): tw holds omega_n^k, k < h,
+// and omega_n^{k+h} = -omega_n^k.  `sign` > 0 conjugates (inverse transform).
+template <typename T2>
+__device__ __forceinline__ T2 twiddle(const T2 *__restrict__ tw, int h, int64_t e, int sign)
+{
+    int64_t k = 2 * (e % h);
+    T2 w;
+    if (k < h) {
+        w = __ldg(tw + k);
+    } else {
+        w = __ldg(tw + (k - h));
+        w.x = -w.x;
+        w.y = -w.y;
+    }
+    if (sign > 0) w.y = -w.y;
+    return w;
+}
+
+// omega_n^k for k < n (n = 2h).
+template <typename T2>
+__device__ __forceinline__ T2 twiddle_n(const T2 *__restrict__ tw, int h, int k, int sign)
+{
+    T2 w;
+    if (k < h) {
+        w = __ldg(tw + k);
+    } else {
+        w = __ldg(tw + (k - h));
+        w.x = -w.x;
+        w.y = -w.y;
+    }
+    if (sign > 0) w.y = -w.y;
+    return w;
+}
+
+// ---------------------------------------------------------------- FFT core
+
+__device__ int factorize(int h, int *rad)
+{
+    int n = 0;
+    while (h % 4 == 0) { rad[n++] = 4; h /= 4; }
+    if (h % 2 == 0) { rad[n++] = 2; h /= 2; }
+    for (int p = 3; p * p <= h; p += 2)
+        while (h % p == 0) { rad[n++] = p; h /= p; }
+    if (h > 1) rad[n++] = h;
+    return n;
+}
+
+// Multiply by sign * i.
+template <typename T2>
+__device__ __forceinline__ T2 mul_i(T2 z, int sign)
+{
+    T2 r;
+    r.x = -sign * z.y;
+    r.y = sign * z.x;
+    return r;
+}
+
+// One Stockham stage: out[k' Lp + j + Ls v] = sum_q omega_p^{q v} omega_Lp^{q j} in[(k' + r q) Ls + j]
+// with Lp = Ls p and r = h / Lp.  Butterflies (k', j) are spread over the CTA.
+template <typename T2>
+__device__ void stockham_stage(const T2 *__restrict__ in, T2 *__restrict__ out, int h, int p,
+                               int Ls, const T2 *__restrict__ tw, int sign)
+{
+    const int Lp = Ls * p;
+    const int r = h / Lp;
+    const int nb = h / p;
+    if (p == 4) {
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+            int kk = b / Ls, j = b - kk * Ls;
+            T2 x0 = in[kk * Ls + j];
+            T2 x1 = in[(kk + r) * Ls + j];
+            T2 x2 = in[(kk + 2 * r) * Ls + j];
+            T2 x3 = in[(kk + 3 * r) * Ls + j];
+            if (Ls > 1) {
+                int64_t e = (int64_t)j * r;
+                x1 = cmul(x1, twiddle(tw, h, e, sign));
+                x2 = cmul(x2, twiddle(tw, h, 2 * e, sign));
+                x3 = cmul(x3, twiddle(tw, h, 3 * e, sign));
+            }
+            T2 a = cadd(x0, x2), bq = csub(x0, x2);
+            T2 c = cadd(x1, x3), d = mul_i(csub(x1, x3), sign);
+            T2 *o = out + kk * Lp + j;
+            o[0] = cadd(a, c);
+            o[Ls] = cadd(bq, d);
+            o[2 * Ls] = csub(a, c);
+            o[3 * Ls] = csub(bq, d);
+        }
+    } else if (p == 2) {
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+            int kk = b / Ls, j = b - kk * Ls;
+            T2 x0 = in[kk * Ls + j];
+            T2 x1 = in[(kk + r) * Ls + j];
+            if (Ls > 1) x1 = cmul(x1, twiddle(tw, h, (int64_t)j * r, sign));
+            T2 *o = out + kk * Lp + j;
+            o[0] = cadd(x0, x1);
+            o[Ls] = csub(x0, x1);
+        }
+    } else {
+        // generic radix: one output (k', j, v) per thread iteration, p terms each
+        for (int o = threadIdx.x; o < h; o += blockDim.x) {
+            int kk = o / Lp, jp = o - kk * Lp;
+            int j = jp % Ls;
+            T2 acc;
+            acc.x = 0;
+            acc.y = 0;
+            // term q: omega_Lp^{q jp} in[(kk + r q) Ls + j];  omega_Lp = omega_h^r
+            for (int q = 0; q < p; ++q) {
+                T2 x = in[(kk + r * q) * Ls + j];
+                int64_t e = ((int64_t)q * jp % Lp) * r;
+                T2 w = twiddle(tw, h, e, sign);
+                acc.x += x.x * w.x - x.y * w.y;
+                acc.y += x.x * w.y + x.y * w.x;
+            }
+            out[o] = acc;
+        }
+    }
+}
+
+// In-shared-memory FFT of length h (ping-pong between a and b); returns the buffer
+// holding the result.  Ends with a __syncthreads().
+template <typename T2>
+__device__ T2 *fft_shared(T2 *a, T2 *b, int h, const T2 *__restrict__ tw, int sign)
+{
+    __shared__ int rad[40];
+    __shared__ int nst;
+    if (threadIdx.x == 0) nst = factorize(h, rad);
+    __syncthreads();
+    int Ls = 1;
+    for (int s = 0; s < nst; ++s) {
+        int p = rad[s];
+        stockham_stage(a, b, h, p, Ls, tw, sign);
+        __syncthreads();
+        T2 *t = a;
+        a = b;
+        b = t;
+        Ls *= p;
+    }
+    return a;
+}
+
+// ---------------------------------------------------------------- analysis
+
+template <typename T, typename Tin>
+__global__ void __launch_bounds__(512) k_ring_analysis(int64_t nside, int64_t L,
+                                                       const Tin *__restrict__ maps,
+                                                       const void *__restrict__ twall,
+                                                       int64_t twcnt,
+                                                       const uint8_t *__restrict__ shifted,
+                                                       typename vec2<T>::type *__restrict__ out)
+{
+    using T2 = typename vec2<T>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int64_t r = blockIdx.x, c = blockIdx.y;
+    const int64_t nring = 4 * nside - 1, npix = 12 * nside * nside;
+    const int n = (int)ring_nphi(nside, r), h = n / 2;
+    const int64_t off = ring_offset(nside, r);
+    T2 *A = reinterpret_cast<T2 *>(smem_raw);
+    T2 *B = A + 2 * nside;
+    const T2 *tw = TwTable<T2>::get(twall, twcnt) + twiddle_offset(n);
+    const Tin *x = maps + c * npix + off;
+    for (int t = threadIdx.x; t < h; t += blockDim.x) {
+        T2 z;
+        z.x = (T)x[2 * t];
+        z.y = (T)x[2 * t + 1];
+        A[t] = z;
+    }
+    __syncthreads();
+    T2 *Z = fft_shared(A, B, h, tw, -1);
+    const T w = (T)(4.0 * M_PI / (double)npix);
+    const bool sh = shifted[r] != 0;
+    T2 *dst = out + (c * nring + r) * L;
+    for (int64_t m = threadIdx.x; m < L; m += blockDim.x) {
+        int k = (int)(m % n);
+        bool conj = k > h;
+        int kk = conj ? n - k : k;
+        // X[kk] = E + omega_n^kk O, E = (Z[kk] + conj Z[h-kk]) / 2, O = (Z[kk] - conj Z[h-kk]) / 2i
+        T2 za = Z[kk % h], zb = Z[(h - kk) % h];
+        T er = (za.x + zb.x) * (T)0.5, ei = (za.y - zb.y) * (T)0.5;
+        T orr = (za.y + zb.y) * (T)0.5, oi = -(za.x - zb.x) * (T)0.5;
+        T2 wn = twiddle_n(tw, h, kk, -1);
+        T xr = er + wn.x * orr - wn.y * oi;
+        T xi = ei + wn.x * oi + wn.y * orr;
+        if (conj) xi = -xi;
+        T pr = 1, pi = 0;
+        if (sh) {
+            // e^{-i m phi0}, phi0 = pi / n
+            if (sizeof(T) == 8) {
+                double s, cc;
+                sincospi(-(double)m / (double)n, &s, &cc);
+                pr = (T)cc;
+                pi = (T)s;
+            } else {
+                float s, cc;
+                sincospif(-(float)(m % (2 * n)) / (float)n, &s, &cc);
+                pr = (T)cc;
+                pi = (T)s;
+            }
+        }
+        T2 g;
+        g.x = w * (xr * pr - xi * pi);
+        g.y = w * (xr * pi + xi * pr);
+        dst[m] = g;
+    }
+}
+
+// ---------------------------------------------------------------- hemisphere pack
+
+template <typename T>
+__global__ void k_pack_rhs(int64_t nside, int64_t L, int64_t ncomp,
+                           const typename vec2<T>::type *__restrict__ spec, T *__restrict__ rhs)
+{
+    using T2 = typename vec2<T>::type;
+    __shared__ T tile[32][33][4];
+    const int64_t nlanes = 2 * nside, nring = 4 * nside - 1;
+    const int64_t m0 = (int64_t)blockIdx.x * 32, j0 = (int64_t)blockIdx.y * 32, c = blockIdx.z;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int jj = ty; jj < 32; jj += 8) {
+        int64_t j = j0 + jj, m = m0 + tx;
+        T v[4] = {0, 0, 0, 0};
+        if (j < nlanes && m < L) {
+            T2 gn = spec[(c * nring + north_ring(j)) * L + m];
+            T2 gs;
+            gs.x = 0;
+            gs.y = 0;
+            if (j != nlanes - 1) gs = spec[(c * nring + south_ring(nside, j)) * L + m];
+            v[0] = gn.x + gs.x;
+            v[1] = gn.y + gs.y;
+            v[2] = gn.x - gs.x;
+            v[3] = gn.y - gs.y;
+        }
+        for (int q = 0; q < 4; ++q) tile[jj][tx][q] = v[q];
+    }
+    __syncthreads();
+    for (int mm = ty; mm < 32; mm += 8) {
+        int64_t m = m0 + mm, j = j0 + tx;
+        if (j < nlanes && m < L) {
+            T *o = rhs + ((m * nlanes + j) * ncomp + c) * 4;
+            for (int q = 0; q < 4; ++q) o[q] = tile[tx][mm][q];
+        }
+    }
+}
+
+// ---------------------------------------------------------------- fold residual
+
+// Sum over the residue class k (mod n) of the synthesised coefficients of one ring
+// side (`part` 0 north, 2 south) with the alternating sign (-1)^{s t} of the ring
+// shift: P_k = sum_t (-1)^{s t} c(k + t n), |k + t n| < L, c(-m) = conj c(m).
+template <typename T>
+__device__ __forceinline__ void residue_sums(const T *__restrict__ syn, int64_t L, int64_t nlanes,
+                                             int64_t ncomp, int64_t j, int64_t c, int k, int n,
+                                             bool sh, bool two_sides, T *pn, T *ps)
+{
+    T nr = 0, ni = 0, sr = 0, si = 0;
+    // t >= 0 : m = k + t n in [0, L)
+    int t = 0;
+    for (int64_t m = k; m < L; m += n, ++t) {
+        const T *e = syn + ((m * nlanes + j) * ncomp + c) * 4;
+        T sg = (sh && (t & 1)) ? (T)-1 : (T)1;
+        nr += sg * e[0];
+        ni += sg * e[1];
+        if (two_sides) {
+            sr += sg * e[2];
+            si += sg * e[3];
+        }
+    }
+    // t < 0 : m = k - t' n (t' >= 1), order m < 0 with -m = t' n - k in (0, L)
+    t = -1;
+    for (int64_t mm = (int64_t)n - k; mm < L; mm += n, --t) {
+        if (mm == 0) continue;
+        const T *e = syn + ((mm * nlanes + j) * ncomp + c) * 4;
+        T sg = (sh && (t & 1)) ? (T)-1 : (T)1;
+        nr += sg * e[0];
+        ni -= sg * e[1];
+        if (two_sides) {
+            sr += sg * e[2];
+            si -= sg * e[3];
+        }
+    }
+    pn[0] = nr;
+    pn[1] = ni;
+    ps[0] = sr;
+    ps[1] = si;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_fold_residual(int64_t nside, int64_t L, int64_t ncomp,
+                                                       const T *__restrict__ syn,
+                                                       const T *__restrict__ rhs_map,
+                                                       const uint8_t *__restrict__ shifted,
+                                                       T *__restrict__ rhs_out)
+{
+    const int64_t j = blockIdx.x, c = blockIdx.y;
+    const int64_t nlanes = 2 * nside, npix = 12 * nside * nside;
+    const int n = (int)ring_nphi(nside, north_ring(j));
+    const bool sh = shifted[north_ring(j)] != 0;
+    const bool two = j != nlanes - 1;
+    const T wn = (T)(4.0 * M_PI / (double)npix * (double)n);
+    for (int k = threadIdx.x; k < n && k < L; k += blockDim.x) {
+        T pn[2], ps[2];
+        residue_sums(syn, L, nlanes, ncomp, j, c, k, n, sh, two, pn, ps);
+        int t = 0;
+        for (int64_t m = k; m < L; m += n, ++t) {
+            T sg = (sh && (t & 1)) ? -wn : wn;
+            T gnr = sg * pn[0], gni = sg * pn[1], gsr = sg * ps[0], gsi = sg * ps[1];
+            const int64_t idx = ((m * nlanes + j) * ncomp + c) * 4;
+            T *o = rhs_out + idx;
+            const T *b = rhs_map + idx;
+            o[0] = gnr + gsr - b[0];
+            o[1] = gni + gsi - b[1];
+            o[2] = gnr - gsr - b[2];
+            o[3] = gni - gsi - b[3];
+        }
+    }
+}
+
+// ---------------------------------------------------------------- synthesis
+
+template <typename T>
+__global__ void __launch_bounds__(512) k_ring_synthesis(int64_t nside, int64_t L, int64_t ncomp,
+                                                        const T *__restrict__ syn,
+                                                        const void *__restrict__ twall,
+                                                        int64_t twcnt,
+                                                        const uint8_t *__restrict__ shifted,
+                                                        double *__restrict__ maps)
+{
+    using T2 = typename vec2<T>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int64_t r = blockIdx.x, c = blockIdx.y;
+    const int64_t npix = 12 * nside * nside, nlanes = 2 * nside;
+    const int n = (int)ring_nphi(nside, r), h = n / 2;
+    const int64_t off = ring_offset(nside, r);
+    const bool south = r >= nlanes;
+    const int64_t j = south ? 4 * nside - 2 - r : r;
+    const bool sh = shifted[r] != 0;
+    T2 *A = reinterpret_cast<T2 *>(smem_raw);
+    T2 *B = A + 2 * nside;
+    const T2 *tw = TwTable<T2>::get(twall, twcnt) + twiddle_offset(n);
+    // Fold into the n-periodic spectrum C_k = e^{i pi s k / n} P_k and build
+    // Z'[k] = (C_k + C_{k+h}) + i (C_k - C_{k+h}) omega_n^{-k}, k < h.
+    const T *base = syn + (south ? 2 : 0);
+    for (int k = threadIdx.x; k < h; k += blockDim.x) {
+        T c0[2], c1[2], dummy[2];
+        residue_sums(base, L, nlanes, ncomp, j, c, k, n, sh, false, c0, dummy);
+        residue_sums(base, L, nlanes, ncomp, j, c, k + h, n, sh, false, c1, dummy);
+        T2 ck = make2<T2, T>(c0[0], c0[1]);
+        T2 ckh = make2<T2, T>(c1[0], c1[1]);
+        if (sh) {
+            if (sizeof(T) == 8) {
+                double s, cc;
+                sincospi((double)k / (double)n, &s, &cc);
+                ck = cmul(ck, make2<T2, T>((T)cc, (T)s));
+                sincospi((double)(k + h) / (double)n, &s, &cc);
+                ckh = cmul(ckh, make2<T2, T>((T)cc, (T)s));
+            } else {
+                float s, cc;
+                sincospif((float)k / (float)n, &s, &cc);
+                ck = cmul(ck, make2<T2, T>((T)cc, (T)s));
+                sincospif((float)(k + h) / (float)n, &s, &cc);
+                ckh = cmul(ckh, make2<T2, T>((T)cc, (T)s));
+            }
+        }
+        T2 sum = cadd(ck, ckh);
+        T2 dif = cmul(csub(ck, ckh), twiddle_n(tw, h, k, +1));
+        T2 z;
+        z.x = sum.x - dif.y;
+        z.y = sum.y + dif.x;
+        A[k] = z;
+    }
+    __syncthreads();
+    T2 *Z = fft_shared(A, B, h, tw, +1);
+    double *dst = maps + c * npix + off;
+    for (int t = threadIdx.x; t < h; t += blockDim.x) {
+        T2 z = Z[t];
+        dst[2 * t] = (double)z.x;
+        dst[2 * t + 1] = (double)z.y;
+    }
+}
+
+}  // namespace gm
+
+using namespace gm;
+
+extern "C" int64_t gm_ring_twiddle_count(int64_t nside) { return nside * (nside + 1); }
+
+extern "C" int gm_ring_twiddles(int64_t nside, void *tw, void *stream)
+{
+    if (nside < 1 || nside > 8192) return GM_ERR_BAD_SHAPE;
+    if (!tw) return GM_ERR_BAD_PTR;
+    int64_t cnt = gm_ring_twiddle_count(nside);
+    double2 *t64 = reinterpret_cast<double2 *>(tw);
+    float2 *t32 = reinterpret_cast<float2 *>(t64 + cnt);
+    int64_t gx = (2 * nside + 255) / 256;
+    if (gx > 64) gx = 64;
+    k_twiddles<<<dim3((unsigned)gx, (unsigned)nside), 256, 0, as_stream(stream)>>>(nside, t64, t32);
+    return check_launch("gm_ring_twiddles");
+}
+
+static size_t ring_smem_bytes(int precision, int64_t nside)
+{
+    size_t elem = precision == GM_FP64 ? sizeof(double2) : sizeof(float2);
+    return 2 * (size_t)(2 * nside) * elem;
+}
+
+static int ring_shape_ok(int precision, int64_t nside, int64_t L, int64_t ncomp)
+{
+    if (nside < 1 || L < 1 || ncomp < 1 || ncomp > 65535) return 0;
+    if (ring_smem_bytes(precision, nside) > 227 * 1024) return 0;
+    return 1;
+}
+
+template <typename K>
+static int set_smem(K kernel, size_t bytes)
+{
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)bytes);
+    if (e != cudaSuccess) {
+        set_error("cudaFuncSetAttribute", e);
+        return GM_ERR_LAUNCH;
+    }
+    return GM_OK;
+}
+
+extern "C" int gm_ring_analysis(int precision, int64_t nside, int64_t L, int64_t ncomp,
+                                const void *maps, int map_dtype_bytes, const void *tw,
+                                const uint8_t *shifted, void *ringspec, void *stream)
+{
+    if (!ring_shape_ok(precision, nside, L, ncomp)) return GM_ERR_BAD_SHAPE;
+    if (!maps || !tw || !shifted || !ringspec) return GM_ERR_BAD_PTR;
+    if (map_dtype_bytes != 8 && map_dtype_bytes != 4) return GM_ERR_UNSUPPORTED;
+    const int64_t nring = 4 * nside - 1, cnt = gm_ring_twiddle_count(nside);
+    size_t smem = ring_smem_bytes(precision, nside);
+    int threads = nside >= 256 ? 512 : 128;
+    dim3 grid((unsigned)nring, (unsigned)ncomp);
+    cudaStream_t s = as_stream(stream);
+    int st;
+    if (precision == GM_FP64) {
+        if (map_dtype_bytes == 8) {
+            if ((st = set_smem(k_ring_analysis<double, double>, smem))) return st;
+            k_ring_analysis<double, double><<<grid, threads, smem, s>>>(
+                nside, L, (const double *)maps, tw, cnt, shifted, (double2 *)ringspec);
+        } else {
+            if ((st = set_smem(k_ring_analysis<double, float>, smem))) return st;
+            k_ring_analysis<double, float><<<grid, threads, smem, s>>>(
+                nside, L, (const float *)maps, tw, cnt, shifted, (double2 *)ringspec);
+        }
+    } else if (precision == GM_MIXED) {
+        if (map_dtype_bytes == 8) {
+            if ((st = set_smem(k_ring_analysis<float, double>, smem))) return st;
+            k_ring_analysis<float, double><<<grid, threads, smem, s>>>(
+                nside, L, (const double *)maps, tw, cnt, shifted, (float2 *)ringspec);
+        } else {
+            if ((st = set_smem(k_ring_analysis<float, float>, smem))) return st;
+            k_ring_analysis<float, float><<<grid, threads, smem, s>>>(
+                nside, L, (const float *)maps, tw, cnt, shifted, (float2 *)ringspec);
+        }
+    } else {
+        return GM_ERR_UNSUPPORTED;
+    }
+    return check_launch("gm_ring_analysis");
+}
+
+extern "C" int gm_pack_rhs(int precision, int64_t nside, int64_t L, int64_t ncomp,
+                           const void *ringspec, void *rhs, void *stream)
+{
+    if (nside < 1 || L < 1 || ncomp < 1 || ncomp > 65535) return GM_ERR_BAD_SHAPE;
+    if (!ringspec || !rhs) return GM_ERR_BAD_PTR;
+    const int64_t nlanes = 2 * nside;
+    dim3 grid((unsigned)((L + 31) / 32), (unsigned)((nlanes + 31) / 32), (unsigned)ncomp);
+    dim3 block(32, 8);
+    cudaStream_t s = as_stream(stream);
+    if (precision == GM_FP64)
+        k_pack_rhs<double><<<grid, block, 0, s>>>(nside, L, ncomp, (const double2 *)ringspec,
+                                                  (double *)rhs);
+    else if (precision == GM_MIXED)
+        k_pack_rhs<float><<<grid, block, 0, s>>>(nside, L, ncomp, (const float2 *)ringspec,
+                                                 (float *)rhs);
+    else
+        return GM_ERR_UNSUPPORTED;
+    return check_launch("gm_pack_rhs");
+}
+
+extern "C" int gm_fold_residual(int precision, int64_t nside, int64_t L, int64_t ncomp,
+                                const void *syn, const void *rhs_map, const uint8_t *shifted,
+                                void *rhs_out, void *stream)
+{
+    if (nside < 1 || L < 1 || ncomp < 1 || ncomp > 65535) return GM_ERR_BAD_SHAPE;
+    if (!syn || !rhs_map || !shifted || !rhs_out) return GM_ERR_BAD_PTR;
+    dim3 grid((unsigned)(2 * nside), (unsigned)ncomp);
+    cudaStream_t s = as_stream(stream);
+    if (precision == GM_FP64)
+        k_fold_residual<double><<<grid, 256, 0, s>>>(nside, L, ncomp, (const double *)syn,
+                                                     (const double *)rhs_map, shifted,
+                                                     (double *)rhs_out);
+    else if (precision == GM_MIXED)
+        k_fold_residual<float><<<grid, 256, 0, s>>>(nside, L, ncomp, (const float *)syn,
+                                                    (const float *)rhs_map, shifted,
+                                                    (float *)rhs_out);
+    else
+        return GM_ERR_UNSUPPORTED;
+    return check_launch("gm_fold_residual");
+}
+
+extern "C" int gm_ring_synthesis(int precision, int64_t nside, int64_t L, int64_t ncomp,
+                                 const void *syn, const void *tw, const uint8_t *shifted,
+                                 double *maps, void *stream)
+{
+    if (!ring_shape_ok(precision, nside, L, ncomp)) return GM_ERR_BAD_SHAPE;
+    if (!syn || !tw || !shifted || !maps) return GM_ERR_BAD_PTR;
+    const int64_t nring = 4 * nside - 1, cnt = gm_ring_twiddle_count(nside);
+    size_t smem = ring_smem_bytes(precision, nside);
+    int threads = nside >= 256 ? 512 : 128;
+    dim3 grid((unsigned)nring, (unsigned)ncomp);
+    cudaStream_t s = as_stream(stream);
+    int st;
+    if (precision == GM_FP64) {
+        if ((st = set_smem(k_ring_synthesis<double>, smem))) return st;
+        k_ring_synthesis<double><<<grid, threads, smem, s>>>(nside, L, ncomp, (const double *)syn,
+                                                             tw, cnt, shifted, maps);
+    } else if (precision == GM_MIXED) {
+        if ((st = set_smem(k_ring_synthesis<float>, smem))) return st;
+        k_ring_synthesis<float><<<grid, threads, smem, s>>>(nside, L, ncomp, (const float *)syn,
+                                                            tw, cnt, shifted, maps);
+    } else {
+        return GM_ERR_UNSUPPORTED;
+    }
+    return check_launch("gm_ring_synthesis");
+}

@@ -1,0 +1,443 @@
+// Pseudo-C_ell, Wigner-3j coupling blocks, binning and the binned decouple (sm_100a).
+//
+// Replaces, from the reference (licongxu/GMaster):
+//   gmaster/workspaces.py:86-95      `_compute_coupled_cell` (XLA segment_sum)
+//   gmaster/workspaces.py:352-517    scalar coupling (threej closed form / GL quadrature)
+//   gmaster/workspaces.py:682-924    spin-0/2 coupling by GL quadrature GEMMs
+//   gmaster/_native/cuda/coupling_tt.cu:18-45  (FP32-product threej kernel, lmax < 48)
+//   gmaster/workspaces.py:1570-1590, 292-310   binned MCM (cuBLAS GEMMs)
+//   gmaster/workspaces.py:2146       decouple solve (cuSOLVER getrf/getrs)
+#include <math.h>
+
+#include "gm_common.cuh"
+
+namespace gm {
+
+__device__ __forceinline__ int64_t alm_idx(int64_t lmax, int64_t l, int64_t m)
+{
+    return m * (2 * lmax + 1 - m) / 2 + l;
+}
+
+// ---------------------------------------------------------------- pseudo-C_ell
+
+constexpr int kPclMChunk = 64;
+
+// grid (l-blocks, m-chunks, pairs); thread l sums its orders of the chunk and adds.
+__global__ void k_pseudo_cl(int64_t lmax, int64_t n1, const double2 *__restrict__ a,
+                            int64_t n2, const double2 *__restrict__ b, double *__restrict__ cls)
+{
+    const int64_t L = lmax + 1, nelem = L * (L + 1) / 2;
+    const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t m0 = (int64_t)blockIdx.y * kPclMChunk;
+    const int64_t pair = blockIdx.z, i = pair / n2, j = pair % n2;
+    if (l >= L || m0 > l) return;
+    const double2 *ai = a + i * nelem;
+    const double2 *bj = b + j * nelem;
+    double s = 0.0;
+    int64_t mend = m0 + kPclMChunk - 1;
+    if (mend > l) mend = l;
+    for (int64_t m = m0; m <= mend; ++m) {
+        const int64_t k = alm_idx(lmax, l, m);
+        const double2 x = ai[k], y = bj[k];
+        const double re = x.x * y.x + x.y * y.y;
+        s += m == 0 ? re : 2.0 * re;
+    }
+    atomicAdd(cls + pair * L + l, s / (2.0 * (double)l + 1.0));
+}
+
+// ---------------------------------------------------------------- Wigner-3j coupling
+
+// Work unit u -> (l1, l2 block) with l1 descending (longest recursions first):
+// t = lmax - l1 has floor(t / 32) + 1 blocks of 32 columns l2 >= l1.
+__device__ __forceinline__ bool unit_to_pair(int64_t u, int64_t lmax, int64_t &l1, int64_t &l2b)
+{
+    // cumulative units before t = 32 G + rr: 16 G (G + 1) + rr (G + 1)
+    int64_t G = (int64_t)floor((sqrt(1.0 + (double)u / 4.0) - 1.0) / 2.0);
+    if (G < 0) G = 0;
+    while (16 * (G + 1) * (G + 2) <= u) ++G;
+    while (G > 0 && 16 * G * (G + 1) > u) --G;
+    const int64_t rem = u - 16 * G * (G + 1);
+    const int64_t rr = rem / (G + 1), b = rem % (G + 1);
+    const int64_t t = 32 * G + rr;
+    if (t > lmax) return false;
+    l1 = lmax - t;
+    l2b = l1 + 32 * b;
+    return true;
+}
+
+__device__ __forceinline__ int64_t total_units(int64_t lmax)
+{
+    // t in [0, lmax]: sum of floor(t/32) + 1
+    const int64_t T = lmax + 1, G = T / 32, rr = T % 32;
+    return 16 * G * (G + 1) + rr * (G + 1);
+}
+
+// One thread per (l1 <= l2) pair: three-term recursion in l3 (Schulten & Gordon 1975)
+// for (l3 l1 l2; 0 2 -2) = (l1 l2 l3; 2 -2 0), and the two-term ratio for (l1 l2 l3; 000),
+// both unnormalised from l3 = l2 - l1 and normalised by sum (2 l3 + 1) f^2 = 1.
+__global__ void __launch_bounds__(128) k_coupling(int64_t lmax, const double *__restrict__ window,
+                                                  int64_t nw, int which,
+                                                  double *__restrict__ blocks,
+                                                  unsigned long long *__restrict__ queue)
+{
+    const int64_t n = lmax + 1, nn = n * n;
+    const int64_t nunits = total_units(lmax);
+    const int lane = threadIdx.x & 31;
+    const bool want_te = which & 2, want_pol = (which & 12) != 0, want_s2 = want_te || want_pol;
+    const double inv4pi = 1.0 / (4.0 * M_PI);
+    for (;;) {
+        unsigned long long u = 0;
+        if (lane == 0) u = atomicAdd(queue, 1ull);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        if ((int64_t)u >= nunits) break;
+        int64_t l1, l2b;
+        if (!unit_to_pair((int64_t)u, lmax, l1, l2b)) break;
+        const int64_t l2 = l2b + lane;
+        if (l2 <= lmax) {
+        const int64_t d = l2 - l1, jmin = d, jmax = l1 + l2;
+        const double S = (double)(l1 + l2 + 1), S2 = S * S, d2 = (double)(d * d);
+        const bool s2ok = want_s2 && l1 >= 2 && l2 >= 2;
+        double f_prev = 0.0, f = 1.0;      // (000), unnormalised
+        double g_prev = 0.0, g = 1.0;      // (2 -2 0), unnormalised
+        double sq = 0.0;                   // sqrt P(j) at the current j
+        double n0 = 0.0, n2s = 0.0, stt = 0.0, ste = 0.0, spp = 0.0, smm = 0.0;
+        for (int64_t j = jmin;; ++j) {
+            const double tj = 2.0 * (double)j + 1.0;
+            const double wj = (j < nw ? __ldg(window + j) : 0.0) * inv4pi * tj;
+            const bool even = ((j - jmin) & 1) == 0;
+            n0 += tj * f * f;
+            stt += wj * f * f;
+            if (s2ok) {
+                n2s += tj * g * g;
+                ste += wj * f * g;
+                if (even) spp += wj * g * g;
+                else smm += wj * g * g;
+            }
+            if (j == jmax) break;
+            const double j1 = (double)(j + 1);
+            const double P1 = (j1 * j1 - d2) * (S2 - j1 * j1);
+            const double r1 = rsqrt(P1);
+            const double sq1 = P1 * r1;
+            const double fn = -sq * r1 * f_prev;
+            f_prev = f;
+            f = fn;
+            if (s2ok) {
+                const double gn = (4.0 * tj * g - sq * g_prev) * r1;
+                g_prev = g;
+                g = gn;
+                if (fabs(g) > 1e150) {
+                    g *= 1e-150;
+                    g_prev *= 1e-150;
+                    n2s *= 1e-300;
+                    spp *= 1e-300;
+                    smm *= 1e-300;
+                    ste *= 1e-150;
+                }
+            }
+            if (fabs(f) > 1e150) {
+                f *= 1e-150;
+                f_prev *= 1e-150;
+                n0 *= 1e-300;
+                stt *= 1e-300;
+                ste *= 1e-150;
+            }
+            sq = sq1;
+        }
+        // Both (l1 l2 l3; 000) and (l1 l2 l3; 2 -2 0) carry the sign (-1)^(l1 - l2) at
+        // l3 = l1 + l2, so the relative sign of the unnormalised product is sign(f g) there.
+        const double tt = stt / n0;
+        double te = 0.0, pp = 0.0, mm = 0.0;
+        if (s2ok) {
+            const double sgn = (f * g) < 0.0 ? -1.0 : 1.0;
+            te = sgn * ste / sqrt(n0 * n2s);
+            pp = spp / n2s;
+            mm = smm / n2s;
+        }
+        const double c1 = 2.0 * (double)l1 + 1.0, c2 = 2.0 * (double)l2 + 1.0;
+        const double vals[4] = {tt, te, pp, mm};
+#pragma unroll
+        for (int x = 0; x < 4; ++x) {
+            if (!(which & (1 << x))) continue;
+            double *bx = blocks + x * nn;
+            bx[l1 * n + l2] = c2 * vals[x];
+            bx[l2 * n + l1] = c1 * vals[x];
+        }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- binning
+
+// Binned block: out[b][b'] = sum_{l in b} wfl[l] sum_{l' in b'} M[l][l'] beam[l'] inv_fl[l'].
+__global__ void k_bin_block(int64_t lmax, int64_t nb, const double *__restrict__ M,
+                            const int32_t *__restrict__ band_ptr, const int32_t *__restrict__ band_ells,
+                            const double *__restrict__ wfl, const double *__restrict__ inv_fl,
+                            const double *__restrict__ beam, double *__restrict__ out)
+{
+    const int64_t b = blockIdx.y, bp = blockIdx.x, n = lmax + 1;
+    const int i0 = band_ptr[b], i1 = band_ptr[b + 1], k0 = band_ptr[bp], k1 = band_ptr[bp + 1];
+    const int nk = k1 - k0, cnt = (i1 - i0) * nk;
+    double s = 0.0;
+    for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+        const int l = band_ells[i0 + t / nk], lp = band_ells[k0 + t % nk];
+        s += wfl[l] * M[(int64_t)l * n + lp] * beam[lp] * inv_fl[lp];
+    }
+    __shared__ double red[256];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[b * nb + bp] = red[0];
+}
+
+// Place binned blocks into the (ncls nb)^2 matrix, band-major channel-minor.
+__global__ void k_place_binned(int64_t nb, int ncls, const double *__restrict__ bb,
+                               double *__restrict__ out)
+{
+    const int64_t N = ncls * nb;
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= N * N) return;
+    const int64_t row = idx / N, col = idx % N;
+    const int64_t b = row / ncls, c1 = row % ncls, bp = col / ncls, c2 = col % ncls;
+    const int64_t nb2 = nb * nb;
+    double v = 0.0;
+    if (ncls == 1) {
+        v = bb[b * nb + bp];
+    } else if (ncls == 2) {
+        if (c1 == c2) v = bb[b * nb + bp];
+    } else {
+        if (c1 == c2) v = bb[b * nb + bp];                       // M+ on the diagonal slots
+        else if (c1 + c2 == 3)                                   // M- on the anti-diagonal
+            v = ((c1 == 1 || c1 == 2) ? -1.0 : 1.0) * bb[nb2 + b * nb + bp];
+    }
+    out[idx] = v;
+}
+
+__global__ void k_bin_cells(int64_t lmax, int64_t nb, int64_t ncls, const double *__restrict__ cls,
+                            const int32_t *__restrict__ band_ptr,
+                            const int32_t *__restrict__ band_ells, const double *__restrict__ wfl,
+                            double *__restrict__ out)
+{
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nb * ncls) return;
+    const int64_t c = idx / nb, b = idx % nb;
+    double s = 0.0;
+    for (int i = band_ptr[b]; i < band_ptr[b + 1]; ++i) {
+        const int l = band_ells[i];
+        s += wfl[l] * cls[c * (lmax + 1) + l];
+    }
+    out[c * nb + b] = s;
+}
+
+// ---------------------------------------------------------------- LU
+
+// Single-CTA right-looking LU with partial pivoting, row-major a (n x n).
+__global__ void __launch_bounds__(1024) k_lu_factor(int64_t n, double *__restrict__ a,
+                                                    int32_t *__restrict__ piv,
+                                                    int32_t *__restrict__ status)
+{
+    __shared__ double sval[32];
+    __shared__ int sidx[32];
+    __shared__ int pivot_row;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    if (tid == 0) *status = 0;
+    for (int64_t k = 0; k < n; ++k) {
+        // pivot search in column k
+        double best = -1.0;
+        int bi = (int)k;
+        for (int64_t i = k + tid; i < n; i += blockDim.x) {
+            const double v = fabs(a[i * n + k]);
+            if (v > best) {
+                best = v;
+                bi = (int)i;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_down_sync(0xffffffffu, best, o);
+            const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+            if (ov > best || (ov == best && oi < bi)) {
+                best = ov;
+                bi = oi;
+            }
+        }
+        if (lane == 0) {
+            sval[warp] = best;
+            sidx[warp] = bi;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double bv = sval[0];
+            int bix = sidx[0];
+            for (int w = 1; w < nwarps; ++w)
+                if (sval[w] > bv || (sval[w] == bv && sidx[w] < bix)) {
+                    bv = sval[w];
+                    bix = sidx[w];
+                }
+            pivot_row = bix;
+            piv[k] = bix;
+            if (bv == 0.0 && *status == 0) *status = (int32_t)(k + 1);
+        }
+        __syncthreads();
+        const int64_t p = pivot_row;
+        if (p != k)
+            for (int64_t jj = tid; jj < n; jj += blockDim.x) {
+                const double t = a[k * n + jj];
+                a[k * n + jj] = a[p * n + jj];
+                a[p * n + jj] = t;
+            }
+        __syncthreads();
+        const double d = a[k * n + k];
+        const double inv = d != 0.0 ? 1.0 / d : 0.0;
+        for (int64_t i = k + 1 + tid; i < n; i += blockDim.x) a[i * n + k] *= inv;
+        __syncthreads();
+        // trailing update, one warp per row, lanes along columns
+        for (int64_t i = k + 1 + warp; i < n; i += nwarps) {
+            const double lik = a[i * n + k];
+            if (lik != 0.0)
+                for (int64_t jj = k + 1 + lane; jj < n; jj += 32) a[i * n + jj] -= lik * a[k * n + jj];
+        }
+        __syncthreads();
+    }
+}
+
+// One warp per right-hand-side column: P, then L (unit) forward, then U backward.
+// b is (n, nrhs) row-major.
+__global__ void k_lu_solve(int64_t n, const double *__restrict__ lu, const int32_t *__restrict__ piv,
+                           int64_t nrhs, double *__restrict__ b)
+{
+    const int64_t col = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (col >= nrhs) return;
+    if (lane == 0)
+        for (int64_t k = 0; k < n; ++k) {
+            const int64_t p = piv[k];
+            if (p != k) {
+                const double t = b[k * nrhs + col];
+                b[k * nrhs + col] = b[p * nrhs + col];
+                b[p * nrhs + col] = t;
+            }
+        }
+    __syncwarp();
+    for (int64_t i = 0; i < n; ++i) {
+        double s = 0.0;
+        for (int64_t jj = lane; jj < i; jj += 32) s += lu[i * n + jj] * b[jj * nrhs + col];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) b[i * nrhs + col] -= s;
+        __syncwarp();
+    }
+    for (int64_t i = n - 1; i >= 0; --i) {
+        double s = 0.0;
+        for (int64_t jj = i + 1 + lane; jj < n; jj += 32) s += lu[i * n + jj] * b[jj * nrhs + col];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) b[i * nrhs + col] = (b[i * nrhs + col] - s) / lu[i * n + i];
+        __syncwarp();
+    }
+}
+
+}  // namespace gm
+
+using namespace gm;
+
+extern "C" int gm_pseudo_cl(int64_t lmax, int64_t n1, const double *alm1, int64_t n2,
+                            const double *alm2, double *cls, void *stream)
+{
+    if (lmax < 0 || n1 < 1 || n2 < 1 || n1 * n2 > 65535) return GM_ERR_BAD_SHAPE;
+    if (!alm1 || !alm2 || !cls) return GM_ERR_BAD_PTR;
+    const int64_t L = lmax + 1;
+    cudaStream_t s = as_stream(stream);
+    cudaError_t e = cudaMemsetAsync(cls, 0, sizeof(double) * n1 * n2 * L, s);
+    if (e != cudaSuccess) {
+        set_error("gm_pseudo_cl memset", e);
+        return GM_ERR_LAUNCH;
+    }
+    dim3 grid((unsigned)((L + 255) / 256), (unsigned)((L + kPclMChunk - 1) / kPclMChunk),
+              (unsigned)(n1 * n2));
+    k_pseudo_cl<<<grid, 256, 0, s>>>(lmax, n1, (const double2 *)alm1, n2, (const double2 *)alm2, cls);
+    return check_launch("gm_pseudo_cl");
+}
+
+extern "C" int gm_coupling_blocks(int64_t lmax, const double *window, int64_t nw, int which,
+                                  double *blocks, int64_t *queue, void *stream)
+{
+    if (lmax < 0 || lmax > 65535 || nw < 0) return GM_ERR_BAD_SHAPE;
+    if (which <= 0 || which > 15) return GM_ERR_UNSUPPORTED;
+    if (!window || !blocks || !queue) return GM_ERR_BAD_PTR;
+    cudaStream_t s = as_stream(stream);
+    const int64_t n = lmax + 1;
+    cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(int64_t), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(blocks, 0, sizeof(double) * 4 * n * n, s);
+    if (e != cudaSuccess) {
+        set_error("gm_coupling_blocks memset", e);
+        return GM_ERR_LAUNCH;
+    }
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    k_coupling<<<nsm * 8, 128, 0, s>>>(lmax, window, nw, which, blocks,
+                                       reinterpret_cast<unsigned long long *>(queue));
+    return check_launch("gm_coupling_blocks");
+}
+
+// Binning operators are passed in CSR form to support any NmtBin.
+extern "C" int gm_bin_coupling_csr(int64_t lmax, int64_t nbands, int ncls, const double *blocks,
+                                   const int32_t *band_ptr, const int32_t *band_ells,
+                                   const double *wfl, const double *inv_fl, const double *beam,
+                                   double *scratch, double *out, void *stream)
+{
+    if (lmax < 0 || nbands < 1 || nbands > 65535 || (ncls != 1 && ncls != 2 && ncls != 4))
+        return GM_ERR_BAD_SHAPE;
+    if (!blocks || !band_ptr || !band_ells || !wfl || !inv_fl || !beam || !scratch || !out)
+        return GM_ERR_BAD_PTR;
+    cudaStream_t s = as_stream(stream);
+    const int64_t n = lmax + 1, nn = n * n, nb2 = nbands * nbands;
+    dim3 grid((unsigned)nbands, (unsigned)nbands);
+    // block slots: tt 0, te 1, pp 2, mm 3
+    if (ncls == 1) {
+        k_bin_block<<<grid, 256, 0, s>>>(lmax, nbands, blocks, band_ptr, band_ells, wfl, inv_fl,
+                                         beam, scratch);
+    } else if (ncls == 2) {
+        k_bin_block<<<grid, 256, 0, s>>>(lmax, nbands, blocks + nn, band_ptr, band_ells, wfl,
+                                         inv_fl, beam, scratch);
+    } else {
+        k_bin_block<<<grid, 256, 0, s>>>(lmax, nbands, blocks + 2 * nn, band_ptr, band_ells, wfl,
+                                         inv_fl, beam, scratch);
+        k_bin_block<<<grid, 256, 0, s>>>(lmax, nbands, blocks + 3 * nn, band_ptr, band_ells, wfl,
+                                         inv_fl, beam, scratch + nb2);
+    }
+    const int64_t N = ncls * nbands;
+    k_place_binned<<<(unsigned)((N * N + 255) / 256), 256, 0, s>>>(nbands, ncls, scratch, out);
+    return check_launch("gm_bin_coupling");
+}
+
+extern "C" int gm_bin_cells_csr(int64_t lmax, int64_t nbands, int64_t ncls, const double *cls,
+                                const int32_t *band_ptr, const int32_t *band_ells,
+                                const double *wfl, double *out, void *stream)
+{
+    if (lmax < 0 || nbands < 1 || ncls < 1) return GM_ERR_BAD_SHAPE;
+    if (!cls || !band_ptr || !band_ells || !wfl || !out) return GM_ERR_BAD_PTR;
+    const int64_t tot = nbands * ncls;
+    k_bin_cells<<<(unsigned)((tot + 255) / 256), 256, 0, as_stream(stream)>>>(
+        lmax, nbands, ncls, cls, band_ptr, band_ells, wfl, out);
+    return check_launch("gm_bin_cells");
+}
+
+extern "C" int gm_lu_factor(int64_t n, double *a, int32_t *piv, int32_t *status, void *stream)
+{
+    if (n < 1 || n > 65535) return GM_ERR_BAD_SHAPE;
+    if (!a || !piv || !status) return GM_ERR_BAD_PTR;
+    k_lu_factor<<<1, 1024, 0, as_stream(stream)>>>(n, a, piv, status);
+    return check_launch("gm_lu_factor");
+}
+
+extern "C" int gm_lu_solve(int64_t n, const double *lu, const int32_t *piv, int64_t nrhs,
+                           double *b, void *stream)
+{
+    if (n < 1 || nrhs < 1) return GM_ERR_BAD_SHAPE;
+    if (!lu || !piv || !b) return GM_ERR_BAD_PTR;
+    const int64_t threads = 256, warps_per = threads / 32;
+    k_lu_solve<<<(unsigned)((nrhs + warps_per - 1) / warps_per), (unsigned)threads, 0,
+                 as_stream(stream)>>>(n, lu, piv, nrhs, b);
+    return check_launch("gm_lu_solve");
+}

@@ -1,0 +1,138 @@
+"""Curved-sky fields (`NmtField`), the counterpart of gmaster/field.py:20-499.
+
+Supported: HEALPix spin-0 and spin-2 fields with a beam, ``n_iter`` / ``n_iter_mask``,
+``lmax`` / ``lmax_mask``, ``masked_on_input`` and ``lite``.  Contaminant templates,
+purification and anisotropic masks are outside this build and raise
+``NotImplementedError``.
+"""
+
+import numpy as np
+import torch
+
+from . import sht
+from ._config import get_precision, nmt_params
+from .utils import NmtAlmInfo, NmtMapInfo, as_device
+
+
+class NmtField:
+    """A masked field: mask, maps and their spherical-harmonic coefficients.
+
+    For spin-0 fields the field and its mask are analysed in one shared latitudinal
+    pass (two maps contracted against the same generated Legendre rows), as the
+    reference does (gmaster/field.py:266-289).
+    """
+
+    def __init__(self, mask, maps, *, spin=None, templates=None, beam=None, purify_e=False,
+                 purify_b=False, n_iter=None, n_iter_mask=None, tol_pinv=None, wcs=None,
+                 lmax=None, lmax_mask=None, masked_on_input=False, lite=False, mask_22=None,
+                 mask_12=None, precision=None):
+        if templates is not None:
+            raise NotImplementedError("contaminant deprojection is not part of this build")
+        if purify_e or purify_b:
+            raise NotImplementedError("E/B purification is not part of this build")
+        if mask_22 is not None or mask_12 is not None:
+            raise NotImplementedError("anisotropic masks are not part of this build")
+        self.lite = bool(lite)
+        self.precision = precision or get_precision()
+        self.n_iter = nmt_params.n_iter_default if n_iter is None else int(n_iter)
+        self.n_iter_mask = nmt_params.n_iter_mask_default if n_iter_mask is None else int(n_iter_mask)
+        self.pure_e = self.pure_b = False
+        self.is_catalog = False
+        self.anisotropic_mask = False
+        self.alm = self.alm_mask = self.maps = self.temp = None
+        self.n_temp = 0
+        self._Nw = self._Nf = 0
+
+        mask_t = as_device(mask, torch.float64)
+        if mask_t.ndim != 1:
+            raise ValueError("Mask must be a one-dimensional HEALPix map")
+        self.minfo = NmtMapInfo(wcs, tuple(mask_t.shape))
+        self.mask = mask_t
+        lmax = self.minfo.get_lmax() if lmax is None else int(lmax)
+        lmax_mask = self.minfo.get_lmax() if lmax_mask is None else int(lmax_mask)
+        if lmax <= 0 or lmax_mask <= 0:
+            raise ValueError("`lmax` and `lmax_mask` must be positive")
+        self.ainfo = NmtAlmInfo(lmax)
+        self.ainfo_mask = NmtAlmInfo(lmax_mask)
+        if beam is None:
+            self.beam = torch.ones(lmax + 1, dtype=torch.float64, device=mask_t.device)
+        else:
+            b = np.asarray(beam.cpu() if isinstance(beam, torch.Tensor) else beam, dtype=np.float64)
+            if b.ndim != 1 or len(b) <= lmax:
+                raise ValueError(f"Input beam must have at least {lmax + 1} elements "
+                                 "given the input map resolution")
+            self.beam = torch.from_numpy(np.ascontiguousarray(b[: lmax + 1])).to(mask_t.device)
+
+        if maps is None:
+            if spin is None:
+                raise ValueError("Please supply field spin")
+            self.spin = int(spin)
+            self.nmaps = 1 if self.spin == 0 else 2
+            return
+        maps_t = as_device(maps, torch.float64)
+        if maps_t.ndim == 1:
+            maps_t = maps_t[None]
+        if maps_t.shape[0] not in (1, 2):
+            raise ValueError("Must supply 1 or 2 maps per field")
+        if maps_t.shape[1] != self.minfo.npix:
+            raise ValueError("Maps and mask have different sizes")
+        if spin is None:
+            spin = 0 if maps_t.shape[0] == 1 else 2
+        if (spin == 0) != (maps_t.shape[0] == 1):
+            raise ValueError("Spin-zero fields are associated with a single map")
+        if spin not in (0, 2):
+            raise NotImplementedError("only spin-0 and spin-2 fields are implemented")
+        self.spin = int(spin)
+        self.nmaps = 1 if self.spin == 0 else 2
+        if not masked_on_input:
+            maps_t = maps_t * self.mask[None, :]
+        nside = self.minfo.nside
+        if (self.spin == 0 and not self.lite and self.ainfo == self.ainfo_mask
+                and self.n_iter == self.n_iter_mask):
+            both = sht.map2alm_device(torch.cat([maps_t, self.mask[None, :]]), 0, nside,
+                                      self.ainfo.lmax, self.n_iter, self.precision)
+            self.alm, self.alm_mask = both[0:1], both[1]
+        else:
+            self.alm = sht.map2alm_device(maps_t, self.spin, nside, self.ainfo.lmax, self.n_iter,
+                                          self.precision)
+        if not self.lite:
+            self.maps = maps_t
+
+    def is_compatible(self, other, strict=True):
+        if strict and self.minfo != other.minfo:
+            return False
+        return self.ainfo_mask == other.ainfo_mask and self.ainfo == other.ainfo
+
+    def get_mask(self):
+        return self.mask
+
+    def get_maps(self):
+        if self.maps is None:
+            raise ValueError("Input maps unavailable for this field")
+        return self.maps
+
+    def get_alms(self):
+        if self.alm is None:
+            raise ValueError("Input alms unavailable for this field")
+        return self.alm
+
+    def get_templates(self):
+        raise ValueError("Input templates unavailable for this field")
+
+    def get_mask_alms(self):
+        """Mask alms (nelem_mask,), computed on first call (gmaster/field.py:348-376)."""
+        if self.alm_mask is None:
+            alms = sht.map2alm_device(self.mask[None, :], 0, self.minfo.nside, self.ainfo_mask.lmax,
+                                      self.n_iter_mask, self.precision)[0]
+            if not self.lite:
+                self.alm_mask = alms
+            return alms
+        return self.alm_mask
+
+    @property
+    def Nw(self):
+        return self._Nw
+
+    @property
+    def Nf(self):
+        return self._Nf

@@ -1,0 +1,263 @@
+"""HEALPix spherical-harmonic transforms on the GPU (host driver of the CUDA kernels).
+
+A transform is two separable stages, each a hand-written sm_100a kernel:
+
+    maps --[ring FFT, ring.cu]--> ring spectra --[hemisphere pack]--> rhs(m, lane)
+         --[Legendre contraction, legendre.cu / legendre_tc.cu]--> alm(l, m)
+
+and ``map2alm`` adds NaMaster's Jacobi refinement ``alm <- alm - A(S(alm) - map)``
+(gmaster/_sht/healpix.py:1059-1068).  Inside the loop the residual is formed in
+lane space by the ring fold (`gm_fold_residual`), so no ring FFT runs in the loop
+(the reference's ring-fold residual, gmaster/_native/cuda/march_v2.cu:409-493).
+
+Precision modes: ``"fp64"`` keeps every stage in double precision (the plain FP64
+path); ``"mixed"`` runs the ring stage and the contraction in single precision (or
+BF16-split tensor-core products, see legendre_tc.cu) with the recurrence, seeds,
+normalisation, alm accumulation and refinement update in double precision.
+"""
+
+import math
+import threading
+
+import numpy as np
+import torch
+
+from . import _lib
+
+_PLANS = {}
+_PLAN_LOCK = threading.Lock()
+
+
+# ----------------------------------------------------------------------------- geometry
+
+def ring_geometry(nside):
+    """HEALPix RING geometry, bit-identical to the reference (gmaster/utils.py:223-249).
+
+    Returns ``theta, phi0, nphi, offsets`` for the ``4 nside - 1`` rings, computed
+    with the same numpy operations in the same order as the reference.
+    """
+    nring = 4 * nside - 1
+    rings = np.arange(1, 4 * nside)
+    north = np.where(rings > 2 * nside, 4 * nside - rings, rings)
+    cap = north < nside
+    npix = 12 * nside ** 2
+    theta = np.empty(nring)
+    phi0 = np.empty(nring)
+    nphi = np.empty(nring, dtype=np.uint64)
+    theta[cap] = 2 * np.arcsin(north[cap] / (np.sqrt(6) * nside))
+    phi0[cap] = np.pi / (4 * north[cap])
+    nphi[cap] = 4 * north[cap]
+    theta[~cap] = np.arccos((2 * nside - north[~cap]) * (8 * nside / npix))
+    phi0[~cap] = np.pi / (4 * nside) * (((north[~cap] - nside) & 1) == 0)
+    nphi[~cap] = 4 * nside
+    south = north != rings
+    theta[south] = np.pi - theta[south]
+    offsets = np.concatenate([[0], np.cumsum(nphi)[:-1]]).astype(np.uint64)
+    return theta, phi0, nphi, offsets
+
+
+def shifted_flags(nside):
+    """1 where a ring's first pixel sits at phi0 = pi / nphi, 0 where phi0 = 0."""
+    _, phi0, nphi, _ = ring_geometry(nside)
+    flags = (phi0 != 0).astype(np.uint8)
+    # every HEALPix ring has phi0 in {0, pi / nphi}; the kernels rely on it
+    shifted = np.pi / nphi.astype(np.float64)
+    if not np.all((phi0 == 0) | np.isclose(phi0, shifted, rtol=0, atol=1e-15)):
+        raise AssertionError("unexpected HEALPix ring phase")
+    return flags
+
+
+def lane_geometry(nside):
+    """(3, 2 nside) float64: cos(theta), log2 sin(theta/2), log2 cos(theta/2) of the
+    northern rings 1..2 nside (the last lane is the equator)."""
+    theta = ring_geometry(nside)[0][: 2 * nside]
+    return np.stack([np.cos(theta), np.log2(np.sin(theta / 2)), np.log2(np.cos(theta / 2))])
+
+
+def _log2_int(n):
+    b = n.bit_length()
+    if b <= 53:
+        return math.log2(n)
+    shift = b - 53
+    return shift + math.log2(n >> shift)
+
+
+def seed_table(L):
+    """Seeds of the Wigner-d rows: (3 variants, L orders, 4) float64.
+
+    Variant 0 is spin 0 (s' = 0), 1 is s' = -2 (the sY_{+2} rows), 2 is s' = +2.  Entry
+    ``[log2 N, sign, pc, ps]`` gives the first row l0 = max(m, |s'|) as
+    ``sign * 2^(log2 N + pc log2 cos(theta/2) + ps log2 sin(theta/2))`` with
+    ``N = sqrt((2 l0 + 1)/4pi) sqrt(binomial)`` from the closed forms
+    d^m_{m,s'} = (-1)^(m-s') sqrt(C(2m, m+s')) cos^(m+s') sin^(m-s') (m >= |s'|) and
+    d^s_{m,+s} = sqrt(C(2s, s+m)) cos^(s+m) sin^(s-m),
+    d^s_{m,-s} = (-1)^(m+s) sqrt(C(2s, s-m)) cos^(s-m) sin^(s+m) (m < s); the binomials
+    are exact integers, so log2 N is accurate to the last bit.
+    """
+    out = np.zeros((3, L, 4))
+    c = 1  # C(2m, m)
+    for m in range(L):
+        if m > 0:
+            c = c * (2 * m) * (2 * m - 1) // (m * m)
+        lc = _log2_int(c)
+        sign = -1.0 if (m & 1) else 1.0
+        out[0, m] = [0.5 * lc + 0.5 * math.log2((2 * m + 1) / (4 * math.pi)), sign, m, m]
+        if m >= 2:
+            # C(2m, m -+ 2) = C(2m, m) m (m-1) / ((m+1)(m+2))
+            lc2 = lc + math.log2(m * (m - 1)) - math.log2((m + 1) * (m + 2))
+            norm = 0.5 * lc2 + 0.5 * math.log2((2 * m + 1) / (4 * math.pi))
+            out[1, m] = [norm, sign, m - 2, m + 2]
+            out[2, m] = [norm, sign, m + 2, m - 2]
+        else:
+            base = 0.5 * math.log2(5 / (4 * math.pi))
+            out[1, m] = [base + 0.5 * math.log2(math.comb(4, 2 - m)), sign, 2 - m, 2 + m]
+            out[2, m] = [base + 0.5 * math.log2(math.comb(4, 2 + m)), 1.0, 2 + m, 2 - m]
+    return out
+
+
+class Plan:
+    """Device-resident constants of one (nside, lmax) geometry, cached per device."""
+
+    def __init__(self, nside, lmax, device):
+        _lib.require_cuda()
+        self.nside, self.lmax, self.L = int(nside), int(lmax), int(lmax) + 1
+        self.device = torch.device(device)
+        self.npix = 12 * self.nside ** 2
+        self.nring = 4 * self.nside - 1
+        self.nlanes = 2 * self.nside
+        self.nelem = self.L * (self.L + 1) // 2
+        lib = _lib.load()
+        cnt = lib.gm_ring_twiddle_count(self.nside)
+        self.tw = torch.empty(cnt * 24, dtype=torch.uint8, device=self.device)
+        _lib.call("gm_ring_twiddles", self.nside, _lib.ptr(self.tw), _lib.stream_handle(self.device))
+        self.shifted = torch.from_numpy(shifted_flags(self.nside)).to(self.device)
+        self.geom = torch.from_numpy(np.ascontiguousarray(lane_geometry(self.nside))).to(self.device)
+        self.seeds = torch.from_numpy(np.ascontiguousarray(seed_table(self.L))).to(self.device)
+        # healpy packing helpers (host)
+        m = np.arange(self.L)
+        self.mstart = m * (2 * self.lmax + 1 - m) // 2
+
+
+def get_plan(nside, lmax, device=None):
+    dev = torch.device(device if device is not None else "cuda")
+    if dev.index is None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+    key = (int(nside), int(lmax), dev.index)
+    with _PLAN_LOCK:
+        plan = _PLANS.get(key)
+        if plan is None:
+            plan = Plan(nside, lmax, dev)
+            _PLANS[key] = plan
+    return plan
+
+
+def _prec(precision):
+    if precision in ("fp64", _lib.FP64):
+        return _lib.FP64
+    if precision in ("mixed", _lib.MIXED):
+        return _lib.MIXED
+    raise ValueError(f"unknown precision {precision!r} (use 'fp64' or 'mixed')")
+
+
+def _real_dtype(prec):
+    return torch.float64 if prec == _lib.FP64 else torch.float32
+
+
+def _complex_dtype(prec):
+    return torch.complex128 if prec == _lib.FP64 else torch.complex64
+
+
+# ----------------------------------------------------------------------------- stages
+
+def ring_analysis(plan, maps, prec):
+    """maps (ncomp, npix) float64/float32 CUDA -> ring spectra (ncomp, nring, L)."""
+    maps = maps.contiguous()
+    ncomp = maps.shape[0]
+    spec = torch.empty((ncomp, plan.nring, plan.L), dtype=_complex_dtype(prec), device=plan.device)
+    _lib.call("gm_ring_analysis", prec, plan.nside, plan.L, ncomp, _lib.ptr(maps),
+              maps.element_size(), _lib.ptr(plan.tw), _lib.ptr(plan.shifted), _lib.ptr(spec),
+              _lib.stream_handle(plan.device))
+    return spec
+
+
+def pack_rhs(plan, spec, prec):
+    ncomp = spec.shape[0]
+    rhs = torch.empty((plan.L, plan.nlanes, ncomp, 4), dtype=_real_dtype(prec), device=plan.device)
+    _lib.call("gm_pack_rhs", prec, plan.nside, plan.L, ncomp, _lib.ptr(spec), _lib.ptr(rhs),
+              _lib.stream_handle(plan.device))
+    return rhs
+
+
+def legendre_analysis(plan, spin, rhs, alm, scale, prec):
+    ncomp = rhs.shape[2]
+    _lib.call("gm_legendre_analysis", prec, spin, plan.nside, plan.lmax, ncomp,
+              _lib.ptr(plan.geom), _lib.ptr(plan.seeds), _lib.ptr(rhs), _lib.ptr(alm),
+              float(scale), _lib.stream_handle(plan.device))
+
+
+def legendre_synthesis(plan, spin, alm, ncomp, prec, out=None):
+    syn = out if out is not None else torch.empty(
+        (plan.L, plan.nlanes, ncomp, 4), dtype=_real_dtype(prec), device=plan.device)
+    _lib.call("gm_legendre_synthesis", prec, spin, plan.nside, plan.lmax, ncomp,
+              _lib.ptr(plan.geom), _lib.ptr(plan.seeds), _lib.ptr(alm), _lib.ptr(syn),
+              _lib.stream_handle(plan.device))
+    return syn
+
+
+def fold_residual(plan, syn, rhs_map, prec, out=None):
+    ncomp = syn.shape[2]
+    res = out if out is not None else torch.empty_like(rhs_map)
+    _lib.call("gm_fold_residual", prec, plan.nside, plan.L, ncomp, _lib.ptr(syn),
+              _lib.ptr(rhs_map), _lib.ptr(plan.shifted), _lib.ptr(res),
+              _lib.stream_handle(plan.device))
+    return res
+
+
+def ring_synthesis(plan, syn, prec):
+    ncomp = syn.shape[2]
+    maps = torch.empty((ncomp, plan.npix), dtype=torch.float64, device=plan.device)
+    _lib.call("gm_ring_synthesis", prec, plan.nside, plan.L, ncomp, _lib.ptr(syn), _lib.ptr(plan.tw),
+              _lib.ptr(plan.shifted), _lib.ptr(maps), _lib.stream_handle(plan.device))
+    return maps
+
+
+# ----------------------------------------------------------------------------- transforms
+
+def map2alm_device(maps, spin, nside, lmax, n_iter, precision="mixed"):
+    """Analysis of ``maps`` (ncomp, npix) on the GPU with ``n_iter`` Jacobi iterations.
+
+    spin 0: ncomp independent maps -> (ncomp, nelem) complex128 alms.
+    spin 2: ncomp = 2 nfields (Q, U pairs) -> (2 nfields, nelem) rows (E, B per field).
+    """
+    prec = _prec(precision)
+    plan = get_plan(nside, lmax, maps.device)
+    ncomp = maps.shape[0]
+    if spin not in (0, 2):
+        raise NotImplementedError("only spin 0 and spin 2 transforms are implemented")
+    if spin == 2 and ncomp % 2:
+        raise ValueError("spin-2 transforms take (Q, U) pairs")
+    spec = ring_analysis(plan, maps, prec)
+    rhs_map = pack_rhs(plan, spec, prec)
+    del spec
+    alm = torch.zeros((ncomp, plan.nelem), dtype=torch.complex128, device=plan.device)
+    legendre_analysis(plan, spin, rhs_map, alm, 1.0, prec)
+    if n_iter > 0:
+        syn = torch.empty_like(rhs_map)
+        res = torch.empty_like(rhs_map)
+        for _ in range(int(n_iter)):
+            legendre_synthesis(plan, spin, alm, ncomp, prec, out=syn)
+            fold_residual(plan, syn, rhs_map, prec, out=res)
+            legendre_analysis(plan, spin, res, alm, -1.0, prec)
+    return alm
+
+
+def alm2map_device(alm, spin, nside, lmax, precision="mixed"):
+    """Synthesis of (nrows, nelem) complex128 alms -> (nrows, npix) float64 maps."""
+    prec = _prec(precision)
+    plan = get_plan(nside, lmax, alm.device)
+    alm = alm.contiguous()
+    ncomp = alm.shape[0]
+    if spin == 2 and ncomp % 2:
+        raise ValueError("spin-2 synthesis takes (E, B) pairs")
+    syn = legendre_synthesis(plan, spin, alm, ncomp, prec)
+    return ring_synthesis(plan, syn, prec)

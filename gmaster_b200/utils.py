@@ -1,0 +1,240 @@
+"""Map and harmonic-space utilities (the counterpart of ``gmaster.utils``).
+
+Geometry: `NmtMapInfo` (HEALPix) and `NmtAlmInfo` (healpy-packed alm layout).
+Transforms: `map2alm`, `alm2map`, `map2alm_pair` on the GPU (spin 0 and spin 2).
+Fixture helpers: `mask_apodization` (C1/C2), `synfast_spherical`, `pix2vec_ring`.
+
+Arrays are returned as CUDA ``torch.Tensor``s; inputs may be numpy arrays or tensors.
+"""
+
+import numpy as np
+import torch
+
+from . import sht
+from ._config import (get_default_params, get_precision, nmt_params, set_n_iter_default,
+                      set_precision, set_sht_calculator, set_tol_pinv_default)
+
+__all__ = [
+    "NmtAlmInfo", "NmtMapInfo", "alm2map", "map2alm", "map2alm_pair", "mask_apodization",
+    "synfast_spherical", "pix2vec_ring", "nmt_params", "get_default_params",
+    "set_n_iter_default", "set_tol_pinv_default", "set_precision", "get_precision",
+    "set_sht_calculator", "as_device",
+]
+
+
+def as_device(x, dtype=None, device=None):
+    """numpy array / tensor -> contiguous CUDA tensor (no copy if already there)."""
+    dev = torch.device(device) if device is not None else torch.device("cuda")
+    if isinstance(x, torch.Tensor):
+        t = x
+    else:
+        t = torch.from_numpy(np.ascontiguousarray(np.asarray(x)))
+    if dtype is not None and t.dtype != dtype:
+        t = t.to(dtype)
+    if t.device.type != "cuda":
+        t = t.to(dev, non_blocking=False)
+    return t.contiguous()
+
+
+class NmtMapInfo:
+    """HEALPix pixelisation (gmaster/utils.py:336-461).  CAR maps are not supported."""
+
+    def __init__(self, wcs, axes):
+        if wcs is not None:
+            raise NotImplementedError("only HEALPix maps are supported")
+        nside = 1
+        while 12 * nside ** 2 != axes[0]:
+            nside *= 2
+            if nside > 65536:
+                raise ValueError("Something is wrong with your input arrays")
+        self.is_healpix = True
+        self.nside = nside
+        self.npix = 12 * nside ** 2
+        self.nx = self.ny = -1
+        theta, phi0, nphi, offsets = sht.ring_geometry(nside)
+        self.theta, self.phi0, self.nphi, self.offsets = theta, phi0, nphi, offsets
+        self.weight = 4 * np.pi / self.npix
+
+    def __eq__(self, other):
+        return isinstance(other, NmtMapInfo) and self.nside == other.nside
+
+    def reform_map(self, maps):
+        if maps.shape[-1] != self.npix:
+            raise ValueError("Incompatible map!")
+        return maps
+
+    def get_lmax(self):
+        return 3 * self.nside - 1
+
+
+class NmtAlmInfo:
+    """Healpy m-major packing, ``a_lm`` at ``mstart[m] + l`` (gmaster/utils.py:493-524)."""
+
+    def __init__(self, lmax):
+        self.lmax = int(lmax)
+        self.mmax = self.lmax
+        m = np.arange(self.mmax + 1)
+        self.mstart = (m * (2 * self.lmax + 1 - m) // 2).astype(np.uint64)
+        self.nelem = (self.lmax + 1) * (self.lmax + 2) // 2
+
+    def __eq__(self, other):
+        return isinstance(other, NmtAlmInfo) and self.lmax == other.lmax
+
+    def ell_m(self):
+        """(ell, m) of every packed coefficient (numpy int64)."""
+        ell = np.concatenate([np.arange(mm, self.lmax + 1) for mm in range(self.lmax + 1)])
+        order = np.repeat(np.arange(self.lmax + 1), self.lmax + 1 - np.arange(self.lmax + 1))
+        return ell, order
+
+
+def map2alm(map, spin, map_info, alm_info, *, n_iter, precision=None):
+    """Spherical-harmonic analysis with Jacobi refinement (gmaster/utils.py:556-605).
+
+    map: (nmaps, npix), nmaps = 1 (spin 0) or 2 (spin 2, Q/U).  Returns (nmaps, nelem)
+    complex128 on the GPU; for spin 2 the rows are E and B.
+    """
+    nmaps = 1 if spin == 0 else 2
+    maps = as_device(map, torch.float64)
+    if maps.ndim != 2 or tuple(maps.shape) != (nmaps, map_info.npix):
+        raise ValueError("Input map has wrong shape")
+    if spin < 0 or spin > alm_info.lmax:
+        raise ValueError("spin must satisfy 0 <= spin <= lmax")
+    return sht.map2alm_device(maps, spin, map_info.nside, alm_info.lmax, int(n_iter),
+                              precision or get_precision())
+
+
+def map2alm_pair(map_a, map_b, map_info, alm_info, *, n_iter, precision=None):
+    """Two spin-0 maps in one shared latitudinal pass (gmaster/utils.py:608-642).
+
+    The Legendre rows are generated once and contracted against both maps.
+    Returns ``(alm_a, alm_b)``, each (1, nelem).
+    """
+    a = as_device(map_a, torch.float64)
+    b = as_device(map_b, torch.float64)
+    if a.shape != (1, map_info.npix) or b.shape != (1, map_info.npix):
+        raise ValueError("shared-band pair expects two (1, npix) spin-0 maps")
+    alm = sht.map2alm_device(torch.cat([a, b]), 0, map_info.nside, alm_info.lmax, int(n_iter),
+                             precision or get_precision())
+    return alm[0:1], alm[1:2]
+
+
+def alm2map(alm, spin, map_info, alm_info, precision=None):
+    """Spherical-harmonic synthesis (gmaster/utils.py:645-672): (nmaps, npix) float64."""
+    nmaps = 1 if spin == 0 else 2
+    a = as_device(alm, torch.complex128)
+    if a.ndim != 2 or tuple(a.shape) != (nmaps, alm_info.nelem):
+        raise ValueError("Input alm has wrong shape")
+    if spin < 0 or spin > alm_info.lmax:
+        raise ValueError("spin must satisfy 0 <= spin <= lmax")
+    return sht.alm2map_device(a, spin, map_info.nside, alm_info.lmax, precision or get_precision())
+
+
+# ----------------------------------------------------------------------------- fixtures
+
+def pix2vec_ring(nside, pix=None):
+    """Unit vectors of HEALPix RING pixel centres (the healpy pix2vec formulas)."""
+    theta, phi0, nphi, offsets = sht.ring_geometry(nside)
+    nphi = nphi.astype(np.int64)
+    ring = np.repeat(np.arange(4 * nside - 1), nphi)
+    within = np.arange(12 * nside ** 2) - offsets.astype(np.int64)[ring]
+    phi = phi0[ring] + 2 * np.pi * within / nphi[ring]
+    th = theta[ring]
+    vec = np.stack([np.sin(th) * np.cos(phi), np.sin(th) * np.sin(phi), np.cos(th)], axis=1)
+    return vec if pix is None else vec[pix]
+
+
+def mask_apodization(mask_in, aposize, apotype="C1"):
+    """C1 / C2 apodisation of a binary HEALPix mask (gmaster/utils.py:61-147 semantics).
+
+    The distance to the nearest masked pixel uses a k-d tree over the pixel unit
+    vectors (scipy), with ``x = sqrt((1 - cos d) / (1 - cos aposize))``.
+    """
+    if apotype not in ("C1", "C2"):
+        raise ValueError(f"Apodization type {apotype} unknown. Choose from ['C1', 'C2']")
+    if aposize < 0:
+        raise ValueError("Apodization scale must be a positive number")
+    mask = np.asarray(mask_in, dtype=np.float64)
+    if mask.ndim != 1:
+        raise ValueError("Mask must be a one-dimensional HEALPix map")
+    if aposize == 0:
+        return mask.copy()
+    from scipy.spatial import cKDTree
+
+    nside = int(round(np.sqrt(len(mask) / 12)))
+    radius = np.radians(aposize)
+    if int(4 * len(mask) * (1 - np.cos(1.2 * radius))) < 2:
+        raise ValueError("Your apodization scale is too small for this pixel size")
+    masked = np.flatnonzero(mask <= 0)
+    if not len(masked):
+        return mask.copy()
+    vectors = pix2vec_ring(nside)
+    distances, _ = cKDTree(vectors[masked]).query(vectors)
+    measure = 0.5 * distances ** 2
+    threshold = 1 - np.cos(radius)
+    affected = (mask > 0) & (measure < threshold)
+    x = np.sqrt(np.maximum(measure[affected], 0) / threshold)
+    factor = x - np.sin(2 * np.pi * x) / (2 * np.pi) if apotype == "C1" else 0.5 * (1 - np.cos(np.pi * x))
+    out = mask.copy()
+    out[affected] *= factor
+    return out
+
+
+def gaussian_alm(cls, lmax, rng):
+    """Gaussian alms (healpy packing) for spectra cls[(ncomp, >= lmax+1)] of independent or
+    correlated fields; `cls` is (n, n, L) covariance or (L,) for one field."""
+    cls = np.asarray(cls, dtype=np.float64)
+    if cls.ndim == 1:
+        cls = cls[None, None, :]
+    n = cls.shape[0]
+    L = lmax + 1
+    info = NmtAlmInfo(lmax)
+    ell, order = info.ell_m()
+    z = (rng.normal(size=(n, info.nelem)) + 1j * rng.normal(size=(n, info.nelem))) / np.sqrt(2)
+    z[:, order == 0] = z[:, order == 0].real * np.sqrt(2)
+    out = np.zeros((n, info.nelem), dtype=np.complex128)
+    for l in range(L):
+        cov = cls[:, :, l]
+        if not np.any(cov):
+            continue
+        w, v = np.linalg.eigh(cov)
+        root = v * np.sqrt(np.maximum(w, 0))
+        sel = ell == l
+        out[:, sel] = root @ z[:, sel]
+    return out
+
+
+def synfast_spherical(nside, cls, spin_arr, seed=-1, beam=None, precision=None):
+    """Gaussian realisation of fields with the given power spectra (gmaster/utils.py:823-927).
+
+    spin_arr lists the spin of each field (0 or 2); `cls` holds the upper-triangular
+    spectra in NaMaster order for the field components.  Returns a list of maps
+    ((1, npix) for spin 0, (2, npix) for spin 2) as CUDA tensors.
+    """
+    spin_arr = list(spin_arr)
+    ncomp = sum(1 if s == 0 else 2 for s in spin_arr)
+    lmax = 3 * nside - 1
+    L = lmax + 1
+    cls = np.asarray(cls, dtype=np.float64)
+    cov = np.zeros((ncomp, ncomp, L))
+    k = 0
+    for i in range(ncomp):
+        for j in range(i, ncomp):
+            row = cls[k][:L]
+            cov[i, j, : len(row)] = row
+            cov[j, i, : len(row)] = row
+            k += 1
+    rng = np.random.default_rng(None if seed < 0 else seed)
+    alm = gaussian_alm(cov, lmax, rng)
+    if beam is not None:
+        info = NmtAlmInfo(lmax)
+        ell, _ = info.ell_m()
+        alm = alm * np.asarray(beam)[:, ell] if np.ndim(beam) == 2 else alm * np.asarray(beam)[ell]
+    out = []
+    ainfo = NmtAlmInfo(lmax)
+    minfo = NmtMapInfo(None, (12 * nside ** 2,))
+    c = 0
+    for s in spin_arr:
+        nm = 1 if s == 0 else 2
+        out.append(alm2map(alm[c:c + nm], s, minfo, ainfo, precision=precision))
+        c += nm
+    return out

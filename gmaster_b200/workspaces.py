@@ -1,0 +1,222 @@
+"""MASTER workspaces and pseudo-spectra (the counterpart of gmaster/workspaces.py).
+
+`compute_coupled_cell` forms the coupled pseudo-C_ell (workspaces.py:86-125);
+`NmtWorkspace` builds the mode-coupling matrix from the masks' pseudo-spectrum with
+the FP64 Wigner-3j recursion kernel, bins it and LU-factors the binned matrix on the
+GPU, and `decouple_cell` returns bandpowers (workspaces.py:1593-2147).
+"""
+
+import numpy as np
+import torch
+
+from . import _lib
+from .bins import NmtBin
+from .utils import as_device
+
+_BLOCK_TT, _BLOCK_TE, _BLOCK_PP, _BLOCK_MM = 0, 1, 2, 3
+
+
+def pseudo_cl(alm1, alm2, lmax):
+    """(n1, nelem) x (n2, nelem) complex128 -> (n1 n2, lmax+1) float64 on the GPU."""
+    a = alm1 if alm1.ndim == 2 else alm1[None]
+    b = alm2 if alm2.ndim == 2 else alm2[None]
+    a = a.contiguous()
+    b = b.contiguous()
+    out = torch.empty((a.shape[0] * b.shape[0], lmax + 1), dtype=torch.float64, device=a.device)
+    _lib.call("gm_pseudo_cl", lmax, a.shape[0], _lib.ptr(a), b.shape[0], _lib.ptr(b),
+              _lib.ptr(out), _lib.stream_handle(a.device))
+    return out
+
+
+def compute_coupled_cell(f1, f2):
+    """Coupled pseudo-C_ell of two fields: (n1 n2, lmax+1) (workspaces.py:98-125)."""
+    if not f1.is_compatible(f2, strict=False):
+        raise ValueError("You're trying to correlate incompatible fields")
+    lmax = min(f1.ainfo.lmax, f2.ainfo.lmax)
+    return pseudo_cl(f1.get_alms(), f2.get_alms(), lmax)
+
+
+def coupling_blocks(window, lmax, which):
+    """(4, lmax+1, lmax+1) coupling blocks [tt, te, pp, mm] from a mask spectrum."""
+    w = as_device(window, torch.float64)
+    blocks = torch.empty((4, lmax + 1, lmax + 1), dtype=torch.float64, device=w.device)
+    queue = torch.zeros(1, dtype=torch.int64, device=w.device)
+    _lib.call("gm_coupling_blocks", lmax, _lib.ptr(w), w.shape[0], which, _lib.ptr(blocks),
+              _lib.ptr(queue), _lib.stream_handle(w.device))
+    return blocks
+
+
+def _which(ncls):
+    return {1: 1, 2: 2, 4: 12}[ncls]
+
+
+class LUFactor:
+    """FP64 LU factorisation with partial pivoting of a square device matrix."""
+
+    def __init__(self, a):
+        self.n = a.shape[0]
+        self.lu = a.contiguous().clone()
+        self.piv = torch.empty(self.n, dtype=torch.int32, device=a.device)
+        self.status = torch.empty(1, dtype=torch.int32, device=a.device)
+        _lib.call("gm_lu_factor", self.n, _lib.ptr(self.lu), _lib.ptr(self.piv),
+                  _lib.ptr(self.status), _lib.stream_handle(a.device))
+
+    def check(self):
+        st = int(self.status.item())
+        if st:
+            raise np.linalg.LinAlgError(f"binned coupling matrix is singular (pivot {st - 1})")
+
+    def solve(self, b):
+        """Solve A x = b for b of shape (n,) or (n, nrhs)."""
+        x = b.contiguous().clone()
+        nrhs = 1 if x.ndim == 1 else x.shape[1]
+        _lib.call("gm_lu_solve", self.n, _lib.ptr(self.lu), _lib.ptr(self.piv), nrhs, _lib.ptr(x),
+                  _lib.stream_handle(b.device))
+        return x
+
+
+class NmtWorkspace:
+    """Curved-sky MASTER workspace (gmaster/workspaces.py:1593-2255)."""
+
+    def __init__(self, fl1=None, fl2=None, bins=None, is_teb=False, l_toeplitz=-1, l_exact=-1,
+                 dl_band=-1, fname=None, normalization="MASTER"):
+        self.mcm_blocks = self.mcm_binned = self._lu = None
+        if fname is not None:
+            raise NotImplementedError("workspace files are not part of this build")
+        if fl1 is not None or fl2 is not None or bins is not None:
+            self.compute_coupling_matrix(fl1, fl2, bins, is_teb=is_teb, l_toeplitz=l_toeplitz,
+                                         l_exact=l_exact, dl_band=dl_band,
+                                         normalization=normalization)
+
+    @classmethod
+    def from_fields(cls, fl1, fl2, bins, **kwargs):
+        return cls(fl1, fl2, bins, **kwargs)
+
+    def compute_coupling_matrix(self, fl1, fl2, bins, is_teb=False, l_toeplitz=-1, l_exact=-1,
+                                dl_band=-1, normalization="MASTER"):
+        if not fl1.is_compatible(fl2, strict=False):
+            raise ValueError("Fields have incompatible pixelizations")
+        if fl1.ainfo.lmax != bins.lmax:
+            raise ValueError(f"Maximum multipoles in bins ({bins.lmax}) and fields "
+                             f"({fl1.ainfo.lmax}) are not the same")
+        if is_teb:
+            raise NotImplementedError("joint TEB workspaces are not part of this build")
+        if l_toeplitz > 0:
+            raise NotImplementedError("the Toeplitz approximation is not part of this build")
+        if normalization not in ("MASTER", "FKP"):
+            raise ValueError(f"Unknown normalization type {normalization}. "
+                             "Allowed options are 'MASTER' and 'FKP'")
+        self.spin1, self.spin2 = fl1.spin, fl2.spin
+        self.nmaps1 = 1 if self.spin1 == 0 else 2
+        self.nmaps2 = 1 if self.spin2 == 0 else 2
+        self.ncls = self.nmaps1 * self.nmaps2
+        self.lmax = fl1.ainfo.lmax
+        self.lmax_mask = fl1.ainfo_mask.lmax
+        self.bins = bins
+        self.nbands = bins.get_n_bands()
+        self.normalization = normalization
+        self.beam1 = fl1.beam
+        self.beam2 = fl2.beam
+        alm1 = fl1.get_mask_alms()
+        alm2 = alm1 if fl2 is fl1 else fl2.get_mask_alms()
+        self.pcl_mask = pseudo_cl(alm1[None], alm2[None], self.lmax_mask)[0]
+        if fl2 is fl1:
+            self.pcl_mask = self.pcl_mask - fl1.Nw
+        nw = min(self.pcl_mask.shape[0], 2 * self.lmax + 1)
+        self.window = self.pcl_mask[:nw].contiguous()
+        self.mcm_blocks = coupling_blocks(self.window, self.lmax, _which(self.ncls))
+        self.wawb = 0.0
+        if normalization == "FKP":
+            self.wawb = float((fl1.get_mask() * fl2.get_mask()).sum() * fl1.minfo.weight / (4 * np.pi))
+        self._postprocess()
+
+    def _postprocess(self):
+        dev = self.mcm_blocks.device
+        ops = self.bins.device_operators(dev)
+        beam = (self.beam1 * self.beam2).contiguous()
+        N = self.ncls * self.nbands
+        if self.normalization == "FKP":
+            self.mcm_binned = self.wawb * torch.eye(N, dtype=torch.float64, device=dev)
+        else:
+            scratch = torch.empty(2 * self.nbands * self.nbands, dtype=torch.float64, device=dev)
+            self.mcm_binned = torch.empty((N, N), dtype=torch.float64, device=dev)
+            _lib.call("gm_bin_coupling_csr", self.lmax, self.nbands, self.ncls,
+                      _lib.ptr(self.mcm_blocks), _lib.ptr(ops["ptr"]), _lib.ptr(ops["ells"]),
+                      _lib.ptr(ops["wfl"]), _lib.ptr(ops["inv_fl"]), _lib.ptr(beam),
+                      _lib.ptr(scratch), _lib.ptr(self.mcm_binned), _lib.stream_handle(dev))
+        self._lu = LUFactor(self.mcm_binned)
+
+    def get_coupling_matrix(self):
+        """Dense (ncls (lmax+1))^2 MCM in ``l * ncls + c`` order (workspaces.py:2005-2025)."""
+        n = self.lmax + 1
+        b = self.mcm_blocks
+        if self.ncls == 1:
+            return b[_BLOCK_TT].clone()
+        out = torch.zeros((n, self.ncls, n, self.ncls), dtype=torch.float64, device=b.device)
+        if self.ncls == 2:
+            for c in range(2):
+                out[:, c, :, c] = b[_BLOCK_TE]
+        else:
+            for c in range(4):
+                out[:, c, :, c] += b[_BLOCK_PP]
+            for c, sign in zip(range(4), (1.0, -1.0, -1.0, 1.0)):
+                out[:, c, :, 3 - c] += sign * b[_BLOCK_MM]
+        return out.reshape(self.ncls * n, self.ncls * n)
+
+    def update_beams(self, beam1, beam2):
+        n = self.lmax + 1
+        if np.shape(beam1) != (n,) or np.shape(beam2) != (n,):
+            raise ValueError(f"The new beams must go up to ell = {self.lmax}")
+        self.beam1 = as_device(beam1, torch.float64)
+        self.beam2 = as_device(beam2, torch.float64)
+        self._postprocess()
+
+    def update_bins(self, bins):
+        if bins.lmax != self.lmax:
+            raise ValueError("The new binning scheme has a different maximum multipole")
+        self.bins = bins
+        self.nbands = bins.get_n_bands()
+        self._postprocess()
+
+    def couple_cell(self, cl_in):
+        """Theory spectra (ncls, >= lmax+1) -> expected coupled spectra (workspaces.py:2060-2104)."""
+        cl = as_device(cl_in, torch.float64)
+        if cl.ndim != 2 or cl.shape[0] != self.ncls or cl.shape[1] < self.lmax + 1:
+            raise ValueError(f"Input power spectrum has wrong shape. Expected "
+                             f"({self.ncls}, {self.lmax + 1}), but got {tuple(cl.shape)}")
+        theory = cl[:, : self.lmax + 1] * (self.beam1 * self.beam2)[None, :]
+        flat = theory.T.reshape(-1)
+        return (self.get_coupling_matrix() @ flat).reshape(self.lmax + 1, self.ncls).T
+
+    def decouple_cell(self, cl_in, cl_bias=None, cl_noise=None):
+        """Bin and decouple coupled spectra into bandpowers (workspaces.py:2106-2147)."""
+        cl = as_device(cl_in, torch.float64)
+        if cl.ndim != 2 or cl.shape[0] != self.ncls or cl.shape[1] < self.lmax + 1:
+            raise ValueError(f"Input power spectrum has wrong shape. Expected "
+                             f"({self.ncls}, {self.lmax + 1}), but got {tuple(cl.shape)}")
+        total = cl[:, : self.lmax + 1]
+        for name, bias in (("bias", cl_bias), ("noise", cl_noise)):
+            if bias is not None:
+                bias = as_device(bias, torch.float64)
+                if bias.ndim != 2 or bias.shape[0] != self.ncls or bias.shape[1] < self.lmax + 1:
+                    raise ValueError(f"Input {name} power spectrum has wrong shape")
+                total = total - bias[:, : self.lmax + 1]
+        binned = self.bins.bin_cell(total.contiguous())
+        vec = binned.T.reshape(-1).contiguous()
+        self._lu.check()
+        sol = self._lu.solve(vec)
+        return sol.reshape(self.nbands, self.ncls).T
+
+    def get_bandpower_windows(self):
+        """(ncls, nbands, ncls, lmax+1) windows W with <C_b> = sum W C_l (workspaces.py:2149-2160)."""
+        n = self.lmax + 1
+        ops = self.bins.device_operators(self.mcm_blocks.device)
+        M = self.get_coupling_matrix() * (self.beam1 * self.beam2).repeat_interleave(self.ncls)[None]
+        B = torch.zeros((self.nbands, n), dtype=torch.float64, device=M.device)
+        ells = torch.from_numpy(self.bins._ells_np.astype(np.int64)).to(M.device)
+        bp = torch.from_numpy(self.bins._bpws_np.astype(np.int64)).to(M.device)
+        B[bp, ells] = ops["wfl"][ells]
+        Bk = torch.kron(B, torch.eye(self.ncls, dtype=torch.float64, device=M.device))
+        one_sided = Bk @ M
+        win = self._lu.solve(one_sided)
+        return win.reshape(self.nbands, self.ncls, n, self.ncls).permute(1, 0, 3, 2)

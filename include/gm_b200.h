@@ -1,0 +1,171 @@
+/*
+ * gm_b200.h -- C ABI of the B200-native pseudo-C_ell MASTER hot path.
+ *
+ * Every entry point takes caller-owned device pointers (plain pointers and sizes,
+ * no framework types), launches on the caller's CUDA stream, allocates nothing and
+ * returns a gm_status.  Scratch is always a caller-provided buffer whose size is
+ * given by the matching *_workspace_bytes / size query.  No entry point
+ * synchronises the stream except where stated.
+ *
+ * Each declaration names the reference (licongxu/GMaster) interface it replaces.
+ * The reference binds its kernels as XLA FFI handlers (gmaster/_native/cuda/*.cu)
+ * or lowers the step to XLA library calls (cuFFT, cuBLAS, cuSOLVER, segment_sum);
+ * INTEGRATION.md shows the jax.ffi / ctypes binding a maintainer adds.
+ *
+ * Data layouts (all row-major, complex values interleaved re/im):
+ *   maps      (ncomp, npix)                  float64 or float32, HEALPix RING order
+ *   ringspec  (ncomp, nring, L)              complex, G_r(m) = w e^{-i m phi0_r} DFT_r[m mod nphi_r]
+ *   rhs       (L, nlanes, ncomp, 4)          real, per north lane j: [Sum re, Sum im, Diff re, Diff im]
+ *                                            with Sum/Diff = G_north(m) +- G_south(m)
+ *   syn       (L, nlanes, ncomp, 4)          real, per lane: [north re, north im, south re, south im]
+ *   alm       (nalm, nelem)                  complex128, healpy m-major packing
+ *   lanes     nlanes = 2 nside (north rings 1..2nside; the last is the equator)
+ * ncomp counts real map components: spin 0 -> one per map, spin 2 -> (Q, U) per field.
+ */
+#ifndef GM_B200_H
+#define GM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    GM_OK = 0,
+    GM_ERR_BAD_SHAPE = 1,   /* sizes inconsistent or out of the supported range */
+    GM_ERR_BAD_PTR = 2,     /* a required pointer is null or misaligned */
+    GM_ERR_LAUNCH = 3,      /* a kernel launch failed (cudaGetLastError) */
+    GM_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up */
+    GM_ERR_UNSUPPORTED = 5  /* precision / spin / option not implemented */
+} gm_status;
+
+typedef enum { GM_FP64 = 0, GM_MIXED = 1 } gm_precision;
+
+/* Last CUDA error string recorded by a failing call on this thread. */
+const char *gm_last_error(void);
+
+/* Library version string. */
+const char *gm_version(void);
+
+/* ---------------------------------------------------------------- ring stage */
+
+/* Number of twiddle entries for all ring lengths of `nside`
+ * (sum over i in [1, nside] of 2i = nside (nside + 1)).  The table buffer holds that
+ * many complex128 entries followed by the same entries as complex64
+ * (24 bytes per entry in total). */
+int64_t gm_ring_twiddle_count(int64_t nside);
+
+/* Fill the twiddle table: tw[i(i-1) + k] = exp(-2 pi i k / (4 i)), k < 2i (both copies).
+ * `shifted` arguments below are one byte per ring: 1 where phi0 = pi / nphi, 0 where
+ * phi0 = 0 (the only two HEALPix cases, utils.py:237-243).
+ * Replaces the chirp-Z constant tables of gmaster/_sht/rings.py:198-248. */
+int gm_ring_twiddles(int64_t nside, void *tw, void *stream);
+
+/* Forward ring transform of real maps (replaces rings.py:251-299
+ * `_forward_ring_fft_positive`, the XLA cuFFT belt FFT + Bluestein caps).
+ * maps: (ncomp, npix) with `map_dtype_bytes` 8 (float64) or 4 (float32).
+ * out ringspec: (ncomp, nring, L) complex128 (GM_FP64) or complex64 (GM_MIXED),
+ * including the quadrature weight 4 pi / npix and the phase e^{-i m phi0}. */
+int gm_ring_analysis(int precision, int64_t nside, int64_t L, int64_t ncomp,
+                     const void *maps, int map_dtype_bytes, const void *tw,
+                     const uint8_t *shifted, void *ringspec, void *stream);
+
+/* Hemisphere pack of a ring spectrum into the lane-major Legendre right-hand side
+ * (replaces march_v2.py:637-663 `_fold_rhs`).  rhs (L, nlanes, ncomp, 4). */
+int gm_pack_rhs(int precision, int64_t nside, int64_t L, int64_t ncomp,
+                const void *ringspec, void *rhs, void *stream);
+
+/* Ring-fold residual in lane space (replaces march_v2.cu:426-493
+ * `ring_fold_residual` + march_v2.py:614-633): for every lane and order m,
+ *   rhs_out = pack( w nphi e^{-i m phi0} sum_{m' = m mod nphi, |m'| < L} c(m') e^{i m' phi0} )
+ *             - rhs_map
+ * where c comes from `syn` (c(-m') = conj c(m')).  This is the analysis-side ring
+ * spectrum of the map synthesised from `syn`, minus the input map's, without any FFT. */
+int gm_fold_residual(int precision, int64_t nside, int64_t L, int64_t ncomp,
+                     const void *syn, const void *rhs_map, const uint8_t *shifted,
+                     void *rhs_out, void *stream);
+
+/* Inverse ring transform (replaces rings.py:477-524 `_inverse_ring_fft_herm` and
+ * healpix.py:462-471): maps[c][p] = sum_{|m| < L} c_r(m) e^{i m phi_p} with the
+ * per-lane coefficients in `syn`.  maps written as float64. */
+int gm_ring_synthesis(int precision, int64_t nside, int64_t L, int64_t ncomp,
+                      const void *syn, const void *tw, const uint8_t *shifted,
+                      double *maps, void *stream);
+
+/* ----------------------------------------------------------- Legendre stage */
+
+/* Per-order seed table length (doubles) for spin s: 3 variants x 4 x L. */
+int64_t gm_seed_table_len(int64_t L);
+
+/* Spherical-harmonic analysis, latitudinal step (replaces march_v2.cu:155-285
+ * `march_analysis` via march_v2.py:666-693 and 817-872):
+ *   alm[f][idx(l,m)] += scale * sum_lanes lambda_lm(theta_j) rhs(...)
+ * spin 0: ncomp maps -> nalm = ncomp rows; spin 2: ncomp = 2 nfields ->
+ * nalm = 2 nfields rows (E, B per field).
+ * lane_geom: (3, nlanes) float64 [cos theta, log2 sin(theta/2), log2 cos(theta/2)].
+ * seeds: gm_seed_table_len(L) doubles (see gmaster_b200/sht.py).
+ * alm is accumulated with double-precision atomics: zero it first for a fresh analysis. */
+int gm_legendre_analysis(int precision, int spin, int64_t nside, int64_t lmax,
+                         int64_t ncomp, const double *lane_geom, const double *seeds,
+                         const void *rhs, double *alm, double scale, void *stream);
+
+/* Synthesis, latitudinal step (replaces march_v2.cu:291-407 `march_synthesis` via
+ * march_v2.py:752-795 and 886-924): syn(m, lane, comp) from alm. */
+int gm_legendre_synthesis(int precision, int spin, int64_t nside, int64_t lmax,
+                          int64_t ncomp, const double *lane_geom, const double *seeds,
+                          const double *alm, void *syn, void *stream);
+
+/* ------------------------------------------------------------- spectra */
+
+/* Coupled pseudo-C_ell of all component pairs (replaces workspaces.py:86-95
+ * `_compute_coupled_cell`): cls[(i n2 + j) (lmax+1) + l]. */
+int gm_pseudo_cl(int64_t lmax, int64_t n1, const double *alm1, int64_t n2,
+                 const double *alm2, double *cls, void *stream);
+
+/* Coupling blocks by the Wigner-3j three-term recursion in l3 (replaces
+ * workspaces.py:352-517 `_coupling_matrix_tt` and 682-924 `_general_coupling_matrix`
+ * / `_coupling_matrices_spin2`, and coupling_tt.cu:18-45):
+ *   S_x[l1][l2] = sum_l3 (2 l3 + 1) W_l3 / (4 pi) * T_x(l1, l2, l3)
+ *   with T_tt = (l1 l2 l3;000)^2, T_te = (000)(2 -2 0) (even J),
+ *   T_pp = (2 -2 0)^2 (even J), T_mm = (2 -2 0)^2 (odd J),
+ *   blocks[x][l1][l2] = (2 l2 + 1) S_x[l1][l2]; `which` is a bit mask
+ *   (1 tt, 2 te, 4 pp, 8 mm); blocks is (4, lmax+1, lmax+1) float64.
+ * window has nw entries (entries beyond nw are zero).
+ * Persistent kernel with a device work queue: `queue` is one int64 the kernel uses as
+ * its counter (zeroed by this call). */
+int gm_coupling_blocks(int64_t lmax, const double *window, int64_t nw, int which,
+                       double *blocks, int64_t *queue, void *stream);
+
+/* Binned coupling matrix B M diag(beam) T for ncls in {1, 2, 4} (replaces
+ * workspaces.py:1570-1590 `_banded_operators` and :292-310 `_BlockMCM.banded`).
+ * The binning is given in CSR form: band b holds multipoles band_ells[band_ptr[b] ..
+ * band_ptr[b+1]); wfl (lmax+1) = weight * f_ell, inv_fl (lmax+1) = 1 / f_ell,
+ * beam (lmax+1) = beam1 * beam2.  blocks is the (4, lmax+1, lmax+1) output of
+ * gm_coupling_blocks.  scratch holds 2 nbands^2 doubles.  out is (ncls nb)^2 float64 in
+ * band-major, channel-minor order with the reference's block slots and signs
+ * (workspaces.py:1856-1912). */
+int gm_bin_coupling_csr(int64_t lmax, int64_t nbands, int ncls, const double *blocks,
+                        const int32_t *band_ptr, const int32_t *band_ells, const double *wfl,
+                        const double *inv_fl, const double *beam, double *scratch, double *out,
+                        void *stream);
+
+/* Bin spectra: out[c][b] = sum_{l in b} wfl[l] cls[c][l] (bins.py:15-20). */
+int gm_bin_cells_csr(int64_t lmax, int64_t nbands, int64_t ncls, const double *cls,
+                     const int32_t *band_ptr, const int32_t *band_ells, const double *wfl,
+                     double *out, void *stream);
+
+/* In-place LU factorisation with partial pivoting of an n x n float64 matrix and
+ * solve of nrhs right-hand sides (replaces the cuSOLVER getrf/getrs behind
+ * jnp.linalg.solve, workspaces.py:2146).  piv: n int32.  status: one int32 set to
+ * 0 on success or k+1 when the k-th pivot is exactly zero. */
+int gm_lu_factor(int64_t n, double *a, int32_t *piv, int32_t *status, void *stream);
+int gm_lu_solve(int64_t n, const double *lu, const int32_t *piv, int64_t nrhs,
+                double *b, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GM_B200_H */
