@@ -1,0 +1,130 @@
+"""Host-side logic of gmaster_b200 (no GPU): geometry, seeds, binning, C ABI exports."""
+
+import ctypes
+import math
+import re
+
+import numpy as np
+import pytest
+
+import oracle
+from gmaster_b200 import _build, sht
+from gmaster_b200.bins import NmtBin
+
+
+@pytest.mark.parametrize("nside", [1, 2, 4, 64, 2048])
+def test_product_geometry_bit_exact(nside):
+    g = np.load("tests/golden/geometry.npz")
+    theta, phi0, nphi, off = sht.ring_geometry(nside)
+    assert np.array_equal(theta, g[f"theta_{nside}"])
+    assert np.array_equal(phi0, g[f"phi0_{nside}"])
+    assert np.array_equal(nphi.astype(np.int64), g[f"nphi_{nside}"])
+    assert np.array_equal(off.astype(np.int64), g[f"offsets_{nside}"])
+
+
+def test_ring_offsets_formula_matches_cumsum():
+    """The kernels compute ring_nphi / ring_offset in closed form (gm_common.cuh)."""
+    for nside in (1, 2, 3, 8, 64):
+        _, _, nphi, off = sht.ring_geometry(nside)
+        npix = 12 * nside * nside
+        for r in range(4 * nside - 1):
+            ring = r + 1
+            north = 4 * nside - ring if ring > 2 * nside else ring
+            n = 4 * north if north < nside else 4 * nside
+            if ring < nside:
+                o = 2 * ring * (ring - 1)
+            elif ring <= 3 * nside:
+                o = 2 * nside * (nside - 1) + (ring - nside) * 4 * nside
+            else:
+                k = 4 * nside - ring
+                o = npix - 2 * k * (k + 1)
+            assert n == nphi[r] and o == off[r]
+
+
+def test_shifted_flags():
+    for nside in (1, 4, 32):
+        flags = sht.shifted_flags(nside)
+        _, phi0, nphi, _ = sht.ring_geometry(nside)
+        assert np.array_equal(flags == 1, phi0 > 0)
+
+
+@pytest.mark.parametrize("m", [0, 1, 2, 3, 10, 150])
+def test_seed_table_reproduces_first_row(m):
+    """sign * 2^(log2N + pc log2 cos + ps log2 sin) is lambda_{l0,m} of the oracle."""
+    L = 200
+    seeds = sht.seed_table(L)
+    for var, sp in ((0, 0), (1, -2), (2, 2)):
+        l0 = max(m, abs(sp))
+        for th in (0.3, 1.1, np.pi / 2):
+            lg, sign, pc, ps = seeds[var, m]
+            f = lg + pc * math.log2(math.cos(th / 2)) + ps * math.log2(math.sin(th / 2))
+            val = sign * 2.0 ** f
+            want = oracle.lambda_row(L - 1, m, sp, th)[l0]
+            if abs(want) > 1e-250:
+                assert abs(val - want) <= 1e-12 * abs(want)
+
+
+def test_nmtbin_linear_matches_reference_bands():
+    g = np.load("tests/golden/bins.npz")
+    b = NmtBin.from_lmax_linear(191, 16)
+    keep = g["bpws_191_16"] >= 0
+    assert np.array_equal(b._ells_np, g["ells_191_16"][keep])
+    assert np.array_equal(b._bpws_np, g["bpws_191_16"][keep])
+    assert b.get_n_bands() == int(g["bpws_191_16"].max()) + 1
+    np.testing.assert_allclose(b.get_weight_list(0), np.full(16, 1 / 16))
+
+
+def test_nmtbin_edges_and_dell():
+    b = NmtBin.from_edges([2, 10, 30], [10, 30, 50], is_Dell=True)
+    assert b.get_n_bands() == 3
+    assert b.lmax == 49
+    np.testing.assert_allclose(b.get_fell_list(1), np.arange(10, 30) * np.arange(11, 31) / (2 * np.pi))
+    with pytest.raises(RuntimeError):
+        NmtBin(bpws=[0, 0], ells=[2, 3], weights=[0, 0])
+
+
+def _header_symbols():
+    text = open("include/gm_b200.h").read()
+    return sorted(set(re.findall(r"^(?:int|int64_t|const char \*)\s*(gm_\w+)\(", text, re.M)))
+
+
+def test_cabi_library_exports_every_header_symbol():
+    """The in-tree library loads on a CPU-only host and exports every declared entry point
+    (no compute calls without a GPU)."""
+    _build.build()
+    lib = ctypes.CDLL(_build.LIB)
+    syms = _header_symbols()
+    assert len(syms) >= 15
+    for name in syms:
+        assert hasattr(lib, name), name
+    lib.gm_version.restype = ctypes.c_char_p
+    assert b"sm_100a" in lib.gm_version()
+    lib.gm_ring_twiddle_count.restype = ctypes.c_int64
+    lib.gm_ring_twiddle_count.argtypes = [ctypes.c_int64]
+    assert lib.gm_ring_twiddle_count(2048) == 2048 * 2049
+
+
+def test_python_binding_covers_header():
+    from gmaster_b200 import _lib
+
+    for name in _header_symbols():
+        assert name in _lib.SIGNATURES, name
+
+
+def test_product_never_imports_oracle():
+    import pathlib
+
+    for path in pathlib.Path("gmaster_b200").rglob("*.py"):
+        text = path.read_text()
+        assert "import oracle" not in text and "from oracle" not in text, path
+
+
+def test_compute_without_gpu_fails_loudly():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("CUDA present")
+    from gmaster_b200 import _lib
+
+    with pytest.raises(RuntimeError):
+        _lib.require_cuda()
