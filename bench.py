@@ -1,0 +1,463 @@
+#!/usr/bin/env python
+"""Throughput of the pseudo-C_ell MASTER estimator on B200 GPUs.
+
+Workload (the Nside 2048 configuration): T, Q, U maps at Nside 2048 (lmax 6143) drawn
+from C_TT = 1e3/(l+10)^2, C_EE = 0.05 C_TT, C_BB = 0.005 C_TT, C_TE = 0.3 sqrt(C_TT C_EE);
+binary mask |b| > 20 deg about a pole tilted to (theta, phi) = (30, 45) deg with 2000
+point-source holes of 5 arcmin (seeded), C1-apodised at 1 deg; n_iter = 3; bands of 16.
+
+One step = one Monte-Carlo simulation through the estimator with a shared, precomputed
+workspace: NmtField(T) and NmtField(Q, U) (map2alm with 3 Jacobi iterations each),
+compute_coupled_cell for TT, TE/TB and EE/EB/BE/BB, and decouple_cell with the three
+binned coupling matrices.  `value` is sims/s with the maps resident on the device;
+`e2e` is the same through the public API from pinned host maps (host->device copy of
+the maps and device->host copy of the bandpowers inside the timed region).  Inputs
+(400 MB per map) are larger than the 126 MB L2, so no explicit flush is needed.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+Under torchrun each rank runs independent simulations (replicas, no collective on the
+data path); value is the total over ranks divided by the max-over-ranks device time.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "MASTER sims/s, Nside 2048 TQU (shared workspace, n_iter=3), mixed precision"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=4)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--nside", type=int, default=2048)
+    p.add_argument("--nlb", type=int, default=16)
+    p.add_argument("--fp64-steps", type=int, default=1)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+# ----------------------------------------------------------------------------- inputs
+
+def config_spectra(lmax):
+    ell = np.arange(lmax + 1, dtype=np.float64)
+    tt = 1e3 / (ell + 10.0) ** 2
+    tt[:2] = 0
+    ee, bb = 0.05 * tt, 0.005 * tt
+    te = 0.3 * np.sqrt(tt * ee)
+    return tt, ee, bb, te
+
+
+def make_mask(nside, device, seed=4, nholes=2000, hole_arcmin=5.0, cut_deg=20.0, apo_deg=1.0):
+    """Analytic C1-apodised mask of the Nside 2048 recipe, built on the GPU.
+
+    The angular distance of each observed pixel to the masked region is the smaller of
+    (|b| - cut) and (distance to the nearest hole centre - hole radius); the C1 factor
+    x - sin(2 pi x)/(2 pi), x = sqrt((1 - cos d)/(1 - cos apo)), is applied within apo.
+    """
+    import torch
+
+    from gmaster_b200.utils import pix2vec_ring
+
+    vec = torch.from_numpy(pix2vec_ring(nside)).to(device)
+    th, ph = np.radians(30.0), np.radians(45.0)
+    pole = torch.tensor([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)],
+                        dtype=torch.float64, device=device)
+    rng = np.random.default_rng(seed)
+    centres = rng.normal(size=(nholes, 3))
+    centres /= np.linalg.norm(centres, axis=1)[:, None]
+    cen = torch.from_numpy(centres).to(device)
+    blat = torch.arcsin((vec @ pole).abs().clamp(max=1.0))
+    d = blat - np.radians(cut_deg)
+    r = np.radians(hole_arcmin / 60.0)
+    chunk = 1 << 20
+    for s in range(0, vec.shape[0], chunk):
+        cosang = (vec[s:s + chunk] @ cen.T).max(dim=1).values.clamp(-1.0, 1.0)
+        d[s:s + chunk] = torch.minimum(d[s:s + chunk], torch.arccos(cosang) - r)
+    mask = (d > 0).to(torch.float64)
+    apo = np.radians(apo_deg)
+    x = torch.sqrt((1 - torch.cos(d.clamp(min=0))) / (1 - np.cos(apo)))
+    c1 = x - torch.sin(2 * np.pi * x) / (2 * np.pi)
+    mask = torch.where((d > 0) & (d < apo), c1, mask)
+    return mask.contiguous()
+
+
+def make_sims(nside, nsims, seed, device):
+    """TQU maps of `nsims` Gaussian simulations (float64 on the device)."""
+    import torch
+
+    from gmaster_b200 import sht
+    from gmaster_b200.utils import gaussian_alm
+
+    lmax = 3 * nside - 1
+    tt, ee, bb, te = config_spectra(lmax)
+    cov = np.zeros((3, 3, lmax + 1))
+    cov[0, 0], cov[1, 1], cov[2, 2] = tt, ee, bb
+    cov[0, 1] = cov[1, 0] = te
+    sims = []
+    for i in range(nsims):
+        alm = gaussian_alm(cov, lmax, np.random.default_rng(seed + i))
+        a = torch.from_numpy(alm).to(device)
+        t = sht.alm2map_device(a[:1].contiguous(), 0, nside, lmax, "fp64")
+        qu = sht.alm2map_device(a[1:].contiguous(), 2, nside, lmax, "fp64")
+        sims.append((t, qu))
+        del a
+    return sims
+
+
+# ----------------------------------------------------------------------------- estimator
+
+def build_workspaces(mask, nside, nlb, precision):
+    import gmaster_b200 as nmt
+
+    f0 = nmt.NmtField(mask, None, spin=0, precision=precision)
+    f2 = nmt.NmtField(mask, None, spin=2, precision=precision)
+    f2.alm_mask = f0.get_mask_alms()
+    b = nmt.NmtBin.from_nside_linear(nside, nlb)
+    return b, {
+        "00": nmt.NmtWorkspace.from_fields(f0, f0, b),
+        "02": nmt.NmtWorkspace.from_fields(f0, f2, b),
+        "22": nmt.NmtWorkspace.from_fields(f2, f2, b),
+    }
+
+
+def estimator_step(mask, t, qu, ws, precision):
+    """One simulation through fields, coupled spectra and decoupling."""
+    import gmaster_b200 as nmt
+
+    ft = nmt.NmtField(mask, t, n_iter=3, lite=True, precision=precision)
+    fp = nmt.NmtField(mask, qu, n_iter=3, lite=True, precision=precision)
+    return (ws["00"].decouple_cell(nmt.compute_coupled_cell(ft, ft)),
+            ws["02"].decouple_cell(nmt.compute_coupled_cell(ft, fp)),
+            ws["22"].decouple_cell(nmt.compute_coupled_cell(fp, fp)))
+
+
+def full_estimator(mask, t, qu, nside, nlb, precision):
+    """The whole estimator from the maps: fields with their mask transforms, three
+    workspaces (pseudo-C_ell of the mask, 3j coupling, binning, LU), spectra."""
+    import gmaster_b200 as nmt
+
+    ft = nmt.NmtField(mask, t, n_iter=3, precision=precision)
+    fp = nmt.NmtField(mask, qu, n_iter=3, precision=precision)
+    b = nmt.NmtBin.from_nside_linear(nside, nlb)
+    out = []
+    for f1, f2 in ((ft, ft), (ft, fp), (fp, fp)):
+        w = nmt.NmtWorkspace.from_fields(f1, f2, b)
+        out.append(w.decouple_cell(nmt.compute_coupled_cell(f1, f2)))
+    return out
+
+
+# ----------------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.file = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for k, name in enumerate(names):
+                if len(r) > 5 + k and "Active" in r[5 + k] and "Not" not in r[5 + k]:
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(np.max(mx)) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- CPU legs
+
+def cpu_oracle_sample(nside, seconds_hint=20.0):
+    """Time the FP64 oracle on a bounded sample of one simulation's transform work and
+    extrapolate to sims/s.  The oracle runs a ring FFT of every ring and the Legendre
+    sums for a sample of orders (spin 0 and spin 2); the per-order Legendre cost scales
+    with (L - m), so the full pass time is the ring time plus the sampled Legendre time
+    times sum_m (L - m) / sum_sample (L - m).  One simulation is 7 passes of each spin
+    (4 analyses + 3 syntheses of map2alm with n_iter = 3; a synthesis costs what an
+    analysis costs in the oracle)."""
+    import oracle
+
+    oracle.build()
+    lmax = 3 * nside - 1
+    L = lmax + 1
+    rng = np.random.default_rng(0)
+    npix = 12 * nside ** 2
+    m0 = rng.normal(size=npix)
+    qu = rng.normal(size=(2, npix))
+    orders = np.arange(0, L, max(1, L // 8))
+    t0 = time.perf_counter()
+    oracle.ring_analysis(nside, L, m0.astype(np.complex128))
+    t_ring0 = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oracle.ana0_orders(m0, nside, lmax, orders)
+    t_a0 = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oracle.ana2_orders(qu, nside, lmax, orders)
+    t_a2 = time.perf_counter() - t0
+    t_ring2 = 2 * t_ring0  # the spin-2 ring stage transforms Q + iU over m in (-L, L)
+    w_all = L * (L + 1) / 2
+    w_s = float(np.sum(L - orders))
+    leg0 = max(t_a0 - t_ring0, 0.0) * w_all / w_s
+    leg2 = max(t_a2 - t_ring2, 0.0) * w_all / w_s
+    sim_seconds = 7 * (t_ring0 + leg0) + 7 * (t_ring2 + leg2)
+    wall = t_ring0 + t_a0 + t_a2
+    return {
+        "value": 1.0 / sim_seconds,
+        "unit": "sims/s",
+        "cores": os.cpu_count(),
+        "kind": "port",
+        "sample": (f"FP64 C oracle (OpenMP, {os.cpu_count()} threads): ring FFT of all "
+                   f"{4 * nside - 1} rings + spin-0 and spin-2 Legendre sums for {len(orders)} of "
+                   f"{L} orders at Nside {nside}, {wall:.1f} s wall, extrapolated by "
+                   f"sum(L-m) to 7 spin-0 + 7 spin-2 passes per simulation"),
+        "sample_wall_s": wall,
+        "seconds_per_sim": sim_seconds,
+    }
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    steps = []
+    for _ in range(args.warmup + args.steps):
+        steps.append(cpu_oracle_sample(args.nside))
+    timed = steps[args.warmup:]
+    value = float(np.median([s["value"] for s in timed]))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "sims/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"Nside {args.nside} TQU MASTER simulation, n_iter=3",
+                   "nside": args.nside, "lmax": 3 * args.nside - 1},
+        "cpu_baseline": {k: timed[-1][k] for k in ("kind", "cores", "sample")} | {"value": value,
+                                                                                  "unit": "sims/s"},
+        "e2e": {"value": value, "unit": "sims/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- GPU leg
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    import gmaster_b200 as nmt
+    from gmaster_b200 import _lib, sht
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=dev)
+    nside, nlb = args.nside, args.nlb
+    lmax = 3 * nside - 1
+    mask = make_mask(nside, dev)
+    sims = make_sims(nside, 2, 1000 + 10 * rank, dev)
+    host_sims = [(t.cpu().pin_memory(), qu.cpu().pin_memory()) for t, qu in sims]
+    torch.cuda.synchronize()
+
+    # full estimator from scratch (seconds per spectrum), after one untimed warm-up
+    s_per_spec = {}
+    for prec in ("mixed", "fp64"):
+        full_estimator(mask, sims[0][0], sims[0][1], nside, nlb, prec)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        full_estimator(mask, sims[0][0], sims[0][1], nside, nlb, prec)
+        torch.cuda.synchronize()
+        s_per_spec[prec] = time.perf_counter() - t0
+
+    _, ws_mixed = build_workspaces(mask, nside, nlb, "mixed")
+    _, ws_fp64 = build_workspaces(mask, nside, nlb, "fp64")
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed_loop(fn, warmup, steps):
+        for i in range(warmup):
+            fn(i)
+        barrier()
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record()
+        for i in range(steps):
+            fn(i)
+        end.record()
+        barrier()
+        ms = start.elapsed_time(end)
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    # device-resident value (mixed), with Legendre kernel events and clocks
+    sampler = ClockSampler(local)
+    calls0 = dict(_lib.CALLS)
+    sht.TIMER = []
+
+    def dev_step(i):
+        t, qu = sims[i % len(sims)]
+        estimator_step(mask, t, qu, ws_mixed, "mixed")
+
+    for i in range(args.warmup):
+        dev_step(i)
+    sht.TIMER.clear()
+    calls0 = dict(_lib.CALLS)
+    sampler.start()
+    ms = timed_loop(dev_step, 0, args.steps)
+    clocks = sampler.stop()
+    launches = sum(_lib.CALLS.get(k, 0) - calls0.get(k, 0) for k in _lib.CALLS)
+    events = list(sht.TIMER)
+    sht.TIMER = None
+    torch.cuda.synchronize()
+    ktime = {}
+    kflops = {}
+    for kind, a, b, fl in events:
+        ktime[kind] = ktime.get(kind, 0.0) + a.elapsed_time(b)
+        kflops[kind] = kflops.get(kind, 0.0) + fl
+    leg_ms = sum(ktime.values())
+    leg_flops = sum(kflops.values())
+    dominant = max(ktime, key=ktime.get)
+    n_dom = sum(1 for e in events if e[0] == dominant)
+    value = world * args.steps / (ms / 1e3)
+
+    # e2e through the public API from pinned host memory
+    h2d = sum(x.numel() * x.element_size() for x in host_sims[0])
+
+    def e2e_step(i):
+        t, qu = host_sims[i % len(host_sims)]
+        out = estimator_step(mask, t, qu, ws_mixed, "mixed")
+        for o in out:
+            o.cpu()
+
+    ms_e2e = timed_loop(e2e_step, 1, args.steps)
+    d2h = sum(o.numel() * 8 for o in estimator_step(mask, *sims[0], ws_mixed, "mixed"))
+    value_e2e = world * args.steps / (ms_e2e / 1e3)
+
+    # FP64 comparison and bandpower agreement on the same simulation
+    ms64 = timed_loop(lambda i: estimator_step(mask, *sims[i % 2], ws_fp64, "fp64"), 1,
+                      args.fp64_steps)
+    value64 = world * args.fp64_steps / (ms64 / 1e3)
+    mixed_bp = [o.cpu().numpy() for o in estimator_step(mask, *sims[0], ws_mixed, "mixed")]
+    fp64_bp = [o.cpu().numpy() for o in estimator_step(mask, *sims[0], ws_fp64, "fp64")]
+    errs = {}
+    for name, a, b in zip(("00", "02", "22"), mixed_bp, fp64_bp):
+        scale = np.max(np.abs(b), axis=1, keepdims=True)
+        errs[name] = float(np.max(np.abs(a - b) / scale))
+    auto = [(mixed_bp[0][0], fp64_bp[0][0]), (mixed_bp[2][0], fp64_bp[2][0]),
+            (mixed_bp[2][3], fp64_bp[2][3])]
+    rel_auto = float(max(np.max(np.abs(a - b) / np.abs(b)) for a, b in auto))
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    import json as _json
+
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peaks = _json.load(fh)
+    except OSError:
+        pass
+    peak = peaks.get("bf16_tflops", 1590.0)
+    dom_tflops = kflops[dominant] / (ktime[dominant] / 1e3) / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": "sims/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 contraction, f64 recurrence/accumulation", "data": "synthetic",
+        "config": {
+            "workload": f"Nside {nside} TQU simulation through NmtField x2, compute_coupled_cell x3, "
+                        f"decouple_cell x3 (shared workspaces), n_iter=3, nlb={nlb}",
+            "nside": nside, "lmax": lmax, "nlb": nlb, "sims_per_step": 1,
+            "l2_flush": "inputs (400 MB maps) larger than L2", "parallelism": f"replicas{world}",
+        },
+        "e2e": {"value": value_e2e, "unit": "sims/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "roofline": {
+            "bound": "tensor", "kernel": dominant,
+            "achieved": dom_tflops, "peak": peak, "unit": "TFLOP/s",
+            "frac": dom_tflops / peak, "traffic": None,
+            "note": "algorithmic flops per launch (4 per complex MAC) / CUDA-event launch time; "
+                    "peak = measured bf16 (MEASURED_PEAKS.json)",
+            "launches": n_dom, "avg_ms": ktime[dominant] / n_dom,
+        },
+        "legendre_share_of_step": leg_ms / ms,
+        "legendre_tflops": leg_flops / (leg_ms / 1e3) / 1e12,
+        "fp64": {"value": value64, "unit": "sims/s", "ms_per_step": ms64 / args.fp64_steps},
+        "speedup_mixed_vs_fp64": value / value64,
+        "s_per_spectrum": s_per_spec,
+        "bandpower_err_mixed_vs_fp64": {"max_abs_over_scale": errs, "max_rel_auto": rel_auto},
+        "clocks": clocks,
+        "gpu_launches": int(launches),
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = {k: v for k, v in cpu_oracle_sample(nside).items()
+                                if k in ("value", "unit", "cores", "kind", "sample")}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

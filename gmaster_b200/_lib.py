@@ -54,6 +54,11 @@ MIXED = 1
 
 _lib = None
 
+# Kernel launches made by each entry point (for launch accounting); default 1.
+LAUNCHES = {"gm_last_error": 0, "gm_version": 0, "gm_ring_twiddle_count": 0,
+            "gm_seed_table_len": 0, "gm_bin_coupling_csr": 3}
+CALLS = {}
+
 
 def load():
     """Load the CUDA library (raises RuntimeError if it is missing or broken)."""
@@ -88,6 +93,7 @@ def call(name, *args):
     """Call a status-returning entry point and raise GMError on failure."""
     fn = getattr(load(), name)
     status = fn(*args)
+    CALLS[name] = CALLS.get(name, 0) + LAUNCHES.get(name, 1)
     if status != 0:
         detail = load().gm_last_error()
         raise GMError(name, status, detail.decode() if detail else "")

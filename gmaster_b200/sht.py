@@ -27,6 +27,31 @@ from . import _lib
 _PLANS = {}
 _PLAN_LOCK = threading.Lock()
 
+# Optional kernel timer: when set to a list, every Legendre launch appends
+# (kind, start_event, end_event, algorithmic_flops) recorded on the current stream.
+TIMER = None
+
+
+def legendre_flops(plan, spin, ncomp):
+    """Algorithmic flops of one Legendre pass: one complex MAC (4 flops) per
+    (l, m, northern lane) per map for spin 0 (4 N_north L(L+1)/2 per map), and per
+    (l, m in (-L, L), ring) per (Q, U) pair for spin 2 (4 nring L^2)."""
+    if spin == 0:
+        return 4.0 * plan.nlanes * plan.L * (plan.L + 1) / 2 * ncomp
+    return 4.0 * plan.nring * plan.L * plan.L * (ncomp // 2)
+
+
+def _timed(kind, plan, spin, ncomp, fn):
+    if TIMER is None:
+        fn()
+        return
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record()
+    fn()
+    end.record()
+    TIMER.append((kind, start, end, legendre_flops(plan, spin, ncomp)))
+
 
 # ----------------------------------------------------------------------------- geometry
 
@@ -190,17 +215,19 @@ def pack_rhs(plan, spec, prec):
 
 def legendre_analysis(plan, spin, rhs, alm, scale, prec):
     ncomp = rhs.shape[2]
-    _lib.call("gm_legendre_analysis", prec, spin, plan.nside, plan.lmax, ncomp,
-              _lib.ptr(plan.geom), _lib.ptr(plan.seeds), _lib.ptr(rhs), _lib.ptr(alm),
-              float(scale), _lib.stream_handle(plan.device))
+    _timed(f"legendre_analysis_s{spin}", plan, spin, ncomp, lambda: _lib.call(
+        "gm_legendre_analysis", prec, spin, plan.nside, plan.lmax, ncomp,
+        _lib.ptr(plan.geom), _lib.ptr(plan.seeds), _lib.ptr(rhs), _lib.ptr(alm),
+        float(scale), _lib.stream_handle(plan.device)))
 
 
 def legendre_synthesis(plan, spin, alm, ncomp, prec, out=None):
     syn = out if out is not None else torch.empty(
         (plan.L, plan.nlanes, ncomp, 4), dtype=_real_dtype(prec), device=plan.device)
-    _lib.call("gm_legendre_synthesis", prec, spin, plan.nside, plan.lmax, ncomp,
-              _lib.ptr(plan.geom), _lib.ptr(plan.seeds), _lib.ptr(alm), _lib.ptr(syn),
-              _lib.stream_handle(plan.device))
+    _timed(f"legendre_synthesis_s{spin}", plan, spin, ncomp, lambda: _lib.call(
+        "gm_legendre_synthesis", prec, spin, plan.nside, plan.lmax, ncomp,
+        _lib.ptr(plan.geom), _lib.ptr(plan.seeds), _lib.ptr(alm), _lib.ptr(syn),
+        _lib.stream_handle(plan.device)))
     return syn
 
 

@@ -82,8 +82,9 @@ class NmtAlmInfo:
 
     def ell_m(self):
         """(ell, m) of every packed coefficient (numpy int64)."""
-        ell = np.concatenate([np.arange(mm, self.lmax + 1) for mm in range(self.lmax + 1)])
-        order = np.repeat(np.arange(self.lmax + 1), self.lmax + 1 - np.arange(self.lmax + 1))
+        L = self.lmax + 1
+        order = np.repeat(np.arange(L), L - np.arange(L))
+        ell = np.arange(self.nelem) - self.mstart.astype(np.int64)[order]
         return ell, order
 
 
@@ -191,15 +192,14 @@ def gaussian_alm(cls, lmax, rng):
     ell, order = info.ell_m()
     z = (rng.normal(size=(n, info.nelem)) + 1j * rng.normal(size=(n, info.nelem))) / np.sqrt(2)
     z[:, order == 0] = z[:, order == 0].real * np.sqrt(2)
-    out = np.zeros((n, info.nelem), dtype=np.complex128)
-    for l in range(L):
-        cov = cls[:, :, l]
-        if not np.any(cov):
-            continue
-        w, v = np.linalg.eigh(cov)
-        root = v * np.sqrt(np.maximum(w, 0))
-        sel = ell == l
-        out[:, sel] = root @ z[:, sel]
+    cov = np.moveaxis(cls[:, :, :L], 2, 0)                      # (L, n, n)
+    w, v = np.linalg.eigh(cov)
+    root = v * np.sqrt(np.maximum(w, 0))[:, None, :]            # (L, n, n)
+    out = np.empty((n, info.nelem), dtype=np.complex128)
+    chunk = 1 << 22
+    for s in range(0, info.nelem, chunk):
+        r = root[ell[s:s + chunk]]                              # (c, n, n)
+        out[:, s:s + chunk] = np.einsum("cij,jc->ic", r, z[:, s:s + chunk])
     return out
 
 

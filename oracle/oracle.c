@@ -84,9 +84,10 @@ static int smallest_factor(int64_t n)
 }
 
 /* x: n complex values read with stride `stride` (interleaved re/im),
- * y: n complex values written contiguously. */
-static void dft_rec(int64_t n, const double *x, int64_t stride, double *y, int sign,
-                    double *work)
+ * y: n complex values written contiguously.  tw holds exp(sign 2 pi i k / N) for the
+ * top-level length N; this level uses tw[(k * tstride) mod N] with tstride = N / n. */
+static void dft_rec(int64_t n, const double *x, int64_t stride, double *y, const double *tw,
+                    int64_t N, int64_t tstride, double *work)
 {
     if (n == 1) {
         y[0] = x[0];
@@ -95,17 +96,16 @@ static void dft_rec(int64_t n, const double *x, int64_t stride, double *y, int s
     }
     int p = smallest_factor(n);
     int64_t q = n / p;
-    /* sub-transforms of the p decimated sequences, stored contiguously in work */
     for (int r = 0; r < p; ++r)
-        dft_rec(q, x + 2 * r * stride, stride * p, work + 2 * r * q, sign,
+        dft_rec(q, x + 2 * r * stride, stride * p, work + 2 * r * q, tw, N, tstride * p,
                 work + 2 * n);
     for (int64_t k = 0; k < q; ++k) {
         for (int v = 0; v < p; ++v) {
             int64_t kk = k + v * q;
             double sr = 0.0, si = 0.0;
             for (int r = 0; r < p; ++r) {
-                double ang = sign * 2.0 * M_PI * (double)((r * kk) % n) / (double)n;
-                double c = cos(ang), s = sin(ang);
+                int64_t e = ((r * kk) % n) * tstride;
+                double c = tw[2 * e], s = tw[2 * e + 1];
                 double ar = work[2 * (r * q + k)], ai = work[2 * (r * q + k) + 1];
                 sr += ar * c - ai * s;
                 si += ar * s + ai * c;
@@ -120,8 +120,15 @@ static void dft_rec(int64_t n, const double *x, int64_t stride, double *y, int s
 void orc_dft(int64_t n, const double *x, double *y, int sign)
 {
     double *work = (double *)malloc(sizeof(double) * 8 * (size_t)n + 64);
-    dft_rec(n, x, 1, y, sign, work);
+    double *tw = (double *)malloc(sizeof(double) * 2 * (size_t)n);
+    for (int64_t k = 0; k < n; ++k) {
+        double ang = sign * 2.0 * M_PI * (double)k / (double)n;
+        tw[2 * k] = cos(ang);
+        tw[2 * k + 1] = sin(ang);
+    }
+    dft_rec(n, x, 1, y, tw, n, 1, work);
     free(work);
+    free(tw);
 }
 
 /* ------------------------------------------------------------------------- */
@@ -705,4 +712,43 @@ void orc_coupling_quadrature(int64_t lmax, int64_t lmax_mask, const double *wind
             odd[l1 * n + l2] = (a - b) / 2;
         }
     free(x); free(w); free(beta); free(first); free(second); free(mask); free(tot); free(sig);
+}
+
+/* Spin-2 analysis (no refinement) restricted to a set of orders, for the bounded
+ * CPU-baseline sample: eb_out[im][2][l] complex (E then B rows). */
+void orc_ana2_orders(int64_t nside, int64_t lmax, const double *theta, const double *phi0,
+                     const double *qu, int64_t nm, const int64_t *ms, double *eb_out)
+{
+    int64_t nring = 4 * nside - 1, L = lmax + 1, npix = 12 * nside * nside;
+    double w = 4.0 * M_PI / (double)npix;
+    double *mapc = malloc(sizeof(double) * 2 * npix);
+    for (int64_t p = 0; p < npix; ++p) { mapc[2 * p] = qu[p]; mapc[2 * p + 1] = qu[npix + p]; }
+    int64_t width = 2 * L - 1;
+    double *F = malloc(sizeof(double) * 2 * nring * width);
+    orc_ring_analysis(nside, L, L - 1, phi0, mapc, F);
+#pragma omp parallel for schedule(dynamic)
+    for (int64_t im = 0; im < nm; ++im) {
+        int64_t m = ms[im];
+        double *lp = malloc(sizeof(double) * L), *lmn = malloc(sizeof(double) * L);
+        double *ap = calloc(2 * L, sizeof(double)), *am = calloc(2 * L, sizeof(double));
+        for (int64_t r = 0; r < nring; ++r) {
+            orc_lambda_row(lmax, m, -2, theta[r], lp);
+            orc_lambda_row(lmax, m, 2, theta[r], lmn);
+            double pr = w * F[2 * (r * width + (L - 1) + m)], pi = w * F[2 * (r * width + (L - 1) + m) + 1];
+            double mr = w * F[2 * (r * width + (L - 1) - m)], mi = -w * F[2 * (r * width + (L - 1) - m) + 1];
+            for (int64_t l = m; l <= lmax; ++l) {
+                ap[2 * l] += lp[l] * pr; ap[2 * l + 1] += lp[l] * pi;
+                am[2 * l] += lmn[l] * mr; am[2 * l + 1] += lmn[l] * mi;
+            }
+        }
+        double *e = eb_out + 4 * im * L, *b = e + 2 * L;
+        for (int64_t l = 0; l <= lmax; ++l) {
+            e[2 * l] = -(ap[2 * l] + am[2 * l]) / 2;
+            e[2 * l + 1] = -(ap[2 * l + 1] + am[2 * l + 1]) / 2;
+            b[2 * l] = -(ap[2 * l + 1] - am[2 * l + 1]) / 2;
+            b[2 * l + 1] = (ap[2 * l] - am[2 * l]) / 2;
+        }
+        free(lp); free(lmn); free(ap); free(am);
+    }
+    free(mapc); free(F);
 }
