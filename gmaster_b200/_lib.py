@@ -44,6 +44,7 @@ SIGNATURES = {
     "gm_bin_cells_csr": ([_c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
     "gm_lu_factor": ([_c_i64, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
     "gm_lu_solve": ([_c_i64, _c_vp, _c_vp, _c_i64, _c_vp, _c_vp], _c_int),
+    "gm_tc_selftest": ([_c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
 }
 
 STATUS = {0: "GM_OK", 1: "GM_ERR_BAD_SHAPE", 2: "GM_ERR_BAD_PTR", 3: "GM_ERR_LAUNCH",

@@ -1,0 +1,40 @@
+"""Host helpers for the tensor-core (tcgen05) operand images."""
+
+import numpy as np
+import torch
+
+from . import _lib
+
+
+def sw128_offsets(R, K):
+    """Byte offsets of element (r, k) in a K-major 128-byte-swizzled image of R rows."""
+    r = np.arange(R)[:, None]
+    k = np.arange(K)[None, :]
+    kk = k % 64
+    chunk = (kk // 8) ^ (r % 8)
+    return (k // 64) * R * 128 + (r // 8) * 1024 + (r % 8) * 128 + chunk * 16 + (kk % 8) * 2
+
+
+def sw128_image(mat16):
+    """uint16 (R, K) matrix -> uint8 image of R*K*2 bytes in the swizzled layout."""
+    R, K = mat16.shape
+    img = np.zeros(R * K, dtype=np.uint16)
+    img[sw128_offsets(R, K) // 2] = mat16
+    return img.view(np.uint8)
+
+
+def selftest(N=128, K=128, seed=0, device="cuda"):
+    """Run the one-CTA tcgen05 GEMM check; returns (max abs error, scale, err flag)."""
+    g = torch.Generator().manual_seed(seed)
+    a = torch.randn(128, K, generator=g).to(torch.bfloat16)
+    b = torch.randn(N, K, generator=g).to(torch.bfloat16)
+    want = a.float() @ b.float().T
+    ai = torch.from_numpy(sw128_image(a.view(torch.int16).numpy().view(np.uint16))).to(device)
+    bi = torch.from_numpy(sw128_image(b.view(torch.int16).numpy().view(np.uint16))).to(device)
+    d = torch.full((128, N), float("nan"), dtype=torch.float32, device=device)
+    err = torch.zeros(1, dtype=torch.int32, device=device)
+    _lib.call("gm_tc_selftest", N, K, _lib.ptr(ai), _lib.ptr(bi), _lib.ptr(d), _lib.ptr(err),
+              _lib.stream_handle(torch.device(device)))
+    torch.cuda.synchronize()
+    got = d.cpu()
+    return float((got - want).abs().max()), float(want.abs().max()), int(err.item())

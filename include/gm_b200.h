@@ -164,6 +164,18 @@ int gm_lu_factor(int64_t n, double *a, int32_t *piv, int32_t *status, void *stre
 int gm_lu_solve(int64_t n, const double *lu, const int32_t *piv, int64_t nrhs,
                 double *b, void *stream);
 
+/* ---------------------------------------------------------- tensor-core check */
+
+/* One-CTA tcgen05 check: D[128 x N] (float32, row-major) = A[128 x K] * B[N x K]^T where
+ * A and B are bf16 operand images in the K-major 128-byte-swizzled layout the tensor-core
+ * kernels use (K in atoms of 64; element (r, k) of an R-row image at byte
+ * (k/64) R 128 + (r/8) 1024 + (r%8) 128 + (((k%64)/8) ^ (r%8)) 16 + (k%8) 2).
+ * N in [16, 256] step 16, K a multiple of 64.  err (one int32) is set non-zero if a
+ * bounded wait timed out.  No counterpart in the reference: a health check of the
+ * tensor-core machinery used by gm_legendre_*_tc. */
+int gm_tc_selftest(int64_t N, int64_t K, const void *aimg, const void *bimg, float *D,
+                   int32_t *err, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
