@@ -44,7 +44,23 @@ SIGNATURES = {
     "gm_bin_cells_csr": ([_c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
     "gm_lu_factor": ([_c_i64, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
     "gm_lu_solve": ([_c_i64, _c_vp, _c_vp, _c_i64, _c_vp, _c_vp], _c_int),
-    "gm_tc_selftest": ([_c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
+    "gm_tc_lane_groups": ([_c_i64], _c_i64),
+    "gm_tc_ana_image_bytes": ([_c_i64, _c_i64], _c_i64),
+    "gm_tc_ana_scratch_bytes": ([_c_i64, _c_i64], _c_i64),
+    "gm_tc_syn_chunk_offsets": ([_c_i64, _c_int, _c_vp], _c_int),
+    "gm_tc_syn_image_bytes": ([_c_i64], _c_i64),
+    "gm_tc_coef_table": ([_c_i64, _c_int, _c_vp, _c_vp], _c_int),
+    "gm_tc_pack": ([_c_i64, _c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
+    "gm_tc_analysis": ([_c_i64, _c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
+                        _c_dbl, _c_vp, _c_i64, _c_vp, _c_vp], _c_int),
+    "gm_tc_prep_syn": ([_c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_i64, _c_vp], _c_int),
+    "gm_tc_synthesis": ([_c_i64, _c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
+                         _c_vp, _c_vp, _c_vp], _c_int),
+    "gm_tc_fold": ([_c_i64, _c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
+                   _c_int),
+    "gm_tc_synd_to_syn": ([_c_i64, _c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
+    "gm_tc_alm_layout": ([_c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_int, _c_vp], _c_int),
+    "gm_tc_selftest": ([_c_i64, _c_i64, _c_int, _c_int, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
 }
 
 STATUS = {0: "GM_OK", 1: "GM_ERR_BAD_SHAPE", 2: "GM_ERR_BAD_PTR", 3: "GM_ERR_LAUNCH",
@@ -57,7 +73,9 @@ _lib = None
 
 # Kernel launches made by each entry point (for launch accounting); default 1.
 LAUNCHES = {"gm_last_error": 0, "gm_version": 0, "gm_ring_twiddle_count": 0,
-            "gm_seed_table_len": 0, "gm_bin_coupling_csr": 3}
+            "gm_seed_table_len": 0, "gm_bin_coupling_csr": 3, "gm_tc_lane_groups": 0,
+            "gm_tc_ana_image_bytes": 0, "gm_tc_ana_scratch_bytes": 0,
+            "gm_tc_syn_chunk_offsets": 0, "gm_tc_syn_image_bytes": 0}
 CALLS = {}
 
 

@@ -1,0 +1,1016 @@
+// Batched Legendre / Wigner-d contraction on the 5th-generation tensor cores (sm_100a).
+//
+// The rows lambda^{s'}_lm(theta) = sqrt((2l+1)/4pi) d^l_{m,s'}(theta) are generated on the
+// fly by the FP64 three-term recurrence in l (one lane = one northern ring per thread),
+// rounded to FP32 and split into bf16 hi + lo, and written straight into the shared-memory
+// operand of tcgen05.mma.  The other operand is a batch of right-hand sides (up to 128
+// real rows: maps x re/im x hemisphere), delivered by the bulk-copy (TMA) engine as a
+// pre-split, pre-swizzled image.  Each product runs as three bf16 MMAs
+// (hi*hi + hi*lo + lo*hi) accumulating in FP32 in tensor memory; the epilogue applies the
+// hemisphere parity and accumulates in FP64.
+//
+// Analysis (map -> alm): D[row, l] = sum_lanes rhs[row, lane] lambda_l(lane).  One
+// persistent CTA per order m at a time walks l in superblocks of 512 (D in 512 TMEM
+// columns) and, inside a superblock, the lanes in groups of 128 (K); the recurrence state
+// of every lane is carried across superblocks in a caller-provided scratch buffer.
+//
+// Synthesis (alm -> ring coefficients): D[row, lane] = sum_l almT[row, l] lambda_l(lane).
+// One CTA per (order m, tile of 256 lanes) walks l in chunks of 64 (K).
+//
+// Replaces gmaster/_native/cuda/march_v2.cu:155-407 (FP32 SIMT march) for batched maps.
+#include <math.h>
+
+#include "gm_common.cuh"
+#include "tc_common.cuh"
+
+namespace gm {
+namespace ltc {
+
+constexpr int kGen = 128;              // generator threads (4 warps)
+constexpr int kThreads = kGen + 32;    // + one warp for the producer / MMA issuer
+constexpr int kSB = 512;               // analysis superblock (TMEM columns)
+constexpr int kNB = 64;                // analysis l-tile (MMA N)
+constexpr int kKC = 128;               // analysis lanes per group (MMA K per group)
+constexpr int kLT = 256;               // synthesis lanes per CTA (MMA N)
+constexpr int kKL = 64;                // synthesis l-chunk (MMA K per chunk)
+constexpr uint32_t kAImg = 128u * kKC * 2u;        // one plane of an analysis A image (32 KB)
+constexpr uint32_t kBTileA = kNB * kKC * 2u;       // one plane of an analysis B tile (16 KB)
+constexpr uint32_t kSImg = 128u * kKL * 2u;        // one plane of a synthesis A image (16 KB)
+constexpr uint32_t kBTileS = kLT * kKL * 2u;       // one plane of a synthesis B tile (32 KB)
+constexpr double kBig = 2.037035976334486e90;      // 2^300
+constexpr double kShrink = 2.409919865102884e-181; // 2^-600
+
+struct Coef {
+    double alpha, beta, c0;
+};
+
+__device__ __forceinline__ int64_t alm_idx(int64_t lmax, int64_t l, int64_t m)
+{
+    return m * (2 * lmax + 1 - m) / 2 + l;
+}
+
+__device__ __forceinline__ void seed_lane(const double *__restrict__ sd, double lsin, double lcos,
+                                          double &v, int &k)
+{
+    double f = sd[0];
+    if (sd[2] != 0.0) f += sd[2] * lcos;
+    if (sd[3] != 0.0) f += sd[3] * lsin;
+    if (!(f > -1.0e300)) {
+        v = 0.0;
+        k = 0;
+        return;
+    }
+    int kk = 0;
+    if (f < -300.0) kk = (int)floor((f + 300.0) / 600.0);
+    v = sd[1] * exp2(f - 600.0 * (double)kk);
+    k = kk;
+}
+
+// One recurrence step to degree l (> l0) using coefficients for (l, m); sgn_c selects
+// x - c0 (s' = +2), x + c0 (s' = -2) or x (s' = 0, c0 = 0).
+__device__ __forceinline__ void step(double x, const Coef &c, double sgn_c, double &v, double &vp,
+                                     int &k)
+{
+    const double nv = c.alpha * ((x - sgn_c * c.c0) * v) - c.beta * vp;
+    vp = v;
+    v = nv;
+    if (k < 0 && fabs(v) > kBig) {
+        v *= kShrink;
+        vp *= kShrink;
+        ++k;
+    }
+}
+
+__device__ __forceinline__ Coef load_coef(const double *__restrict__ tab, int64_t idx)
+{
+    Coef c;
+    c.alpha = __ldg(tab + 3 * idx);
+    c.beta = __ldg(tab + 3 * idx + 1);
+    c.c0 = __ldg(tab + 3 * idx + 2);
+    return c;
+}
+
+__device__ __forceinline__ void pack8(const float (&v)[8], uint4 &hi, uint4 &lo)
+{
+    tc::split_bf16x2(v[0], v[1], hi.x, lo.x);
+    tc::split_bf16x2(v[2], v[3], hi.y, lo.y);
+    tc::split_bf16x2(v[4], v[5], hi.z, lo.z);
+    tc::split_bf16x2(v[6], v[7], hi.w, lo.w);
+}
+
+__device__ __forceinline__ void sts128(uint32_t addr, const uint4 &v)
+{
+    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(v.x), "r"(v.y), "r"(v.z),
+                 "r"(v.w)
+                 : "memory");
+}
+
+struct Params {
+    int64_t nside, lmax, nlanes;
+    int sp;          // s' of the rows: 0, -2 or +2
+    int H;           // rows per half (maps x re/im); valid rows 2H <= 128
+    int NR;          // rows of the interleaved alm (spin 0: H, spin 2: 2H)
+    int o0, o1;      // output row base of the first / second half (analysis)
+    double scale;    // analysis: alm += scale * result
+    const double *geom;   // (3, nlanes)
+    const double *seeds;  // (3, L, 4)
+    const double *coef;   // (nelem, 3) for this spin
+    int var;              // seed variant 0 / 1 / 2
+};
+
+__device__ __forceinline__ double sgn_of(int sp) { return sp > 0 ? 1.0 : (sp < 0 ? -1.0 : 0.0); }
+
+// ------------------------------------------------------------------------------- analysis
+
+struct __align__(8) AnaShared {
+    uint64_t a_full[2], a_free[2], b_full[2], b_free[2], d_full, d_free;
+    uint32_t tmem;
+    int abort;
+};
+
+__device__ __forceinline__ bool wait_or_abort(uint64_t *bar, uint32_t parity, volatile int *abort,
+                                              int *err)
+{
+    if (*abort) return false;
+    if (tc::mbar_wait(bar, parity)) return true;
+    *abort = 1;
+    atomicExch(err, 1);
+    return false;
+}
+
+// The m handled in slot i of CTA c (snake order over gridDim.x CTAs).
+__device__ __forceinline__ int64_t snake_m(int64_t i, int64_t c, int64_t G)
+{
+    const int64_t round = i, pos = (round & 1) ? (G - 1 - c) : c;
+    return round * G + pos;
+}
+
+__global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t *__restrict__ aimg,
+                                                        double *__restrict__ alm_i,
+                                                        double *__restrict__ scratch,
+                                                        int *__restrict__ err)
+{
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ AnaShared sh;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t base = (tc::smem_u32(smem_raw) + 1023u) & ~1023u;
+    uint8_t *smem = smem_raw + (base - tc::smem_u32(smem_raw));
+    uint8_t *sA = smem;                      // 2 x 64 KB
+    uint8_t *sB = smem + 4 * kAImg;          // 2 x 32 KB
+    const int64_t L = p.lmax + 1, NG = (p.nlanes + kKC - 1) / kKC;
+    const int64_t G = gridDim.x, c = blockIdx.x;
+    const int l0min = abs(p.sp);
+
+    if (tid == 0) {
+        for (int i = 0; i < 2; ++i) {
+            tc::mbar_init(&sh.a_full[i], 1);
+            tc::mbar_init(&sh.a_free[i], 1);
+            tc::mbar_init(&sh.b_full[i], 4);
+            tc::mbar_init(&sh.b_free[i], 1);
+        }
+        tc::mbar_init(&sh.d_full, 1);
+        tc::mbar_init(&sh.d_free, 4);
+        sh.abort = 0;
+        tc::fence_mbar_init();
+    }
+    if (warp == 4) {
+        tc::tmem_alloc(&sh.tmem, kSB);
+        tc::tmem_relinquish();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = sh.tmem;
+    volatile int *abort = &sh.abort;
+
+    if (warp == 4) {
+        // ------------------------------------------------ producer + MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_f16(128, kNB, 1, 1, 1);
+            uint32_t j = 0, u = 0, q = 0;   // job, B-tile and superblock counters
+            // job list: (slot i -> m, superblock s, group g)
+            auto job_m = [&](int64_t i) { return snake_m(i, c, G); };
+            // prefetch the first job
+            int64_t i = 0, s = 0, g = 0;
+            bool have = job_m(i) <= p.lmax;
+            if (have) {
+                tc::mbar_arrive_expect_tx(&sh.a_full[0], 2 * kAImg);
+                tc::bulk_g2s(sA, aimg + ((job_m(i) * NG + g) * 2) * (int64_t)kAImg, 2 * kAImg, &sh.a_full[0]);
+            }
+            while (have && !*abort) {
+                const int64_t m = job_m(i);
+                const int64_t l0 = m > l0min ? m : l0min;
+                const int64_t nsb = (L - l0 + kSB - 1) / kSB;
+                // next job
+                int64_t ni = i, ns = s, ng = g + 1;
+                if (ng == NG) { ng = 0; ++ns; }
+                if (ns == nsb) { ns = 0; ++ni; }
+                const bool next = job_m(ni) <= p.lmax;
+                if (next) {
+                    const uint32_t nb = (j + 1) & 1;
+                    if (!wait_or_abort(&sh.a_free[nb], (((j + 1) >> 1) & 1) ^ 1, abort, err)) break;
+                    tc::mbar_arrive_expect_tx(&sh.a_full[nb], 2 * kAImg);
+                    tc::bulk_g2s(sA + nb * 2 * kAImg, aimg + ((job_m(ni) * NG + ng) * 2) * (int64_t)kAImg,
+                                 2 * kAImg, &sh.a_full[nb]);
+                }
+                const uint32_t buf = j & 1;
+                if (!wait_or_abort(&sh.a_full[buf], (j >> 1) & 1, abort, err)) break;
+                if (g == 0 && !wait_or_abort(&sh.d_free, (q & 1) ^ 1, abort, err)) break;
+                tc::tc_fence_after();
+                const uint32_t a0 = tc::smem_u32(sA + buf * 2 * kAImg);
+                for (int t = 0; t < kSB / kNB; ++t, ++u) {
+                    const uint32_t st = u & 1;
+                    if (!wait_or_abort(&sh.b_full[st], (u >> 1) & 1, abort, err)) break;
+                    tc::tc_fence_after();
+                    const uint32_t b0 = tc::smem_u32(sB + st * 2 * kBTileA);
+                    const uint32_t d = tmem + t * kNB;
+#pragma unroll
+                    for (int ks = 0; ks < kKC / 16; ++ks) {
+                        const uint64_t ah = tc::desc_sw128_mn(a0 + ks * 4096, 1024, 2048);
+                        const uint64_t al = tc::desc_sw128_mn(a0 + kAImg + ks * 4096, 1024, 2048);
+                        const uint64_t bh = tc::desc_sw128_mn(b0 + ks * 2048, 1024, 1024);
+                        const uint64_t bl = tc::desc_sw128_mn(b0 + kBTileA + ks * 2048, 1024, 1024);
+                        tc::mma_f16(d, ah, bh, idesc, (g > 0 || ks > 0) ? 1u : 0u);
+                        tc::mma_f16(d, ah, bl, idesc, 1u);
+                        tc::mma_f16(d, al, bh, idesc, 1u);
+                    }
+                    tc::mma_commit(&sh.b_free[st]);
+                }
+                if (*abort) break;
+                tc::mma_commit(&sh.a_free[buf]);
+                if (g == NG - 1) {
+                    tc::mma_commit(&sh.d_full);
+                    ++q;
+                }
+                ++j;
+                i = ni;
+                s = ns;
+                g = ng;
+                have = next;
+            }
+        }
+    } else {
+        // ------------------------------------------------ generators + epilogue
+        const double sgn_c = sgn_of(p.sp);
+        uint32_t u = 0, q = 0;
+        double *my_scratch = scratch + (int64_t)c * p.nlanes * 3;
+        for (int64_t i = 0;; ++i) {
+            const int64_t m = snake_m(i, c, G);
+            if (m > p.lmax || *abort) break;
+            const int64_t l0 = m > l0min ? m : l0min;
+            const int64_t nsb = (L - l0 + kSB - 1) / kSB;
+            const int64_t mb = alm_idx(p.lmax, 0, m);   // coefficient / alm base of order m
+            for (int64_t s = 0; s < nsb && !*abort; ++s) {
+                const int64_t lb = l0 + s * kSB;
+                for (int64_t g = 0; g < NG && !*abort; ++g) {
+                    const int64_t jl = g * kKC + tid;
+                    const bool valid = jl < p.nlanes;
+                    double x = 0.0, v = 0.0, vp = 0.0;
+                    int k = 0;
+                    if (valid) {
+                        x = p.geom[jl];
+                        if (s == 0) {
+                            seed_lane(p.seeds + ((int64_t)p.var * L + m) * 4, p.geom[p.nlanes + jl],
+                                      p.geom[2 * p.nlanes + jl], v, k);
+                        } else {
+                            v = my_scratch[jl * 3];
+                            vp = my_scratch[jl * 3 + 1];
+                            k = (int)my_scratch[jl * 3 + 2];
+                        }
+                    }
+                    for (int t = 0; t < kSB / kNB; ++t, ++u) {
+                        const uint32_t st = u & 1;
+                        if (!wait_or_abort(&sh.b_free[st], ((u >> 1) & 1) ^ 1, abort, err)) break;
+                        const uint32_t b0 = tc::smem_u32(sB + st * 2 * kBTileA);
+                        const uint32_t rowbase = b0 + (tid >> 3) * 1024 + (tid & 7) * 128;
+#pragma unroll 1
+                        for (int cc = 0; cc < kNB / 8; ++cc) {
+                            float vals[8];
+#pragma unroll
+                            for (int e = 0; e < 8; ++e) {
+                                const int64_t l = lb + t * kNB + cc * 8 + e;
+                                if (l > l0 && l < L) step(x, load_coef(p.coef, mb + l), sgn_c, v, vp, k);
+                                vals[e] = (valid && l < L && k == 0) ? (float)v : 0.0f;
+                            }
+                            uint4 hi, lo;
+                            pack8(vals, hi, lo);
+                            const uint32_t off = ((cc ^ (tid & 7)) << 4);
+                            sts128(rowbase + off, hi);
+                            sts128(rowbase + kBTileA + off, lo);
+                        }
+                        tc::fence_async_smem();
+                        __syncwarp();
+                        if (lane == 0) tc::mbar_arrive(&sh.b_full[st]);
+                    }
+                    if (valid && s + 1 < nsb) {
+                        my_scratch[jl * 3] = v;
+                        my_scratch[jl * 3 + 1] = vp;
+                        my_scratch[jl * 3 + 2] = (double)k;
+                    }
+                }
+                // epilogue of superblock s
+                if (!wait_or_abort(&sh.d_full, q & 1, abort, err)) break;
+                tc::tc_fence_after();
+                const int row = warp * 32 + lane;
+                const bool rvalid = row < 2 * p.H;
+                const int orow = row < p.H ? p.o0 + row : p.o1 + (row - p.H);
+                const bool parity_row = row >= p.H;
+                for (int cb = 0; cb < kSB; cb += 16) {
+                    uint32_t r[16];
+                    tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, r);
+                    tc::tmem_ld_wait();
+                    if (rvalid) {
+#pragma unroll
+                        for (int e = 0; e < 16; ++e) {
+                            const int64_t l = lb + cb + e;
+                            if (l < L) {
+                                double val = (double)__uint_as_float(r[e]) * p.scale;
+                                if (parity_row && ((l + m) & 1)) val = -val;
+                                atomicAdd(alm_i + (mb + l) * p.NR + orow, val);
+                            }
+                        }
+                    }
+                }
+                tc::tc_fence_before();
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(&sh.d_free);
+                ++q;
+            }
+        }
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 4) tc::tmem_dealloc(tmem, kSB);
+}
+
+// ------------------------------------------------------------------------------- synthesis
+
+struct __align__(8) SynShared {
+    uint64_t a_full[2], a_free[2], b_full[2], b_free[2], d_full;
+    uint32_t tmem;
+    int abort;
+};
+
+// almT images: chunk cc of order m covers l in [64 (c0(m) + cc), +64), c0(m) = floor(l0(m)/64);
+// image index = choff[m] + cc.
+__global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t *__restrict__ simg,
+                                                        const int64_t *__restrict__ choff,
+                                                        float *__restrict__ synd, int R2,
+                                                        int *__restrict__ err)
+{
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ SynShared sh;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t base = (tc::smem_u32(smem_raw) + 1023u) & ~1023u;
+    uint8_t *smem = smem_raw + (base - tc::smem_u32(smem_raw));
+    uint8_t *sA = smem;                    // 2 x 32 KB
+    uint8_t *sB = smem + 4 * kSImg;        // 2 x 64 KB
+    const int64_t L = p.lmax + 1;
+    const int64_t m = blockIdx.y, tile = blockIdx.x;
+    const int l0min = abs(p.sp);
+    const int64_t l0 = m > l0min ? m : l0min;
+    if (l0 > p.lmax) return;
+    const int64_t c0 = l0 / kKL, nch = (L + kKL - 1) / kKL - c0;
+
+    if (tid == 0) {
+        for (int i = 0; i < 2; ++i) {
+            tc::mbar_init(&sh.a_full[i], 1);
+            tc::mbar_init(&sh.a_free[i], 1);
+            tc::mbar_init(&sh.b_full[i], 4);
+            tc::mbar_init(&sh.b_free[i], 1);
+        }
+        tc::mbar_init(&sh.d_full, 1);
+        sh.abort = 0;
+        tc::fence_mbar_init();
+    }
+    if (warp == 4) {
+        tc::tmem_alloc(&sh.tmem, kLT);
+        tc::tmem_relinquish();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = sh.tmem;
+    volatile int *abort = &sh.abort;
+    const uint8_t *img = simg + choff[m] * 2 * (int64_t)kSImg;
+
+    if (warp == 4) {
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_f16(128, kLT, 1, 1, 0);
+            tc::mbar_arrive_expect_tx(&sh.a_full[0], 2 * kSImg);
+            tc::bulk_g2s(sA, img, 2 * kSImg, &sh.a_full[0]);
+            for (int64_t cc = 0; cc < nch && !*abort; ++cc) {
+                if (cc + 1 < nch) {
+                    const uint32_t nb = (uint32_t)(cc + 1) & 1;
+                    if (!wait_or_abort(&sh.a_free[nb], ((uint32_t)((cc + 1) >> 1) & 1) ^ 1, abort, err)) break;
+                    tc::mbar_arrive_expect_tx(&sh.a_full[nb], 2 * kSImg);
+                    tc::bulk_g2s(sA + nb * 2 * kSImg, img + (cc + 1) * 2 * (int64_t)kSImg, 2 * kSImg,
+                                 &sh.a_full[nb]);
+                }
+                const uint32_t st = (uint32_t)cc & 1, ph = (uint32_t)(cc >> 1) & 1;
+                if (!wait_or_abort(&sh.a_full[st], ph, abort, err)) break;
+                if (!wait_or_abort(&sh.b_full[st], ph, abort, err)) break;
+                tc::tc_fence_after();
+                const uint32_t a0 = tc::smem_u32(sA + st * 2 * kSImg);
+                const uint32_t b0 = tc::smem_u32(sB + st * 2 * kBTileS);
+#pragma unroll
+                for (int ks = 0; ks < kKL / 16; ++ks) {
+                    const uint64_t ah = tc::desc_sw128_mn(a0 + ks * 4096, 1024, 2048);
+                    const uint64_t al = tc::desc_sw128_mn(a0 + kSImg + ks * 4096, 1024, 2048);
+                    const uint64_t bh = tc::desc_sw128(b0 + ks * 32);
+                    const uint64_t bl = tc::desc_sw128(b0 + kBTileS + ks * 32);
+                    tc::mma_f16(tmem, ah, bh, idesc, (cc > 0 || ks > 0) ? 1u : 0u);
+                    tc::mma_f16(tmem, ah, bl, idesc, 1u);
+                    tc::mma_f16(tmem, al, bh, idesc, 1u);
+                }
+                tc::mma_commit(&sh.b_free[st]);
+                tc::mma_commit(&sh.a_free[st]);
+            }
+            if (!*abort) tc::mma_commit(&sh.d_full);
+        }
+    } else {
+        const double sgn_c = sgn_of(p.sp);
+        const int64_t mb = alm_idx(p.lmax, 0, m);
+        double x[2], v[2], vp[2];
+        int k[2];
+        bool valid[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int64_t jl = tile * kLT + h * kGen + tid;
+            valid[h] = jl < p.nlanes;
+            x[h] = valid[h] ? p.geom[jl] : 0.0;
+            v[h] = vp[h] = 0.0;
+            k[h] = 0;
+            if (valid[h])
+                seed_lane(p.seeds + ((int64_t)p.var * L + m) * 4, p.geom[p.nlanes + jl],
+                          p.geom[2 * p.nlanes + jl], v[h], k[h]);
+        }
+        for (int64_t cc = 0; cc < nch; ++cc) {
+            const uint32_t st = (uint32_t)cc & 1;
+            if (!wait_or_abort(&sh.b_free[st], ((uint32_t)(cc >> 1) & 1) ^ 1, abort, err)) break;
+            const uint32_t b0 = tc::smem_u32(sB + st * 2 * kBTileS);
+#pragma unroll 1
+            for (int sub = 0; sub < kKL / 8; ++sub) {
+                float vals[2][8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    const int64_t l = (c0 + cc) * kKL + sub * 8 + e;
+                    Coef cf;
+                    const bool adv = l > l0 && l < L;
+                    if (adv) cf = load_coef(p.coef, mb + l);
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        if (adv) step(x[h], cf, sgn_c, v[h], vp[h], k[h]);
+                        vals[h][e] = (valid[h] && l >= l0 && l < L && k[h] == 0) ? (float)v[h] : 0.0f;
+                    }
+                }
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    uint4 hi, lo;
+                    pack8(vals[h], hi, lo);
+                    const uint32_t row = h * kGen + tid;
+                    const uint32_t off = (row >> 3) * 1024 + (row & 7) * 128 + (((uint32_t)sub ^ (row & 7)) << 4);
+                    sts128(b0 + off, hi);
+                    sts128(b0 + kBTileS + off, lo);
+                }
+            }
+            tc::fence_async_smem();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(&sh.b_full[st]);
+        }
+        // epilogue: D[row, lane] -> synd[m][lane][row]
+        if (wait_or_abort(&sh.d_full, 0, abort, err)) {
+            tc::tc_fence_after();
+            const int row = warp * 32 + lane;
+            for (int cb = 0; cb < kLT; cb += 16) {
+                uint32_t r[16];
+                tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, r);
+                tc::tmem_ld_wait();
+                if (row < R2) {
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        const int64_t jl = tile * kLT + cb + e;
+                        if (jl < p.nlanes) synd[(m * p.nlanes + jl) * R2 + row] = __uint_as_float(r[e]);
+                    }
+                }
+            }
+        }
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 4) tc::tmem_dealloc(tmem, kLT);
+}
+
+// ------------------------------------------------------------------------------- tables
+
+// coef[(mstart[m] + l) * 3 + {0,1,2}] = (alpha, beta, c0) of target degree l for s'^2 = s2.
+__global__ void k_coef_table(int64_t lmax, int spin, double *__restrict__ tab)
+{
+    const int64_t m = blockIdx.y;
+    const int64_t L = lmax + 1;
+    const int64_t l0 = spin == 0 ? m : (m > 2 ? m : 2);
+    const double dm = (double)m, ds = (double)spin;
+    for (int64_t l = m + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < L;
+         l += (int64_t)gridDim.x * blockDim.x) {
+        double a = 0.0, b = 0.0, c0 = 0.0;
+        if (l > l0) {
+            const double dl = (double)l;
+            const double den = sqrt((dl * dl - dm * dm) * (dl * dl - ds * ds));
+            a = sqrt((2.0 * dl + 1.0) * (2.0 * dl - 1.0)) * dl / den;
+            if (l >= l0 + 2) {
+                const double dl1 = dl - 1.0;
+                const double num = sqrt((dl1 * dl1 - dm * dm) * (dl1 * dl1 - ds * ds));
+                b = sqrt((2.0 * dl + 1.0) / (2.0 * dl - 3.0)) * dl * num / (dl1 * den);
+            }
+            if (spin != 0) c0 = 2.0 * dm / ((dl - 1.0) * dl);
+        }
+        const int64_t idx = alm_idx(lmax, l, m);
+        tab[3 * idx] = a;
+        tab[3 * idx + 1] = b;
+        tab[3 * idx + 2] = c0;
+    }
+}
+
+// ------------------------------------------------------------------------------- images
+
+// Write 8 consecutive MN rows (one 16-byte chunk per plane) of an MN-major image with 128
+// rows at K index kk: element (r, kk) -> sw128_mn_offset(128, r, kk).
+__device__ __forceinline__ void put_rows8(uint8_t *img, uint32_t plane_bytes, int r0, int kk,
+                                          const float (&v)[8])
+{
+    uint4 hi, lo;
+    pack8(v, hi, lo);
+    const uint32_t off = tc::sw128_mn_offset(128, (uint32_t)r0, (uint32_t)kk);
+    *reinterpret_cast<uint4 *>(img + off) = hi;
+    *reinterpret_cast<uint4 *>(img + plane_bytes + off) = lo;
+}
+
+// Rows of the analysis right-hand side for one (m, lane) from the per-comp ring values
+// gn[c], gs[c] (complex, float): spin 0 rows [G_N | G_S]; spin 2 variant +2 rows
+// [Mt_N | Pt_S], variant -2 rows [Pt_N | Mt_S], with Pt = G_Q + i G_U, Mt = G_Q - i G_U.
+// Writes the 128-row image column (zero rows beyond 2H) for both planes.
+__device__ void write_rhs_column(uint8_t *img, int kk, int spin, int sp, int ncomp, const float2 *gn,
+                                 const float2 *gs)
+{
+    const int H = spin == 0 ? 2 * ncomp : ncomp;  // spin 2: ncomp = 2F -> H = 2F
+    float rowv[8];
+    for (int r0 = 0; r0 < 128; r0 += 8) {
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const int r = r0 + e;
+            float val = 0.0f;
+            if (r < 2 * H) {
+                const bool second = r >= H;
+                const int rr = second ? r - H : r;
+                const int item = rr >> 1, im = rr & 1;
+                if (spin == 0) {
+                    const float2 g = second ? gs[item] : gn[item];
+                    val = im ? g.y : g.x;
+                } else {
+                    // field `item`: comps 2 item (Q), 2 item + 1 (U)
+                    // sp = -2 rows [Pt_N | Mt_S]; sp = +2 rows [Mt_N | Pt_S]
+                    const bool north = !second;
+                    const bool plus = (sp < 0) ? !second : second;
+                    const float2 q = north ? gn[2 * item] : gs[2 * item];
+                    const float2 u = north ? gn[2 * item + 1] : gs[2 * item + 1];
+                    // Pt = q + i u = (q.x - u.y, q.y + u.x); Mt = q - i u = (q.x + u.y, q.y - u.x)
+                    if (plus) val = im ? (q.y + u.x) : (q.x - u.y);
+                    else val = im ? (q.y - u.x) : (q.x + u.y);
+                }
+            }
+            rowv[e] = val;
+        }
+        put_rows8(img, kAImg, r0, kk, rowv);
+    }
+}
+
+// Initial right-hand side from the ring spectra: ringspec (ncomp, nring, L) complex64 ->
+// rhs_map (L, nlanes, ncomp) of float4 (G_N re, im, G_S re, im) and the analysis images.
+__global__ void k_pack_tc(int64_t nside, int64_t L, int ncomp, int spin,
+                          const float2 *__restrict__ spec, float4 *__restrict__ rhs_map,
+                          uint8_t *__restrict__ img_a, uint8_t *__restrict__ img_b)
+{
+    const int64_t nlanes = 2 * nside, nring = 4 * nside - 1, NG = (nlanes + kKC - 1) / kKC;
+    const int64_t m = blockIdx.y;
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= NG * kKC) return;
+    float2 gn[64], gs[64];
+    for (int c = 0; c < ncomp; ++c) {
+        float2 n = make_float2(0.f, 0.f), s = make_float2(0.f, 0.f);
+        if (j < nlanes) {
+            n = spec[((int64_t)c * nring + north_ring(j)) * L + m];
+            if (j != nlanes - 1) s = spec[((int64_t)c * nring + south_ring(nside, j)) * L + m];
+            rhs_map[(m * nlanes + j) * ncomp + c] = make_float4(n.x, n.y, s.x, s.y);
+        }
+        gn[c] = n;
+        gs[c] = s;
+    }
+    const int64_t g = j / kKC;
+    const int kk = (int)(j % kKC);
+    uint8_t *ia = img_a + ((m * NG + g) * 2) * (int64_t)kAImg;
+    write_rhs_column(ia, kk, spin, spin == 0 ? 0 : -2, ncomp, gn, gs);
+    if (spin != 0) {
+        uint8_t *ib = img_b + ((m * NG + g) * 2) * (int64_t)kAImg;
+        write_rhs_column(ib, kk, spin, +2, ncomp, gn, gs);
+    }
+}
+
+// Synthesis operand images from the interleaved alm (nelem, NR) float64.
+// Rows: spin 0 [a | s a] (src row r mod H); spin 2 variant -2 (lambda+): [2a | s -2a]
+// (src row r); variant +2 (lambda-): [-2a | s 2a] (src r < H ? H + r : r - H); s = (-1)^(l+m).
+__global__ void k_prep_syn(int64_t lmax, int spin, int sp, int H, int NR,
+                           const double *__restrict__ alm_i, const int64_t *__restrict__ choff,
+                           uint8_t *__restrict__ simg)
+{
+    const int64_t m = blockIdx.y, L = lmax + 1;
+    const int l0min = abs(sp);
+    const int64_t l0 = m > l0min ? m : l0min;
+    if (l0 > lmax) return;
+    const int64_t c0 = l0 / kKL, nch = (L + kKL - 1) / kKL - c0;
+    const int64_t mb = alm_idx(lmax, 0, m);
+    // thread -> (chunk cc, l within chunk, 8-row group)
+    const int64_t per = (int64_t)kKL * 16;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nch * per;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t cc = t / per;
+        const int kl = (int)((t % per) / 16), r0 = (int)(t % 16) * 8;
+        const int64_t l = (c0 + cc) * kKL + kl;
+        float v[8];
+        const bool lok = l >= l0 && l < L;
+        const double sgn = ((l + m) & 1) ? -1.0 : 1.0;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const int r = r0 + e;
+            float val = 0.0f;
+            if (lok && r < 2 * H) {
+                const bool second = r >= H;
+                int src;
+                if (spin == 0) src = second ? r - H : r;
+                else if (sp < 0) src = r;
+                else src = second ? r - H : H + r;
+                double a = alm_i[(mb + l) * NR + src];
+                if (second) a *= sgn;
+                val = (float)a;
+            }
+            v[e] = val;
+        }
+        uint8_t *img = simg + (choff[m] + cc) * 2 * (int64_t)kSImg;
+        uint4 hi, lo;
+        pack8(v, hi, lo);
+        const uint32_t off = tc::sw128_mn_offset(128, (uint32_t)r0, (uint32_t)kl);
+        *reinterpret_cast<uint4 *>(img + off) = hi;
+        *reinterpret_cast<uint4 *>(img + kSImg + off) = lo;
+    }
+}
+
+// Ring-fold residual for the batched path, one CTA per lane: reads the synthesis outputs
+// (spin 0: synd rows [f_N | f_S]; spin 2: synd_a rows [sum l+ 2a | s sum l+ -2a],
+// synd_b rows [sum l- -2a | s sum l- 2a]), forms the ring coefficients per real comp,
+// folds them into the analysis-side ring spectrum, subtracts rhs_map and writes the next
+// analysis images.
+__global__ void __launch_bounds__(128) k_fold_tc(int64_t nside, int64_t L, int ncomp, int spin,
+                                                 const float *__restrict__ synd_a,
+                                                 const float *__restrict__ synd_b, int R2,
+                                                 const float4 *__restrict__ rhs_map,
+                                                 const uint8_t *__restrict__ shifted,
+                                                 uint8_t *__restrict__ img_a,
+                                                 uint8_t *__restrict__ img_b)
+{
+    const int64_t j = blockIdx.x;
+    const int64_t nlanes = 2 * nside, npix = 12 * nside * nside, NG = (nlanes + kKC - 1) / kKC;
+    const int n = (int)ring_nphi(nside, north_ring(j));
+    const bool sh = shifted[north_ring(j)] != 0;
+    const bool two = j != nlanes - 1;
+    const float wn = (float)(4.0 * M_PI / (double)npix * (double)n);
+    const int H = spin == 0 ? 2 * ncomp : ncomp;
+    const int64_t g = j / kKC;
+    const int kk = (int)(j % kKC);
+    for (int k = threadIdx.x; k < n && k < L; k += blockDim.x) {
+        // residue sums per comp, north / south
+        float2 pn[64], ps[64];
+        for (int c = 0; c < ncomp; ++c) {
+            pn[c] = make_float2(0.f, 0.f);
+            ps[c] = make_float2(0.f, 0.f);
+        }
+        auto coef = [&](int64_t mm, int c, float2 &cn, float2 &cs) {
+            // ring coefficients of comp c at order mm >= 0 for this lane (north, south)
+            const float *a = synd_a + (mm * nlanes + j) * R2;
+            if (spin == 0) {
+                cn = make_float2(a[2 * c], a[2 * c + 1]);
+                cs = make_float2(a[H + 2 * c], a[H + 2 * c + 1]);
+            } else {
+                const float *b = synd_b + (mm * nlanes + j) * R2;
+                const int f = c >> 1;
+                // U1 = a[f], U2 = a[H + f], V1 = b[f], V2 = b[H + f] (complex per field)
+                const float2 u1 = make_float2(a[2 * f], a[2 * f + 1]), u2 = make_float2(a[H + 2 * f], a[H + 2 * f + 1]);
+                const float2 v1 = make_float2(b[2 * f], b[2 * f + 1]), v2 = make_float2(b[H + 2 * f], b[H + 2 * f + 1]);
+                if ((c & 1) == 0) {
+                    // Q_N = (U1 + V1)/2, Q_S = (U2 + V2)/2
+                    cn = make_float2(0.5f * (u1.x + v1.x), 0.5f * (u1.y + v1.y));
+                    cs = make_float2(0.5f * (u2.x + v2.x), 0.5f * (u2.y + v2.y));
+                } else {
+                    // U_N = i (V1 - U1)/2, U_S = i (U2 - V2)/2 ; i (x + i y) = (-y, x)
+                    cn = make_float2(-0.5f * (v1.y - u1.y), 0.5f * (v1.x - u1.x));
+                    cs = make_float2(-0.5f * (u2.y - v2.y), 0.5f * (u2.x - v2.x));
+                }
+            }
+        };
+        int t = 0;
+        for (int64_t mm = k; mm < L; mm += n, ++t) {
+            const float sg = (sh && (t & 1)) ? -1.f : 1.f;
+            for (int c = 0; c < ncomp; ++c) {
+                float2 cn, cs;
+                coef(mm, c, cn, cs);
+                pn[c].x += sg * cn.x;
+                pn[c].y += sg * cn.y;
+                ps[c].x += sg * cs.x;
+                ps[c].y += sg * cs.y;
+            }
+        }
+        t = -1;
+        for (int64_t mm = (int64_t)n - k; mm < L; mm += n, --t) {
+            const float sg = (sh && (t & 1)) ? -1.f : 1.f;
+            for (int c = 0; c < ncomp; ++c) {
+                float2 cn, cs;
+                coef(mm, c, cn, cs);
+                pn[c].x += sg * cn.x;
+                pn[c].y -= sg * cn.y;
+                ps[c].x += sg * cs.x;
+                ps[c].y -= sg * cs.y;
+            }
+        }
+        t = 0;
+        for (int64_t m = k; m < L; m += n, ++t) {
+            const float sg = (sh && (t & 1)) ? -wn : wn;
+            float2 gn[64], gs[64];
+            for (int c = 0; c < ncomp; ++c) {
+                const float4 b = rhs_map[(m * nlanes + j) * ncomp + c];
+                gn[c] = make_float2(sg * pn[c].x - b.x, sg * pn[c].y - b.y);
+                gs[c] = two ? make_float2(sg * ps[c].x - b.z, sg * ps[c].y - b.w) : make_float2(-b.z, -b.w);
+            }
+            uint8_t *ia = img_a + ((m * NG + g) * 2) * (int64_t)kAImg;
+            write_rhs_column(ia, kk, spin, spin == 0 ? 0 : -2, ncomp, gn, gs);
+            if (spin != 0) {
+                uint8_t *ib = img_b + ((m * NG + g) * 2) * (int64_t)kAImg;
+                write_rhs_column(ib, kk, spin, +2, ncomp, gn, gs);
+            }
+        }
+    }
+}
+
+// Interleaved alm (nelem, NR) -> API layout (nalm, nelem) complex128 and back.
+// Spin 0: rows (map, re/im).  Spin 2: rows [2a (H) | -2a (H)] with
+// E = -(2a + -2a)/2, B = i (2a - -2a)/2 per field; to_api = 1 converts to (E, B),
+// to_api = 0 converts (E, B) to (2a, -2a) = (-(E + i B), -(E - i B)).
+__global__ void k_alm_layout(int64_t nelem, int spin, int nfield, double *__restrict__ alm_i,
+                             double *__restrict__ alm_api, int to_api)
+{
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nelem) return;
+    if (spin == 0) {
+        const int NR = 2 * nfield;
+        for (int f = 0; f < nfield; ++f) {
+            double *a = alm_api + 2 * ((int64_t)f * nelem + idx);
+            double *b = alm_i + idx * NR + 2 * f;
+            if (to_api) { a[0] = b[0]; a[1] = b[1]; }
+            else { b[0] = a[0]; b[1] = a[1]; }
+        }
+        return;
+    }
+    const int H = 2 * nfield, NR = 2 * H;
+    for (int f = 0; f < nfield; ++f) {
+        double *p2 = alm_i + idx * NR + 2 * f;       // 2a
+        double *m2 = alm_i + idx * NR + H + 2 * f;   // -2a
+        double *e = alm_api + 2 * ((int64_t)(2 * f) * nelem + idx);
+        double *b = alm_api + 2 * ((int64_t)(2 * f + 1) * nelem + idx);
+        if (to_api) {
+            e[0] = -0.5 * (p2[0] + m2[0]);
+            e[1] = -0.5 * (p2[1] + m2[1]);
+            // i (x + i y) / 2 with x + i y = 2a - -2a
+            b[0] = -0.5 * (p2[1] - m2[1]);
+            b[1] = 0.5 * (p2[0] - m2[0]);
+        } else {
+            // 2a = -(E + i B), -2a = -(E - i B)
+            p2[0] = -(e[0] - b[1]);
+            p2[1] = -(e[1] + b[0]);
+            m2[0] = -(e[0] + b[1]);
+            m2[1] = -(e[1] - b[0]);
+        }
+    }
+}
+
+// Tensor-core synthesis output -> per-comp ring coefficients in the lane layout
+// syn (L, nlanes, ncomp, 4) float [north re, im, south re, im] used by gm_ring_synthesis.
+__global__ void k_synd_to_syn(int64_t nlanes, int64_t L, int ncomp, int spin,
+                              const float *__restrict__ synd_a, const float *__restrict__ synd_b,
+                              int R2, float *__restrict__ syn)
+{
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= L * nlanes * ncomp) return;
+    const int c = (int)(idx % ncomp);
+    const int64_t ml = idx / ncomp;   // m * nlanes + lane
+    const int H = R2 / 2;
+    const float *a = synd_a + ml * R2;
+    float4 o;
+    if (spin == 0) {
+        o = make_float4(a[2 * c], a[2 * c + 1], a[H + 2 * c], a[H + 2 * c + 1]);
+    } else {
+        const float *b = synd_b + ml * R2;
+        const int f = c >> 1;
+        const float2 u1 = make_float2(a[2 * f], a[2 * f + 1]), u2 = make_float2(a[H + 2 * f], a[H + 2 * f + 1]);
+        const float2 v1 = make_float2(b[2 * f], b[2 * f + 1]), v2 = make_float2(b[H + 2 * f], b[H + 2 * f + 1]);
+        if ((c & 1) == 0)
+            o = make_float4(0.5f * (u1.x + v1.x), 0.5f * (u1.y + v1.y), 0.5f * (u2.x + v2.x), 0.5f * (u2.y + v2.y));
+        else
+            o = make_float4(-0.5f * (v1.y - u1.y), 0.5f * (v1.x - u1.x), -0.5f * (u2.y - v2.y), 0.5f * (u2.x - v2.x));
+    }
+    reinterpret_cast<float4 *>(syn)[idx] = o;
+}
+
+}  // namespace ltc
+}  // namespace gm
+
+using namespace gm;
+using namespace gm::ltc;
+
+extern "C" int64_t gm_tc_lane_groups(int64_t nside) { return (2 * nside + kKC - 1) / kKC; }
+
+extern "C" int64_t gm_tc_ana_image_bytes(int64_t nside, int64_t lmax)
+{
+    return (lmax + 1) * gm_tc_lane_groups(nside) * 2 * (int64_t)kAImg;
+}
+
+extern "C" int64_t gm_tc_ana_scratch_bytes(int64_t nside, int64_t nctas)
+{
+    return nctas * 2 * nside * 3 * (int64_t)sizeof(double);
+}
+
+// Per-order synthesis chunk offsets for spin (|s'|): choff[m], total in choff[L].
+extern "C" int gm_tc_syn_chunk_offsets(int64_t lmax, int spin, int64_t *choff_host)
+{
+    if (lmax < 0 || !choff_host) return GM_ERR_BAD_SHAPE;
+    const int64_t L = lmax + 1;
+    int64_t acc = 0;
+    for (int64_t m = 0; m < L; ++m) {
+        choff_host[m] = acc;
+        const int64_t l0 = spin == 0 ? m : (m > 2 ? m : 2);
+        if (l0 <= lmax) acc += (L + kKL - 1) / kKL - l0 / kKL;
+    }
+    choff_host[L] = acc;
+    return GM_OK;
+}
+
+extern "C" int64_t gm_tc_syn_image_bytes(int64_t nchunks) { return nchunks * 2 * (int64_t)kSImg; }
+
+extern "C" int gm_tc_coef_table(int64_t lmax, int spin, double *tab, void *stream)
+{
+    if (lmax < 0 || lmax > 65535 || (spin != 0 && spin != 2)) return GM_ERR_BAD_SHAPE;
+    if (!tab) return GM_ERR_BAD_PTR;
+    k_coef_table<<<dim3(8, (unsigned)(lmax + 1)), 256, 0, as_stream(stream)>>>(lmax, spin, tab);
+    return check_launch("gm_tc_coef_table");
+}
+
+static int tc_shape_ok(int spin, int64_t ncomp)
+{
+    if (spin == 0) return ncomp >= 1 && ncomp <= 32;
+    if (spin == 2) return ncomp >= 2 && ncomp <= 64 && ncomp % 2 == 0;
+    return 0;
+}
+
+extern "C" int gm_tc_pack(int64_t nside, int64_t lmax, int spin, int64_t ncomp, const void *ringspec,
+                          void *rhs_map, void *img_a, void *img_b, void *stream)
+{
+    if (nside < 1 || lmax < 0 || !tc_shape_ok(spin, ncomp)) return GM_ERR_BAD_SHAPE;
+    if (!ringspec || !rhs_map || !img_a || (spin && !img_b)) return GM_ERR_BAD_PTR;
+    const int64_t NG = gm_tc_lane_groups(nside);
+    cudaStream_t s = as_stream(stream);
+    cudaError_t e = cudaMemsetAsync(img_a, 0, gm_tc_ana_image_bytes(nside, lmax), s);
+    if (e == cudaSuccess && spin) e = cudaMemsetAsync(img_b, 0, gm_tc_ana_image_bytes(nside, lmax), s);
+    if (e != cudaSuccess) {
+        set_error("gm_tc_pack memset", e);
+        return GM_ERR_LAUNCH;
+    }
+    dim3 grid((unsigned)((NG * kKC + 127) / 128), (unsigned)(lmax + 1));
+    k_pack_tc<<<grid, 128, 0, s>>>(nside, lmax + 1, (int)ncomp, spin, (const float2 *)ringspec,
+                                   (float4 *)rhs_map, (uint8_t *)img_a, (uint8_t *)img_b);
+    return check_launch("gm_tc_pack");
+}
+
+static Params make_params(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                          const double *geom, const double *seeds, const double *coef, double scale)
+{
+    Params p;
+    p.nside = nside;
+    p.lmax = lmax;
+    p.nlanes = 2 * nside;
+    p.sp = sp;
+    p.H = spin == 0 ? (int)(2 * ncomp) : (int)ncomp;
+    p.NR = spin == 0 ? p.H : 2 * p.H;
+    if (spin == 0) { p.o0 = 0; p.o1 = 0; }
+    else if (sp < 0) { p.o0 = 0; p.o1 = p.H; }
+    else { p.o0 = p.H; p.o1 = 0; }
+    p.scale = scale;
+    p.geom = geom;
+    p.seeds = seeds;
+    p.coef = coef;
+    p.var = sp == 0 ? 0 : (sp < 0 ? 1 : 2);
+    return p;
+}
+
+extern "C" int gm_tc_analysis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                              const double *geom, const double *seeds, const double *coef,
+                              const void *img, double *alm_i, double scale, double *scratch,
+                              int64_t nctas, int32_t *err, void *stream)
+{
+    if (nside < 1 || lmax < 2 || !tc_shape_ok(spin, ncomp) || nctas < 1 || nctas > 4096)
+        return GM_ERR_BAD_SHAPE;
+    if ((spin == 0) != (sp == 0) || (spin == 2 && sp != 2 && sp != -2)) return GM_ERR_BAD_SHAPE;
+    if (!geom || !seeds || !coef || !img || !alm_i || !scratch || !err) return GM_ERR_BAD_PTR;
+    const size_t smem = 4 * kAImg + 4 * kBTileA + 1024;
+    cudaError_t e = cudaFuncSetAttribute(k_ana_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) {
+        set_error("gm_tc_analysis attr", e);
+        return GM_ERR_LAUNCH;
+    }
+    Params p = make_params(nside, lmax, spin, sp, ncomp, geom, seeds, coef, scale);
+    k_ana_tc<<<(unsigned)nctas, kThreads, smem, as_stream(stream)>>>(p, (const uint8_t *)img, alm_i,
+                                                                    scratch, (int *)err);
+    return check_launch("gm_tc_analysis");
+}
+
+extern "C" int gm_tc_prep_syn(int64_t lmax, int spin, int sp, int64_t ncomp, const double *alm_i,
+                              const int64_t *choff, void *simg, int64_t simg_bytes, void *stream)
+{
+    if (lmax < 2 || !tc_shape_ok(spin, ncomp)) return GM_ERR_BAD_SHAPE;
+    if (!alm_i || !choff || !simg) return GM_ERR_BAD_PTR;
+    const int H = spin == 0 ? (int)(2 * ncomp) : (int)ncomp;
+    const int NR = spin == 0 ? H : 2 * H;
+    cudaStream_t s = as_stream(stream);
+    cudaError_t e = cudaMemsetAsync(simg, 0, (size_t)simg_bytes, s);
+    if (e != cudaSuccess) {
+        set_error("gm_tc_prep_syn memset", e);
+        return GM_ERR_LAUNCH;
+    }
+    k_prep_syn<<<dim3(16, (unsigned)(lmax + 1)), 256, 0, s>>>(lmax, spin, sp, H, NR, alm_i, choff,
+                                                             (uint8_t *)simg);
+    return check_launch("gm_tc_prep_syn");
+}
+
+extern "C" int gm_tc_synthesis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                               const double *geom, const double *seeds, const double *coef,
+                               const void *simg, const int64_t *choff, float *synd, int32_t *err,
+                               void *stream)
+{
+    if (nside < 1 || lmax < 2 || !tc_shape_ok(spin, ncomp)) return GM_ERR_BAD_SHAPE;
+    if ((spin == 0) != (sp == 0) || (spin == 2 && sp != 2 && sp != -2)) return GM_ERR_BAD_SHAPE;
+    if (!geom || !seeds || !coef || !simg || !choff || !synd || !err) return GM_ERR_BAD_PTR;
+    const size_t smem = 4 * kSImg + 4 * kBTileS + 1024;
+    cudaError_t e = cudaFuncSetAttribute(k_syn_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) {
+        set_error("gm_tc_synthesis attr", e);
+        return GM_ERR_LAUNCH;
+    }
+    Params p = make_params(nside, lmax, spin, sp, ncomp, geom, seeds, coef, 1.0);
+    const int R2 = 2 * p.H;
+    dim3 grid((unsigned)((p.nlanes + kLT - 1) / kLT), (unsigned)(lmax + 1));
+    k_syn_tc<<<grid, kThreads, smem, as_stream(stream)>>>(p, (const uint8_t *)simg, choff, synd, R2,
+                                                         (int *)err);
+    return check_launch("gm_tc_synthesis");
+}
+
+extern "C" int gm_tc_fold(int64_t nside, int64_t lmax, int spin, int64_t ncomp, const float *synd_a,
+                          const float *synd_b, const void *rhs_map, const uint8_t *shifted,
+                          void *img_a, void *img_b, void *stream)
+{
+    if (nside < 1 || lmax < 2 || !tc_shape_ok(spin, ncomp)) return GM_ERR_BAD_SHAPE;
+    if (!synd_a || (spin && !synd_b) || !rhs_map || !shifted || !img_a || (spin && !img_b))
+        return GM_ERR_BAD_PTR;
+    const int H = spin == 0 ? (int)(2 * ncomp) : (int)ncomp;
+    k_fold_tc<<<(unsigned)(2 * nside), 128, 0, as_stream(stream)>>>(
+        nside, lmax + 1, (int)ncomp, spin, synd_a, synd_b, 2 * H, (const float4 *)rhs_map, shifted,
+        (uint8_t *)img_a, (uint8_t *)img_b);
+    return check_launch("gm_tc_fold");
+}
+
+extern "C" int gm_tc_alm_layout(int64_t lmax, int spin, int64_t nfield, double *alm_i,
+                                double *alm_api, int to_api, void *stream)
+{
+    if (lmax < 0 || nfield < 1 || nfield > 64 || (spin != 0 && spin != 2)) return GM_ERR_BAD_SHAPE;
+    if (!alm_i || !alm_api) return GM_ERR_BAD_PTR;
+    const int64_t nelem = (lmax + 1) * (lmax + 2) / 2;
+    k_alm_layout<<<(unsigned)((nelem + 255) / 256), 256, 0, as_stream(stream)>>>(
+        nelem, spin, (int)nfield, alm_i, alm_api, to_api);
+    return check_launch("gm_tc_alm_layout");
+}
+
+extern "C" int gm_tc_synd_to_syn(int64_t nside, int64_t lmax, int spin, int64_t ncomp,
+                                 const float *synd_a, const float *synd_b, float *syn, void *stream)
+{
+    if (nside < 1 || lmax < 2 || !tc_shape_ok(spin, ncomp)) return GM_ERR_BAD_SHAPE;
+    if (!synd_a || (spin && !synd_b) || !syn) return GM_ERR_BAD_PTR;
+    const int H = spin == 0 ? (int)(2 * ncomp) : (int)ncomp;
+    const int64_t tot = (lmax + 1) * 2 * nside * ncomp;
+    k_synd_to_syn<<<(unsigned)((tot + 255) / 256), 256, 0, as_stream(stream)>>>(
+        2 * nside, lmax + 1, (int)ncomp, spin, synd_a, synd_b, 2 * H, syn);
+    return check_launch("gm_tc_synd_to_syn");
+}

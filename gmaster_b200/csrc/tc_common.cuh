@@ -8,8 +8,15 @@
 namespace gm {
 namespace tc {
 
-// Spin limit for mbarrier waits (each try_wait itself suspends for a while).
-constexpr uint32_t kWaitLimit = 1u << 24;
+// Time limit of an mbarrier wait in nanoseconds (of the global timer).
+constexpr uint64_t kWaitNs = 2000000000ull;
+
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
@@ -40,11 +47,13 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t by
                  : "memory");
 }
 
-// Wait for the phase with parity `parity` to complete.  Returns false on timeout.
+// Wait for the phase with parity `parity` to complete.  Returns false once kWaitNs of
+// global time have passed without completion.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
 {
     const uint32_t addr = smem_u32(bar);
-    for (uint32_t it = 0; it < kWaitLimit; ++it) {
+    uint64_t start = 0;
+    for (uint32_t it = 0;; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -54,8 +63,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
             : "r"(addr), "r"(parity)
             : "memory");
         if (done) return true;
+        if ((it & 255) == 0) {
+            const uint64_t now = global_ns();
+            if (it == 0) start = now;
+            else if (now - start > kWaitNs) return false;
+        }
     }
-    return false;
 }
 
 // Bulk (non-tensor) copy global -> shared, completing `bytes` on the mbarrier.
@@ -145,11 +158,33 @@ __device__ __forceinline__ uint64_t desc_sw128(uint32_t smem_addr)
     return d;
 }
 
-// Instruction descriptor: kind::f16, A/B bf16 (fmt 1) or f16 (fmt 0), D f32, K-major, M x N.
-__host__ __device__ constexpr uint32_t idesc_f16(int M, int N, int fmt)
+// Shared-memory matrix descriptor, MN-major, 128-byte swizzle: atoms of 64 MN-elements x
+// 8 K-rows (1024 bytes); `lbo` = byte stride between 64-element MN blocks, `sbo` = byte
+// stride between groups of 8 K-rows.
+__device__ __forceinline__ uint64_t desc_sw128_mn(uint32_t smem_addr, uint32_t lbo, uint32_t sbo)
 {
-    return (1u << 4) | ((uint32_t)fmt << 7) | ((uint32_t)fmt << 10) | ((uint32_t)(N >> 3) << 17) |
-           ((uint32_t)(M >> 4) << 24);
+    uint64_t d = 0;
+    d |= (uint64_t)((smem_addr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;
+    return d;
+}
+
+// Byte offset of element (r, k) in an MN-major SW128 image with R MN-rows (R % 64 == 0):
+// K in groups of 8 (stride (R/64) 1024 bytes), MN in blocks of 64 (stride 1024 bytes).
+__host__ __device__ __forceinline__ uint32_t sw128_mn_offset(uint32_t R, uint32_t r, uint32_t k)
+{
+    const uint32_t chunk = ((r & 63) >> 3) ^ (k & 7);
+    return (k >> 3) * (R >> 6) * 1024u + (r >> 6) * 1024u + (k & 7) * 128u + chunk * 16u + (r & 7) * 2u;
+}
+
+// Instruction descriptor: kind::f16, A/B bf16 (fmt 1) or f16 (fmt 0), D f32, K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_f16(int M, int N, int fmt, int a_mn = 0, int b_mn = 0)
+{
+    return (1u << 4) | ((uint32_t)fmt << 7) | ((uint32_t)fmt << 10) | ((uint32_t)a_mn << 15) |
+           ((uint32_t)b_mn << 16) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
 // Byte offset of element (row r, k) in a K-major SW128 image of R rows: K is split into

@@ -7,7 +7,8 @@
 
 namespace gm {
 
-__global__ void __launch_bounds__(128) k_tc_selftest(int N, int K, const uint8_t *__restrict__ aimg,
+__global__ void __launch_bounds__(128) k_tc_selftest(int N, int K, int a_mn, int b_mn,
+                                                     const uint8_t *__restrict__ aimg,
                                                      const uint8_t *__restrict__ bimg,
                                                      float *__restrict__ D, int *__restrict__ err)
 {
@@ -42,14 +43,20 @@ __global__ void __launch_bounds__(128) k_tc_selftest(int N, int K, const uint8_t
     const bool loaded = tc::mbar_wait(&bar_load, 0);
     if (tid == 0) {
         if (loaded) {
-            const uint32_t idesc = tc::idesc_f16(128, N, 1);
-            const int atoms = K / 64;
-            for (int a = 0; a < atoms; ++a)
-                for (int kk = 0; kk < 4; ++kk) {
-                    const uint64_t da = tc::desc_sw128(tc::smem_u32(sA) + a * 128 * 128 + kk * 32);
-                    const uint64_t db = tc::desc_sw128(tc::smem_u32(sB) + a * N * 128 + kk * 32);
-                    tc::mma_f16(taddr, da, db, idesc, (a | kk) != 0);
-                }
+            const uint32_t idesc = tc::idesc_f16(128, N, 1, a_mn, b_mn);
+            for (int ks = 0; ks < K / 16; ++ks) {
+                const int a = ks >> 2, kk = ks & 3;
+                // K-major: atom of 64 K x rows of 128 B, +32 B per K step of 16.
+                // MN-major: K groups of 8 at stride (R/64) 1024 B, two groups per K step.
+                const uint64_t da = a_mn
+                    ? tc::desc_sw128_mn(tc::smem_u32(sA) + ks * 2 * 2048, 1024, 2048)
+                    : tc::desc_sw128(tc::smem_u32(sA) + a * 128 * 128 + kk * 32);
+                const uint32_t bsbo = (uint32_t)(N >= 64 ? N / 64 : 1) * 1024u;
+                const uint64_t db = b_mn
+                    ? tc::desc_sw128_mn(tc::smem_u32(sB) + ks * 2 * bsbo, 1024, bsbo)
+                    : tc::desc_sw128(tc::smem_u32(sB) + a * N * 128 + kk * 32);
+                tc::mma_f16(taddr, da, db, idesc, ks != 0);
+            }
             tc::mma_commit(&bar_mma);
         } else {
             atomicExch(err, 1);
@@ -78,11 +85,12 @@ __global__ void __launch_bounds__(128) k_tc_selftest(int N, int K, const uint8_t
 
 using namespace gm;
 
-extern "C" int gm_tc_selftest(int64_t N, int64_t K, const void *aimg, const void *bimg, float *D,
-                              int32_t *err, void *stream)
+extern "C" int gm_tc_selftest(int64_t N, int64_t K, int a_mn, int b_mn, const void *aimg,
+                              const void *bimg, float *D, int32_t *err, void *stream)
 {
     if (N < 16 || N > 256 || (N % 16) || K < 64 || (K % 64) || 128 * K * 2 + N * K * 2 > 200 * 1024)
         return GM_ERR_BAD_SHAPE;
+    if (b_mn && (N % 64)) return GM_ERR_BAD_SHAPE;
     if (!aimg || !bimg || !D || !err) return GM_ERR_BAD_PTR;
     const size_t smem = (size_t)(128 * K * 2 + N * K * 2) + 1024;
     cudaError_t e = cudaFuncSetAttribute(k_tc_selftest, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -90,7 +98,7 @@ extern "C" int gm_tc_selftest(int64_t N, int64_t K, const void *aimg, const void
         set_error("gm_tc_selftest attr", e);
         return GM_ERR_LAUNCH;
     }
-    k_tc_selftest<<<1, 128, smem, as_stream(stream)>>>((int)N, (int)K, (const uint8_t *)aimg,
+    k_tc_selftest<<<1, 128, smem, as_stream(stream)>>>((int)N, (int)K, a_mn, b_mn, (const uint8_t *)aimg,
                                                       (const uint8_t *)bimg, D, (int *)err);
     return check_launch("gm_tc_selftest");
 }

@@ -1,0 +1,188 @@
+"""Batched spherical-harmonic transforms on the tcgen05 tensor cores.
+
+Many maps of one geometry share each generated Legendre row: spin 0 takes up to 32 maps
+per launch, spin 2 up to 32 (Q, U) fields.  The ring stage, the hemisphere pack, the
+ring-fold residual of the Jacobi refinement and the alm bookkeeping are the kernels of
+``legendre_tc.cu``; the contraction runs as bf16 hi/lo three-term MMAs with FP32
+accumulation in tensor memory and FP64 accumulation of the alms.
+"""
+
+import ctypes
+import threading
+
+import numpy as np
+import torch
+
+from . import _lib, sht
+
+MAX_MAPS_SPIN0 = 32
+MAX_FIELDS_SPIN2 = 32
+
+_TC_PLANS = {}
+_LOCK = threading.Lock()
+
+
+class TCPlan:
+    """Device constants of the batched path for one (nside, lmax) geometry."""
+
+    def __init__(self, plan):
+        self.plan = plan
+        lmax, dev = plan.lmax, plan.device
+        self.coef = {}
+        self.choff = {}
+        self.nchunks = {}
+        lib = _lib.load()
+        for spin in (0, 2):
+            tab = torch.empty((plan.nelem, 3), dtype=torch.float64, device=dev)
+            _lib.call("gm_tc_coef_table", lmax, spin, _lib.ptr(tab), _lib.stream_handle(dev))
+            self.coef[spin] = tab
+            host = np.zeros(plan.L + 1, dtype=np.int64)
+            _lib.call("gm_tc_syn_chunk_offsets", lmax, spin, host.ctypes.data_as(ctypes.c_void_p))
+            self.choff[spin] = torch.from_numpy(host).to(dev)
+            self.nchunks[spin] = int(host[-1])
+        self.nctas = torch.cuda.get_device_properties(dev).multi_processor_count
+        self.img_bytes = lib.gm_tc_ana_image_bytes(plan.nside, lmax)
+        self.scratch = torch.empty(lib.gm_tc_ana_scratch_bytes(plan.nside, self.nctas) // 8,
+                                   dtype=torch.float64, device=dev)
+        self.err = torch.zeros(1, dtype=torch.int32, device=dev)
+
+
+def get_tc_plan(nside, lmax, device=None):
+    plan = sht.get_plan(nside, lmax, device)
+    key = (plan.nside, plan.lmax, plan.device.index)
+    with _LOCK:
+        tp = _TC_PLANS.get(key)
+        if tp is None:
+            tp = TCPlan(plan)
+            _TC_PLANS[key] = tp
+    return tp
+
+
+def _variants(spin):
+    return (0,) if spin == 0 else (-2, 2)
+
+
+def _rows(spin, ncomp):
+    """(H, NR): rows per half and interleaved alm rows."""
+    H = 2 * ncomp if spin == 0 else ncomp
+    return H, (H if spin == 0 else 2 * H)
+
+
+def _check(tp):
+    if int(tp.err.item()):
+        tp.err.zero_()
+        raise RuntimeError("tensor-core Legendre kernel: a bounded wait timed out")
+
+
+class _Batch:
+    """Buffers of one batched transform."""
+
+    def __init__(self, tp, spin, ncomp):
+        p = tp.plan
+        self.tp, self.spin, self.ncomp = tp, spin, ncomp
+        self.H, self.NR = _rows(spin, ncomp)
+        dev = p.device
+        self.alm_i = torch.zeros((p.nelem, self.NR), dtype=torch.float64, device=dev)
+        self.img = [torch.empty(tp.img_bytes, dtype=torch.uint8, device=dev) for _ in _variants(spin)]
+
+    def analysis(self, scale):
+        p, tp = self.tp.plan, self.tp
+        for sp, img in zip(_variants(self.spin), self.img):
+            _lib.call("gm_tc_analysis", p.nside, p.lmax, self.spin, sp, self.ncomp, _lib.ptr(p.geom),
+                      _lib.ptr(p.seeds), _lib.ptr(tp.coef[self.spin]), _lib.ptr(img),
+                      _lib.ptr(self.alm_i), float(scale), _lib.ptr(tp.scratch), tp.nctas,
+                      _lib.ptr(tp.err), _lib.stream_handle(p.device))
+
+    def synthesis(self, synd=None):
+        """-> list of synd tensors (L, nlanes, 2H) float32, one per row variant."""
+        p, tp = self.tp.plan, self.tp
+        nch = tp.nchunks[self.spin]
+        simg_bytes = _lib.load().gm_tc_syn_image_bytes(nch)
+        simg = torch.empty(simg_bytes, dtype=torch.uint8, device=p.device)
+        outs = synd if synd is not None else [
+            torch.empty((p.L, p.nlanes, 2 * self.H), dtype=torch.float32, device=p.device)
+            for _ in _variants(self.spin)]
+        for sp, out in zip(_variants(self.spin), outs):
+            _lib.call("gm_tc_prep_syn", p.lmax, self.spin, sp, self.ncomp, _lib.ptr(self.alm_i),
+                      _lib.ptr(tp.choff[self.spin]), _lib.ptr(simg), simg_bytes,
+                      _lib.stream_handle(p.device))
+            _lib.call("gm_tc_synthesis", p.nside, p.lmax, self.spin, sp, self.ncomp, _lib.ptr(p.geom),
+                      _lib.ptr(p.seeds), _lib.ptr(tp.coef[self.spin]), _lib.ptr(simg),
+                      _lib.ptr(tp.choff[self.spin]), _lib.ptr(out), _lib.ptr(tp.err),
+                      _lib.stream_handle(p.device))
+        return outs
+
+    def to_api(self):
+        p = self.tp.plan
+        nfield = self.ncomp if self.spin == 0 else self.ncomp // 2
+        out = torch.empty((self.ncomp, p.nelem), dtype=torch.complex128, device=p.device)
+        _lib.call("gm_tc_alm_layout", p.lmax, self.spin, nfield, _lib.ptr(self.alm_i), _lib.ptr(out), 1,
+                  _lib.stream_handle(p.device))
+        return out
+
+    def from_api(self, alm):
+        p = self.tp.plan
+        nfield = self.ncomp if self.spin == 0 else self.ncomp // 2
+        alm = alm.contiguous()
+        _lib.call("gm_tc_alm_layout", p.lmax, self.spin, nfield, _lib.ptr(self.alm_i), _lib.ptr(alm), 0,
+                  _lib.stream_handle(p.device))
+
+
+def _check_batch(spin, ncomp):
+    if spin == 0 and not 1 <= ncomp <= MAX_MAPS_SPIN0:
+        raise ValueError(f"spin-0 batches hold 1..{MAX_MAPS_SPIN0} maps")
+    if spin == 2 and not (ncomp % 2 == 0 and 2 <= ncomp <= 2 * MAX_FIELDS_SPIN2):
+        raise ValueError(f"spin-2 batches hold 1..{MAX_FIELDS_SPIN2} (Q, U) fields")
+    if spin not in (0, 2):
+        raise NotImplementedError("only spin 0 and spin 2")
+
+
+def map2alm_tc(maps, spin, nside, lmax, n_iter):
+    """Batched analysis: maps (ncomp, npix) float64/float32 CUDA -> (ncomp, nelem) complex128
+    (spin 2: rows E, B per field), with n_iter Jacobi iterations."""
+    ncomp = maps.shape[0]
+    _check_batch(spin, ncomp)
+    tp = get_tc_plan(nside, lmax, maps.device)
+    p = tp.plan
+    spec = sht.ring_analysis(p, maps, _lib.MIXED)
+    b = _Batch(tp, spin, ncomp)
+    rhs_map = torch.empty((p.L, p.nlanes, ncomp, 4), dtype=torch.float32, device=p.device)
+    _lib.call("gm_tc_pack", p.nside, p.lmax, spin, ncomp, _lib.ptr(spec), _lib.ptr(rhs_map),
+              _lib.ptr(b.img[0]), _lib.ptr(b.img[1]) if spin else None, _lib.stream_handle(p.device))
+    del spec
+    sht._timed(f"tc_analysis_s{spin}", p, spin, ncomp, lambda: b.analysis(1.0))
+    synd = None
+    for _ in range(int(n_iter)):
+        synd = _timed_syn(b, synd)
+        _lib.call("gm_tc_fold", p.nside, p.lmax, spin, ncomp, _lib.ptr(synd[0]),
+                  _lib.ptr(synd[1]) if spin else None, _lib.ptr(rhs_map), _lib.ptr(p.shifted),
+                  _lib.ptr(b.img[0]), _lib.ptr(b.img[1]) if spin else None,
+                  _lib.stream_handle(p.device))
+        sht._timed(f"tc_analysis_s{spin}", p, spin, ncomp, lambda: b.analysis(-1.0))
+    out = b.to_api()
+    _check(tp)
+    return out
+
+
+def _timed_syn(b, synd):
+    box = []
+    sht._timed(f"tc_synthesis_s{b.spin}", b.tp.plan, b.spin, b.ncomp, lambda: box.append(b.synthesis(synd)))
+    return box[0]
+
+
+def alm2map_tc(alm, spin, nside, lmax):
+    """Batched synthesis: (nrows, nelem) complex128 -> (nrows, npix) float64 maps."""
+    ncomp = alm.shape[0]
+    _check_batch(spin, ncomp)
+    tp = get_tc_plan(nside, lmax, alm.device)
+    p = tp.plan
+    b = _Batch(tp, spin, ncomp)
+    b.img = []
+    b.from_api(alm.to(torch.complex128))
+    synd = b.synthesis()
+    syn = torch.empty((p.L, p.nlanes, ncomp, 4), dtype=torch.float32, device=p.device)
+    _lib.call("gm_tc_synd_to_syn", p.nside, p.lmax, spin, ncomp, _lib.ptr(synd[0]),
+              _lib.ptr(synd[1]) if spin else None, _lib.ptr(syn), _lib.stream_handle(p.device))
+    maps = sht.ring_synthesis(p, syn, _lib.MIXED)
+    _check(tp)
+    return maps

@@ -164,17 +164,71 @@ int gm_lu_factor(int64_t n, double *a, int32_t *piv, int32_t *status, void *stre
 int gm_lu_solve(int64_t n, const double *lu, const int32_t *piv, int64_t nrhs,
                 double *b, void *stream);
 
+/* ----------------------------------------------- batched tensor-core Legendre stage */
+
+/* Batched transforms on tcgen05 (replace march_v2.cu:155-407 for many maps per launch).
+ * A batch holds up to 128 real right-hand-side rows: spin 0, ncomp <= 32 maps (rows
+ * [G_north | G_south] x re/im); spin 2, ncomp = 2F <= 64 (Q, U of F fields; two row
+ * variants s' = -2 with rows [P_N | M_S] and s' = +2 with rows [M_N | P_S], P = G_Q + i G_U,
+ * M = G_Q - i G_U).  Operand images are bf16 hi/lo planes in the 128-byte-swizzled
+ * MN-major layout of gm_tc_selftest.  The interleaved alm alm_i is (nelem, NR) float64
+ * with NR = 2 ncomp (spin 0: map x re/im) or 2 ncomp (spin 2: [a_{+2} | a_{-2}] x re/im). */
+
+/* Lane groups of 128 lanes and analysis image bytes ((lmax+1) x groups x 64 KB). */
+int64_t gm_tc_lane_groups(int64_t nside);
+int64_t gm_tc_ana_image_bytes(int64_t nside, int64_t lmax);
+/* Scratch for the analysis recurrence state: nctas x 2 nside x 3 float64. */
+int64_t gm_tc_ana_scratch_bytes(int64_t nside, int64_t nctas);
+/* Synthesis chunk offsets (host array of lmax+2 int64; total chunks in choff[lmax+1]) and
+ * image bytes for that many chunks (32 KB each). */
+int gm_tc_syn_chunk_offsets(int64_t lmax, int spin, int64_t *choff_host);
+int64_t gm_tc_syn_image_bytes(int64_t nchunks);
+/* Recurrence coefficient table (nelem, 3) float64 for spin 0 or 2. */
+int gm_tc_coef_table(int64_t lmax, int spin, double *tab, void *stream);
+/* Ring spectra (ncomp, nring, L) complex64 -> rhs_map (L, nlanes, ncomp) float4
+ * [G_N re, im, G_S re, im] and the analysis images (img_b only for spin 2). */
+int gm_tc_pack(int64_t nside, int64_t lmax, int spin, int64_t ncomp, const void *ringspec,
+               void *rhs_map, void *img_a, void *img_b, void *stream);
+/* alm_i += scale * analysis of the rows of `img` for row variant sp (0, -2, +2).
+ * scratch: gm_tc_ana_scratch_bytes(nside, nctas); nctas persistent CTAs (one per SM).
+ * err (int32) set non-zero if a bounded wait timed out. */
+int gm_tc_analysis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                   const double *geom, const double *seeds, const double *coef, const void *img,
+                   double *alm_i, double scale, double *scratch, int64_t nctas, int32_t *err,
+                   void *stream);
+/* Synthesis operand images from alm_i for row variant sp (device choff). */
+int gm_tc_prep_syn(int64_t lmax, int spin, int sp, int64_t ncomp, const double *alm_i,
+                   const int64_t *choff, void *simg, int64_t simg_bytes, void *stream);
+/* synd (L, nlanes, 2H) float32 = rows of the synthesis for row variant sp. */
+int gm_tc_synthesis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                    const double *geom, const double *seeds, const double *coef, const void *simg,
+                    const int64_t *choff, float *synd, int32_t *err, void *stream);
+/* Ring-fold residual of the batched synthesis minus rhs_map, written as the next
+ * analysis images (replaces march_v2.cu:426-493 for the batched path). */
+int gm_tc_fold(int64_t nside, int64_t lmax, int spin, int64_t ncomp, const float *synd_a,
+               const float *synd_b, const void *rhs_map, const uint8_t *shifted, void *img_a,
+               void *img_b, void *stream);
+/* Batched synthesis output -> syn layout of gm_ring_synthesis. */
+int gm_tc_synd_to_syn(int64_t nside, int64_t lmax, int spin, int64_t ncomp, const float *synd_a,
+                      const float *synd_b, float *syn, void *stream);
+/* alm_i <-> API layout (nalm, nelem) complex128 (spin 2: E, B per field). */
+int gm_tc_alm_layout(int64_t lmax, int spin, int64_t nfield, double *alm_i, double *alm_api,
+                     int to_api, void *stream);
+
 /* ---------------------------------------------------------- tensor-core check */
 
 /* One-CTA tcgen05 check: D[128 x N] (float32, row-major) = A[128 x K] * B[N x K]^T where
  * A and B are bf16 operand images in the K-major 128-byte-swizzled layout the tensor-core
  * kernels use (K in atoms of 64; element (r, k) of an R-row image at byte
  * (k/64) R 128 + (r/8) 1024 + (r%8) 128 + (((k%64)/8) ^ (r%8)) 16 + (k%8) 2).
+ * With a_mn / b_mn set, that operand is MN-major instead: element (r, k) of an R-row
+ * image (R % 64 == 0) at byte (k/8) (R/64) 1024 + (r/64) 1024 + (k%8) 128
+ * + (((r%64)/8) ^ (k%8)) 16 + (r%8) 2.
  * N in [16, 256] step 16, K a multiple of 64.  err (one int32) is set non-zero if a
  * bounded wait timed out.  No counterpart in the reference: a health check of the
  * tensor-core machinery used by gm_legendre_*_tc. */
-int gm_tc_selftest(int64_t N, int64_t K, const void *aimg, const void *bimg, float *D,
-                   int32_t *err, void *stream);
+int gm_tc_selftest(int64_t N, int64_t K, int a_mn, int b_mn, const void *aimg,
+                   const void *bimg, float *D, int32_t *err, void *stream);
 
 #ifdef __cplusplus
 }
