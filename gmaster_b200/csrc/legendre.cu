@@ -173,14 +173,14 @@ __global__ void __launch_bounds__(kThreads) k_legendre_ana(
 #pragma unroll
                         for (int r = 0; r < R; ++r) {
                             if (SPIN == 0) {
-                                double nv = cf.alpha * (x[r] * v[0][r]) - cf.beta * vp[0][r];
+                                double nv = fma(cf.alpha * x[r], v[0][r], -cf.beta * vp[0][r]);
                                 vp[0][r] = v[0][r];
                                 v[0][r] = nv;
                                 rescale(v[0][r], vp[0][r], kx[0][r]);
                             } else {
                                 // s' = -2: x - m s'/((l-1)l) = x + c0 ; s' = +2: x - c0
-                                double nva = cf.alpha * ((x[r] + cf.c0) * v[0][r]) - cf.beta * vp[0][r];
-                                double nvb = cf.alpha * ((x[r] - cf.c0) * v[1][r]) - cf.beta * vp[1][r];
+                                double nva = fma(cf.alpha * (x[r] + cf.c0), v[0][r], -cf.beta * vp[0][r]);
+                                double nvb = fma(cf.alpha * (x[r] - cf.c0), v[1][r], -cf.beta * vp[1][r]);
                                 vp[0][r] = v[0][r];
                                 v[0][r] = nva;
                                 vp[1][r] = v[1][r];
@@ -339,13 +339,13 @@ __global__ void __launch_bounds__(kThreads) k_legendre_syn(
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     if (SPIN == 0) {
-                        double nv = cf.alpha * (x[r] * v[0][r]) - cf.beta * vp[0][r];
+                        double nv = fma(cf.alpha * x[r], v[0][r], -cf.beta * vp[0][r]);
                         vp[0][r] = v[0][r];
                         v[0][r] = nv;
                         rescale(v[0][r], vp[0][r], kx[0][r]);
                     } else {
-                        double nva = cf.alpha * ((x[r] + cf.c0) * v[0][r]) - cf.beta * vp[0][r];
-                        double nvb = cf.alpha * ((x[r] - cf.c0) * v[1][r]) - cf.beta * vp[1][r];
+                        double nva = fma(cf.alpha * (x[r] + cf.c0), v[0][r], -cf.beta * vp[0][r]);
+                        double nvb = fma(cf.alpha * (x[r] - cf.c0), v[1][r], -cf.beta * vp[1][r]);
                         vp[0][r] = v[0][r];
                         v[0][r] = nva;
                         vp[1][r] = v[1][r];

@@ -67,13 +67,22 @@ __device__ __forceinline__ void seed_lane(const double *__restrict__ sd, double 
 }
 
 // One recurrence step to degree l (> l0) using coefficients for (l, m); sgn_c selects
-// x - c0 (s' = +2), x + c0 (s' = -2) or x (s' = 0, c0 = 0).
-__device__ __forceinline__ void step(double x, const Coef &c, double sgn_c, double &v, double &vp,
-                                     int &k)
+// x - c0 (s' = +2), x + c0 (s' = -2) or x (s' = 0, c0 = 0).  Written so that a single
+// FMA sits on the dependent chain: a = alpha (x - c) and b = beta v_{l-2} do not depend on
+// v_{l-1}.
+__device__ __forceinline__ void step(double x, const Coef &c, double sgn_c, double &v, double &vp)
 {
-    const double nv = c.alpha * ((x - sgn_c * c.c0) * v) - c.beta * vp;
+    const double a = c.alpha * (x - sgn_c * c.c0);
+    const double b = c.beta * vp;
+    const double nv = fma(a, v, -b);
     vp = v;
     v = nv;
+}
+
+// Binary-exponent carry, applied once per 8 steps: a lane still below 2^-300 (k < 0) is
+// renormalised when it passes 2^300 (growth over 8 steps stays far below 2^700).
+__device__ __forceinline__ void rescale(double &v, double &vp, int &k)
+{
     if (k < 0 && fabs(v) > kBig) {
         v *= kShrink;
         vp *= kShrink;
@@ -118,6 +127,8 @@ struct Params {
     int var;              // seed variant 0 / 1 / 2
 };
 
+__device__ __forceinline__ void gen_barrier() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
 __device__ __forceinline__ double sgn_of(int sp) { return sp > 0 ? 1.0 : (sp < 0 ? -1.0 : 0.0); }
 
 // ------------------------------------------------------------------------------- analysis
@@ -145,6 +156,7 @@ __device__ __forceinline__ int64_t snake_m(int64_t i, int64_t c, int64_t G)
     return round * G + pos;
 }
 
+template <int SPIN>
 __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t *__restrict__ aimg,
                                                         double *__restrict__ alm_i,
                                                         double *__restrict__ scratch,
@@ -157,6 +169,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
     uint8_t *smem = smem_raw + (base - tc::smem_u32(smem_raw));
     uint8_t *sA = smem;                      // 2 x 64 KB
     uint8_t *sB = smem + 4 * kAImg;          // 2 x 32 KB
+    double2 *sAB = reinterpret_cast<double2 *>(smem + 4 * kAImg + 4 * kBTileA);   // (alpha, beta) x kSB
+    double *sC0 = reinterpret_cast<double *>(sAB + kSB);                          // c0 x kSB (spin 2)
     const int64_t L = p.lmax + 1, NG = (p.nlanes + kKC - 1) / kKC;
     const int64_t G = gridDim.x, c = blockIdx.x;
     const int l0min = abs(p.sp);
@@ -262,10 +276,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
             const int64_t mb = alm_idx(p.lmax, 0, m);   // coefficient / alm base of order m
             for (int64_t s = 0; s < nsb && !*abort; ++s) {
                 const int64_t lb = l0 + s * kSB;
+                // coefficients of this superblock into shared memory (every generator has
+                // finished the previous superblock: its epilogue waited for all its tiles)
+                for (int e = tid; e < kSB; e += kGen) {
+                    const int64_t l = lb + e;
+                    const Coef cf = (l < L) ? load_coef(p.coef, mb + l) : Coef{0.0, 0.0, 0.0};
+                    sAB[e] = make_double2(cf.alpha, cf.beta);
+                    if (SPIN) sC0[e] = sgn_c * cf.c0;
+                }
+                gen_barrier();
                 for (int64_t g = 0; g < NG && !*abort; ++g) {
                     const int64_t jl = g * kKC + tid;
                     const bool valid = jl < p.nlanes;
-                    double x = 0.0, v = 0.0, vp = 0.0;
+                    double x = 0.0, v = 0.0, vp = 0.0;   // padding lanes stay exactly zero
                     int k = 0;
                     if (valid) {
                         x = p.geom[jl];
@@ -278,20 +301,47 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
                             k = (int)my_scratch[jl * 3 + 2];
                         }
                     }
+                    bool emit = (k == 0);
                     for (int t = 0; t < kSB / kNB; ++t, ++u) {
                         const uint32_t st = u & 1;
                         if (!wait_or_abort(&sh.b_free[st], ((u >> 1) & 1) ^ 1, abort, err)) break;
                         const uint32_t b0 = tc::smem_u32(sB + st * 2 * kBTileA);
                         const uint32_t rowbase = b0 + (tid >> 3) * 1024 + (tid & 7) * 128;
+                        // rows of this tile with l < L; the seed row (l == l0) is the first row
+                        // of the first tile of superblock 0 and is emitted without a step
+                        const int nvalid = (int)((L - (lb + t * kNB)) < kNB ? (L - (lb + t * kNB)) : kNB);
+                        const bool seed_tile = (s == 0 && t == 0);
 #pragma unroll 1
                         for (int cc = 0; cc < kNB / 8; ++cc) {
                             float vals[8];
+                            const int r0 = t * kNB + cc * 8;
+                            if (cc * 8 + 8 <= nvalid && !(seed_tile && cc == 0)) {
 #pragma unroll
-                            for (int e = 0; e < 8; ++e) {
-                                const int64_t l = lb + t * kNB + cc * 8 + e;
-                                if (l > l0 && l < L) step(x, load_coef(p.coef, mb + l), sgn_c, v, vp, k);
-                                vals[e] = (valid && l < L && k == 0) ? (float)v : 0.0f;
+                                for (int e = 0; e < 8; ++e) {
+                                    const double2 ab = sAB[r0 + e];
+                                    const double xs = SPIN ? x - sC0[r0 + e] : x;
+                                    const double nv = fma(ab.x * xs, v, -ab.y * vp);
+                                    vp = v;
+                                    v = nv;
+                                    vals[e] = emit ? (float)v : 0.0f;
+                                }
+                            } else {
+#pragma unroll
+                                for (int e = 0; e < 8; ++e) {
+                                    const int row = cc * 8 + e;
+                                    const bool live = row < nvalid;
+                                    if (live && !(seed_tile && row == 0)) {
+                                        const double2 ab = sAB[r0 + e];
+                                        const double xs = SPIN ? x - sC0[r0 + e] : x;
+                                        const double nv = fma(ab.x * xs, v, -ab.y * vp);
+                                        vp = v;
+                                        v = nv;
+                                    }
+                                    vals[e] = (live && emit) ? (float)v : 0.0f;
+                                }
                             }
+                            rescale(v, vp, k);
+                            emit = (k == 0);
                             uint4 hi, lo;
                             pack8(vals, hi, lo);
                             const uint32_t off = ((cc ^ (tid & 7)) << 4);
@@ -353,6 +403,7 @@ struct __align__(8) SynShared {
 
 // almT images: chunk cc of order m covers l in [64 (c0(m) + cc), +64), c0(m) = floor(l0(m)/64);
 // image index = choff[m] + cc.
+template <int SPIN>
 __global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t *__restrict__ simg,
                                                         const int64_t *__restrict__ choff,
                                                         float *__restrict__ synd, int R2,
@@ -365,6 +416,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t 
     uint8_t *smem = smem_raw + (base - tc::smem_u32(smem_raw));
     uint8_t *sA = smem;                    // 2 x 32 KB
     uint8_t *sB = smem + 4 * kSImg;        // 2 x 64 KB
+    double2 *sAB = reinterpret_cast<double2 *>(smem + 4 * kSImg + 4 * kBTileS);   // 2 x kKL (alpha, beta)
+    double *sC0 = reinterpret_cast<double *>(sAB + 2 * kKL);                      // 2 x kKL c0
     const int64_t L = p.lmax + 1;
     const int64_t m = blockIdx.y, tile = blockIdx.x;
     const int l0min = abs(p.sp);
@@ -445,24 +498,61 @@ __global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t 
                 seed_lane(p.seeds + ((int64_t)p.var * L + m) * 4, p.geom[p.nlanes + jl],
                           p.geom[2 * p.nlanes + jl], v[h], k[h]);
         }
+        bool emit[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) emit[h] = (k[h] == 0);
         for (int64_t cc = 0; cc < nch; ++cc) {
             const uint32_t st = (uint32_t)cc & 1;
+            double2 *cab = sAB + st * kKL;
+            double *cc0 = sC0 + st * kKL;
+            if (tid < kKL) {
+                const int64_t l = (c0 + cc) * kKL + tid;
+                const Coef cf = (l > l0 && l < L) ? load_coef(p.coef, mb + l) : Coef{0.0, 0.0, 0.0};
+                cab[tid] = make_double2(cf.alpha, cf.beta);
+                if (SPIN) cc0[tid] = sgn_c * cf.c0;
+            }
+            gen_barrier();
             if (!wait_or_abort(&sh.b_free[st], ((uint32_t)(cc >> 1) & 1) ^ 1, abort, err)) break;
             const uint32_t b0 = tc::smem_u32(sB + st * 2 * kBTileS);
 #pragma unroll 1
             for (int sub = 0; sub < kKL / 8; ++sub) {
                 float vals[2][8];
+                const int64_t lsub = (c0 + cc) * kKL + sub * 8;
+                if (lsub > l0 && lsub + 8 <= L) {
 #pragma unroll
-                for (int e = 0; e < 8; ++e) {
-                    const int64_t l = (c0 + cc) * kKL + sub * 8 + e;
-                    Coef cf;
-                    const bool adv = l > l0 && l < L;
-                    if (adv) cf = load_coef(p.coef, mb + l);
+                    for (int e = 0; e < 8; ++e) {
+                        const double2 ab = cab[sub * 8 + e];
+                        const double cs = SPIN ? cc0[sub * 8 + e] : 0.0;
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        if (adv) step(x[h], cf, sgn_c, v[h], vp[h], k[h]);
-                        vals[h][e] = (valid[h] && l >= l0 && l < L && k[h] == 0) ? (float)v[h] : 0.0f;
+                        for (int h = 0; h < 2; ++h) {
+                            const double nv = fma(ab.x * (SPIN ? x[h] - cs : x[h]), v[h], -ab.y * vp[h]);
+                            vp[h] = v[h];
+                            v[h] = nv;
+                            vals[h][e] = emit[h] ? (float)v[h] : 0.0f;
+                        }
                     }
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) {
+                        const int64_t l = lsub + e;
+                        const bool adv = l > l0 && l < L;
+                        const double2 ab = cab[sub * 8 + e];
+                        const double cs = SPIN ? cc0[sub * 8 + e] : 0.0;
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            if (adv) {
+                                const double nv = fma(ab.x * (SPIN ? x[h] - cs : x[h]), v[h], -ab.y * vp[h]);
+                                vp[h] = v[h];
+                                v[h] = nv;
+                            }
+                            vals[h][e] = (l >= l0 && l < L && emit[h]) ? (float)v[h] : 0.0f;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    rescale(v[h], vp[h], k[h]);
+                    emit[h] = (k[h] == 0);
                 }
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
@@ -926,15 +1016,16 @@ extern "C" int gm_tc_analysis(int64_t nside, int64_t lmax, int spin, int sp, int
         return GM_ERR_BAD_SHAPE;
     if ((spin == 0) != (sp == 0) || (spin == 2 && sp != 2 && sp != -2)) return GM_ERR_BAD_SHAPE;
     if (!geom || !seeds || !coef || !img || !alm_i || !scratch || !err) return GM_ERR_BAD_PTR;
-    const size_t smem = 4 * kAImg + 4 * kBTileA + 1024;
-    cudaError_t e = cudaFuncSetAttribute(k_ana_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t smem = 4 * kAImg + 4 * kBTileA + kSB * (sizeof(double2) + sizeof(double)) + 1024;
+    auto kern = spin == 0 ? k_ana_tc<0> : k_ana_tc<2>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) {
         set_error("gm_tc_analysis attr", e);
         return GM_ERR_LAUNCH;
     }
     Params p = make_params(nside, lmax, spin, sp, ncomp, geom, seeds, coef, scale);
-    k_ana_tc<<<(unsigned)nctas, kThreads, smem, as_stream(stream)>>>(p, (const uint8_t *)img, alm_i,
-                                                                    scratch, (int *)err);
+    kern<<<(unsigned)nctas, kThreads, smem, as_stream(stream)>>>(p, (const uint8_t *)img, alm_i,
+                                                                scratch, (int *)err);
     return check_launch("gm_tc_analysis");
 }
 
@@ -964,8 +1055,9 @@ extern "C" int gm_tc_synthesis(int64_t nside, int64_t lmax, int spin, int sp, in
     if (nside < 1 || lmax < 2 || !tc_shape_ok(spin, ncomp)) return GM_ERR_BAD_SHAPE;
     if ((spin == 0) != (sp == 0) || (spin == 2 && sp != 2 && sp != -2)) return GM_ERR_BAD_SHAPE;
     if (!geom || !seeds || !coef || !simg || !choff || !synd || !err) return GM_ERR_BAD_PTR;
-    const size_t smem = 4 * kSImg + 4 * kBTileS + 1024;
-    cudaError_t e = cudaFuncSetAttribute(k_syn_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t smem = 4 * kSImg + 4 * kBTileS + 2 * kKL * (sizeof(double2) + sizeof(double)) + 1024;
+    auto kern = spin == 0 ? k_syn_tc<0> : k_syn_tc<2>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) {
         set_error("gm_tc_synthesis attr", e);
         return GM_ERR_LAUNCH;
@@ -973,8 +1065,8 @@ extern "C" int gm_tc_synthesis(int64_t nside, int64_t lmax, int spin, int sp, in
     Params p = make_params(nside, lmax, spin, sp, ncomp, geom, seeds, coef, 1.0);
     const int R2 = 2 * p.H;
     dim3 grid((unsigned)((p.nlanes + kLT - 1) / kLT), (unsigned)(lmax + 1));
-    k_syn_tc<<<grid, kThreads, smem, as_stream(stream)>>>(p, (const uint8_t *)simg, choff, synd, R2,
-                                                         (int *)err);
+    kern<<<grid, kThreads, smem, as_stream(stream)>>>(p, (const uint8_t *)simg, choff, synd, R2,
+                                                     (int *)err);
     return check_launch("gm_tc_synthesis");
 }
 
