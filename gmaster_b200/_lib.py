@@ -53,6 +53,8 @@ SIGNATURES = {
     "gm_tc_pack": ([_c_i64, _c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
     "gm_tc_analysis": ([_c_i64, _c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
                         _c_dbl, _c_vp, _c_i64, _c_vp, _c_vp], _c_int),
+    "gm_tc_analysis_noalloc": ([_c_i64, _c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp,
+                                _c_vp, _c_dbl, _c_i64, _c_vp, _c_vp], _c_int),
     "gm_tc_prep_syn": ([_c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_i64, _c_vp], _c_int),
     "gm_tc_synthesis": ([_c_i64, _c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
                          _c_vp, _c_vp, _c_vp], _c_int),

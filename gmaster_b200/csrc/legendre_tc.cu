@@ -20,6 +20,8 @@
 // Replaces gmaster/_native/cuda/march_v2.cu:155-407 (FP32 SIMT march) for batched maps.
 #include <math.h>
 
+#include <mutex>
+
 #include "gm_common.cuh"
 #include "tc_common.cuh"
 
@@ -1105,4 +1107,67 @@ extern "C" int gm_tc_synd_to_syn(int64_t nside, int64_t lmax, int spin, int64_t 
     k_synd_to_syn<<<(unsigned)((tot + 255) / 256), 256, 0, as_stream(stream)>>>(
         2 * nside, lmax + 1, (int)ncomp, spin, synd_a, synd_b, 2 * H, syn);
     return check_launch("gm_tc_synd_to_syn");
+}
+
+// ------------------------------------------------------------------ allocation-free variant
+//
+// gm_tc_analysis_noalloc is gm_tc_analysis for callers that cannot call cudaMalloc (see
+// include/gm_b200.h).  Its recurrence-state scratch is this file-scope device array
+// instead of a caller buffer: up to kNoAllocLaneSlots (CTA, lane) slots of 3 doubles,
+// 148 CTAs x 4096 lanes (Nside 2048 on every SM of a B200), 14.5 MB, held by every GPU
+// that loads the library until the process exits.  The kernel writes each slot before
+// reading it, so no clearing is needed; the array keeps the last call's contents, and
+// calls that overlap on the GPU race on it.
+namespace gm {
+namespace ltc {
+
+constexpr int64_t kNoAllocLaneSlots = 148 * 4096;
+static __device__ __align__(256) double g_ana_state[kNoAllocLaneSlots * 3];
+
+// Device address of g_ana_state, looked up once per device with that device current.
+static double *noalloc_state_ptr(int dev, cudaError_t &err)
+{
+    static std::mutex mu;
+    static double *ptrs[64] = {nullptr};
+    err = cudaSuccess;
+    if (dev < 0 || dev >= 64) {
+        err = cudaErrorInvalidDevice;
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ptrs[dev]) {
+        void *p = nullptr;
+        err = cudaGetSymbolAddress(&p, g_ana_state);
+        if (err != cudaSuccess) return nullptr;
+        ptrs[dev] = static_cast<double *>(p);
+    }
+    return ptrs[dev];
+}
+
+}  // namespace ltc
+}  // namespace gm
+
+extern "C" int gm_tc_analysis_noalloc(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                                      const double *geom, const double *seeds, const double *coef,
+                                      const void *img, double *alm_i, double scale, int64_t nctas,
+                                      int32_t *err, void *stream)
+{
+    if (nside < 1 || nctas < 1 || nctas * 2 * nside > gm::ltc::kNoAllocLaneSlots) {
+        gm::set_error_msg("gm_tc_analysis_noalloc: nctas * 2 * nside exceeds the 606208 lane slots "
+                          "of the static scratch (e.g. at most 148 CTAs at Nside 2048)");
+        return GM_ERR_BAD_SHAPE;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        gm::set_error("gm_tc_analysis_noalloc cudaGetDevice", e);
+        return GM_ERR_LAUNCH;
+    }
+    double *state = gm::ltc::noalloc_state_ptr(dev, e);
+    if (!state) {
+        gm::set_error("gm_tc_analysis_noalloc cudaGetSymbolAddress", e);
+        return GM_ERR_LAUNCH;
+    }
+    return gm_tc_analysis(nside, lmax, spin, sp, ncomp, geom, seeds, coef, img, alm_i, scale, state,
+                          nctas, err, stream);
 }

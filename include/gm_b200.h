@@ -196,6 +196,24 @@ int gm_tc_analysis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
                    const double *geom, const double *seeds, const double *coef, const void *img,
                    double *alm_i, double scale, double *scratch, int64_t nctas, int32_t *err,
                    void *stream);
+/* gm_tc_analysis without any caller-allocated memory.  No counterpart in the reference.
+ * For callers that cannot call cudaMalloc or hand over a scratch buffer: for example a
+ * custom call inside a framework that owns every device allocation (an XLA/JAX FFI
+ * handler draws only on the framework's own pool), or a service that reserves its device
+ * memory once at start-up and must not allocate afterwards (cudaMalloc may synchronise the
+ * device and fragments the reserved space).  The recurrence-state scratch is a file-scope
+ * device array of 606208 (CTA, lane) slots x 3 float64 (14.5 MB, enough for nctas = 148 at
+ * Nside 2048), held by every GPU that loads the library until the process exits; calls with
+ * nctas * 2 * nside above 606208 return GM_ERR_BAD_SHAPE.  The first call on a device looks
+ * up the array's device address with that device current; make that first call before any
+ * stream capture.  The array keeps the last call's contents (nothing in it needs clearing)
+ * and calls that overlap on the GPU race on it.  Inputs and outputs as gm_tc_analysis: the
+ * caller zeroes alm_i before the first accumulation and *err before the call. */
+int gm_tc_analysis_noalloc(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                           const double *geom, const double *seeds, const double *coef,
+                           const void *img, double *alm_i, double scale, int64_t nctas,
+                           int32_t *err, void *stream);
+
 /* Synthesis operand images from alm_i for row variant sp (device choff). */
 int gm_tc_prep_syn(int64_t lmax, int spin, int sp, int64_t ncomp, const double *alm_i,
                    const int64_t *choff, void *simg, int64_t simg_bytes, void *stream);
