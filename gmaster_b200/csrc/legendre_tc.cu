@@ -280,9 +280,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
                 const int64_t lb = l0 + s * kSB;
                 // coefficients of this superblock into shared memory (every generator has
                 // finished the previous superblock: its epilogue waited for all its tiles)
+                // Every row is one uniform step v_l = alpha (x - c) v_{l-1} - beta v_{l-2}: the
+                // seed row l0 uses (alpha, beta) = (0, -1) with the state entering as
+                // (v, vp) = (0, seed), and rows past lmax use (0, 0), which emit exact zeros.
                 for (int e = tid; e < kSB; e += kGen) {
                     const int64_t l = lb + e;
-                    const Coef cf = (l < L) ? load_coef(p.coef, mb + l) : Coef{0.0, 0.0, 0.0};
+                    Coef cf = Coef{0.0, 0.0, 0.0};
+                    if (l == l0) cf.beta = -1.0;
+                    else if (l < L) cf = load_coef(p.coef, mb + l);
                     sAB[e] = make_double2(cf.alpha, cf.beta);
                     if (SPIN) sC0[e] = sgn_c * cf.c0;
                 }
@@ -296,7 +301,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
                         x = p.geom[jl];
                         if (s == 0) {
                             seed_lane(p.seeds + ((int64_t)p.var * L + m) * 4, p.geom[p.nlanes + jl],
-                                      p.geom[2 * p.nlanes + jl], v, k);
+                                      p.geom[2 * p.nlanes + jl], vp, k);
                         } else {
                             v = my_scratch[jl * 3];
                             vp = my_scratch[jl * 3 + 1];
@@ -309,38 +314,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
                         if (!wait_or_abort(&sh.b_free[st], ((u >> 1) & 1) ^ 1, abort, err)) break;
                         const uint32_t b0 = tc::smem_u32(sB + st * 2 * kBTileA);
                         const uint32_t rowbase = b0 + (tid >> 3) * 1024 + (tid & 7) * 128;
-                        // rows of this tile with l < L; the seed row (l == l0) is the first row
-                        // of the first tile of superblock 0 and is emitted without a step
-                        const int nvalid = (int)((L - (lb + t * kNB)) < kNB ? (L - (lb + t * kNB)) : kNB);
-                        const bool seed_tile = (s == 0 && t == 0);
+                        const double2 *cab = sAB + t * kNB;
+                        const double *cc0 = sC0 + t * kNB;
 #pragma unroll 1
                         for (int cc = 0; cc < kNB / 8; ++cc) {
                             float vals[8];
-                            const int r0 = t * kNB + cc * 8;
-                            if (cc * 8 + 8 <= nvalid && !(seed_tile && cc == 0)) {
 #pragma unroll
-                                for (int e = 0; e < 8; ++e) {
-                                    const double2 ab = sAB[r0 + e];
-                                    const double xs = SPIN ? x - sC0[r0 + e] : x;
-                                    const double nv = fma(ab.x * xs, v, -ab.y * vp);
-                                    vp = v;
-                                    v = nv;
-                                    vals[e] = emit ? (float)v : 0.0f;
-                                }
-                            } else {
-#pragma unroll
-                                for (int e = 0; e < 8; ++e) {
-                                    const int row = cc * 8 + e;
-                                    const bool live = row < nvalid;
-                                    if (live && !(seed_tile && row == 0)) {
-                                        const double2 ab = sAB[r0 + e];
-                                        const double xs = SPIN ? x - sC0[r0 + e] : x;
-                                        const double nv = fma(ab.x * xs, v, -ab.y * vp);
-                                        vp = v;
-                                        v = nv;
-                                    }
-                                    vals[e] = (live && emit) ? (float)v : 0.0f;
-                                }
+                            for (int e = 0; e < 8; ++e) {
+                                const double2 ab = cab[cc * 8 + e];
+                                const double xs = SPIN ? x - cc0[cc * 8 + e] : x;
+                                const double nv = fma(ab.x * xs, v, -ab.y * vp);
+                                vp = v;
+                                v = nv;
+                                vals[e] = emit ? (float)v : 0.0f;
                             }
                             rescale(v, vp, k);
                             emit = (k == 0);
@@ -520,7 +506,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t 
             for (int sub = 0; sub < kKL / 8; ++sub) {
                 float vals[2][8];
                 const int64_t lsub = (c0 + cc) * kKL + sub * 8;
-                if (lsub > l0 && lsub + 8 <= L) {
+                if (lsub > l0) {   // rows past lmax have zero coefficients and emit zeros
 #pragma unroll
                     for (int e = 0; e < 8; ++e) {
                         const double2 ab = cab[sub * 8 + e];

@@ -47,6 +47,11 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t by
                  : "memory");
 }
 
+// Suspend-time hint of one try_wait (ns): the waiting thread sleeps in hardware until the
+// phase completes or the hint expires, instead of spinning on the issue slots that the
+// warps sharing its scheduler need.
+constexpr uint32_t kSuspendNs = 200000u;
+
 // Wait for the phase with parity `parity` to complete.  Returns false once kWaitNs of
 // global time have passed without completion.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
@@ -57,17 +62,15 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
             "selp.u32 %0, 1, 0, p;\n\t}"
             : "=r"(done)
-            : "r"(addr), "r"(parity)
+            : "r"(addr), "r"(parity), "r"(kSuspendNs)
             : "memory");
         if (done) return true;
-        if ((it & 255) == 0) {
-            const uint64_t now = global_ns();
-            if (it == 0) start = now;
-            else if (now - start > kWaitNs) return false;
-        }
+        const uint64_t now = global_ns();
+        if (it == 0) start = now;
+        else if (now - start > kWaitNs) return false;
     }
 }
 
