@@ -6,15 +6,18 @@ from C_TT = 1e3/(l+10)^2, C_EE = 0.05 C_TT, C_BB = 0.005 C_TT, C_TE = 0.3 sqrt(C
 binary mask |b| > 20 deg about a pole tilted to (theta, phi) = (30, 45) deg with 2000
 point-source holes of 5 arcmin (seeded), C1-apodised at 1 deg; n_iter = 3; bands of 16.
 
-One step = one Monte-Carlo simulation through the estimator with a shared, precomputed
-workspace: NmtField(T) and NmtField(Q, U) (map2alm with 3 Jacobi iterations each),
-compute_coupled_cell for TT, TE/TB and EE/EB/BE/BB, and decouple_cell with the three
-binned coupling matrices.  `value` is sims/s with the maps resident on the device;
-`e2e` is the same through the public API from pinned host maps (host->device copy of
-the maps and device->host copy of the bandpowers inside the timed region).  Inputs
-(400 MB per map) are larger than the 126 MB L2, so no explicit flush is needed.
+One step = one batch of Monte-Carlo simulations (32 by default) through the estimator
+with shared, precomputed workspaces: fields_from_maps for T and for (Q, U) (map2alm with
+3 Jacobi iterations, batched on the tensor cores), compute_coupled_cells for TT, TE/TB
+and EE/EB/BE/BB, and decouple_cells with the three binned coupling matrices.  `value` is
+sims/s with the maps resident on the device; `e2e` is the same through the public API
+from pinned host maps (host->device copy of the maps and device->host copy of the
+bandpowers inside the timed region).  Inputs (400 MB per map) are larger than the
+126 MB L2, so no explicit flush is needed.  The plain FP64 GPU path (one simulation at
+a time) is timed beside it, and the mixed/FP64 bandpowers of the same simulation are
+compared.
 
-Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--batch S] [--impl reference]
 Under torchrun each rank runs independent simulations (replicas, no collective on the
 data path); value is the total over ranks divided by the max-over-ranks device time.
 """
@@ -34,6 +37,7 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 METRIC = "MASTER sims/s, Nside 2048 TQU (shared workspace, n_iter=3), mixed precision"
+os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "expandable_segments:True")
 
 
 def parse():
@@ -44,6 +48,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--nside", type=int, default=2048)
     p.add_argument("--nlb", type=int, default=16)
+    p.add_argument("--batch", type=int, default=32)
     p.add_argument("--fp64-steps", type=int, default=1)
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -95,26 +100,51 @@ def make_mask(nside, device, seed=4, nholes=2000, hole_arcmin=5.0, cut_deg=20.0,
 
 
 def make_sims(nside, nsims, seed, device):
-    """TQU maps of `nsims` Gaussian simulations (float64 on the device)."""
+    """T maps (nsims, npix) and Q, U maps (nsims, 2, npix), float64 on the device, of
+    `nsims` seeded Gaussian TQU simulations of the configuration spectra.  The alms are
+    drawn on the GPU (unit complex normals, real at m = 0, mixed through the Cholesky
+    factor of the (T, E, B) covariance at each l) and synthesised with the batched
+    tensor-core alm2map."""
     import torch
 
-    from gmaster_b200 import sht
-    from gmaster_b200.utils import gaussian_alm
+    from gmaster_b200 import sht_tc
+    from gmaster_b200.utils import NmtAlmInfo
 
     lmax = 3 * nside - 1
     tt, ee, bb, te = config_spectra(lmax)
-    cov = np.zeros((3, 3, lmax + 1))
-    cov[0, 0], cov[1, 1], cov[2, 2] = tt, ee, bb
-    cov[0, 1] = cov[1, 0] = te
-    sims = []
-    for i in range(nsims):
-        alm = gaussian_alm(cov, lmax, np.random.default_rng(seed + i))
-        a = torch.from_numpy(alm).to(device)
-        t = sht.alm2map_device(a[:1].contiguous(), 0, nside, lmax, "fp64")
-        qu = sht.alm2map_device(a[1:].contiguous(), 2, nside, lmax, "fp64")
-        sims.append((t, qu))
-        del a
-    return sims
+    l00 = np.sqrt(tt)
+    l10 = np.divide(te, l00, out=np.zeros_like(te), where=l00 > 0)
+    l11 = np.sqrt(np.maximum(ee - l10 ** 2, 0.0))
+    l22 = np.sqrt(bb)
+    ell, order = NmtAlmInfo(lmax).ell_m()
+    ell_t = torch.from_numpy(ell).to(device)
+    m0 = torch.from_numpy(order == 0).to(device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    dev_f = lambda a: torch.from_numpy(a).to(device)[ell_t]
+
+    def unit():
+        re = torch.randn((nsims, ell.shape[0]), generator=gen, device=device, dtype=torch.float64)
+        im = torch.randn((nsims, ell.shape[0]), generator=gen, device=device, dtype=torch.float64)
+        re[:, m0] *= np.sqrt(2.0)
+        im[:, m0] = 0.0
+        return torch.complex(re, im) / np.sqrt(2.0)
+
+    step0, step2 = sht_tc.MAX_MAPS_SPIN0, sht_tc.MAX_FIELDS_SPIN2
+    z0 = unit()
+    a_t = z0 * dev_f(l00)
+    t = torch.cat([sht_tc.alm2map_tc(a_t[i:i + step0], 0, nside, lmax) for i in range(0, nsims, step0)])
+    del a_t
+    a_e = z0 * dev_f(l10)
+    del z0
+    a_e += unit() * dev_f(l11)
+    a_b = unit() * dev_f(l22)
+    eb = torch.stack([a_e, a_b], dim=1)                       # (nsims, 2, nelem)
+    del a_e, a_b
+    qu = torch.cat([sht_tc.alm2map_tc(eb[i:i + step2].reshape(-1, eb.shape[2]), 2, nside, lmax)
+                    for i in range(0, nsims, step2)])
+    del eb
+    return t.contiguous(), qu.reshape(nsims, 2, -1).contiguous()
 
 
 # ----------------------------------------------------------------------------- estimator
@@ -142,6 +172,17 @@ def estimator_step(mask, t, qu, ws, precision):
     return (ws["00"].decouple_cell(nmt.compute_coupled_cell(ft, ft)),
             ws["02"].decouple_cell(nmt.compute_coupled_cell(ft, fp)),
             ws["22"].decouple_cell(nmt.compute_coupled_cell(fp, fp)))
+
+
+def batch_step(mask, t, qu, ws, precision="mixed"):
+    """A batch of simulations through the Monte-Carlo batch API (shared workspaces)."""
+    import gmaster_b200 as nmt
+
+    ft = nmt.fields_from_maps(mask, t, spin=0, n_iter=3, precision=precision)
+    fp = nmt.fields_from_maps(mask, qu, spin=2, n_iter=3, precision=precision)
+    return (nmt.decouple_cells(ws["00"], nmt.compute_coupled_cells(ft, ft)),
+            nmt.decouple_cells(ws["02"], nmt.compute_coupled_cells(ft, fp)),
+            nmt.decouple_cells(ws["22"], nmt.compute_coupled_cells(fp, fp)))
 
 
 def full_estimator(mask, t, qu, nside, nlb, precision):
@@ -292,7 +333,6 @@ def main():
     import torch
     import torch.distributed as dist
 
-    import gmaster_b200 as nmt
     from gmaster_b200 import _lib, sht
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -305,20 +345,19 @@ def main():
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=dev)
-    nside, nlb = args.nside, args.nlb
+    nside, nlb, S = args.nside, args.nlb, args.batch
     lmax = 3 * nside - 1
     mask = make_mask(nside, dev)
-    sims = make_sims(nside, 2, 1000 + 10 * rank, dev)
-    host_sims = [(t.cpu().pin_memory(), qu.cpu().pin_memory()) for t, qu in sims]
+    t_all, qu_all = make_sims(nside, S, 1000 + 7919 * rank, dev)
     torch.cuda.synchronize()
 
-    # full estimator from scratch (seconds per spectrum), after one untimed warm-up
+    # full estimator from scratch for one simulation (seconds per spectrum)
     s_per_spec = {}
     for prec in ("mixed", "fp64"):
-        full_estimator(mask, sims[0][0], sims[0][1], nside, nlb, prec)
+        full_estimator(mask, t_all[:1], qu_all[0], nside, nlb, prec)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        full_estimator(mask, sims[0][0], sims[0][1], nside, nlb, prec)
+        full_estimator(mask, t_all[:1], qu_all[0], nside, nlb, prec)
         torch.cuda.synchronize()
         s_per_spec[prec] = time.perf_counter() - t0
 
@@ -344,61 +383,42 @@ def main():
         barrier()
         ms = start.elapsed_time(end)
         if world > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+            tt = torch.tensor([ms], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = float(tt.item())
         return ms
 
-    # device-resident value (mixed), with Legendre kernel events and clocks
-    sampler = ClockSampler(local)
-    calls0 = dict(_lib.CALLS)
-    sht.TIMER = []
-
-    def dev_step(i):
-        t, qu = sims[i % len(sims)]
-        estimator_step(mask, t, qu, ws_mixed, "mixed")
-
+    # device-resident value (mixed, batched), with Legendre kernel events and clocks
     for i in range(args.warmup):
-        dev_step(i)
-    sht.TIMER.clear()
+        batch_step(mask, t_all, qu_all, ws_mixed)
+    sampler = ClockSampler(local)
+    sht.TIMER = []
     calls0 = dict(_lib.CALLS)
     sampler.start()
-    ms = timed_loop(dev_step, 0, args.steps)
+    ms = timed_loop(lambda i: batch_step(mask, t_all, qu_all, ws_mixed), 0, args.steps)
     clocks = sampler.stop()
     launches = sum(_lib.CALLS.get(k, 0) - calls0.get(k, 0) for k in _lib.CALLS)
     events = list(sht.TIMER)
     sht.TIMER = None
     torch.cuda.synchronize()
-    ktime = {}
-    kflops = {}
+    ktime, kflops, kcount = {}, {}, {}
     for kind, a, b, fl in events:
         ktime[kind] = ktime.get(kind, 0.0) + a.elapsed_time(b)
         kflops[kind] = kflops.get(kind, 0.0) + fl
+        kcount[kind] = kcount.get(kind, 0) + 1
     leg_ms = sum(ktime.values())
     leg_flops = sum(kflops.values())
     dominant = max(ktime, key=ktime.get)
-    n_dom = sum(1 for e in events if e[0] == dominant)
-    value = world * args.steps / (ms / 1e3)
+    value = world * args.steps * S / (ms / 1e3)
+    mixed_bp = [o[0].cpu().numpy() for o in batch_step(mask, t_all, qu_all, ws_mixed)]
 
-    # e2e through the public API from pinned host memory
-    h2d = sum(x.numel() * x.element_size() for x in host_sims[0])
-
-    def e2e_step(i):
-        t, qu = host_sims[i % len(host_sims)]
-        out = estimator_step(mask, t, qu, ws_mixed, "mixed")
-        for o in out:
-            o.cpu()
-
-    ms_e2e = timed_loop(e2e_step, 1, args.steps)
-    d2h = sum(o.numel() * 8 for o in estimator_step(mask, *sims[0], ws_mixed, "mixed"))
-    value_e2e = world * args.steps / (ms_e2e / 1e3)
-
-    # FP64 comparison and bandpower agreement on the same simulation
-    ms64 = timed_loop(lambda i: estimator_step(mask, *sims[i % 2], ws_fp64, "fp64"), 1,
+    # plain FP64 GPU path, one simulation at a time, and the unbatched mixed path
+    t0_dev, qu0_dev = t_all[:1].clone(), qu_all[0].clone()
+    ms64 = timed_loop(lambda i: estimator_step(mask, t0_dev, qu0_dev, ws_fp64, "fp64"), 1,
                       args.fp64_steps)
     value64 = world * args.fp64_steps / (ms64 / 1e3)
-    mixed_bp = [o.cpu().numpy() for o in estimator_step(mask, *sims[0], ws_mixed, "mixed")]
-    fp64_bp = [o.cpu().numpy() for o in estimator_step(mask, *sims[0], ws_fp64, "fp64")]
+    fp64_bp = [o.cpu().numpy() for o in estimator_step(mask, t0_dev, qu0_dev, ws_fp64, "fp64")]
+    ms1 = timed_loop(lambda i: estimator_step(mask, t0_dev, qu0_dev, ws_mixed, "mixed"), 1, 1)
     errs = {}
     for name, a, b in zip(("00", "02", "22"), mixed_bp, fp64_bp):
         scale = np.max(np.abs(b), axis=1, keepdims=True)
@@ -407,44 +427,72 @@ def main():
             (mixed_bp[2][3], fp64_bp[2][3])]
     rel_auto = float(max(np.max(np.abs(a - b) / np.abs(b)) for a, b in auto))
 
+    # e2e through the public API from pinned host memory (device copies released first)
+    t_host = t_all.cpu()
+    qu_host = qu_all.cpu()
+    del t_all, qu_all
+    torch.cuda.empty_cache()
+    try:
+        t_host, qu_host = t_host.pin_memory(), qu_host.pin_memory()
+        pinned = True
+    except RuntimeError:
+        pinned = False
+    h2d = t_host.numel() * 8 + qu_host.numel() * 8
+    d2h = [0]
+
+    def e2e_step(i):
+        out = batch_step(mask, t_host, qu_host, ws_mixed)
+        d2h[0] = sum(o.numel() * 8 for group in out for o in group)
+        for group in out:
+            for o in group:
+                o.cpu()
+
+    ms_e2e = timed_loop(e2e_step, 1, args.steps)
+    value_e2e = world * args.steps * S / (ms_e2e / 1e3)
+
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
         return
-    import json as _json
-
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
-            peaks = _json.load(fh)
+            peaks = json.load(fh)
     except OSError:
         pass
     peak = peaks.get("bf16_tflops", 1590.0)
+    dom_avg_ms = ktime[dominant] / kcount[dominant]
     dom_tflops = kflops[dominant] / (ktime[dominant] / 1e3) / 1e12
     line = {
         "metric": METRIC, "value": value, "unit": "sims/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 contraction, f64 recurrence/accumulation", "data": "synthetic",
+        "dtype": "bf16x3 tensor-core contraction (f32 accumulate), f64 recurrence/accumulation",
+        "data": "synthetic (seeded Gaussian TQU sims and analytic mask of the Nside 2048 recipe)",
         "config": {
-            "workload": f"Nside {nside} TQU simulation through NmtField x2, compute_coupled_cell x3, "
-                        f"decouple_cell x3 (shared workspaces), n_iter=3, nlb={nlb}",
-            "nside": nside, "lmax": lmax, "nlb": nlb, "sims_per_step": 1,
+            "workload": f"batch of {S} Nside {nside} TQU simulations through fields_from_maps x2, "
+                        f"compute_coupled_cells x3, decouple_cells x3 (shared workspaces), "
+                        f"n_iter=3, nlb={nlb}",
+            "nside": nside, "lmax": lmax, "nlb": nlb, "sims_per_step": S,
             "l2_flush": "inputs (400 MB maps) larger than L2", "parallelism": f"replicas{world}",
         },
         "e2e": {"value": value_e2e, "unit": "sims/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h)},
+                "d2h_bytes_per_step": int(d2h[0]), "pinned": pinned},
         "roofline": {
             "bound": "tensor", "kernel": dominant,
             "achieved": dom_tflops, "peak": peak, "unit": "TFLOP/s",
             "frac": dom_tflops / peak, "traffic": None,
-            "note": "algorithmic flops per launch (4 per complex MAC) / CUDA-event launch time; "
-                    "peak = measured bf16 (MEASURED_PEAKS.json)",
-            "launches": n_dom, "avg_ms": ktime[dominant] / n_dom,
+            "note": "algorithmic flops per launch (one complex MAC = 4 flops per (l, m, lane) and "
+                    "map; the bf16x3 split issues 3x these on the tensor pipe) / CUDA-event time "
+                    "of the launch; peak = measured bf16 dense (MEASURED_PEAKS.json)",
+            "launches": kcount[dominant], "avg_ms": dom_avg_ms,
+            "tensor_pipe_tflops_issued": 3 * dom_tflops,
         },
         "legendre_share_of_step": leg_ms / ms,
         "legendre_tflops": leg_flops / (leg_ms / 1e3) / 1e12,
-        "fp64": {"value": value64, "unit": "sims/s", "ms_per_step": ms64 / args.fp64_steps},
+        "fp64": {"value": value64, "unit": "sims/s", "ms_per_sim": ms64 / args.fp64_steps,
+                 "path": "plain FP64 GPU estimator, one simulation at a time"},
+        "mixed_unbatched": {"value": world * 1e3 / ms1, "unit": "sims/s", "ms_per_sim": ms1},
         "speedup_mixed_vs_fp64": value / value64,
         "s_per_spectrum": s_per_spec,
         "bandpower_err_mixed_vs_fp64": {"max_abs_over_scale": errs, "max_rel_auto": rel_auto},

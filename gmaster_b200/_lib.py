@@ -25,7 +25,7 @@ SIGNATURES = {
     "gm_version": ([], ctypes.c_char_p),
     "gm_ring_twiddle_count": ([_c_i64], _c_i64),
     "gm_ring_twiddles": ([_c_i64, _c_vp, _c_vp], _c_int),
-    "gm_ring_analysis": ([_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_int, _c_vp, _c_vp, _c_vp, _c_vp],
+    "gm_ring_analysis": ([_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_int, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
                          _c_int),
     "gm_pack_rhs": ([_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp], _c_int),
     "gm_fold_residual": ([_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
@@ -50,16 +50,16 @@ SIGNATURES = {
     "gm_tc_syn_chunk_offsets": ([_c_i64, _c_int, _c_vp], _c_int),
     "gm_tc_syn_image_bytes": ([_c_i64], _c_i64),
     "gm_tc_coef_table": ([_c_i64, _c_int, _c_vp, _c_vp], _c_int),
-    "gm_tc_pack": ([_c_i64, _c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
+    "gm_tc_pack": ([_c_i64, _c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_vp], _c_int),
     "gm_tc_analysis": ([_c_i64, _c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
                         _c_dbl, _c_vp, _c_i64, _c_vp, _c_vp], _c_int),
     "gm_tc_analysis_noalloc": ([_c_i64, _c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp,
                                 _c_vp, _c_dbl, _c_i64, _c_vp, _c_vp], _c_int),
-    "gm_tc_prep_syn": ([_c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_i64, _c_vp], _c_int),
+    "gm_tc_prep_syn": ([_c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_i64, _c_dbl, _c_vp], _c_int),
     "gm_tc_synthesis": ([_c_i64, _c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
-                         _c_vp, _c_vp, _c_vp], _c_int),
-    "gm_tc_fold": ([_c_i64, _c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
-                   _c_int),
+                         _c_vp, _c_dbl, _c_vp, _c_vp], _c_int),
+    "gm_tc_fold": ([_c_i64, _c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl,
+                    _c_vp], _c_int),
     "gm_tc_synd_to_syn": ([_c_i64, _c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
     "gm_tc_alm_layout": ([_c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_int, _c_vp], _c_int),
     "gm_tc_selftest": ([_c_i64, _c_i64, _c_int, _c_int, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),

@@ -1,0 +1,120 @@
+"""Monte-Carlo batches: many simulations that share one mask and one workspace.
+
+A NaMaster-style Monte-Carlo loop builds one ``NmtField`` per simulated map and decouples
+each spectrum with the same workspace (the reference does exactly this, one field at a
+time: gmaster/field.py:78-98, gmaster/workspaces.py:2106-2147).  The helpers here run
+that loop for a whole batch at once:
+
+* ``fields_from_maps`` builds the (lite) fields of a batch.  In mixed precision the
+  spherical-harmonic analyses, ``n_iter`` Jacobi iterations included, run as batched
+  tensor-core transforms: up to 32 spin-0 maps or 32 spin-2 (Q, U) pairs share every
+  generated Legendre row.  In FP64 each field goes through the FP64 transform.
+* ``compute_coupled_cells`` returns the coupled spectra of field pairs.
+* ``decouple_cells`` bins and decouples many spectra with one LU solve of many
+  right-hand sides.
+"""
+
+import torch
+
+from . import sht, sht_tc
+from ._config import get_precision, nmt_params
+from .field import NmtField
+from .utils import as_device
+from .workspaces import compute_coupled_cell
+
+
+def fields_from_maps(mask, maps, *, spin=None, n_iter=None, beam=None, lmax=None,
+                     masked_on_input=False, precision=None):
+    """Lite fields of a batch of simulations sharing one mask.
+
+    ``maps`` is (nsims, npix) or (nsims, 1, npix) for spin 0 and (nsims, 2, npix) for
+    spin 2 (Q, U), float64 on the host or the device.  Returns a list of ``nsims``
+    ``NmtField`` objects whose alms equal those of ``NmtField(mask, maps[i], ...)``
+    up to the precision of the chosen transform.
+    """
+    precision = precision or get_precision()
+    n_iter = nmt_params.n_iter_default if n_iter is None else int(n_iter)
+    mask_t = as_device(mask, torch.float64)
+    maps_t = as_device(maps, torch.float64)
+    if maps_t.ndim == 2:
+        maps_t = maps_t[:, None, :]
+    if maps_t.ndim != 3 or maps_t.shape[1] not in (1, 2):
+        raise ValueError("maps must be (nsims, npix), (nsims, 1, npix) or (nsims, 2, npix)")
+    if maps_t.shape[2] != mask_t.shape[0]:
+        raise ValueError("Maps and mask have different sizes")
+    nmaps = maps_t.shape[1]
+    if spin is None:
+        spin = 0 if nmaps == 1 else 2
+    if (spin == 0) != (nmaps == 1):
+        raise ValueError("Spin-zero fields are associated with a single map")
+    if spin not in (0, 2):
+        raise NotImplementedError("only spin-0 and spin-2 fields are implemented")
+
+    # one template field carries the geometry, lmax and beam checks of NmtField
+    proto = NmtField(mask_t, None, spin=spin, n_iter=n_iter, beam=beam, lmax=lmax, lite=True,
+                     precision=precision)
+    nside, lm = proto.minfo.nside, proto.ainfo.lmax
+    nsims = maps_t.shape[0]
+    per_launch = sht_tc.MAX_MAPS_SPIN0 if spin == 0 else sht_tc.MAX_FIELDS_SPIN2
+    alms = []
+    for s0 in range(0, nsims, per_launch):
+        chunk = maps_t[s0:s0 + per_launch]
+        flat = chunk.reshape(-1, chunk.shape[2]).contiguous()
+        if precision == "fp64":
+            if not masked_on_input:
+                flat = flat * mask_t[None, :]
+            a = torch.cat([sht.map2alm_device(flat[i * nmaps:(i + 1) * nmaps], spin, nside, lm,
+                                              n_iter, "fp64") for i in range(chunk.shape[0])])
+        else:
+            # the ring stage multiplies by the mask as it reads the maps: no masked copy
+            a = sht_tc.map2alm_tc(flat, spin, nside, lm, n_iter,
+                                  mask=None if masked_on_input else mask_t)
+        del flat, chunk
+        alms.append(a.reshape(-1, nmaps, a.shape[1]))
+    alms = torch.cat(alms)
+    fields = []
+    for i in range(nsims):
+        f = NmtField(mask_t, None, spin=spin, n_iter=n_iter, beam=beam, lmax=lmax, lite=True,
+                     precision=precision)
+        f.alm = alms[i]
+        fields.append(f)
+    return fields
+
+
+def compute_coupled_cells(fields1, fields2):
+    """Coupled pseudo-C_ell of each pair (fields1[i], fields2[i])."""
+    if len(fields1) != len(fields2):
+        raise ValueError("the two field lists must have the same length")
+    return [compute_coupled_cell(a, b) for a, b in zip(fields1, fields2)]
+
+
+def decouple_cells(workspace, cls, cl_bias=None, cl_noise=None):
+    """Bandpowers of many coupled spectra (each (ncls, lmax+1)) with one LU solve.
+
+    Equivalent to ``[workspace.decouple_cell(c, cl_bias, cl_noise) for c in cls]``.
+    """
+    w = workspace
+    if len(cls) == 0:
+        return []
+    stack = []
+    for c in cls:
+        c = as_device(c, torch.float64)
+        if c.ndim != 2 or c.shape[0] != w.ncls or c.shape[1] < w.lmax + 1:
+            raise ValueError(f"Input power spectrum has wrong shape. Expected "
+                             f"({w.ncls}, {w.lmax + 1}), but got {tuple(c.shape)}")
+        c = c[:, : w.lmax + 1]
+        for name, bias in (("bias", cl_bias), ("noise", cl_noise)):
+            if bias is not None:
+                bias = as_device(bias, torch.float64)
+                if bias.ndim != 2 or bias.shape[0] != w.ncls or bias.shape[1] < w.lmax + 1:
+                    raise ValueError(f"Input {name} power spectrum has wrong shape")
+                c = c - bias[:, : w.lmax + 1]
+        stack.append(c)
+    allcl = torch.cat(stack).contiguous()                      # (nsims ncls, L)
+    binned = w.bins.bin_cell(allcl)                            # (nsims ncls, nb)
+    nb = binned.shape[1]
+    rhs = binned.reshape(len(cls), w.ncls, nb).permute(2, 1, 0).reshape(nb * w.ncls, len(cls))
+    w._lu.check()
+    sol = w._lu.solve(rhs.contiguous())                        # (nb ncls, nsims)
+    out = sol.reshape(nb, w.ncls, len(cls)).permute(2, 1, 0)
+    return [out[i] for i in range(len(cls))]

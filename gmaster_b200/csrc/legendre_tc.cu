@@ -2,17 +2,20 @@
 //
 // The rows lambda^{s'}_lm(theta) = sqrt((2l+1)/4pi) d^l_{m,s'}(theta) are generated on the
 // fly by the FP64 three-term recurrence in l (one lane = one northern ring per thread),
-// rounded to FP32 and split into bf16 hi + lo, and written straight into the shared-memory
+// rounded to FP32 and split into f16 hi + lo, and written straight into the shared-memory
 // operand of tcgen05.mma.  The other operand is a batch of right-hand sides (up to 128
 // real rows: maps x re/im x hemisphere), delivered by the bulk-copy (TMA) engine as a
-// pre-split, pre-swizzled image.  Each product runs as three bf16 MMAs
-// (hi*hi + hi*lo + lo*hi) accumulating in FP32 in tensor memory; the epilogue applies the
-// hemisphere parity and accumulates in FP64.
+// pre-split, pre-swizzled, power-of-two-scaled image.  Each product runs as three f16 MMAs
+// (hi*hi + hi*lo + lo*hi) accumulating in FP32 in tensor memory, hi*hi and the two cross
+// products in separate accumulators (the tensor-core accumulation truncates, so its bias
+// grows with the chain of MMAs into one accumulator); the epilogue adds the two, applies
+// the hemisphere parity and accumulates in FP64.
 //
 // Analysis (map -> alm): D[row, l] = sum_lanes rhs[row, lane] lambda_l(lane).  One
-// persistent CTA per order m at a time walks l in superblocks of 512 (D in 512 TMEM
-// columns) and, inside a superblock, the lanes in groups of 128 (K); the recurrence state
-// of every lane is carried across superblocks in a caller-provided scratch buffer.
+// persistent CTA per order m at a time walks l in superblocks of 256 (two 256-column
+// accumulators fill the 512 TMEM columns) and, inside a superblock, the lanes in groups
+// of 128 (K); the recurrence state of every lane is carried across superblocks in a
+// caller-provided scratch buffer.
 //
 // Synthesis (alm -> ring coefficients): D[row, lane] = sum_l almT[row, l] lambda_l(lane).
 // One CTA per (order m, tile of 256 lanes) walks l in chunks of 64 (K).
@@ -30,7 +33,8 @@ namespace ltc {
 
 constexpr int kGen = 128;              // generator threads (4 warps)
 constexpr int kThreads = kGen + 32;    // + one warp for the producer / MMA issuer
-constexpr int kSB = 512;               // analysis superblock (TMEM columns)
+constexpr int kSB = 256;               // analysis superblock (l per D accumulator)
+constexpr int kTmemCols = 512;         // TMEM columns: the hi*hi and the cross accumulators
 constexpr int kNB = 64;                // analysis l-tile (MMA N)
 constexpr int kKC = 128;               // analysis lanes per group (MMA K per group)
 constexpr int kLT = 256;               // synthesis lanes per CTA (MMA N)
@@ -101,12 +105,16 @@ __device__ __forceinline__ Coef load_coef(const double *__restrict__ tab, int64_
     return c;
 }
 
+// Operands are f16 hi/lo pairs (22 significant bits; the products hi*hi + hi*lo + lo*hi
+// run as three kind::f16 MMAs).  The generated rows are bounded by sqrt((2l+1)/4pi); the
+// right-hand-side and alm images are scaled by a power of two so their largest entry sits
+// near 2^13.
 __device__ __forceinline__ void pack8(const float (&v)[8], uint4 &hi, uint4 &lo)
 {
-    tc::split_bf16x2(v[0], v[1], hi.x, lo.x);
-    tc::split_bf16x2(v[2], v[3], hi.y, lo.y);
-    tc::split_bf16x2(v[4], v[5], hi.z, lo.z);
-    tc::split_bf16x2(v[6], v[7], hi.w, lo.w);
+    tc::split_f16x2(v[0], v[1], hi.x, lo.x);
+    tc::split_f16x2(v[2], v[3], hi.y, lo.y);
+    tc::split_f16x2(v[4], v[5], hi.z, lo.z);
+    tc::split_f16x2(v[6], v[7], hi.w, lo.w);
 }
 
 __device__ __forceinline__ void sts128(uint32_t addr, const uint4 &v)
@@ -190,7 +198,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
         tc::fence_mbar_init();
     }
     if (warp == 4) {
-        tc::tmem_alloc(&sh.tmem, kSB);
+        tc::tmem_alloc(&sh.tmem, kTmemCols);
         tc::tmem_relinquish();
     }
     tc::tc_fence_before();
@@ -202,7 +210,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
     if (warp == 4) {
         // ------------------------------------------------ producer + MMA issuer
         if (lane == 0) {
-            const uint32_t idesc = tc::idesc_f16(128, kNB, 1, 1, 1);
+            const uint32_t idesc = tc::idesc_f16(128, kNB, 0, 1, 1);
             uint32_t j = 0, u = 0, q = 0;   // job, B-tile and superblock counters
             // job list: (slot i -> m, superblock s, group g)
             auto job_m = [&](int64_t i) { return snake_m(i, c, G); };
@@ -239,16 +247,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
                     if (!wait_or_abort(&sh.b_full[st], (u >> 1) & 1, abort, err)) break;
                     tc::tc_fence_after();
                     const uint32_t b0 = tc::smem_u32(sB + st * 2 * kBTileA);
-                    const uint32_t d = tmem + t * kNB;
+                    // hi*hi into D_hh (columns [0, kSB)), hi*lo + lo*hi into D_x
+                    // (columns [kSB, 2 kSB)): the tensor-core accumulation rounds toward
+                    // zero, so its relative bias grows with the number of MMAs chained into
+                    // one accumulator; D_x is 2^-11 smaller and its bias is negligible.
+                    const uint32_t dh = tmem + t * kNB, dx = tmem + kSB + t * kNB;
+                    const uint32_t acc = g > 0 ? 1u : 0u;
 #pragma unroll
                     for (int ks = 0; ks < kKC / 16; ++ks) {
                         const uint64_t ah = tc::desc_sw128_mn(a0 + ks * 4096, 1024, 2048);
                         const uint64_t al = tc::desc_sw128_mn(a0 + kAImg + ks * 4096, 1024, 2048);
                         const uint64_t bh = tc::desc_sw128_mn(b0 + ks * 2048, 1024, 1024);
                         const uint64_t bl = tc::desc_sw128_mn(b0 + kBTileA + ks * 2048, 1024, 1024);
-                        tc::mma_f16(d, ah, bh, idesc, (g > 0 || ks > 0) ? 1u : 0u);
-                        tc::mma_f16(d, ah, bl, idesc, 1u);
-                        tc::mma_f16(d, al, bh, idesc, 1u);
+                        tc::mma_f16(dh, ah, bh, idesc, (acc || ks > 0) ? 1u : 0u);
+                        tc::mma_f16(dx, ah, bl, idesc, (acc || ks > 0) ? 1u : 0u);
+                        tc::mma_f16(dx, al, bh, idesc, 1u);
                     }
                     tc::mma_commit(&sh.b_free[st]);
                 }
@@ -354,15 +367,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
                 const int orow = row < p.H ? p.o0 + row : p.o1 + (row - p.H);
                 const bool parity_row = row >= p.H;
                 for (int cb = 0; cb < kSB; cb += 16) {
-                    uint32_t r[16];
-                    tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, r);
+                    uint32_t r[16], rx[16];
+                    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb;
+                    tc::tmem_ld16(trow, r);
+                    tc::tmem_ld16(trow + kSB, rx);
                     tc::tmem_ld_wait();
                     if (rvalid) {
 #pragma unroll
                         for (int e = 0; e < 16; ++e) {
                             const int64_t l = lb + cb + e;
                             if (l < L) {
-                                double val = (double)__uint_as_float(r[e]) * p.scale;
+                                double val = ((double)__uint_as_float(r[e]) + (double)__uint_as_float(rx[e])) *
+                                             p.scale;
                                 if (parity_row && ((l + m) & 1)) val = -val;
                                 atomicAdd(alm_i + (mb + l) * p.NR + orow, val);
                             }
@@ -378,7 +394,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
     }
     tc::tc_fence_before();
     __syncthreads();
-    if (warp == 4) tc::tmem_dealloc(tmem, kSB);
+    if (warp == 4) tc::tmem_dealloc(tmem, kTmemCols);
 }
 
 // ------------------------------------------------------------------------------- synthesis
@@ -425,7 +441,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t 
         tc::fence_mbar_init();
     }
     if (warp == 4) {
-        tc::tmem_alloc(&sh.tmem, kLT);
+        tc::tmem_alloc(&sh.tmem, kTmemCols);
         tc::tmem_relinquish();
     }
     tc::tc_fence_before();
@@ -437,7 +453,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t 
 
     if (warp == 4) {
         if (lane == 0) {
-            const uint32_t idesc = tc::idesc_f16(128, kLT, 1, 1, 0);
+            const uint32_t idesc = tc::idesc_f16(128, kLT, 0, 1, 0);
             tc::mbar_arrive_expect_tx(&sh.a_full[0], 2 * kSImg);
             tc::bulk_g2s(sA, img, 2 * kSImg, &sh.a_full[0]);
             for (int64_t cc = 0; cc < nch && !*abort; ++cc) {
@@ -460,9 +476,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t 
                     const uint64_t al = tc::desc_sw128_mn(a0 + kSImg + ks * 4096, 1024, 2048);
                     const uint64_t bh = tc::desc_sw128(b0 + ks * 32);
                     const uint64_t bl = tc::desc_sw128(b0 + kBTileS + ks * 32);
+                    // hi*hi into D_hh (columns [0, kLT)), the cross products into D_x
+                    // (columns [kLT, 2 kLT)), as in the analysis
                     tc::mma_f16(tmem, ah, bh, idesc, (cc > 0 || ks > 0) ? 1u : 0u);
-                    tc::mma_f16(tmem, ah, bl, idesc, 1u);
-                    tc::mma_f16(tmem, al, bh, idesc, 1u);
+                    tc::mma_f16(tmem + kLT, ah, bl, idesc, (cc > 0 || ks > 0) ? 1u : 0u);
+                    tc::mma_f16(tmem + kLT, al, bh, idesc, 1u);
                 }
                 tc::mma_commit(&sh.b_free[st]);
                 tc::mma_commit(&sh.a_free[st]);
@@ -561,14 +579,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t 
             tc::tc_fence_after();
             const int row = warp * 32 + lane;
             for (int cb = 0; cb < kLT; cb += 16) {
-                uint32_t r[16];
-                tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, r);
+                uint32_t r[16], rx[16];
+                const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb;
+                tc::tmem_ld16(trow, r);
+                tc::tmem_ld16(trow + kLT, rx);
                 tc::tmem_ld_wait();
                 if (row < R2) {
 #pragma unroll
                     for (int e = 0; e < 16; ++e) {
                         const int64_t jl = tile * kLT + cb + e;
-                        if (jl < p.nlanes) synd[(m * p.nlanes + jl) * R2 + row] = __uint_as_float(r[e]);
+                        if (jl < p.nlanes)
+                            synd[(m * p.nlanes + jl) * R2 + row] =
+                                (__uint_as_float(r[e]) + __uint_as_float(rx[e])) * (float)p.scale;
                     }
                 }
             }
@@ -576,7 +598,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t 
     }
     tc::tc_fence_before();
     __syncthreads();
-    if (warp == 4) tc::tmem_dealloc(tmem, kLT);
+    if (warp == 4) tc::tmem_dealloc(tmem, kTmemCols);
 }
 
 // ------------------------------------------------------------------------------- tables
@@ -628,7 +650,7 @@ __device__ __forceinline__ void put_rows8(uint8_t *img, uint32_t plane_bytes, in
 // [Mt_N | Pt_S], variant -2 rows [Pt_N | Mt_S], with Pt = G_Q + i G_U, Mt = G_Q - i G_U.
 // Writes the 128-row image column (zero rows beyond 2H) for both planes.
 __device__ void write_rhs_column(uint8_t *img, int kk, int spin, int sp, int ncomp, const float2 *gn,
-                                 const float2 *gs)
+                                 const float2 *gs, float scale)
 {
     const int H = spin == 0 ? 2 * ncomp : ncomp;  // spin 2: ncomp = 2F -> H = 2F
     float rowv[8];
@@ -656,7 +678,7 @@ __device__ void write_rhs_column(uint8_t *img, int kk, int spin, int sp, int nco
                     else val = im ? (q.y - u.x) : (q.x + u.y);
                 }
             }
-            rowv[e] = val;
+            rowv[e] = val * scale;
         }
         put_rows8(img, kAImg, r0, kk, rowv);
     }
@@ -666,7 +688,7 @@ __device__ void write_rhs_column(uint8_t *img, int kk, int spin, int sp, int nco
 // rhs_map (L, nlanes, ncomp) of float4 (G_N re, im, G_S re, im) and the analysis images.
 __global__ void k_pack_tc(int64_t nside, int64_t L, int ncomp, int spin,
                           const float2 *__restrict__ spec, float4 *__restrict__ rhs_map,
-                          uint8_t *__restrict__ img_a, uint8_t *__restrict__ img_b)
+                          uint8_t *__restrict__ img_a, uint8_t *__restrict__ img_b, float scale)
 {
     const int64_t nlanes = 2 * nside, nring = 4 * nside - 1, NG = (nlanes + kKC - 1) / kKC;
     const int64_t m = blockIdx.y;
@@ -686,10 +708,10 @@ __global__ void k_pack_tc(int64_t nside, int64_t L, int ncomp, int spin,
     const int64_t g = j / kKC;
     const int kk = (int)(j % kKC);
     uint8_t *ia = img_a + ((m * NG + g) * 2) * (int64_t)kAImg;
-    write_rhs_column(ia, kk, spin, spin == 0 ? 0 : -2, ncomp, gn, gs);
+    write_rhs_column(ia, kk, spin, spin == 0 ? 0 : -2, ncomp, gn, gs, scale);
     if (spin != 0) {
         uint8_t *ib = img_b + ((m * NG + g) * 2) * (int64_t)kAImg;
-        write_rhs_column(ib, kk, spin, +2, ncomp, gn, gs);
+        write_rhs_column(ib, kk, spin, +2, ncomp, gn, gs, scale);
     }
 }
 
@@ -698,7 +720,7 @@ __global__ void k_pack_tc(int64_t nside, int64_t L, int ncomp, int spin,
 // (src row r); variant +2 (lambda-): [-2a | s 2a] (src r < H ? H + r : r - H); s = (-1)^(l+m).
 __global__ void k_prep_syn(int64_t lmax, int spin, int sp, int H, int NR,
                            const double *__restrict__ alm_i, const int64_t *__restrict__ choff,
-                           uint8_t *__restrict__ simg)
+                           uint8_t *__restrict__ simg, double scale)
 {
     const int64_t m = blockIdx.y, L = lmax + 1;
     const int l0min = abs(sp);
@@ -726,7 +748,7 @@ __global__ void k_prep_syn(int64_t lmax, int spin, int sp, int H, int NR,
                 if (spin == 0) src = second ? r - H : r;
                 else if (sp < 0) src = r;
                 else src = second ? r - H : H + r;
-                double a = alm_i[(mb + l) * NR + src];
+                double a = alm_i[(mb + l) * NR + src] * scale;
                 if (second) a *= sgn;
                 val = (float)a;
             }
@@ -752,7 +774,7 @@ __global__ void __launch_bounds__(128) k_fold_tc(int64_t nside, int64_t L, int n
                                                  const float4 *__restrict__ rhs_map,
                                                  const uint8_t *__restrict__ shifted,
                                                  uint8_t *__restrict__ img_a,
-                                                 uint8_t *__restrict__ img_b)
+                                                 uint8_t *__restrict__ img_b, float scale)
 {
     const int64_t j = blockIdx.x;
     const int64_t nlanes = 2 * nside, npix = 12 * nside * nside, NG = (nlanes + kKC - 1) / kKC;
@@ -827,10 +849,10 @@ __global__ void __launch_bounds__(128) k_fold_tc(int64_t nside, int64_t L, int n
                 gs[c] = two ? make_float2(sg * ps[c].x - b.z, sg * ps[c].y - b.w) : make_float2(-b.z, -b.w);
             }
             uint8_t *ia = img_a + ((m * NG + g) * 2) * (int64_t)kAImg;
-            write_rhs_column(ia, kk, spin, spin == 0 ? 0 : -2, ncomp, gn, gs);
+            write_rhs_column(ia, kk, spin, spin == 0 ? 0 : -2, ncomp, gn, gs, scale);
             if (spin != 0) {
                 uint8_t *ib = img_b + ((m * NG + g) * 2) * (int64_t)kAImg;
-                write_rhs_column(ib, kk, spin, +2, ncomp, gn, gs);
+                write_rhs_column(ib, kk, spin, +2, ncomp, gn, gs, scale);
             }
         }
     }
@@ -956,9 +978,9 @@ static int tc_shape_ok(int spin, int64_t ncomp)
 }
 
 extern "C" int gm_tc_pack(int64_t nside, int64_t lmax, int spin, int64_t ncomp, const void *ringspec,
-                          void *rhs_map, void *img_a, void *img_b, void *stream)
+                          void *rhs_map, void *img_a, void *img_b, double img_scale, void *stream)
 {
-    if (nside < 1 || lmax < 0 || !tc_shape_ok(spin, ncomp)) return GM_ERR_BAD_SHAPE;
+    if (nside < 1 || lmax < 0 || !tc_shape_ok(spin, ncomp) || !(img_scale > 0.0)) return GM_ERR_BAD_SHAPE;
     if (!ringspec || !rhs_map || !img_a || (spin && !img_b)) return GM_ERR_BAD_PTR;
     const int64_t NG = gm_tc_lane_groups(nside);
     cudaStream_t s = as_stream(stream);
@@ -970,7 +992,8 @@ extern "C" int gm_tc_pack(int64_t nside, int64_t lmax, int spin, int64_t ncomp, 
     }
     dim3 grid((unsigned)((NG * kKC + 127) / 128), (unsigned)(lmax + 1));
     k_pack_tc<<<grid, 128, 0, s>>>(nside, lmax + 1, (int)ncomp, spin, (const float2 *)ringspec,
-                                   (float4 *)rhs_map, (uint8_t *)img_a, (uint8_t *)img_b);
+                                   (float4 *)rhs_map, (uint8_t *)img_a, (uint8_t *)img_b,
+                                   (float)img_scale);
     return check_launch("gm_tc_pack");
 }
 
@@ -1018,9 +1041,10 @@ extern "C" int gm_tc_analysis(int64_t nside, int64_t lmax, int spin, int sp, int
 }
 
 extern "C" int gm_tc_prep_syn(int64_t lmax, int spin, int sp, int64_t ncomp, const double *alm_i,
-                              const int64_t *choff, void *simg, int64_t simg_bytes, void *stream)
+                              const int64_t *choff, void *simg, int64_t simg_bytes, double alm_scale,
+                              void *stream)
 {
-    if (lmax < 2 || !tc_shape_ok(spin, ncomp)) return GM_ERR_BAD_SHAPE;
+    if (lmax < 2 || !tc_shape_ok(spin, ncomp) || !(alm_scale > 0.0)) return GM_ERR_BAD_SHAPE;
     if (!alm_i || !choff || !simg) return GM_ERR_BAD_PTR;
     const int H = spin == 0 ? (int)(2 * ncomp) : (int)ncomp;
     const int NR = spin == 0 ? H : 2 * H;
@@ -1031,16 +1055,16 @@ extern "C" int gm_tc_prep_syn(int64_t lmax, int spin, int sp, int64_t ncomp, con
         return GM_ERR_LAUNCH;
     }
     k_prep_syn<<<dim3(16, (unsigned)(lmax + 1)), 256, 0, s>>>(lmax, spin, sp, H, NR, alm_i, choff,
-                                                             (uint8_t *)simg);
+                                                             (uint8_t *)simg, alm_scale);
     return check_launch("gm_tc_prep_syn");
 }
 
 extern "C" int gm_tc_synthesis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
                                const double *geom, const double *seeds, const double *coef,
-                               const void *simg, const int64_t *choff, float *synd, int32_t *err,
-                               void *stream)
+                               const void *simg, const int64_t *choff, float *synd, double out_scale,
+                               int32_t *err, void *stream)
 {
-    if (nside < 1 || lmax < 2 || !tc_shape_ok(spin, ncomp)) return GM_ERR_BAD_SHAPE;
+    if (nside < 1 || lmax < 2 || !tc_shape_ok(spin, ncomp) || !(out_scale > 0.0)) return GM_ERR_BAD_SHAPE;
     if ((spin == 0) != (sp == 0) || (spin == 2 && sp != 2 && sp != -2)) return GM_ERR_BAD_SHAPE;
     if (!geom || !seeds || !coef || !simg || !choff || !synd || !err) return GM_ERR_BAD_PTR;
     const size_t smem = 4 * kSImg + 4 * kBTileS + 2 * kKL * (sizeof(double2) + sizeof(double)) + 1024;
@@ -1050,7 +1074,7 @@ extern "C" int gm_tc_synthesis(int64_t nside, int64_t lmax, int spin, int sp, in
         set_error("gm_tc_synthesis attr", e);
         return GM_ERR_LAUNCH;
     }
-    Params p = make_params(nside, lmax, spin, sp, ncomp, geom, seeds, coef, 1.0);
+    Params p = make_params(nside, lmax, spin, sp, ncomp, geom, seeds, coef, out_scale);
     const int R2 = 2 * p.H;
     dim3 grid((unsigned)((p.nlanes + kLT - 1) / kLT), (unsigned)(lmax + 1));
     kern<<<grid, kThreads, smem, as_stream(stream)>>>(p, (const uint8_t *)simg, choff, synd, R2,
@@ -1060,15 +1084,15 @@ extern "C" int gm_tc_synthesis(int64_t nside, int64_t lmax, int spin, int sp, in
 
 extern "C" int gm_tc_fold(int64_t nside, int64_t lmax, int spin, int64_t ncomp, const float *synd_a,
                           const float *synd_b, const void *rhs_map, const uint8_t *shifted,
-                          void *img_a, void *img_b, void *stream)
+                          void *img_a, void *img_b, double img_scale, void *stream)
 {
-    if (nside < 1 || lmax < 2 || !tc_shape_ok(spin, ncomp)) return GM_ERR_BAD_SHAPE;
+    if (nside < 1 || lmax < 2 || !tc_shape_ok(spin, ncomp) || !(img_scale > 0.0)) return GM_ERR_BAD_SHAPE;
     if (!synd_a || (spin && !synd_b) || !rhs_map || !shifted || !img_a || (spin && !img_b))
         return GM_ERR_BAD_PTR;
     const int H = spin == 0 ? (int)(2 * ncomp) : (int)ncomp;
     k_fold_tc<<<(unsigned)(2 * nside), 128, 0, as_stream(stream)>>>(
         nside, lmax + 1, (int)ncomp, spin, synd_a, synd_b, 2 * H, (const float4 *)rhs_map, shifted,
-        (uint8_t *)img_a, (uint8_t *)img_b);
+        (uint8_t *)img_a, (uint8_t *)img_b, (float)img_scale);
     return check_launch("gm_tc_fold");
 }
 

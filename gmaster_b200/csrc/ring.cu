@@ -193,6 +193,7 @@ __device__ T2 *fft_shared(T2 *a, T2 *b, int h, const T2 *__restrict__ tw, int si
 template <typename T, typename Tin>
 __global__ void __launch_bounds__(512) k_ring_analysis(int64_t nside, int64_t L,
                                                        const Tin *__restrict__ maps,
+                                                       const double *__restrict__ mask,
                                                        const void *__restrict__ twall,
                                                        int64_t twcnt,
                                                        const uint8_t *__restrict__ shifted,
@@ -208,11 +209,22 @@ __global__ void __launch_bounds__(512) k_ring_analysis(int64_t nside, int64_t L,
     T2 *B = A + 2 * nside;
     const T2 *tw = TwTable<T2>::get(twall, twcnt) + twiddle_offset(n);
     const Tin *x = maps + c * npix + off;
-    for (int t = threadIdx.x; t < h; t += blockDim.x) {
-        T2 z;
-        z.x = (T)x[2 * t];
-        z.y = (T)x[2 * t + 1];
-        A[t] = z;
+    if (mask) {
+        // masked field: the FP64 product map * mask, rounded once to T
+        const double *w = mask + off;
+        for (int t = threadIdx.x; t < h; t += blockDim.x) {
+            T2 z;
+            z.x = (T)((double)x[2 * t] * w[2 * t]);
+            z.y = (T)((double)x[2 * t + 1] * w[2 * t + 1]);
+            A[t] = z;
+        }
+    } else {
+        for (int t = threadIdx.x; t < h; t += blockDim.x) {
+            T2 z;
+            z.x = (T)x[2 * t];
+            z.y = (T)x[2 * t + 1];
+            A[t] = z;
+        }
     }
     __syncthreads();
     T2 *Z = fft_shared(A, B, h, tw, -1);
@@ -471,8 +483,9 @@ static int set_smem(K kernel, size_t bytes)
 }
 
 extern "C" int gm_ring_analysis(int precision, int64_t nside, int64_t L, int64_t ncomp,
-                                const void *maps, int map_dtype_bytes, const void *tw,
-                                const uint8_t *shifted, void *ringspec, void *stream)
+                                const void *maps, int map_dtype_bytes, const double *mask,
+                                const void *tw, const uint8_t *shifted, void *ringspec,
+                                void *stream)
 {
     if (!ring_shape_ok(precision, nside, L, ncomp)) return GM_ERR_BAD_SHAPE;
     if (!maps || !tw || !shifted || !ringspec) return GM_ERR_BAD_PTR;
@@ -487,21 +500,21 @@ extern "C" int gm_ring_analysis(int precision, int64_t nside, int64_t L, int64_t
         if (map_dtype_bytes == 8) {
             if ((st = set_smem(k_ring_analysis<double, double>, smem))) return st;
             k_ring_analysis<double, double><<<grid, threads, smem, s>>>(
-                nside, L, (const double *)maps, tw, cnt, shifted, (double2 *)ringspec);
+                nside, L, (const double *)maps, mask, tw, cnt, shifted, (double2 *)ringspec);
         } else {
             if ((st = set_smem(k_ring_analysis<double, float>, smem))) return st;
             k_ring_analysis<double, float><<<grid, threads, smem, s>>>(
-                nside, L, (const float *)maps, tw, cnt, shifted, (double2 *)ringspec);
+                nside, L, (const float *)maps, mask, tw, cnt, shifted, (double2 *)ringspec);
         }
     } else if (precision == GM_MIXED) {
         if (map_dtype_bytes == 8) {
             if ((st = set_smem(k_ring_analysis<float, double>, smem))) return st;
             k_ring_analysis<float, double><<<grid, threads, smem, s>>>(
-                nside, L, (const double *)maps, tw, cnt, shifted, (float2 *)ringspec);
+                nside, L, (const double *)maps, mask, tw, cnt, shifted, (float2 *)ringspec);
         } else {
             if ((st = set_smem(k_ring_analysis<float, float>, smem))) return st;
             k_ring_analysis<float, float><<<grid, threads, smem, s>>>(
-                nside, L, (const float *)maps, tw, cnt, shifted, (float2 *)ringspec);
+                nside, L, (const float *)maps, mask, tw, cnt, shifted, (float2 *)ringspec);
         }
     } else {
         return GM_ERR_UNSUPPORTED;

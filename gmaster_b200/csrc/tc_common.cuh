@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <stdint.h>
 
 namespace gm {
@@ -197,6 +198,18 @@ __host__ __device__ __forceinline__ uint32_t sw128_offset(uint32_t R, uint32_t r
     const uint32_t atom = k >> 6, kk = k & 63;
     const uint32_t chunk = (kk >> 3) ^ (r & 7);
     return atom * R * 128u + (r >> 3) * 1024u + (r & 7) * 128u + chunk * 16u + (kk & 7) * 2u;
+}
+
+// Split two floats into f16 hi + f16 lo pairs: hi + lo carries 22 significant bits for
+// magnitudes in [2^-3, 2^15]; below that lo is subnormal and the absolute error is at
+// most 2^-25.  Callers scale their operands by a power of two into that range.
+__device__ __forceinline__ void split_f16x2(float a, float b, uint32_t &hi, uint32_t &lo)
+{
+    __half2 h = __floats2half2_rn(a, b);
+    float2 hf = __half22float2(h);
+    __half2 l = __floats2half2_rn(a - hf.x, b - hf.y);
+    hi = *reinterpret_cast<uint32_t *>(&h);
+    lo = *reinterpret_cast<uint32_t *>(&l);
 }
 
 // Split a float into bf16 hi + bf16 lo (hi + lo carries 16 significant bits).

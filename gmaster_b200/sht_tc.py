@@ -68,6 +68,20 @@ def _rows(spin, ncomp):
     return H, (H if spin == 0 else 2 * H)
 
 
+# Largest operand entry after scaling: 2^13 leaves headroom for the f16 range (65504)
+# in the Jacobi residuals and the spin-2 row combinations.
+_TARGET_LOG2 = 13
+
+
+def pow2_scale(t):
+    """Power of two that brings max |t| to about 2^13 (1.0 for an all-zero tensor)."""
+    lo, hi = torch.aminmax(t)
+    amax = max(abs(float(lo)), abs(float(hi)))
+    if not amax > 0.0 or not np.isfinite(amax):
+        return 1.0
+    return float(2.0 ** (_TARGET_LOG2 - int(np.ceil(np.log2(amax)))))
+
+
 def _check(tp):
     if int(tp.err.item()):
         tp.err.zero_()
@@ -77,21 +91,27 @@ def _check(tp):
 class _Batch:
     """Buffers of one batched transform."""
 
-    def __init__(self, tp, spin, ncomp):
+    def __init__(self, tp, spin, ncomp, images=True):
         p = tp.plan
         self.tp, self.spin, self.ncomp = tp, spin, ncomp
         self.H, self.NR = _rows(spin, ncomp)
-        dev = p.device
-        self.alm_i = torch.zeros((p.nelem, self.NR), dtype=torch.float64, device=dev)
-        self.img = [torch.empty(tp.img_bytes, dtype=torch.uint8, device=dev) for _ in _variants(spin)]
+        self.alm_i = None
+        self.img_scale = 1.0
+        self.img = [torch.empty(tp.img_bytes, dtype=torch.uint8, device=p.device)
+                    for _ in _variants(spin)] if images else []
+
+    def zero_alm(self):
+        p = self.tp.plan
+        self.alm_i = torch.zeros((p.nelem, self.NR), dtype=torch.float64, device=p.device)
 
     def analysis(self, scale):
+        """alm_i += scale * analysis of the images (which carry img_scale)."""
         p, tp = self.tp.plan, self.tp
         for sp, img in zip(_variants(self.spin), self.img):
             _lib.call("gm_tc_analysis", p.nside, p.lmax, self.spin, sp, self.ncomp, _lib.ptr(p.geom),
                       _lib.ptr(p.seeds), _lib.ptr(tp.coef[self.spin]), _lib.ptr(img),
-                      _lib.ptr(self.alm_i), float(scale), _lib.ptr(tp.scratch), tp.nctas,
-                      _lib.ptr(tp.err), _lib.stream_handle(p.device))
+                      _lib.ptr(self.alm_i), float(scale) / self.img_scale, _lib.ptr(tp.scratch),
+                      tp.nctas, _lib.ptr(tp.err), _lib.stream_handle(p.device))
 
     def synthesis(self, synd=None):
         """-> list of synd tensors (L, nlanes, 2H) float32, one per row variant."""
@@ -102,14 +122,15 @@ class _Batch:
         outs = synd if synd is not None else [
             torch.empty((p.L, p.nlanes, 2 * self.H), dtype=torch.float32, device=p.device)
             for _ in _variants(self.spin)]
+        alm_scale = pow2_scale(self.alm_i)
         for sp, out in zip(_variants(self.spin), outs):
             _lib.call("gm_tc_prep_syn", p.lmax, self.spin, sp, self.ncomp, _lib.ptr(self.alm_i),
-                      _lib.ptr(tp.choff[self.spin]), _lib.ptr(simg), simg_bytes,
+                      _lib.ptr(tp.choff[self.spin]), _lib.ptr(simg), simg_bytes, alm_scale,
                       _lib.stream_handle(p.device))
             _lib.call("gm_tc_synthesis", p.nside, p.lmax, self.spin, sp, self.ncomp, _lib.ptr(p.geom),
                       _lib.ptr(p.seeds), _lib.ptr(tp.coef[self.spin]), _lib.ptr(simg),
-                      _lib.ptr(tp.choff[self.spin]), _lib.ptr(out), _lib.ptr(tp.err),
-                      _lib.stream_handle(p.device))
+                      _lib.ptr(tp.choff[self.spin]), _lib.ptr(out), 1.0 / alm_scale,
+                      _lib.ptr(tp.err), _lib.stream_handle(p.device))
         return outs
 
     def to_api(self):
@@ -137,28 +158,40 @@ def _check_batch(spin, ncomp):
         raise NotImplementedError("only spin 0 and spin 2")
 
 
-def map2alm_tc(maps, spin, nside, lmax, n_iter):
+def map2alm_tc(maps, spin, nside, lmax, n_iter, mask=None):
     """Batched analysis: maps (ncomp, npix) float64/float32 CUDA -> (ncomp, nelem) complex128
-    (spin 2: rows E, B per field), with n_iter Jacobi iterations."""
+    (spin 2: rows E, B per field), with n_iter Jacobi iterations.  `mask` (npix,), if
+    given, multiplies every map as the ring stage reads it.
+
+    Device memory: the ring spectra are released before the alm accumulator is made, and
+    the iteration buffers before the final alm layout, so the peak is the right-hand
+    sides, their operand images, the alm accumulator and the synthesis outputs (about
+    106 GB for 64 maps at Nside 2048) besides the caller's maps."""
     ncomp = maps.shape[0]
     _check_batch(spin, ncomp)
     tp = get_tc_plan(nside, lmax, maps.device)
     p = tp.plan
-    spec = sht.ring_analysis(p, maps, _lib.MIXED)
+    spec = sht.ring_analysis(p, maps, _lib.MIXED, mask=mask)
     b = _Batch(tp, spin, ncomp)
+    # the spin-2 rows G_Q -+ i G_U are at most twice the largest ring value
+    b.img_scale = pow2_scale(spec.view(torch.float32)) / (2.0 if spin else 1.0)
     rhs_map = torch.empty((p.L, p.nlanes, ncomp, 4), dtype=torch.float32, device=p.device)
     _lib.call("gm_tc_pack", p.nside, p.lmax, spin, ncomp, _lib.ptr(spec), _lib.ptr(rhs_map),
-              _lib.ptr(b.img[0]), _lib.ptr(b.img[1]) if spin else None, _lib.stream_handle(p.device))
+              _lib.ptr(b.img[0]), _lib.ptr(b.img[1]) if spin else None, b.img_scale,
+              _lib.stream_handle(p.device))
     del spec
+    b.zero_alm()
     sht._timed(f"tc_analysis_s{spin}", p, spin, ncomp, lambda: b.analysis(1.0))
     synd = None
     for _ in range(int(n_iter)):
         synd = _timed_syn(b, synd)
         _lib.call("gm_tc_fold", p.nside, p.lmax, spin, ncomp, _lib.ptr(synd[0]),
                   _lib.ptr(synd[1]) if spin else None, _lib.ptr(rhs_map), _lib.ptr(p.shifted),
-                  _lib.ptr(b.img[0]), _lib.ptr(b.img[1]) if spin else None,
+                  _lib.ptr(b.img[0]), _lib.ptr(b.img[1]) if spin else None, b.img_scale,
                   _lib.stream_handle(p.device))
         sht._timed(f"tc_analysis_s{spin}", p, spin, ncomp, lambda: b.analysis(-1.0))
+    del synd, rhs_map
+    b.img = []
     out = b.to_api()
     _check(tp)
     return out
@@ -176,8 +209,8 @@ def alm2map_tc(alm, spin, nside, lmax):
     _check_batch(spin, ncomp)
     tp = get_tc_plan(nside, lmax, alm.device)
     p = tp.plan
-    b = _Batch(tp, spin, ncomp)
-    b.img = []
+    b = _Batch(tp, spin, ncomp, images=False)
+    b.zero_alm()
     b.from_api(alm.to(torch.complex128))
     synd = b.synthesis()
     syn = torch.empty((p.L, p.nlanes, ncomp, 4), dtype=torch.float32, device=p.device)

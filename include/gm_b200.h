@@ -66,11 +66,14 @@ int gm_ring_twiddles(int64_t nside, void *tw, void *stream);
 /* Forward ring transform of real maps (replaces rings.py:251-299
  * `_forward_ring_fft_positive`, the XLA cuFFT belt FFT + Bluestein caps).
  * maps: (ncomp, npix) with `map_dtype_bytes` 8 (float64) or 4 (float32).
+ * mask: NULL, or (npix) float64 multiplied into every map as it is read (the masking of
+ * gmaster/field.py:219-229 without a masked copy of the maps; the FP64 product is
+ * rounded once, as for a pre-masked map).
  * out ringspec: (ncomp, nring, L) complex128 (GM_FP64) or complex64 (GM_MIXED),
  * including the quadrature weight 4 pi / npix and the phase e^{-i m phi0}. */
 int gm_ring_analysis(int precision, int64_t nside, int64_t L, int64_t ncomp,
-                     const void *maps, int map_dtype_bytes, const void *tw,
-                     const uint8_t *shifted, void *ringspec, void *stream);
+                     const void *maps, int map_dtype_bytes, const double *mask,
+                     const void *tw, const uint8_t *shifted, void *ringspec, void *stream);
 
 /* Hemisphere pack of a ring spectrum into the lane-major Legendre right-hand side
  * (replaces march_v2.py:637-663 `_fold_rhs`).  rhs (L, nlanes, ncomp, 4). */
@@ -170,8 +173,12 @@ int gm_lu_solve(int64_t n, const double *lu, const int32_t *piv, int64_t nrhs,
  * A batch holds up to 128 real right-hand-side rows: spin 0, ncomp <= 32 maps (rows
  * [G_north | G_south] x re/im); spin 2, ncomp = 2F <= 64 (Q, U of F fields; two row
  * variants s' = -2 with rows [P_N | M_S] and s' = +2 with rows [M_N | P_S], P = G_Q + i G_U,
- * M = G_Q - i G_U).  Operand images are bf16 hi/lo planes in the 128-byte-swizzled
- * MN-major layout of gm_tc_selftest.  The interleaved alm alm_i is (nelem, NR) float64
+ * M = G_Q - i G_U).  Operand images are f16 hi/lo planes (22 significant bits; the
+ * products run as three kind::f16 MMAs, hi*hi + hi*lo + lo*hi, accumulating in FP32) in
+ * the 128-byte-swizzled MN-major layout of gm_tc_selftest.  Right-hand-side and alm
+ * images carry a caller-chosen power-of-two scale (img_scale, alm_scale) that puts their
+ * largest entry near 2^13, inside the f16 range; the analysis `scale` and the synthesis
+ * `out_scale` undo it.  The interleaved alm alm_i is (nelem, NR) float64
  * with NR = 2 ncomp (spin 0: map x re/im) or 2 ncomp (spin 2: [a_{+2} | a_{-2}] x re/im). */
 
 /* Lane groups of 128 lanes and analysis image bytes ((lmax+1) x groups x 64 KB). */
@@ -186,9 +193,10 @@ int64_t gm_tc_syn_image_bytes(int64_t nchunks);
 /* Recurrence coefficient table (nelem, 3) float64 for spin 0 or 2. */
 int gm_tc_coef_table(int64_t lmax, int spin, double *tab, void *stream);
 /* Ring spectra (ncomp, nring, L) complex64 -> rhs_map (L, nlanes, ncomp) float4
- * [G_N re, im, G_S re, im] and the analysis images (img_b only for spin 2). */
+ * [G_N re, im, G_S re, im] and the analysis images scaled by img_scale (img_b only for
+ * spin 2). */
 int gm_tc_pack(int64_t nside, int64_t lmax, int spin, int64_t ncomp, const void *ringspec,
-               void *rhs_map, void *img_a, void *img_b, void *stream);
+               void *rhs_map, void *img_a, void *img_b, double img_scale, void *stream);
 /* alm_i += scale * analysis of the rows of `img` for row variant sp (0, -2, +2).
  * scratch: gm_tc_ana_scratch_bytes(nside, nctas); nctas persistent CTAs (one per SM).
  * err (int32) set non-zero if a bounded wait timed out. */
@@ -214,18 +222,21 @@ int gm_tc_analysis_noalloc(int64_t nside, int64_t lmax, int spin, int sp, int64_
                            const void *img, double *alm_i, double scale, int64_t nctas,
                            int32_t *err, void *stream);
 
-/* Synthesis operand images from alm_i for row variant sp (device choff). */
+/* Synthesis operand images from alm_scale * alm_i for row variant sp (device choff). */
 int gm_tc_prep_syn(int64_t lmax, int spin, int sp, int64_t ncomp, const double *alm_i,
-                   const int64_t *choff, void *simg, int64_t simg_bytes, void *stream);
-/* synd (L, nlanes, 2H) float32 = rows of the synthesis for row variant sp. */
+                   const int64_t *choff, void *simg, int64_t simg_bytes, double alm_scale,
+                   void *stream);
+/* synd (L, nlanes, 2H) float32 = out_scale * rows of the synthesis for row variant sp. */
 int gm_tc_synthesis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
                     const double *geom, const double *seeds, const double *coef, const void *simg,
-                    const int64_t *choff, float *synd, int32_t *err, void *stream);
+                    const int64_t *choff, float *synd, double out_scale, int32_t *err,
+                    void *stream);
 /* Ring-fold residual of the batched synthesis minus rhs_map, written as the next
- * analysis images (replaces march_v2.cu:426-493 for the batched path). */
+ * analysis images scaled by img_scale (replaces march_v2.cu:426-493 for the batched
+ * path). */
 int gm_tc_fold(int64_t nside, int64_t lmax, int spin, int64_t ncomp, const float *synd_a,
                const float *synd_b, const void *rhs_map, const uint8_t *shifted, void *img_a,
-               void *img_b, void *stream);
+               void *img_b, double img_scale, void *stream);
 /* Batched synthesis output -> syn layout of gm_ring_synthesis. */
 int gm_tc_synd_to_syn(int64_t nside, int64_t lmax, int spin, int64_t ncomp, const float *synd_a,
                       const float *synd_b, float *syn, void *stream);

@@ -1,0 +1,105 @@
+"""Monte-Carlo batch API: batched fields, spectra and decoupling against the per-field
+API and against the FP64 oracle."""
+
+import numpy as np
+import pytest
+import torch
+
+import gmaster_b200 as nmt
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(got, want):
+    return float(np.max(np.abs(got - want)) / max(np.max(np.abs(want)), 1e-300))
+
+
+def _mask(nside, seed=2):
+    from gmaster_b200.utils import pix2vec_ring
+
+    rng = np.random.default_rng(seed)
+    vec = pix2vec_ring(nside)
+    mask = (vec[:, 2] > np.cos(np.radians(60))).astype(float)
+    centres = rng.normal(size=(20, 3))
+    centres /= np.linalg.norm(centres, axis=1)[:, None]
+    for c in centres:
+        mask[vec @ c > np.cos(np.radians(4.0))] = 0
+    return mask
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("mixed", 2e-4)])
+def test_batched_estimator_matches_oracle(cuda, precision, tol):
+    """TQU simulations through fields_from_maps / compute_coupled_cells / decouple_cells,
+    each simulation checked against the oracle's estimator (shared workspaces)."""
+    nside, nlb, nsims = 16, 4, 3
+    lmax = 3 * nside - 1
+    rng = np.random.default_rng(11)
+    t = rng.normal(size=(nsims, 12 * nside ** 2))
+    qu = rng.normal(size=(nsims, 2, 12 * nside ** 2))
+    mask = _mask(nside)
+    ft = nmt.fields_from_maps(mask, t, n_iter=3, precision=precision)
+    fp = nmt.fields_from_maps(mask, qu, n_iter=3, precision=precision)
+    b = nmt.NmtBin.from_nside_linear(nside, nlb)
+    f0 = nmt.NmtField(mask, None, spin=0, precision=precision)
+    f2 = nmt.NmtField(mask, None, spin=2, precision=precision)
+    f2.alm_mask = f0.get_mask_alms()
+    w00 = nmt.NmtWorkspace.from_fields(f0, f0, b)
+    w02 = nmt.NmtWorkspace.from_fields(f0, f2, b)
+    w22 = nmt.NmtWorkspace.from_fields(f2, f2, b)
+    bp00 = nmt.decouple_cells(w00, nmt.compute_coupled_cells(ft, ft))
+    bp02 = nmt.decouple_cells(w02, nmt.compute_coupled_cells(ft, fp))
+    bp22 = nmt.decouple_cells(w22, nmt.compute_coupled_cells(fp, fp))
+
+    am = oracle.map2alm(mask[None], 0, nside, lmax, 3)
+    wmask = oracle.pcl(am, am, lmax)[0]
+    m00 = oracle.binned_mcm(oracle.coupling_tt_closed(wmask, lmax), lmax, nlb, 1)
+    m02 = oracle.binned_mcm(oracle.assemble_mcm(oracle.coupling_blocks(wmask, lmax, 0, 2), lmax, 0, 2),
+                            lmax, nlb, 2)
+    m22 = oracle.binned_mcm(oracle.assemble_mcm(oracle.coupling_blocks(wmask, lmax, 2, 2), lmax, 2, 2),
+                            lmax, nlb, 4)
+    for i in range(nsims):
+        at = oracle.map2alm(t[i:i + 1] * mask, 0, nside, lmax, 3)
+        eb = oracle.map2alm(qu[i] * mask, 2, nside, lmax, 3)
+        assert _rel(bp00[i].cpu().numpy(), oracle.decouple(m00, oracle.pcl(at, at, lmax), lmax, nlb)) < tol
+        assert _rel(bp02[i].cpu().numpy(), oracle.decouple(m02, oracle.pcl(at, eb, lmax), lmax, nlb)) < tol
+        assert _rel(bp22[i].cpu().numpy(), oracle.decouple(m22, oracle.pcl(eb, eb, lmax), lmax, nlb)) < tol
+
+
+def test_batched_fields_match_single_fields(cuda):
+    """Batched mixed-precision alms agree with one-at-a-time fields, over more simulations
+    than one tensor-core launch holds (33 > 32)."""
+    nside, nsims = 8, 33
+    lmax = 3 * nside - 1
+    rng = np.random.default_rng(12)
+    t = torch.from_numpy(rng.normal(size=(nsims, 12 * nside ** 2))).cuda()
+    mask = torch.from_numpy(_mask(nside, seed=3)).cuda()
+    fb = nmt.fields_from_maps(mask, t, n_iter=2, precision="mixed")
+    for i in (0, 31, 32):
+        f = nmt.NmtField(mask, t[i:i + 1], n_iter=2, precision="fp64", lite=True)
+        assert _rel(fb[i].get_alms().cpu().numpy(), f.get_alms().cpu().numpy()) < 5e-5
+
+
+def test_decouple_cells_equals_decouple_cell(cuda):
+    nside, nlb = 16, 4
+    mask = _mask(nside, seed=4)
+    b = nmt.NmtBin.from_nside_linear(nside, nlb)
+    f0 = nmt.NmtField(mask, None, spin=0, precision="fp64")
+    w = nmt.NmtWorkspace.from_fields(f0, f0, b)
+    rng = np.random.default_rng(13)
+    cls = [torch.from_numpy(rng.normal(size=(1, 3 * nside))).cuda() for _ in range(5)]
+    bias = torch.from_numpy(rng.normal(size=(1, 3 * nside))).cuda()
+    many = nmt.decouple_cells(w, cls, cl_bias=bias)
+    for c, got in zip(cls, many):
+        want = w.decouple_cell(c, cl_bias=bias)
+        np.testing.assert_allclose(got.cpu().numpy(), want.cpu().numpy(), rtol=1e-12, atol=1e-14)
+
+
+def test_batch_shape_errors(cuda):
+    mask = _mask(8)
+    with pytest.raises(ValueError):
+        nmt.fields_from_maps(mask, np.zeros((2, 3, 12 * 64)))
+    with pytest.raises(ValueError):
+        nmt.fields_from_maps(mask, np.zeros((2, 12 * 64 + 1)))
+    with pytest.raises(ValueError):
+        nmt.fields_from_maps(mask, np.zeros((2, 2, 12 * 64)), spin=0)

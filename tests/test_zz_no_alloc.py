@@ -29,9 +29,12 @@ def test_noalloc_analysis_matches_scratch_entry_point(cuda, spin, ncomp):
     maps = torch.from_numpy(rng.normal(size=(ncomp, 12 * nside ** 2))).cuda()
     spec = sht.ring_analysis(p, maps, _lib.MIXED)
     b = sht_tc._Batch(tp, spin, ncomp)
+    b.zero_alm()
     rhs_map = torch.empty((p.L, p.nlanes, ncomp, 4), dtype=torch.float32, device=p.device)
+    img_scale = sht_tc.pow2_scale(spec.view(torch.float32)) / 2.0
     _lib.call("gm_tc_pack", p.nside, p.lmax, spin, ncomp, _lib.ptr(spec), _lib.ptr(rhs_map),
-              _lib.ptr(b.img[0]), _lib.ptr(b.img[1]) if spin else None, _lib.stream_handle(p.device))
+              _lib.ptr(b.img[0]), _lib.ptr(b.img[1]) if spin else None, img_scale,
+              _lib.stream_handle(p.device))
     stream = _lib.stream_handle(p.device)
     variants = (0,) if spin == 0 else (-2, 2)
 
@@ -40,7 +43,7 @@ def test_noalloc_analysis_matches_scratch_entry_point(cuda, spin, ncomp):
         err = torch.zeros(1, dtype=torch.int32, device=p.device)
         for sp, img in zip(variants, b.img):
             common = (p.nside, p.lmax, spin, sp, ncomp, _lib.ptr(p.geom), _lib.ptr(p.seeds),
-                      _lib.ptr(tp.coef[spin]), _lib.ptr(img), _lib.ptr(alm), 1.0)
+                      _lib.ptr(tp.coef[spin]), _lib.ptr(img), _lib.ptr(alm), 1.0 / img_scale)
             if noalloc:
                 _lib.call("gm_tc_analysis_noalloc", *common, tp.nctas, _lib.ptr(err), stream)
             else:
