@@ -395,7 +395,9 @@ def main():
     sht.TIMER = []
     calls0 = dict(_lib.CALLS)
     sampler.start()
+    torch.cuda.nvtx.range_push("bench_timed")
     ms = timed_loop(lambda i: batch_step(mask, t_all, qu_all, ws_mixed), 0, args.steps)
+    torch.cuda.nvtx.range_pop()
     clocks = sampler.stop()
     launches = sum(_lib.CALLS.get(k, 0) - calls0.get(k, 0) for k in _lib.CALLS)
     events = list(sht.TIMER)

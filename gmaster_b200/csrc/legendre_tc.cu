@@ -633,85 +633,84 @@ __global__ void k_coef_table(int64_t lmax, int spin, double *__restrict__ tab)
 
 // ------------------------------------------------------------------------------- images
 
-// Write 8 consecutive MN rows (one 16-byte chunk per plane) of an MN-major image with 128
-// rows at K index kk: element (r, kk) -> sw128_mn_offset(128, r, kk).
-__device__ __forceinline__ void put_rows8(uint8_t *img, uint32_t plane_bytes, int r0, int kk,
-                                          const float (&v)[8])
-{
-    uint4 hi, lo;
-    pack8(v, hi, lo);
-    const uint32_t off = tc::sw128_mn_offset(128, (uint32_t)r0, (uint32_t)kk);
-    *reinterpret_cast<uint4 *>(img + off) = hi;
-    *reinterpret_cast<uint4 *>(img + plane_bytes + off) = lo;
-}
-
-// Rows of the analysis right-hand side for one (m, lane) from the per-comp ring values
-// gn[c], gs[c] (complex, float): spin 0 rows [G_N | G_S]; spin 2 variant +2 rows
-// [Mt_N | Pt_S], variant -2 rows [Pt_N | Mt_S], with Pt = G_Q + i G_U, Mt = G_Q - i G_U.
-// Writes the 128-row image column (zero rows beyond 2H) for both planes.
-__device__ void write_rhs_column(uint8_t *img, int kk, int spin, int sp, int ncomp, const float2 *gn,
-                                 const float2 *gs, float scale)
-{
-    const int H = spin == 0 ? 2 * ncomp : ncomp;  // spin 2: ncomp = 2F -> H = 2F
-    float rowv[8];
-    for (int r0 = 0; r0 < 128; r0 += 8) {
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-            const int r = r0 + e;
-            float val = 0.0f;
-            if (r < 2 * H) {
-                const bool second = r >= H;
-                const int rr = second ? r - H : r;
-                const int item = rr >> 1, im = rr & 1;
-                if (spin == 0) {
-                    const float2 g = second ? gs[item] : gn[item];
-                    val = im ? g.y : g.x;
-                } else {
-                    // field `item`: comps 2 item (Q), 2 item + 1 (U)
-                    // sp = -2 rows [Pt_N | Mt_S]; sp = +2 rows [Mt_N | Pt_S]
-                    const bool north = !second;
-                    const bool plus = (sp < 0) ? !second : second;
-                    const float2 q = north ? gn[2 * item] : gs[2 * item];
-                    const float2 u = north ? gn[2 * item + 1] : gs[2 * item + 1];
-                    // Pt = q + i u = (q.x - u.y, q.y + u.x); Mt = q - i u = (q.x + u.y, q.y - u.x)
-                    if (plus) val = im ? (q.y + u.x) : (q.x - u.y);
-                    else val = im ? (q.y - u.x) : (q.x + u.y);
-                }
-            }
-            rowv[e] = val * scale;
-        }
-        put_rows8(img, kAImg, r0, kk, rowv);
-    }
-}
-
 // Initial right-hand side from the ring spectra: ringspec (ncomp, nring, L) complex64 ->
 // rhs_map (L, nlanes, ncomp) of float4 (G_N re, im, G_S re, im) and the analysis images.
-__global__ void k_pack_tc(int64_t nside, int64_t L, int ncomp, int spin,
-                          const float2 *__restrict__ spec, float4 *__restrict__ rhs_map,
-                          uint8_t *__restrict__ img_a, uint8_t *__restrict__ img_b, float scale)
+// One CTA per (block of kPackM orders, lane): the north and south ring spectra of the
+// block are read along m (coalesced) into shared memory, rhs_map is written along the
+// comps, and each image row (thread = row) is written as f16 hi/lo; rows beyond 2H are
+// zeroed.  Image a rows: spin 0 [G_N | G_S] x re/im; spin 2 [P_N | M_S]; image b rows
+// (spin 2) [M_N | P_S], P = G_Q + i G_U, M = G_Q - i G_U.
+constexpr int kPackM = 32;
+
+__device__ __forceinline__ void put_f16(uint8_t *img, uint32_t plane_bytes, float x)
 {
-    const int64_t nlanes = 2 * nside, nring = 4 * nside - 1, NG = (nlanes + kKC - 1) / kKC;
-    const int64_t m = blockIdx.y;
-    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= NG * kKC) return;
-    float2 gn[64], gs[64];
-    for (int c = 0; c < ncomp; ++c) {
-        float2 n = make_float2(0.f, 0.f), s = make_float2(0.f, 0.f);
-        if (j < nlanes) {
-            n = spec[((int64_t)c * nring + north_ring(j)) * L + m];
-            if (j != nlanes - 1) s = spec[((int64_t)c * nring + south_ring(nside, j)) * L + m];
-            rhs_map[(m * nlanes + j) * ncomp + c] = make_float4(n.x, n.y, s.x, s.y);
-        }
-        gn[c] = n;
-        gs[c] = s;
+    const __half hi = __float2half_rn(x);
+    const __half lo = __float2half_rn(x - __half2float(hi));
+    *reinterpret_cast<__half *>(img) = hi;
+    *reinterpret_cast<__half *>(img + plane_bytes) = lo;
+}
+
+// Row value of image variant v (0: a, 1: b) from the comps' (G_N, G_S) of one order.
+__device__ __forceinline__ float image_row(const float4 *__restrict__ g, int spin, int H, int r, int v)
+{
+    if (r >= 2 * H) return 0.0f;
+    const bool south = r >= H;
+    const int rr = south ? r - H : r;
+    const int item = rr >> 1;
+    const bool im = rr & 1;
+    if (spin == 0) {
+        const float4 q = g[item];
+        return south ? (im ? q.w : q.z) : (im ? q.y : q.x);
     }
+    const float4 q = g[2 * item], u = g[2 * item + 1];
+    const float qr = south ? q.z : q.x, qi = south ? q.w : q.y;
+    const float ur = south ? u.z : u.x, ui = south ? u.w : u.y;
+    const bool plus = (v == 0) ? !south : south;
+    return plus ? (im ? qi + ur : qr - ui) : (im ? qi - ur : qr + ui);
+}
+
+__global__ void __launch_bounds__(128) k_pack_tc(int64_t nside, int64_t L, int ncomp, int spin,
+                                                 const float2 *__restrict__ spec,
+                                                 float4 *__restrict__ rhs_map,
+                                                 uint8_t *__restrict__ img_a,
+                                                 uint8_t *__restrict__ img_b, float scale)
+{
+    __shared__ float4 tile[kPackM][64];
+    const int64_t nlanes = 2 * nside, nring = 4 * nside - 1, NG = (nlanes + kKC - 1) / kKC;
+    const int64_t m0 = (int64_t)blockIdx.x * kPackM, j = blockIdx.y;
+    const int tid = threadIdx.x;
+    const bool two = j != nlanes - 1;
+    const int64_t rn = north_ring(j), rs = two ? south_ring(nside, j) : 0;
+    // spectra of the block: thread -> (hemisphere, order)
+    {
+        const int hemi = tid / kPackM, mi = tid % kPackM;   // 4 x 32: hemi 0/1 used, 2/3 idle
+        const int64_t m = m0 + mi;
+        if (hemi < 2) {
+            for (int c = 0; c < ncomp; ++c) {
+                float2 v = make_float2(0.f, 0.f);
+                if (m < L && (hemi == 0 || two))
+                    v = spec[((int64_t)c * nring + (hemi ? rs : rn)) * L + m];
+                float *t = reinterpret_cast<float *>(&tile[mi][c]);
+                t[2 * hemi] = v.x;
+                t[2 * hemi + 1] = v.y;
+            }
+        }
+    }
+    __syncthreads();
+    for (int e = tid; e < kPackM * ncomp; e += blockDim.x) {
+        const int mi = e / ncomp, c = e % ncomp;
+        const int64_t m = m0 + mi;
+        if (m < L) rhs_map[(m * nlanes + j) * ncomp + c] = tile[mi][c];
+    }
+    const int H = spin == 0 ? 2 * ncomp : ncomp;
+    const uint32_t roff = tc::sw128_mn_offset(128, (uint32_t)tid, (uint32_t)(j % kKC));
     const int64_t g = j / kKC;
-    const int kk = (int)(j % kKC);
-    uint8_t *ia = img_a + ((m * NG + g) * 2) * (int64_t)kAImg;
-    write_rhs_column(ia, kk, spin, spin == 0 ? 0 : -2, ncomp, gn, gs, scale);
-    if (spin != 0) {
-        uint8_t *ib = img_b + ((m * NG + g) * 2) * (int64_t)kAImg;
-        write_rhs_column(ib, kk, spin, +2, ncomp, gn, gs, scale);
+    for (int mi = 0; mi < kPackM; ++mi) {
+        const int64_t m = m0 + mi;
+        if (m >= L) break;
+        const int64_t base = (m * NG + g) * 2 * (int64_t)kAImg + roff;
+        put_f16(img_a + base, kAImg, image_row(tile[mi], spin, H, tid, 0) * scale);
+        if (spin) put_f16(img_b + base, kAImg, image_row(tile[mi], spin, H, tid, 1) * scale);
     }
 }
 
@@ -763,12 +762,24 @@ __global__ void k_prep_syn(int64_t lmax, int spin, int sp, int H, int NR,
     }
 }
 
-// Ring-fold residual for the batched path, one CTA per lane: reads the synthesis outputs
-// (spin 0: synd rows [f_N | f_S]; spin 2: synd_a rows [sum l+ 2a | s sum l+ -2a],
-// synd_b rows [sum l- -2a | s sum l- 2a]), forms the ring coefficients per real comp,
-// folds them into the analysis-side ring spectrum, subtracts rhs_map and writes the next
-// analysis images.
-__global__ void __launch_bounds__(128) k_fold_tc(int64_t nside, int64_t L, int ncomp, int spin,
+// Ring-fold residual for the batched path: one CTA per lane, one thread per image row.
+//
+// The synthesis outputs are already in image-row form: spin 0 synd rows [f_N | f_S] x
+// re/im are the rows of the analysis image; spin 2 synd_a rows are [P_N | M_S] and synd_b
+// rows [M_N | P_S] (with Q_N = (U1 + V1)/2, U_N = i (V1 - U1)/2 one has P_N = U1 and
+// M_N = V1, and likewise P_S = V2, M_S = U2), i.e. the rows of analysis image a and b.
+// The fold for residue k of the ring length n sums the row over the orders m' = k + t n
+// with the sign (-1)^t of a shifted ring, plus the conjugates of the negative orders
+// m' = -k + t n, whose value for a real map is the conjugate of the partner row (the same
+// row for spin 0; for spin 2 P(-m') = conj M(m'), i.e. the other variant).  Residues k
+// and n - k read each other's orders, so they are summed together and every synthesis
+// value is read once.  The image of order m = k + t n is then
+//   (-1)^t w n P_k - rhs(m), scaled by `scale`, as f16 hi/lo.
+// Reads the synthesis and rhs_map once, writes each image row once (coalesced across the
+// row threads); rows beyond 2H and the absent south ring of the equator lane keep the
+// zeros the pack wrote.
+template <int SPIN>
+__global__ void __launch_bounds__(128) k_fold_tc(int64_t nside, int64_t L, int ncomp,
                                                  const float *__restrict__ synd_a,
                                                  const float *__restrict__ synd_b, int R2,
                                                  const float4 *__restrict__ rhs_map,
@@ -777,83 +788,104 @@ __global__ void __launch_bounds__(128) k_fold_tc(int64_t nside, int64_t L, int n
                                                  uint8_t *__restrict__ img_b, float scale)
 {
     const int64_t j = blockIdx.x;
+    const int r = threadIdx.x;
     const int64_t nlanes = 2 * nside, npix = 12 * nside * nside, NG = (nlanes + kKC - 1) / kKC;
     const int n = (int)ring_nphi(nside, north_ring(j));
     const bool sh = shifted[north_ring(j)] != 0;
-    const bool two = j != nlanes - 1;
+    const int H = SPIN == 0 ? 2 * ncomp : ncomp;
+    const bool south = r >= H;
+    if (r >= 2 * H || (south && j == nlanes - 1)) return;
     const float wn = (float)(4.0 * M_PI / (double)npix * (double)n);
-    const int H = spin == 0 ? 2 * ncomp : ncomp;
-    const int64_t g = j / kKC;
-    const int kk = (int)(j % kKC);
-    for (int k = threadIdx.x; k < n && k < L; k += blockDim.x) {
-        // residue sums per comp, north / south
-        float2 pn[64], ps[64];
-        for (int c = 0; c < ncomp; ++c) {
-            pn[c] = make_float2(0.f, 0.f);
-            ps[c] = make_float2(0.f, 0.f);
+    const int rr = south ? r - H : r;
+    const int item = rr >> 1;
+    const bool im = rr & 1;
+    const float cs = im ? -1.0f : 1.0f;                 // conjugation of this row
+    const int64_t stride = nlanes * R2;
+    const float *pa = synd_a + j * R2 + r;
+    const float *pb = (SPIN ? synd_b : synd_a) + j * R2 + r;
+    const uint32_t roff = tc::sw128_mn_offset(128, (uint32_t)r, (uint32_t)(j % kKC));
+    const int64_t istride = NG * 2 * (int64_t)kAImg;
+    uint8_t *ia = img_a + (j / kKC) * 2 * (int64_t)kAImg + roff;
+    uint8_t *ib = SPIN ? img_b + (j / kKC) * 2 * (int64_t)kAImg + roff : nullptr;
+    const float4 *rb = rhs_map + j * ncomp;
+
+    // rhs of this row at order m for variant v (0: image a, 1: image b)
+    auto rhs = [&](int64_t m, int v) -> float {
+        const float4 *b = rb + m * nlanes * ncomp;
+        if (SPIN == 0) {
+            const float4 q = b[item];
+            return south ? (im ? q.w : q.z) : (im ? q.y : q.x);
         }
-        auto coef = [&](int64_t mm, int c, float2 &cn, float2 &cs) {
-            // ring coefficients of comp c at order mm >= 0 for this lane (north, south)
-            const float *a = synd_a + (mm * nlanes + j) * R2;
-            if (spin == 0) {
-                cn = make_float2(a[2 * c], a[2 * c + 1]);
-                cs = make_float2(a[H + 2 * c], a[H + 2 * c + 1]);
-            } else {
-                const float *b = synd_b + (mm * nlanes + j) * R2;
-                const int f = c >> 1;
-                // U1 = a[f], U2 = a[H + f], V1 = b[f], V2 = b[H + f] (complex per field)
-                const float2 u1 = make_float2(a[2 * f], a[2 * f + 1]), u2 = make_float2(a[H + 2 * f], a[H + 2 * f + 1]);
-                const float2 v1 = make_float2(b[2 * f], b[2 * f + 1]), v2 = make_float2(b[H + 2 * f], b[H + 2 * f + 1]);
-                if ((c & 1) == 0) {
-                    // Q_N = (U1 + V1)/2, Q_S = (U2 + V2)/2
-                    cn = make_float2(0.5f * (u1.x + v1.x), 0.5f * (u1.y + v1.y));
-                    cs = make_float2(0.5f * (u2.x + v2.x), 0.5f * (u2.y + v2.y));
-                } else {
-                    // U_N = i (V1 - U1)/2, U_S = i (U2 - V2)/2 ; i (x + i y) = (-y, x)
-                    cn = make_float2(-0.5f * (v1.y - u1.y), 0.5f * (v1.x - u1.x));
-                    cs = make_float2(-0.5f * (u2.y - v2.y), 0.5f * (u2.x - v2.x));
-                }
+        const float4 q = b[2 * item], u = b[2 * item + 1];
+        const float qr = south ? q.z : q.x, qi = south ? q.w : q.y;
+        const float ur = south ? u.z : u.x, ui = south ? u.w : u.y;
+        // image a rows [P_N | M_S], image b rows [M_N | P_S]; P = Q + iU, M = Q - iU
+        const bool plus = (v == 0) ? !south : south;
+        return plus ? (im ? qi + ur : qr - ui) : (im ? qi - ur : qr + ui);
+    };
+    auto put = [&](uint8_t *img, int64_t m, float val) {
+        const float x = val * scale;
+        const __half hi = __float2half_rn(x);
+        const __half lo = __float2half_rn(x - __half2float(hi));
+        *reinterpret_cast<__half *>(img + m * istride) = hi;
+        *reinterpret_cast<__half *>(img + m * istride + kAImg) = lo;
+    };
+    // write the images of residue k from its sums (pa_k: variant a, pb_k: variant b)
+    auto emit = [&](int k, float sa, float sb) {
+        int t = 0;
+        for (int64_t m = k; m < L; m += n, ++t) {
+            const float f = (sh && (t & 1)) ? -wn : wn;
+            put(ia, m, f * sa - rhs(m, 0));
+            if (SPIN) put(ib, m, f * sb - rhs(m, 1));
+        }
+    };
+    const float neg = sh ? -1.0f : 1.0f;   // sign of an order read as a negative alias, relative
+                                           // to its sign as a positive alias
+
+    // residue 0: orders t n (t >= 0), and t n (t >= 1) as negative aliases
+    {
+        float s0a = 0.f, s0b = 0.f;
+        int t = 0;
+        for (int64_t mm = 0; mm < L; mm += n, ++t) {
+            const float sg = (sh && (t & 1)) ? -1.f : 1.f;
+            const float a = pa[mm * stride], b = SPIN ? pb[mm * stride] : a;
+            s0a += sg * a;
+            if (SPIN) s0b += sg * b;
+            if (mm > 0) {
+                s0a += sg * cs * b;                 // conj of the partner row
+                if (SPIN) s0b += sg * cs * a;
             }
-        };
+        }
+        emit(0, s0a, s0b);
+    }
+    // residue pairs (k, n - k), 0 < k < n / 2, and the self-paired residue n / 2
+    for (int k = 1; 2 * k <= n && k < L; ++k) {
+        const int k2 = n - k;
+        float pka = 0.f, pkb = 0.f, p2a = 0.f, p2b = 0.f;
         int t = 0;
         for (int64_t mm = k; mm < L; mm += n, ++t) {
             const float sg = (sh && (t & 1)) ? -1.f : 1.f;
-            for (int c = 0; c < ncomp; ++c) {
-                float2 cn, cs;
-                coef(mm, c, cn, cs);
-                pn[c].x += sg * cn.x;
-                pn[c].y += sg * cn.y;
-                ps[c].x += sg * cs.x;
-                ps[c].y += sg * cs.y;
-            }
+            const float a = pa[mm * stride], b = SPIN ? pb[mm * stride] : a;
+            pka += sg * a;
+            if (SPIN) pkb += sg * b;
+            p2a += neg * sg * cs * b;
+            if (SPIN) p2b += neg * sg * cs * a;
         }
-        t = -1;
-        for (int64_t mm = (int64_t)n - k; mm < L; mm += n, --t) {
-            const float sg = (sh && (t & 1)) ? -1.f : 1.f;
-            for (int c = 0; c < ncomp; ++c) {
-                float2 cn, cs;
-                coef(mm, c, cn, cs);
-                pn[c].x += sg * cn.x;
-                pn[c].y -= sg * cn.y;
-                ps[c].x += sg * cs.x;
-                ps[c].y -= sg * cs.y;
+        if (k2 != k) {
+            t = 0;
+            for (int64_t mm = k2; mm < L; mm += n, ++t) {
+                const float sg = (sh && (t & 1)) ? -1.f : 1.f;
+                const float a = pa[mm * stride], b = SPIN ? pb[mm * stride] : a;
+                p2a += sg * a;
+                if (SPIN) p2b += sg * b;
+                pka += neg * sg * cs * b;
+                if (SPIN) pkb += neg * sg * cs * a;
             }
-        }
-        t = 0;
-        for (int64_t m = k; m < L; m += n, ++t) {
-            const float sg = (sh && (t & 1)) ? -wn : wn;
-            float2 gn[64], gs[64];
-            for (int c = 0; c < ncomp; ++c) {
-                const float4 b = rhs_map[(m * nlanes + j) * ncomp + c];
-                gn[c] = make_float2(sg * pn[c].x - b.x, sg * pn[c].y - b.y);
-                gs[c] = two ? make_float2(sg * ps[c].x - b.z, sg * ps[c].y - b.w) : make_float2(-b.z, -b.w);
-            }
-            uint8_t *ia = img_a + ((m * NG + g) * 2) * (int64_t)kAImg;
-            write_rhs_column(ia, kk, spin, spin == 0 ? 0 : -2, ncomp, gn, gs, scale);
-            if (spin != 0) {
-                uint8_t *ib = img_b + ((m * NG + g) * 2) * (int64_t)kAImg;
-                write_rhs_column(ib, kk, spin, +2, ncomp, gn, gs, scale);
-            }
+            emit(k, pka, pkb);
+            if (k2 < L) emit(k2, p2a, p2b);
+        } else {
+            // k = n / 2: the set is its own partner; p2 holds the conjugate part
+            emit(k, pka + p2a, pkb + p2b);
         }
     }
 }
@@ -984,13 +1016,17 @@ extern "C" int gm_tc_pack(int64_t nside, int64_t lmax, int spin, int64_t ncomp, 
     if (!ringspec || !rhs_map || !img_a || (spin && !img_b)) return GM_ERR_BAD_PTR;
     const int64_t NG = gm_tc_lane_groups(nside);
     cudaStream_t s = as_stream(stream);
-    cudaError_t e = cudaMemsetAsync(img_a, 0, gm_tc_ana_image_bytes(nside, lmax), s);
-    if (e == cudaSuccess && spin) e = cudaMemsetAsync(img_b, 0, gm_tc_ana_image_bytes(nside, lmax), s);
-    if (e != cudaSuccess) {
-        set_error("gm_tc_pack memset", e);
-        return GM_ERR_LAUNCH;
+    // the kernel writes every row of every lane; only the padding lanes of a last, partial
+    // group (nside not a multiple of 64) need clearing
+    if (NG * kKC != 2 * nside) {
+        const size_t bytes = (size_t)(lmax + 1) * NG * 2 * kAImg;
+        if (cudaMemsetAsync(img_a, 0, bytes, s) != cudaSuccess ||
+            (spin && cudaMemsetAsync(img_b, 0, bytes, s) != cudaSuccess)) {
+            set_error("gm_tc_pack memset", cudaGetLastError());
+            return GM_ERR_LAUNCH;
+        }
     }
-    dim3 grid((unsigned)((NG * kKC + 127) / 128), (unsigned)(lmax + 1));
+    dim3 grid((unsigned)((lmax + 1 + kPackM - 1) / kPackM), (unsigned)(2 * nside));
     k_pack_tc<<<grid, 128, 0, s>>>(nside, lmax + 1, (int)ncomp, spin, (const float2 *)ringspec,
                                    (float4 *)rhs_map, (uint8_t *)img_a, (uint8_t *)img_b,
                                    (float)img_scale);
@@ -1090,8 +1126,9 @@ extern "C" int gm_tc_fold(int64_t nside, int64_t lmax, int spin, int64_t ncomp, 
     if (!synd_a || (spin && !synd_b) || !rhs_map || !shifted || !img_a || (spin && !img_b))
         return GM_ERR_BAD_PTR;
     const int H = spin == 0 ? (int)(2 * ncomp) : (int)ncomp;
-    k_fold_tc<<<(unsigned)(2 * nside), 128, 0, as_stream(stream)>>>(
-        nside, lmax + 1, (int)ncomp, spin, synd_a, synd_b, 2 * H, (const float4 *)rhs_map, shifted,
+    auto kern = spin == 0 ? k_fold_tc<0> : k_fold_tc<2>;
+    kern<<<(unsigned)(2 * nside), 128, 0, as_stream(stream)>>>(
+        nside, lmax + 1, (int)ncomp, synd_a, synd_b, 2 * H, (const float4 *)rhs_map, shifted,
         (uint8_t *)img_a, (uint8_t *)img_b, (float)img_scale);
     return check_launch("gm_tc_fold");
 }

@@ -48,17 +48,19 @@ template <> struct TwTable<float2> {
     }
 };
 
-// omega_h^e for a ring of half-length h (n = 2h): tw holds omega_n^k, k < h,
-// and omega_n^{k+h} = -omega_n^k.  `sign` > 0 conjugates (inverse transform).
-template <typename T2>
-__device__ __forceinline__ T2 twiddle(const T2 *__restrict__ tw, int h, int64_t e, int sign)
+// omega_h^e for an FFT of length h and 0 <= e < h, from the table of n = TM h: tw holds
+// omega_n^k for k < n / 2, and omega_n^{k + n/2} = -omega_n^k.  TM = 2 is the ring
+// transform (n = 2h, the ring's own table); TM = 1 a length-h FFT with its own table
+// (h = n).  `sign` > 0 conjugates (inverse transform).
+template <int TM = 2, typename T2>
+__device__ __forceinline__ T2 twiddle(const T2 *__restrict__ tw, int h, int e, int sign)
 {
-    int64_t k = 2 * (e % h);
+    const int k = TM * e, half = TM * h / 2;
     T2 w;
-    if (k < h) {
+    if (k < half) {
         w = __ldg(tw + k);
     } else {
-        w = __ldg(tw + (k - h));
+        w = __ldg(tw + (k - half));
         w.x = -w.x;
         w.y = -w.y;
     }
@@ -78,6 +80,17 @@ __device__ __forceinline__ T2 twiddle_n(const T2 *__restrict__ tw, int h, int k,
         w.x = -w.x;
         w.y = -w.y;
     }
+    if (sign > 0) w.y = -w.y;
+    return w;
+}
+
+// e^{sign i pi q2 / n} for 0 <= q2 < 2n from the table: omega_n^{q2/2} (times e^{-i pi / n}
+// for odd q2), conjugated for sign > 0.  c1 = e^{-i pi / n}.
+template <typename T2>
+__device__ __forceinline__ T2 phase_pi(const T2 *__restrict__ tw, int h, int q2, T2 c1, int sign)
+{
+    T2 w = twiddle_n(tw, h, q2 >> 1, -1);
+    if (q2 & 1) w = cmul(w, c1);
     if (sign > 0) w.y = -w.y;
     return w;
 }
@@ -107,7 +120,7 @@ __device__ __forceinline__ T2 mul_i(T2 z, int sign)
 
 // One Stockham stage: out[k' Lp + j + Ls v] = sum_q omega_p^{q v} omega_Lp^{q j} in[(k' + r q) Ls + j]
 // with Lp = Ls p and r = h / Lp.  Butterflies (k', j) are spread over the CTA.
-template <typename T2>
+template <int TM, typename T2>
 __device__ void stockham_stage(const T2 *__restrict__ in, T2 *__restrict__ out, int h, int p,
                                int Ls, const T2 *__restrict__ tw, int sign)
 {
@@ -122,10 +135,10 @@ __device__ void stockham_stage(const T2 *__restrict__ in, T2 *__restrict__ out, 
             T2 x2 = in[(kk + 2 * r) * Ls + j];
             T2 x3 = in[(kk + 3 * r) * Ls + j];
             if (Ls > 1) {
-                int64_t e = (int64_t)j * r;
-                x1 = cmul(x1, twiddle(tw, h, e, sign));
-                x2 = cmul(x2, twiddle(tw, h, 2 * e, sign));
-                x3 = cmul(x3, twiddle(tw, h, 3 * e, sign));
+                const int e = j * r;   // < h / 4
+                x1 = cmul(x1, twiddle<TM>(tw, h, e, sign));
+                x2 = cmul(x2, twiddle<TM>(tw, h, 2 * e, sign));
+                x3 = cmul(x3, twiddle<TM>(tw, h, 3 * e, sign));
             }
             T2 a = cadd(x0, x2), bq = csub(x0, x2);
             T2 c = cadd(x1, x3), d = mul_i(csub(x1, x3), sign);
@@ -140,7 +153,7 @@ __device__ void stockham_stage(const T2 *__restrict__ in, T2 *__restrict__ out, 
             int kk = b / Ls, j = b - kk * Ls;
             T2 x0 = in[kk * Ls + j];
             T2 x1 = in[(kk + r) * Ls + j];
-            if (Ls > 1) x1 = cmul(x1, twiddle(tw, h, (int64_t)j * r, sign));
+            if (Ls > 1) x1 = cmul(x1, twiddle<TM>(tw, h, j * r, sign));   // j r < h / 2
             T2 *o = out + kk * Lp + j;
             o[0] = cadd(x0, x1);
             o[Ls] = csub(x0, x1);
@@ -153,13 +166,16 @@ __device__ void stockham_stage(const T2 *__restrict__ in, T2 *__restrict__ out, 
             T2 acc;
             acc.x = 0;
             acc.y = 0;
-            // term q: omega_Lp^{q jp} in[(kk + r q) Ls + j];  omega_Lp = omega_h^r
+            // term q: omega_Lp^{q jp} in[(kk + r q) Ls + j];  omega_Lp = omega_h^r, with
+            // the exponent q jp mod Lp stepped incrementally
+            int eq = 0;
             for (int q = 0; q < p; ++q) {
                 T2 x = in[(kk + r * q) * Ls + j];
-                int64_t e = ((int64_t)q * jp % Lp) * r;
-                T2 w = twiddle(tw, h, e, sign);
+                T2 w = twiddle<TM>(tw, h, eq * r, sign);
                 acc.x += x.x * w.x - x.y * w.y;
                 acc.y += x.x * w.y + x.y * w.x;
+                eq += jp;
+                if (eq >= Lp) eq -= Lp;
             }
             out[o] = acc;
         }
@@ -168,7 +184,7 @@ __device__ void stockham_stage(const T2 *__restrict__ in, T2 *__restrict__ out, 
 
 // In-shared-memory FFT of length h (ping-pong between a and b); returns the buffer
 // holding the result.  Ends with a __syncthreads().
-template <typename T2>
+template <int TM = 2, typename T2>
 __device__ T2 *fft_shared(T2 *a, T2 *b, int h, const T2 *__restrict__ tw, int sign)
 {
     __shared__ int rad[40];
@@ -178,7 +194,7 @@ __device__ T2 *fft_shared(T2 *a, T2 *b, int h, const T2 *__restrict__ tw, int si
     int Ls = 1;
     for (int s = 0; s < nst; ++s) {
         int p = rad[s];
-        stockham_stage(a, b, h, p, Ls, tw, sign);
+        stockham_stage<TM>(a, b, h, p, Ls, tw, sign);
         __syncthreads();
         T2 *t = a;
         a = b;
@@ -190,53 +206,84 @@ __device__ T2 *fft_shared(T2 *a, T2 *b, int h, const T2 *__restrict__ tw, int si
 
 // ---------------------------------------------------------------- analysis
 
-template <typename T, typename Tin>
-__global__ void __launch_bounds__(512) k_ring_analysis(int64_t nside, int64_t L,
-                                                       const Tin *__restrict__ maps,
-                                                       const double *__restrict__ mask,
-                                                       const void *__restrict__ twall,
-                                                       int64_t twcnt,
-                                                       const uint8_t *__restrict__ shifted,
-                                                       typename vec2<T>::type *__restrict__ out)
+// Rings whose half-length h has a prime factor above 64 are transformed by Bluestein's
+// chirp-z method in single precision (three power-of-two FFTs of length
+// M = nextpow2(2h - 1) <= mcap), instead of a generic radix-p stage costing h p.
+__host__ __device__ __forceinline__ int largest_prime_factor(int h)
 {
-    using T2 = typename vec2<T>::type;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int64_t r = blockIdx.x, c = blockIdx.y;
-    const int64_t nring = 4 * nside - 1, npix = 12 * nside * nside;
-    const int n = (int)ring_nphi(nside, r), h = n / 2;
-    const int64_t off = ring_offset(nside, r);
-    T2 *A = reinterpret_cast<T2 *>(smem_raw);
-    T2 *B = A + 2 * nside;
-    const T2 *tw = TwTable<T2>::get(twall, twcnt) + twiddle_offset(n);
-    const Tin *x = maps + c * npix + off;
-    if (mask) {
-        // masked field: the FP64 product map * mask, rounded once to T
-        const double *w = mask + off;
-        for (int t = threadIdx.x; t < h; t += blockDim.x) {
-            T2 z;
-            z.x = (T)((double)x[2 * t] * w[2 * t]);
-            z.y = (T)((double)x[2 * t + 1] * w[2 * t + 1]);
-            A[t] = z;
+    int p = 1;
+    for (int q = 2; q * q <= h; ++q)
+        while (h % q == 0) {
+            p = q;
+            h /= q;
         }
-    } else {
-        for (int t = threadIdx.x; t < h; t += blockDim.x) {
-            T2 z;
+    return h > p ? h : p;
+}
+
+__host__ __device__ __forceinline__ int next_pow2(int x)
+{
+    int m = 1;
+    while (m < x) m <<= 1;
+    return m;
+}
+
+__host__ __device__ __forceinline__ bool use_bluestein(int h, int mcap)
+{
+    return largest_prime_factor(h) > 64 && next_pow2(2 * h - 1) <= mcap;
+}
+
+// Largest power-of-two FFT length of the Bluestein path: its table must exist (a ring
+// length 4i with i <= nside) and three buffers of it must fit in shared memory.
+static inline int bluestein_mcap(int64_t nside)
+{
+    int64_t m = 1;
+    while (2 * m <= 4 * nside && 2 * m <= 8192) m *= 2;
+    return (int)m;
+}
+
+// Load one ring of one map (times the mask) as h complex z_t = x_2t + i x_2t+1, each
+// multiplied by f(t) (the Bluestein chirp, or 1).
+template <typename T, typename Tin, typename T2, typename F>
+__device__ __forceinline__ void load_ring(const Tin *__restrict__ x, const double *__restrict__ mask,
+                                          int h, T2 *__restrict__ dst, F f)
+{
+    for (int t = threadIdx.x; t < h; t += blockDim.x) {
+        T2 z;
+        if (mask) {
+            // masked field: the FP64 product map * mask, rounded once to T
+            z.x = (T)((double)x[2 * t] * mask[2 * t]);
+            z.y = (T)((double)x[2 * t + 1] * mask[2 * t + 1]);
+        } else {
             z.x = (T)x[2 * t];
             z.y = (T)x[2 * t + 1];
-            A[t] = z;
         }
+        dst[t] = f(t, z);
     }
-    __syncthreads();
-    T2 *Z = fft_shared(A, B, h, tw, -1);
-    const T w = (T)(4.0 * M_PI / (double)npix);
-    const bool sh = shifted[r] != 0;
-    T2 *dst = out + (c * nring + r) * L;
-    for (int64_t m = threadIdx.x; m < L; m += blockDim.x) {
-        int k = (int)(m % n);
-        bool conj = k > h;
-        int kk = conj ? n - k : k;
+}
+
+// Unpack the half-length transform Z of one real ring into its spectrum for m < L, with
+// the quadrature weight and the ring phase e^{-i m phi0}: dst[m] = w e^{-i m phi0} X[m mod n].
+template <typename T, typename T2>
+__device__ __forceinline__ void ring_outputs(const T2 *__restrict__ Z, int n, int64_t L,
+                                             const T2 *__restrict__ tw, bool sh, T w,
+                                             T2 *__restrict__ dst)
+{
+    const int h = n / 2;
+    T2 c1;   // e^{-i pi / n}
+    {
+        double s1, c1d;
+        sincospi(-1.0 / (double)n, &s1, &c1d);
+        c1.x = (T)c1d;
+        c1.y = (T)s1;
+    }
+    const unsigned n2 = 2u * (unsigned)n;
+    for (int m = threadIdx.x; m < (int)L; m += blockDim.x) {
+        const unsigned m2 = (unsigned)m % n2;           // m mod 2n
+        const int k = (int)(m2 < (unsigned)n ? m2 : m2 - (unsigned)n);
+        const bool conj = k > h;
+        const int kk = conj ? n - k : k;                // 0..h
         // X[kk] = E + omega_n^kk O, E = (Z[kk] + conj Z[h-kk]) / 2, O = (Z[kk] - conj Z[h-kk]) / 2i
-        T2 za = Z[kk % h], zb = Z[(h - kk) % h];
+        const T2 za = Z[kk == h ? 0 : kk], zb = Z[kk == 0 ? 0 : h - kk];
         T er = (za.x + zb.x) * (T)0.5, ei = (za.y - zb.y) * (T)0.5;
         T orr = (za.y + zb.y) * (T)0.5, oi = -(za.x - zb.x) * (T)0.5;
         T2 wn = twiddle_n(tw, h, kk, -1);
@@ -246,22 +293,115 @@ __global__ void __launch_bounds__(512) k_ring_analysis(int64_t nside, int64_t L,
         T pr = 1, pi = 0;
         if (sh) {
             // e^{-i m phi0}, phi0 = pi / n
-            if (sizeof(T) == 8) {
-                double s, cc;
-                sincospi(-(double)m / (double)n, &s, &cc);
-                pr = (T)cc;
-                pi = (T)s;
-            } else {
-                float s, cc;
-                sincospif(-(float)(m % (2 * n)) / (float)n, &s, &cc);
-                pr = (T)cc;
-                pi = (T)s;
-            }
+            const T2 ph = phase_pi(tw, h, (int)m2, c1, -1);
+            pr = ph.x;
+            pi = ph.y;
         }
         T2 g;
         g.x = w * (xr * pr - xi * pi);
         g.y = w * (xr * pi + xi * pr);
         dst[m] = g;
+    }
+}
+
+// One CTA per (ring, map component): mixed-radix Stockham FFT in shared memory.  In single
+// precision the rings of the Bluestein path (use_bluestein with `mcap` > 0) are left to
+// k_ring_analysis_bluestein.
+template <typename T, typename Tin>
+__global__ void __launch_bounds__(512) k_ring_analysis(int64_t nside, int64_t L,
+                                                       const Tin *__restrict__ maps,
+                                                       const double *__restrict__ mask,
+                                                       const void *__restrict__ twall,
+                                                       int64_t twcnt,
+                                                       const uint8_t *__restrict__ shifted,
+                                                       typename vec2<T>::type *__restrict__ out,
+                                                       int mcap)
+{
+    using T2 = typename vec2<T>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int64_t r = blockIdx.x, c = blockIdx.y;
+    const int64_t nring = 4 * nside - 1, npix = 12 * nside * nside;
+    const int n = (int)ring_nphi(nside, r), h = n / 2;
+    if (mcap > 0 && use_bluestein(h, mcap)) return;
+    const int64_t off = ring_offset(nside, r);
+    T2 *A = reinterpret_cast<T2 *>(smem_raw);
+    T2 *B = A + 2 * nside;
+    const T2 *tw = TwTable<T2>::get(twall, twcnt) + twiddle_offset(n);
+    load_ring<T>(maps + c * npix + off, mask ? mask + off : nullptr, h, A,
+                 [](int, T2 z) { return z; });
+    __syncthreads();
+    T2 *Z = fft_shared(A, B, h, tw, -1);
+    ring_outputs<T>(Z, n, L, tw, shifted[r] != 0, (T)(4.0 * M_PI / (double)npix),
+                    out + (c * nring + r) * L);
+}
+
+// Bluestein path, single precision: one CTA per (ring, block of `cpc` components).
+//   X_k = sum_j z_j omega_h^{jk} = c_k sum_j (z_j c_j) conj(c_{k-j}),  c_j = e^{-i pi j^2 / h}
+// evaluated as a circular convolution of length M: the transform of the wrapped conjugate
+// chirp once per CTA, then per component one forward and one inverse FFT.  The chirp is
+// read exactly from the ring's table: c_j = omega_{2h}^{j^2 mod 2h}.
+template <typename Tin>
+__global__ void __launch_bounds__(512) k_ring_analysis_bluestein(int64_t nside, int64_t L,
+                                                                 int64_t ncomp, int cpc, int mcap,
+                                                                 const Tin *__restrict__ maps,
+                                                                 const double *__restrict__ mask,
+                                                                 const void *__restrict__ twall,
+                                                                 int64_t twcnt,
+                                                                 const uint8_t *__restrict__ shifted,
+                                                                 float2 *__restrict__ out)
+{
+    using T2 = float2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int64_t r = blockIdx.x;
+    const int n = (int)ring_nphi(nside, r), h = n / 2;
+    if (!use_bluestein(h, mcap)) return;
+    const int M = next_pow2(2 * h - 1);
+    const int64_t nring = 4 * nside - 1, npix = 12 * nside * nside;
+    const int64_t off = ring_offset(nside, r);
+    T2 *buf0 = reinterpret_cast<T2 *>(smem_raw);
+    T2 *buf1 = buf0 + mcap, *buf2 = buf1 + mcap;
+    const T2 *tw32 = TwTable<T2>::get(twall, twcnt);
+    const T2 *tw = tw32 + twiddle_offset(n);     // omega_n^k, k < h
+    const T2 *twM = tw32 + twiddle_offset(M);    // omega_M^k, k < M / 2 (M = 4i, i <= nside)
+    auto chirp = [&](int j) {
+        const unsigned q = ((unsigned)j * (unsigned)j) % (unsigned)n;
+        return twiddle_n(tw, h, (int)q, -1);
+    };
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+        T2 v = make_float2(0.f, 0.f);
+        if (m < h) v = chirp(m);
+        else if (m > M - h) v = chirp(M - m);
+        v.y = -v.y;
+        buf0[m] = v;
+    }
+    __syncthreads();
+    const T2 *FB = fft_shared<1>(buf0, buf1, M, twM, -1);
+    T2 *X = (FB == buf0) ? buf1 : buf0;
+    T2 *Y = buf2;
+    const float invM = 1.0f / (float)M;
+    const bool sh = shifted[r] != 0;
+    const float w = (float)(4.0 * M_PI / (double)npix);
+    const int64_t c1 = (int64_t)(blockIdx.y + 1) * cpc < ncomp ? (int64_t)(blockIdx.y + 1) * cpc : ncomp;
+    for (int64_t c = (int64_t)blockIdx.y * cpc; c < c1; ++c) {
+        for (int j = h + threadIdx.x; j < M; j += blockDim.x) X[j] = make_float2(0.f, 0.f);
+        load_ring<float>(maps + c * npix + off, mask ? mask + off : nullptr, h, X,
+                         [&](int t, T2 z) { return cmul(z, chirp(t)); });
+        __syncthreads();
+        T2 *FA = fft_shared<1>(X, Y, M, twM, -1);
+        T2 *G = (FA == X) ? Y : X;
+        for (int m = threadIdx.x; m < M; m += blockDim.x) {
+            T2 v = cmul(FA[m], FB[m]);
+            v.x *= invM;
+            v.y *= invM;
+            FA[m] = v;
+        }
+        __syncthreads();
+        T2 *R = fft_shared<1>(FA, G, M, twM, +1);
+        T2 *Z = (R == FA) ? G : FA;
+        for (int k = threadIdx.x; k < h; k += blockDim.x) Z[k] = cmul(R[k], chirp(k));
+        __syncthreads();
+        ring_outputs<float>(Z, n, L, tw, sh, w, out + (c * nring + r) * L);
+        __syncthreads();
     }
 }
 
@@ -397,6 +537,13 @@ __global__ void __launch_bounds__(512) k_ring_synthesis(int64_t nside, int64_t L
     T2 *A = reinterpret_cast<T2 *>(smem_raw);
     T2 *B = A + 2 * nside;
     const T2 *tw = TwTable<T2>::get(twall, twcnt) + twiddle_offset(n);
+    T2 cpi;   // e^{-i pi / n}
+    {
+        double s1, c1d;
+        sincospi(-1.0 / (double)n, &s1, &c1d);
+        cpi.x = (T)c1d;
+        cpi.y = (T)s1;
+    }
     // Fold into the n-periodic spectrum C_k = e^{i pi s k / n} P_k and build
     // Z'[k] = (C_k + C_{k+h}) + i (C_k - C_{k+h}) omega_n^{-k}, k < h.
     const T *base = syn + (south ? 2 : 0);
@@ -407,19 +554,9 @@ __global__ void __launch_bounds__(512) k_ring_synthesis(int64_t nside, int64_t L
         T2 ck = make2<T2, T>(c0[0], c0[1]);
         T2 ckh = make2<T2, T>(c1[0], c1[1]);
         if (sh) {
-            if (sizeof(T) == 8) {
-                double s, cc;
-                sincospi((double)k / (double)n, &s, &cc);
-                ck = cmul(ck, make2<T2, T>((T)cc, (T)s));
-                sincospi((double)(k + h) / (double)n, &s, &cc);
-                ckh = cmul(ckh, make2<T2, T>((T)cc, (T)s));
-            } else {
-                float s, cc;
-                sincospif((float)k / (float)n, &s, &cc);
-                ck = cmul(ck, make2<T2, T>((T)cc, (T)s));
-                sincospif((float)(k + h) / (float)n, &s, &cc);
-                ckh = cmul(ckh, make2<T2, T>((T)cc, (T)s));
-            }
+            // e^{i pi k / n} and e^{i pi (k + h) / n}
+            ck = cmul(ck, phase_pi(tw, h, k, cpi, +1));
+            ckh = cmul(ckh, phase_pi(tw, h, k + h, cpi, +1));
         }
         T2 sum = cadd(ck, ckh);
         T2 dif = cmul(csub(ck, ckh), twiddle_n(tw, h, k, +1));
@@ -500,21 +637,33 @@ extern "C" int gm_ring_analysis(int precision, int64_t nside, int64_t L, int64_t
         if (map_dtype_bytes == 8) {
             if ((st = set_smem(k_ring_analysis<double, double>, smem))) return st;
             k_ring_analysis<double, double><<<grid, threads, smem, s>>>(
-                nside, L, (const double *)maps, mask, tw, cnt, shifted, (double2 *)ringspec);
+                nside, L, (const double *)maps, mask, tw, cnt, shifted, (double2 *)ringspec, 0);
         } else {
             if ((st = set_smem(k_ring_analysis<double, float>, smem))) return st;
             k_ring_analysis<double, float><<<grid, threads, smem, s>>>(
-                nside, L, (const float *)maps, mask, tw, cnt, shifted, (double2 *)ringspec);
+                nside, L, (const float *)maps, mask, tw, cnt, shifted, (double2 *)ringspec, 0);
         }
     } else if (precision == GM_MIXED) {
+        const int mcap = bluestein_mcap(nside);
+        const size_t bs_smem = 3 * (size_t)mcap * sizeof(float2);
+        const int cpc = 8;
+        dim3 bs_grid((unsigned)nring, (unsigned)((ncomp + cpc - 1) / cpc));
         if (map_dtype_bytes == 8) {
             if ((st = set_smem(k_ring_analysis<float, double>, smem))) return st;
             k_ring_analysis<float, double><<<grid, threads, smem, s>>>(
-                nside, L, (const double *)maps, mask, tw, cnt, shifted, (float2 *)ringspec);
+                nside, L, (const double *)maps, mask, tw, cnt, shifted, (float2 *)ringspec, mcap);
+            if ((st = set_smem(k_ring_analysis_bluestein<double>, bs_smem))) return st;
+            k_ring_analysis_bluestein<double><<<bs_grid, 512, bs_smem, s>>>(
+                nside, L, ncomp, cpc, mcap, (const double *)maps, mask, tw, cnt, shifted,
+                (float2 *)ringspec);
         } else {
             if ((st = set_smem(k_ring_analysis<float, float>, smem))) return st;
             k_ring_analysis<float, float><<<grid, threads, smem, s>>>(
-                nside, L, (const float *)maps, mask, tw, cnt, shifted, (float2 *)ringspec);
+                nside, L, (const float *)maps, mask, tw, cnt, shifted, (float2 *)ringspec, mcap);
+            if ((st = set_smem(k_ring_analysis_bluestein<float>, bs_smem))) return st;
+            k_ring_analysis_bluestein<float><<<bs_grid, 512, bs_smem, s>>>(
+                nside, L, ncomp, cpc, mcap, (const float *)maps, mask, tw, cnt, shifted,
+                (float2 *)ringspec);
         }
     } else {
         return GM_ERR_UNSUPPORTED;

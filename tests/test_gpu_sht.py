@@ -34,7 +34,8 @@ def _rand_alm(lmax, nrows, rng, spin=0):
     return alm
 
 
-@pytest.mark.parametrize("nside,L", [(4, 12), (8, 24), (16, 47), (16, 71), (32, 96), (2, 9)])
+@pytest.mark.parametrize("nside,L", [(4, 12), (8, 24), (16, 47), (16, 71), (32, 96), (2, 9),
+                                     (128, 384), (96, 200)])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_ring_analysis_matches_direct_dft(cuda, nside, L, precision):
     """Every ring's m block is w e^{-i m phi0} sum_p x_p e^{-2 pi i p m / nphi}
@@ -49,6 +50,23 @@ def test_ring_analysis_matches_direct_dft(cuda, nside, L, precision):
     for c in range(2):
         want = w * oracle.ring_analysis(nside, L, maps[c].astype(np.complex128))
         assert _rel(spec[c], want) < TOL[precision]
+
+
+def _lpf(h):
+    p, q = 1, 2
+    while q * q <= h:
+        while h % q == 0:
+            p, h = q, h // q
+        q += 1
+    return max(p, h)
+
+
+def test_chirp_z_rings_exist_in_the_parity_cases():
+    """Nside 128 and 96 (parity cases above) have polar rings whose half-length 2i has a
+    prime factor above 64: the mixed-precision ring stage sends those through the chirp-z
+    (Bluestein) path, so the direct-DFT check covers it."""
+    assert [i for i in range(1, 128) if _lpf(2 * i) > 64] == [67, 71, 73, 79, 83, 89, 97, 101, 103,
+                                                              107, 109, 113, 127]
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
