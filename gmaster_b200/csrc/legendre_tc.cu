@@ -283,13 +283,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
         const double sgn_c = sgn_of(p.sp);
         uint32_t u = 0, q = 0;
         double *my_scratch = scratch + (int64_t)c * p.nlanes * 3;
+        // After a timed-out wait (abort) a generator stops working but keeps taking part in
+        // every named barrier of the loops, which are bounded by the work list, so no
+        // thread can wait on a barrier that its peers have left.
+        bool dead = false;
         for (int64_t i = 0;; ++i) {
             const int64_t m = snake_m(i, c, G);
-            if (m > p.lmax || *abort) break;
+            if (m > p.lmax) break;
             const int64_t l0 = m > l0min ? m : l0min;
             const int64_t nsb = (L - l0 + kSB - 1) / kSB;
             const int64_t mb = alm_idx(p.lmax, 0, m);   // coefficient / alm base of order m
-            for (int64_t s = 0; s < nsb && !*abort; ++s) {
+            for (int64_t s = 0; s < nsb; ++s) {
                 const int64_t lb = l0 + s * kSB;
                 // coefficients of this superblock into shared memory (every generator has
                 // finished the previous superblock: its epilogue waited for all its tiles)
@@ -305,26 +309,49 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
                     if (SPIN) sC0[e] = sgn_c * cf.c0;
                 }
                 gen_barrier();
-                for (int64_t g = 0; g < NG && !*abort; ++g) {
+                // lane state of group g + 1 is loaded while group g is generated
+                // (x, then seed inputs or the carried recurrence state)
+                double nx = 0.0, na = 0.0, nb = 0.0, nc = 0.0;
+                auto prefetch = [&](int64_t gg) {
+                    const int64_t jn = gg * kKC + tid;
+                    nx = na = nb = nc = 0.0;
+                    if (gg < NG && jn < p.nlanes) {
+                        nx = p.geom[jn];
+                        if (s == 0) {
+                            na = p.geom[p.nlanes + jn];
+                            nb = p.geom[2 * p.nlanes + jn];
+                        } else {
+                            na = my_scratch[jn * 3];
+                            nb = my_scratch[jn * 3 + 1];
+                            nc = my_scratch[jn * 3 + 2];
+                        }
+                    }
+                };
+                dead = dead || *abort;
+                if (!dead) prefetch(0);
+                for (int64_t g = 0; g < NG && !dead; ++g) {
                     const int64_t jl = g * kKC + tid;
                     const bool valid = jl < p.nlanes;
                     double x = 0.0, v = 0.0, vp = 0.0;   // padding lanes stay exactly zero
                     int k = 0;
                     if (valid) {
-                        x = p.geom[jl];
+                        x = nx;
                         if (s == 0) {
-                            seed_lane(p.seeds + ((int64_t)p.var * L + m) * 4, p.geom[p.nlanes + jl],
-                                      p.geom[2 * p.nlanes + jl], vp, k);
+                            seed_lane(p.seeds + ((int64_t)p.var * L + m) * 4, na, nb, vp, k);
                         } else {
-                            v = my_scratch[jl * 3];
-                            vp = my_scratch[jl * 3 + 1];
-                            k = (int)my_scratch[jl * 3 + 2];
+                            v = na;
+                            vp = nb;
+                            k = (int)nc;
                         }
                     }
+                    prefetch(g + 1);
                     bool emit = (k == 0);
                     for (int t = 0; t < kSB / kNB; ++t, ++u) {
                         const uint32_t st = u & 1;
-                        if (!wait_or_abort(&sh.b_free[st], ((u >> 1) & 1) ^ 1, abort, err)) break;
+                        if (!wait_or_abort(&sh.b_free[st], ((u >> 1) & 1) ^ 1, abort, err)) {
+                            dead = true;
+                            break;
+                        }
                         const uint32_t b0 = tc::smem_u32(sB + st * 2 * kBTileA);
                         const uint32_t rowbase = b0 + (tid >> 3) * 1024 + (tid & 7) * 128;
                         const double2 *cab = sAB + t * kNB;
@@ -353,14 +380,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
                         __syncwarp();
                         if (lane == 0) tc::mbar_arrive(&sh.b_full[st]);
                     }
-                    if (valid && s + 1 < nsb) {
+                    if (valid && s + 1 < nsb && !dead) {
                         my_scratch[jl * 3] = v;
                         my_scratch[jl * 3 + 1] = vp;
                         my_scratch[jl * 3 + 2] = (double)k;
                     }
                 }
                 // epilogue of superblock s
-                if (!wait_or_abort(&sh.d_full, q & 1, abort, err)) break;
+                if (dead || !wait_or_abort(&sh.d_full, q & 1, abort, err)) {
+                    dead = true;
+                    continue;
+                }
                 tc::tc_fence_after();
                 const int row = warp * 32 + lane;
                 const bool rvalid = row < 2 * p.H;
@@ -507,18 +537,38 @@ __global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t 
         bool emit[2];
 #pragma unroll
         for (int h = 0; h < 2; ++h) emit[h] = (k[h] == 0);
+        // Coefficients of chunk cc sit in shared stage cc & 1.  Threads tid < kKL load the
+        // chunk two ahead into registers while the current one is generated, and publish
+        // the next one right after the barrier that frees its stage.
+        auto fetch = [&](int64_t ch) -> Coef {
+            const int64_t l = (c0 + ch) * kKL + tid;
+            return (tid < kKL && ch < nch && l > l0 && l < L) ? load_coef(p.coef, mb + l)
+                                                              : Coef{0.0, 0.0, 0.0};
+        };
+        auto publish = [&](int64_t ch, const Coef &cf) {
+            if (tid < kKL) {
+                const int64_t so = (ch & 1) * kKL;
+                sAB[so + tid] = make_double2(cf.alpha, cf.beta);
+                if (SPIN) sC0[so + tid] = sgn_c * cf.c0;
+            }
+        };
+        Coef pre = fetch(0);
+        publish(0, pre);
+        pre = fetch(1);
+        bool dead = false;
         for (int64_t cc = 0; cc < nch; ++cc) {
             const uint32_t st = (uint32_t)cc & 1;
             double2 *cab = sAB + st * kKL;
             double *cc0 = sC0 + st * kKL;
-            if (tid < kKL) {
-                const int64_t l = (c0 + cc) * kKL + tid;
-                const Coef cf = (l > l0 && l < L) ? load_coef(p.coef, mb + l) : Coef{0.0, 0.0, 0.0};
-                cab[tid] = make_double2(cf.alpha, cf.beta);
-                if (SPIN) cc0[tid] = sgn_c * cf.c0;
+            gen_barrier();   // stage st is complete; stage st ^ 1 (chunk cc - 1) is free
+            // after a timed-out wait a generator keeps meeting the barrier every chunk (the
+            // loop is bounded) but does no more work
+            if (dead || !wait_or_abort(&sh.b_free[st], ((uint32_t)(cc >> 1) & 1) ^ 1, abort, err)) {
+                dead = true;
+                continue;
             }
-            gen_barrier();
-            if (!wait_or_abort(&sh.b_free[st], ((uint32_t)(cc >> 1) & 1) ^ 1, abort, err)) break;
+            publish(cc + 1, pre);
+            pre = fetch(cc + 2);
             const uint32_t b0 = tc::smem_u32(sB + st * 2 * kBTileS);
 #pragma unroll 1
             for (int sub = 0; sub < kKL / 8; ++sub) {
@@ -575,7 +625,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t 
             if (lane == 0) tc::mbar_arrive(&sh.b_full[st]);
         }
         // epilogue: D[row, lane] -> synd[m][lane][row]
-        if (wait_or_abort(&sh.d_full, 0, abort, err)) {
+        if (!dead && wait_or_abort(&sh.d_full, 0, abort, err)) {
             tc::tc_fence_after();
             const int row = warp * 32 + lane;
             for (int cb = 0; cb < kLT; cb += 16) {
