@@ -96,12 +96,15 @@ __device__ __forceinline__ void rescale(double &v, double &vp, int &k)
     }
 }
 
+// Coefficient table entries are 32 bytes: (alpha, beta) then (c0, 0), so one 16-byte load
+// fetches (alpha, beta).
 __device__ __forceinline__ Coef load_coef(const double *__restrict__ tab, int64_t idx)
 {
+    const double2 ab = __ldg(reinterpret_cast<const double2 *>(tab) + 2 * idx);
     Coef c;
-    c.alpha = __ldg(tab + 3 * idx);
-    c.beta = __ldg(tab + 3 * idx + 1);
-    c.c0 = __ldg(tab + 3 * idx + 2);
+    c.alpha = ab.x;
+    c.beta = ab.y;
+    c.c0 = __ldg(tab + 4 * idx + 2);
     return c;
 }
 
@@ -133,7 +136,7 @@ struct Params {
     double scale;    // analysis: alm += scale * result
     const double *geom;   // (3, nlanes)
     const double *seeds;  // (3, L, 4)
-    const double *coef;   // (nelem, 3) for this spin
+    const double *coef;   // (nelem, 4) for this spin: alpha, beta, c0, 0
     int var;              // seed variant 0 / 1 / 2
 };
 
@@ -230,13 +233,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
                 if (ng == NG) { ng = 0; ++ns; }
                 if (ns == nsb) { ns = 0; ++ni; }
                 const bool next = job_m(ni) <= p.lmax;
-                if (next) {
-                    const uint32_t nb = (j + 1) & 1;
-                    if (!wait_or_abort(&sh.a_free[nb], (((j + 1) >> 1) & 1) ^ 1, abort, err)) break;
-                    tc::mbar_arrive_expect_tx(&sh.a_full[nb], 2 * kAImg);
-                    tc::bulk_g2s(sA + nb * 2 * kAImg, aimg + ((job_m(ni) * NG + ng) * 2) * (int64_t)kAImg,
-                                 2 * kAImg, &sh.a_full[nb]);
-                }
                 const uint32_t buf = j & 1;
                 if (!wait_or_abort(&sh.a_full[buf], (j >> 1) & 1, abort, err)) break;
                 if (g == 0 && !wait_or_abort(&sh.d_free, (q & 1) ^ 1, abort, err)) break;
@@ -264,6 +260,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
                         tc::mma_f16(dx, al, bh, idesc, 1u);
                     }
                     tc::mma_commit(&sh.b_free[st]);
+                    // with the first tile's MMAs queued, refill the other image buffer once
+                    // the previous job's MMAs (which read it) are done
+                    if (t == 0 && next) {
+                        const uint32_t nb = (j + 1) & 1;
+                        if (!wait_or_abort(&sh.a_free[nb], (((j + 1) >> 1) & 1) ^ 1, abort, err)) break;
+                        tc::mbar_arrive_expect_tx(&sh.a_full[nb], 2 * kAImg);
+                        tc::bulk_g2s(sA + nb * 2 * kAImg, aimg + ((job_m(ni) * NG + ng) * 2) * (int64_t)kAImg,
+                                     2 * kAImg, &sh.a_full[nb]);
+                    }
                 }
                 if (*abort) break;
                 tc::mma_commit(&sh.a_free[buf]);
@@ -487,13 +492,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t 
             tc::mbar_arrive_expect_tx(&sh.a_full[0], 2 * kSImg);
             tc::bulk_g2s(sA, img, 2 * kSImg, &sh.a_full[0]);
             for (int64_t cc = 0; cc < nch && !*abort; ++cc) {
-                if (cc + 1 < nch) {
-                    const uint32_t nb = (uint32_t)(cc + 1) & 1;
-                    if (!wait_or_abort(&sh.a_free[nb], ((uint32_t)((cc + 1) >> 1) & 1) ^ 1, abort, err)) break;
-                    tc::mbar_arrive_expect_tx(&sh.a_full[nb], 2 * kSImg);
-                    tc::bulk_g2s(sA + nb * 2 * kSImg, img + (cc + 1) * 2 * (int64_t)kSImg, 2 * kSImg,
-                                 &sh.a_full[nb]);
-                }
                 const uint32_t st = (uint32_t)cc & 1, ph = (uint32_t)(cc >> 1) & 1;
                 if (!wait_or_abort(&sh.a_full[st], ph, abort, err)) break;
                 if (!wait_or_abort(&sh.b_full[st], ph, abort, err)) break;
@@ -514,6 +512,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t 
                 }
                 tc::mma_commit(&sh.b_free[st]);
                 tc::mma_commit(&sh.a_free[st]);
+                // with this chunk's MMAs queued, load the next chunk's image into the buffer
+                // of the previous chunk once its MMAs are done
+                if (cc + 1 < nch) {
+                    const uint32_t nb = (uint32_t)(cc + 1) & 1;
+                    if (!wait_or_abort(&sh.a_free[nb], ((uint32_t)((cc + 1) >> 1) & 1) ^ 1, abort, err)) break;
+                    tc::mbar_arrive_expect_tx(&sh.a_full[nb], 2 * kSImg);
+                    tc::bulk_g2s(sA + nb * 2 * kSImg, img + (cc + 1) * 2 * (int64_t)kSImg, 2 * kSImg,
+                                 &sh.a_full[nb]);
+                }
             }
             if (!*abort) tc::mma_commit(&sh.d_full);
         }
@@ -653,7 +660,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t 
 
 // ------------------------------------------------------------------------------- tables
 
-// coef[(mstart[m] + l) * 3 + {0,1,2}] = (alpha, beta, c0) of target degree l for s'^2 = s2.
+// coef[(mstart[m] + l) * 4 + {0,1,2,3}] = (alpha, beta, c0, 0) of target degree l for s'^2 = s2.
 __global__ void k_coef_table(int64_t lmax, int spin, double *__restrict__ tab)
 {
     const int64_t m = blockIdx.y;
@@ -675,9 +682,10 @@ __global__ void k_coef_table(int64_t lmax, int spin, double *__restrict__ tab)
             if (spin != 0) c0 = 2.0 * dm / ((dl - 1.0) * dl);
         }
         const int64_t idx = alm_idx(lmax, l, m);
-        tab[3 * idx] = a;
-        tab[3 * idx + 1] = b;
-        tab[3 * idx + 2] = c0;
+        tab[4 * idx] = a;
+        tab[4 * idx + 1] = b;
+        tab[4 * idx + 2] = c0;
+        tab[4 * idx + 3] = 0.0;
     }
 }
 

@@ -33,7 +33,7 @@ class TCPlan:
         self.nchunks = {}
         lib = _lib.load()
         for spin in (0, 2):
-            tab = torch.empty((plan.nelem, 3), dtype=torch.float64, device=dev)
+            tab = torch.empty((plan.nelem, 4), dtype=torch.float64, device=dev)
             _lib.call("gm_tc_coef_table", lmax, spin, _lib.ptr(tab), _lib.stream_handle(dev))
             self.coef[spin] = tab
             host = np.zeros(plan.L + 1, dtype=np.int64)

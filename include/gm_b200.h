@@ -190,7 +190,8 @@ int64_t gm_tc_ana_scratch_bytes(int64_t nside, int64_t nctas);
  * image bytes for that many chunks (32 KB each). */
 int gm_tc_syn_chunk_offsets(int64_t lmax, int spin, int64_t *choff_host);
 int64_t gm_tc_syn_image_bytes(int64_t nchunks);
-/* Recurrence coefficient table (nelem, 3) float64 for spin 0 or 2. */
+/* Recurrence coefficient table (nelem, 4) float64 for spin 0 or 2: entry idx(l, m) holds
+ * (alpha, beta, c0, 0), 32 bytes so that (alpha, beta) is one aligned 16-byte load. */
 int gm_tc_coef_table(int64_t lmax, int spin, double *tab, void *stream);
 /* Ring spectra (ncomp, nring, L) complex64 -> rhs_map (L, nlanes, ncomp) float4
  * [G_N re, im, G_S re, im] and the analysis images scaled by img_scale (img_b only for
