@@ -75,6 +75,73 @@ __device__ __forceinline__ int64_t total_units(int64_t lmax)
 // One thread per (l1 <= l2) pair: three-term recursion in l3 (Schulten & Gordon 1975)
 // for (l3 l1 l2; 0 2 -2) = (l1 l2 l3; 2 -2 0), and the two-term ratio for (l1 l2 l3; 000),
 // both unnormalised from l3 = l2 - l1 and normalised by sum (2 l3 + 1) f^2 = 1.
+// Coupling sums of one pair (l1 <= l2): vals[x] = S_x(l1, l2) for x = tt, te, pp, mm,
+// S_x = sum_l3 (2 l3 + 1) W_l3 / (4 pi) T_x(l1, l2, l3) (the blocks divided by 2 l2 + 1).
+__device__ void coupling_pair(int64_t l1, int64_t l2, const double *__restrict__ window, int64_t nw,
+                              bool want_s2, double (&vals)[4])
+{
+    const double inv4pi = 1.0 / (4.0 * M_PI);
+    const int64_t d = l2 - l1, jmin = d, jmax = l1 + l2;
+    const double S = (double)(l1 + l2 + 1), S2 = S * S, d2 = (double)(d * d);
+    const bool s2ok = want_s2 && l1 >= 2 && l2 >= 2;
+    double f_prev = 0.0, f = 1.0;      // (000), unnormalised
+    double g_prev = 0.0, g = 1.0;      // (2 -2 0), unnormalised
+    double sq = 0.0;                   // sqrt P(j) at the current j
+    double n0 = 0.0, n2s = 0.0, stt = 0.0, ste = 0.0, spp = 0.0, smm = 0.0;
+    for (int64_t j = jmin;; ++j) {
+        const double tj = 2.0 * (double)j + 1.0;
+        const double wj = (j < nw ? __ldg(window + j) : 0.0) * inv4pi * tj;
+        const bool even = ((j - jmin) & 1) == 0;
+        n0 += tj * f * f;
+        stt += wj * f * f;
+        if (s2ok) {
+            n2s += tj * g * g;
+            ste += wj * f * g;
+            if (even) spp += wj * g * g;
+            else smm += wj * g * g;
+        }
+        if (j == jmax) break;
+        const double j1 = (double)(j + 1);
+        const double P1 = (j1 * j1 - d2) * (S2 - j1 * j1);
+        const double r1 = rsqrt(P1);
+        const double sq1 = P1 * r1;
+        const double fn = -sq * r1 * f_prev;
+        f_prev = f;
+        f = fn;
+        if (s2ok) {
+            const double gn = (4.0 * tj * g - sq * g_prev) * r1;
+            g_prev = g;
+            g = gn;
+            if (fabs(g) > 1e150) {
+                g *= 1e-150;
+                g_prev *= 1e-150;
+                n2s *= 1e-300;
+                spp *= 1e-300;
+                smm *= 1e-300;
+                ste *= 1e-150;
+            }
+        }
+        if (fabs(f) > 1e150) {
+            f *= 1e-150;
+            f_prev *= 1e-150;
+            n0 *= 1e-300;
+            stt *= 1e-300;
+            ste *= 1e-150;
+        }
+        sq = sq1;
+    }
+    // Both (l1 l2 l3; 000) and (l1 l2 l3; 2 -2 0) carry the sign (-1)^(l1 - l2) at
+    // l3 = l1 + l2, so the relative sign of the unnormalised product is sign(f g) there.
+    vals[0] = stt / n0;
+    vals[1] = vals[2] = vals[3] = 0.0;
+    if (s2ok) {
+        const double sgn = (f * g) < 0.0 ? -1.0 : 1.0;
+        vals[1] = sgn * ste / sqrt(n0 * n2s);
+        vals[2] = spp / n2s;
+        vals[3] = smm / n2s;
+    }
+}
+
 __global__ void __launch_bounds__(128) k_coupling(int64_t lmax, const double *__restrict__ window,
                                                   int64_t nw, int which,
                                                   double *__restrict__ blocks,
@@ -83,8 +150,7 @@ __global__ void __launch_bounds__(128) k_coupling(int64_t lmax, const double *__
     const int64_t n = lmax + 1, nn = n * n;
     const int64_t nunits = total_units(lmax);
     const int lane = threadIdx.x & 31;
-    const bool want_te = which & 2, want_pol = (which & 12) != 0, want_s2 = want_te || want_pol;
-    const double inv4pi = 1.0 / (4.0 * M_PI);
+    const bool want_s2 = (which & 14) != 0;
     for (;;) {
         unsigned long long u = 0;
         if (lane == 0) u = atomicAdd(queue, 1ull);
@@ -94,76 +160,83 @@ __global__ void __launch_bounds__(128) k_coupling(int64_t lmax, const double *__
         if (!unit_to_pair((int64_t)u, lmax, l1, l2b)) break;
         const int64_t l2 = l2b + lane;
         if (l2 <= lmax) {
-        const int64_t d = l2 - l1, jmin = d, jmax = l1 + l2;
-        const double S = (double)(l1 + l2 + 1), S2 = S * S, d2 = (double)(d * d);
-        const bool s2ok = want_s2 && l1 >= 2 && l2 >= 2;
-        double f_prev = 0.0, f = 1.0;      // (000), unnormalised
-        double g_prev = 0.0, g = 1.0;      // (2 -2 0), unnormalised
-        double sq = 0.0;                   // sqrt P(j) at the current j
-        double n0 = 0.0, n2s = 0.0, stt = 0.0, ste = 0.0, spp = 0.0, smm = 0.0;
-        for (int64_t j = jmin;; ++j) {
-            const double tj = 2.0 * (double)j + 1.0;
-            const double wj = (j < nw ? __ldg(window + j) : 0.0) * inv4pi * tj;
-            const bool even = ((j - jmin) & 1) == 0;
-            n0 += tj * f * f;
-            stt += wj * f * f;
-            if (s2ok) {
-                n2s += tj * g * g;
-                ste += wj * f * g;
-                if (even) spp += wj * g * g;
-                else smm += wj * g * g;
-            }
-            if (j == jmax) break;
-            const double j1 = (double)(j + 1);
-            const double P1 = (j1 * j1 - d2) * (S2 - j1 * j1);
-            const double r1 = rsqrt(P1);
-            const double sq1 = P1 * r1;
-            const double fn = -sq * r1 * f_prev;
-            f_prev = f;
-            f = fn;
-            if (s2ok) {
-                const double gn = (4.0 * tj * g - sq * g_prev) * r1;
-                g_prev = g;
-                g = gn;
-                if (fabs(g) > 1e150) {
-                    g *= 1e-150;
-                    g_prev *= 1e-150;
-                    n2s *= 1e-300;
-                    spp *= 1e-300;
-                    smm *= 1e-300;
-                    ste *= 1e-150;
-                }
-            }
-            if (fabs(f) > 1e150) {
-                f *= 1e-150;
-                f_prev *= 1e-150;
-                n0 *= 1e-300;
-                stt *= 1e-300;
-                ste *= 1e-150;
-            }
-            sq = sq1;
-        }
-        // Both (l1 l2 l3; 000) and (l1 l2 l3; 2 -2 0) carry the sign (-1)^(l1 - l2) at
-        // l3 = l1 + l2, so the relative sign of the unnormalised product is sign(f g) there.
-        const double tt = stt / n0;
-        double te = 0.0, pp = 0.0, mm = 0.0;
-        if (s2ok) {
-            const double sgn = (f * g) < 0.0 ? -1.0 : 1.0;
-            te = sgn * ste / sqrt(n0 * n2s);
-            pp = spp / n2s;
-            mm = smm / n2s;
-        }
-        const double c1 = 2.0 * (double)l1 + 1.0, c2 = 2.0 * (double)l2 + 1.0;
-        const double vals[4] = {tt, te, pp, mm};
+            double vals[4];
+            coupling_pair(l1, l2, window, nw, want_s2, vals);
+            const double c1 = 2.0 * (double)l1 + 1.0, c2 = 2.0 * (double)l2 + 1.0;
 #pragma unroll
-        for (int x = 0; x < 4; ++x) {
-            if (!(which & (1 << x))) continue;
-            double *bx = blocks + x * nn;
-            bx[l1 * n + l2] = c2 * vals[x];
-            bx[l2 * n + l1] = c1 * vals[x];
-        }
+            for (int x = 0; x < 4; ++x) {
+                if (!(which & (1 << x))) continue;
+                double *bx = blocks + x * nn;
+                bx[l1 * n + l2] = c2 * vals[x];
+                bx[l2 * n + l1] = c1 * vals[x];
+            }
         }
     }
+}
+
+// Scalar coupling sums S_tt(l1, l2) of an explicit list of pairs, written symmetrically
+// into the dense (lmax+1)^2 matrix S (entries not listed are left as they are).
+__global__ void k_coupling_pairs_tt(int64_t lmax, const double *__restrict__ window, int64_t nw,
+                                    const int32_t *__restrict__ pairs, int64_t npairs,
+                                    double *__restrict__ S)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= npairs) return;
+    const int64_t a = pairs[2 * t], b = pairs[2 * t + 1], n = lmax + 1;
+    const int64_t l1 = a < b ? a : b, l2 = a < b ? b : a;
+    double vals[4];
+    coupling_pair(l1, l2, window, nw, false, vals);
+    S[l1 * n + l2] = vals[0];
+    S[l2 * n + l1] = vals[0];
+}
+
+// NaMaster's Toeplitz approximation of the scalar coupling (Louis et al. 2020), filled
+// from the exact entries of S = M / (2 l' + 1) that it reads: the diagonal, column
+// l_toeplitz, columns 0..l_exact and the dl_band sub-diagonals.  With d_l = |S_ll|, the
+// correlation c_l = S(l, lt) / sqrt(d_l d_lt) and the column correlation
+// e_l = S(l, le) / sqrt(d_l d_le) (zero where d vanishes), entry (r >= q) of the lower
+// triangle is, by the first rule that applies:
+//   le <= q <= lt and r >= n - 1 - lt + q :  e_{r - q + le} sqrt(d_q d_r)
+//   1 <= r - q <= dl_band and q <= lt      :  S(q, r)
+//   r == q                                  :  S(r, r)
+//   r >= lt and q >= lt                     :  c_{(r - q + lt) mod n} sqrt(d_r d_q)
+//   r - q <= dl_band                        :  S(q, r)
+//   q <= le                                 :  S(r, q)
+//   otherwise                               :  c_{(r - q + lt) mod n} sqrt(d_r d_q)
+// and the matrix is symmetric; out(i, j) = T(i, j) (2 j + 1).
+__global__ void k_toeplitz_fill(int64_t lmax, int64_t lt, int64_t le, int64_t dlb,
+                                const double *__restrict__ S, double *__restrict__ out)
+{
+    const int64_t n = lmax + 1;
+    const int64_t i = blockIdx.y, j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const int64_t r = i > j ? i : j, q = i > j ? j : i;
+    auto d = [&](int64_t l) { return fabs(S[l * n + l]); };
+    auto corr = [&](int64_t l) {
+        const double den = sqrt(d(l) * d(lt));
+        return den > 0.0 ? S[l * n + lt] / den : 0.0;
+    };
+    auto pure = [&]() { return corr((r - q + lt) % n) * sqrt(d(r) * d(q)); };
+    double v;
+    if (q >= le && q <= lt && r >= n - 1 - lt + q) {
+        const int64_t l = r - q + le;
+        const double dl = d(l);
+        const double e = dl > 0.0 ? S[l * n + le] / sqrt(dl * d(le)) : 0.0;
+        v = e * sqrt(d(q) * d(r));
+    } else if (r - q >= 1 && r - q <= dlb && q <= lt) {
+        v = S[q * n + r];
+    } else if (r == q) {
+        v = S[r * n + r];
+    } else if (r >= lt && q >= lt) {
+        v = pure();
+    } else if (r - q <= dlb) {
+        v = S[q * n + r];
+    } else if (q <= le) {
+        v = S[r * n + q];
+    } else {
+        v = pure();
+    }
+    out[i * n + j] = v * (2.0 * (double)j + 1.0);
 }
 
 // ---------------------------------------------------------------- binning
@@ -378,6 +451,30 @@ extern "C" int gm_coupling_blocks(int64_t lmax, const double *window, int64_t nw
     k_coupling<<<nsm * 8, 128, 0, s>>>(lmax, window, nw, which, blocks,
                                        reinterpret_cast<unsigned long long *>(queue));
     return check_launch("gm_coupling_blocks");
+}
+
+extern "C" int gm_coupling_pairs_tt(int64_t lmax, const double *window, int64_t nw,
+                                    const int32_t *pairs, int64_t npairs, double *S, void *stream)
+{
+    if (lmax < 0 || nw < 0 || npairs < 0) return GM_ERR_BAD_SHAPE;
+    if (npairs == 0) return GM_OK;
+    if (!window || !pairs || !S) return GM_ERR_BAD_PTR;
+    k_coupling_pairs_tt<<<(unsigned)((npairs + 127) / 128), 128, 0, as_stream(stream)>>>(
+        lmax, window, nw, pairs, npairs, S);
+    return check_launch("gm_coupling_pairs_tt");
+}
+
+extern "C" int gm_toeplitz_fill(int64_t lmax, int64_t l_toeplitz, int64_t l_exact, int64_t dl_band,
+                                const double *S, double *out, void *stream)
+{
+    if (lmax < 1 || l_toeplitz < 1 || l_exact < 0 || dl_band < 0 || l_exact > l_toeplitz ||
+        l_toeplitz >= lmax || dl_band >= lmax || lmax >= 65535)
+        return GM_ERR_BAD_SHAPE;
+    if (!S || !out) return GM_ERR_BAD_PTR;
+    const int64_t n = lmax + 1;
+    dim3 grid((unsigned)((n + 127) / 128), (unsigned)n);
+    k_toeplitz_fill<<<grid, 128, 0, as_stream(stream)>>>(lmax, l_toeplitz, l_exact, dl_band, S, out);
+    return check_launch("gm_toeplitz_fill");
 }
 
 // Binning operators are passed in CSR form to support any NmtBin.

@@ -46,6 +46,54 @@ def coupling_blocks(window, lmax, which):
     return blocks
 
 
+def toeplitz_sanity(l_toeplitz, l_exact, dl_band, lmax):
+    """Toeplitz parameter checks of the reference (workspaces.py:1125-1138); a no-op when
+    ``l_toeplitz <= 0``."""
+    if l_toeplitz <= 0:
+        return
+    if l_exact <= 0 or dl_band < 0:
+        raise ValueError("`l_exact` and `dl_band` must be positive numbers")
+    if l_exact > l_toeplitz:
+        raise ValueError("`l_exact` must be `<= l_toeplitz")
+    if l_toeplitz >= lmax or l_exact >= lmax or dl_band >= lmax:
+        raise ValueError("`l_toeplitz`, `l_exact` and `dl_band` must be smaller than `l_max`")
+
+
+def toeplitz_exact_pairs(n, l_toeplitz, l_exact, dl_band):
+    """(npairs, 2) int32 array of the (l1 <= l2) pairs whose exact coupling the Toeplitz
+    fill reads: the diagonal, column l_toeplitz, columns 0..l_exact and the dl_band
+    off-diagonals (the pair set of workspaces.py:521-538)."""
+    ell = np.arange(n)
+    parts = [np.stack([ell, ell], 1), np.stack([ell, np.full(n, l_toeplitz)], 1)]
+    for c in range(l_exact + 1):
+        parts.append(np.stack([ell, np.full(n, c)], 1))
+    for off in range(1, dl_band + 1):
+        parts.append(np.stack([ell[: n - off], ell[: n - off] + off], 1))
+    p = np.concatenate(parts)
+    p = np.sort(p, axis=1)
+    return np.unique(p, axis=0).astype(np.int32)
+
+
+def toeplitz_fill(S, lmax, l_toeplitz, l_exact, dl_band):
+    """Toeplitz approximation (times 2 l' + 1) from a symmetric S = block / (2 l' + 1)."""
+    out = torch.empty_like(S)
+    _lib.call("gm_toeplitz_fill", lmax, l_toeplitz, l_exact, dl_band, _lib.ptr(S.contiguous()),
+              _lib.ptr(out), _lib.stream_handle(S.device))
+    return out
+
+
+def coupling_tt_toeplitz(window, lmax, l_toeplitz, l_exact, dl_band):
+    """Scalar (TT) coupling block under the Toeplitz approximation: only the entries the
+    fill reads are computed by the 3j recursion (workspaces.py:546-590)."""
+    w = as_device(window, torch.float64)
+    n = lmax + 1
+    pairs = torch.from_numpy(toeplitz_exact_pairs(n, l_toeplitz, l_exact, dl_band)).to(w.device)
+    S = torch.zeros((n, n), dtype=torch.float64, device=w.device)
+    _lib.call("gm_coupling_pairs_tt", lmax, _lib.ptr(w), w.shape[0], _lib.ptr(pairs), pairs.shape[0],
+              _lib.ptr(S), _lib.stream_handle(w.device))
+    return toeplitz_fill(S, lmax, l_toeplitz, l_exact, dl_band)
+
+
 def _which(ncls):
     return {1: 1, 2: 2, 4: 12}[ncls]
 
@@ -101,8 +149,7 @@ class NmtWorkspace:
                              f"({fl1.ainfo.lmax}) are not the same")
         if is_teb:
             raise NotImplementedError("joint TEB workspaces are not part of this build")
-        if l_toeplitz > 0:
-            raise NotImplementedError("the Toeplitz approximation is not part of this build")
+        toeplitz_sanity(l_toeplitz, l_exact, dl_band, fl1.ainfo.lmax)
         if normalization not in ("MASTER", "FKP"):
             raise ValueError(f"Unknown normalization type {normalization}. "
                              "Allowed options are 'MASTER' and 'FKP'")
@@ -124,7 +171,23 @@ class NmtWorkspace:
             self.pcl_mask = self.pcl_mask - fl1.Nw
         nw = min(self.pcl_mask.shape[0], 2 * self.lmax + 1)
         self.window = self.pcl_mask[:nw].contiguous()
-        self.mcm_blocks = coupling_blocks(self.window, self.lmax, _which(self.ncls))
+        self.l_toeplitz, self.l_exact, self.dl_band = int(l_toeplitz), int(l_exact), int(dl_band)
+        if l_toeplitz > 0 and self.ncls == 1:
+            # only the entries the Toeplitz fill reads are computed exactly
+            n = self.lmax + 1
+            self.mcm_blocks = torch.zeros((4, n, n), dtype=torch.float64, device=self.window.device)
+            self.mcm_blocks[_BLOCK_TT] = coupling_tt_toeplitz(self.window, self.lmax, l_toeplitz,
+                                                              l_exact, dl_band)
+        else:
+            self.mcm_blocks = coupling_blocks(self.window, self.lmax, _which(self.ncls))
+            if l_toeplitz > 0:
+                # polarised blocks: exact blocks, then the same Toeplitz fill
+                # (workspaces.py:1833-1844)
+                col = (2.0 * torch.arange(self.lmax + 1, dtype=torch.float64,
+                                          device=self.window.device) + 1.0)[None, :]
+                for x in ((_BLOCK_TE,) if self.ncls == 2 else (_BLOCK_PP, _BLOCK_MM)):
+                    self.mcm_blocks[x] = toeplitz_fill((self.mcm_blocks[x] / col).contiguous(),
+                                                       self.lmax, l_toeplitz, l_exact, dl_band)
         self.wawb = 0.0
         if normalization == "FKP":
             self.wawb = float((fl1.get_mask() * fl2.get_mask()).sum() * fl1.minfo.weight / (4 * np.pi))

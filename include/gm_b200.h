@@ -141,6 +141,23 @@ int gm_pseudo_cl(int64_t lmax, int64_t n1, const double *alm1, int64_t n2,
 int gm_coupling_blocks(int64_t lmax, const double *window, int64_t nw, int which,
                        double *blocks, int64_t *queue, void *stream);
 
+/* Scalar coupling sums S_tt(l1, l2) = sum_l3 (2 l3 + 1) W_l3 / (4 pi) (l1 l2 l3; 000)^2 of
+ * an explicit list of npairs (l1, l2) pairs (int32 pairs), written symmetrically into the
+ * dense (lmax+1)^2 float64 matrix S; unlisted entries are left untouched.  Computes only
+ * the entries the Toeplitz approximation reads (replaces workspaces.py:546-590
+ * `_coupling_matrix_tt_toeplitz`, with the pair set of :521-538). */
+int gm_coupling_pairs_tt(int64_t lmax, const double *window, int64_t nw, const int32_t *pairs,
+                         int64_t npairs, double *S, void *stream);
+
+/* Toeplitz approximation of the scalar coupling matrix (replaces workspaces.py:1141-1194
+ * `_apply_toeplitz`, NaMaster's Louis et al. 2020 scheme): from S holding the exact entries
+ * on the diagonal, in column l_toeplitz, in columns 0..l_exact and on the dl_band
+ * sub-diagonals, writes the full symmetric approximation times (2 l' + 1), i.e. the TT
+ * coupling block, into out ((lmax+1)^2 float64).  Requires 0 <= l_exact <= l_toeplitz < lmax
+ * and 0 <= dl_band < lmax. */
+int gm_toeplitz_fill(int64_t lmax, int64_t l_toeplitz, int64_t l_exact, int64_t dl_band,
+                     const double *S, double *out, void *stream);
+
 /* Binned coupling matrix B M diag(beam) T for ncls in {1, 2, 4} (replaces
  * workspaces.py:1570-1590 `_banded_operators` and :292-310 `_BlockMCM.banded`).
  * The binning is given in CSR form: band b holds multipoles band_ells[band_ptr[b] ..

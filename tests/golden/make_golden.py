@@ -17,6 +17,10 @@ Fixtures written:
   bins.npz       gmaster/bins.py:_linear_bands for several (lmax, nlb).
   coupling_tt.npz  tests/test_workspaces.py:_shrinking_offset_tt on seeded windows, and
                  _triangle_cuda_indexing (float64 and float32-product arms).
+  toeplitz.npz   gmaster/workspaces.py:_apply_toeplitz on exact scalar couplings and on a
+                 random symmetric matrix, and _toeplitz_exact_pairs.  _apply_toeplitz is
+                 written against jax.numpy's functional updates (``x.at[i].set(v)``); it is
+                 run here with numpy behind a minimal stand-in for those calls.
 """
 
 import ast
@@ -45,6 +49,43 @@ def extract(path, names, extra_globals=None):
         namespace.update(extra_globals)
     exec(compile(module, path, "exec"), namespace)
     return {name: namespace[name] for name in names}
+
+
+class _Updatable(np.ndarray):
+    """numpy array with jax-style functional updates: ``x.at[index].set(values)``."""
+
+    @property
+    def at(self):
+        array = self
+
+        class _Index:
+            def __getitem__(self, index):
+                class _Setter:
+                    def set(self, values):
+                        out = np.array(array, copy=True)
+                        out[index] = values
+                        return out.view(_Updatable)
+
+                return _Setter()
+
+        return _Index()
+
+
+class _NumpyAsJnp:
+    """The jax.numpy calls used by the reference's _apply_toeplitz, on numpy."""
+
+    @staticmethod
+    def asarray(x):
+        return np.asarray(x, dtype=np.float64).view(_Updatable)
+
+    def __getattr__(self, name):
+        fn = getattr(np, name)
+
+        def wrapped(*args, **kwargs):
+            out = fn(*args, **kwargs)
+            return out.view(_Updatable) if isinstance(out, np.ndarray) else out
+
+        return wrapped
 
 
 def main(ref_root):
@@ -89,6 +130,28 @@ def main(ref_root):
     coupling["tri64"] = fns["_triangle_cuda_indexing"](window, 24, use_f32=False)
     coupling["tri32"] = fns["_triangle_cuda_indexing"](window, 24, use_f32=True)
     np.savez_compressed(os.path.join(HERE, "coupling_tt.npz"), **coupling)
+
+    ws = os.path.join(ref_root, "gmaster", "workspaces.py")
+    toe = extract(ws, ["_apply_toeplitz", "_toeplitz_exact_pairs"], {"jnp": _NumpyAsJnp()})
+    toeplitz = {}
+    cases = [(31, 16, 4, 3), (40, 20, 5, 2), (12, 6, 3, 2), (25, 10, 10, 0), (30, 28, 1, 4)]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        for k, (lmax, lt, le, db) in enumerate(cases):
+            window = np.random.default_rng(40 + k).uniform(size=2 * lmax + 1)
+            cols = 2 * np.arange(lmax + 1) + 1
+            S = fns["_shrinking_offset_tt"](window, lmax) / cols[None]
+            toeplitz[f"case_{k}"] = np.array([lmax, lt, le, db], dtype=np.int64)
+            toeplitz[f"window_{k}"] = window
+            toeplitz[f"S_{k}"] = S
+            toeplitz[f"out_{k}"] = np.asarray(toe["_apply_toeplitz"](S, lt, le, db))
+            rows, columns = toe["_toeplitz_exact_pairs"](lmax + 1, lt, le, db)
+            toeplitz[f"pairs_{k}"] = np.stack([rows, columns], 1).astype(np.int64)
+        rng = np.random.default_rng(50)
+        A = rng.uniform(0.1, 1.0, size=(20, 20))
+        A = A + A.T
+        toeplitz["random_S"] = A
+        toeplitz["random_out"] = np.asarray(toe["_apply_toeplitz"](A, 9, 2, 3))
+    np.savez_compressed(os.path.join(HERE, "toeplitz.npz"), **toeplitz)
     print("wrote", sorted(os.listdir(HERE)))
 
 

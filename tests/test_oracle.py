@@ -221,3 +221,45 @@ def test_gauss_legendre_integrates_polynomials():
     x, w = oracle.gauss_legendre(33)
     for k in range(0, 65, 4):
         np.testing.assert_allclose(np.sum(w * x ** k), 2 / (k + 1), rtol=1e-13)
+
+
+def test_toeplitz_oracle_matches_reference_golden():
+    """apply_toeplitz vs the reference's _apply_toeplitz run on the same inputs
+    (tests/golden/toeplitz.npz, made by tests/golden/make_golden.py)."""
+    g = np.load("tests/golden/toeplitz.npz")
+    k = 0
+    while f"case_{k}" in g:
+        lmax, lt, le, db = (int(v) for v in g[f"case_{k}"])
+        got = oracle.apply_toeplitz(g[f"S_{k}"], lt, le, db)
+        np.testing.assert_allclose(got, g[f"out_{k}"], rtol=1e-14, atol=1e-16)
+        k += 1
+    assert k >= 5
+    got = oracle.apply_toeplitz(g["random_S"], 9, 2, 3)
+    np.testing.assert_allclose(got, g["random_out"], rtol=1e-14, atol=1e-16)
+
+
+def test_toeplitz_exact_pairs_match_reference_golden():
+    """The pair set the product computes exactly equals the reference's
+    _toeplitz_exact_pairs (as unordered pairs)."""
+    from gmaster_b200.workspaces import toeplitz_exact_pairs
+
+    g = np.load("tests/golden/toeplitz.npz")
+    k = 0
+    while f"case_{k}" in g:
+        lmax, lt, le, db = (int(v) for v in g[f"case_{k}"])
+        ref = {tuple(sorted(p)) for p in g[f"pairs_{k}"].tolist()}
+        got = {tuple(p) for p in toeplitz_exact_pairs(lmax + 1, lt, le, db).tolist()}
+        assert got == ref
+        k += 1
+
+
+def test_toeplitz_parameter_checks():
+    from gmaster_b200.workspaces import toeplitz_sanity
+
+    toeplitz_sanity(-1, -1, -1, 10)
+    with pytest.raises(ValueError):
+        toeplitz_sanity(5, 0, 2, 10)
+    with pytest.raises(ValueError):
+        toeplitz_sanity(5, 6, 2, 10)
+    with pytest.raises(ValueError):
+        toeplitz_sanity(10, 3, 2, 10)
