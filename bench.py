@@ -156,6 +156,27 @@ def make_sims(nside, nsims, seed, device):
     return t.contiguous(), qu.reshape(nsims, 2, -1).contiguous()
 
 
+# ----------------------------------------------------------------------------- ranks
+
+def max_over_ranks(value, device):
+    """Maximum of a per-rank float over all ranks of the process group (the value itself
+    when there is no group or one rank)."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def throughput(world, steps, per_step, ms):
+    """Whole-job units per second: every rank processes steps x per_step units, the job
+    lasts the slowest rank's ms."""
+    return world * steps * per_step / (ms / 1e3)
+
+
 # ----------------------------------------------------------------------------- estimator
 
 def build_workspaces(mask, nside, nlb, precision):
@@ -184,14 +205,13 @@ def estimator_step(mask, t, qu, ws, precision):
 
 
 def batch_step(mask, t, qu, ws, precision="mixed"):
-    """A batch of simulations through the Monte-Carlo batch API (shared workspaces)."""
+    """A batch of simulations through the Monte-Carlo batch API (shared workspaces):
+    fields_from_maps for T and (Q, U), compute_coupled_cells and decouple_cells, with the
+    host-to-device copy of host maps overlapping the transforms."""
     import gmaster_b200 as nmt
 
-    ft = nmt.fields_from_maps(mask, t, spin=0, n_iter=3, precision=precision)
-    fp = nmt.fields_from_maps(mask, qu, spin=2, n_iter=3, precision=precision)
-    return (nmt.decouple_cells(ws["00"], nmt.compute_coupled_cells(ft, ft)),
-            nmt.decouple_cells(ws["02"], nmt.compute_coupled_cells(ft, fp)),
-            nmt.decouple_cells(ws["22"], nmt.compute_coupled_cells(fp, fp)))
+    return nmt.mc_bandpowers(mask, t, qu, ws["00"], ws["02"], ws["22"], n_iter=3,
+                             precision=precision)
 
 
 def full_estimator(mask, t, qu, nside, nlb, precision):
@@ -390,12 +410,7 @@ def main():
             fn(i)
         end.record()
         barrier()
-        ms = start.elapsed_time(end)
-        if world > 1:
-            tt = torch.tensor([ms], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ms = float(tt.item())
-        return ms
+        return max_over_ranks(start.elapsed_time(end), dev)
 
     # device-resident value (mixed, batched), with Legendre kernel events and clocks
     for i in range(args.warmup):
@@ -420,14 +435,14 @@ def main():
     leg_ms = sum(ktime.values())
     leg_flops = sum(kflops.values())
     dominant = max(ktime, key=ktime.get)
-    value = world * args.steps * S / (ms / 1e3)
+    value = throughput(world, args.steps, S, ms)
     mixed_bp = [o[0].cpu().numpy() for o in batch_step(mask, t_all, qu_all, ws_mixed)]
 
     # plain FP64 GPU path, one simulation at a time, and the unbatched mixed path
     t0_dev, qu0_dev = t_all[:1].clone(), qu_all[0].clone()
     ms64 = timed_loop(lambda i: estimator_step(mask, t0_dev, qu0_dev, ws_fp64, "fp64"), 1,
                       args.fp64_steps)
-    value64 = world * args.fp64_steps / (ms64 / 1e3)
+    value64 = throughput(world, args.fp64_steps, 1, ms64)
     fp64_bp = [o.cpu().numpy() for o in estimator_step(mask, t0_dev, qu0_dev, ws_fp64, "fp64")]
     ms1 = timed_loop(lambda i: estimator_step(mask, t0_dev, qu0_dev, ws_mixed, "mixed"), 1, 1)
     errs = {}
@@ -459,7 +474,7 @@ def main():
                 o.cpu()
 
     ms_e2e = timed_loop(e2e_step, 1, args.steps)
-    value_e2e = world * args.steps * S / (ms_e2e / 1e3)
+    value_e2e = throughput(world, args.steps, S, ms_e2e)
 
     if rank != 0:
         if world > 1:

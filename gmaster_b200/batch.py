@@ -12,8 +12,12 @@ that loop for a whole batch at once:
 * ``compute_coupled_cells`` returns the coupled spectra of field pairs.
 * ``decouple_cells`` bins and decouples many spectra with one LU solve of many
   right-hand sides.
+* ``mc_bandpowers`` runs the whole estimator for a batch of TQU simulations; maps given
+  in (pinned) host memory are copied on a side stream, so that the copy of the (Q, U)
+  maps overlaps the T transforms.
 """
 
+import numpy as np
 import torch
 
 from . import sht, sht_tc
@@ -118,3 +122,58 @@ def decouple_cells(workspace, cls, cl_bias=None, cl_noise=None):
     sol = w._lu.solve(rhs.contiguous())                        # (nb ncls, nsims)
     out = sol.reshape(nb, w.ncls, len(cls)).permute(2, 1, 0)
     return [out[i] for i in range(len(cls))]
+
+
+_COPY_STREAMS = {}
+
+
+def _copy_stream(dev):
+    st = _COPY_STREAMS.get(dev.index)
+    if st is None:
+        st = torch.cuda.Stream(device=dev)
+        _COPY_STREAMS[dev.index] = st
+    return st
+
+
+def _upload(x, dev):
+    """Start the host-to-device copy of x on the side stream; returns (tensor, event)."""
+    if isinstance(x, torch.Tensor) and x.is_cuda:
+        return x, None
+    h = x if isinstance(x, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(x))
+    if h.dtype != torch.float64:
+        h = h.to(torch.float64)
+    side = _copy_stream(dev)
+    side.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(side):
+        d = h.to(dev, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(side)
+    d.record_stream(torch.cuda.current_stream(dev))
+    return d, ev
+
+
+def mc_bandpowers(mask, t_maps, qu_maps, w00, w02, w22, *, n_iter=None, precision=None):
+    """Bandpowers of a batch of TQU simulations sharing one mask and three workspaces.
+
+    ``t_maps`` (nsims, npix) and ``qu_maps`` (nsims, 2, npix), float64 on the device or in
+    host memory (pinned host memory lets the copies run asynchronously: the (Q, U) maps
+    are copied while the T fields are transformed).  Returns three lists over the
+    simulations: TT (1, nb); TE, TB (2, nb); EE, EB, BE, BB (4, nb) -- the per-simulation
+    result of ``w.decouple_cell(compute_coupled_cell(f1, f2))``.
+    """
+    dev = torch.device("cuda", torch.cuda.current_device())
+    mask_t = as_device(mask, torch.float64)
+    t_dev, ev_t = _upload(t_maps, dev)
+    qu_dev, ev_qu = _upload(qu_maps, dev)
+    main = torch.cuda.current_stream(dev)
+    if ev_t is not None:
+        main.wait_event(ev_t)
+    ft = fields_from_maps(mask_t, t_dev, spin=0, n_iter=n_iter, precision=precision)
+    del t_dev
+    if ev_qu is not None:
+        main.wait_event(ev_qu)
+    fp = fields_from_maps(mask_t, qu_dev, spin=2, n_iter=n_iter, precision=precision)
+    del qu_dev
+    return (decouple_cells(w00, compute_coupled_cells(ft, ft)),
+            decouple_cells(w02, compute_coupled_cells(ft, fp)),
+            decouple_cells(w22, compute_coupled_cells(fp, fp)))

@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
                         const uint32_t rowbase = b0 + (tid >> 3) * 1024 + (tid & 7) * 128;
                         const double2 *cab = sAB + t * kNB;
                         const double *cc0 = sC0 + t * kNB;
-#pragma unroll 1
+#pragma unroll 2
                         for (int cc = 0; cc < kNB / 8; ++cc) {
                             float vals[8];
 #pragma unroll
@@ -577,7 +577,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t 
             publish(cc + 1, pre);
             pre = fetch(cc + 2);
             const uint32_t b0 = tc::smem_u32(sB + st * 2 * kBTileS);
-#pragma unroll 1
+#pragma unroll 2
             for (int sub = 0; sub < kKL / 8; ++sub) {
                 float vals[2][8];
                 const int64_t lsub = (c0 + cc) * kKL + sub * 8;

@@ -103,3 +103,33 @@ def test_batch_shape_errors(cuda):
         nmt.fields_from_maps(mask, np.zeros((2, 12 * 64 + 1)))
     with pytest.raises(ValueError):
         nmt.fields_from_maps(mask, np.zeros((2, 2, 12 * 64)), spin=0)
+
+
+def test_mc_bandpowers_equals_step_by_step_api(cuda):
+    """mc_bandpowers on device maps and on pinned host maps (copied on a side stream)
+    gives the results of fields_from_maps / compute_coupled_cells / decouple_cells (to the
+    last bits: the pseudo-C_ell sums order chunks with atomics)."""
+    nside, nlb, nsims = 16, 4, 3
+    rng = np.random.default_rng(21)
+    t = torch.from_numpy(rng.normal(size=(nsims, 12 * nside ** 2)))
+    qu = torch.from_numpy(rng.normal(size=(nsims, 2, 12 * nside ** 2)))
+    mask = _mask(nside, seed=5)
+    b = nmt.NmtBin.from_nside_linear(nside, nlb)
+    f0 = nmt.NmtField(mask, None, spin=0, precision="mixed")
+    f2 = nmt.NmtField(mask, None, spin=2, precision="mixed")
+    f2.alm_mask = f0.get_mask_alms()
+    w00 = nmt.NmtWorkspace.from_fields(f0, f0, b)
+    w02 = nmt.NmtWorkspace.from_fields(f0, f2, b)
+    w22 = nmt.NmtWorkspace.from_fields(f2, f2, b)
+    ft = nmt.fields_from_maps(mask, t.cuda(), n_iter=3, precision="mixed")
+    fp = nmt.fields_from_maps(mask, qu.cuda(), n_iter=3, precision="mixed")
+    want = (nmt.decouple_cells(w00, nmt.compute_coupled_cells(ft, ft)),
+            nmt.decouple_cells(w02, nmt.compute_coupled_cells(ft, fp)),
+            nmt.decouple_cells(w22, nmt.compute_coupled_cells(fp, fp)))
+    for src in ((t.cuda(), qu.cuda()), (t.pin_memory(), qu.pin_memory())):
+        got = nmt.mc_bandpowers(mask, src[0], src[1], w00, w02, w22, n_iter=3, precision="mixed")
+        torch.cuda.synchronize()
+        for g, w in zip(got, want):
+            for gi, wi in zip(g, w):
+                np.testing.assert_allclose(gi.cpu().numpy(), wi.cpu().numpy(), rtol=1e-12,
+                                           atol=1e-12 * float(wi.abs().max()))
