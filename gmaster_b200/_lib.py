@@ -39,6 +39,8 @@ SIGNATURES = {
                                _c_vp], _c_int),
     "gm_pseudo_cl": ([_c_i64, _c_i64, _c_vp, _c_i64, _c_vp, _c_vp, _c_vp], _c_int),
     "gm_coupling_blocks": ([_c_i64, _c_vp, _c_i64, _c_int, _c_vp, _c_vp, _c_vp], _c_int),
+    "gm_coupling_units": ([_c_i64], _c_i64),
+    "gm_coupling_blocks_multi": ([_c_i64, _c_vp, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
     "gm_coupling_pairs_tt": ([_c_i64, _c_vp, _c_i64, _c_vp, _c_i64, _c_vp, _c_vp], _c_int),
     "gm_toeplitz_fill": ([_c_i64, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp], _c_int),
     "gm_bin_coupling_csr": ([_c_i64, _c_i64, _c_int, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,

@@ -12,6 +12,9 @@ that loop for a whole batch at once:
 * ``compute_coupled_cells`` returns the coupled spectra of field pairs.
 * ``decouple_cells`` bins and decouples many spectra with one LU solve of many
   right-hand sides.
+* ``workspaces_from_fields`` builds many workspaces -- of uneven lmax too -- whose
+  coupling blocks come from one persistent FP64 Wigner-3j launch sharing a device work
+  queue, instead of one launch per workspace.
 * ``mc_bandpowers`` runs the whole estimator for a batch of TQU simulations; maps given
   in (pinned) host memory are copied on a side stream, so that the copy of the (Q, U)
   maps overlaps the T transforms.
@@ -24,7 +27,7 @@ from . import sht, sht_tc
 from ._config import get_precision, nmt_params
 from .field import NmtField
 from .utils import as_device
-from .workspaces import compute_coupled_cell
+from .workspaces import NmtWorkspace, _which, compute_coupled_cell, coupling_blocks_multi
 
 
 def fields_from_maps(mask, maps, *, spin=None, n_iter=None, beam=None, lmax=None,
@@ -122,6 +125,35 @@ def decouple_cells(workspace, cls, cl_bias=None, cl_noise=None):
     sol = w._lu.solve(rhs.contiguous())                        # (nb ncls, nsims)
     out = sol.reshape(nb, w.ncls, len(cls)).permute(2, 1, 0)
     return [out[i] for i in range(len(cls))]
+
+
+def workspaces_from_fields(field_pairs, bins, **kwargs):
+    """``[NmtWorkspace.from_fields(f1, f2, b, **kwargs) for (f1, f2), b in ...]`` with all
+    coupling blocks built in one launch.
+
+    ``field_pairs`` is a list of (fl1, fl2); ``bins`` one NmtBin for every pair or a list
+    of them.  The workspaces may differ in lmax and spins.  Scalar workspaces with the
+    Toeplitz approximation keep their own launch (they compute only the entries the fill
+    reads); every other workspace takes its exact blocks from the shared launch.
+    """
+    pairs = list(field_pairs)
+    if not isinstance(bins, (list, tuple)):
+        bins = [bins] * len(pairs)
+    if len(bins) != len(pairs):
+        raise ValueError("one NmtBin per field pair is needed")
+    wss = []
+    for (f1, f2), b in zip(pairs, bins):
+        w = NmtWorkspace()
+        w._prepare(f1, f2, b, **kwargs)
+        wss.append(w)
+    shared = [w for w in wss if not (w.l_toeplitz > 0 and w.ncls == 1)]
+    blocks = coupling_blocks_multi([w.window for w in shared], [w.lmax for w in shared],
+                                   [_which(w.ncls) for w in shared])
+    given = {id(w): bl for w, bl in zip(shared, blocks)}
+    for w in wss:
+        w._compute_blocks(given.get(id(w)))
+        w._postprocess()
+    return wss
 
 
 _COPY_STREAMS = {}

@@ -65,7 +65,7 @@ __device__ __forceinline__ bool unit_to_pair(int64_t u, int64_t lmax, int64_t &l
     return true;
 }
 
-__device__ __forceinline__ int64_t total_units(int64_t lmax)
+__host__ __device__ __forceinline__ int64_t total_units(int64_t lmax)
 {
     // t in [0, lmax]: sum of floor(t/32) + 1
     const int64_t T = lmax + 1, G = T / 32, rr = T % 32;
@@ -167,6 +167,52 @@ __global__ void __launch_bounds__(128) k_coupling(int64_t lmax, const double *__
             for (int x = 0; x < 4; ++x) {
                 if (!(which & (1 << x))) continue;
                 double *bx = blocks + x * nn;
+                bx[l1 * n + l2] = c2 * vals[x];
+                bx[l2 * n + l1] = c1 * vals[x];
+            }
+        }
+    }
+}
+
+// Many coupling matrices of different lmax in one persistent launch.  Job j is the row
+// jobs[6 j .. 6 j + 5] = (lmax, window offset, nw, which, blocks offset, first unit); units
+// are numbered consecutively over the jobs (job j owns [first_j, first_{j+1}) and
+// nunits in total), the jobs being ordered by decreasing lmax so the longest recursions
+// go first.  Each warp takes the next unit from the shared queue, finds its job by binary
+// search and computes its pair block as k_coupling does.
+__global__ void __launch_bounds__(128) k_coupling_multi(int64_t njobs, const int64_t *__restrict__ jobs,
+                                                        int64_t nunits,
+                                                        const double *__restrict__ windows,
+                                                        double *__restrict__ blocks,
+                                                        unsigned long long *__restrict__ queue)
+{
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        unsigned long long u = 0;
+        if (lane == 0) u = atomicAdd(queue, 1ull);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        if ((int64_t)u >= nunits) break;
+        int64_t lo = 0, hi = njobs - 1;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi + 1) / 2;
+            if (jobs[6 * mid + 5] <= (int64_t)u) lo = mid;
+            else hi = mid - 1;
+        }
+        const int64_t *jb = jobs + 6 * lo;
+        const int64_t lmax = jb[0], n = lmax + 1, nn = n * n;
+        const int which = (int)jb[3];
+        int64_t l1, l2b;
+        if (!unit_to_pair((int64_t)u - jb[5], lmax, l1, l2b)) continue;
+        const int64_t l2 = l2b + lane;
+        if (l2 <= lmax) {
+            double vals[4];
+            coupling_pair(l1, l2, windows + jb[1], jb[2], (which & 14) != 0, vals);
+            const double c1 = 2.0 * (double)l1 + 1.0, c2 = 2.0 * (double)l2 + 1.0;
+            double *bj = blocks + jb[4];
+#pragma unroll
+            for (int x = 0; x < 4; ++x) {
+                if (!(which & (1 << x))) continue;
+                double *bx = bj + x * nn;
                 bx[l1 * n + l2] = c2 * vals[x];
                 bx[l2 * n + l1] = c1 * vals[x];
             }
@@ -451,6 +497,28 @@ extern "C" int gm_coupling_blocks(int64_t lmax, const double *window, int64_t nw
     k_coupling<<<nsm * 8, 128, 0, s>>>(lmax, window, nw, which, blocks,
                                        reinterpret_cast<unsigned long long *>(queue));
     return check_launch("gm_coupling_blocks");
+}
+
+extern "C" int64_t gm_coupling_units(int64_t lmax) { return lmax < 0 ? 0 : total_units(lmax); }
+
+extern "C" int gm_coupling_blocks_multi(int64_t njobs, const int64_t *jobs, int64_t nunits,
+                                        const double *windows, double *blocks, int64_t *queue,
+                                        void *stream)
+{
+    if (njobs < 1 || nunits < 1) return GM_ERR_BAD_SHAPE;
+    if (!jobs || !windows || !blocks || !queue) return GM_ERR_BAD_PTR;
+    cudaStream_t s = as_stream(stream);
+    cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(int64_t), s);
+    if (e != cudaSuccess) {
+        set_error("gm_coupling_blocks_multi memset", e);
+        return GM_ERR_LAUNCH;
+    }
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    k_coupling_multi<<<nsm * 8, 128, 0, s>>>(njobs, jobs, nunits, windows, blocks,
+                                             reinterpret_cast<unsigned long long *>(queue));
+    return check_launch("gm_coupling_blocks_multi");
 }
 
 extern "C" int gm_coupling_pairs_tt(int64_t lmax, const double *window, int64_t nw,

@@ -46,6 +46,43 @@ def coupling_blocks(window, lmax, which):
     return blocks
 
 
+def coupling_blocks_multi(windows, lmaxs, whiches):
+    """Coupling blocks of many workspaces of different lmax in one persistent launch.
+
+    ``windows`` is a list of float64 device mask spectra, ``lmaxs`` and ``whiches`` the
+    lmax and block mask of each workspace.  Returns a list of (4, lmax+1, lmax+1) blocks,
+    bit-identical to ``coupling_blocks`` of each workspace in turn (unused blocks are
+    zero).  The jobs are queued by decreasing lmax so the longest recursions start first.
+    """
+    if len(windows) == 0:
+        return []
+    dev = windows[0].device
+    order = sorted(range(len(windows)), key=lambda i: -int(lmaxs[i]))
+    rows, wparts, woff, boff, first = [], [], 0, 0, 0
+    offsets = [None] * len(windows)
+    for i in order:
+        w = as_device(windows[i], torch.float64).contiguous()
+        lmax = int(lmaxs[i])
+        n = lmax + 1
+        rows.append([lmax, woff, w.shape[0], int(whiches[i]), boff, first])
+        offsets[i] = boff
+        wparts.append(w)
+        woff += w.shape[0]
+        boff += 4 * n * n
+        first += int(_lib.load().gm_coupling_units(lmax))
+    jobs = torch.tensor(rows, dtype=torch.int64).to(dev)
+    allw = torch.cat(wparts) if woff else torch.zeros(1, dtype=torch.float64, device=dev)
+    blocks = torch.zeros(boff, dtype=torch.float64, device=dev)
+    queue = torch.zeros(1, dtype=torch.int64, device=dev)
+    _lib.call("gm_coupling_blocks_multi", len(rows), _lib.ptr(jobs), first, _lib.ptr(allw),
+              _lib.ptr(blocks), _lib.ptr(queue), _lib.stream_handle(dev))
+    out = []
+    for i in range(len(windows)):
+        n = int(lmaxs[i]) + 1
+        out.append(blocks[offsets[i]:offsets[i] + 4 * n * n].view(4, n, n))
+    return out
+
+
 def toeplitz_sanity(l_toeplitz, l_exact, dl_band, lmax):
     """Toeplitz parameter checks of the reference (workspaces.py:1125-1138); a no-op when
     ``l_toeplitz <= 0``."""
@@ -142,6 +179,13 @@ class NmtWorkspace:
 
     def compute_coupling_matrix(self, fl1, fl2, bins, is_teb=False, l_toeplitz=-1, l_exact=-1,
                                 dl_band=-1, normalization="MASTER"):
+        self._prepare(fl1, fl2, bins, is_teb, l_toeplitz, l_exact, dl_band, normalization)
+        self._compute_blocks()
+        self._postprocess()
+
+    def _prepare(self, fl1, fl2, bins, is_teb=False, l_toeplitz=-1, l_exact=-1, dl_band=-1,
+                 normalization="MASTER"):
+        """Checks, mask pseudo-spectrum and normalisation: everything but the blocks."""
         if not fl1.is_compatible(fl2, strict=False):
             raise ValueError("Fields have incompatible pixelizations")
         if fl1.ainfo.lmax != bins.lmax:
@@ -172,26 +216,33 @@ class NmtWorkspace:
         nw = min(self.pcl_mask.shape[0], 2 * self.lmax + 1)
         self.window = self.pcl_mask[:nw].contiguous()
         self.l_toeplitz, self.l_exact, self.dl_band = int(l_toeplitz), int(l_exact), int(dl_band)
-        if l_toeplitz > 0 and self.ncls == 1:
+        self.wawb = 0.0
+        if normalization == "FKP":
+            self.wawb = float((fl1.get_mask() * fl2.get_mask()).sum() * fl1.minfo.weight / (4 * np.pi))
+
+    def _compute_blocks(self, blocks=None):
+        """Coupling blocks, or the exact ``blocks`` given (from a multi-workspace launch),
+        then the Toeplitz fill when it is enabled."""
+        l_toeplitz, l_exact, dl_band = self.l_toeplitz, self.l_exact, self.dl_band
+        if blocks is not None:
+            self.mcm_blocks = blocks
+        elif l_toeplitz > 0 and self.ncls == 1:
             # only the entries the Toeplitz fill reads are computed exactly
             n = self.lmax + 1
             self.mcm_blocks = torch.zeros((4, n, n), dtype=torch.float64, device=self.window.device)
             self.mcm_blocks[_BLOCK_TT] = coupling_tt_toeplitz(self.window, self.lmax, l_toeplitz,
                                                               l_exact, dl_band)
+            return
         else:
             self.mcm_blocks = coupling_blocks(self.window, self.lmax, _which(self.ncls))
-            if l_toeplitz > 0:
-                # polarised blocks: exact blocks, then the same Toeplitz fill
-                # (workspaces.py:1833-1844)
-                col = (2.0 * torch.arange(self.lmax + 1, dtype=torch.float64,
-                                          device=self.window.device) + 1.0)[None, :]
-                for x in ((_BLOCK_TE,) if self.ncls == 2 else (_BLOCK_PP, _BLOCK_MM)):
-                    self.mcm_blocks[x] = toeplitz_fill((self.mcm_blocks[x] / col).contiguous(),
-                                                       self.lmax, l_toeplitz, l_exact, dl_band)
-        self.wawb = 0.0
-        if normalization == "FKP":
-            self.wawb = float((fl1.get_mask() * fl2.get_mask()).sum() * fl1.minfo.weight / (4 * np.pi))
-        self._postprocess()
+        if l_toeplitz > 0:
+            # exact blocks, then the Toeplitz fill (workspaces.py:1833-1844)
+            col = (2.0 * torch.arange(self.lmax + 1, dtype=torch.float64,
+                                      device=self.window.device) + 1.0)[None, :]
+            slots = {1: (_BLOCK_TT,), 2: (_BLOCK_TE,), 4: (_BLOCK_PP, _BLOCK_MM)}[self.ncls]
+            for x in slots:
+                self.mcm_blocks[x] = toeplitz_fill((self.mcm_blocks[x] / col).contiguous(),
+                                                   self.lmax, l_toeplitz, l_exact, dl_band)
 
     def _postprocess(self):
         dev = self.mcm_blocks.device

@@ -141,6 +141,20 @@ int gm_pseudo_cl(int64_t lmax, int64_t n1, const double *alm1, int64_t n2,
 int gm_coupling_blocks(int64_t lmax, const double *window, int64_t nw, int which,
                        double *blocks, int64_t *queue, void *stream);
 
+/* Work units of gm_coupling_blocks for one lmax (a unit is one l1 and 32 consecutive l2). */
+int64_t gm_coupling_units(int64_t lmax);
+
+/* Coupling blocks of many workspaces of different lmax in one persistent launch (the
+ * uneven-workspace batch; the reference builds each workspace separately,
+ * workspaces.py:1760-1912).  Job j is the row jobs[6j .. 6j+5] of a device int64 table:
+ * (lmax, offset of its window in `windows`, nw, which, offset of its (4, lmax+1, lmax+1)
+ * blocks in `blocks`, index of its first unit); units number consecutively over the jobs
+ * (gm_coupling_units(lmax_j) each, nunits in total).  Order the jobs by decreasing lmax so
+ * the longest recursions start first.  The caller zeroes `blocks`; `queue` is one int64
+ * the kernel uses as its counter (zeroed by this call). */
+int gm_coupling_blocks_multi(int64_t njobs, const int64_t *jobs, int64_t nunits,
+                             const double *windows, double *blocks, int64_t *queue, void *stream);
+
 /* Scalar coupling sums S_tt(l1, l2) = sum_l3 (2 l3 + 1) W_l3 / (4 pi) (l1 l2 l3; 000)^2 of
  * an explicit list of npairs (l1, l2) pairs (int32 pairs), written symmetrically into the
  * dense (lmax+1)^2 float64 matrix S; unlisted entries are left untouched.  Computes only

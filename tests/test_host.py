@@ -102,6 +102,13 @@ def test_cabi_library_exports_every_header_symbol():
     lib.gm_ring_twiddle_count.restype = ctypes.c_int64
     lib.gm_ring_twiddle_count.argtypes = [ctypes.c_int64]
     assert lib.gm_ring_twiddle_count(2048) == 2048 * 2049
+    # coupling work units: one per l1 and 32 consecutive l2 >= l1
+    lib.gm_coupling_units.restype = ctypes.c_int64
+    lib.gm_coupling_units.argtypes = [ctypes.c_int64]
+    for lmax in (0, 1, 31, 32, 33, 95, 767, 6143):
+        want = sum((lmax - l1) // 32 + 1 for l1 in range(lmax + 1))
+        assert lib.gm_coupling_units(lmax) == want, lmax
+    assert lib.gm_coupling_units(-1) == 0
 
 
 def test_python_binding_covers_header():
