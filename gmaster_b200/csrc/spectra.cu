@@ -72,74 +72,111 @@ __host__ __device__ __forceinline__ int64_t total_units(int64_t lmax)
     return 16 * G * (G + 1) + rr * (G + 1);
 }
 
-// One thread per (l1 <= l2) pair: three-term recursion in l3 (Schulten & Gordon 1975)
-// for (l3 l1 l2; 0 2 -2) = (l1 l2 l3; 2 -2 0), and the two-term ratio for (l1 l2 l3; 000),
-// both unnormalised from l3 = l2 - l1 and normalised by sum (2 l3 + 1) f^2 = 1.
 // Coupling sums of one pair (l1 <= l2): vals[x] = S_x(l1, l2) for x = tt, te, pp, mm,
-// S_x = sum_l3 (2 l3 + 1) W_l3 / (4 pi) T_x(l1, l2, l3) (the blocks divided by 2 l2 + 1).
-__device__ void coupling_pair(int64_t l1, int64_t l2, const double *__restrict__ window, int64_t nw,
-                              bool want_s2, double (&vals)[4])
+// S_x = sum_l3 (2 l3 + 1) W_l3 / (4 pi) T_x(l1, l2, l3) (the blocks divided by 2 l2 + 1),
+// with T_tt = (l1 l2 l3; 000)^2, T_te = (000)(2 -2 0), T_pp / T_mm = (2 -2 0)^2 on the
+// l1 + l2 + l3 even / odd terms.
+//
+// Recurrences in j = l3 from j_min = l2 - l1 to j_max = l1 + l2 (Schulten & Gordon 1975,
+// m3 = 0): with P(j) = (j^2 - d^2)(S^2 - j^2), d = l2 - l1, S = l1 + l2 + 1,
+//   sqrt P(j+1) f_{j+1} = -sqrt P(j) f_{j-1}                    for (000)
+//   sqrt P(j+1) g_{j+1} = 4 (2j+1) g_j - sqrt P(j) g_{j-1}      for (2 -2 0),
+// both unnormalised from f = g = 1 at j_min and normalised by sum (2j+1) f^2 = 1.  The
+// substitution f^_j = f_j s_j, g^_j = g_j s_j with s_j = prod_{i <= j} sqrt P(i) removes
+// every square root and division:
+//   f^_{j+1} = -P(j) f^_{j-1},   g^_{j+1} = 4 (2j+1) g^_j - P(j) g^_{j-1},
+// and f^2, f g, g^2 become the hatted products over D_j = prod_{i <= j} P(i).  Each sum
+// sum_j c_j X^_j / D_j is carried as A / D_j with A_j = A_{j-1} P(j) + c_j X^_j (Horner
+// form); D cancels in every quotient of the results, so it is never formed.  The odd-offset
+// (000) terms vanish, so the loop steps j by two.  The products grow by ~P^2 per step;
+// whenever a normalising sum passes 2^512 its family is scaled down by an exact power of
+// two (f^ or g^ by 2^-256, their squared sums by 2^-512).
+template <bool TT, bool TE, bool PM>
+__device__ __forceinline__ void coupling_sums(int64_t l1, int64_t l2, const double *__restrict__ window,
+                                              int64_t nw, double (&vals)[4])
 {
+    constexpr bool F = TT || TE, G = TE || PM;
     const double inv4pi = 1.0 / (4.0 * M_PI);
     const int64_t d = l2 - l1, jmin = d, jmax = l1 + l2;
     const double S = (double)(l1 + l2 + 1), S2 = S * S, d2 = (double)(d * d);
-    const bool s2ok = want_s2 && l1 >= 2 && l2 >= 2;
-    double f_prev = 0.0, f = 1.0;      // (000), unnormalised
-    double g_prev = 0.0, g = 1.0;      // (2 -2 0), unnormalised
-    double sq = 0.0;                   // sqrt P(j) at the current j
-    double n0 = 0.0, n2s = 0.0, stt = 0.0, ste = 0.0, spp = 0.0, smm = 0.0;
-    for (int64_t j = jmin;; ++j) {
-        const double tj = 2.0 * (double)j + 1.0;
-        const double wj = (j < nw ? __ldg(window + j) : 0.0) * inv4pi * tj;
-        const bool even = ((j - jmin) & 1) == 0;
-        n0 += tj * f * f;
-        stt += wj * f * f;
-        if (s2ok) {
-            n2s += tj * g * g;
-            ste += wj * f * g;
-            if (even) spp += wj * g * g;
-            else smm += wj * g * g;
+    const double lo = 0x1p-256, lo2 = 0x1p-512;
+    const int big = (1023 + 512) << 20;  // high word of 2^512
+    const double t0 = 2.0 * (double)jmin + 1.0;
+    const double w0 = (jmin < nw ? __ldg(window + jmin) : 0.0) * t0;
+    double f0 = 1.0, g0 = 1.0, gm1 = 0.0, P0 = 0.0;
+    double an0 = t0, att = w0, an2 = t0, ate = w0, app = w0, amm = 0.0;
+    double jd = (double)jmin;
+    for (int64_t j = jmin; j < jmax; j += 2) {
+        const double j1 = jd + 1.0, j2 = jd + 2.0;
+        const double P1 = fma(j1, j1, -d2) * fma(-j1, j1, S2);
+        const double P2 = fma(j2, j2, -d2) * fma(-j2, j2, S2);
+        const double t1 = 2.0 * j1 + 1.0, t2 = 2.0 * j2 + 1.0;
+        const double w2 = (j + 2 < nw ? __ldg(window + j + 2) : 0.0) * t2;
+        const double PP = P1 * P2;
+        double f2 = 0.0, g2 = 0.0;
+        if (F) {
+            f2 = -P1 * f0;
+            const double ff2 = f2 * f2;
+            an0 = fma(an0, PP, t2 * ff2);
+            if (TT) att = fma(att, PP, w2 * ff2);
         }
-        if (j == jmax) break;
-        const double j1 = (double)(j + 1);
-        const double P1 = (j1 * j1 - d2) * (S2 - j1 * j1);
-        const double r1 = rsqrt(P1);
-        const double sq1 = P1 * r1;
-        const double fn = -sq * r1 * f_prev;
-        f_prev = f;
-        f = fn;
-        if (s2ok) {
-            const double gn = (4.0 * tj * g - sq * g_prev) * r1;
-            g_prev = g;
-            g = gn;
-            if (fabs(g) > 1e150) {
-                g *= 1e-150;
-                g_prev *= 1e-150;
-                n2s *= 1e-300;
-                spp *= 1e-300;
-                smm *= 1e-300;
-                ste *= 1e-150;
+        if (G) {
+            const double g1 = fma(4.0 * (2.0 * jd + 1.0), g0, -P0 * gm1);
+            g2 = fma(4.0 * t1, g1, -P1 * g0);
+            const double gg1 = g1 * g1, gg2 = g2 * g2;
+            an2 = fma(fma(an2, P1, t1 * gg1), P2, t2 * gg2);
+            if (PM) {
+                const double w1 = (j + 1 < nw ? __ldg(window + j + 1) : 0.0) * t1;
+                app = fma(app, PP, w2 * gg2);
+                amm = fma(amm, P1, w1 * gg1) * P2;
             }
+            if (TE) ate = fma(ate, PP, w2 * f2 * g2);
+            gm1 = g1;
+            g0 = g2;
         }
-        if (fabs(f) > 1e150) {
-            f *= 1e-150;
-            f_prev *= 1e-150;
-            n0 *= 1e-300;
-            stt *= 1e-300;
-            ste *= 1e-150;
+        f0 = f2;
+        P0 = P2;
+        jd = j2;
+        if (F && __double2hiint(an0) > big) {
+            f0 *= lo;
+            an0 *= lo2;
+            att *= lo2;
+            ate *= lo;
         }
-        sq = sq1;
+        if (G && __double2hiint(an2) > big) {
+            g0 *= lo;
+            gm1 *= lo;
+            an2 *= lo2;
+            app *= lo2;
+            amm *= lo2;
+            ate *= lo;
+        }
     }
-    // Both (l1 l2 l3; 000) and (l1 l2 l3; 2 -2 0) carry the sign (-1)^(l1 - l2) at
-    // l3 = l1 + l2, so the relative sign of the unnormalised product is sign(f g) there.
-    vals[0] = stt / n0;
-    vals[1] = vals[2] = vals[3] = 0.0;
-    if (s2ok) {
-        const double sgn = (f * g) < 0.0 ? -1.0 : 1.0;
-        vals[1] = sgn * ste / sqrt(n0 * n2s);
-        vals[2] = spp / n2s;
-        vals[3] = smm / n2s;
+    if (TT) vals[0] = inv4pi * att / an0;
+    if (TE) {
+        // (000) and (2 -2 0) both carry (-1)^(l1 - l2) at l3 = l1 + l2, so the relative
+        // sign of the unnormalised product is sign(f g) there.
+        const double sgn = (f0 * g0) < 0.0 ? -1.0 : 1.0;
+        vals[1] = sgn * inv4pi * ate / (sqrt(an0) * sqrt(an2));
     }
+    if (PM) {
+        vals[2] = inv4pi * app / an2;
+        vals[3] = inv4pi * amm / an2;
+    }
+}
+
+// Coupling sums of the blocks `which` asks for (bit x = block x); the others are zero.
+// Spin-2 sums vanish unless l1, l2 >= 2.
+__device__ __forceinline__ void coupling_pair(int64_t l1, int64_t l2, const double *__restrict__ window,
+                                              int64_t nw, int which, double (&vals)[4])
+{
+    vals[0] = vals[1] = vals[2] = vals[3] = 0.0;
+    const bool s2ok = l1 >= 2 && l2 >= 2;
+    const int w = s2ok ? which : (which & 1);
+    if (w == 1) coupling_sums<true, false, false>(l1, l2, window, nw, vals);
+    else if (w == 2) coupling_sums<false, true, false>(l1, l2, window, nw, vals);
+    else if (w == 4 || w == 8 || w == 12) coupling_sums<false, false, true>(l1, l2, window, nw, vals);
+    else if (w != 0) coupling_sums<true, true, true>(l1, l2, window, nw, vals);
 }
 
 __global__ void __launch_bounds__(128) k_coupling(int64_t lmax, const double *__restrict__ window,
@@ -150,7 +187,6 @@ __global__ void __launch_bounds__(128) k_coupling(int64_t lmax, const double *__
     const int64_t n = lmax + 1, nn = n * n;
     const int64_t nunits = total_units(lmax);
     const int lane = threadIdx.x & 31;
-    const bool want_s2 = (which & 14) != 0;
     for (;;) {
         unsigned long long u = 0;
         if (lane == 0) u = atomicAdd(queue, 1ull);
@@ -161,7 +197,7 @@ __global__ void __launch_bounds__(128) k_coupling(int64_t lmax, const double *__
         const int64_t l2 = l2b + lane;
         if (l2 <= lmax) {
             double vals[4];
-            coupling_pair(l1, l2, window, nw, want_s2, vals);
+            coupling_pair(l1, l2, window, nw, which, vals);
             const double c1 = 2.0 * (double)l1 + 1.0, c2 = 2.0 * (double)l2 + 1.0;
 #pragma unroll
             for (int x = 0; x < 4; ++x) {
@@ -206,7 +242,7 @@ __global__ void __launch_bounds__(128) k_coupling_multi(int64_t njobs, const int
         const int64_t l2 = l2b + lane;
         if (l2 <= lmax) {
             double vals[4];
-            coupling_pair(l1, l2, windows + jb[1], jb[2], (which & 14) != 0, vals);
+            coupling_pair(l1, l2, windows + jb[1], jb[2], which, vals);
             const double c1 = 2.0 * (double)l1 + 1.0, c2 = 2.0 * (double)l2 + 1.0;
             double *bj = blocks + jb[4];
 #pragma unroll
@@ -231,7 +267,7 @@ __global__ void k_coupling_pairs_tt(int64_t lmax, const double *__restrict__ win
     const int64_t a = pairs[2 * t], b = pairs[2 * t + 1], n = lmax + 1;
     const int64_t l1 = a < b ? a : b, l2 = a < b ? b : a;
     double vals[4];
-    coupling_pair(l1, l2, window, nw, false, vals);
+    coupling_pair(l1, l2, window, nw, 1, vals);
     S[l1 * n + l2] = vals[0];
     S[l2 * n + l1] = vals[0];
 }
