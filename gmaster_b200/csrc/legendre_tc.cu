@@ -38,6 +38,9 @@ constexpr int kTmemCols = 512;         // TMEM columns: the hi*hi and the cross 
 constexpr int kNB = 64;                // analysis l-tile (MMA N)
 constexpr int kKC = 128;               // analysis lanes per group (MMA K per group)
 constexpr int kLT = 256;               // synthesis lanes per CTA (MMA N)
+constexpr int kGenS = kLT;             // synthesis generator threads (8 warps, one lane each)
+constexpr int kThreadsS = kGenS + 32;  // + the producer / MMA warp
+constexpr int kMmaWarpS = kGenS / 32;  // warp index of the synthesis producer / MMA warp
 constexpr int kKL = 64;                // synthesis l-chunk (MMA K per chunk)
 constexpr uint32_t kAImg = 128u * kKC * 2u;        // one plane of an analysis A image (32 KB)
 constexpr uint32_t kBTileA = kNB * kKC * 2u;       // one plane of an analysis B tile (16 KB)
@@ -141,6 +144,7 @@ struct Params {
 };
 
 __device__ __forceinline__ void gen_barrier() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+__device__ __forceinline__ void gen_barrier_s() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 
 __device__ __forceinline__ double sgn_of(int sp) { return sp > 0 ? 1.0 : (sp < 0 ? -1.0 : 0.0); }
 
@@ -443,7 +447,7 @@ struct __align__(8) SynShared {
 // almT images: chunk cc of order m covers l in [64 (c0(m) + cc), +64), c0(m) = floor(l0(m)/64);
 // image index = choff[m] + cc.
 template <int SPIN>
-__global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t *__restrict__ simg,
+__global__ void __launch_bounds__(kThreadsS, 1) k_syn_tc(Params p, const uint8_t *__restrict__ simg,
                                                         const int64_t *__restrict__ choff,
                                                         float *__restrict__ synd, int R2,
                                                         int *__restrict__ err)
@@ -468,14 +472,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t 
         for (int i = 0; i < 2; ++i) {
             tc::mbar_init(&sh.a_full[i], 1);
             tc::mbar_init(&sh.a_free[i], 1);
-            tc::mbar_init(&sh.b_full[i], 4);
+            tc::mbar_init(&sh.b_full[i], kGenS / 32);
             tc::mbar_init(&sh.b_free[i], 1);
         }
         tc::mbar_init(&sh.d_full, 1);
         sh.abort = 0;
         tc::fence_mbar_init();
     }
-    if (warp == 4) {
+    if (warp == kMmaWarpS) {
         tc::tmem_alloc(&sh.tmem, kTmemCols);
         tc::tmem_relinquish();
     }
@@ -486,7 +490,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t 
     volatile int *abort = &sh.abort;
     const uint8_t *img = simg + choff[m] * 2 * (int64_t)kSImg;
 
-    if (warp == 4) {
+    if (warp == kMmaWarpS) {
         if (lane == 0) {
             const uint32_t idesc = tc::idesc_f16(128, kLT, 0, 1, 0);
             tc::mbar_arrive_expect_tx(&sh.a_full[0], 2 * kSImg);
@@ -527,23 +531,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t 
     } else {
         const double sgn_c = sgn_of(p.sp);
         const int64_t mb = alm_idx(p.lmax, 0, m);
-        double x[2], v[2], vp[2];
-        int k[2];
-        bool valid[2];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int64_t jl = tile * kLT + h * kGen + tid;
-            valid[h] = jl < p.nlanes;
-            x[h] = valid[h] ? p.geom[jl] : 0.0;
-            v[h] = vp[h] = 0.0;
-            k[h] = 0;
-            if (valid[h])
-                seed_lane(p.seeds + ((int64_t)p.var * L + m) * 4, p.geom[p.nlanes + jl],
-                          p.geom[2 * p.nlanes + jl], v[h], k[h]);
-        }
-        bool emit[2];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) emit[h] = (k[h] == 0);
+        // one lane (northern ring) per generator thread
+        const int64_t jl = tile * kLT + tid;
+        const bool valid = jl < p.nlanes;
+        const double x = valid ? p.geom[jl] : 0.0;
+        double v = 0.0, vp = 0.0;
+        int k = 0;
+        if (valid)
+            seed_lane(p.seeds + ((int64_t)p.var * L + m) * 4, p.geom[p.nlanes + jl],
+                      p.geom[2 * p.nlanes + jl], v, k);
+        bool emit = (k == 0);
         // Coefficients of chunk cc sit in shared stage cc & 1.  Threads tid < kKL load the
         // chunk two ahead into registers while the current one is generated, and publish
         // the next one right after the barrier that frees its stage.
@@ -567,7 +564,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t 
             const uint32_t st = (uint32_t)cc & 1;
             double2 *cab = sAB + st * kKL;
             double *cc0 = sC0 + st * kKL;
-            gen_barrier();   // stage st is complete; stage st ^ 1 (chunk cc - 1) is free
+            gen_barrier_s();   // stage st is complete; stage st ^ 1 (chunk cc - 1) is free
             // after a timed-out wait a generator keeps meeting the barrier every chunk (the
             // loop is bounded) but does no more work
             if (dead || !wait_or_abort(&sh.b_free[st], ((uint32_t)(cc >> 1) & 1) ^ 1, abort, err)) {
@@ -579,65 +576,54 @@ __global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t 
             const uint32_t b0 = tc::smem_u32(sB + st * 2 * kBTileS);
 #pragma unroll 2
             for (int sub = 0; sub < kKL / 8; ++sub) {
-                float vals[2][8];
+                float vals[8];
                 const int64_t lsub = (c0 + cc) * kKL + sub * 8;
                 if (lsub > l0) {   // rows past lmax have zero coefficients and emit zeros
 #pragma unroll
                     for (int e = 0; e < 8; ++e) {
                         const double2 ab = cab[sub * 8 + e];
-                        const double cs = SPIN ? cc0[sub * 8 + e] : 0.0;
-#pragma unroll
-                        for (int h = 0; h < 2; ++h) {
-                            const double nv = fma(ab.x * (SPIN ? x[h] - cs : x[h]), v[h], -ab.y * vp[h]);
-                            vp[h] = v[h];
-                            v[h] = nv;
-                            vals[h][e] = emit[h] ? (float)v[h] : 0.0f;
-                        }
+                        const double xs = SPIN ? x - cc0[sub * 8 + e] : x;
+                        const double nv = fma(ab.x * xs, v, -ab.y * vp);
+                        vp = v;
+                        v = nv;
+                        vals[e] = emit ? (float)v : 0.0f;
                     }
                 } else {
 #pragma unroll
                     for (int e = 0; e < 8; ++e) {
                         const int64_t l = lsub + e;
-                        const bool adv = l > l0 && l < L;
                         const double2 ab = cab[sub * 8 + e];
-                        const double cs = SPIN ? cc0[sub * 8 + e] : 0.0;
-#pragma unroll
-                        for (int h = 0; h < 2; ++h) {
-                            if (adv) {
-                                const double nv = fma(ab.x * (SPIN ? x[h] - cs : x[h]), v[h], -ab.y * vp[h]);
-                                vp[h] = v[h];
-                                v[h] = nv;
-                            }
-                            vals[h][e] = (l >= l0 && l < L && emit[h]) ? (float)v[h] : 0.0f;
+                        const double xs = SPIN ? x - cc0[sub * 8 + e] : x;
+                        if (l > l0 && l < L) {
+                            const double nv = fma(ab.x * xs, v, -ab.y * vp);
+                            vp = v;
+                            v = nv;
                         }
+                        vals[e] = (l >= l0 && l < L && emit) ? (float)v : 0.0f;
                     }
                 }
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    rescale(v[h], vp[h], k[h]);
-                    emit[h] = (k[h] == 0);
-                }
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    uint4 hi, lo;
-                    pack8(vals[h], hi, lo);
-                    const uint32_t row = h * kGen + tid;
-                    const uint32_t off = (row >> 3) * 1024 + (row & 7) * 128 + (((uint32_t)sub ^ (row & 7)) << 4);
-                    sts128(b0 + off, hi);
-                    sts128(b0 + kBTileS + off, lo);
-                }
+                rescale(v, vp, k);
+                emit = (k == 0);
+                uint4 hi, lo;
+                pack8(vals, hi, lo);
+                const uint32_t row = tid;
+                const uint32_t off = (row >> 3) * 1024 + (row & 7) * 128 + (((uint32_t)sub ^ (row & 7)) << 4);
+                sts128(b0 + off, hi);
+                sts128(b0 + kBTileS + off, lo);
             }
             tc::fence_async_smem();
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(&sh.b_full[st]);
         }
-        // epilogue: D[row, lane] -> synd[m][lane][row]
+        // epilogue: D[row, lane] -> synd[m][lane][row]; a warp reads the TMEM lanes
+        // 32 (warp % 4) + [0, 32) (rows), the two warpgroups split the columns (lanes)
         if (!dead && wait_or_abort(&sh.d_full, 0, abort, err)) {
             tc::tc_fence_after();
-            const int row = warp * 32 + lane;
-            for (int cb = 0; cb < kLT; cb += 16) {
+            const int wq = warp & 3, row = wq * 32 + lane;
+            const int cbeg = (warp >> 2) * (kLT / 2);
+            for (int cb = cbeg; cb < cbeg + kLT / 2; cb += 16) {
                 uint32_t r[16], rx[16];
-                const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb;
+                const uint32_t trow = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)cb;
                 tc::tmem_ld16(trow, r);
                 tc::tmem_ld16(trow + kLT, rx);
                 tc::tmem_ld_wait();
@@ -655,7 +641,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_syn_tc(Params p, const uint8_t 
     }
     tc::tc_fence_before();
     __syncthreads();
-    if (warp == 4) tc::tmem_dealloc(tmem, kTmemCols);
+    if (warp == kMmaWarpS) tc::tmem_dealloc(tmem, kTmemCols);
 }
 
 // ------------------------------------------------------------------------------- tables
@@ -1171,7 +1157,7 @@ extern "C" int gm_tc_synthesis(int64_t nside, int64_t lmax, int spin, int sp, in
     Params p = make_params(nside, lmax, spin, sp, ncomp, geom, seeds, coef, out_scale);
     const int R2 = 2 * p.H;
     dim3 grid((unsigned)((p.nlanes + kLT - 1) / kLT), (unsigned)(lmax + 1));
-    kern<<<grid, kThreads, smem, as_stream(stream)>>>(p, (const uint8_t *)simg, choff, synd, R2,
+    kern<<<grid, kThreadsS, smem, as_stream(stream)>>>(p, (const uint8_t *)simg, choff, synd, R2,
                                                      (int *)err);
     return check_launch("gm_tc_synthesis");
 }
