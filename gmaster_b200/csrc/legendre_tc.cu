@@ -12,10 +12,10 @@
 // the hemisphere parity and accumulates in FP64.
 //
 // Analysis (map -> alm): D[row, l] = sum_lanes rhs[row, lane] lambda_l(lane).  One
-// persistent CTA per order m at a time walks l in superblocks of 256 (two 256-column
-// accumulators fill the 512 TMEM columns) and, inside a superblock, the lanes in groups
-// of 128 (K); the recurrence state of every lane is carried across superblocks in a
-// caller-provided scratch buffer.
+// persistent CTA per order m at a time walks l in superblocks of 256 (two 128-row tiles,
+// each with a hi x hi and a cross-product accumulator of 128 columns: the 512 TMEM
+// columns) and, inside a superblock, the lanes in groups of 128 (K); the recurrence state
+// of every lane is carried across superblocks in a caller-provided scratch buffer.
 //
 // Synthesis (alm -> ring coefficients): D[row, lane] = sum_l almT[row, l] lambda_l(lane).
 // One CTA per (order m, tile of 256 lanes) walks l in chunks of 64 (K).
@@ -35,7 +35,7 @@ constexpr int kGen = 128;              // generator threads (4 warps)
 constexpr int kThreads = kGen + 32;    // + one warp for the producer / MMA issuer
 constexpr int kSB = 256;               // analysis superblock (l per D accumulator)
 constexpr int kTmemCols = 512;         // TMEM columns: the hi*hi and the cross accumulators
-constexpr int kNB = 64;                // analysis l-tile (MMA N)
+constexpr int kNB = 128;               // analysis l-tile (MMA N of the hi x hi product)
 constexpr int kKC = 128;               // analysis lanes per group (MMA K per group)
 constexpr int kLT = 256;               // synthesis lanes per CTA (MMA N)
 constexpr int kGenS = kLT;             // synthesis generator threads (8 warps, one lane each)
@@ -43,7 +43,7 @@ constexpr int kThreadsS = kGenS + 32;  // + the producer / MMA warp
 constexpr int kMmaWarpS = kGenS / 32;  // warp index of the synthesis producer / MMA warp
 constexpr int kKL = 64;                // synthesis l-chunk (MMA K per chunk)
 constexpr uint32_t kAImg = 128u * kKC * 2u;        // one plane of an analysis A image (32 KB)
-constexpr uint32_t kBTileA = kNB * kKC * 2u;       // one plane of an analysis B tile (16 KB)
+constexpr uint32_t kBTileA = kNB * kKC * 2u;       // one plane of an analysis B tile (32 KB)
 constexpr uint32_t kSImg = 128u * kKL * 2u;        // one plane of a synthesis A image (16 KB)
 constexpr uint32_t kBTileS = kLT * kKL * 2u;       // one plane of a synthesis B tile (32 KB)
 constexpr double kBig = 2.037035976334486e90;      // 2^300
@@ -184,9 +184,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t base = (tc::smem_u32(smem_raw) + 1023u) & ~1023u;
     uint8_t *smem = smem_raw + (base - tc::smem_u32(smem_raw));
-    uint8_t *sA = smem;                      // 2 x 64 KB
-    uint8_t *sB = smem + 4 * kAImg;          // 2 x 32 KB
-    double2 *sAB = reinterpret_cast<double2 *>(smem + 4 * kAImg + 4 * kBTileA);   // (alpha, beta) x kSB
+    uint8_t *sA = smem;                      // right-hand-side image, hi and lo planes (64 KB)
+    uint8_t *sB = smem + 2 * kAImg;          // 2 stages of generated tiles, hi and lo (2 x 64 KB)
+    double2 *sAB = reinterpret_cast<double2 *>(smem + 2 * kAImg + 4 * kBTileA);   // (alpha, beta) x kSB
     double *sC0 = reinterpret_cast<double *>(sAB + kSB);                          // c0 x kSB (spin 2)
     const int64_t L = p.lmax + 1, NG = (p.nlanes + kKC - 1) / kKC;
     const int64_t G = gridDim.x, c = blockIdx.x;
@@ -217,11 +217,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
     if (warp == 4) {
         // ------------------------------------------------ producer + MMA issuer
         if (lane == 0) {
-            const uint32_t idesc = tc::idesc_f16(128, kNB, 0, 1, 1);
+            // The first MMA of a K step multiplies the hi image by the hi and lo generated
+            // planes at once (N = 2 kNB: they sit side by side in the tile), writing the
+            // hi x hi half and the hi x lo half of the tile's accumulator; the second adds
+            // lo x hi into the cross half.  Reading the image once for both products keeps
+            // the tensor core's shared-memory traffic, which stalls the generators' own
+            // shared-memory accesses, down.
+            const uint32_t idesc_cat = tc::idesc_f16(128, 2 * kNB, 0, 1, 1);
+            const uint32_t idesc_hi = tc::idesc_f16(128, kNB, 0, 1, 1);
             uint32_t j = 0, u = 0, q = 0;   // job, B-tile and superblock counters
             // job list: (slot i -> m, superblock s, group g)
             auto job_m = [&](int64_t i) { return snake_m(i, c, G); };
-            // prefetch the first job
             int64_t i = 0, s = 0, g = 0;
             bool have = job_m(i) <= p.lmax;
             if (have) {
@@ -237,48 +243,44 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
                 if (ng == NG) { ng = 0; ++ns; }
                 if (ns == nsb) { ns = 0; ++ni; }
                 const bool next = job_m(ni) <= p.lmax;
-                const uint32_t buf = j & 1;
-                if (!wait_or_abort(&sh.a_full[buf], (j >> 1) & 1, abort, err)) break;
+                if (!wait_or_abort(&sh.a_full[0], j & 1, abort, err)) break;
                 if (g == 0 && !wait_or_abort(&sh.d_free, (q & 1) ^ 1, abort, err)) break;
                 tc::tc_fence_after();
-                const uint32_t a0 = tc::smem_u32(sA + buf * 2 * kAImg);
+                const uint32_t a0 = tc::smem_u32(sA);
                 for (int t = 0; t < kSB / kNB; ++t, ++u) {
                     const uint32_t st = u & 1;
                     if (!wait_or_abort(&sh.b_full[st], (u >> 1) & 1, abort, err)) break;
                     tc::tc_fence_after();
                     const uint32_t b0 = tc::smem_u32(sB + st * 2 * kBTileA);
-                    // hi*hi into D_hh (columns [0, kSB)), hi*lo + lo*hi into D_x
-                    // (columns [kSB, 2 kSB)): the tensor-core accumulation rounds toward
-                    // zero, so its relative bias grows with the number of MMAs chained into
-                    // one accumulator; D_x is 2^-11 smaller and its bias is negligible.
-                    const uint32_t dh = tmem + t * kNB, dx = tmem + kSB + t * kNB;
+                    // tile t owns the columns [2 kNB t, 2 kNB (t + 1)): hi x hi first, then the
+                    // cross products.  The tensor-core accumulation rounds toward zero, so its
+                    // relative bias grows with the number of MMAs chained into one accumulator;
+                    // the cross half is 2^-11 smaller and its bias is negligible.
+                    const uint32_t dh = tmem + t * 2 * kNB, dx = dh + kNB;
                     const uint32_t acc = g > 0 ? 1u : 0u;
 #pragma unroll
                     for (int ks = 0; ks < kKC / 16; ++ks) {
                         const uint64_t ah = tc::desc_sw128_mn(a0 + ks * 4096, 1024, 2048);
                         const uint64_t al = tc::desc_sw128_mn(a0 + kAImg + ks * 4096, 1024, 2048);
-                        const uint64_t bh = tc::desc_sw128_mn(b0 + ks * 2048, 1024, 1024);
-                        const uint64_t bl = tc::desc_sw128_mn(b0 + kBTileA + ks * 2048, 1024, 1024);
-                        tc::mma_f16(dh, ah, bh, idesc, (acc || ks > 0) ? 1u : 0u);
-                        tc::mma_f16(dx, ah, bl, idesc, (acc || ks > 0) ? 1u : 0u);
-                        tc::mma_f16(dx, al, bh, idesc, 1u);
+                        const uint64_t bt = tc::desc_sw128_mn(b0 + ks * 8192, 1024, 4096);
+                        tc::mma_f16(dh, ah, bt, idesc_cat, (acc || ks > 0) ? 1u : 0u);
+                        tc::mma_f16(dx, al, bt, idesc_hi, 1u);
                     }
                     tc::mma_commit(&sh.b_free[st]);
-                    // with the first tile's MMAs queued, refill the other image buffer once
-                    // the previous job's MMAs (which read it) are done
-                    if (t == 0 && next) {
-                        const uint32_t nb = (j + 1) & 1;
-                        if (!wait_or_abort(&sh.a_free[nb], (((j + 1) >> 1) & 1) ^ 1, abort, err)) break;
-                        tc::mbar_arrive_expect_tx(&sh.a_full[nb], 2 * kAImg);
-                        tc::bulk_g2s(sA + nb * 2 * kAImg, aimg + ((job_m(ni) * NG + ng) * 2) * (int64_t)kAImg,
-                                     2 * kAImg, &sh.a_full[nb]);
-                    }
                 }
                 if (*abort) break;
-                tc::mma_commit(&sh.a_free[buf]);
+                tc::mma_commit(&sh.a_free[0]);
                 if (g == NG - 1) {
                     tc::mma_commit(&sh.d_full);
                     ++q;
+                }
+                if (next) {
+                    // one image buffer: refill it once this job's MMAs have read it (the
+                    // generators run ahead into the free tile stages meanwhile)
+                    if (!wait_or_abort(&sh.a_free[0], j & 1, abort, err)) break;
+                    tc::mbar_arrive_expect_tx(&sh.a_full[0], 2 * kAImg);
+                    tc::bulk_g2s(sA, aimg + ((job_m(ni) * NG + ng) * 2) * (int64_t)kAImg, 2 * kAImg,
+                                 &sh.a_full[0]);
                 }
                 ++j;
                 i = ni;
@@ -361,11 +363,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
                             dead = true;
                             break;
                         }
+                        // tile layout: MN-major, 128-byte swizzle, 256 MN rows = kNB hi rows
+                        // then kNB lo rows (sw128_mn_offset(256, r, lane)); a thread writes
+                        // 8 consecutive rows of its lane as one 16-byte store per plane
                         const uint32_t b0 = tc::smem_u32(sB + st * 2 * kBTileA);
-                        const uint32_t rowbase = b0 + (tid >> 3) * 1024 + (tid & 7) * 128;
+                        const uint32_t rowbase = b0 + (tid >> 3) * 4096 + (tid & 7) * 128;
                         const double2 *cab = sAB + t * kNB;
                         const double *cc0 = sC0 + t * kNB;
-#pragma unroll 2
+#pragma unroll 8
                         for (int cc = 0; cc < kNB / 8; ++cc) {
                             float vals[8];
 #pragma unroll
@@ -381,9 +386,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
                             emit = (k == 0);
                             uint4 hi, lo;
                             pack8(vals, hi, lo);
-                            const uint32_t off = ((cc ^ (tid & 7)) << 4);
+                            const uint32_t off = (cc >> 3) * 1024 + (((cc & 7) ^ (tid & 7)) << 4);
                             sts128(rowbase + off, hi);
-                            sts128(rowbase + kBTileA + off, lo);
+                            sts128(rowbase + 2048 + off, lo);
                         }
                         tc::fence_async_smem();
                         __syncwarp();
@@ -407,9 +412,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
                 const bool parity_row = row >= p.H;
                 for (int cb = 0; cb < kSB; cb += 16) {
                     uint32_t r[16], rx[16];
-                    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb;
+                    // column cb of the superblock: tile cb / kNB, hi x hi half then cross half
+                    const uint32_t col = (uint32_t)((cb / kNB) * 2 * kNB + cb % kNB);
+                    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16) + col;
                     tc::tmem_ld16(trow, r);
-                    tc::tmem_ld16(trow + kSB, rx);
+                    tc::tmem_ld16(trow + kNB, rx);
                     tc::tmem_ld_wait();
                     if (rvalid) {
 #pragma unroll
@@ -1107,7 +1114,7 @@ extern "C" int gm_tc_analysis(int64_t nside, int64_t lmax, int spin, int sp, int
         return GM_ERR_BAD_SHAPE;
     if ((spin == 0) != (sp == 0) || (spin == 2 && sp != 2 && sp != -2)) return GM_ERR_BAD_SHAPE;
     if (!geom || !seeds || !coef || !img || !alm_i || !scratch || !err) return GM_ERR_BAD_PTR;
-    const size_t smem = 4 * kAImg + 4 * kBTileA + kSB * (sizeof(double2) + sizeof(double)) + 1024;
+    const size_t smem = 2 * kAImg + 4 * kBTileA + kSB * (sizeof(double2) + sizeof(double)) + 1024;
     auto kern = spin == 0 ? k_ana_tc<0> : k_ana_tc<2>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) {
