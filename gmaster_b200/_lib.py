@@ -65,6 +65,16 @@ SIGNATURES = {
     "gm_tc_fold": ([_c_i64, _c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl,
                     _c_vp], _c_int),
     "gm_tc_synd_to_syn": ([_c_i64, _c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
+    "gm_tc_pack_window": ([_c_i64, _c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_i64,
+                           _c_i64, _c_vp], _c_int),
+    "gm_tc_analysis_window": ([_c_i64, _c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
+                               _c_dbl, _c_vp, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp], _c_int),
+    "gm_tc_prep_syn_window": ([_c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_i64, _c_dbl, _c_i64,
+                               _c_i64, _c_vp], _c_int),
+    "gm_tc_synthesis_window": ([_c_i64, _c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
+                                _c_vp, _c_dbl, _c_i64, _c_i64, _c_vp, _c_vp], _c_int),
+    "gm_tc_synd_to_syn_window": ([_c_i64, _c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_i64, _c_i64,
+                                  _c_vp], _c_int),
     "gm_tc_alm_layout": ([_c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_int, _c_vp], _c_int),
     "gm_tc_selftest": ([_c_i64, _c_i64, _c_int, _c_int, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
 }

@@ -141,6 +141,7 @@ struct Params {
     const double *seeds;  // (3, L, 4)
     const double *coef;   // (nelem, 4) for this spin: alpha, beta, c0, 0
     int var;              // seed variant 0 / 1 / 2
+    int64_t mbeg, mend;   // orders handled, [mbeg, mend); images and outputs are indexed by m - mbeg
 };
 
 __device__ __forceinline__ void gen_barrier() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
@@ -227,12 +228,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
             const uint32_t idesc_hi = tc::idesc_f16(128, kNB, 0, 1, 1);
             uint32_t j = 0, u = 0, q = 0;   // job, B-tile and superblock counters
             // job list: (slot i -> m, superblock s, group g)
-            auto job_m = [&](int64_t i) { return snake_m(i, c, G); };
+            auto job_m = [&](int64_t i) { return p.mbeg + snake_m(i, c, G); };
             int64_t i = 0, s = 0, g = 0;
-            bool have = job_m(i) <= p.lmax;
+            bool have = job_m(i) < p.mend;
             if (have) {
                 tc::mbar_arrive_expect_tx(&sh.a_full[0], 2 * kAImg);
-                tc::bulk_g2s(sA, aimg + ((job_m(i) * NG + g) * 2) * (int64_t)kAImg, 2 * kAImg, &sh.a_full[0]);
+                tc::bulk_g2s(sA, aimg + (((job_m(i) - p.mbeg) * NG + g) * 2) * (int64_t)kAImg, 2 * kAImg,
+                             &sh.a_full[0]);
             }
             while (have && !*abort) {
                 const int64_t m = job_m(i);
@@ -242,7 +244,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
                 int64_t ni = i, ns = s, ng = g + 1;
                 if (ng == NG) { ng = 0; ++ns; }
                 if (ns == nsb) { ns = 0; ++ni; }
-                const bool next = job_m(ni) <= p.lmax;
+                const bool next = job_m(ni) < p.mend;
                 if (!wait_or_abort(&sh.a_full[0], j & 1, abort, err)) break;
                 if (g == 0 && !wait_or_abort(&sh.d_free, (q & 1) ^ 1, abort, err)) break;
                 tc::tc_fence_after();
@@ -279,7 +281,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
                     // generators run ahead into the free tile stages meanwhile)
                     if (!wait_or_abort(&sh.a_free[0], j & 1, abort, err)) break;
                     tc::mbar_arrive_expect_tx(&sh.a_full[0], 2 * kAImg);
-                    tc::bulk_g2s(sA, aimg + ((job_m(ni) * NG + ng) * 2) * (int64_t)kAImg, 2 * kAImg,
+                    tc::bulk_g2s(sA, aimg + (((job_m(ni) - p.mbeg) * NG + ng) * 2) * (int64_t)kAImg, 2 * kAImg,
                                  &sh.a_full[0]);
                 }
                 ++j;
@@ -299,8 +301,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
         // thread can wait on a barrier that its peers have left.
         bool dead = false;
         for (int64_t i = 0;; ++i) {
-            const int64_t m = snake_m(i, c, G);
-            if (m > p.lmax) break;
+            const int64_t m = p.mbeg + snake_m(i, c, G);
+            if (m >= p.mend) break;
             const int64_t l0 = m > l0min ? m : l0min;
             const int64_t nsb = (L - l0 + kSB - 1) / kSB;
             const int64_t mb = alm_idx(p.lmax, 0, m);   // coefficient / alm base of order m
@@ -469,7 +471,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) k_syn_tc(Params p, const uint8_t
     double2 *sAB = reinterpret_cast<double2 *>(smem + 4 * kSImg + 4 * kBTileS);   // 2 x kKL (alpha, beta)
     double *sC0 = reinterpret_cast<double *>(sAB + 2 * kKL);                      // 2 x kKL c0
     const int64_t L = p.lmax + 1;
-    const int64_t m = blockIdx.y, tile = blockIdx.x;
+    const int64_t m = p.mbeg + blockIdx.y, tile = blockIdx.x;
     const int l0min = abs(p.sp);
     const int64_t l0 = m > l0min ? m : l0min;
     if (l0 > p.lmax) return;
@@ -495,7 +497,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) k_syn_tc(Params p, const uint8_t
     tc::tc_fence_after();
     const uint32_t tmem = sh.tmem;
     volatile int *abort = &sh.abort;
-    const uint8_t *img = simg + choff[m] * 2 * (int64_t)kSImg;
+    const uint8_t *img = simg + (choff[m] - choff[p.mbeg]) * 2 * (int64_t)kSImg;
 
     if (warp == kMmaWarpS) {
         if (lane == 0) {
@@ -639,7 +641,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) k_syn_tc(Params p, const uint8_t
                     for (int e = 0; e < 16; ++e) {
                         const int64_t jl = tile * kLT + cb + e;
                         if (jl < p.nlanes)
-                            synd[(m * p.nlanes + jl) * R2 + row] =
+                            synd[((m - p.mbeg) * p.nlanes + jl) * R2 + row] =
                                 (__uint_as_float(r[e]) + __uint_as_float(rx[e])) * (float)p.scale;
                     }
                 }
@@ -724,11 +726,12 @@ __global__ void __launch_bounds__(128) k_pack_tc(int64_t nside, int64_t L, int n
                                                  const float2 *__restrict__ spec,
                                                  float4 *__restrict__ rhs_map,
                                                  uint8_t *__restrict__ img_a,
-                                                 uint8_t *__restrict__ img_b, float scale)
+                                                 uint8_t *__restrict__ img_b, float scale,
+                                                 int64_t mbeg, int64_t mend)
 {
     __shared__ float4 tile[kPackM][64];
     const int64_t nlanes = 2 * nside, nring = 4 * nside - 1, NG = (nlanes + kKC - 1) / kKC;
-    const int64_t m0 = (int64_t)blockIdx.x * kPackM, j = blockIdx.y;
+    const int64_t m0 = mbeg + (int64_t)blockIdx.x * kPackM, j = blockIdx.y;
     const int tid = threadIdx.x;
     const bool two = j != nlanes - 1;
     const int64_t rn = north_ring(j), rs = two ? south_ring(nside, j) : 0;
@@ -739,7 +742,7 @@ __global__ void __launch_bounds__(128) k_pack_tc(int64_t nside, int64_t L, int n
         if (hemi < 2) {
             for (int c = 0; c < ncomp; ++c) {
                 float2 v = make_float2(0.f, 0.f);
-                if (m < L && (hemi == 0 || two))
+                if (m < mend && (hemi == 0 || two))
                     v = spec[((int64_t)c * nring + (hemi ? rs : rn)) * L + m];
                 float *t = reinterpret_cast<float *>(&tile[mi][c]);
                 t[2 * hemi] = v.x;
@@ -751,15 +754,15 @@ __global__ void __launch_bounds__(128) k_pack_tc(int64_t nside, int64_t L, int n
     for (int e = tid; e < kPackM * ncomp; e += blockDim.x) {
         const int mi = e / ncomp, c = e % ncomp;
         const int64_t m = m0 + mi;
-        if (m < L) rhs_map[(m * nlanes + j) * ncomp + c] = tile[mi][c];
+        if (m < mend && rhs_map) rhs_map[(m * nlanes + j) * ncomp + c] = tile[mi][c];
     }
     const int H = spin == 0 ? 2 * ncomp : ncomp;
     const uint32_t roff = tc::sw128_mn_offset(128, (uint32_t)tid, (uint32_t)(j % kKC));
     const int64_t g = j / kKC;
     for (int mi = 0; mi < kPackM; ++mi) {
         const int64_t m = m0 + mi;
-        if (m >= L) break;
-        const int64_t base = (m * NG + g) * 2 * (int64_t)kAImg + roff;
+        if (m >= mend) break;
+        const int64_t base = ((m - mbeg) * NG + g) * 2 * (int64_t)kAImg + roff;
         put_f16(img_a + base, kAImg, image_row(tile[mi], spin, H, tid, 0) * scale);
         if (spin) put_f16(img_b + base, kAImg, image_row(tile[mi], spin, H, tid, 1) * scale);
     }
@@ -770,9 +773,9 @@ __global__ void __launch_bounds__(128) k_pack_tc(int64_t nside, int64_t L, int n
 // (src row r); variant +2 (lambda-): [-2a | s 2a] (src r < H ? H + r : r - H); s = (-1)^(l+m).
 __global__ void k_prep_syn(int64_t lmax, int spin, int sp, int H, int NR,
                            const double *__restrict__ alm_i, const int64_t *__restrict__ choff,
-                           uint8_t *__restrict__ simg, double scale)
+                           uint8_t *__restrict__ simg, double scale, int64_t mbeg)
 {
-    const int64_t m = blockIdx.y, L = lmax + 1;
+    const int64_t m = mbeg + blockIdx.y, L = lmax + 1;
     const int l0min = abs(sp);
     const int64_t l0 = m > l0min ? m : l0min;
     if (l0 > lmax) return;
@@ -804,7 +807,7 @@ __global__ void k_prep_syn(int64_t lmax, int spin, int sp, int H, int NR,
             }
             v[e] = val;
         }
-        uint8_t *img = simg + (choff[m] + cc) * 2 * (int64_t)kSImg;
+        uint8_t *img = simg + (choff[m] - choff[mbeg] + cc) * 2 * (int64_t)kSImg;
         uint4 hi, lo;
         pack8(v, hi, lo);
         const uint32_t off = tc::sw128_mn_offset(128, (uint32_t)r0, (uint32_t)kl);
@@ -984,14 +987,14 @@ __global__ void k_alm_layout(int64_t nelem, int spin, int nfield, double *__rest
 
 // Tensor-core synthesis output -> per-comp ring coefficients in the lane layout
 // syn (L, nlanes, ncomp, 4) float [north re, im, south re, im] used by gm_ring_synthesis.
-__global__ void k_synd_to_syn(int64_t nlanes, int64_t L, int ncomp, int spin,
+__global__ void k_synd_to_syn(int64_t nlanes, int64_t nm, int ncomp, int spin,
                               const float *__restrict__ synd_a, const float *__restrict__ synd_b,
-                              int R2, float *__restrict__ syn)
+                              int R2, float *__restrict__ syn, int64_t mbeg)
 {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= L * nlanes * ncomp) return;
+    if (idx >= nm * nlanes * ncomp) return;
     const int c = (int)(idx % ncomp);
-    const int64_t ml = idx / ncomp;   // m * nlanes + lane
+    const int64_t ml = idx / ncomp;   // (m - mbeg) * nlanes + lane
     const int H = R2 / 2;
     const float *a = synd_a + ml * R2;
     float4 o;
@@ -1007,7 +1010,7 @@ __global__ void k_synd_to_syn(int64_t nlanes, int64_t L, int ncomp, int spin,
         else
             o = make_float4(-0.5f * (v1.y - u1.y), 0.5f * (v1.x - u1.x), -0.5f * (u2.y - v2.y), 0.5f * (u2.x - v2.x));
     }
-    reinterpret_cast<float4 *>(syn)[idx] = o;
+    reinterpret_cast<float4 *>(syn)[mbeg * nlanes * ncomp + idx] = o;
 }
 
 }  // namespace ltc
@@ -1060,28 +1063,44 @@ static int tc_shape_ok(int spin, int64_t ncomp)
     return 0;
 }
 
-extern "C" int gm_tc_pack(int64_t nside, int64_t lmax, int spin, int64_t ncomp, const void *ringspec,
-                          void *rhs_map, void *img_a, void *img_b, double img_scale, void *stream)
+static bool window_ok(int64_t lmax, int64_t mbeg, int64_t mend)
 {
-    if (nside < 1 || lmax < 0 || !tc_shape_ok(spin, ncomp) || !(img_scale > 0.0)) return GM_ERR_BAD_SHAPE;
-    if (!ringspec || !rhs_map || !img_a || (spin && !img_b)) return GM_ERR_BAD_PTR;
+    return mbeg >= 0 && mbeg < mend && mend <= lmax + 1;
+}
+
+extern "C" int gm_tc_pack_window(int64_t nside, int64_t lmax, int spin, int64_t ncomp,
+                                 const void *ringspec, void *rhs_map, void *img_a, void *img_b,
+                                 double img_scale, int64_t mbeg, int64_t mend, void *stream)
+{
+    if (nside < 1 || lmax < 0 || !tc_shape_ok(spin, ncomp) || !(img_scale > 0.0) ||
+        !window_ok(lmax, mbeg, mend))
+        return GM_ERR_BAD_SHAPE;
+    if (!ringspec || !img_a || (spin && !img_b)) return GM_ERR_BAD_PTR;
     const int64_t NG = gm_tc_lane_groups(nside);
     cudaStream_t s = as_stream(stream);
     // the kernel writes every row of every lane; only the padding lanes of a last, partial
     // group (nside not a multiple of 64) need clearing
     if (NG * kKC != 2 * nside) {
-        const size_t bytes = (size_t)(lmax + 1) * NG * 2 * kAImg;
+        const size_t bytes = (size_t)(mend - mbeg) * NG * 2 * kAImg;
         if (cudaMemsetAsync(img_a, 0, bytes, s) != cudaSuccess ||
             (spin && cudaMemsetAsync(img_b, 0, bytes, s) != cudaSuccess)) {
             set_error("gm_tc_pack memset", cudaGetLastError());
             return GM_ERR_LAUNCH;
         }
     }
-    dim3 grid((unsigned)((lmax + 1 + kPackM - 1) / kPackM), (unsigned)(2 * nside));
+    dim3 grid((unsigned)((mend - mbeg + kPackM - 1) / kPackM), (unsigned)(2 * nside));
     k_pack_tc<<<grid, 128, 0, s>>>(nside, lmax + 1, (int)ncomp, spin, (const float2 *)ringspec,
                                    (float4 *)rhs_map, (uint8_t *)img_a, (uint8_t *)img_b,
-                                   (float)img_scale);
+                                   (float)img_scale, mbeg, mend);
     return check_launch("gm_tc_pack");
+}
+
+extern "C" int gm_tc_pack(int64_t nside, int64_t lmax, int spin, int64_t ncomp, const void *ringspec,
+                          void *rhs_map, void *img_a, void *img_b, double img_scale, void *stream)
+{
+    if (!rhs_map) return GM_ERR_BAD_PTR;
+    return gm_tc_pack_window(nside, lmax, spin, ncomp, ringspec, rhs_map, img_a, img_b, img_scale, 0,
+                             lmax + 1, stream);
 }
 
 static Params make_params(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
@@ -1102,15 +1121,19 @@ static Params make_params(int64_t nside, int64_t lmax, int spin, int sp, int64_t
     p.seeds = seeds;
     p.coef = coef;
     p.var = sp == 0 ? 0 : (sp < 0 ? 1 : 2);
+    p.mbeg = 0;
+    p.mend = lmax + 1;
     return p;
 }
 
-extern "C" int gm_tc_analysis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
-                              const double *geom, const double *seeds, const double *coef,
-                              const void *img, double *alm_i, double scale, double *scratch,
-                              int64_t nctas, int32_t *err, void *stream)
+extern "C" int gm_tc_analysis_window(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                                     const double *geom, const double *seeds, const double *coef,
+                                     const void *img, double *alm_i, double scale, double *scratch,
+                                     int64_t nctas, int64_t mbeg, int64_t mend, int32_t *err,
+                                     void *stream)
 {
-    if (nside < 1 || lmax < 2 || !tc_shape_ok(spin, ncomp) || nctas < 1 || nctas > 4096)
+    if (nside < 1 || lmax < 2 || !tc_shape_ok(spin, ncomp) || nctas < 1 || nctas > 4096 ||
+        !window_ok(lmax, mbeg, mend))
         return GM_ERR_BAD_SHAPE;
     if ((spin == 0) != (sp == 0) || (spin == 2 && sp != 2 && sp != -2)) return GM_ERR_BAD_SHAPE;
     if (!geom || !seeds || !coef || !img || !alm_i || !scratch || !err) return GM_ERR_BAD_PTR;
@@ -1122,16 +1145,28 @@ extern "C" int gm_tc_analysis(int64_t nside, int64_t lmax, int spin, int sp, int
         return GM_ERR_LAUNCH;
     }
     Params p = make_params(nside, lmax, spin, sp, ncomp, geom, seeds, coef, scale);
+    p.mbeg = mbeg;
+    p.mend = mend;
     kern<<<(unsigned)nctas, kThreads, smem, as_stream(stream)>>>(p, (const uint8_t *)img, alm_i,
                                                                 scratch, (int *)err);
     return check_launch("gm_tc_analysis");
 }
 
-extern "C" int gm_tc_prep_syn(int64_t lmax, int spin, int sp, int64_t ncomp, const double *alm_i,
-                              const int64_t *choff, void *simg, int64_t simg_bytes, double alm_scale,
-                              void *stream)
+extern "C" int gm_tc_analysis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                              const double *geom, const double *seeds, const double *coef,
+                              const void *img, double *alm_i, double scale, double *scratch,
+                              int64_t nctas, int32_t *err, void *stream)
 {
-    if (lmax < 2 || !tc_shape_ok(spin, ncomp) || !(alm_scale > 0.0)) return GM_ERR_BAD_SHAPE;
+    return gm_tc_analysis_window(nside, lmax, spin, sp, ncomp, geom, seeds, coef, img, alm_i, scale,
+                                 scratch, nctas, 0, lmax + 1, err, stream);
+}
+
+extern "C" int gm_tc_prep_syn_window(int64_t lmax, int spin, int sp, int64_t ncomp, const double *alm_i,
+                                     const int64_t *choff, void *simg, int64_t simg_bytes,
+                                     double alm_scale, int64_t mbeg, int64_t mend, void *stream)
+{
+    if (lmax < 2 || !tc_shape_ok(spin, ncomp) || !(alm_scale > 0.0) || !window_ok(lmax, mbeg, mend))
+        return GM_ERR_BAD_SHAPE;
     if (!alm_i || !choff || !simg) return GM_ERR_BAD_PTR;
     const int H = spin == 0 ? (int)(2 * ncomp) : (int)ncomp;
     const int NR = spin == 0 ? H : 2 * H;
@@ -1141,17 +1176,28 @@ extern "C" int gm_tc_prep_syn(int64_t lmax, int spin, int sp, int64_t ncomp, con
         set_error("gm_tc_prep_syn memset", e);
         return GM_ERR_LAUNCH;
     }
-    k_prep_syn<<<dim3(16, (unsigned)(lmax + 1)), 256, 0, s>>>(lmax, spin, sp, H, NR, alm_i, choff,
-                                                             (uint8_t *)simg, alm_scale);
+    k_prep_syn<<<dim3(16, (unsigned)(mend - mbeg)), 256, 0, s>>>(lmax, spin, sp, H, NR, alm_i, choff,
+                                                                (uint8_t *)simg, alm_scale, mbeg);
     return check_launch("gm_tc_prep_syn");
 }
 
-extern "C" int gm_tc_synthesis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
-                               const double *geom, const double *seeds, const double *coef,
-                               const void *simg, const int64_t *choff, float *synd, double out_scale,
-                               int32_t *err, void *stream)
+extern "C" int gm_tc_prep_syn(int64_t lmax, int spin, int sp, int64_t ncomp, const double *alm_i,
+                              const int64_t *choff, void *simg, int64_t simg_bytes, double alm_scale,
+                              void *stream)
 {
-    if (nside < 1 || lmax < 2 || !tc_shape_ok(spin, ncomp) || !(out_scale > 0.0)) return GM_ERR_BAD_SHAPE;
+    return gm_tc_prep_syn_window(lmax, spin, sp, ncomp, alm_i, choff, simg, simg_bytes, alm_scale, 0,
+                                 lmax + 1, stream);
+}
+
+extern "C" int gm_tc_synthesis_window(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                                      const double *geom, const double *seeds, const double *coef,
+                                      const void *simg, const int64_t *choff, float *synd,
+                                      double out_scale, int64_t mbeg, int64_t mend, int32_t *err,
+                                      void *stream)
+{
+    if (nside < 1 || lmax < 2 || !tc_shape_ok(spin, ncomp) || !(out_scale > 0.0) ||
+        !window_ok(lmax, mbeg, mend))
+        return GM_ERR_BAD_SHAPE;
     if ((spin == 0) != (sp == 0) || (spin == 2 && sp != 2 && sp != -2)) return GM_ERR_BAD_SHAPE;
     if (!geom || !seeds || !coef || !simg || !choff || !synd || !err) return GM_ERR_BAD_PTR;
     const size_t smem = 4 * kSImg + 4 * kBTileS + 2 * kKL * (sizeof(double2) + sizeof(double)) + 1024;
@@ -1162,11 +1208,22 @@ extern "C" int gm_tc_synthesis(int64_t nside, int64_t lmax, int spin, int sp, in
         return GM_ERR_LAUNCH;
     }
     Params p = make_params(nside, lmax, spin, sp, ncomp, geom, seeds, coef, out_scale);
+    p.mbeg = mbeg;
+    p.mend = mend;
     const int R2 = 2 * p.H;
-    dim3 grid((unsigned)((p.nlanes + kLT - 1) / kLT), (unsigned)(lmax + 1));
+    dim3 grid((unsigned)((p.nlanes + kLT - 1) / kLT), (unsigned)(mend - mbeg));
     kern<<<grid, kThreadsS, smem, as_stream(stream)>>>(p, (const uint8_t *)simg, choff, synd, R2,
                                                      (int *)err);
     return check_launch("gm_tc_synthesis");
+}
+
+extern "C" int gm_tc_synthesis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                               const double *geom, const double *seeds, const double *coef,
+                               const void *simg, const int64_t *choff, float *synd, double out_scale,
+                               int32_t *err, void *stream)
+{
+    return gm_tc_synthesis_window(nside, lmax, spin, sp, ncomp, geom, seeds, coef, simg, choff, synd,
+                                  out_scale, 0, lmax + 1, err, stream);
 }
 
 extern "C" int gm_tc_fold(int64_t nside, int64_t lmax, int spin, int64_t ncomp, const float *synd_a,
@@ -1195,16 +1252,24 @@ extern "C" int gm_tc_alm_layout(int64_t lmax, int spin, int64_t nfield, double *
     return check_launch("gm_tc_alm_layout");
 }
 
+extern "C" int gm_tc_synd_to_syn_window(int64_t nside, int64_t lmax, int spin, int64_t ncomp,
+                                        const float *synd_a, const float *synd_b, float *syn,
+                                        int64_t mbeg, int64_t mend, void *stream)
+{
+    if (nside < 1 || lmax < 2 || !tc_shape_ok(spin, ncomp) || !window_ok(lmax, mbeg, mend))
+        return GM_ERR_BAD_SHAPE;
+    if (!synd_a || (spin && !synd_b) || !syn) return GM_ERR_BAD_PTR;
+    const int H = spin == 0 ? (int)(2 * ncomp) : (int)ncomp;
+    const int64_t tot = (mend - mbeg) * 2 * nside * ncomp;
+    k_synd_to_syn<<<(unsigned)((tot + 255) / 256), 256, 0, as_stream(stream)>>>(
+        2 * nside, mend - mbeg, (int)ncomp, spin, synd_a, synd_b, 2 * H, syn, mbeg);
+    return check_launch("gm_tc_synd_to_syn");
+}
+
 extern "C" int gm_tc_synd_to_syn(int64_t nside, int64_t lmax, int spin, int64_t ncomp,
                                  const float *synd_a, const float *synd_b, float *syn, void *stream)
 {
-    if (nside < 1 || lmax < 2 || !tc_shape_ok(spin, ncomp)) return GM_ERR_BAD_SHAPE;
-    if (!synd_a || (spin && !synd_b) || !syn) return GM_ERR_BAD_PTR;
-    const int H = spin == 0 ? (int)(2 * ncomp) : (int)ncomp;
-    const int64_t tot = (lmax + 1) * 2 * nside * ncomp;
-    k_synd_to_syn<<<(unsigned)((tot + 255) / 256), 256, 0, as_stream(stream)>>>(
-        2 * nside, lmax + 1, (int)ncomp, spin, synd_a, synd_b, 2 * H, syn);
-    return check_launch("gm_tc_synd_to_syn");
+    return gm_tc_synd_to_syn_window(nside, lmax, spin, ncomp, synd_a, synd_b, syn, 0, lmax + 1, stream);
 }
 
 // ------------------------------------------------------------------ allocation-free variant

@@ -30,6 +30,7 @@ class TCPlan:
         lmax, dev = plan.lmax, plan.device
         self.coef = {}
         self.choff = {}
+        self.choff_host = {}
         self.nchunks = {}
         lib = _lib.load()
         for spin in (0, 2):
@@ -39,9 +40,11 @@ class TCPlan:
             host = np.zeros(plan.L + 1, dtype=np.int64)
             _lib.call("gm_tc_syn_chunk_offsets", lmax, spin, host.ctypes.data_as(ctypes.c_void_p))
             self.choff[spin] = torch.from_numpy(host).to(dev)
+            self.choff_host[spin] = host
             self.nchunks[spin] = int(host[-1])
         self.nctas = torch.cuda.get_device_properties(dev).multi_processor_count
         self.img_bytes = lib.gm_tc_ana_image_bytes(plan.nside, lmax)
+        self.img_bytes_per_order = lib.gm_tc_ana_image_bytes(plan.nside, 0)
         self.scratch = torch.empty(lib.gm_tc_ana_scratch_bytes(plan.nside, self.nctas) // 8,
                                    dtype=torch.float64, device=dev)
         self.err = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -158,7 +161,42 @@ def _check_batch(spin, ncomp):
         raise NotImplementedError("only spin 0 and spin 2")
 
 
-def map2alm_tc(maps, spin, nside, lmax, n_iter, mask=None):
+# Per-order buffers of an order window are sized to at most this many bytes.
+WINDOW_BYTES = 24 << 30
+
+
+def _syn_bytes_per_order(tp, spin, ncomp):
+    """Largest synthesis image + output bytes of one order (order 0 has the most chunks)."""
+    p = tp.plan
+    H, _ = _rows(spin, ncomp)
+    chunks0 = int(tp.choff_host[spin][1] - tp.choff_host[spin][0])
+    return len(_variants(spin)) * (chunks0 * _lib.load().gm_tc_syn_image_bytes(1)
+                                   + p.nlanes * 2 * H * 4)
+
+
+def window_orders(tp, spin, ncomp, budget=None):
+    """Orders per window so that the per-order buffers take at most `budget` bytes."""
+    budget = WINDOW_BYTES if budget is None else int(budget)
+    per = max(len(_variants(spin)) * tp.img_bytes_per_order, _syn_bytes_per_order(tp, spin, ncomp))
+    return int(max(1, min(tp.plan.L, budget // per)))
+
+
+def _full_path_bytes(tp, spin, ncomp, n_iter):
+    """Peak device bytes of the single-window map2alm: the ring spectra, right-hand sides
+    and images while packing; then (spectra released) the right-hand sides, images, alm
+    accumulator and synthesis buffers."""
+    p = tp.plan
+    H, NR = _rows(spin, ncomp)
+    nv = len(_variants(spin))
+    spec = ncomp * p.nring * p.L * 8
+    base = nv * tp.img_bytes + p.L * p.nlanes * ncomp * 16
+    later = base + p.nelem * NR * 8
+    if n_iter > 0:
+        later += nv * p.L * p.nlanes * 2 * H * 4 + tp.nchunks[spin] * _lib.load().gm_tc_syn_image_bytes(1)
+    return max(spec + base, later)
+
+
+def map2alm_tc(maps, spin, nside, lmax, n_iter, mask=None, window=None):
     """Batched analysis: maps (ncomp, npix) float64/float32 CUDA -> (ncomp, nelem) complex128
     (spin 2: rows E, B per field), with n_iter Jacobi iterations.  `mask` (npix,), if
     given, multiplies every map as the ring stage reads it.
@@ -166,11 +204,20 @@ def map2alm_tc(maps, spin, nside, lmax, n_iter, mask=None):
     Device memory: the ring spectra are released before the alm accumulator is made, and
     the iteration buffers before the final alm layout, so the peak is the right-hand
     sides, their operand images, the alm accumulator and the synthesis outputs (about
-    106 GB for 64 maps at Nside 2048) besides the caller's maps."""
+    106 GB for 64 maps at Nside 2048) besides the caller's maps.  When that does not fit in
+    the free device memory (or `window`, a number of orders, is given) the transform runs
+    over windows of orders instead (`map2alm_tc_windowed`)."""
     ncomp = maps.shape[0]
     _check_batch(spin, ncomp)
     tp = get_tc_plan(nside, lmax, maps.device)
     p = tp.plan
+    if window is None:
+        free, _ = torch.cuda.mem_get_info(p.device)
+        free += torch.cuda.memory_reserved(p.device) - torch.cuda.memory_allocated(p.device)
+        if _full_path_bytes(tp, spin, ncomp, n_iter) > 0.95 * free:
+            window = window_orders(tp, spin, ncomp)
+    if window is not None:
+        return map2alm_tc_windowed(maps, spin, nside, lmax, n_iter, mask=mask, window=window)
     spec = sht.ring_analysis(p, maps, _lib.MIXED, mask=mask)
     b = _Batch(tp, spin, ncomp)
     # the spin-2 rows G_Q -+ i G_U are at most twice the largest ring value
@@ -203,8 +250,95 @@ def _timed_syn(b, synd):
     return box[0]
 
 
-def alm2map_tc(alm, spin, nside, lmax):
-    """Batched synthesis: (nrows, nelem) complex128 -> (nrows, npix) float64 maps."""
+def _analysis_windowed(b, spec, scale, window, imgs):
+    """alm_i += scale * analysis of the ring spectra, one window of orders at a time."""
+    tp, spin, ncomp = b.tp, b.spin, b.ncomp
+    p = tp.plan
+    img_scale = pow2_scale(spec.view(torch.float32)) / (2.0 if spin else 1.0)
+    st = _lib.stream_handle(p.device)
+    for m0 in range(0, p.L, window):
+        m1 = min(p.L, m0 + window)
+        _lib.call("gm_tc_pack_window", p.nside, p.lmax, spin, ncomp, _lib.ptr(spec), None,
+                  _lib.ptr(imgs[0]), _lib.ptr(imgs[1]) if spin else None, img_scale, m0, m1, st)
+        for sp, img in zip(_variants(spin), imgs):
+            _lib.call("gm_tc_analysis_window", p.nside, p.lmax, spin, sp, ncomp, _lib.ptr(p.geom),
+                      _lib.ptr(p.seeds), _lib.ptr(tp.coef[spin]), _lib.ptr(img), _lib.ptr(b.alm_i),
+                      float(scale) / img_scale, _lib.ptr(tp.scratch), tp.nctas, m0, m1,
+                      _lib.ptr(tp.err), st)
+
+
+def _synthesis_windowed(b, window):
+    """Ring coefficients syn (L, nlanes, ncomp, 4) float32 of the alm accumulator, one
+    window of orders at a time."""
+    tp, spin, ncomp = b.tp, b.spin, b.ncomp
+    p = tp.plan
+    H, _ = _rows(spin, ncomp)
+    host = tp.choff_host[spin]
+    st = _lib.stream_handle(p.device)
+    syn = torch.empty((p.L, p.nlanes, ncomp, 4), dtype=torch.float32, device=p.device)
+    wmax = max(int(host[min(p.L, m0 + window)] - host[m0]) for m0 in range(0, p.L, window))
+    simg = torch.empty(max(1, wmax) * _lib.load().gm_tc_syn_image_bytes(1), dtype=torch.uint8,
+                       device=p.device)
+    synd = [torch.empty((window, p.nlanes, 2 * H), dtype=torch.float32, device=p.device)
+            for _ in _variants(spin)]
+    alm_scale = pow2_scale(b.alm_i)
+    for m0 in range(0, p.L, window):
+        m1 = min(p.L, m0 + window)
+        nbytes = int(host[m1] - host[m0]) * _lib.load().gm_tc_syn_image_bytes(1)
+        for sp, out in zip(_variants(spin), synd):
+            _lib.call("gm_tc_prep_syn_window", p.lmax, spin, sp, ncomp, _lib.ptr(b.alm_i),
+                      _lib.ptr(tp.choff[spin]), _lib.ptr(simg), nbytes, alm_scale, m0, m1, st)
+            _lib.call("gm_tc_synthesis_window", p.nside, p.lmax, spin, sp, ncomp, _lib.ptr(p.geom),
+                      _lib.ptr(p.seeds), _lib.ptr(tp.coef[spin]), _lib.ptr(simg),
+                      _lib.ptr(tp.choff[spin]), _lib.ptr(out), 1.0 / alm_scale, m0, m1,
+                      _lib.ptr(tp.err), st)
+        _lib.call("gm_tc_synd_to_syn_window", p.nside, p.lmax, spin, ncomp, _lib.ptr(synd[0]),
+                  _lib.ptr(synd[1]) if spin else None, _lib.ptr(syn), m0, m1, st)
+    return syn
+
+
+def map2alm_tc_windowed(maps, spin, nside, lmax, n_iter, mask=None, window=None):
+    """map2alm_tc over windows of `window` orders, for geometries whose full-size operand
+    buffers do not fit (Nside 4096 batches, Nside 8192).  The per-order buffers (operand
+    images, synthesis images and outputs) hold one window; the Jacobi refinement takes its
+    residual in map space (synthesis to the rings, S(alm) - mask * map, ring analysis)
+    instead of the ring-fold, whose aliasing couples all orders."""
+    ncomp = maps.shape[0]
+    _check_batch(spin, ncomp)
+    tp = get_tc_plan(nside, lmax, maps.device)
+    p = tp.plan
+    window = window_orders(tp, spin, ncomp) if window is None else int(max(1, min(p.L, window)))
+    b = _Batch(tp, spin, ncomp, images=False)
+    b.zero_alm()
+    imgs = [torch.empty(window * tp.img_bytes_per_order, dtype=torch.uint8, device=p.device)
+            for _ in _variants(spin)]
+    spec = sht.ring_analysis(p, maps, _lib.MIXED, mask=mask)
+    sht._timed(f"tc_analysis_s{spin}", p, spin, ncomp, lambda: _analysis_windowed(b, spec, 1.0, window, imgs))
+    del spec
+    for _ in range(int(n_iter)):
+        box = []
+        sht._timed(f"tc_synthesis_s{spin}", p, spin, ncomp,
+                   lambda: box.append(_synthesis_windowed(b, window)))
+        rec = sht.ring_synthesis(p, box.pop(), _lib.MIXED)
+        if mask is None:
+            rec.sub_(maps)
+        else:
+            rec.addcmul_(maps, mask[None, :].to(maps.dtype), value=-1.0)
+        spec = sht.ring_analysis(p, rec, _lib.MIXED)
+        del rec
+        sht._timed(f"tc_analysis_s{spin}", p, spin, ncomp,
+                   lambda: _analysis_windowed(b, spec, -1.0, window, imgs))
+        del spec
+    del imgs
+    out = b.to_api()
+    _check(tp)
+    return out
+
+
+def alm2map_tc(alm, spin, nside, lmax, window=None):
+    """Batched synthesis: (nrows, nelem) complex128 -> (nrows, npix) float64 maps.  With
+    `window` (a number of orders), or when the full-size buffers do not fit, the operand
+    images and outputs hold one window of orders at a time."""
     ncomp = alm.shape[0]
     _check_batch(spin, ncomp)
     tp = get_tc_plan(nside, lmax, alm.device)
@@ -212,6 +346,19 @@ def alm2map_tc(alm, spin, nside, lmax):
     b = _Batch(tp, spin, ncomp, images=False)
     b.zero_alm()
     b.from_api(alm.to(torch.complex128))
+    H, _ = _rows(spin, ncomp)
+    if window is None:
+        free, _ = torch.cuda.mem_get_info(p.device)
+        free += torch.cuda.memory_reserved(p.device) - torch.cuda.memory_allocated(p.device)
+        full = (len(_variants(spin)) * p.L * p.nlanes * 2 * H * 4
+                + tp.nchunks[spin] * _lib.load().gm_tc_syn_image_bytes(1) + p.L * p.nlanes * ncomp * 16)
+        if full > 0.9 * free:
+            window = window_orders(tp, spin, ncomp)
+    if window is not None:
+        syn = _synthesis_windowed(b, int(max(1, min(p.L, window))))
+        maps = sht.ring_synthesis(p, syn, _lib.MIXED)
+        _check(tp)
+        return maps
     synd = b.synthesis()
     syn = torch.empty((p.L, p.nlanes, ncomp, 4), dtype=torch.float32, device=p.device)
     _lib.call("gm_tc_synd_to_syn", p.nside, p.lmax, spin, ncomp, _lib.ptr(synd[0]),

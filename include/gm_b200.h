@@ -272,6 +272,34 @@ int gm_tc_fold(int64_t nside, int64_t lmax, int spin, int64_t ncomp, const float
 /* Batched synthesis output -> syn layout of gm_ring_synthesis. */
 int gm_tc_synd_to_syn(int64_t nside, int64_t lmax, int spin, int64_t ncomp, const float *synd_a,
                       const float *synd_b, float *syn, void *stream);
+/* Order windows of the batched transforms, for geometries whose full-size buffers do not
+ * fit (Nside 4096 batches, Nside 8192): each entry handles the orders m in [mbeg, mend)
+ * only, and its per-order buffers hold just those orders, indexed by m - mbeg (analysis
+ * images: (mend - mbeg) x gm_tc_lane_groups(nside) x 64 KB; synthesis images: from
+ * choff[mbeg] to choff[mend]; synd: (mend - mbeg, nlanes, rows)).  rhs_map of
+ * gm_tc_pack_window may be NULL (transforms without the ring-fold refinement).  The alm
+ * accumulator, the ring spectra and the syn buffer keep their full size.  The entries
+ * above are these with the window [0, lmax + 1).  Same reference interfaces as above
+ * (march_v2.py:637-663, march_v2.cu:155-407); the reference runs its latitudinal
+ * transform on order ranges the same way when it splits the orders [0, split) and
+ * [split, L) between two GPUs (healpix.py:528-548). */
+int gm_tc_pack_window(int64_t nside, int64_t lmax, int spin, int64_t ncomp, const void *ringspec,
+                      void *rhs_map, void *img_a, void *img_b, double img_scale, int64_t mbeg,
+                      int64_t mend, void *stream);
+int gm_tc_analysis_window(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                          const double *geom, const double *seeds, const double *coef,
+                          const void *img, double *alm_i, double scale, double *scratch,
+                          int64_t nctas, int64_t mbeg, int64_t mend, int32_t *err, void *stream);
+int gm_tc_prep_syn_window(int64_t lmax, int spin, int sp, int64_t ncomp, const double *alm_i,
+                          const int64_t *choff, void *simg, int64_t simg_bytes, double alm_scale,
+                          int64_t mbeg, int64_t mend, void *stream);
+int gm_tc_synthesis_window(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                           const double *geom, const double *seeds, const double *coef,
+                           const void *simg, const int64_t *choff, float *synd, double out_scale,
+                           int64_t mbeg, int64_t mend, int32_t *err, void *stream);
+int gm_tc_synd_to_syn_window(int64_t nside, int64_t lmax, int spin, int64_t ncomp,
+                             const float *synd_a, const float *synd_b, float *syn, int64_t mbeg,
+                             int64_t mend, void *stream);
 /* alm_i <-> API layout (nalm, nelem) complex128 (spin 2: E, B per field). */
 int gm_tc_alm_layout(int64_t lmax, int spin, int64_t nfield, double *alm_i, double *alm_api,
                      int to_api, void *stream);
