@@ -60,9 +60,10 @@ def parse():
     p.add_argument("--batch", type=int, default=32)
     p.add_argument("--fp64-steps", type=int, default=1)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="mc", choices=["mc", "uneven_workspaces"],
+    p.add_argument("--workload", default="mc", choices=["mc", "uneven_workspaces", "nside4096"],
                    help="mc: the Monte-Carlo estimator (default); uneven_workspaces: TT "
-                        "coupling matrices of 32 masks of mixed Nside in one launch")
+                        "coupling matrices of 32 masks of mixed Nside in one launch; nside4096: "
+                        "batched map2alm (n_iter=0) and alm2map at Nside 4096")
     p.add_argument("--nmasks", type=int, default=32)
     return p.parse_args()
 
@@ -445,6 +446,102 @@ def run_uneven_workspaces(args):
     print(json.dumps(line), flush=True)
 
 
+def run_nside4096(args):
+    """Batched transforms at Nside 4096 (lmax 12287): FP32 maps of Gaussian alms with
+    C_l = 1/(l+10)^2 (seeds 10 + i), spin 0 and spin 2 (E and B from the same C_l), batches
+    of 1, 8 (and 16 spin-0 maps); one step = map2alm with n_iter = 0, or alm2map, of the
+    batch.  The transforms run over windows of orders (their single-window operand images
+    alone would take 51.5 GB per row variant).  Batch 1 of each spin is also transformed
+    by the SIMT mixed-precision path as a cross-check (the FP64 ring stage is limited to
+    Nside 2048 by shared memory)."""
+    import torch
+
+    from gmaster_b200 import _lib, sht, sht_tc
+    from gmaster_b200.utils import NmtAlmInfo
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    nside = 4096
+    lmax = 3 * nside - 1
+    ell, order = NmtAlmInfo(lmax).ell_m()
+    ell_t = torch.from_numpy(ell).to(dev)
+    m0 = torch.from_numpy(order == 0).to(dev)
+    amp = torch.from_numpy(1.0 / (np.arange(lmax + 1) + 10.0)).to(dev)[ell_t]
+
+    def alms(n, seed, spin):
+        out = torch.empty((n, ell.shape[0]), dtype=torch.complex128, device=dev)
+        for i in range(n):
+            gen = torch.Generator(device=dev)
+            gen.manual_seed(10 + seed + i)
+            re = torch.randn(ell.shape[0], generator=gen, device=dev, dtype=torch.float64)
+            im = torch.randn(ell.shape[0], generator=gen, device=dev, dtype=torch.float64)
+            re[m0] *= np.sqrt(2.0)
+            im[m0] = 0.0
+            a = torch.complex(re, im) * (amp / np.sqrt(2.0))
+            if spin:
+                a[ell_t < 2] = 0
+            out[i] = a
+        return out
+
+    def timed(fn, warmup, steps):
+        for _ in range(warmup):
+            out = fn()
+            del out
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            out = fn()
+            del out
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps / 1e3
+
+    cases = []
+    calls0 = dict(_lib.CALLS)
+    sampler = ClockSampler(0)
+    sampler.start()
+    for spin, batches in ((0, (1, 8, 16)), (2, (1, 8))):
+        for batch in batches:
+            ncomp = batch if spin == 0 else 2 * batch
+            torch.cuda.reset_peak_memory_stats(dev)
+            a = alms(ncomp, 1000 * spin + 100 * batch, spin)
+            maps = sht_tc.alm2map_tc(a, spin, nside, lmax).to(torch.float32)
+            torch.cuda.empty_cache()
+            t_ana = timed(lambda: sht_tc.map2alm_tc(maps, spin, nside, lmax, 0), 1, args.steps)
+            t_syn = timed(lambda: sht_tc.alm2map_tc(a, spin, nside, lmax), 1, args.steps)
+            case = {"spin": spin, "batch": batch, "maps": ncomp,
+                    "map2alm_s": t_ana, "alm2map_s": t_syn,
+                    "map2alm_maps_per_s": ncomp / t_ana, "alm2map_maps_per_s": ncomp / t_syn,
+                    "window_orders": sht_tc.window_orders(sht_tc.get_tc_plan(nside, lmax, dev), spin, ncomp),
+                    "peak_gb": torch.cuda.max_memory_allocated(dev) / 1e9}
+            if batch == 1:
+                tc = sht_tc.map2alm_tc(maps, spin, nside, lmax, 0)
+                simt = sht.map2alm_device(maps.to(torch.float64), spin, nside, lmax, 0, "mixed")
+                case["map2alm_rel_diff_vs_simt_mixed"] = float((tc - simt).abs().max() / simt.abs().max())
+                del tc, simt
+            cases.append(case)
+            del a, maps
+            torch.cuda.empty_cache()
+            print(json.dumps(case), file=sys.stderr, flush=True)
+    clocks = sampler.stop()
+    launches = sum(_lib.CALLS.get(k, 0) - calls0.get(k, 0) for k in _lib.CALLS)
+    best = max(cases, key=lambda c: c["map2alm_maps_per_s"] if c["spin"] == 0 else 0)
+    line = {
+        "metric": "batched map2alm (n_iter=0) maps/s at Nside 4096, lmax 12287",
+        "value": best["map2alm_maps_per_s"], "unit": "maps/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": 1, "ms_per_step": best["map2alm_s"] * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f16x3 tensor-core products (f32 accumulate), f64 recurrence, f32 ring FFTs",
+        "data": "synthetic (Gaussian alms, C_l = 1/(l+10)^2, seeds 10+i)",
+        "config": {"workload": "Nside 4096 batched transforms, spin 0 batches 1/8/16, spin 2 "
+                               "batches 1/8 fields, FP32 maps, windows of orders",
+                   "l2_flush": "inputs (0.8 GB per map) larger than L2"},
+        "cases": cases, "clocks": clocks, "gpu_launches": int(launches),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -452,6 +549,9 @@ def main():
         return
     if args.workload == "uneven_workspaces":
         run_uneven_workspaces(args)
+        return
+    if args.workload == "nside4096":
+        run_nside4096(args)
         return
     import torch
     import torch.distributed as dist
