@@ -9,8 +9,8 @@ there is no CPU fallback.  Arrays are CUDA ``torch.Tensor``s.
 
 from ._config import (get_default_params, get_precision, nmt_params, set_n_iter_default,
                       set_precision, set_sht_calculator, set_tol_pinv_default)
-from .batch import (compute_coupled_cells, decouple_cells, fields_from_maps, mc_bandpowers,
-                    workspaces_from_fields)
+from .batch import (SimulationGraph, compute_coupled_cells, decouple_cells, fields_from_maps,
+                    mc_bandpowers, workspaces_from_fields)
 from .bins import NmtBin
 from .field import NmtField
 from .utils import (NmtAlmInfo, NmtMapInfo, alm2map, map2alm, map2alm_pair, mask_apodization,
@@ -20,7 +20,7 @@ from .workspaces import NmtWorkspace, compute_coupled_cell
 __all__ = [
     "NmtAlmInfo", "NmtBin", "NmtField", "NmtMapInfo", "NmtWorkspace", "alm2map",
     "compute_coupled_cell", "compute_coupled_cells", "decouple_cells", "fields_from_maps",
-    "mc_bandpowers", "workspaces_from_fields",
+    "mc_bandpowers", "workspaces_from_fields", "SimulationGraph",
     "get_default_params", "get_precision", "map2alm", "map2alm_pair",
     "mask_apodization", "nmt_params", "set_n_iter_default", "set_precision",
     "set_sht_calculator", "set_tol_pinv_default", "synfast_spherical",

@@ -65,6 +65,11 @@ SIGNATURES = {
     "gm_tc_fold": ([_c_i64, _c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl,
                     _c_vp], _c_int),
     "gm_tc_synd_to_syn": ([_c_i64, _c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
+    "gm_legendre_tiles": ([_c_int, _c_vp, _c_int], _c_int),
+    "gm_legendre_analysis_tile": ([_c_int, _c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp,
+                                   _c_dbl, _c_int, _c_vp], _c_int),
+    "gm_legendre_synthesis_tile": ([_c_int, _c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp,
+                                    _c_int, _c_vp], _c_int),
     "gm_tc_pack_window": ([_c_i64, _c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_i64,
                            _c_i64, _c_vp], _c_int),
     "gm_tc_analysis_window": ([_c_i64, _c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
@@ -91,7 +96,8 @@ _lib = None
 LAUNCHES = {"gm_last_error": 0, "gm_version": 0, "gm_ring_twiddle_count": 0,
             "gm_seed_table_len": 0, "gm_bin_coupling_csr": 3, "gm_tc_lane_groups": 0,
             "gm_tc_ana_image_bytes": 0, "gm_tc_ana_scratch_bytes": 0,
-            "gm_tc_syn_chunk_offsets": 0, "gm_tc_syn_image_bytes": 0}
+            "gm_tc_syn_chunk_offsets": 0, "gm_tc_syn_image_bytes": 0, "gm_legendre_tiles": 0,
+            "gm_coupling_units": 0}
 CALLS = {}
 
 

@@ -15,6 +15,10 @@ that loop for a whole batch at once:
 * ``workspaces_from_fields`` builds many workspaces -- of uneven lmax too -- whose
   coupling blocks come from one persistent FP64 Wigner-3j launch sharing a device work
   queue, instead of one launch per workspace.
+* ``SimulationGraph`` captures the whole per-simulation estimator (masking, the two
+  field transforms with their Jacobi iterations, three pseudo-spectra, binning and the
+  three LU solves) as one CUDA graph and replays it for each simulation, so a loop over
+  simulations issues one graph launch instead of some hundred kernel launches.
 * ``mc_bandpowers`` runs the whole estimator for a batch of TQU simulations; maps given
   in (pinned) host memory are copied on a side stream, so that the copy of the (Q, U)
   maps overlaps the T transforms.
@@ -27,7 +31,8 @@ from . import sht, sht_tc
 from ._config import get_precision, nmt_params
 from .field import NmtField
 from .utils import as_device
-from .workspaces import NmtWorkspace, _which, compute_coupled_cell, coupling_blocks_multi
+from .workspaces import (NmtWorkspace, _which, compute_coupled_cell, coupling_blocks_multi,
+                         pseudo_cl)
 
 
 def fields_from_maps(mask, maps, *, spin=None, n_iter=None, beam=None, lmax=None,
@@ -154,6 +159,77 @@ def workspaces_from_fields(field_pairs, bins, **kwargs):
         w._compute_blocks(given.get(id(w)))
         w._postprocess()
     return wss
+
+
+class SimulationGraph:
+    """The estimator of one TQU simulation, captured once as a CUDA graph.
+
+    ``SimulationGraph(mask, w00, w02, w22)(t, qu)`` returns the bandpowers TT (1, nb),
+    TE/TB (2, nb) and EE/EB/BE/BB (4, nb) of ``w.decouple_cell(compute_coupled_cell(...))``
+    for fields ``NmtField(mask, t)`` and ``NmtField(mask, qu)``, using the one-field
+    transforms of ``precision`` (the SIMT kernels).  The first call runs the pipeline twice
+    on a side stream (plans, tables and workspace operators are built there) and then
+    captures it; every call copies the maps into the graph's static input buffers and
+    replays the graph on the current stream.  The graph keeps its own memory pool; the
+    returned tensors are copies.  The workspaces' LU factors are checked once, before the
+    capture (a singular binned matrix raises there).
+    """
+
+    def __init__(self, mask, w00, w02, w22, *, n_iter=None, precision=None):
+        self.precision = precision or get_precision()
+        self.n_iter = nmt_params.n_iter_default if n_iter is None else int(n_iter)
+        self.mask = as_device(mask, torch.float64).contiguous()
+        npix = self.mask.shape[0]
+        self.nside = int(round(np.sqrt(npix / 12)))
+        if 12 * self.nside ** 2 != npix:
+            raise ValueError("mask is not a HEALPix map")
+        self.ws = (w00, w02, w22)
+        if (w00.ncls, w02.ncls, w22.ncls) != (1, 2, 4):
+            raise ValueError("workspaces must be spin 0x0, 0x2 and 2x2")
+        self.lmax = w00.lmax
+        for w in self.ws:
+            w._lu.check()
+        dev = self.mask.device
+        self.t = torch.zeros((1, npix), dtype=torch.float64, device=dev)
+        self.qu = torch.zeros((2, npix), dtype=torch.float64, device=dev)
+        self.graph = None
+        self.out = None
+
+    def _step(self):
+        at = sht.map2alm_device(self.t * self.mask[None, :], 0, self.nside, self.lmax, self.n_iter,
+                                self.precision)
+        aq = sht.map2alm_device(self.qu * self.mask[None, :], 2, self.nside, self.lmax, self.n_iter,
+                                self.precision)
+        out = []
+        for w, (a, b) in zip(self.ws, ((at, at), (at, aq), (aq, aq))):
+            binned = w.bins.bin_cell(pseudo_cl(a, b, self.lmax))
+            sol = w._lu.solve(binned.T.reshape(-1).contiguous())
+            out.append(sol.reshape(w.nbands, w.ncls).T)
+        return out
+
+    def capture(self):
+        dev = self.mask.device
+        side = torch.cuda.Stream(device=dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(side):
+            for _ in range(2):
+                self._step()
+        torch.cuda.current_stream(dev).wait_stream(side)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph, capture_error_mode="relaxed"):
+            self.out = self._step()
+
+    def __call__(self, t, qu):
+        t = as_device(t, torch.float64).reshape(1, -1)
+        qu = as_device(qu, torch.float64).reshape(2, -1)
+        if t.shape[1] != self.t.shape[1] or qu.shape[1] != self.qu.shape[1]:
+            raise ValueError("Maps and mask have different sizes")
+        if self.graph is None:
+            self.capture()
+        self.t.copy_(t)
+        self.qu.copy_(qu)
+        self.graph.replay()
+        return [o.clone() for o in self.out]
 
 
 _COPY_STREAMS = {}

@@ -496,6 +496,124 @@ static int dispatch_syn(int spin, int64_t nside, int64_t lmax, int64_t ncomp, co
     return launch_syn<T, 2, 2, 2>(nside, lmax, ncomp, geom, seeds, alm, syn, s);
 }
 
+// Tile shapes the autotuner chooses from: (NC, R) = (components per CTA, lanes per thread).
+// Spin 0 takes NC in {1, 2, 4, 8} (the reduce-scatter needs 2 NC to divide 32); spin 2
+// handles one (Q, U) pair per CTA (NC = 2).  Index -1 selects the built-in heuristic.
+static const int kTiles0[][2] = {{1, 1}, {1, 2}, {1, 4}, {2, 1}, {2, 2}, {2, 4}, {4, 1}, {4, 2}, {8, 1}};
+static const int kTiles2[][2] = {{2, 1}, {2, 2}, {2, 4}};
+constexpr int kNTiles0 = sizeof(kTiles0) / sizeof(kTiles0[0]);
+constexpr int kNTiles2 = sizeof(kTiles2) / sizeof(kTiles2[0]);
+
+template <typename T>
+static int tile_ana(int spin, int tile, int64_t nside, int64_t lmax, int64_t ncomp,
+                    const double *geom, const double *seeds, const void *rhs, double *alm,
+                    double scale, cudaStream_t s)
+{
+#define GM_ANA(SP, NC, R) return launch_ana<T, SP, NC, R>(nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s)
+    if (spin == 0) {
+        switch (tile) {
+        case 0: GM_ANA(0, 1, 1);
+        case 1: GM_ANA(0, 1, 2);
+        case 2: GM_ANA(0, 1, 4);
+        case 3: GM_ANA(0, 2, 1);
+        case 4: GM_ANA(0, 2, 2);
+        case 5: GM_ANA(0, 2, 4);
+        case 6: GM_ANA(0, 4, 1);
+        case 7: GM_ANA(0, 4, 2);
+        case 8: GM_ANA(0, 8, 1);
+        default: return GM_ERR_BAD_SHAPE;
+        }
+    }
+    switch (tile) {
+    case 0: GM_ANA(2, 2, 1);
+    case 1: GM_ANA(2, 2, 2);
+    case 2: GM_ANA(2, 2, 4);
+    default: return GM_ERR_BAD_SHAPE;
+    }
+#undef GM_ANA
+}
+
+template <typename T>
+static int tile_syn(int spin, int tile, int64_t nside, int64_t lmax, int64_t ncomp,
+                    const double *geom, const double *seeds, const double *alm, void *syn,
+                    cudaStream_t s)
+{
+#define GM_SYN(SP, NC, R) return launch_syn<T, SP, NC, R>(nside, lmax, ncomp, geom, seeds, alm, syn, s)
+    if (spin == 0) {
+        switch (tile) {
+        case 0: GM_SYN(0, 1, 1);
+        case 1: GM_SYN(0, 1, 2);
+        case 2: GM_SYN(0, 1, 4);
+        case 3: GM_SYN(0, 2, 1);
+        case 4: GM_SYN(0, 2, 2);
+        case 5: GM_SYN(0, 2, 4);
+        case 6: GM_SYN(0, 4, 1);
+        case 7: GM_SYN(0, 4, 2);
+        case 8: GM_SYN(0, 8, 1);
+        default: return GM_ERR_BAD_SHAPE;
+        }
+    }
+    switch (tile) {
+    case 0: GM_SYN(2, 2, 1);
+    case 1: GM_SYN(2, 2, 2);
+    case 2: GM_SYN(2, 2, 4);
+    default: return GM_ERR_BAD_SHAPE;
+    }
+#undef GM_SYN
+}
+
+extern "C" int gm_legendre_tiles(int spin, int32_t *nc_r, int capacity)
+{
+    if (spin != 0 && spin != 2) return -1;
+    const int n = spin == 0 ? kNTiles0 : kNTiles2;
+    for (int i = 0; i < n && i < capacity; ++i) {
+        nc_r[2 * i] = spin == 0 ? kTiles0[i][0] : kTiles2[i][0];
+        nc_r[2 * i + 1] = spin == 0 ? kTiles0[i][1] : kTiles2[i][1];
+    }
+    return n;
+}
+
+extern "C" int gm_legendre_analysis_tile(int precision, int spin, int64_t nside, int64_t lmax,
+                                         int64_t ncomp, const double *lane_geom, const double *seeds,
+                                         const void *rhs, double *alm, double scale, int tile,
+                                         void *stream)
+{
+    if (nside < 1 || lmax < 0 || lmax + 1 > 65535 || ncomp < 1 || ncomp > 65535)
+        return GM_ERR_BAD_SHAPE;
+    if (spin != 0 && spin != 2) return GM_ERR_UNSUPPORTED;
+    if (spin == 2 && (ncomp % 2)) return GM_ERR_BAD_SHAPE;
+    if (tile < -1 || tile >= (spin == 0 ? kNTiles0 : kNTiles2)) return GM_ERR_BAD_SHAPE;
+    if (!lane_geom || !seeds || !rhs || !alm) return GM_ERR_BAD_PTR;
+    cudaStream_t s = as_stream(stream);
+    if (precision == GM_FP64)
+        return tile < 0 ? dispatch_ana<double>(spin, nside, lmax, ncomp, lane_geom, seeds, rhs, alm, scale, s)
+                        : tile_ana<double>(spin, tile, nside, lmax, ncomp, lane_geom, seeds, rhs, alm, scale, s);
+    if (precision == GM_MIXED)
+        return tile < 0 ? dispatch_ana<float>(spin, nside, lmax, ncomp, lane_geom, seeds, rhs, alm, scale, s)
+                        : tile_ana<float>(spin, tile, nside, lmax, ncomp, lane_geom, seeds, rhs, alm, scale, s);
+    return GM_ERR_UNSUPPORTED;
+}
+
+extern "C" int gm_legendre_synthesis_tile(int precision, int spin, int64_t nside, int64_t lmax,
+                                          int64_t ncomp, const double *lane_geom, const double *seeds,
+                                          const double *alm, void *syn, int tile, void *stream)
+{
+    if (nside < 1 || lmax < 0 || lmax + 1 > 65535 || ncomp < 1 || ncomp > 65535)
+        return GM_ERR_BAD_SHAPE;
+    if (spin != 0 && spin != 2) return GM_ERR_UNSUPPORTED;
+    if (spin == 2 && (ncomp % 2)) return GM_ERR_BAD_SHAPE;
+    if (tile < -1 || tile >= (spin == 0 ? kNTiles0 : kNTiles2)) return GM_ERR_BAD_SHAPE;
+    if (!lane_geom || !seeds || !alm || !syn) return GM_ERR_BAD_PTR;
+    cudaStream_t s = as_stream(stream);
+    if (precision == GM_FP64)
+        return tile < 0 ? dispatch_syn<double>(spin, nside, lmax, ncomp, lane_geom, seeds, alm, syn, s)
+                        : tile_syn<double>(spin, tile, nside, lmax, ncomp, lane_geom, seeds, alm, syn, s);
+    if (precision == GM_MIXED)
+        return tile < 0 ? dispatch_syn<float>(spin, nside, lmax, ncomp, lane_geom, seeds, alm, syn, s)
+                        : tile_syn<float>(spin, tile, nside, lmax, ncomp, lane_geom, seeds, alm, syn, s);
+    return GM_ERR_UNSUPPORTED;
+}
+
 extern "C" int gm_legendre_analysis(int precision, int spin, int64_t nside, int64_t lmax,
                                     int64_t ncomp, const double *lane_geom, const double *seeds,
                                     const void *rhs, double *alm, double scale, void *stream)

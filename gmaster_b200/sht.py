@@ -22,7 +22,7 @@ import threading
 import numpy as np
 import torch
 
-from . import _lib
+from . import _lib, autotune
 
 _PLANS = {}
 _PLAN_LOCK = threading.Lock()
@@ -221,18 +221,20 @@ def pack_rhs(plan, spec, prec):
 
 def legendre_analysis(plan, spin, rhs, alm, scale, prec):
     ncomp = rhs.shape[2]
+    tile = autotune.tile_for(plan, spin, ncomp, prec, "ana")
     _timed(f"legendre_analysis_s{spin}", plan, spin, ncomp, lambda: _lib.call(
-        "gm_legendre_analysis", prec, spin, plan.nside, plan.lmax, ncomp,
+        "gm_legendre_analysis_tile", prec, spin, plan.nside, plan.lmax, ncomp,
         _lib.ptr(plan.geom), _lib.ptr(plan.seeds), _lib.ptr(rhs), _lib.ptr(alm),
-        float(scale), _lib.stream_handle(plan.device)))
+        float(scale), tile, _lib.stream_handle(plan.device)))
 
 
 def legendre_synthesis(plan, spin, alm, ncomp, prec, out=None):
     syn = out if out is not None else torch.empty(
         (plan.L, plan.nlanes, ncomp, 4), dtype=_real_dtype(prec), device=plan.device)
+    tile = autotune.tile_for(plan, spin, ncomp, prec, "syn")
     _timed(f"legendre_synthesis_s{spin}", plan, spin, ncomp, lambda: _lib.call(
-        "gm_legendre_synthesis", prec, spin, plan.nside, plan.lmax, ncomp,
-        _lib.ptr(plan.geom), _lib.ptr(plan.seeds), _lib.ptr(alm), _lib.ptr(syn),
+        "gm_legendre_synthesis_tile", prec, spin, plan.nside, plan.lmax, ncomp,
+        _lib.ptr(plan.geom), _lib.ptr(plan.seeds), _lib.ptr(alm), _lib.ptr(syn), tile,
         _lib.stream_handle(plan.device)))
     return syn
 

@@ -120,6 +120,19 @@ int gm_legendre_synthesis(int precision, int spin, int64_t nside, int64_t lmax,
                           int64_t ncomp, const double *lane_geom, const double *seeds,
                           const double *alm, void *syn, void *stream);
 
+/* Tile shapes of the two entries above, for the autotuner (gmaster_b200/autotune.py):
+ * gm_legendre_tiles writes up to `capacity` pairs (NC, R) = (components per CTA, lanes
+ * per thread) of `spin` into nc_r and returns their number (-1 for another spin).  The
+ * _tile entries run tile `tile` of that list (-1: the built-in choice).  The reference
+ * picks its march tiles by fixed rules (march_v2.py:290-332); it has no tuner. */
+int gm_legendre_tiles(int spin, int32_t *nc_r, int capacity);
+int gm_legendre_analysis_tile(int precision, int spin, int64_t nside, int64_t lmax,
+                              int64_t ncomp, const double *lane_geom, const double *seeds,
+                              const void *rhs, double *alm, double scale, int tile, void *stream);
+int gm_legendre_synthesis_tile(int precision, int spin, int64_t nside, int64_t lmax,
+                               int64_t ncomp, const double *lane_geom, const double *seeds,
+                               const double *alm, void *syn, int tile, void *stream);
+
 /* ------------------------------------------------------------- spectra */
 
 /* Coupled pseudo-C_ell of all component pairs (replaces workspaces.py:86-95

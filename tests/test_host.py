@@ -135,3 +135,16 @@ def test_compute_without_gpu_fails_loudly():
 
     with pytest.raises(RuntimeError):
         _lib.require_cuda()
+
+
+def test_legendre_tile_list():
+    """The autotuner's tile shapes are listed by the library without a GPU."""
+    from gmaster_b200 import autotune
+
+    t0, t2 = autotune.tiles(0), autotune.tiles(2)
+    assert (1, 1) in t0 and len(t0) == len(set(t0))
+    assert all(32 % (2 * nc) == 0 for nc, _ in t0)
+    assert all(nc == 2 for nc, _ in t2)
+    with pytest.raises(ValueError):
+        autotune.tiles(1)
+    assert not autotune.autotune_enabled() or "GMASTER_B200_AUTOTUNE" in __import__("os").environ
