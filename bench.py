@@ -736,6 +736,16 @@ def main():
     auto = [(mixed_bp[0][0], fp64_bp[0][0]), (mixed_bp[2][0], fp64_bp[2][0]),
             (mixed_bp[2][3], fp64_bp[2][3])]
     rel_auto = float(max(np.max(np.abs(a - b) / np.abs(b)) for a, b in auto))
+    # the same differences in units of the Gaussian cosmic variance of each band,
+    # sigma_b = sqrt(2 / ((2 l_b + 1) nlb f_sky)) |C_b| (f_sky = mean of the squared mask)
+    import gmaster_b200 as nmt
+
+    l_eff = nmt.NmtBin.from_nside_linear(nside, nlb).get_effective_ells()
+    fsky = float((mask ** 2).mean())
+    sig_cv = {}
+    for name, (a, b) in zip(("TT", "EE", "BB"), auto):
+        sigma = np.sqrt(2.0 / ((2.0 * l_eff + 1.0) * nlb * fsky)) * np.abs(b)
+        sig_cv[name] = float(np.max(np.abs(a - b) / sigma))
 
     # e2e through the public API from pinned host memory (device copies released first)
     t_host = t_all.cpu()
@@ -811,7 +821,8 @@ def main():
         "mixed_unbatched": {"value": world * 1e3 / ms1, "unit": "sims/s", "ms_per_sim": ms1},
         "speedup_mixed_vs_fp64": value / value64,
         "s_per_spectrum": s_per_spec,
-        "bandpower_err_mixed_vs_fp64": {"max_abs_over_scale": errs, "max_rel_auto": rel_auto},
+        "bandpower_err_mixed_vs_fp64": {"max_abs_over_scale": errs, "max_rel_auto": rel_auto,
+                                        "max_in_sigma_cv": sig_cv, "fsky": fsky},
         "clocks": clocks,
         "gpu_launches": int(launches),
     }
