@@ -50,6 +50,27 @@ class NmtBin:
         self._weights_np, self._f_ell_np = weights, f_ell
         self._dev = {}
 
+    def _fits_table(self, extname="BANDPOWERS"):
+        """The bandpower table of workspace files (gmaster/bins.py:288-302): one row per l
+        with its band (-1 outside every band), weight and f_l."""
+        bands = np.full(self.lmax + 1, -1, dtype=np.int32)
+        weights = np.zeros(self.lmax + 1)
+        f_ell = np.zeros(self.lmax + 1)
+        bands[self._ells_np] = self._bpws_np
+        weights[self._ells_np] = self._weights_np
+        f_ell[self._ells_np] = self._f_ell_np
+        return {"kind": "table", "name": extname,
+                "columns": [("BAND", bands), ("ELLS", np.arange(self.lmax + 1, dtype=np.int32)),
+                            ("WEIGHTS", weights), ("F_ELL", f_ell)],
+                "header": {"ELL_MAX": self.lmax, "N_BANDS": self.n_bands}}
+
+    @classmethod
+    def _from_fits_table(cls, hdu):
+        """Inverse of ``_fits_table`` (gmaster/bins.py:276-286)."""
+        d = hdu["data"]
+        return cls(lmax=int(hdu["header"]["ELL_MAX"]), bpws=d["BAND"], ells=d["ELLS"],
+                   weights=d["WEIGHTS"].astype(np.float64), f_ell=d["F_ELL"].astype(np.float64))
+
     @classmethod
     def from_nside_linear(cls, nside, nlb, is_Dell=False, f_ell=None):
         return cls.from_lmax_linear(3 * nside - 1, nlb, is_Dell, f_ell)

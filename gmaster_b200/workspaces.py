@@ -9,7 +9,7 @@ GPU, and `decouple_cell` returns bandpowers (workspaces.py:1593-2147).
 import numpy as np
 import torch
 
-from . import _lib
+from . import _lib, fits
 from .bins import NmtBin
 from .utils import as_device
 
@@ -131,6 +131,41 @@ def coupling_tt_toeplitz(window, lmax, l_toeplitz, l_exact, dl_band):
     return toeplitz_fill(S, lmax, l_toeplitz, l_exact, dl_band)
 
 
+def _blocks_from_dense(dense, lmax, ncls, device):
+    """(4, L, L) blocks [tt, te, pp, mm] of a dense (ncls L)^2 coupling matrix in
+    ``l * ncls + c`` order; the inverse of ``NmtWorkspace.get_coupling_matrix``.  Raises if
+    the matrix does not have the structure of a spin 0x0, 0x2 or 2x2 workspace."""
+    n = lmax + 1
+    d = np.asarray(dense, dtype=np.float64)
+    if d.shape != (ncls * n, ncls * n):
+        raise ValueError(f"coupling matrix of shape {d.shape}, expected {(ncls * n, ncls * n)}")
+    blocks = np.zeros((4, n, n))
+    if ncls == 1:
+        blocks[_BLOCK_TT] = d
+        rebuilt = d
+    else:
+        q = d.reshape(n, ncls, n, ncls)
+        rebuilt = np.zeros_like(q)
+        if ncls == 2:
+            blocks[_BLOCK_TE] = q[:, 0, :, 0]
+            for c in range(2):
+                rebuilt[:, c, :, c] = blocks[_BLOCK_TE]
+        elif ncls == 4:
+            blocks[_BLOCK_PP] = q[:, 0, :, 0]
+            blocks[_BLOCK_MM] = q[:, 0, :, 3]
+            for c in range(4):
+                rebuilt[:, c, :, c] += blocks[_BLOCK_PP]
+            for c, sign in zip(range(4), (1.0, -1.0, -1.0, 1.0)):
+                rebuilt[:, c, :, 3 - c] += sign * blocks[_BLOCK_MM]
+        else:
+            raise ValueError(f"unsupported number of spectra {ncls}")
+        rebuilt = rebuilt.reshape(ncls * n, ncls * n)
+    if not np.array_equal(rebuilt, d):
+        raise NotImplementedError("the coupling matrix is not that of a standard spin 0x0, 0x2 or "
+                                  "2x2 workspace")
+    return torch.from_numpy(blocks).to(device)
+
+
 def _which(ncls):
     return {1: 1, 2: 2, 4: 12}[ncls]
 
@@ -167,7 +202,8 @@ class NmtWorkspace:
                  dl_band=-1, fname=None, normalization="MASTER"):
         self.mcm_blocks = self.mcm_binned = self._lu = None
         if fname is not None:
-            raise NotImplementedError("workspace files are not part of this build")
+            self.read_from(fname)
+            return
         if fl1 is not None or fl2 is not None or bins is not None:
             self.compute_coupling_matrix(fl1, fl2, bins, is_teb=is_teb, l_toeplitz=l_toeplitz,
                                          l_exact=l_exact, dl_band=dl_band,
@@ -176,6 +212,77 @@ class NmtWorkspace:
     @classmethod
     def from_fields(cls, fl1, fl2, bins, **kwargs):
         return cls(fl1, fl2, bins, **kwargs)
+
+    @classmethod
+    def from_file(cls, fname):
+        """Workspace read from a NaMaster-compatible FITS file (workspaces.py:1674-1676)."""
+        return cls(fname=fname)
+
+    def write_to(self, fname):
+        """Write the workspace to a NaMaster-compatible FITS file (workspaces.py:2211-2255):
+        the dense coupling matrix with the workspace keywords in the primary HDU, then the
+        BEAMS, PCL_MASKS and BANDPOWERS tables.  An existing file is overwritten."""
+        if self.mcm_blocks is None:
+            raise RuntimeError("the workspace holds no coupling matrix")
+        header = {
+            "LMAX": self.lmax, "LMAX_MASK": self.lmax_mask, "IS_TEB": False, "NCLS": self.ncls,
+            "NORM_TYPE": 0 if self.normalization == "MASTER" else 1, "WAWB": float(self.wawb),
+            "SPIN1": self.spin1, "SPIN2": self.spin2, "ANISO1": False, "ANISO2": False,
+            "PURE_E1": False, "PURE_B1": False, "PURE_E2": False, "PURE_B2": False,
+            "L_TOEPLITZ": self.l_toeplitz, "L_EXACT": self.l_exact, "DL_BAND": self.dl_band,
+        }
+        ell = np.arange(self.lmax + 1, dtype=np.int32)
+        pcl = self.pcl_mask.cpu().numpy()
+        fits.write(fname, [
+            {"kind": "image", "name": "WSP_PRIMARY", "data": self.get_coupling_matrix().cpu().numpy(),
+             "header": header},
+            {"kind": "table", "name": "BEAMS",
+             "columns": [("L", ell), ("BEAM1", self.beam1.cpu().numpy()),
+                         ("BEAM2", self.beam2.cpu().numpy())]},
+            {"kind": "table", "name": "PCL_MASKS",
+             "columns": [("L", np.arange(len(pcl), dtype=np.int32)), ("PCL_MASKS", pcl)]},
+            self.bins._fits_table("BANDPOWERS"),
+        ])
+
+    def read_from(self, fname, device=None):
+        """Read a workspace from a NaMaster-compatible FITS file (workspaces.py:2162-2209)
+        onto `device` (the current CUDA device by default), then bin and LU-factor it."""
+        hdus = {h["name"]: h for h in fits.read(fname)}
+        prim = hdus.get("WSP_PRIMARY") or fits.read(fname)[0]
+        h = prim["header"]
+        if bool(h.get("IS_TEB", False)):
+            raise NotImplementedError("joint TEB workspaces are not part of this build")
+        if any(bool(h.get(k, False)) for k in ("PURE_E1", "PURE_B1", "PURE_E2", "PURE_B2",
+                                               "ANISO1", "ANISO2")):
+            raise NotImplementedError("purified or anisotropic workspaces are not part of this build")
+        dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+        self.lmax = int(h["LMAX"])
+        self.lmax_mask = int(h["LMAX_MASK"])
+        self.ncls = int(h["NCLS"])
+        self.normalization = "MASTER" if int(h.get("NORM_TYPE", 0)) == 0 else "FKP"
+        self.wawb = float(h.get("WAWB", 0.0))
+        self.spin1 = int(h.get("SPIN1", 0 if self.ncls == 1 else 2))
+        self.spin2 = int(h.get("SPIN2", 0 if self.ncls == 1 else 2))
+        self.nmaps1 = 1 if self.spin1 == 0 else 2
+        self.nmaps2 = 1 if self.spin2 == 0 else 2
+        self.l_toeplitz = int(h.get("L_TOEPLITZ", -1))
+        self.l_exact = int(h.get("L_EXACT", -1))
+        self.dl_band = int(h.get("DL_BAND", -1))
+        self.mcm_blocks = _blocks_from_dense(prim["data"], self.lmax, self.ncls, dev)
+        beams = hdus["BEAMS"]["data"]
+        if "BEAMS" in beams:
+            b1 = b2 = np.sqrt(beams["BEAMS"].astype(np.float64))
+        else:
+            b1, b2 = beams["BEAM1"].astype(np.float64), beams["BEAM2"].astype(np.float64)
+        self.beam1 = torch.from_numpy(np.ascontiguousarray(b1)).to(dev)
+        self.beam2 = torch.from_numpy(np.ascontiguousarray(b2)).to(dev)
+        self.pcl_mask = torch.from_numpy(
+            np.ascontiguousarray(hdus["PCL_MASKS"]["data"]["PCL_MASKS"], dtype=np.float64)).to(dev)
+        nw = min(self.pcl_mask.shape[0], 2 * self.lmax + 1)
+        self.window = self.pcl_mask[:nw].contiguous()
+        self.bins = NmtBin._from_fits_table(hdus["BINS"] if "BINS" in hdus else hdus["BANDPOWERS"])
+        self.nbands = self.bins.get_n_bands()
+        self._postprocess()
 
     def compute_coupling_matrix(self, fl1, fl2, bins, is_teb=False, l_toeplitz=-1, l_exact=-1,
                                 dl_band=-1, normalization="MASTER"):
