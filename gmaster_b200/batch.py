@@ -27,7 +27,7 @@ that loop for a whole batch at once:
 import numpy as np
 import torch
 
-from . import sht, sht_tc
+from . import _lib, sht, sht_tc
 from ._config import get_precision, nmt_params
 from .field import NmtField
 from .utils import as_device
@@ -36,13 +36,15 @@ from .workspaces import (NmtWorkspace, _which, compute_coupled_cell, coupling_bl
 
 
 def fields_from_maps(mask, maps, *, spin=None, n_iter=None, beam=None, lmax=None,
-                     masked_on_input=False, precision=None):
+                     masked_on_input=False, precision=None, ring_spectra=None):
     """Lite fields of a batch of simulations sharing one mask.
 
     ``maps`` is (nsims, npix) or (nsims, 1, npix) for spin 0 and (nsims, 2, npix) for
     spin 2 (Q, U), float64 on the host or the device.  Returns a list of ``nsims``
     ``NmtField`` objects whose alms equal those of ``NmtField(mask, maps[i], ...)``
-    up to the precision of the chosen transform.
+    up to the precision of the chosen transform.  ``ring_spectra`` (mixed precision, one
+    tensor-core launch) may hand over the ring spectra of the masked maps already
+    computed, in a one-element list that is emptied so the spectra can be released early.
     """
     precision = precision or get_precision()
     n_iter = nmt_params.n_iter_default if n_iter is None else int(n_iter)
@@ -79,8 +81,12 @@ def fields_from_maps(mask, maps, *, spin=None, n_iter=None, beam=None, lmax=None
                                               n_iter, "fp64") for i in range(chunk.shape[0])])
         else:
             # the ring stage multiplies by the mask as it reads the maps: no masked copy
+            spec = None
+            if ring_spectra and s0 == 0 and nsims <= per_launch:
+                spec = ring_spectra.pop()
             a = sht_tc.map2alm_tc(flat, spin, nside, lm, n_iter,
-                                  mask=None if masked_on_input else mask_t)
+                                  mask=None if masked_on_input else mask_t, ring_spectra=spec)
+            del spec
         del flat, chunk
         alms.append(a.reshape(-1, nmaps, a.shape[1]))
     alms = torch.cat(alms)
@@ -260,6 +266,36 @@ def _upload(x, dev):
     return d, ev
 
 
+def _stream_ring_spectra(t_maps, mask_t, dev, parts=4):
+    """Copy host T maps (nsims, npix) to the device in `parts` pieces on the side stream and
+    compute each piece's masked single-precision ring spectra on the current stream once
+    it has arrived.  Returns (device maps, [spectra])."""
+    h = t_maps if isinstance(t_maps, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(t_maps))
+    if h.dtype != torch.float64:
+        h = h.to(torch.float64)
+    h = h.reshape(h.shape[0], -1)
+    nsims, npix = h.shape
+    nside = int(round(np.sqrt(npix / 12)))
+    plan = sht.get_plan(nside, 3 * nside - 1, dev)
+    d = torch.empty((nsims, npix), dtype=torch.float64, device=dev)
+    spec = torch.empty((nsims, plan.nring, plan.L), dtype=torch.complex64, device=dev)
+    main = torch.cuda.current_stream(dev)
+    side = _copy_stream(dev)
+    side.wait_stream(main)
+    bounds = np.linspace(0, nsims, min(parts, nsims) + 1).astype(int)
+    events = []
+    with torch.cuda.stream(side):
+        for a, b in zip(bounds[:-1], bounds[1:]):
+            d[a:b].copy_(h[a:b], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(side)
+            events.append(ev)
+    for (a, b), ev in zip(zip(bounds[:-1], bounds[1:]), events):
+        main.wait_event(ev)
+        sht.ring_analysis(plan, d[a:b], _lib.MIXED, mask=mask_t, out=spec[a:b])
+    return d, [spec]
+
+
 def mc_bandpowers(mask, t_maps, qu_maps, w00, w02, w22, *, n_iter=None, precision=None):
     """Bandpowers of a batch of TQU simulations sharing one mask and three workspaces.
 
@@ -271,13 +307,24 @@ def mc_bandpowers(mask, t_maps, qu_maps, w00, w02, w22, *, n_iter=None, precisio
     """
     dev = torch.device("cuda", torch.cuda.current_device())
     mask_t = as_device(mask, torch.float64)
-    t_dev, ev_t = _upload(t_maps, dev)
-    qu_dev, ev_qu = _upload(qu_maps, dev)
+    precision = precision or get_precision()
     main = torch.cuda.current_stream(dev)
-    if ev_t is not None:
-        main.wait_event(ev_t)
-    ft = fields_from_maps(mask_t, t_dev, spin=0, n_iter=n_iter, precision=precision)
-    del t_dev
+    streamed = (precision != "fp64" and not (isinstance(t_maps, torch.Tensor) and t_maps.is_cuda)
+                and 1 <= len(t_maps) <= sht_tc.MAX_MAPS_SPIN0)
+    spec_box = None
+    if streamed:
+        # T maps in parts: the ring transform of each part runs as soon as it has arrived,
+        # behind the copies of the next parts and of the (Q, U) maps
+        t_dev, spec_box = _stream_ring_spectra(t_maps, mask_t, dev)
+        qu_dev, ev_qu = _upload(qu_maps, dev)
+    else:
+        t_dev, ev_t = _upload(t_maps, dev)
+        qu_dev, ev_qu = _upload(qu_maps, dev)
+        if ev_t is not None:
+            main.wait_event(ev_t)
+    ft = fields_from_maps(mask_t, t_dev, spin=0, n_iter=n_iter, precision=precision,
+                          ring_spectra=spec_box)
+    del t_dev, spec_box
     if ev_qu is not None:
         main.wait_event(ev_qu)
     fp = fields_from_maps(mask_t, qu_dev, spin=2, n_iter=n_iter, precision=precision)

@@ -194,16 +194,23 @@ def _complex_dtype(prec):
 
 # ----------------------------------------------------------------------------- stages
 
-def ring_analysis(plan, maps, prec, mask=None):
+def ring_analysis(plan, maps, prec, mask=None, out=None):
     """maps (ncomp, npix) float64/float32 CUDA -> ring spectra (ncomp, nring, L); `mask`
-    (npix,) float64, if given, multiplies every map as it is read."""
+    (npix,) float64, if given, multiplies every map as it is read.  `out`, if given, is a
+    contiguous (ncomp, nring, L) tensor of the precision's complex type to write into."""
     maps = maps.contiguous()
     ncomp = maps.shape[0]
     if mask is not None:
         mask = mask.to(torch.float64).contiguous()
         if mask.shape != (plan.npix,):
             raise ValueError("mask must be one HEALPix map of the same resolution")
-    spec = torch.empty((ncomp, plan.nring, plan.L), dtype=_complex_dtype(prec), device=plan.device)
+    if out is not None:
+        if (out.shape != (ncomp, plan.nring, plan.L) or out.dtype != _complex_dtype(prec)
+                or not out.is_contiguous()):
+            raise ValueError("out must be a contiguous (ncomp, nring, L) spectrum tensor")
+        spec = out
+    else:
+        spec = torch.empty((ncomp, plan.nring, plan.L), dtype=_complex_dtype(prec), device=plan.device)
     _lib.call("gm_ring_analysis", prec, plan.nside, plan.L, ncomp, _lib.ptr(maps),
               maps.element_size(), _lib.ptr(mask) if mask is not None else None,
               _lib.ptr(plan.tw), _lib.ptr(plan.shifted), _lib.ptr(spec),

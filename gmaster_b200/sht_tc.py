@@ -196,7 +196,7 @@ def _full_path_bytes(tp, spin, ncomp, n_iter):
     return max(spec + base, later)
 
 
-def map2alm_tc(maps, spin, nside, lmax, n_iter, mask=None, window=None):
+def map2alm_tc(maps, spin, nside, lmax, n_iter, mask=None, window=None, ring_spectra=None):
     """Batched analysis: maps (ncomp, npix) float64/float32 CUDA -> (ncomp, nelem) complex128
     (spin 2: rows E, B per field), with n_iter Jacobi iterations.  `mask` (npix,), if
     given, multiplies every map as the ring stage reads it.
@@ -206,7 +206,9 @@ def map2alm_tc(maps, spin, nside, lmax, n_iter, mask=None, window=None):
     sides, their operand images, the alm accumulator and the synthesis outputs (about
     106 GB for 64 maps at Nside 2048) besides the caller's maps.  When that does not fit in
     the free device memory (or `window`, a number of orders, is given) the transform runs
-    over windows of orders instead (`map2alm_tc_windowed`)."""
+    over windows of orders instead (`map2alm_tc_windowed`).  `ring_spectra`, if given, are
+    the single-precision ring spectra of the (masked) maps, already computed (a caller
+    that streams the maps in can transform each part as it arrives)."""
     ncomp = maps.shape[0]
     _check_batch(spin, ncomp)
     tp = get_tc_plan(nside, lmax, maps.device)
@@ -218,7 +220,10 @@ def map2alm_tc(maps, spin, nside, lmax, n_iter, mask=None, window=None):
             window = window_orders(tp, spin, ncomp)
     if window is not None:
         return map2alm_tc_windowed(maps, spin, nside, lmax, n_iter, mask=mask, window=window)
-    spec = sht.ring_analysis(p, maps, _lib.MIXED, mask=mask)
+    if ring_spectra is not None and ring_spectra.shape != (ncomp, p.nring, p.L):
+        raise ValueError("ring_spectra must be (ncomp, nring, L)")
+    spec = ring_spectra if ring_spectra is not None else sht.ring_analysis(p, maps, _lib.MIXED, mask=mask)
+    ring_spectra = None   # the spectra are released after packing unless the caller holds them
     b = _Batch(tp, spin, ncomp)
     # the spin-2 rows G_Q -+ i G_U are at most twice the largest ring value
     b.img_scale = pow2_scale(spec.view(torch.float32)) / (2.0 if spin else 1.0)
