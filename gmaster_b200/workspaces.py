@@ -134,40 +134,51 @@ def coupling_tt_toeplitz(window, lmax, l_toeplitz, l_exact, dl_band):
 def _blocks_from_dense(dense, lmax, ncls, device):
     """(4, L, L) blocks [tt, te, pp, mm] of a dense (ncls L)^2 coupling matrix in
     ``l * ncls + c`` order; the inverse of ``NmtWorkspace.get_coupling_matrix``.  Raises if
-    the matrix does not have the structure of a spin 0x0, 0x2 or 2x2 workspace."""
+    the matrix does not have the structure of a spin 0x0, 0x2, 2x2 or joint TEB workspace."""
     n = lmax + 1
     d = np.asarray(dense, dtype=np.float64)
     if d.shape != (ncls * n, ncls * n):
         raise ValueError(f"coupling matrix of shape {d.shape}, expected {(ncls * n, ncls * n)}")
+    if ncls not in (1, 2, 4, 7):
+        raise ValueError(f"unsupported number of spectra {ncls}")
+    q = d.reshape(n, ncls, n, ncls)
     blocks = np.zeros((4, n, n))
-    if ncls == 1:
-        blocks[_BLOCK_TT] = d
-        rebuilt = d
-    else:
-        q = d.reshape(n, ncls, n, ncls)
-        rebuilt = np.zeros_like(q)
-        if ncls == 2:
-            blocks[_BLOCK_TE] = q[:, 0, :, 0]
-            for c in range(2):
-                rebuilt[:, c, :, c] = blocks[_BLOCK_TE]
-        elif ncls == 4:
-            blocks[_BLOCK_PP] = q[:, 0, :, 0]
-            blocks[_BLOCK_MM] = q[:, 0, :, 3]
-            for c in range(4):
-                rebuilt[:, c, :, c] += blocks[_BLOCK_PP]
-            for c, sign in zip(range(4), (1.0, -1.0, -1.0, 1.0)):
-                rebuilt[:, c, :, 3 - c] += sign * blocks[_BLOCK_MM]
-        else:
-            raise ValueError(f"unsupported number of spectra {ncls}")
-        rebuilt = rebuilt.reshape(ncls * n, ncls * n)
+    seen = set()
+    for x, r, c, sign in _slots(ncls):
+        if x not in seen:
+            blocks[x] = sign * q[:, r, :, c]
+            seen.add(x)
+    rebuilt = np.zeros_like(q)
+    for x, r, c, sign in _slots(ncls):
+        rebuilt[:, r, :, c] += sign * blocks[x]
+    rebuilt = rebuilt.reshape(ncls * n, ncls * n)
     if not np.array_equal(rebuilt, d):
-        raise NotImplementedError("the coupling matrix is not that of a standard spin 0x0, 0x2 or "
-                                  "2x2 workspace")
+        raise NotImplementedError("the coupling matrix is not that of a standard spin 0x0, 0x2, "
+                                  "2x2 or joint TEB workspace")
     return torch.from_numpy(blocks).to(device)
 
 
 def _which(ncls):
-    return {1: 1, 2: 2, 4: 12}[ncls]
+    return {1: 1, 2: 2, 4: 12, 7: 15}[ncls]
+
+
+_MM_SIGNS = (1.0, -1.0, -1.0, 1.0)
+
+
+def _slots(ncls):
+    """(block, row channel, column channel, sign) of every block placement in the
+    (ncls L)^2 coupling matrix (workspaces.py:1856-1903): spin 0x0 [TT]; 0x2 [TE, TB];
+    2x2 [EE, EB, BE, BB]; joint TEB [TT, TE, TB, EE, EB, BE, BB].  The EE..BB part takes
+    M+ on its diagonal and M- on its anti-diagonal."""
+    if ncls == 1:
+        return [(_BLOCK_TT, 0, 0, 1.0)]
+    if ncls == 2:
+        return [(_BLOCK_TE, 0, 0, 1.0), (_BLOCK_TE, 1, 1, 1.0)]
+    off = 3 if ncls == 7 else 0
+    out = [(_BLOCK_TT, 0, 0, 1.0), (_BLOCK_TE, 1, 1, 1.0), (_BLOCK_TE, 2, 2, 1.0)] if ncls == 7 else []
+    out += [(_BLOCK_PP, off + c, off + c, 1.0) for c in range(4)]
+    out += [(_BLOCK_MM, off + c, off + 3 - c, _MM_SIGNS[c]) for c in range(4)]
+    return out
 
 
 class LUFactor:
@@ -185,6 +196,15 @@ class LUFactor:
         st = int(self.status.item())
         if st:
             raise np.linalg.LinAlgError(f"binned coupling matrix is singular (pivot {st - 1})")
+
+    def inverse(self):
+        """A^-1 (computed once from the factors, one right-hand side per column).  Many
+        right-hand sides at once are cheaper as one FP64 matrix product with it than as
+        triangular solves, which walk the rows one after another."""
+        if getattr(self, "_inv", None) is None:
+            eye = torch.eye(self.n, dtype=torch.float64, device=self.lu.device)
+            self._inv = self.solve(eye)
+        return self._inv
 
     def solve(self, b):
         """Solve A x = b for b of shape (n,) or (n, nrhs)."""
@@ -225,7 +245,8 @@ class NmtWorkspace:
         if self.mcm_blocks is None:
             raise RuntimeError("the workspace holds no coupling matrix")
         header = {
-            "LMAX": self.lmax, "LMAX_MASK": self.lmax_mask, "IS_TEB": False, "NCLS": self.ncls,
+            "LMAX": self.lmax, "LMAX_MASK": self.lmax_mask, "IS_TEB": bool(getattr(self, "is_teb", False)),
+            "NCLS": self.ncls,
             "NORM_TYPE": 0 if self.normalization == "MASTER" else 1, "WAWB": float(self.wawb),
             "SPIN1": self.spin1, "SPIN2": self.spin2, "ANISO1": False, "ANISO2": False,
             "PURE_E1": False, "PURE_B1": False, "PURE_E2": False, "PURE_B2": False,
@@ -250,8 +271,6 @@ class NmtWorkspace:
         hdus = {h["name"]: h for h in fits.read(fname)}
         prim = hdus.get("WSP_PRIMARY") or fits.read(fname)[0]
         h = prim["header"]
-        if bool(h.get("IS_TEB", False)):
-            raise NotImplementedError("joint TEB workspaces are not part of this build")
         if any(bool(h.get(k, False)) for k in ("PURE_E1", "PURE_B1", "PURE_E2", "PURE_B2",
                                                "ANISO1", "ANISO2")):
             raise NotImplementedError("purified or anisotropic workspaces are not part of this build")
@@ -259,6 +278,7 @@ class NmtWorkspace:
         self.lmax = int(h["LMAX"])
         self.lmax_mask = int(h["LMAX_MASK"])
         self.ncls = int(h["NCLS"])
+        self.is_teb = bool(h.get("IS_TEB", False))
         self.normalization = "MASTER" if int(h.get("NORM_TYPE", 0)) == 0 else "FKP"
         self.wawb = float(h.get("WAWB", 0.0))
         self.spin1 = int(h.get("SPIN1", 0 if self.ncls == 1 else 2))
@@ -298,8 +318,10 @@ class NmtWorkspace:
         if fl1.ainfo.lmax != bins.lmax:
             raise ValueError(f"Maximum multipoles in bins ({bins.lmax}) and fields "
                              f"({fl1.ainfo.lmax}) are not the same")
-        if is_teb:
-            raise NotImplementedError("joint TEB workspaces are not part of this build")
+        if is_teb and (fl1.spin != 0 or fl2.spin == 0):
+            raise ValueError("If is_teb=True, fl1 must be spin-0 and fl2 non-zero spin")
+        if is_teb and fl2.spin != 2:
+            raise NotImplementedError("only spin 0 and spin 2 fields are implemented")
         toeplitz_sanity(l_toeplitz, l_exact, dl_band, fl1.ainfo.lmax)
         if normalization not in ("MASTER", "FKP"):
             raise ValueError(f"Unknown normalization type {normalization}. "
@@ -307,7 +329,8 @@ class NmtWorkspace:
         self.spin1, self.spin2 = fl1.spin, fl2.spin
         self.nmaps1 = 1 if self.spin1 == 0 else 2
         self.nmaps2 = 1 if self.spin2 == 0 else 2
-        self.ncls = self.nmaps1 * self.nmaps2
+        self.ncls = 7 if is_teb else self.nmaps1 * self.nmaps2
+        self.is_teb = bool(is_teb)
         self.lmax = fl1.ainfo.lmax
         self.lmax_mask = fl1.ainfo_mask.lmax
         self.bins = bins
@@ -346,7 +369,7 @@ class NmtWorkspace:
             # exact blocks, then the Toeplitz fill (workspaces.py:1833-1844)
             col = (2.0 * torch.arange(self.lmax + 1, dtype=torch.float64,
                                       device=self.window.device) + 1.0)[None, :]
-            slots = {1: (_BLOCK_TT,), 2: (_BLOCK_TE,), 4: (_BLOCK_PP, _BLOCK_MM)}[self.ncls]
+            slots = sorted({x for x, _, _, _ in _slots(self.ncls)})
             for x in slots:
                 self.mcm_blocks[x] = toeplitz_fill((self.mcm_blocks[x] / col).contiguous(),
                                                    self.lmax, l_toeplitz, l_exact, dl_band)
@@ -358,6 +381,22 @@ class NmtWorkspace:
         N = self.ncls * self.nbands
         if self.normalization == "FKP":
             self.mcm_binned = self.wawb * torch.eye(N, dtype=torch.float64, device=dev)
+        elif self.ncls == 7:
+            # joint TEB: each distinct block binned on its own, then placed with its sign
+            nb = self.nbands
+            binned = {}
+            for x in sorted({x for x, _, _, _ in _slots(7)}):
+                scratch = torch.empty(2 * nb * nb, dtype=torch.float64, device=dev)
+                out = torch.empty((nb, nb), dtype=torch.float64, device=dev)
+                blk = self.mcm_blocks[x].contiguous()
+                _lib.call("gm_bin_coupling_csr", self.lmax, nb, 1, _lib.ptr(blk), _lib.ptr(ops["ptr"]),
+                          _lib.ptr(ops["ells"]), _lib.ptr(ops["wfl"]), _lib.ptr(ops["inv_fl"]),
+                          _lib.ptr(beam), _lib.ptr(scratch), _lib.ptr(out), _lib.stream_handle(dev))
+                binned[x] = out
+            full = torch.zeros((nb, 7, nb, 7), dtype=torch.float64, device=dev)
+            for x, r, c, sign in _slots(7):
+                full[:, r, :, c] += sign * binned[x]
+            self.mcm_binned = full.reshape(N, N)
         else:
             scratch = torch.empty(2 * self.nbands * self.nbands, dtype=torch.float64, device=dev)
             self.mcm_binned = torch.empty((N, N), dtype=torch.float64, device=dev)
@@ -374,14 +413,8 @@ class NmtWorkspace:
         if self.ncls == 1:
             return b[_BLOCK_TT].clone()
         out = torch.zeros((n, self.ncls, n, self.ncls), dtype=torch.float64, device=b.device)
-        if self.ncls == 2:
-            for c in range(2):
-                out[:, c, :, c] = b[_BLOCK_TE]
-        else:
-            for c in range(4):
-                out[:, c, :, c] += b[_BLOCK_PP]
-            for c, sign in zip(range(4), (1.0, -1.0, -1.0, 1.0)):
-                out[:, c, :, 3 - c] += sign * b[_BLOCK_MM]
+        for x, r, c, sign in _slots(self.ncls):
+            out[:, r, :, c] += sign * b[x]
         return out.reshape(self.ncls * n, self.ncls * n)
 
     def update_beams(self, beam1, beam2):
