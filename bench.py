@@ -220,18 +220,41 @@ def batch_step(mask, t, qu, ws, precision="mixed"):
                              precision=precision)
 
 
-def full_estimator(mask, t, qu, nside, nlb, precision):
+def full_estimator(mask, t, qu, nside, nlb, precision, stages=None):
     """The whole estimator from the maps: fields with their mask transforms, three
-    workspaces (pseudo-C_ell of the mask, 3j coupling, binning, LU), spectra."""
+    workspaces (pseudo-C_ell of the mask, 3j coupling, binning, LU), spectra.  With a dict
+    `stages`, the device time of each stage (ms, CUDA events) is added to it."""
+    import torch
+
     import gmaster_b200 as nmt
 
+    marks = []
+
+    def mark(name):
+        if stages is not None:
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record()
+            marks.append((name, ev))
+
+    # a fresh mask tensor: the mask alms are computed once per call (shared by the two
+    # fields of the call), not served from an earlier call
+    mask = mask.clone()
+    mark("start")
     ft = nmt.NmtField(mask, t, n_iter=3, precision=precision)
+    mark("T field (map and mask transforms)")
     fp = nmt.NmtField(mask, qu, n_iter=3, precision=precision)
+    mark("QU field")
     b = nmt.NmtBin.from_nside_linear(nside, nlb)
     out = []
-    for f1, f2 in ((ft, ft), (ft, fp), (fp, fp)):
+    for name, (f1, f2) in zip(("00", "02", "22"), ((ft, ft), (ft, fp), (fp, fp))):
         w = nmt.NmtWorkspace.from_fields(f1, f2, b)
+        mark(f"workspace {name}")
         out.append(w.decouple_cell(nmt.compute_coupled_cell(f1, f2)))
+        mark(f"spectra {name}")
+    if stages is not None:
+        torch.cuda.synchronize()
+        for (_, a), (name, b_) in zip(marks[:-1], marks[1:]):
+            stages[name] = stages.get(name, 0.0) + a.elapsed_time(b_)
     return out
 
 
@@ -666,6 +689,7 @@ def main():
 
     # full estimator from scratch for one simulation (seconds per spectrum)
     s_per_spec = {}
+    spec_stages = {}
     for prec in ("mixed", "fp64"):
         full_estimator(mask, t_all[:1], qu_all[0], nside, nlb, prec)
         torch.cuda.synchronize()
@@ -673,6 +697,9 @@ def main():
         full_estimator(mask, t_all[:1], qu_all[0], nside, nlb, prec)
         torch.cuda.synchronize()
         s_per_spec[prec] = time.perf_counter() - t0
+        stages = {}
+        full_estimator(mask, t_all[:1], qu_all[0], nside, nlb, prec, stages=stages)
+        spec_stages[prec] = {k: round(v, 2) for k, v in stages.items()}
 
     _, ws_mixed = build_workspaces(mask, nside, nlb, "mixed")
     _, ws_fp64 = build_workspaces(mask, nside, nlb, "fp64")
@@ -821,6 +848,7 @@ def main():
         "mixed_unbatched": {"value": world * 1e3 / ms1, "unit": "sims/s", "ms_per_sim": ms1},
         "speedup_mixed_vs_fp64": value / value64,
         "s_per_spectrum": s_per_spec,
+        "s_per_spectrum_stages_ms": spec_stages,
         "bandpower_err_mixed_vs_fp64": {"max_abs_over_scale": errs, "max_rel_auto": rel_auto,
                                         "max_in_sigma_cv": sig_cv, "fsky": fsky},
         "clocks": clocks,

@@ -70,6 +70,8 @@ SIGNATURES = {
                                    _c_dbl, _c_int, _c_vp], _c_int),
     "gm_legendre_synthesis_tile": ([_c_int, _c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp,
                                     _c_int, _c_vp], _c_int),
+    "gm_lu_panel": ([_c_i64, _c_vp, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp], _c_int),
+    "gm_lu_trsm": ([_c_i64, _c_vp, _c_i64, _c_i64, _c_vp], _c_int),
     "gm_tc_pack_window": ([_c_i64, _c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_i64,
                            _c_i64, _c_vp], _c_int),
     "gm_tc_analysis_window": ([_c_i64, _c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,

@@ -457,6 +457,89 @@ __global__ void __launch_bounds__(1024) k_lu_factor(int64_t n, double *__restric
     }
 }
 
+// Blocked LU, panel step: columns [k0, k1) of the row-major (n, n) matrix, rows k0..n-1,
+// one CTA.  Partial pivoting as in k_lu_factor (the pivot swap moves whole rows, all n
+// columns, so the left factor and the trailing part stay consistent); the rank-1 updates
+// are confined to the panel's columns.  The caller then solves for the U rows right of
+// the panel (k_lu_trsm) and updates the trailing matrix with one GEMM.
+__global__ void __launch_bounds__(1024) k_lu_panel(int64_t n, int64_t k0, int64_t k1,
+                                                   double *__restrict__ a, int32_t *__restrict__ piv,
+                                                   int32_t *__restrict__ status)
+{
+    __shared__ double sval[32];
+    __shared__ int sidx[32];
+    __shared__ int pivot_row;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    for (int64_t k = k0; k < k1; ++k) {
+        double best = -1.0;
+        int bi = (int)k;
+        for (int64_t i = k + tid; i < n; i += blockDim.x) {
+            const double v = fabs(a[i * n + k]);
+            if (v > best) {
+                best = v;
+                bi = (int)i;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_down_sync(0xffffffffu, best, o);
+            const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+            if (ov > best || (ov == best && oi < bi)) {
+                best = ov;
+                bi = oi;
+            }
+        }
+        if (lane == 0) {
+            sval[warp] = best;
+            sidx[warp] = bi;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double bv = sval[0];
+            int bix = sidx[0];
+            for (int w = 1; w < nwarps; ++w)
+                if (sval[w] > bv || (sval[w] == bv && sidx[w] < bix)) {
+                    bv = sval[w];
+                    bix = sidx[w];
+                }
+            pivot_row = bix;
+            piv[k] = bix;
+            if (bv == 0.0 && *status == 0) *status = (int32_t)(k + 1);
+        }
+        __syncthreads();
+        const int64_t p = pivot_row;
+        if (p != k)
+            for (int64_t jj = tid; jj < n; jj += blockDim.x) {
+                const double t = a[k * n + jj];
+                a[k * n + jj] = a[p * n + jj];
+                a[p * n + jj] = t;
+            }
+        __syncthreads();
+        const double d = a[k * n + k];
+        const double inv = d != 0.0 ? 1.0 / d : 0.0;
+        for (int64_t i = k + 1 + tid; i < n; i += blockDim.x) a[i * n + k] *= inv;
+        __syncthreads();
+        for (int64_t i = k + 1 + warp; i < n; i += nwarps) {
+            const double lik = a[i * n + k];
+            if (lik != 0.0)
+                for (int64_t jj = k + 1 + lane; jj < k1; jj += 32) a[i * n + jj] -= lik * a[k * n + jj];
+        }
+        __syncthreads();
+    }
+}
+
+// Blocked LU, U rows right of the panel: rows [k0, k1), columns [k1, n) become
+// L11^-1 times themselves (L11 unit lower triangular); one thread per column.
+__global__ void k_lu_trsm(int64_t n, int64_t k0, int64_t k1, double *__restrict__ a)
+{
+    const int64_t col = k1 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= n) return;
+    for (int64_t i = k0 + 1; i < k1; ++i) {
+        double s = a[i * n + col];
+        for (int64_t j = k0; j < i; ++j) s -= a[i * n + j] * a[j * n + col];
+        a[i * n + col] = s;
+    }
+}
+
 // One warp per right-hand-side column: P, then L (unit) forward, then U backward.
 // b is (n, nrhs) row-major.
 __global__ void k_lu_solve(int64_t n, const double *__restrict__ lu, const int32_t *__restrict__ piv,
@@ -630,6 +713,24 @@ extern "C" int gm_lu_factor(int64_t n, double *a, int32_t *piv, int32_t *status,
     if (!a || !piv || !status) return GM_ERR_BAD_PTR;
     k_lu_factor<<<1, 1024, 0, as_stream(stream)>>>(n, a, piv, status);
     return check_launch("gm_lu_factor");
+}
+
+extern "C" int gm_lu_panel(int64_t n, double *a, int64_t k0, int64_t k1, int32_t *piv,
+                           int32_t *status, void *stream)
+{
+    if (n < 1 || n > 65535 || k0 < 0 || k1 <= k0 || k1 > n) return GM_ERR_BAD_SHAPE;
+    if (!a || !piv || !status) return GM_ERR_BAD_PTR;
+    k_lu_panel<<<1, 1024, 0, as_stream(stream)>>>(n, k0, k1, a, piv, status);
+    return check_launch("gm_lu_panel");
+}
+
+extern "C" int gm_lu_trsm(int64_t n, double *a, int64_t k0, int64_t k1, void *stream)
+{
+    if (n < 1 || n > 65535 || k0 < 0 || k1 <= k0 || k1 > n) return GM_ERR_BAD_SHAPE;
+    if (!a) return GM_ERR_BAD_PTR;
+    if (k1 == n) return GM_OK;
+    k_lu_trsm<<<(unsigned)((n - k1 + 127) / 128), 128, 0, as_stream(stream)>>>(n, k0, k1, a);
+    return check_launch("gm_lu_trsm");
 }
 
 extern "C" int gm_lu_solve(int64_t n, const double *lu, const int32_t *piv, int64_t nrhs,

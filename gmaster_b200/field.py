@@ -6,12 +6,43 @@ purification and anisotropic masks are outside this build and raise
 ``NotImplementedError``.
 """
 
+import weakref
+
 import numpy as np
 import torch
 
 from . import sht
 from ._config import get_precision, nmt_params
 from .utils import NmtAlmInfo, NmtMapInfo, as_device
+
+
+# Mask alms shared by the fields built on the same mask tensor: a TQU estimator makes a
+# spin-0 and a spin-2 field on one mask, and each would otherwise transform the mask.
+# Keyed by the identity of the mask tensor (a weak reference confirms it is still the same
+# object; the entry is dropped when the tensor is released), then by its in-place version
+# counter and the transform parameters, so a mask changed in place is never served stale.
+_MASK_ALMS = {}
+
+
+def _mask_key(field):
+    return (field.mask._version, field.ainfo_mask.lmax, field.n_iter_mask, field.precision)
+
+
+def _cached_mask_alms(field):
+    entry = _MASK_ALMS.get(id(field.mask))
+    if entry is None or entry[0]() is not field.mask:
+        return None
+    return entry[1].get(_mask_key(field))
+
+
+def _store_mask_alms(field, alms):
+    key = id(field.mask)
+    entry = _MASK_ALMS.get(key)
+    if entry is None or entry[0]() is not field.mask:
+        ref = weakref.ref(field.mask, lambda _r, k=key: _MASK_ALMS.pop(k, None))
+        entry = (ref, {})
+        _MASK_ALMS[key] = entry
+    entry[1][_mask_key(field)] = alms
 
 
 class NmtField:
@@ -87,11 +118,15 @@ class NmtField:
         if not masked_on_input:
             maps_t = maps_t * self.mask[None, :]
         nside = self.minfo.nside
-        if (self.spin == 0 and not self.lite and self.ainfo == self.ainfo_mask
+        cached = _cached_mask_alms(self)
+        if cached is not None and not self.lite:
+            self.alm_mask = cached
+        if (self.spin == 0 and not self.lite and cached is None and self.ainfo == self.ainfo_mask
                 and self.n_iter == self.n_iter_mask):
             both = sht.map2alm_device(torch.cat([maps_t, self.mask[None, :]]), 0, nside,
                                       self.ainfo.lmax, self.n_iter, self.precision)
             self.alm, self.alm_mask = both[0:1], both[1]
+            _store_mask_alms(self, self.alm_mask)
         else:
             self.alm = sht.map2alm_device(maps_t, self.spin, nside, self.ainfo.lmax, self.n_iter,
                                           self.precision)
@@ -122,8 +157,11 @@ class NmtField:
     def get_mask_alms(self):
         """Mask alms (nelem_mask,), computed on first call (gmaster/field.py:348-376)."""
         if self.alm_mask is None:
-            alms = sht.map2alm_device(self.mask[None, :], 0, self.minfo.nside, self.ainfo_mask.lmax,
-                                      self.n_iter_mask, self.precision)[0]
+            alms = _cached_mask_alms(self)
+            if alms is None:
+                alms = sht.map2alm_device(self.mask[None, :], 0, self.minfo.nside, self.ainfo_mask.lmax,
+                                          self.n_iter_mask, self.precision)[0]
+                _store_mask_alms(self, alms)
             if not self.lite:
                 self.alm_mask = alms
             return alms

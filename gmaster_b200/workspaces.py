@@ -184,13 +184,28 @@ def _slots(ncls):
 class LUFactor:
     """FP64 LU factorisation with partial pivoting of a square device matrix."""
 
+    # matrices above this order are factored in panels of _PANEL columns, the trailing
+    # updates as FP64 GEMMs; smaller ones in one single-CTA kernel
+    _BLOCKED_FROM = 256
+    _PANEL = 64
+
     def __init__(self, a):
         self.n = a.shape[0]
         self.lu = a.contiguous().clone()
         self.piv = torch.empty(self.n, dtype=torch.int32, device=a.device)
-        self.status = torch.empty(1, dtype=torch.int32, device=a.device)
-        _lib.call("gm_lu_factor", self.n, _lib.ptr(self.lu), _lib.ptr(self.piv),
-                  _lib.ptr(self.status), _lib.stream_handle(a.device))
+        self.status = torch.zeros(1, dtype=torch.int32, device=a.device)
+        st = _lib.stream_handle(a.device)
+        if self.n <= self._BLOCKED_FROM:
+            _lib.call("gm_lu_factor", self.n, _lib.ptr(self.lu), _lib.ptr(self.piv),
+                      _lib.ptr(self.status), st)
+            return
+        n, A = self.n, self.lu
+        for k0 in range(0, n, self._PANEL):
+            k1 = min(n, k0 + self._PANEL)
+            _lib.call("gm_lu_panel", n, _lib.ptr(A), k0, k1, _lib.ptr(self.piv), _lib.ptr(self.status), st)
+            if k1 < n:
+                _lib.call("gm_lu_trsm", n, _lib.ptr(A), k0, k1, st)
+                A[k1:, k1:].addmm_(A[k1:, k0:k1], A[k0:k1, k1:], alpha=-1.0)
 
     def check(self):
         st = int(self.status.item())

@@ -148,3 +148,34 @@ def test_legendre_tile_list():
     with pytest.raises(ValueError):
         autotune.tiles(1)
     assert not autotune.autotune_enabled() or "GMASTER_B200_AUTOTUNE" in __import__("os").environ
+
+
+def test_mask_alm_cache_follows_the_mask_tensor():
+    """Mask alms are shared between fields of one mask tensor, never served after the
+    mask changed in place, and dropped with the tensor."""
+    import gc
+
+    import torch
+
+    from gmaster_b200 import field as F
+
+    class _Info:
+        lmax = 5
+
+    class _Field:
+        pass
+
+    f = _Field()
+    f.mask, f.ainfo_mask, f.n_iter_mask, f.precision = torch.zeros(12), _Info(), 3, "mixed"
+    assert F._cached_mask_alms(f) is None
+    F._store_mask_alms(f, torch.ones(3))
+    assert F._cached_mask_alms(f) is not None
+    f.precision = "fp64"
+    assert F._cached_mask_alms(f) is None
+    f.precision = "mixed"
+    f.mask.add_(1.0)
+    assert F._cached_mask_alms(f) is None
+    n = len(F._MASK_ALMS)
+    del f.mask
+    gc.collect()
+    assert len(F._MASK_ALMS) == n - 1
