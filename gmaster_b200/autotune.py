@@ -7,8 +7,10 @@ tuner times every shape on operands of the real size, with CUDA events, the firs
 (device, kind, precision, spin, nside, lmax, ncomp) combination is transformed, and keeps
 the fastest.  The reference fixes its march tiles by rule (march_v2.py:290-332).
 
-Tuning is off unless ``set_autotune(True)`` is called or ``GMASTER_B200_AUTOTUNE=1`` is
-set; without it the kernels' built-in choice runs.  Choices live in memory; with
+Tuning is on by default; ``set_autotune(False)`` or ``GMASTER_B200_AUTOTUNE=0`` turns it
+off, and the kernels' built-in choice runs.  Tuning launches kernels and waits on events,
+so a transform captured in a CUDA graph must have run once before the capture (its choice
+is then cached).  Choices live in memory; with
 ``GMASTER_B200_TUNE_CACHE`` naming a JSON file they are also read from and written to it.
 """
 
@@ -24,7 +26,7 @@ from . import _lib
 _CACHE = {}
 _TIMINGS = {}
 _LOCK = threading.Lock()
-_STATE = {"enabled": os.environ.get("GMASTER_B200_AUTOTUNE", "0") == "1", "loaded": False}
+_STATE = {"enabled": os.environ.get("GMASTER_B200_AUTOTUNE", "1") != "0", "loaded": False}
 
 
 def set_autotune(flag):

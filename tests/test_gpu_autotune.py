@@ -46,6 +46,7 @@ def test_every_tile_matches_default(cuda, prec, tol, spin, ncomp):
 
 def test_autotuner_choice_is_cached_and_used(cuda):
     plan = sht.get_plan(16, 47)
+    was = autotune.autotune_enabled()
     autotune.set_autotune(True)
     try:
         maps = torch.randn((2, plan.npix), dtype=torch.float64, device="cuda")
@@ -56,4 +57,5 @@ def test_autotuner_choice_is_cached_and_used(cuda):
     finally:
         autotune.set_autotune(False)
     want = sht.map2alm_device(maps, 2, 16, 47, 1, "mixed")
+    autotune.set_autotune(was)
     assert float((got - want).abs().max() / want.abs().max()) < 2e-6
