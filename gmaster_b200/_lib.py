@@ -72,6 +72,11 @@ SIGNATURES = {
                                     _c_int, _c_vp], _c_int),
     "gm_lu_panel": ([_c_i64, _c_vp, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp], _c_int),
     "gm_lu_trsm": ([_c_i64, _c_vp, _c_i64, _c_i64, _c_vp], _c_int),
+    "gm_ring_big_scratch_bytes": ([_c_i64, _c_i64], _c_i64),
+    "gm_ring_analysis_ws": ([_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_int, _c_vp, _c_vp, _c_vp, _c_vp,
+                             _c_vp, _c_i64, _c_i64, _c_i64, _c_vp], _c_int),
+    "gm_ring_synthesis_ws": ([_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_i64,
+                              _c_i64, _c_i64, _c_vp], _c_int),
     "gm_tc_pack_window": ([_c_i64, _c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_i64,
                            _c_i64, _c_vp], _c_int),
     "gm_tc_analysis_window": ([_c_i64, _c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
@@ -99,7 +104,7 @@ LAUNCHES = {"gm_last_error": 0, "gm_version": 0, "gm_ring_twiddle_count": 0,
             "gm_seed_table_len": 0, "gm_bin_coupling_csr": 3, "gm_tc_lane_groups": 0,
             "gm_tc_ana_image_bytes": 0, "gm_tc_ana_scratch_bytes": 0,
             "gm_tc_syn_chunk_offsets": 0, "gm_tc_syn_image_bytes": 0, "gm_legendre_tiles": 0,
-            "gm_coupling_units": 0}
+            "gm_coupling_units": 0, "gm_ring_big_scratch_bytes": 0}
 CALLS = {}
 
 

@@ -241,6 +241,22 @@ static inline int bluestein_mcap(int64_t nside)
     return (int)m;
 }
 
+// Rings beyond the shared-memory kernels: half-length above `hcap` (the ping-pong buffers
+// would not fit), or, in single precision, a prime factor above 64 with a Bluestein length
+// 2h - 1 < M above `bsmin` (8192, the shared-memory Bluestein length; 0: none) for which the
+// M-point table exists (M <= 4 nside).  They are transformed by the persistent *_big kernels
+// in global scratch.
+__host__ __device__ __forceinline__ bool bluestein_big(int h, int nside, int bsmin)
+{
+    const int M = next_pow2(2 * h - 1);
+    return bsmin > 0 && largest_prime_factor(h) > 64 && M > bsmin && M <= 4 * nside;
+}
+
+__host__ __device__ __forceinline__ bool ring_big(int h, int hcap, int nside, int bsmin)
+{
+    return h > hcap || bluestein_big(h, nside, bsmin);
+}
+
 // Load one ring of one map (times the mask) as h complex z_t = x_2t + i x_2t+1, each
 // multiplied by f(t) (the Bluestein chirp, or 1).
 template <typename T, typename Tin, typename T2, typename F>
@@ -315,7 +331,7 @@ __global__ void __launch_bounds__(512) k_ring_analysis(int64_t nside, int64_t L,
                                                        int64_t twcnt,
                                                        const uint8_t *__restrict__ shifted,
                                                        typename vec2<T>::type *__restrict__ out,
-                                                       int mcap)
+                                                       int mcap, int hcap, int bsmin)
 {
     using T2 = typename vec2<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -323,9 +339,10 @@ __global__ void __launch_bounds__(512) k_ring_analysis(int64_t nside, int64_t L,
     const int64_t nring = 4 * nside - 1, npix = 12 * nside * nside;
     const int n = (int)ring_nphi(nside, r), h = n / 2;
     if (mcap > 0 && use_bluestein(h, mcap)) return;
+    if (ring_big(h, hcap, (int)nside, bsmin)) return;   // left to k_ring_analysis_big
     const int64_t off = ring_offset(nside, r);
     T2 *A = reinterpret_cast<T2 *>(smem_raw);
-    T2 *B = A + 2 * nside;
+    T2 *B = A + hcap;
     const T2 *tw = TwTable<T2>::get(twall, twcnt) + twiddle_offset(n);
     load_ring<T>(maps + c * npix + off, mask ? mask + off : nullptr, h, A,
                  [](int, T2 z) { return z; });
@@ -343,6 +360,7 @@ __global__ void __launch_bounds__(512) k_ring_analysis(int64_t nside, int64_t L,
 template <typename Tin>
 __global__ void __launch_bounds__(512) k_ring_analysis_bluestein(int64_t nside, int64_t L,
                                                                  int64_t ncomp, int cpc, int mcap,
+                                                                 int hcap, int bsmin,
                                                                  const Tin *__restrict__ maps,
                                                                  const double *__restrict__ mask,
                                                                  const void *__restrict__ twall,
@@ -354,7 +372,7 @@ __global__ void __launch_bounds__(512) k_ring_analysis_bluestein(int64_t nside, 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int64_t r = blockIdx.x;
     const int n = (int)ring_nphi(nside, r), h = n / 2;
-    if (!use_bluestein(h, mcap)) return;
+    if (!use_bluestein(h, mcap) || ring_big(h, hcap, (int)nside, bsmin)) return;
     const int M = next_pow2(2 * h - 1);
     const int64_t nring = 4 * nside - 1, npix = 12 * nside * nside;
     const int64_t off = ring_offset(nside, r);
@@ -523,19 +541,21 @@ __global__ void __launch_bounds__(512) k_ring_synthesis(int64_t nside, int64_t L
                                                         const void *__restrict__ twall,
                                                         int64_t twcnt,
                                                         const uint8_t *__restrict__ shifted,
-                                                        double *__restrict__ maps)
+                                                        double *__restrict__ maps, int hcap,
+                                                        int bsmin)
 {
     using T2 = typename vec2<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int64_t r = blockIdx.x, c = blockIdx.y;
     const int64_t npix = 12 * nside * nside, nlanes = 2 * nside;
     const int n = (int)ring_nphi(nside, r), h = n / 2;
+    if (ring_big(h, hcap, (int)nside, bsmin)) return;   // left to k_ring_synthesis_big
     const int64_t off = ring_offset(nside, r);
     const bool south = r >= nlanes;
     const int64_t j = south ? 4 * nside - 2 - r : r;
     const bool sh = shifted[r] != 0;
     T2 *A = reinterpret_cast<T2 *>(smem_raw);
-    T2 *B = A + 2 * nside;
+    T2 *B = A + hcap;
     const T2 *tw = TwTable<T2>::get(twall, twcnt) + twiddle_offset(n);
     T2 cpi;   // e^{-i pi / n}
     {
@@ -572,6 +592,179 @@ __global__ void __launch_bounds__(512) k_ring_synthesis(int64_t nside, int64_t L
         T2 z = Z[t];
         dst[2 * t] = (double)z.x;
         dst[2 * t + 1] = (double)z.y;
+    }
+}
+
+
+// ---------------------------------------------------------------- rings beyond shared memory
+//
+// One persistent CTA per slot of the global scratch (three buffers of Mmax complex floats
+// each) walks the rings; only the rings of ring_big are transformed, with the arithmetic of
+// the shared-memory kernels: a Stockham FFT of length h, or Bluestein's method with a
+// power-of-two length M.  __syncthreads orders the CTA's global-memory accesses.
+
+__device__ __forceinline__ float2 bs_chirp(const float2 *__restrict__ tw, int h, int n, int j, int sign)
+{
+    const unsigned q = ((unsigned)j * (unsigned)j) % (unsigned)n;
+    return twiddle_n(tw, h, (int)q, sign);   // e^{sign i pi j^2 / h}
+}
+
+// Bluestein filter: the transform of the wrapped conjugate chirp of length M; returns the
+// buffer holding it (b0 or b1).
+__device__ float2 *bs_filter(int h, int n, int M, const float2 *__restrict__ tw,
+                             const float2 *__restrict__ twM, int sign, float2 *b0, float2 *b1)
+{
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+        float2 v = make_float2(0.f, 0.f);
+        int j = -1;
+        if (m < h) j = m;
+        else if (m > M - h) j = M - m;
+        if (j >= 0) {
+            v = bs_chirp(tw, h, n, j, sign);
+            v.y = -v.y;
+        }
+        b0[m] = v;
+    }
+    __syncthreads();
+    return fft_shared<1>(b0, b1, M, twM, -1);
+}
+
+// X[0, h) holds z_j c_j; zero-pads to M, convolves with the filter FB and returns the buffer
+// holding the DFT sum_j z_j e^{sign 2 pi i jk / h}, k < h.
+__device__ float2 *bs_apply(float2 *X, float2 *Y, const float2 *FB, int h, int n, int M,
+                            const float2 *__restrict__ tw, const float2 *__restrict__ twM, int sign)
+{
+    for (int j = h + threadIdx.x; j < M; j += blockDim.x) X[j] = make_float2(0.f, 0.f);
+    __syncthreads();
+    float2 *FA = fft_shared<1>(X, Y, M, twM, -1);
+    float2 *G = (FA == X) ? Y : X;
+    const float invM = 1.0f / (float)M;
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+        float2 v = cmul(FA[m], FB[m]);
+        v.x *= invM;
+        v.y *= invM;
+        FA[m] = v;
+    }
+    __syncthreads();
+    float2 *R = fft_shared<1>(FA, G, M, twM, +1);
+    float2 *Z = (R == FA) ? G : FA;
+    for (int k = threadIdx.x; k < h; k += blockDim.x) Z[k] = cmul(R[k], bs_chirp(tw, h, n, k, sign));
+    __syncthreads();
+    return Z;
+}
+
+template <typename Tin>
+__global__ void __launch_bounds__(512) k_ring_analysis_big(int64_t nside, int64_t L, int64_t ncomp,
+                                                           const Tin *__restrict__ maps,
+                                                           const double *__restrict__ mask,
+                                                           const void *__restrict__ twall,
+                                                           int64_t twcnt,
+                                                           const uint8_t *__restrict__ shifted,
+                                                           float2 *__restrict__ out, int hcap,
+                                                           int bsmin, float2 *__restrict__ gbuf,
+                                                           int64_t Mmax)
+{
+    const int64_t nring = 4 * nside - 1, npix = 12 * nside * nside;
+    float2 *b0 = gbuf + (int64_t)blockIdx.x * 3 * Mmax, *b1 = b0 + Mmax, *b2 = b1 + Mmax;
+    const float2 *tw32 = TwTable<float2>::get(twall, twcnt);
+    const float w = (float)(4.0 * M_PI / (double)npix);
+    for (int64_t r = blockIdx.x; r < nring; r += gridDim.x) {
+        const int n = (int)ring_nphi(nside, r), h = n / 2;
+        if (!ring_big(h, hcap, (int)nside, bsmin)) continue;
+        const int64_t off = ring_offset(nside, r);
+        const float2 *tw = tw32 + twiddle_offset(n);
+        const bool sh = shifted[r] != 0;
+        const bool bs = bluestein_big(h, (int)nside, bsmin);
+        const int M = bs ? next_pow2(2 * h - 1) : 0;
+        const float2 *twM = bs ? tw32 + twiddle_offset(M) : nullptr;
+        float2 *FB = nullptr, *X = b0, *Y = b1;
+        if (bs) {
+            FB = bs_filter(h, n, M, tw, twM, -1, b0, b1);
+            X = (FB == b0) ? b1 : b0;
+            Y = b2;
+        }
+        for (int64_t c = 0; c < ncomp; ++c) {
+            float2 *Z;
+            if (bs) {
+                load_ring<float>(maps + c * npix + off, mask ? mask + off : nullptr, h, X,
+                                 [&](int t, float2 z) { return cmul(z, bs_chirp(tw, h, n, t, -1)); });
+                __syncthreads();
+                Z = bs_apply(X, Y, FB, h, n, M, tw, twM, -1);
+            } else {
+                load_ring<float>(maps + c * npix + off, mask ? mask + off : nullptr, h, X,
+                                 [](int, float2 z) { return z; });
+                __syncthreads();
+                Z = fft_shared(X, Y, h, tw, -1);
+            }
+            ring_outputs<float>(Z, n, L, tw, sh, w, out + (c * nring + r) * L);
+            __syncthreads();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(512) k_ring_synthesis_big(int64_t nside, int64_t L, int64_t ncomp,
+                                                            const float *__restrict__ syn,
+                                                            const void *__restrict__ twall,
+                                                            int64_t twcnt,
+                                                            const uint8_t *__restrict__ shifted,
+                                                            double *__restrict__ maps, int hcap,
+                                                            int bsmin, float2 *__restrict__ gbuf,
+                                                            int64_t Mmax)
+{
+    const int64_t nring = 4 * nside - 1, npix = 12 * nside * nside, nlanes = 2 * nside;
+    float2 *b0 = gbuf + (int64_t)blockIdx.x * 3 * Mmax, *b1 = b0 + Mmax, *b2 = b1 + Mmax;
+    const float2 *tw32 = TwTable<float2>::get(twall, twcnt);
+    for (int64_t r = blockIdx.x; r < nring; r += gridDim.x) {
+        const int n = (int)ring_nphi(nside, r), h = n / 2;
+        if (!ring_big(h, hcap, (int)nside, bsmin)) continue;
+        const int64_t off = ring_offset(nside, r);
+        const bool south = r >= nlanes;
+        const int64_t j = south ? 4 * nside - 2 - r : r;
+        const bool sh = shifted[r] != 0;
+        const float2 *tw = tw32 + twiddle_offset(n);
+        float2 cpi;
+        {
+            double s1, c1d;
+            sincospi(-1.0 / (double)n, &s1, &c1d);
+            cpi = make_float2((float)c1d, (float)s1);
+        }
+        const bool bs = bluestein_big(h, (int)nside, bsmin);
+        const int M = bs ? next_pow2(2 * h - 1) : 0;
+        const float2 *twM = bs ? tw32 + twiddle_offset(M) : nullptr;
+        float2 *FB = nullptr, *X = b0, *Y = b1;
+        if (bs) {
+            FB = bs_filter(h, n, M, tw, twM, +1, b0, b1);
+            X = (FB == b0) ? b1 : b0;
+            Y = b2;
+        }
+        const float *base = syn + (south ? 2 : 0);
+        for (int64_t c = 0; c < ncomp; ++c) {
+            for (int k = threadIdx.x; k < h; k += blockDim.x) {
+                float c0[2], c1[2], dummy[2];
+                residue_sums(base, L, nlanes, ncomp, j, c, k, n, sh, false, c0, dummy);
+                residue_sums(base, L, nlanes, ncomp, j, c, k + h, n, sh, false, c1, dummy);
+                float2 ck = make_float2(c0[0], c0[1]);
+                float2 ckh = make_float2(c1[0], c1[1]);
+                if (sh) {
+                    ck = cmul(ck, phase_pi(tw, h, k, cpi, +1));
+                    ckh = cmul(ckh, phase_pi(tw, h, k + h, cpi, +1));
+                }
+                const float2 sum = cadd(ck, ckh);
+                const float2 dif = cmul(csub(ck, ckh), twiddle_n(tw, h, k, +1));
+                float2 z = make_float2(sum.x - dif.y, sum.y + dif.x);
+                if (bs) z = cmul(z, bs_chirp(tw, h, n, k, +1));
+                X[k] = z;
+            }
+            __syncthreads();
+            float2 *Z = bs ? bs_apply(X, Y, FB, h, n, M, tw, twM, +1) : fft_shared(X, Y, h, tw, +1);
+            double *dst = maps + c * npix + off;
+            for (int t = threadIdx.x; t < h; t += blockDim.x) {
+                const float2 z = Z[t];
+                dst[2 * t] = (double)z.x;
+                dst[2 * t + 1] = (double)z.y;
+            }
+            __syncthreads();
+        }
     }
 }
 
@@ -619,16 +812,38 @@ static int set_smem(K kernel, size_t bytes)
     return GM_OK;
 }
 
-extern "C" int gm_ring_analysis(int precision, int64_t nside, int64_t L, int64_t ncomp,
-                                const void *maps, int map_dtype_bytes, const double *mask,
-                                const void *tw, const uint8_t *shifted, void *ringspec,
-                                void *stream)
+// Shared memory of the ring kernels: ping-pong buffers of hcap complex values.
+static int ring_hcap(int precision, int64_t nside, bool big)
 {
-    if (!ring_shape_ok(precision, nside, L, ncomp)) return GM_ERR_BAD_SHAPE;
+    const size_t elem = precision == GM_FP64 ? sizeof(double2) : sizeof(float2);
+    const int64_t fit = (int64_t)(227 * 1024 / (2 * elem));
+    const int64_t h = 2 * nside;
+    return (int)(big && h > fit ? fit : h);
+}
+
+extern "C" int64_t gm_ring_big_scratch_bytes(int64_t nside, int64_t nslots)
+{
+    return nside < 1 || nslots < 1 ? 0 : nslots * 3 * 4 * nside * (int64_t)sizeof(float2);
+}
+
+extern "C" int gm_ring_analysis_ws(int precision, int64_t nside, int64_t L, int64_t ncomp,
+                                   const void *maps, int map_dtype_bytes, const double *mask,
+                                   const void *tw, const uint8_t *shifted, void *ringspec,
+                                   void *scratch, int64_t scratch_bytes, int64_t hcap_max,
+                                   int64_t bs_min, void *stream)
+{
+    const bool big = precision == GM_MIXED && scratch != nullptr;
+    if (nside < 1 || nside > 8192 || L < 1 || ncomp < 1 || ncomp > 65535) return GM_ERR_BAD_SHAPE;
+    if (!big && !ring_shape_ok(precision, nside, L, ncomp)) return GM_ERR_BAD_SHAPE;
     if (!maps || !tw || !shifted || !ringspec) return GM_ERR_BAD_PTR;
     if (map_dtype_bytes != 8 && map_dtype_bytes != 4) return GM_ERR_UNSUPPORTED;
+    const int64_t nslots = big ? scratch_bytes / gm_ring_big_scratch_bytes(nside, 1) : 0;
+    if (big && nslots < 1) return GM_ERR_BAD_SHAPE;
     const int64_t nring = 4 * nside - 1, cnt = gm_ring_twiddle_count(nside);
-    size_t smem = ring_smem_bytes(precision, nside);
+    int hcap = ring_hcap(precision, nside, big);
+    if (big && hcap_max > 0 && hcap_max < hcap) hcap = (int)hcap_max;
+    const int bsmin = big ? (bs_min > 0 ? (int)bs_min : 8192) : 0;
+    const size_t smem = 2 * (size_t)hcap * (precision == GM_FP64 ? sizeof(double2) : sizeof(float2));
     int threads = nside >= 256 ? 512 : 128;
     dim3 grid((unsigned)nring, (unsigned)ncomp);
     cudaStream_t s = as_stream(stream);
@@ -637,38 +852,56 @@ extern "C" int gm_ring_analysis(int precision, int64_t nside, int64_t L, int64_t
         if (map_dtype_bytes == 8) {
             if ((st = set_smem(k_ring_analysis<double, double>, smem))) return st;
             k_ring_analysis<double, double><<<grid, threads, smem, s>>>(
-                nside, L, (const double *)maps, mask, tw, cnt, shifted, (double2 *)ringspec, 0);
+                nside, L, (const double *)maps, mask, tw, cnt, shifted, (double2 *)ringspec, 0, hcap, 0);
         } else {
             if ((st = set_smem(k_ring_analysis<double, float>, smem))) return st;
             k_ring_analysis<double, float><<<grid, threads, smem, s>>>(
-                nside, L, (const float *)maps, mask, tw, cnt, shifted, (double2 *)ringspec, 0);
+                nside, L, (const float *)maps, mask, tw, cnt, shifted, (double2 *)ringspec, 0, hcap, 0);
         }
     } else if (precision == GM_MIXED) {
         const int mcap = bluestein_mcap(nside);
         const size_t bs_smem = 3 * (size_t)mcap * sizeof(float2);
         const int cpc = 8;
         dim3 bs_grid((unsigned)nring, (unsigned)((ncomp + cpc - 1) / cpc));
+        const unsigned gbig = (unsigned)(nslots < nring ? nslots : nring);
         if (map_dtype_bytes == 8) {
             if ((st = set_smem(k_ring_analysis<float, double>, smem))) return st;
             k_ring_analysis<float, double><<<grid, threads, smem, s>>>(
-                nside, L, (const double *)maps, mask, tw, cnt, shifted, (float2 *)ringspec, mcap);
+                nside, L, (const double *)maps, mask, tw, cnt, shifted, (float2 *)ringspec, mcap, hcap, bsmin);
             if ((st = set_smem(k_ring_analysis_bluestein<double>, bs_smem))) return st;
             k_ring_analysis_bluestein<double><<<bs_grid, 512, bs_smem, s>>>(
-                nside, L, ncomp, cpc, mcap, (const double *)maps, mask, tw, cnt, shifted,
+                nside, L, ncomp, cpc, mcap, hcap, bsmin, (const double *)maps, mask, tw, cnt, shifted,
                 (float2 *)ringspec);
+            if (big)
+                k_ring_analysis_big<double><<<gbig, 512, 0, s>>>(
+                    nside, L, ncomp, (const double *)maps, mask, tw, cnt, shifted, (float2 *)ringspec,
+                    hcap, bsmin, (float2 *)scratch, 4 * nside);
         } else {
             if ((st = set_smem(k_ring_analysis<float, float>, smem))) return st;
             k_ring_analysis<float, float><<<grid, threads, smem, s>>>(
-                nside, L, (const float *)maps, mask, tw, cnt, shifted, (float2 *)ringspec, mcap);
+                nside, L, (const float *)maps, mask, tw, cnt, shifted, (float2 *)ringspec, mcap, hcap, bsmin);
             if ((st = set_smem(k_ring_analysis_bluestein<float>, bs_smem))) return st;
             k_ring_analysis_bluestein<float><<<bs_grid, 512, bs_smem, s>>>(
-                nside, L, ncomp, cpc, mcap, (const float *)maps, mask, tw, cnt, shifted,
+                nside, L, ncomp, cpc, mcap, hcap, bsmin, (const float *)maps, mask, tw, cnt, shifted,
                 (float2 *)ringspec);
+            if (big)
+                k_ring_analysis_big<float><<<gbig, 512, 0, s>>>(
+                    nside, L, ncomp, (const float *)maps, mask, tw, cnt, shifted, (float2 *)ringspec,
+                    hcap, bsmin, (float2 *)scratch, 4 * nside);
         }
     } else {
         return GM_ERR_UNSUPPORTED;
     }
     return check_launch("gm_ring_analysis");
+}
+
+extern "C" int gm_ring_analysis(int precision, int64_t nside, int64_t L, int64_t ncomp,
+                                const void *maps, int map_dtype_bytes, const double *mask,
+                                const void *tw, const uint8_t *shifted, void *ringspec,
+                                void *stream)
+{
+    return gm_ring_analysis_ws(precision, nside, L, ncomp, maps, map_dtype_bytes, mask, tw, shifted,
+                               ringspec, nullptr, 0, 0, 0, stream);
 }
 
 extern "C" int gm_pack_rhs(int precision, int64_t nside, int64_t L, int64_t ncomp,
@@ -712,14 +945,22 @@ extern "C" int gm_fold_residual(int precision, int64_t nside, int64_t L, int64_t
     return check_launch("gm_fold_residual");
 }
 
-extern "C" int gm_ring_synthesis(int precision, int64_t nside, int64_t L, int64_t ncomp,
-                                 const void *syn, const void *tw, const uint8_t *shifted,
-                                 double *maps, void *stream)
+extern "C" int gm_ring_synthesis_ws(int precision, int64_t nside, int64_t L, int64_t ncomp,
+                                    const void *syn, const void *tw, const uint8_t *shifted,
+                                    double *maps, void *scratch, int64_t scratch_bytes,
+                                    int64_t hcap_max, int64_t bs_min, void *stream)
 {
-    if (!ring_shape_ok(precision, nside, L, ncomp)) return GM_ERR_BAD_SHAPE;
+    const bool big = precision == GM_MIXED && scratch != nullptr;
+    if (nside < 1 || nside > 8192 || L < 1 || ncomp < 1 || ncomp > 65535) return GM_ERR_BAD_SHAPE;
+    if (!big && !ring_shape_ok(precision, nside, L, ncomp)) return GM_ERR_BAD_SHAPE;
     if (!syn || !tw || !shifted || !maps) return GM_ERR_BAD_PTR;
+    const int64_t nslots = big ? scratch_bytes / gm_ring_big_scratch_bytes(nside, 1) : 0;
+    if (big && nslots < 1) return GM_ERR_BAD_SHAPE;
     const int64_t nring = 4 * nside - 1, cnt = gm_ring_twiddle_count(nside);
-    size_t smem = ring_smem_bytes(precision, nside);
+    int hcap = ring_hcap(precision, nside, big);
+    if (big && hcap_max > 0 && hcap_max < hcap) hcap = (int)hcap_max;
+    const int bsmin = big ? (bs_min > 0 ? (int)bs_min : 8192) : 0;
+    const size_t smem = 2 * (size_t)hcap * (precision == GM_FP64 ? sizeof(double2) : sizeof(float2));
     int threads = nside >= 256 ? 512 : 128;
     dim3 grid((unsigned)nring, (unsigned)ncomp);
     cudaStream_t s = as_stream(stream);
@@ -727,13 +968,25 @@ extern "C" int gm_ring_synthesis(int precision, int64_t nside, int64_t L, int64_
     if (precision == GM_FP64) {
         if ((st = set_smem(k_ring_synthesis<double>, smem))) return st;
         k_ring_synthesis<double><<<grid, threads, smem, s>>>(nside, L, ncomp, (const double *)syn,
-                                                             tw, cnt, shifted, maps);
+                                                             tw, cnt, shifted, maps, hcap, 0);
     } else if (precision == GM_MIXED) {
         if ((st = set_smem(k_ring_synthesis<float>, smem))) return st;
         k_ring_synthesis<float><<<grid, threads, smem, s>>>(nside, L, ncomp, (const float *)syn,
-                                                            tw, cnt, shifted, maps);
+                                                            tw, cnt, shifted, maps, hcap, bsmin);
+        if (big)
+            k_ring_synthesis_big<<<(unsigned)(nslots < nring ? nslots : nring), 512, 0, s>>>(
+                nside, L, ncomp, (const float *)syn, tw, cnt, shifted, maps, hcap, bsmin,
+                (float2 *)scratch, 4 * nside);
     } else {
         return GM_ERR_UNSUPPORTED;
     }
     return check_launch("gm_ring_synthesis");
+}
+
+extern "C" int gm_ring_synthesis(int precision, int64_t nside, int64_t L, int64_t ncomp,
+                                 const void *syn, const void *tw, const uint8_t *shifted,
+                                 double *maps, void *stream)
+{
+    return gm_ring_synthesis_ws(precision, nside, L, ncomp, syn, tw, shifted, maps, nullptr, 0, 0, 0,
+                                stream);
 }

@@ -211,11 +211,30 @@ def ring_analysis(plan, maps, prec, mask=None, out=None):
         spec = out
     else:
         spec = torch.empty((ncomp, plan.nring, plan.L), dtype=_complex_dtype(prec), device=plan.device)
-    _lib.call("gm_ring_analysis", prec, plan.nside, plan.L, ncomp, _lib.ptr(maps),
+    scratch, sbytes = _ring_scratch(plan, prec)
+    _lib.call("gm_ring_analysis_ws", prec, plan.nside, plan.L, ncomp, _lib.ptr(maps),
               maps.element_size(), _lib.ptr(mask) if mask is not None else None,
-              _lib.ptr(plan.tw), _lib.ptr(plan.shifted), _lib.ptr(spec),
-              _lib.stream_handle(plan.device))
+              _lib.ptr(plan.tw), _lib.ptr(plan.shifted), _lib.ptr(spec), _lib.ptr(scratch), sbytes,
+              RING_TUNING["hcap_max"], RING_TUNING["bs_min"], _lib.stream_handle(plan.device))
     return spec
+
+
+# Global-memory ring path (single precision): a scratch of two slots per SM for the rings
+# that do not fit the shared-memory kernels (Nside above 4096).  The knobs lower the
+# thresholds that send a ring there (0: the defaults); they exist for tests.
+RING_TUNING = {"hcap_max": 0, "bs_min": 0}
+
+
+def _ring_scratch(plan, prec):
+    if prec != _lib.MIXED:
+        return None, 0
+    sc = getattr(plan, "_ring_scratch_buf", None)
+    if sc is None:
+        nslots = 2 * torch.cuda.get_device_properties(plan.device).multi_processor_count
+        nbytes = int(_lib.load().gm_ring_big_scratch_bytes(plan.nside, nslots))
+        sc = torch.empty(nbytes, dtype=torch.uint8, device=plan.device)
+        plan._ring_scratch_buf = sc
+    return sc, sc.numel()
 
 
 def pack_rhs(plan, spec, prec):
@@ -258,8 +277,10 @@ def fold_residual(plan, syn, rhs_map, prec, out=None):
 def ring_synthesis(plan, syn, prec):
     ncomp = syn.shape[2]
     maps = torch.empty((ncomp, plan.npix), dtype=torch.float64, device=plan.device)
-    _lib.call("gm_ring_synthesis", prec, plan.nside, plan.L, ncomp, _lib.ptr(syn), _lib.ptr(plan.tw),
-              _lib.ptr(plan.shifted), _lib.ptr(maps), _lib.stream_handle(plan.device))
+    scratch, sbytes = _ring_scratch(plan, prec)
+    _lib.call("gm_ring_synthesis_ws", prec, plan.nside, plan.L, ncomp, _lib.ptr(syn), _lib.ptr(plan.tw),
+              _lib.ptr(plan.shifted), _lib.ptr(maps), _lib.ptr(scratch), sbytes,
+              RING_TUNING["hcap_max"], RING_TUNING["bs_min"], _lib.stream_handle(plan.device))
     return maps
 
 

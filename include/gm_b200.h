@@ -97,6 +97,24 @@ int gm_ring_synthesis(int precision, int64_t nside, int64_t L, int64_t ncomp,
                       const void *syn, const void *tw, const uint8_t *shifted,
                       double *maps, void *stream);
 
+/* The two ring stages above with a global scratch for the rings that do not fit the
+ * shared-memory kernels (single precision only; NULL scratch gives the entries above):
+ * belt rings above Nside 7264, whose ping-pong buffers exceed 227 KB, and rings needing
+ * Bluestein's method longer than 8192 points (a prime factor above 64, h > 4096).
+ * Persistent CTAs, one per scratch slot of gm_ring_big_scratch_bytes(nside, 1) bytes,
+ * walk those rings.  hcap_max > 0 lowers the largest half-length kept in shared memory
+ * and bs_min > 0 the Bluestein length above which the global path takes a ring (0:
+ * defaults; small values route small rings through the global path, for testing).
+ * Same reference interfaces (rings.py:251-299, 477-524). */
+int64_t gm_ring_big_scratch_bytes(int64_t nside, int64_t nslots);
+int gm_ring_analysis_ws(int precision, int64_t nside, int64_t L, int64_t ncomp, const void *maps,
+                        int map_dtype_bytes, const double *mask, const void *tw,
+                        const uint8_t *shifted, void *ringspec, void *scratch,
+                        int64_t scratch_bytes, int64_t hcap_max, int64_t bs_min, void *stream);
+int gm_ring_synthesis_ws(int precision, int64_t nside, int64_t L, int64_t ncomp, const void *syn,
+                         const void *tw, const uint8_t *shifted, double *maps, void *scratch,
+                         int64_t scratch_bytes, int64_t hcap_max, int64_t bs_min, void *stream);
+
 /* ----------------------------------------------------------- Legendre stage */
 
 /* Per-order seed table length (doubles) for spin s: 3 variants x 4 x L. */
