@@ -60,11 +60,13 @@ def parse():
     p.add_argument("--batch", type=int, default=32)
     p.add_argument("--fp64-steps", type=int, default=1)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="mc", choices=["mc", "uneven_workspaces", "nside4096", "mc1024"],
+    p.add_argument("--workload", default="mc", choices=["mc", "uneven_workspaces", "nside4096", "mc1024", "nside8192"],
                    help="mc: the Monte-Carlo estimator (default); uneven_workspaces: TT "
                         "coupling matrices of 32 masks of mixed Nside in one launch; nside4096: "
                         "batched map2alm (n_iter=0) and alm2map at Nside 4096; mc1024: 512 TQU "
-                        "simulations at Nside 1024, batched and per simulation as a CUDA graph")
+                        "simulations at Nside 1024, batched and per simulation as a CUDA graph; "
+                        "nside8192: one spin-2 spectrum at Nside 8192 with the exact and the "
+                        "Toeplitz coupling matrix")
     p.add_argument("--nmasks", type=int, default=32)
     return p.parse_args()
 
@@ -652,6 +654,150 @@ def run_mc1024(args):
     print(json.dumps(line), flush=True)
 
 
+def make_mask_gpu(nside, device, seed=4, nholes=10000, hole_arcmin=2.0, cut_deg=20.0, apo_deg=0.5,
+                  chunk=1 << 16):
+    """The analytic mask recipe of `make_mask` with the pixel centres computed on the GPU in
+    chunks (for Nside 8192, where the host pixel vectors would take 19 GB)."""
+    import torch
+
+    from gmaster_b200 import sht
+
+    theta, phi0, nphi, offsets = sht.ring_geometry(nside)
+    th_t = torch.from_numpy(theta).to(device)
+    ph_t = torch.from_numpy(phi0).to(device)
+    nphi_t = torch.from_numpy(nphi.astype(np.int64)).to(device)
+    off_t = torch.from_numpy(offsets.astype(np.int64)).to(device)
+    th, ph = np.radians(30.0), np.radians(45.0)
+    pole = torch.tensor([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)],
+                        dtype=torch.float64, device=device)
+    rng = np.random.default_rng(seed)
+    centres = rng.normal(size=(nholes, 3))
+    centres /= np.linalg.norm(centres, axis=1)[:, None]
+    cen = torch.from_numpy(centres).to(device)
+    npix = 12 * nside * nside
+    r = np.radians(hole_arcmin / 60.0)
+    apo = np.radians(apo_deg)
+    mask = torch.empty(npix, dtype=torch.float64, device=device)
+    for s0 in range(0, npix, chunk):
+        pix = torch.arange(s0, min(npix, s0 + chunk), dtype=torch.int64, device=device)
+        ring = torch.searchsorted(off_t, pix, right=True) - 1
+        phi = ph_t[ring] + 2 * np.pi * (pix - off_t[ring]).to(torch.float64) / nphi_t[ring].to(torch.float64)
+        t = th_t[ring]
+        vec = torch.stack([torch.sin(t) * torch.cos(phi), torch.sin(t) * torch.sin(phi), torch.cos(t)], 1)
+        d = torch.arcsin((vec @ pole).abs().clamp(max=1.0)) - np.radians(cut_deg)
+        cosang = (vec @ cen.T).max(dim=1).values.clamp(-1.0, 1.0)
+        d = torch.minimum(d, torch.arccos(cosang) - r)
+        m = (d > 0).to(torch.float64)
+        x = torch.sqrt((1 - torch.cos(d.clamp(min=0))) / (1 - np.cos(apo)))
+        m = torch.where((d > 0) & (d < apo), x - torch.sin(2 * np.pi * x) / (2 * np.pi), m)
+        mask[s0:s0 + len(pix)] = m
+    return mask
+
+
+def run_nside8192(args):
+    """One spin-2 MASTER spectrum at Nside 8192 (lmax 24575): the config mask recipe with
+    10000 holes of 2 arcmin and 0.5 deg apodisation, (Q, U) maps of Gaussian E and B alms
+    (C_EE = 0.05 C_TT, C_BB = 0.005 C_TT, C_TT = 1e3/(l+10)^2), n_iter = 3, bands of 16; the
+    field (with its mask transform), the exact FP64 3j workspace and the decoupled
+    bandpowers, then the same with the Toeplitz approximation beside it.  Transforms in
+    mixed precision (the one-field SIMT kernels; the ring stage's widest rings go through
+    its global-memory path).  Tile tuning is off (it would time every tile at this size)."""
+    import torch
+
+    import gmaster_b200 as nmt
+    from gmaster_b200 import _lib, autotune, sht
+    from gmaster_b200.utils import NmtAlmInfo
+
+    autotune.set_autotune(False)
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    nside, nlb = 8192, 16
+    lmax = 3 * nside - 1
+    t0 = time.perf_counter()
+    mask = make_mask_gpu(nside, dev)
+    _, ee, bb, _ = config_spectra(lmax)
+    ell, order = NmtAlmInfo(lmax).ell_m()
+    ell_t = torch.from_numpy(ell).to(dev)
+    m0 = torch.from_numpy(order == 0).to(dev)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(3)
+
+    def unit():
+        re = torch.randn(ell.shape[0], generator=gen, device=dev, dtype=torch.float64)
+        im = torch.randn(ell.shape[0], generator=gen, device=dev, dtype=torch.float64)
+        re[m0] *= np.sqrt(2.0)
+        im[m0] = 0.0
+        return torch.complex(re, im) / np.sqrt(2.0)
+
+    eb = torch.stack([unit() * torch.from_numpy(np.sqrt(ee)).to(dev)[ell_t],
+                      unit() * torch.from_numpy(np.sqrt(bb)).to(dev)[ell_t]])
+    qu = sht.alm2map_device(eb, 2, nside, lmax, "mixed")
+    del eb
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    torch.cuda.reset_peak_memory_stats(dev)
+    calls0 = dict(_lib.CALLS)
+    sampler = ClockSampler(0)
+    sampler.start()
+    marks = []
+
+    def mark(name):
+        torch.cuda.synchronize()
+        marks.append((name, time.perf_counter()))
+
+    mark("start")
+    f2 = nmt.NmtField(mask, qu, spin=2, n_iter=3, precision="mixed")
+    f2.get_mask_alms()
+    mark("field (maps and mask transforms)")
+    b = nmt.NmtBin.from_nside_linear(nside, nlb)
+    w = nmt.NmtWorkspace.from_fields(f2, f2, b)
+    mark("workspace (exact 3j coupling, binning, LU)")
+    pcl = nmt.compute_coupled_cell(f2, f2)
+    cl = w.decouple_cell(pcl)
+    mark("spectra")
+    del w
+    torch.cuda.empty_cache()
+    kw = dict(l_toeplitz=nside, l_exact=nside // 4, dl_band=64)
+    wt = nmt.NmtWorkspace.from_fields(f2, f2, b, **kw)
+    cl_t = wt.decouple_cell(pcl)
+    mark("Toeplitz workspace and spectra")
+    clocks = sampler.stop()
+    launches = sum(_lib.CALLS.get(k, 0) - calls0.get(k, 0) for k in _lib.CALLS)
+    stages = {b_[0]: round(b_[1] - a[1], 3) for a, b_ in zip(marks[:-1], marks[1:])}
+    s_spec = marks[3][1] - marks[0][1]
+    l_eff = b.get_effective_ells()
+    fsky = float((mask ** 2).mean())
+    sigma = np.sqrt(2.0 / ((2.0 * l_eff + 1.0) * nlb * fsky))
+    c, ct = cl.cpu().numpy(), cl_t.cpu().numpy()
+    toep = {}
+    for i, name in ((0, "EE"), (3, "BB")):
+        toep[name] = {"max_rel": float(np.max(np.abs(ct[i] - c[i]) / np.abs(c[i]).max())),
+                      "max_in_sigma_cv": float(np.max(np.abs(ct[i] - c[i]) / (sigma * np.abs(c[i]))))}
+    # recovered EE against the input spectrum, binned (a sanity check, cosmic variance ~1 %)
+    ee_in = b.bin_cell(torch.from_numpy(ee[None]).to(dev)).cpu().numpy()[0]
+    sel = (l_eff > 100) & (l_eff < 2 * nside)
+    ee_ratio = float(np.median(c[0][sel] / ee_in[sel]))
+    line = {
+        "metric": "MASTER s/spectrum, Nside 8192 spin 2 (exact FP64 3j workspace), mixed precision",
+        "value": s_spec, "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 0,
+        "ms_per_step": s_spec * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 transforms (f64 recurrence and alm accumulation), f64 coupling and LU",
+        "data": "synthetic (config mask recipe, 10000 holes of 2 arcmin, 0.5 deg apodisation; "
+                "Gaussian E/B alms)",
+        "config": {"workload": "one spin-2 spectrum from the maps at Nside 8192, lmax 24575, "
+                               "n_iter=3, nlb=16, plus a Toeplitz workspace beside it",
+                   "nside": nside, "lmax": lmax, "nlb": nlb, "toeplitz": kw,
+                   "l2_flush": "inputs (6.4 GB per map) larger than L2"},
+        "stages_s": stages, "setup_s": setup_s,
+        "peak_device_gb": torch.cuda.max_memory_allocated(dev) / 1e9,
+        "toeplitz_vs_exact": toep, "fsky": fsky,
+        "recovered_ee_over_input_median": ee_ratio,
+        "clocks": clocks, "gpu_launches": int(launches),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -665,6 +811,9 @@ def main():
         return
     if args.workload == "mc1024":
         run_mc1024(args)
+        return
+    if args.workload == "nside8192":
+        run_nside8192(args)
         return
     import torch
     import torch.distributed as dist

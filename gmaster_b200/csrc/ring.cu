@@ -816,7 +816,8 @@ static int set_smem(K kernel, size_t bytes)
 static int ring_hcap(int precision, int64_t nside, bool big)
 {
     const size_t elem = precision == GM_FP64 ? sizeof(double2) : sizeof(float2);
-    const int64_t fit = (int64_t)(227 * 1024 / (2 * elem));
+    // 227 KB of dynamic shared memory per block, less 1 KB left to the kernels' static arrays
+    const int64_t fit = (int64_t)((227 * 1024 - 1024) / (2 * elem));
     const int64_t h = 2 * nside;
     return (int)(big && h > fit ? fit : h);
 }

@@ -99,7 +99,7 @@ int gm_ring_synthesis(int precision, int64_t nside, int64_t L, int64_t ncomp,
 
 /* The two ring stages above with a global scratch for the rings that do not fit the
  * shared-memory kernels (single precision only; NULL scratch gives the entries above):
- * belt rings above Nside 7264, whose ping-pong buffers exceed 227 KB, and rings needing
+ * belt rings above Nside 7232, whose ping-pong buffers exceed 226 KB, and rings needing
  * Bluestein's method longer than 8192 points (a prime factor above 64, h > 4096).
  * Persistent CTAs, one per scratch slot of gm_ring_big_scratch_bytes(nside, 1) bytes,
  * walk those rings.  hcap_max > 0 lowers the largest half-length kept in shared memory
