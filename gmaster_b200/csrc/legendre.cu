@@ -114,6 +114,7 @@ __global__ void __launch_bounds__(kThreads) k_legendre_ana(
     constexpr int LB = 32 / NV;
     constexpr int NVAR = SPIN == 0 ? 1 : 2;
     static_assert(LB * NV == 32, "reduce-scatter width");
+    static_assert(LB % 2 == 0 && kWindow % 2 == 0, "row parity is fixed by the row index");
     __shared__ Coef coef[kWindow];
     __shared__ double red[kWarps][kWindow * NV];
 
@@ -153,6 +154,22 @@ __global__ void __launch_bounds__(kThreads) k_legendre_ana(
                                   : (T)0;
     }
 
+    // The rows of a reduce-scatter block start at l0 + (an even offset: kWindow and LB are
+    // even), so the parity of l + m in unrolled row s is ((l0 + m) + s) & 1.  With the two
+    // hemisphere halves of the right-hand side swapped once here when l0 + m is odd, row s
+    // takes half s & 1, chosen at compile time instead of by selects on every element.
+    if ((l0 + m) & 1) {
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                T t0 = rh[r][c][0], t1 = rh[r][c][1];
+                rh[r][c][0] = rh[r][c][2];
+                rh[r][c][1] = rh[r][c][3];
+                rh[r][c][2] = t0;
+                rh[r][c][3] = t1;
+            }
+    }
     for (int lb = l0; lb < L; lb += kWindow) {
         if (threadIdx.x < kWindow) {
             const int l = lb + threadIdx.x;
@@ -190,7 +207,7 @@ __global__ void __launch_bounds__(kThreads) k_legendre_ana(
                             }
                         }
                     }
-                    const int par = (l + m) & 1;
+                    const int par = s & 1;   // relative to (l0 + m) & 1, see above
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         if (SPIN == 0) {
@@ -331,69 +348,88 @@ __global__ void __launch_bounds__(kThreads) k_legendre_syn(
         }
         __syncthreads();
         const int lend = (lb + kWindow < L) ? kWindow : (int)(L - lb);
-#pragma unroll 4
-        for (int s = 0; s < lend; ++s) {
-            const int l = lb + s;
-            if (l > l0) {
-                const Coef cf = coef[buf][s];
+        // blocks start at l0 + multiples of kWindow (even), so row s has the parity of
+        // l + m relative to (l0 + m) & 1 given by s & 1: rows go in pairs and each
+        // accumulates into its half at compile time (no multiplications by zero); the
+        // halves are put in true parity order before the output
+#pragma unroll 2
+        for (int s0 = 0; s0 < lend; s0 += 2) {
+#pragma unroll
+            for (int hh = 0; hh < 2; ++hh) {
+                const int s = s0 + hh;
+                if (s >= lend) break;
+                const int l = lb + s;
+                if (l > l0) {
+                    const Coef cf = coef[buf][s];
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        if (SPIN == 0) {
+                            double nv = fma(cf.alpha * x[r], v[0][r], -cf.beta * vp[0][r]);
+                            vp[0][r] = v[0][r];
+                            v[0][r] = nv;
+                            rescale(v[0][r], vp[0][r], kx[0][r]);
+                        } else {
+                            double nva = fma(cf.alpha * (x[r] + cf.c0), v[0][r], -cf.beta * vp[0][r]);
+                            double nvb = fma(cf.alpha * (x[r] - cf.c0), v[1][r], -cf.beta * vp[1][r]);
+                            vp[0][r] = v[0][r];
+                            v[0][r] = nva;
+                            vp[1][r] = v[1][r];
+                            v[1][r] = nvb;
+                            rescale(v[0][r], vp[0][r], kx[0][r]);
+                            rescale(v[1][r], vp[1][r], kx[1][r]);
+                        }
+                    }
+                }
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     if (SPIN == 0) {
-                        double nv = fma(cf.alpha * x[r], v[0][r], -cf.beta * vp[0][r]);
-                        vp[0][r] = v[0][r];
-                        v[0][r] = nv;
-                        rescale(v[0][r], vp[0][r], kx[0][r]);
+                        const T val = kx[0][r] == 0 ? (T)v[0][r] : (T)0;
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) {
+                            acc[r][4 * c + 2 * hh] += val * aw[buf][s][c][0];
+                            acc[r][4 * c + 2 * hh + 1] += val * aw[buf][s][c][1];
+                        }
                     } else {
-                        double nva = fma(cf.alpha * (x[r] + cf.c0), v[0][r], -cf.beta * vp[0][r]);
-                        double nvb = fma(cf.alpha * (x[r] - cf.c0), v[1][r], -cf.beta * vp[1][r]);
-                        vp[0][r] = v[0][r];
-                        v[0][r] = nva;
-                        vp[1][r] = v[1][r];
-                        v[1][r] = nvb;
-                        rescale(v[0][r], vp[0][r], kx[0][r]);
-                        rescale(v[1][r], vp[1][r], kx[1][r]);
+                        const double lp = kx[0][r] == 0 ? v[0][r] : 0.0;
+                        const double lm = kx[1][r] == 0 ? v[1][r] : 0.0;
+                        const T f1 = (T)(0.5 * (lp + lm)), f2 = (T)(0.5 * (lp - lm));
+                        const T er = aw[buf][s][0][0], ei = aw[buf][s][0][1];
+                        const T br = aw[buf][s][1][0], bi = aw[buf][s][1][1];
+                        // per parity: [S1E re, im, S1B re, im, S2E re, im, S2B re, im]
+                        T *a = &acc[r][8 * hh];
+                        a[0] += f1 * er;
+                        a[1] += f1 * ei;
+                        a[2] += f1 * br;
+                        a[3] += f1 * bi;
+                        a[4] += f2 * er;
+                        a[5] += f2 * ei;
+                        a[6] += f2 * br;
+                        a[7] += f2 * bi;
                     }
                 }
             }
-            const int par = (l + m) & 1;
+        }
+    }
+
+    if ((l0 + m) & 1) {
+        // the even rows of the blocks had odd l + m: swap the halves into parity order
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                if (SPIN == 0) {
-                    const T val = kx[0][r] == 0 ? (T)v[0][r] : (T)0;
-                    const T ve = par ? (T)0 : val, vo = par ? val : (T)0;
+        for (int r = 0; r < R; ++r) {
+            if (SPIN == 0) {
 #pragma unroll
-                    for (int c = 0; c < NC; ++c) {
-                        const T ar = aw[buf][s][c][0], ai = aw[buf][s][c][1];
-                        acc[r][4 * c] += ve * ar;
-                        acc[r][4 * c + 1] += ve * ai;
-                        acc[r][4 * c + 2] += vo * ar;
-                        acc[r][4 * c + 3] += vo * ai;
-                    }
-                } else {
-                    const double lp = kx[0][r] == 0 ? v[0][r] : 0.0;
-                    const double lm = kx[1][r] == 0 ? v[1][r] : 0.0;
-                    const T f1 = (T)(0.5 * (lp + lm)), f2 = (T)(0.5 * (lp - lm));
-                    const T er = aw[buf][s][0][0], ei = aw[buf][s][0][1];
-                    const T br = aw[buf][s][1][0], bi = aw[buf][s][1][1];
-                    // per parity: [S1E re, im, S1B re, im, S2E re, im, S2B re, im]
-                    const T f1e = par ? (T)0 : f1, f1o = par ? f1 : (T)0;
-                    const T f2e = par ? (T)0 : f2, f2o = par ? f2 : (T)0;
-                    acc[r][0] += f1e * er;
-                    acc[r][1] += f1e * ei;
-                    acc[r][2] += f1e * br;
-                    acc[r][3] += f1e * bi;
-                    acc[r][4] += f2e * er;
-                    acc[r][5] += f2e * ei;
-                    acc[r][6] += f2e * br;
-                    acc[r][7] += f2e * bi;
-                    acc[r][8] += f1o * er;
-                    acc[r][9] += f1o * ei;
-                    acc[r][10] += f1o * br;
-                    acc[r][11] += f1o * bi;
-                    acc[r][12] += f2o * er;
-                    acc[r][13] += f2o * ei;
-                    acc[r][14] += f2o * br;
-                    acc[r][15] += f2o * bi;
+                for (int c = 0; c < NC; ++c) {
+                    const T t0 = acc[r][4 * c], t1 = acc[r][4 * c + 1];
+                    acc[r][4 * c] = acc[r][4 * c + 2];
+                    acc[r][4 * c + 1] = acc[r][4 * c + 3];
+                    acc[r][4 * c + 2] = t0;
+                    acc[r][4 * c + 3] = t1;
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const T t = acc[r][q];
+                    acc[r][q] = acc[r][8 + q];
+                    acc[r][8 + q] = t;
                 }
             }
         }
