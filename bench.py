@@ -60,13 +60,17 @@ def parse():
     p.add_argument("--batch", type=int, default=32)
     p.add_argument("--fp64-steps", type=int, default=1)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="mc", choices=["mc", "uneven_workspaces", "nside4096", "mc1024", "nside8192"],
+    p.add_argument("--workload", default="mc",
+                   choices=["mc", "uneven_workspaces", "nside4096", "mc1024", "nside8192", "apodize"],
                    help="mc: the Monte-Carlo estimator (default); uneven_workspaces: TT "
                         "coupling matrices of 32 masks of mixed Nside in one launch; nside4096: "
                         "batched map2alm (n_iter=0) and alm2map at Nside 4096; mc1024: 512 TQU "
                         "simulations at Nside 1024, batched and per simulation as a CUDA graph; "
                         "nside8192: one spin-2 spectrum at Nside 8192 with the exact and the "
-                        "Toeplitz coupling matrix")
+                        "Toeplitz coupling matrix; apodize: C1 apodisation of the binary "
+                        "Nside 2048 and 8192 config masks on the GPU")
+    p.add_argument("--apo-nsides", default="2048,8192",
+                   help="apodize workload: the Nside values to run (the first is the headline)")
     p.add_argument("--nmasks", type=int, default=32)
     return p.parse_args()
 
@@ -688,8 +692,9 @@ def make_mask_gpu(nside, device, seed=4, nholes=10000, hole_arcmin=2.0, cut_deg=
         cosang = (vec @ cen.T).max(dim=1).values.clamp(-1.0, 1.0)
         d = torch.minimum(d, torch.arccos(cosang) - r)
         m = (d > 0).to(torch.float64)
-        x = torch.sqrt((1 - torch.cos(d.clamp(min=0))) / (1 - np.cos(apo)))
-        m = torch.where((d > 0) & (d < apo), x - torch.sin(2 * np.pi * x) / (2 * np.pi), m)
+        if apo > 0:
+            x = torch.sqrt((1 - torch.cos(d.clamp(min=0))) / (1 - np.cos(apo)))
+            m = torch.where((d > 0) & (d < apo), x - torch.sin(2 * np.pi * x) / (2 * np.pi), m)
         mask[s0:s0 + len(pix)] = m
     return mask
 
@@ -798,6 +803,124 @@ def run_nside8192(args):
     print(json.dumps(line), flush=True)
 
 
+APO_RECIPES = {2048: dict(nholes=2000, hole_arcmin=5.0, apo_deg=1.0),
+               8192: dict(nholes=10000, hole_arcmin=2.0, apo_deg=0.5)}
+
+
+def kdtree_apodization_sample(mask_np, nside, apo_deg, nquery=2_000_000, seed=0):
+    """The reference's C1 apodisation step (gmaster/utils.py:130-146: a scipy k-d tree over the
+    masked pixels' unit vectors, one nearest-neighbour query per pixel) timed on the host
+    for a bounded sample: the tree over all masked pixels plus `nquery` random pixels,
+    the query time scaled to all pixels.  Uses the oracle's pixel vectors."""
+    import oracle
+    from scipy.spatial import cKDTree
+
+    vec = oracle.pix2vec(nside)
+    masked = np.flatnonzero(mask_np <= 0)
+    t0 = time.perf_counter()
+    tree = cKDTree(vec[masked])
+    t1 = time.perf_counter()
+    pick = np.random.default_rng(seed).choice(len(mask_np), min(nquery, len(mask_np)), replace=False)
+    tree.query(vec[pick])
+    t2 = time.perf_counter()
+    total = (t1 - t0) + (t2 - t1) * len(mask_np) / len(pick)
+    return {"value": total, "unit": "s/mask", "cores": 1, "kind": "port",
+            "sample": f"scipy cKDTree over all {len(masked)} masked pixels (built in {t1 - t0:.1f} s) "
+                      f"and {len(pick)} of {len(mask_np)} pixel queries ({t2 - t1:.1f} s), "
+                      f"query time scaled to all pixels"}
+
+
+def run_apodize(args):
+    """C1 apodisation of binary masks of the configuration recipes (|b| > 20 deg about a
+    tilted pole plus holes) on the GPU: Nside 2048 (2000 holes of 5', 1 deg) and Nside
+    8192 (10000 holes of 2', 0.5 deg).  One step = gm_mask_ring_runs + gm_mask_apodize
+    through `mask_apodization` on a device-resident mask; e2e adds the host->device copy of
+    the mask from pinned memory and the copy of the result back."""
+    import torch
+
+    import gmaster_b200 as nmt
+    from gmaster_b200 import _lib
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    nsides = [int(x) for x in args.apo_nsides.split(",") if x]
+    runs = {}
+    for nside in nsides:
+        rec = APO_RECIPES.get(nside, APO_RECIPES[2048])
+        binary = make_mask_gpu(nside, dev, nholes=rec["nholes"], hole_arcmin=rec["hole_arcmin"],
+                               apo_deg=0.0)
+        apo = rec["apo_deg"]
+        for _ in range(args.warmup):
+            nmt.mask_apodization(binary, apo, apotype="C1")
+        torch.cuda.synchronize()
+        calls0 = dict(_lib.CALLS)
+        sampler = ClockSampler(0)
+        sampler.start()
+        # per-kernel device time: events around each launch on the launching stream
+        st = torch.cuda.current_stream(dev)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(st)
+        for _ in range(args.steps):
+            out = nmt.mask_apodization(binary, apo, apotype="C1")
+        ev[1].record(st)
+        torch.cuda.synchronize()
+        ms = ev[0].elapsed_time(ev[1]) / args.steps
+        clocks = sampler.stop()
+        launches = sum(_lib.CALLS.get(k, 0) - calls0.get(k, 0) for k in _lib.CALLS)
+        host = binary.cpu().pin_memory()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.steps):
+            res = nmt.mask_apodization(host.to(dev, non_blocking=True), apo, apotype="C1").cpu()
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms_e2e = e0.elapsed_time(e1) / args.steps
+        npix = 12 * nside * nside
+        tapered = int(((out > 0) & (out < 1)).sum())
+        runs[nside] = {"ms": ms, "ms_e2e": ms_e2e, "clocks": clocks, "launches": launches,
+                       "npix": npix, "masked": int((binary <= 0).sum()), "tapered": tapered,
+                       "apo_deg": apo, "nholes": rec["nholes"], "hole_arcmin": rec["hole_arcmin"],
+                       "mask_np": binary.cpu().numpy() if nside == nsides[0] else None}
+        del binary, out, res, host
+        torch.cuda.empty_cache()
+    head = runs[nsides[0]]
+    nside0 = nsides[0]
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peaks = json.load(fh)
+    except OSError:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    # algorithmic bytes per pixel: the mask read by both kernels (16 B), prev/next written
+    # (8 B), the output written (8 B)
+    algo = 32.0 * head["npix"]
+    line = {
+        "metric": "mask apodisation s/mask (C1, exact nearest masked pixel)",
+        "value": head["ms"] / 1e3, "unit": "s/mask", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms"], "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (binary config mask recipes, built on the GPU)",
+        "config": {"workload": f"C1 apodisation of a binary Nside {nside0} mask "
+                               f"({head['nholes']} holes of {head['hole_arcmin']}', |b| > 20 deg) "
+                               f"at {head['apo_deg']} deg",
+                   "nside": nside0, "l2_flush": f"inputs ({head['npix'] * 8 / 1e6:.0f} MB mask, "
+                                                 f"{head['npix'] * 8 / 1e6:.0f} MB prev/next) larger than L2"},
+        "e2e": {"value": head["ms_e2e"] / 1e3, "unit": "s/mask",
+                "h2d_bytes_per_step": 8 * head["npix"], "d2h_bytes_per_step": 8 * head["npix"]},
+        "roofline": {"bound": "hbm", "achieved": algo / (head["ms"] / 1e3) / 1e9, "peak": hbm,
+                     "unit": "GB/s", "frac": algo / (head["ms"] / 1e3) / 1e9 / hbm, "traffic": None,
+                     "note": "both kernels of one step against their algorithmic bytes (32 B per "
+                             "pixel); the ring search is instruction-bound, not HBM-bound"},
+        "per_nside": {str(n): {k: v for k, v in r.items() if k != "mask_np"} for n, r in runs.items()},
+        "clocks": head["clocks"], "gpu_launches": int(head["launches"]),
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = kdtree_apodization_sample(head["mask_np"], nside0, head["apo_deg"])
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -814,6 +937,9 @@ def main():
         return
     if args.workload == "nside8192":
         run_nside8192(args)
+        return
+    if args.workload == "apodize":
+        run_apodize(args)
         return
     import torch
     import torch.distributed as dist

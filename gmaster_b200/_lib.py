@@ -89,6 +89,9 @@ SIGNATURES = {
                                   _c_vp], _c_int),
     "gm_tc_alm_layout": ([_c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_int, _c_vp], _c_int),
     "gm_tc_selftest": ([_c_i64, _c_i64, _c_int, _c_int, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
+    "gm_mask_ring_runs": ([_c_i64, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
+    "gm_mask_apodize": ([_c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_dbl, _c_int, _c_vp, _c_vp],
+                        _c_int),
 }
 
 STATUS = {0: "GM_OK", 1: "GM_ERR_BAD_SHAPE", 2: "GM_ERR_BAD_PTR", 3: "GM_ERR_LAUNCH",

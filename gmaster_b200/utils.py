@@ -2,7 +2,8 @@
 
 Geometry: `NmtMapInfo` (HEALPix) and `NmtAlmInfo` (healpy-packed alm layout).
 Transforms: `map2alm`, `alm2map`, `map2alm_pair` on the GPU (spin 0 and spin 2).
-Fixture helpers: `mask_apodization` (C1/C2), `synfast_spherical`, `pix2vec_ring`.
+Masks: `mask_apodization` (C1 / C2 / Smooth, on the GPU).
+Fixture helpers: `synfast_spherical`, `pix2vec_ring`.
 
 Arrays are returned as CUDA ``torch.Tensor``s; inputs may be numpy arrays or tensors.
 """
@@ -10,7 +11,7 @@ Arrays are returned as CUDA ``torch.Tensor``s; inputs may be numpy arrays or ten
 import numpy as np
 import torch
 
-from . import sht
+from . import _lib, sht
 from ._config import (get_default_params, get_precision, nmt_params, set_n_iter_default,
                       set_precision, set_sht_calculator, set_tol_pinv_default)
 
@@ -18,7 +19,7 @@ __all__ = [
     "NmtAlmInfo", "NmtMapInfo", "alm2map", "map2alm", "map2alm_pair", "mask_apodization",
     "synfast_spherical", "pix2vec_ring", "nmt_params", "get_default_params",
     "set_n_iter_default", "set_tol_pinv_default", "set_precision", "get_precision",
-    "set_sht_calculator", "as_device",
+    "set_sht_calculator", "as_device", "max_pixel_radius",
 ]
 
 
@@ -144,40 +145,121 @@ def pix2vec_ring(nside, pix=None):
     return vec if pix is None else vec[pix]
 
 
-def mask_apodization(mask_in, aposize, apotype="C1"):
-    """C1 / C2 apodisation of a binary HEALPix mask (gmaster/utils.py:61-147 semantics).
+_APO_TABLES = {}
 
-    The distance to the nearest masked pixel uses a k-d tree over the pixel unit
-    vectors (scipy), with ``x = sqrt((1 - cos d) / (1 - cos aposize))``.
+
+def _apo_ring_table(nside, device):
+    """(3, nring) float64 [cos theta; sin theta; phi0] of the rings on `device` (cached)."""
+    key = (int(nside), device.index)
+    tab = _APO_TABLES.get(key)
+    if tab is None:
+        theta, phi0, _, _ = sht.ring_geometry(nside)
+        host = np.stack([np.cos(theta), np.sin(theta), phi0])
+        tab = torch.from_numpy(host).to(device)
+        _APO_TABLES[key] = tab
+    return tab
+
+
+def max_pixel_radius(nside):
+    """Upper bound of the angular distance from a HEALPix pixel centre to its pixel's edge.
+
+    At the latitude of ring k the pixel vertices interleave with ring k's centres, half an
+    azimuthal step (pi / nphi_k) from them.  A pixel of ring j has its vertices on the
+    latitudes of rings j - 1, j and j + 1 (the poles beyond the first and last ring), each
+    within half that latitude's step of the centre's longitude; the bound is the largest
+    such distance over all rings.
     """
-    if apotype not in ("C1", "C2"):
-        raise ValueError(f"Apodization type {apotype} unknown. Choose from ['C1', 'C2']")
+    theta, _, nphi, _ = sht.ring_geometry(nside)
+    half = np.pi / nphi.astype(np.float64)
+    north_t = np.concatenate([[0.0], theta[:-1]])
+    north_h = np.concatenate([[0.0], half[:-1]])
+    south_t = np.concatenate([theta[1:], [np.pi]])
+    south_h = np.concatenate([half[1:], [0.0]])
+
+    def dist(t1, t2, dphi):
+        # great-circle angle between (t1, 0) and (t2, dphi), haversine form
+        h = np.sin(0.5 * (t2 - t1)) ** 2 + np.sin(t1) * np.sin(t2) * np.sin(0.5 * dphi) ** 2
+        return 2 * np.arcsin(np.sqrt(np.minimum(h, 1.0)))
+
+    return float(max(dist(theta, north_t, north_h).max(), dist(theta, south_t, south_h).max(),
+                     dist(theta, theta, half).max()))
+
+
+def mask_apodization(mask_in, aposize, apotype="C1"):
+    """Apodise a binary HEALPix mask on the GPU (gmaster/utils.py:61-147).
+
+    A pixel counts as masked where the mask is <= 0.  With theta the angular distance from
+    a pixel to the nearest masked pixel, theta_* = `aposize` (degrees) and
+    x = sqrt((1 - cos theta) / (1 - cos theta_*)), unmasked pixels closer than theta_* are
+    multiplied by x - sin(2 pi x) / (2 pi) ("C1") or (1 - cos(pi x)) / 2 ("C2").  The
+    distance is exact over all masked pixels (the reference queries a k-d tree of their unit
+    vectors; here the CUDA kernel walks the HEALPix rings, gm_mask_apodize).
+
+    "Smooth": pixels within 2.5 theta_* of a masked pixel are zeroed, the result is
+    smoothed with a Gaussian beam of standard deviation theta_* (map2alm with n_iter = 3,
+    alm2map) and multiplied by the mask.  The reference selects the zeroed pixels with
+    healpy's inclusive query_disc (pixels overlapping the discs, "maybe a few more"); here
+    a pixel is zeroed when its centre lies within 2.5 theta_* + `max_pixel_radius(nside)`
+    of a masked pixel's centre, which contains every overlapping pixel.
+
+    Returns a numpy array for "C1"/"C2" when `mask_in` is not a tensor, else a CUDA tensor;
+    "Smooth" always returns a CUDA tensor (the reference returns a device array there).
+    """
+    if apotype not in ("C1", "C2", "Smooth"):
+        raise ValueError(
+            f"Apodization type {apotype} unknown. Choose from ['C1', 'C2', 'Smooth']")
     if aposize < 0:
         raise ValueError("Apodization scale must be a positive number")
-    mask = np.asarray(mask_in, dtype=np.float64)
-    if mask.ndim != 1:
+    as_numpy = not isinstance(mask_in, torch.Tensor) and apotype != "Smooth"
+    if isinstance(mask_in, torch.Tensor) and mask_in.ndim != 1:
         raise ValueError("Mask must be a one-dimensional HEALPix map")
-    if aposize == 0:
-        return mask.copy()
-    from scipy.spatial import cKDTree
+    if not isinstance(mask_in, torch.Tensor) and np.ndim(mask_in) != 1:
+        raise ValueError("Mask must be a one-dimensional HEALPix map")
+    _lib.require_cuda()
+    mask = as_device(mask_in, torch.float64)
 
-    nside = int(round(np.sqrt(len(mask) / 12)))
+    def result(t):
+        return t.cpu().numpy() if as_numpy else t
+
+    if aposize == 0:
+        return result(mask.clone())
+    npix = mask.shape[0]
+    nside = int(round(np.sqrt(npix / 12)))
+    if 12 * nside * nside != npix:
+        raise ValueError("Mask size is not a valid HEALPix map size")
     radius = np.radians(aposize)
-    if int(4 * len(mask) * (1 - np.cos(1.2 * radius))) < 2:
+    scale = 2.5 if apotype == "Smooth" else 1.2
+    if int(4 * npix * (1 - np.cos(scale * radius))) < 2:
         raise ValueError("Your apodization scale is too small for this pixel size")
-    masked = np.flatnonzero(mask <= 0)
-    if not len(masked):
-        return mask.copy()
-    vectors = pix2vec_ring(nside)
-    distances, _ = cKDTree(vectors[masked]).query(vectors)
-    measure = 0.5 * distances ** 2
+    if not bool((mask <= 0).any()):
+        return result(mask.clone())
+    dev = mask.device
+    prev = torch.empty(npix, dtype=torch.int32, device=dev)
+    nxt = torch.empty(npix, dtype=torch.int32, device=dev)
+    out = torch.empty_like(mask)
+    stream = _lib.stream_handle(dev)
+    _lib.call("gm_mask_ring_runs", nside, _lib.ptr(mask), _lib.ptr(prev), _lib.ptr(nxt), stream)
+    table = _apo_ring_table(nside, dev)
+    if apotype == "Smooth":
+        reach = min(2.5 * radius + max_pixel_radius(nside), np.pi)
+        chord2 = 4.0 * np.sin(0.5 * reach) ** 2
+        if reach >= np.pi:
+            chord2 = 5.0   # every pixel is within reach
+        _lib.call("gm_mask_apodize", nside, _lib.ptr(table), _lib.ptr(mask), _lib.ptr(prev),
+                  _lib.ptr(nxt), float(chord2), 0.0, 2, _lib.ptr(out), stream)
+        del prev, nxt
+        lmax = 3 * nside - 1
+        prec = get_precision()
+        alm = sht.map2alm_device(out[None], 0, nside, lmax, 3, prec)
+        ell = torch.from_numpy(NmtAlmInfo(lmax).ell_m()[0].astype(np.float64)).to(dev)
+        beam = torch.exp(-0.5 * ell * (ell + 1) * radius ** 2)
+        smoothed = sht.alm2map_device(alm * beam[None], 0, nside, lmax, prec)[0]
+        return smoothed * mask
     threshold = 1 - np.cos(radius)
-    affected = (mask > 0) & (measure < threshold)
-    x = np.sqrt(np.maximum(measure[affected], 0) / threshold)
-    factor = x - np.sin(2 * np.pi * x) / (2 * np.pi) if apotype == "C1" else 0.5 * (1 - np.cos(np.pi * x))
-    out = mask.copy()
-    out[affected] *= factor
-    return out
+    _lib.call("gm_mask_apodize", nside, _lib.ptr(table), _lib.ptr(mask), _lib.ptr(prev),
+              _lib.ptr(nxt), float(2 * threshold), float(threshold),
+              0 if apotype == "C1" else 1, _lib.ptr(out), stream)
+    return result(out)
 
 
 def gaussian_alm(cls, lmax, rng):

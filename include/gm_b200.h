@@ -343,6 +343,26 @@ int gm_tc_synd_to_syn_window(int64_t nside, int64_t lmax, int spin, int64_t ncom
 int gm_tc_alm_layout(int64_t lmax, int spin, int64_t nfield, double *alm_i, double *alm_api,
                      int to_api, void *stream);
 
+/* ---------------------------------------------------------- mask apodisation */
+
+/* Replaces the host k-d tree and query_disc of mask_apodization (gmaster/utils.py:61-147).
+ * gm_mask_ring_runs: for every pixel p of a RING-ordered (npix,) mask, prev[p] / next[p] =
+ * ring-local index of the masked pixel (mask <= 0) at or before / at or after p, cyclically
+ * within p's ring; -1 on rings without masked pixels.  prev and next are caller-owned int32
+ * (npix,) buffers.  nside in [1, 16384].
+ * gm_mask_apodize: ring_table = (3, 4 nside - 1) float64 [cos theta; sin theta; phi0] of
+ * the rings.  For every pixel, the chord^2 d^2 to the nearest masked pixel (exact, over all
+ * masked pixels) is found when below chord2_max (exclusive).  mode 0 (C1) / 1 (C2): out =
+ * mask * f(x), x = sqrt(d^2 / 2 / threshold), for pixels with mask > 0 and d^2 <
+ * chord2_max, else out = mask; f = x - sin(2 pi x)/(2 pi) (C1) or (1 - cos(pi x))/2 (C2).
+ * mode 2 (zeroing step of "Smooth"): out = 0 for masked pixels and for pixels with d^2 <
+ * chord2_max, else mask.  out may not alias mask. */
+int gm_mask_ring_runs(int64_t nside, const double *mask, int32_t *prev, int32_t *next,
+                      void *stream);
+int gm_mask_apodize(int64_t nside, const double *ring_table, const double *mask,
+                    const int32_t *prev, const int32_t *next, double chord2_max,
+                    double threshold, int mode, double *out, void *stream);
+
 /* ---------------------------------------------------------- tensor-core check */
 
 /* One-CTA tcgen05 check: D[128 x N] (float32, row-major) = A[128 x K] * B[N x K]^T where

@@ -181,3 +181,51 @@ def test_mask_alm_cache_follows_the_mask_tensor():
     del f.mask
     gc.collect()
     assert len(F._MASK_ALMS) == n - 1
+
+
+def test_mask_apodization_validates_before_any_device_work():
+    """Argument errors of mask_apodization (gmaster/utils.py:92-101) need no GPU."""
+    from gmaster_b200 import mask_apodization
+
+    mask = np.ones(12 * 8 ** 2)
+    with pytest.raises(ValueError, match="unknown"):
+        mask_apodization(mask, 1.0, apotype="C3")
+    with pytest.raises(ValueError, match="positive"):
+        mask_apodization(mask, -1.0)
+    with pytest.raises(ValueError, match="one-dimensional"):
+        mask_apodization(np.ones((2, 768)), 1.0)
+
+
+def test_pixel_radius_bound_matches_oracle_and_bounds_the_pixels():
+    """The Smooth zeroing margin: the product's bound equals the oracle's restatement, and
+    it exceeds the distance from every pixel centre to the nearest centre of a neighbouring
+    ring (the vertices lie at least that far apart)."""
+    import oracle
+    from gmaster_b200.utils import max_pixel_radius
+
+    for nside in (1, 2, 4, 16, 256, 2048):
+        got = max_pixel_radius(nside)
+        assert abs(got - oracle.pixel_radius_bound(nside)) < 1e-9 * got
+        theta = oracle.geometry(nside)[0]
+        assert got >= 0.5 * np.max(np.diff(theta))
+        assert got < 1.25 / nside + 0.2 / nside ** 2
+
+
+def test_oracle_apodization_nearest_pixel_is_exact():
+    """The oracle's k-d tree distances (C1/C2) against a brute-force minimum over all
+    masked pixels at Nside 8: pins the restatement of gmaster/utils.py:130-146."""
+    import oracle
+
+    nside = 8
+    vec = oracle.pix2vec(nside)
+    mask = (vec[:, 2] < 0.3).astype(float)
+    mask[[17, 300, 555]] = 0.0
+    for apotype in ("C1", "C2"):
+        got = oracle.mask_apodization(mask, 25.0, apotype)
+        mv = vec[mask <= 0]
+        d2 = ((vec[:, None, :] - mv[None, :, :]) ** 2).sum(axis=2).min(axis=1)
+        thr = 1 - np.cos(np.radians(25.0))
+        x = np.sqrt(0.5 * d2 / thr)
+        f = x - np.sin(2 * np.pi * x) / (2 * np.pi) if apotype == "C1" else 0.5 * (1 - np.cos(np.pi * x))
+        want = np.where((mask > 0) & (0.5 * d2 < thr), mask * f, mask)
+        np.testing.assert_allclose(got, want, rtol=0, atol=1e-14)
