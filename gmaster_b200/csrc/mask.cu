@@ -28,6 +28,7 @@ namespace {
 constexpr int kRunThreads = 1024;
 constexpr int kApoThreads = 256;
 constexpr double kTwoPi = 6.283185307179586;   // 2 pi rounded to double, as numpy's 2*np.pi
+constexpr double kInvTwoPi = 0.15915494309189535;
 
 // One CTA per ring (grid-stride over rings).  Thread t scans a contiguous chunk of the ring;
 // two block-wide scans give the last masked pixel before each chunk and the first after.
@@ -89,6 +90,11 @@ __global__ void __launch_bounds__(kRunThreads) k_ring_runs(int64_t nside,
     }
 }
 
+// Ring table rows (each nring doubles): cos theta, sin theta, phi0, 2 pi / nphi, nphi / (2 pi).
+struct Rings {
+    const double *z, *s, *phi0, *step, *inv;
+};
+
 struct Query {
     double z, s, phi;
     double best;   // smallest chord^2 found so far (starts at the search radius, exclusive)
@@ -96,20 +102,18 @@ struct Query {
 };
 
 // Visit ring jj for query q: false once the ring's latitude alone is out of reach.
-__device__ __forceinline__ bool probe(int64_t nside, int64_t jj, const double *__restrict__ rz,
-                                      const double *__restrict__ rs,
-                                      const double *__restrict__ rphi0,
+__device__ __forceinline__ bool probe(int64_t nside, int64_t jj, const Rings &rg,
                                       const int32_t *__restrict__ prev,
                                       const int32_t *__restrict__ next, Query &q)
 {
-    const double zc = rz[jj], sc = rs[jj];
+    const double zc = rg.z[jj], sc = rg.s[jj];
     const double dz = q.z - zc, ds = q.s - sc;
     const double lb = dz * dz + ds * ds;   // chord^2 to the ring point at the same phi
     if (lb >= q.best) return false;
     const int64_t nn = ring_nphi(nside, jj);
     const int64_t off = ring_offset(nside, jj);
-    const double phi0 = rphi0[jj];
-    const double tpos = (q.phi - phi0) * ((double)nn / kTwoPi);
+    const double phi0 = rg.phi0[jj], step = rg.step[jj];
+    const double tpos = (q.phi - phi0) * rg.inv[jj];
     // phi_q < 2 pi + pi/4 and phi0 >= 0, so floor(tpos) lies in [-1, 9 nn / 8]
     int k = (int)floor(tpos);
     if (k < 0) k += (int)nn;
@@ -122,8 +126,8 @@ __device__ __forceinline__ bool probe(int64_t nside, int64_t jj, const double *_
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
         const int32_t c = u == 0 ? a : b;
-        double dphi = phi0 + kTwoPi * (double)c / (double)nn - q.phi;
-        dphi -= kTwoPi * rint(dphi / kTwoPi);   // into [-pi, pi]
+        double dphi = fma((double)c, step, phi0 - q.phi);
+        dphi -= kTwoPi * rint(dphi * kInvTwoPi);   // into [-pi, pi]
         // sin(|x|/2) >= |x|/pi on [0, pi]: skip the sine when even that bound loses
         const double rough = lb + w * (dphi * dphi) * (1.0 / (M_PI * M_PI));
         if (rough >= q.best) continue;
@@ -141,8 +145,7 @@ __device__ __forceinline__ bool probe(int64_t nside, int64_t jj, const double *_
 // radius, x = sqrt(0.5 d^2 / threshold)); mode 2: zeroing step (out = 0 for masked pixels
 // and for pixels closer than the radius to a masked one, else the mask value).
 __global__ void __launch_bounds__(kApoThreads) k_mask_apodize(
-    int64_t nside, const double *__restrict__ rz, const double *__restrict__ rs,
-    const double *__restrict__ rphi0, const double *__restrict__ mask,
+    int64_t nside, Rings rg, const double *__restrict__ mask,
     const int32_t *__restrict__ prev, const int32_t *__restrict__ next, double chord2_max,
     double threshold, int mode, double *__restrict__ out)
 {
@@ -158,15 +161,15 @@ __global__ void __launch_bounds__(kApoThreads) k_mask_apodize(
         return;
     }
     Query q;
-    q.z = rz[j];
-    q.s = rs[j];
-    q.phi = rphi0[j] + kTwoPi * (double)i / (double)n;
+    q.z = rg.z[j];
+    q.s = rg.s[j];
+    q.phi = fma((double)i, rg.step[j], rg.phi0[j]);
     q.best = chord2_max;
     q.found = false;
     bool up = true, dn = true;
     for (int64_t d = 0; up || dn; ++d) {
-        if (up) up = j + d < nring && probe(nside, j + d, rz, rs, rphi0, prev, next, q);
-        if (dn) dn = j - 1 - d >= 0 && probe(nside, j - 1 - d, rz, rs, rphi0, prev, next, q);
+        if (up) up = j + d < nring && probe(nside, j + d, rg, prev, next, q);
+        if (dn) dn = j - 1 - d >= 0 && probe(nside, j - 1 - d, rg, prev, next, q);
     }
     if (!q.found) {
         out[p] = m;
@@ -207,8 +210,9 @@ extern "C" int gm_mask_apodize(int64_t nside, const double *ring_table, const do
     if (!(chord2_max > 0.0) || (mode != 2 && !(threshold > 0.0))) return GM_ERR_BAD_SHAPE;
     const int64_t nring = 4 * nside - 1;
     const dim3 grid((unsigned)((4 * nside + kApoThreads - 1) / kApoThreads), (unsigned)nring);
-    k_mask_apodize<<<grid, kApoThreads, 0, as_stream(stream)>>>(
-        nside, ring_table, ring_table + nring, ring_table + 2 * nring, mask, prev, next,
-        chord2_max, threshold, mode, out);
+    const Rings rg{ring_table, ring_table + nring, ring_table + 2 * nring, ring_table + 3 * nring,
+                   ring_table + 4 * nring};
+    k_mask_apodize<<<grid, kApoThreads, 0, as_stream(stream)>>>(nside, rg, mask, prev, next,
+                                                                 chord2_max, threshold, mode, out);
     return check_launch("gm_mask_apodize");
 }

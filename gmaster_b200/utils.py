@@ -149,12 +149,14 @@ _APO_TABLES = {}
 
 
 def _apo_ring_table(nside, device):
-    """(3, nring) float64 [cos theta; sin theta; phi0] of the rings on `device` (cached)."""
+    """(5, nring) float64 [cos theta; sin theta; phi0; 2 pi / nphi; nphi / (2 pi)] of the
+    rings on `device` (cached)."""
     key = (int(nside), device.index)
     tab = _APO_TABLES.get(key)
     if tab is None:
-        theta, phi0, _, _ = sht.ring_geometry(nside)
-        host = np.stack([np.cos(theta), np.sin(theta), phi0])
+        theta, phi0, nphi, _ = sht.ring_geometry(nside)
+        n = nphi.astype(np.float64)
+        host = np.stack([np.cos(theta), np.sin(theta), phi0, 2 * np.pi / n, n / (2 * np.pi)])
         tab = torch.from_numpy(host).to(device)
         _APO_TABLES[key] = tab
     return tab

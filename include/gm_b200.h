@@ -350,8 +350,8 @@ int gm_tc_alm_layout(int64_t lmax, int spin, int64_t nfield, double *alm_i, doub
  * ring-local index of the masked pixel (mask <= 0) at or before / at or after p, cyclically
  * within p's ring; -1 on rings without masked pixels.  prev and next are caller-owned int32
  * (npix,) buffers.  nside in [1, 16384].
- * gm_mask_apodize: ring_table = (3, 4 nside - 1) float64 [cos theta; sin theta; phi0] of
- * the rings.  For every pixel, the chord^2 d^2 to the nearest masked pixel (exact, over all
+ * gm_mask_apodize: ring_table = (5, 4 nside - 1) float64 [cos theta; sin theta; phi0;
+ * 2 pi / nphi; nphi / (2 pi)] of the rings.  For every pixel, the chord^2 d^2 to the nearest masked pixel (exact, over all
  * masked pixels) is found when below chord2_max (exclusive).  mode 0 (C1) / 1 (C2): out =
  * mask * f(x), x = sqrt(d^2 / 2 / threshold), for pixels with mask > 0 and d^2 <
  * chord2_max, else out = mask; f = x - sin(2 pi x)/(2 pi) (C1) or (1 - cos(pi x))/2 (C2).

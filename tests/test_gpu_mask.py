@@ -87,7 +87,7 @@ def test_errors(cuda):
         nmt.mask_apodization(np.ones(100), 5.0)
     dev = torch.zeros(12 * 16, dtype=torch.float64, device="cuda")
     i32 = torch.zeros(12 * 16, dtype=torch.int32, device="cuda")
-    tab = torch.zeros(3 * 7, dtype=torch.float64, device="cuda")
+    tab = torch.zeros(5 * 7, dtype=torch.float64, device="cuda")
     st = _lib.stream_handle()
     lib = _lib.load()
     assert lib.gm_mask_apodize(4, _lib.ptr(tab), _lib.ptr(dev), _lib.ptr(i32), _lib.ptr(i32), 1.0,
