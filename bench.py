@@ -61,14 +61,16 @@ def parse():
     p.add_argument("--fp64-steps", type=int, default=1)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", default="mc",
-                   choices=["mc", "uneven_workspaces", "nside4096", "mc1024", "nside8192", "apodize"],
+                   choices=["mc", "uneven_workspaces", "nside4096", "mc1024", "nside8192", "apodize",
+                            "covariance"],
                    help="mc: the Monte-Carlo estimator (default); uneven_workspaces: TT "
                         "coupling matrices of 32 masks of mixed Nside in one launch; nside4096: "
                         "batched map2alm (n_iter=0) and alm2map at Nside 4096; mc1024: 512 TQU "
                         "simulations at Nside 1024, batched and per simulation as a CUDA graph; "
                         "nside8192: one spin-2 spectrum at Nside 8192 with the exact and the "
                         "Toeplitz coupling matrix; apodize: C1 apodisation of the binary "
-                        "Nside 2048 and 8192 config masks on the GPU")
+                        "Nside 2048 and 8192 config masks on the GPU; covariance: Gaussian "
+                        "(NKA) covariance workspaces and bandpower covariances at Nside 2048")
     p.add_argument("--apo-nsides", default="2048,8192",
                    help="apodize workload: the Nside values to run (the first is the headline)")
     p.add_argument("--nmasks", type=int, default=32)
@@ -921,6 +923,83 @@ def run_apodize(args):
     print(json.dumps(line), flush=True)
 
 
+def run_covariance(args):
+    """Gaussian covariance at Nside 2048 (lmax 6143, bands of 16) on the config mask: the
+    covariance workspace (mask-product transform, 3j kernels) and the decoupled bandpower
+    covariance, for TT x TT (spins 0,0,0,0), TE x TE (0,2,0,2) and the spin-2 auto
+    covariance (2,2,2,2) with iNKA input spectra."""
+    import torch
+
+    import gmaster_b200 as nmt
+    from gmaster_b200 import _lib
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    nside, nlb = args.nside, args.nlb
+    lmax = 3 * nside - 1
+    mask = make_mask(nside, dev)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(7)
+    t = torch.randn((1, 12 * nside * nside), generator=gen, device=dev, dtype=torch.float64)
+    qu = torch.randn((2, 12 * nside * nside), generator=gen, device=dev, dtype=torch.float64)
+    f0 = nmt.NmtField(mask, t, n_iter=0, precision="mixed")
+    f2 = nmt.NmtField(mask, qu, spin=2, n_iter=0, precision="mixed")
+    f0.get_mask_alms()
+    b = nmt.NmtBin.from_nside_linear(nside, nlb)
+    ws = {(0, 0): nmt.NmtWorkspace.from_fields(f0, f0, b),
+          (0, 2): nmt.NmtWorkspace.from_fields(f0, f2, b),
+          (2, 2): nmt.NmtWorkspace.from_fields(f2, f2, b)}
+    fld = {0: f0, 2: f2}
+    cells = {}
+    for s1, s2 in ((0, 0), (0, 2), (2, 0), (2, 2)):
+        cells[(s1, s2)] = nmt.get_iNKA_cell(fld[s1], fld[s2])
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    calls0 = dict(_lib.CALLS)
+    res = {}
+    st = torch.cuda.current_stream(dev)
+    for spins in ((0, 0, 0, 0), (0, 2, 0, 2), (2, 2, 2, 2)):
+        a1, a2, b1, b2 = (fld[s] for s in spins)
+        for _ in range(args.warmup):
+            cw = nmt.NmtCovarianceWorkspace.from_fields(a1, a2, b1, b2)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record(st)
+        for _ in range(args.steps):
+            cw = nmt.NmtCovarianceWorkspace.from_fields(a1, a2, b1, b2)
+        e[1].record(st)
+        cl = (cells[(spins[0], spins[2])], cells[(spins[0], spins[3])],
+              cells[(spins[1], spins[2])], cells[(spins[1], spins[3])])
+        wa, wb = ws[(spins[0], spins[1])], ws[(spins[2], spins[3])]
+        for _ in range(args.steps):
+            cov = cw.gaussian_covariance(*cl, wa, wb)
+        e[2].record(st)
+        torch.cuda.synchronize()
+        res["".join(map(str, spins))] = {
+            "workspace_s": e[0].elapsed_time(e[1]) / 1e3 / args.steps,
+            "covariance_s": e[1].elapsed_time(e[2]) / 1e3 / args.steps,
+            "shape": list(cov.shape),
+            "min_diag": float(torch.diagonal(cov).min()),
+        }
+    clocks = sampler.stop()
+    launches = sum(_lib.CALLS.get(k, 0) - calls0.get(k, 0) for k in _lib.CALLS)
+    head = res["2222"]
+    line = {
+        "metric": "Gaussian covariance s (workspace + decoupled bandpower covariance), Nside 2048",
+        "value": head["workspace_s"] + head["covariance_s"], "unit": "s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": (head["workspace_s"] + head["covariance_s"]) * 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (mask transforms mixed precision)",
+        "data": "synthetic (config mask recipe; iNKA spectra of Gaussian maps)",
+        "config": {"workload": f"NKA covariance of the spin-2 auto spectrum (2,2,2,2), Nside "
+                               f"{nside}, lmax {lmax}, bands of {nlb}; TT and TE beside it",
+                   "nside": nside, "lmax": lmax, "nlb": nlb},
+        "per_spins": res, "clocks": clocks, "gpu_launches": int(launches),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -940,6 +1019,9 @@ def main():
         return
     if args.workload == "apodize":
         run_apodize(args)
+        return
+    if args.workload == "covariance":
+        run_covariance(args)
         return
     import torch
     import torch.distributed as dist

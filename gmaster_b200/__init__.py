@@ -12,13 +12,15 @@ from ._config import (get_default_params, get_precision, nmt_params, set_n_iter_
 from .batch import (SimulationGraph, compute_coupled_cells, decouple_cells, fields_from_maps,
                     mc_bandpowers, workspaces_from_fields)
 from .bins import NmtBin
+from .covariance import NmtCovarianceWorkspace, gaussian_covariance, get_iNKA_cell
 from .field import NmtField
 from .utils import (NmtAlmInfo, NmtMapInfo, alm2map, map2alm, map2alm_pair, mask_apodization,
                     synfast_spherical)
 from .workspaces import NmtWorkspace, compute_coupled_cell
 
 __all__ = [
-    "NmtAlmInfo", "NmtBin", "NmtField", "NmtMapInfo", "NmtWorkspace", "alm2map",
+    "NmtAlmInfo", "NmtBin", "NmtCovarianceWorkspace", "NmtField", "NmtMapInfo", "NmtWorkspace",
+    "alm2map", "gaussian_covariance", "get_iNKA_cell",
     "compute_coupled_cell", "compute_coupled_cells", "decouple_cells", "fields_from_maps",
     "mc_bandpowers", "workspaces_from_fields", "SimulationGraph",
     "get_default_params", "get_precision", "map2alm", "map2alm_pair",

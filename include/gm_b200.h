@@ -363,6 +363,27 @@ int gm_mask_apodize(int64_t nside, const double *ring_table, const double *mask,
                     const int32_t *prev, const int32_t *next, double chord2_max,
                     double threshold, int mode, double *out, void *stream);
 
+/* ---------------------------------------------------------- Gaussian covariance */
+
+/* Narrow-kernel Gaussian covariance of two pseudo-C_ell power spectra (replaces the jnp
+ * assembly and binning of NmtCovarianceWorkspace.gaussian_covariance,
+ * gmaster/covariance.py:407-575).  Output block x (< nblocks <= 16) is
+ *   cov_x(l1, l2) = sum over terms t in [block_ptr[x], block_ptr[x+1]) of
+ *     signs[t] * (A(l1) B(l2) + A(l2) B(l1)) / 2 * xi[k](l1, l2),
+ * (k, ra, rb) = terms[3t .. 3t+2], A = spec[ra], B = spec[rb] (rows of L = lmax + 1
+ * doubles), xi = (nk, L, L) float64 coupling kernels.  All indices are trusted.
+ * gm_cov_binned: out (nblocks, nbands_a, nbands_b) = sum over l1 in band p (CSR ptr_a /
+ * ells_a) and l2 in band q of w_a[l1] w_b[l2] cov_x(l1, l2); nbands_a <= 65535.
+ * gm_cov_coupled: out (nblocks, L, L) = cov_x; L <= 65535. */
+int gm_cov_binned(int64_t lmax, int64_t nblocks, const double *xi, const double *spec,
+                  const int32_t *terms, const double *signs, const int32_t *block_ptr,
+                  int64_t nbands_a, const int32_t *ptr_a, const int32_t *ells_a,
+                  const double *w_a, int64_t nbands_b, const int32_t *ptr_b,
+                  const int32_t *ells_b, const double *w_b, double *out, void *stream);
+int gm_cov_coupled(int64_t lmax, int64_t nblocks, const double *xi, const double *spec,
+                   const int32_t *terms, const double *signs, const int32_t *block_ptr,
+                   double *out, void *stream);
+
 /* ---------------------------------------------------------- tensor-core check */
 
 /* One-CTA tcgen05 check: D[128 x N] (float32, row-major) = A[128 x K] * B[N x K]^T where

@@ -229,3 +229,50 @@ def test_oracle_apodization_nearest_pixel_is_exact():
         f = x - np.sin(2 * np.pi * x) / (2 * np.pi) if apotype == "C1" else 0.5 * (1 - np.cos(np.pi * x))
         want = np.where((mask > 0) & (0.5 * d2 < thr), mask * f, mask)
         np.testing.assert_allclose(got, want, rtol=0, atol=1e-14)
+
+
+def _emulate_cov_terms(kernels, rows, signs, bptr, spec):
+    """The per-element sum of gm_cov_binned / gm_cov_coupled, restated in numpy."""
+    L = spec.shape[1]
+    out = np.zeros((len(bptr) - 1, L, L))
+    for x in range(len(bptr) - 1):
+        for t in range(bptr[x], bptr[x + 1]):
+            k, ra, rb = rows[t]
+            A, B = spec[ra], spec[rb]
+            sym = 0.5 * (A[:, None] * B[None, :] + A[None, :] * B[:, None])
+            out[x] += signs[t] * sym * np.asarray(kernels[k])
+    return out
+
+
+@pytest.mark.parametrize("spins", [(a, b, c, d) for a in (0, 2) for b in (0, 2)
+                                   for c in (0, 2) for d in (0, 2)])
+def test_covariance_term_table_matches_oracle_assembly(spins):
+    """The term table the CUDA covariance kernels evaluate (kernel, spectra rows, sign per
+    output block) reproduces the reference's assembly loops (gmaster/covariance.py:
+    407-429) restated in the oracle, for every spin combination, with random kernels."""
+    import oracle
+    import torch
+
+    from gmaster_b200.covariance import NmtCovarianceWorkspace, _kernel_spins
+
+    rng = np.random.default_rng(sum(s << i for i, s in enumerate(spins)))
+    L = 5
+    cw = NmtCovarianceWorkspace()
+    cw.spins = spins
+    cw._post_init()
+    names = {(0, 0): ("00",), (0, 2): ("0s",), (2, 2): ("pp", "mm")}
+    pairs = (_kernel_spins(spins[0], spins[1], spins[2], spins[3]),
+             _kernel_spins(spins[0], spins[1], spins[3], spins[2]))
+    cw.xiSS = []
+    for pair in pairs:
+        d = {n: None for n in ("00", "0s", "pp", "mm")}
+        for n in names[pair]:
+            d[n] = torch.from_numpy(rng.normal(size=(L, L)))
+        cw.xiSS.append(d)
+    na, nb, nc, nd = cw.nmaps
+    cls = [rng.normal(size=(r, L)) for r in (na * nc, na * nd, nb * nc, nb * nd)]
+    kernels, rows, signs, bptr = cw._terms()
+    got = _emulate_cov_terms([k.numpy() for k in kernels], rows, signs, bptr, np.concatenate(cls))
+    xis = [{k: (None if v is None else v.numpy()) for k, v in d.items()} for d in cw.xiSS]
+    want = oracle.nka_assemble(spins, xis, *cls, L).reshape(cw.nclsa * cw.nclsb, L, L)
+    np.testing.assert_allclose(got, want, rtol=0, atol=1e-12)
