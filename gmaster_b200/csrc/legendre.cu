@@ -56,7 +56,7 @@ __device__ __forceinline__ void rescale(double &v, double &vp, int &k)
 // Recurrence coefficients for target degree l (lambda_l from lambda_{l-1}, lambda_{l-2}):
 //   lambda_l = alpha (x - m s'/((l-1) l)) lambda_{l-1} - beta lambda_{l-2}.
 struct Coef {
-    double alpha, beta, c0;  // c0 = 2 m / ((l-1) l) for spin 2, 0 for spin 0
+    double alpha, beta, c0;  // c0 = alpha 2 m / ((l-1) l) for spin 2, 0 for spin 0
 };
 
 __device__ __forceinline__ Coef make_coef(int l, int m, int s, int l0)
@@ -72,7 +72,8 @@ __device__ __forceinline__ Coef make_coef(int l, int m, int s, int l0)
     } else {
         c.beta = 0.0;
     }
-    c.c0 = (s != 0 && l >= 2) ? 2.0 * dm / ((dl - 1.0) * dl) : 0.0;
+    // alpha (x -+ c) = fma(alpha, x, -+alpha c): one FMA per row variant in the recurrence
+    c.c0 = (s != 0 && l >= 2) ? c.alpha * (2.0 * dm / ((dl - 1.0) * dl)) : 0.0;
     return c;
 }
 
@@ -195,9 +196,10 @@ __global__ void __launch_bounds__(kThreads) k_legendre_ana(
                                 v[0][r] = nv;
                                 rescale(v[0][r], vp[0][r], kx[0][r]);
                             } else {
-                                // s' = -2: x - m s'/((l-1)l) = x + c0 ; s' = +2: x - c0
-                                double nva = fma(cf.alpha * (x[r] + cf.c0), v[0][r], -cf.beta * vp[0][r]);
-                                double nvb = fma(cf.alpha * (x[r] - cf.c0), v[1][r], -cf.beta * vp[1][r]);
+                                // s' = -2: alpha (x - m s'/((l-1)l)) = fma(alpha, x, c0);
+                                // s' = +2: fma(alpha, x, -c0)  (c0 carries alpha)
+                                double nva = fma(fma(cf.alpha, x[r], cf.c0), v[0][r], -cf.beta * vp[0][r]);
+                                double nvb = fma(fma(cf.alpha, x[r], -cf.c0), v[1][r], -cf.beta * vp[1][r]);
                                 vp[0][r] = v[0][r];
                                 v[0][r] = nva;
                                 vp[1][r] = v[1][r];
@@ -369,8 +371,8 @@ __global__ void __launch_bounds__(kThreads) k_legendre_syn(
                             v[0][r] = nv;
                             rescale(v[0][r], vp[0][r], kx[0][r]);
                         } else {
-                            double nva = fma(cf.alpha * (x[r] + cf.c0), v[0][r], -cf.beta * vp[0][r]);
-                            double nvb = fma(cf.alpha * (x[r] - cf.c0), v[1][r], -cf.beta * vp[1][r]);
+                            double nva = fma(fma(cf.alpha, x[r], cf.c0), v[0][r], -cf.beta * vp[0][r]);
+                            double nvb = fma(fma(cf.alpha, x[r], -cf.c0), v[1][r], -cf.beta * vp[1][r]);
                             vp[0][r] = v[0][r];
                             v[0][r] = nva;
                             vp[1][r] = v[1][r];

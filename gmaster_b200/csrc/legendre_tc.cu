@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
                     if (l == l0) cf.beta = -1.0;
                     else if (l < L) cf = load_coef(p.coef, mb + l);
                     sAB[e] = make_double2(cf.alpha, cf.beta);
-                    if (SPIN) sC0[e] = sgn_c * cf.c0;
+                    if (SPIN) sC0[e] = sgn_c * cf.c0 * cf.alpha;   // alpha (x - c) = fma(alpha, x, -alpha c)
                 }
                 gen_barrier();
                 // lane state of group g + 1 is loaded while group g is generated
@@ -378,8 +378,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_ana_tc(Params p, const uint8_t 
 #pragma unroll
                             for (int e = 0; e < 8; ++e) {
                                 const double2 ab = cab[cc * 8 + e];
-                                const double xs = SPIN ? x - cc0[cc * 8 + e] : x;
-                                const double nv = fma(ab.x * xs, v, -ab.y * vp);
+                                const double a = SPIN ? fma(ab.x, x, -cc0[cc * 8 + e]) : ab.x * x;
+                                const double nv = fma(a, v, -ab.y * vp);
                                 vp = v;
                                 v = nv;
                                 vals[e] = emit ? (float)v : 0.0f;
@@ -562,7 +562,7 @@ __global__ void __launch_bounds__(kThreadsS, 1) k_syn_tc(Params p, const uint8_t
             if (tid < kKL) {
                 const int64_t so = (ch & 1) * kKL;
                 sAB[so + tid] = make_double2(cf.alpha, cf.beta);
-                if (SPIN) sC0[so + tid] = sgn_c * cf.c0;
+                if (SPIN) sC0[so + tid] = sgn_c * cf.c0 * cf.alpha;
             }
         };
         Coef pre = fetch(0);
@@ -591,8 +591,8 @@ __global__ void __launch_bounds__(kThreadsS, 1) k_syn_tc(Params p, const uint8_t
 #pragma unroll
                     for (int e = 0; e < 8; ++e) {
                         const double2 ab = cab[sub * 8 + e];
-                        const double xs = SPIN ? x - cc0[sub * 8 + e] : x;
-                        const double nv = fma(ab.x * xs, v, -ab.y * vp);
+                        const double a = SPIN ? fma(ab.x, x, -cc0[sub * 8 + e]) : ab.x * x;
+                        const double nv = fma(a, v, -ab.y * vp);
                         vp = v;
                         v = nv;
                         vals[e] = emit ? (float)v : 0.0f;
@@ -602,9 +602,9 @@ __global__ void __launch_bounds__(kThreadsS, 1) k_syn_tc(Params p, const uint8_t
                     for (int e = 0; e < 8; ++e) {
                         const int64_t l = lsub + e;
                         const double2 ab = cab[sub * 8 + e];
-                        const double xs = SPIN ? x - cc0[sub * 8 + e] : x;
+                        const double a = SPIN ? fma(ab.x, x, -cc0[sub * 8 + e]) : ab.x * x;
                         if (l > l0 && l < L) {
-                            const double nv = fma(ab.x * xs, v, -ab.y * vp);
+                            const double nv = fma(a, v, -ab.y * vp);
                             vp = v;
                             v = nv;
                         }
