@@ -43,7 +43,7 @@ def tiles(spin):
     buf = (ctypes.c_int32 * 64)()
     n = _lib.load().gm_legendre_tiles(int(spin), buf, 32)
     if n < 0:
-        raise ValueError("tiles exist for spin 0 and 2 only")
+        raise ValueError("no tiles for this spin (spins 0..8 have tiles)")
     return [(buf[2 * i], buf[2 * i + 1]) for i in range(n)]
 
 

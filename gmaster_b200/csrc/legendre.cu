@@ -23,6 +23,17 @@ namespace gm {
 constexpr int kThreads = 128;
 constexpr int kWarps = kThreads / 32;
 constexpr int kWindow = 32;
+// Spins 1..kMaxSpin share the polarised kernels (template SPIN = 2) with the spin passed at
+// run time; the seed table holds 2 kMaxSpin + 1 variants.
+constexpr int kMaxSpin = 8;
+
+// First seed-table variant of spin s >= 1 (s' = -s; the next one is s' = +s): spin 2 keeps
+// variants 1 and 2 (the tensor-core kernels read them), spin 1 takes 3 and 4, spin s >= 3
+// takes 2s - 1 and 2s.
+__host__ __device__ __forceinline__ int seed_variant(int s)
+{
+    return s == 2 ? 1 : (s == 1 ? 3 : 2 * s - 1);
+}
 constexpr double kBig = 2.037035976334486e90;     // 2^300
 constexpr double kShrink = 2.409919865102884e-181;  // 2^-600
 
@@ -56,7 +67,7 @@ __device__ __forceinline__ void rescale(double &v, double &vp, int &k)
 // Recurrence coefficients for target degree l (lambda_l from lambda_{l-1}, lambda_{l-2}):
 //   lambda_l = alpha (x - m s'/((l-1) l)) lambda_{l-1} - beta lambda_{l-2}.
 struct Coef {
-    double alpha, beta, c0;  // c0 = alpha 2 m / ((l-1) l) for spin 2, 0 for spin 0
+    double alpha, beta, c0;  // c0 = alpha s m / ((l-1) l) for spin s >= 1, 0 for spin 0
 };
 
 __device__ __forceinline__ Coef make_coef(int l, int m, int s, int l0)
@@ -73,7 +84,7 @@ __device__ __forceinline__ Coef make_coef(int l, int m, int s, int l0)
         c.beta = 0.0;
     }
     // alpha (x -+ c) = fma(alpha, x, -+alpha c): one FMA per row variant in the recurrence
-    c.c0 = (s != 0 && l >= 2) ? c.alpha * (2.0 * dm / ((dl - 1.0) * dl)) : 0.0;
+    c.c0 = (s != 0 && l >= 2) ? c.alpha * (ds * dm / ((dl - 1.0) * dl)) : 0.0;
     return c;
 }
 
@@ -109,7 +120,7 @@ template <typename T, int SPIN, int NC, int R>
 __global__ void __launch_bounds__(kThreads) k_legendre_ana(
     int64_t nside, int64_t lmax, int64_t ncomp, const double *__restrict__ geom,
     const double *__restrict__ seeds, const T *__restrict__ rhs, double *__restrict__ alm,
-    double scale)
+    double scale, int spin)
 {
     constexpr int NV = SPIN == 0 ? 2 * NC : 8;
     constexpr int LB = 32 / NV;
@@ -123,7 +134,8 @@ __global__ void __launch_bounds__(kThreads) k_legendre_ana(
     const int m = blockIdx.y;
     const int64_t c0 = (int64_t)blockIdx.z * NC;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int l0 = SPIN == 0 ? m : (m > 2 ? m : 2);
+    const int sv = SPIN == 0 ? 0 : spin;   // the field's spin (SPIN = 2: any spin >= 1)
+    const int l0 = m > sv ? m : sv;
     if (l0 > lmax) return;
 
     double x[R], v[NVAR][R], vp[NVAR][R];
@@ -137,7 +149,8 @@ __global__ void __launch_bounds__(kThreads) k_legendre_ana(
         const double ls = ok ? geom[nlanes + j] : 0.0, lc = ok ? geom[2 * nlanes + j] : 0.0;
 #pragma unroll
         for (int q = 0; q < NVAR; ++q) {
-            const int var = SPIN == 0 ? 0 : 1 + q;  // 1: s' = -2 (lambda+), 2: s' = +2 (lambda-)
+            // seed variants: s' = -s (lambda+), then s' = +s (lambda-, times (-1)^s)
+            const int var = SPIN == 0 ? 0 : seed_variant(sv) + q;
             if (ok) {
                 seed_lane(seeds + ((int64_t)var * L + m) * 4, ls, lc, v[q][r], kx[q][r]);
             } else {
@@ -155,11 +168,13 @@ __global__ void __launch_bounds__(kThreads) k_legendre_ana(
                                   : (T)0;
     }
 
-    // The rows of a reduce-scatter block start at l0 + (an even offset: kWindow and LB are
-    // even), so the parity of l + m in unrolled row s is ((l0 + m) + s) & 1.  With the two
-    // hemisphere halves of the right-hand side swapped once here when l0 + m is odd, row s
-    // takes half s & 1, chosen at compile time instead of by selects on every element.
-    if ((l0 + m) & 1) {
+    // The southern ring's rows are the northern ones times (-1)^(l + m + s) (for spin s,
+    // with the (-1)^s of the +s variant in its seed).  The rows of a reduce-scatter block
+    // start at l0 + (an even offset: kWindow and LB are even), so that parity in unrolled
+    // row s is ((l0 + m + sv) + s) & 1.  With the two hemisphere halves of the right-hand
+    // side swapped once here when l0 + m + sv is odd, row s takes half s & 1, chosen at
+    // compile time instead of by selects on every element.
+    if ((l0 + m + sv) & 1) {
 #pragma unroll
         for (int r = 0; r < R; ++r)
 #pragma unroll
@@ -174,7 +189,7 @@ __global__ void __launch_bounds__(kThreads) k_legendre_ana(
     for (int lb = l0; lb < L; lb += kWindow) {
         if (threadIdx.x < kWindow) {
             const int l = lb + threadIdx.x;
-            coef[threadIdx.x] = make_coef(l, m, SPIN, l0);
+            coef[threadIdx.x] = make_coef(l, m, sv, l0);
         }
         __syncthreads();
 #pragma unroll 1
@@ -209,7 +224,7 @@ __global__ void __launch_bounds__(kThreads) k_legendre_ana(
                             }
                         }
                     }
-                    const int par = s & 1;   // relative to (l0 + m) & 1, see above
+                    const int par = s & 1;   // relative to (l0 + m + sv) & 1, see above
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         if (SPIN == 0) {
@@ -291,7 +306,8 @@ __global__ void __launch_bounds__(kThreads) k_legendre_ana(
 template <typename T, int SPIN, int NC, int R>
 __global__ void __launch_bounds__(kThreads) k_legendre_syn(
     int64_t nside, int64_t lmax, int64_t ncomp, const double *__restrict__ geom,
-    const double *__restrict__ seeds, const double *__restrict__ alm, T *__restrict__ syn)
+    const double *__restrict__ seeds, const double *__restrict__ alm, T *__restrict__ syn,
+    int spin)
 {
     constexpr int NVAR = SPIN == 0 ? 1 : 2;
     constexpr int NA = SPIN == 0 ? NC : 2;  // complex alm rows per degree (maps, or E and B)
@@ -302,7 +318,8 @@ __global__ void __launch_bounds__(kThreads) k_legendre_syn(
     const int64_t L = lmax + 1, nlanes = 2 * nside, nelem = L * (L + 1) / 2;
     const int m = blockIdx.y;
     const int64_t c0 = (int64_t)blockIdx.z * NC;
-    const int l0 = SPIN == 0 ? m : (m > 2 ? m : 2);
+    const int sv = SPIN == 0 ? 0 : spin;
+    const int l0 = m > sv ? m : sv;
 
     double x[R], v[NVAR][R], vp[NVAR][R];
     int kx[NVAR][R];
@@ -315,7 +332,7 @@ __global__ void __launch_bounds__(kThreads) k_legendre_syn(
         const double ls = ok ? geom[nlanes + j] : 0.0, lc = ok ? geom[2 * nlanes + j] : 0.0;
 #pragma unroll
         for (int q = 0; q < NVAR; ++q) {
-            const int var = SPIN == 0 ? 0 : 1 + q;
+            const int var = SPIN == 0 ? 0 : seed_variant(sv) + q;
             if (ok) {
                 seed_lane(seeds + ((int64_t)var * L + m) * 4, ls, lc, v[q][r], kx[q][r]);
             } else {
@@ -332,7 +349,7 @@ __global__ void __launch_bounds__(kThreads) k_legendre_syn(
     for (int lb = l0; lb < L; lb += kWindow, buf ^= 1) {
         if (threadIdx.x < kWindow) {
             const int l = lb + threadIdx.x;
-            coef[buf][threadIdx.x] = make_coef(l, m, SPIN, l0);
+            coef[buf][threadIdx.x] = make_coef(l, m, sv, l0);
 #pragma unroll
             for (int a = 0; a < NA; ++a) {
                 T re = 0, im = 0;
@@ -413,8 +430,8 @@ __global__ void __launch_bounds__(kThreads) k_legendre_syn(
         }
     }
 
-    if ((l0 + m) & 1) {
-        // the even rows of the blocks had odd l + m: swap the halves into parity order
+    if ((l0 + m + sv) & 1) {
+        // the even rows of the blocks had odd l + m + s: swap the halves into parity order
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             if (SPIN == 0) {
@@ -480,10 +497,10 @@ __global__ void __launch_bounds__(kThreads) k_legendre_syn(
 
 using namespace gm;
 
-extern "C" int64_t gm_seed_table_len(int64_t L) { return 3 * 4 * L; }
+extern "C" int64_t gm_seed_table_len(int64_t L) { return (2 * kMaxSpin + 1) * 4 * L; }
 
 template <typename T, int SPIN, int NC, int R>
-static int launch_ana(int64_t nside, int64_t lmax, int64_t ncomp, const double *geom,
+static int launch_ana(int spin, int64_t nside, int64_t lmax, int64_t ncomp, const double *geom,
                       const double *seeds, const void *rhs, double *alm, double scale,
                       cudaStream_t s)
 {
@@ -491,19 +508,19 @@ static int launch_ana(int64_t nside, int64_t lmax, int64_t ncomp, const double *
     dim3 grid((unsigned)((nlanes + kThreads * R - 1) / (kThreads * R)), (unsigned)(lmax + 1),
               (unsigned)((ncomp + NC - 1) / NC));
     k_legendre_ana<T, SPIN, NC, R><<<grid, kThreads, 0, s>>>(nside, lmax, ncomp, geom, seeds,
-                                                             (const T *)rhs, alm, scale);
+                                                             (const T *)rhs, alm, scale, spin);
     return check_launch("gm_legendre_analysis");
 }
 
 template <typename T, int SPIN, int NC, int R>
-static int launch_syn(int64_t nside, int64_t lmax, int64_t ncomp, const double *geom,
+static int launch_syn(int spin, int64_t nside, int64_t lmax, int64_t ncomp, const double *geom,
                       const double *seeds, const double *alm, void *syn, cudaStream_t s)
 {
     const int64_t nlanes = 2 * nside;
     dim3 grid((unsigned)((nlanes + kThreads * R - 1) / (kThreads * R)), (unsigned)(lmax + 1),
               (unsigned)((ncomp + NC - 1) / NC));
     k_legendre_syn<T, SPIN, NC, R><<<grid, kThreads, 0, s>>>(nside, lmax, ncomp, geom, seeds, alm,
-                                                             (T *)syn);
+                                                             (T *)syn, spin);
     return check_launch("gm_legendre_synthesis");
 }
 
@@ -514,12 +531,12 @@ static int dispatch_ana(int spin, int64_t nside, int64_t lmax, int64_t ncomp, co
 {
     if (spin == 0) {
         if (ncomp == 1)
-            return launch_ana<T, 0, 1, 4>(nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s);
+            return launch_ana<T, 0, 1, 4>(spin, nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s);
         if (ncomp == 2)
-            return launch_ana<T, 0, 2, 4>(nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s);
-        return launch_ana<T, 0, 4, 2>(nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s);
+            return launch_ana<T, 0, 2, 4>(spin, nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s);
+        return launch_ana<T, 0, 4, 2>(spin, nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s);
     }
-    return launch_ana<T, 2, 2, 2>(nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s);
+    return launch_ana<T, 2, 2, 2>(spin, nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s);
 }
 
 template <typename T>
@@ -527,11 +544,11 @@ static int dispatch_syn(int spin, int64_t nside, int64_t lmax, int64_t ncomp, co
                         const double *seeds, const double *alm, void *syn, cudaStream_t s)
 {
     if (spin == 0) {
-        if (ncomp == 1) return launch_syn<T, 0, 1, 2>(nside, lmax, ncomp, geom, seeds, alm, syn, s);
-        if (ncomp == 2) return launch_syn<T, 0, 2, 2>(nside, lmax, ncomp, geom, seeds, alm, syn, s);
-        return launch_syn<T, 0, 4, 1>(nside, lmax, ncomp, geom, seeds, alm, syn, s);
+        if (ncomp == 1) return launch_syn<T, 0, 1, 2>(spin, nside, lmax, ncomp, geom, seeds, alm, syn, s);
+        if (ncomp == 2) return launch_syn<T, 0, 2, 2>(spin, nside, lmax, ncomp, geom, seeds, alm, syn, s);
+        return launch_syn<T, 0, 4, 1>(spin, nside, lmax, ncomp, geom, seeds, alm, syn, s);
     }
-    return launch_syn<T, 2, 2, 2>(nside, lmax, ncomp, geom, seeds, alm, syn, s);
+    return launch_syn<T, 2, 2, 2>(spin, nside, lmax, ncomp, geom, seeds, alm, syn, s);
 }
 
 // Tile shapes the autotuner chooses from: (NC, R) = (components per CTA, lanes per thread).
@@ -547,7 +564,7 @@ static int tile_ana(int spin, int tile, int64_t nside, int64_t lmax, int64_t nco
                     const double *geom, const double *seeds, const void *rhs, double *alm,
                     double scale, cudaStream_t s)
 {
-#define GM_ANA(SP, NC, R) return launch_ana<T, SP, NC, R>(nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s)
+#define GM_ANA(SP, NC, R) return launch_ana<T, SP, NC, R>(spin, nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s)
     if (spin == 0) {
         switch (tile) {
         case 0: GM_ANA(0, 1, 1);
@@ -576,7 +593,7 @@ static int tile_syn(int spin, int tile, int64_t nside, int64_t lmax, int64_t nco
                     const double *geom, const double *seeds, const double *alm, void *syn,
                     cudaStream_t s)
 {
-#define GM_SYN(SP, NC, R) return launch_syn<T, SP, NC, R>(nside, lmax, ncomp, geom, seeds, alm, syn, s)
+#define GM_SYN(SP, NC, R) return launch_syn<T, SP, NC, R>(spin, nside, lmax, ncomp, geom, seeds, alm, syn, s)
     if (spin == 0) {
         switch (tile) {
         case 0: GM_SYN(0, 1, 1);
@@ -602,7 +619,7 @@ static int tile_syn(int spin, int tile, int64_t nside, int64_t lmax, int64_t nco
 
 extern "C" int gm_legendre_tiles(int spin, int32_t *nc_r, int capacity)
 {
-    if (spin != 0 && spin != 2) return -1;
+    if (spin < 0 || spin > kMaxSpin) return -1;
     const int n = spin == 0 ? kNTiles0 : kNTiles2;
     for (int i = 0; i < n && i < capacity; ++i) {
         nc_r[2 * i] = spin == 0 ? kTiles0[i][0] : kTiles2[i][0];
@@ -618,8 +635,8 @@ extern "C" int gm_legendre_analysis_tile(int precision, int spin, int64_t nside,
 {
     if (nside < 1 || lmax < 0 || lmax + 1 > 65535 || ncomp < 1 || ncomp > 65535)
         return GM_ERR_BAD_SHAPE;
-    if (spin != 0 && spin != 2) return GM_ERR_UNSUPPORTED;
-    if (spin == 2 && (ncomp % 2)) return GM_ERR_BAD_SHAPE;
+    if (spin < 0 || spin > kMaxSpin) return GM_ERR_UNSUPPORTED;
+    if (spin != 0 && (ncomp % 2)) return GM_ERR_BAD_SHAPE;
     if (tile < -1 || tile >= (spin == 0 ? kNTiles0 : kNTiles2)) return GM_ERR_BAD_SHAPE;
     if (!lane_geom || !seeds || !rhs || !alm) return GM_ERR_BAD_PTR;
     cudaStream_t s = as_stream(stream);
@@ -638,8 +655,8 @@ extern "C" int gm_legendre_synthesis_tile(int precision, int spin, int64_t nside
 {
     if (nside < 1 || lmax < 0 || lmax + 1 > 65535 || ncomp < 1 || ncomp > 65535)
         return GM_ERR_BAD_SHAPE;
-    if (spin != 0 && spin != 2) return GM_ERR_UNSUPPORTED;
-    if (spin == 2 && (ncomp % 2)) return GM_ERR_BAD_SHAPE;
+    if (spin < 0 || spin > kMaxSpin) return GM_ERR_UNSUPPORTED;
+    if (spin != 0 && (ncomp % 2)) return GM_ERR_BAD_SHAPE;
     if (tile < -1 || tile >= (spin == 0 ? kNTiles0 : kNTiles2)) return GM_ERR_BAD_SHAPE;
     if (!lane_geom || !seeds || !alm || !syn) return GM_ERR_BAD_PTR;
     cudaStream_t s = as_stream(stream);
@@ -658,8 +675,8 @@ extern "C" int gm_legendre_analysis(int precision, int spin, int64_t nside, int6
 {
     if (nside < 1 || lmax < 0 || lmax + 1 > 65535 || ncomp < 1 || ncomp > 65535)
         return GM_ERR_BAD_SHAPE;
-    if (spin != 0 && spin != 2) return GM_ERR_UNSUPPORTED;
-    if (spin == 2 && (ncomp % 2)) return GM_ERR_BAD_SHAPE;
+    if (spin < 0 || spin > kMaxSpin) return GM_ERR_UNSUPPORTED;
+    if (spin != 0 && (ncomp % 2)) return GM_ERR_BAD_SHAPE;
     if (!lane_geom || !seeds || !rhs || !alm) return GM_ERR_BAD_PTR;
     cudaStream_t s = as_stream(stream);
     if (precision == GM_FP64)
@@ -675,8 +692,8 @@ extern "C" int gm_legendre_synthesis(int precision, int spin, int64_t nside, int
 {
     if (nside < 1 || lmax < 0 || lmax + 1 > 65535 || ncomp < 1 || ncomp > 65535)
         return GM_ERR_BAD_SHAPE;
-    if (spin != 0 && spin != 2) return GM_ERR_UNSUPPORTED;
-    if (spin == 2 && (ncomp % 2)) return GM_ERR_BAD_SHAPE;
+    if (spin < 0 || spin > kMaxSpin) return GM_ERR_UNSUPPORTED;
+    if (spin != 0 && (ncomp % 2)) return GM_ERR_BAD_SHAPE;
     if (!lane_geom || !seeds || !alm || !syn) return GM_ERR_BAD_PTR;
     cudaStream_t s = as_stream(stream);
     if (precision == GM_FP64)

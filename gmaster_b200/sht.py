@@ -107,10 +107,17 @@ def _log2_int(n):
     return shift + math.log2(n >> shift)
 
 
-def seed_table(L):
-    """Seeds of the Wigner-d rows: (3 variants, L orders, 4) float64.
+MAX_SPIN = 8   # spins 1..MAX_SPIN run through the polarised SIMT kernels
 
-    Variant 0 is spin 0 (s' = 0), 1 is s' = -2 (the sY_{+2} rows), 2 is s' = +2.  Entry
+
+def seed_table(L, max_spin=MAX_SPIN):
+    """Seeds of the Wigner-d rows: (2 max_spin + 1 variants, L orders, 4) float64.
+
+    Variant 0 is spin 0 (s' = 0); spin s >= 1 has the pair of variants from
+    `seed_variant(s)`: first s' = -s (the sY_{+s} rows), then s' = +s multiplied by (-1)^s
+    (the sign the E/B combination of the minus-m part carries, healpix.py:800-814, folded
+    into the row).  Spin 2 keeps variants 1 and 2, spin 1 takes 3 and 4, spin s >= 3 takes
+    2s - 1 and 2s.  Entry
     ``[log2 N, sign, pc, ps]`` gives the first row l0 = max(m, |s'|) as
     ``sign * 2^(log2 N + pc log2 cos(theta/2) + ps log2 sin(theta/2))`` with
     ``N = sqrt((2 l0 + 1)/4pi) sqrt(binomial)`` from the closed forms
@@ -119,7 +126,7 @@ def seed_table(L):
     d^s_{m,-s} = (-1)^(m+s) sqrt(C(2s, s-m)) cos^(s-m) sin^(s+m) (m < s); the binomials
     are exact integers, so log2 N is accurate to the last bit.
     """
-    out = np.zeros((3, L, 4))
+    out = np.zeros((2 * max_spin + 1, L, 4))
     c = 1  # C(2m, m)
     for m in range(L):
         if m > 0:
@@ -127,17 +134,31 @@ def seed_table(L):
         lc = _log2_int(c)
         sign = -1.0 if (m & 1) else 1.0
         out[0, m] = [0.5 * lc + 0.5 * math.log2((2 * m + 1) / (4 * math.pi)), sign, m, m]
-        if m >= 2:
-            # C(2m, m -+ 2) = C(2m, m) m (m-1) / ((m+1)(m+2))
-            lc2 = lc + math.log2(m * (m - 1)) - math.log2((m + 1) * (m + 2))
-            norm = 0.5 * lc2 + 0.5 * math.log2((2 * m + 1) / (4 * math.pi))
-            out[1, m] = [norm, sign, m - 2, m + 2]
-            out[2, m] = [norm, sign, m + 2, m - 2]
-        else:
-            base = 0.5 * math.log2(5 / (4 * math.pi))
-            out[1, m] = [base + 0.5 * math.log2(math.comb(4, 2 - m)), sign, 2 - m, 2 + m]
-            out[2, m] = [base + 0.5 * math.log2(math.comb(4, 2 + m)), 1.0, 2 + m, 2 - m]
+        for sp in range(1, max_spin + 1):
+            flip = -1.0 if (sp & 1) else 1.0   # (-1)^s on the +s variant
+            if m >= sp:
+                # C(2m, m -+ s) = C(2m, m) prod_k (m - k) / (m + 1 + k), k < s
+                num = math.prod(m - k for k in range(sp))
+                den = math.prod(m + 1 + k for k in range(sp))
+                lc2 = lc + math.log2(num) - math.log2(den)
+                norm = 0.5 * lc2 + 0.5 * math.log2((2 * m + 1) / (4 * math.pi))
+                sg = -sign if (sp & 1) else sign   # (-1)^(m + s)
+                vm = seed_variant(sp)
+                out[vm, m] = [norm, sg, m - sp, m + sp]
+                out[vm + 1, m] = [norm, sg * flip, m + sp, m - sp]
+            else:
+                vm = seed_variant(sp)
+                base = 0.5 * math.log2((2 * sp + 1) / (4 * math.pi))
+                sg = -1.0 if ((m + sp) & 1) else 1.0
+                out[vm, m] = [base + 0.5 * math.log2(math.comb(2 * sp, sp - m)), sg, sp - m, sp + m]
+                out[vm + 1, m] = [base + 0.5 * math.log2(math.comb(2 * sp, sp + m)), flip,
+                                  sp + m, sp - m]
     return out
+
+
+def seed_variant(spin):
+    """First of the two seed variants of spin >= 1 (s' = -s, then s' = +s)."""
+    return 1 if spin == 2 else (3 if spin == 1 else 2 * spin - 1)
 
 
 class Plan:
@@ -295,10 +316,10 @@ def map2alm_device(maps, spin, nside, lmax, n_iter, precision="mixed"):
     prec = _prec(precision)
     plan = get_plan(nside, lmax, maps.device)
     ncomp = maps.shape[0]
-    if spin not in (0, 2):
-        raise NotImplementedError("only spin 0 and spin 2 transforms are implemented")
-    if spin == 2 and ncomp % 2:
-        raise ValueError("spin-2 transforms take (Q, U) pairs")
+    if spin < 0 or spin > MAX_SPIN:
+        raise NotImplementedError(f"transforms are implemented for spins 0..{MAX_SPIN}")
+    if spin != 0 and ncomp % 2:
+        raise ValueError("spin transforms take (Q, U) pairs")
     spec = ring_analysis(plan, maps, prec)
     rhs_map = pack_rhs(plan, spec, prec)
     del spec
@@ -320,7 +341,9 @@ def alm2map_device(alm, spin, nside, lmax, precision="mixed"):
     plan = get_plan(nside, lmax, alm.device)
     alm = alm.contiguous()
     ncomp = alm.shape[0]
-    if spin == 2 and ncomp % 2:
-        raise ValueError("spin-2 synthesis takes (E, B) pairs")
+    if spin < 0 or spin > MAX_SPIN:
+        raise NotImplementedError(f"transforms are implemented for spins 0..{MAX_SPIN}")
+    if spin != 0 and ncomp % 2:
+        raise ValueError("spin synthesis takes (E, B) pairs")
     syn = legendre_synthesis(plan, spin, alm, ncomp, prec)
     return ring_synthesis(plan, syn, prec)

@@ -117,14 +117,17 @@ int gm_ring_synthesis_ws(int precision, int64_t nside, int64_t L, int64_t ncomp,
 
 /* ----------------------------------------------------------- Legendre stage */
 
-/* Per-order seed table length (doubles) for spin s: 3 variants x 4 x L. */
+/* Seed table length (doubles): 17 variants x L orders x 4.  Variant 0 is spin 0; spin
+ * s in 1..8 has two consecutive variants (s' = -s, then s' = +s times (-1)^s) starting at
+ * 1 for spin 2, 3 for spin 1 and 2s - 1 for s >= 3 (gmaster_b200/sht.py:seed_table). */
 int64_t gm_seed_table_len(int64_t L);
 
 /* Spherical-harmonic analysis, latitudinal step (replaces march_v2.cu:155-285
  * `march_analysis` via march_v2.py:666-693 and 817-872):
  *   alm[f][idx(l,m)] += scale * sum_lanes lambda_lm(theta_j) rhs(...)
- * spin 0: ncomp maps -> nalm = ncomp rows; spin 2: ncomp = 2 nfields ->
- * nalm = 2 nfields rows (E, B per field).
+ * spin 0: ncomp maps -> nalm = ncomp rows; spin s in 1..8: ncomp = 2 nfields ->
+ * nalm = 2 nfields rows (E, B per field, healpix.py:800-814); other spins return
+ * GM_ERR_UNSUPPORTED.
  * lane_geom: (3, nlanes) float64 [cos theta, log2 sin(theta/2), log2 cos(theta/2)].
  * seeds: gm_seed_table_len(L) doubles (see gmaster_b200/sht.py).
  * alm is accumulated with double-precision atomics: zero it first for a fresh analysis. */

@@ -440,7 +440,8 @@ static void ana2(int64_t nside, int64_t lmax, const double *theta, const double 
 
 /* Spin-2 synthesis: (E, B) -> (Q, U), with a2_lm = -(E + iB) for m >= 0 and
  * a2_{l,-m} = -(-1)^m (E* + i B*) (healpix.py:599-611). */
-static void syn2(int64_t nside, int64_t lmax, const double *theta, const double *phi0, const double *eb, double *qu)
+static void syns(int64_t nside, int64_t lmax, int64_t spin, const double *theta, const double *phi0,
+                 const double *eb, double *qu)
 {
     int64_t nring = 4 * nside - 1, L = lmax + 1, npix = 12 * nside * nside;
     int64_t nelem = L * (L + 1) / 2;
@@ -452,7 +453,7 @@ static void syn2(int64_t nside, int64_t lmax, const double *theta, const double 
         double *lam = malloc(sizeof(double) * L);
         for (int64_t mm = -lmax; mm <= lmax; ++mm) {
             int64_t m = mm < 0 ? -mm : mm;
-            orc_lambda_row(lmax, mm, -2, theta[r], lam);
+            orc_lambda_row(lmax, mm, -spin, theta[r], lam);
             double sr = 0.0, si = 0.0;
             for (int64_t l = m; l <= lmax; ++l) {
                 int64_t i = alm_index(lmax, l, m);
@@ -479,31 +480,96 @@ static void syn2(int64_t nside, int64_t lmax, const double *theta, const double 
     free(mapc); free(C); 
 }
 
+/* Spin-s analysis (s >= 1) in the reference's literal form (healpix.py:800-814): with
+ * plus(l, m) = sum over rings of w lambda_{l,m,-s} F(m), F the ring FFT of Q + iU for every
+ * order -L < m < L, minus(l, m) = (-1)^m conj(plus(l, -m)), E = -(plus + minus)/2 and
+ * B = i (plus - minus)/2. */
+static void anas(int64_t nside, int64_t lmax, int64_t spin, const double *theta, const double *phi0,
+                 const double *qu, double *eb)
+{
+    int64_t nring = 4 * nside - 1, L = lmax + 1, npix = 12 * nside * nside;
+    double w = 4.0 * M_PI / (double)npix;
+    int64_t nelem = L * (L + 1) / 2;
+    double *mapc = malloc(sizeof(double) * 2 * npix);
+    for (int64_t p = 0; p < npix; ++p) { mapc[2 * p] = qu[p]; mapc[2 * p + 1] = qu[npix + p]; }
+    int64_t width = 2 * L - 1;
+    double *F = malloc(sizeof(double) * 2 * nring * width);
+    orc_ring_analysis(nside, L, L - 1, phi0, mapc, F);
+#pragma omp parallel for schedule(dynamic)
+    for (int64_t m = 0; m <= lmax; ++m) {
+        double *lp = malloc(sizeof(double) * L), *ln = malloc(sizeof(double) * L);
+        double *pp = calloc(2 * L, sizeof(double)), *pn = calloc(2 * L, sizeof(double));
+        for (int64_t r = 0; r < nring; ++r) {
+            orc_lambda_row(lmax, m, -spin, theta[r], lp);
+            orc_lambda_row(lmax, -m, -spin, theta[r], ln);
+            double fr = w * F[2 * (r * width + (L - 1) + m)], fi = w * F[2 * (r * width + (L - 1) + m) + 1];
+            double gr = w * F[2 * (r * width + (L - 1) - m)], gi = w * F[2 * (r * width + (L - 1) - m) + 1];
+            for (int64_t l = m; l <= lmax; ++l) {
+                pp[2 * l] += lp[l] * fr; pp[2 * l + 1] += lp[l] * fi;
+                pn[2 * l] += ln[l] * gr; pn[2 * l + 1] += ln[l] * gi;
+            }
+        }
+        double sg = (m & 1) ? -1.0 : 1.0;
+        for (int64_t l = m; l <= lmax; ++l) {
+            int64_t i = alm_index(lmax, l, m);
+            double qr = sg * pn[2 * l], qi = -sg * pn[2 * l + 1];   /* minus = (-1)^m conj(plus(-m)) */
+            eb[2 * i] = -(pp[2 * l] + qr) / 2;
+            eb[2 * i + 1] = -(pp[2 * l + 1] + qi) / 2;
+            eb[2 * (nelem + i)] = -(pp[2 * l + 1] - qi) / 2;
+            eb[2 * (nelem + i) + 1] = (pp[2 * l] - qr) / 2;
+        }
+        free(lp); free(ln); free(pp); free(pn);
+    }
+    free(mapc); free(F);
+}
+
 void orc_alm2map(int64_t nside, int64_t lmax, int64_t spin, const double *theta,
                  const double *phi0, const double *alm, double *map)
 {
     if (spin == 0) syn0(nside, lmax, theta, phi0, alm, map);
-    else syn2(nside, lmax, theta, phi0, alm, map);
+    else syns(nside, lmax, spin, theta, phi0, alm, map);
+}
+
+/* One analysis pass: spin 0, the spin-2 form pinned against the golden vectors, or the
+ * literal spin-s form (`general` forces it for spin 2 too). */
+static void ana_any(int64_t nside, int64_t lmax, int64_t spin, int general, const double *theta,
+                    const double *phi0, const double *map, double *alm)
+{
+    if (spin == 0) ana0(nside, lmax, theta, phi0, map, alm);
+    else if (spin == 2 && !general) ana2(nside, lmax, theta, phi0, map, alm);
+    else anas(nside, lmax, spin, theta, phi0, map, alm);
 }
 
 /* map2alm with n_iter Jacobi refinement (healpix.py:1059-1068). */
-void orc_map2alm(int64_t nside, int64_t lmax, int64_t spin, int64_t n_iter,
-                 const double *theta, const double *phi0, const double *map, double *alm)
+static void map2alm_iter(int64_t nside, int64_t lmax, int64_t spin, int64_t n_iter, int general,
+                         const double *theta, const double *phi0, const double *map, double *alm)
 {
     int64_t npix = 12 * nside * nside, L = lmax + 1, nelem = L * (L + 1) / 2;
     int64_t nmaps = spin == 0 ? 1 : 2;
-    if (spin == 0) ana0(nside, lmax, theta, phi0, map, alm);
-    else ana2(nside, lmax, theta, phi0, map, alm);
+    ana_any(nside, lmax, spin, general, theta, phi0, map, alm);
     double *res = malloc(sizeof(double) * nmaps * npix);
     double *delta = malloc(sizeof(double) * 2 * nmaps * nelem);
     for (int64_t it = 0; it < n_iter; ++it) {
         orc_alm2map(nside, lmax, spin, theta, phi0, alm, res);
         for (int64_t p = 0; p < nmaps * npix; ++p) res[p] -= map[p];
-        if (spin == 0) ana0(nside, lmax, theta, phi0, res, delta);
-        else ana2(nside, lmax, theta, phi0, res, delta);
+        ana_any(nside, lmax, spin, general, theta, phi0, res, delta);
         for (int64_t i = 0; i < 2 * nmaps * nelem; ++i) alm[i] -= delta[i];
     }
     free(res); free(delta);
+}
+
+void orc_map2alm(int64_t nside, int64_t lmax, int64_t spin, int64_t n_iter,
+                 const double *theta, const double *phi0, const double *map, double *alm)
+{
+    map2alm_iter(nside, lmax, spin, n_iter, 0, theta, phi0, map, alm);
+}
+
+/* As orc_map2alm, with the literal spin-s analysis for every spin >= 1 (checks it against
+ * the spin-2 form). */
+void orc_map2alm_general(int64_t nside, int64_t lmax, int64_t spin, int64_t n_iter,
+                         const double *theta, const double *phi0, const double *map, double *alm)
+{
+    map2alm_iter(nside, lmax, spin, n_iter, 1, theta, phi0, map, alm);
 }
 
 /* Analysis restricted to a set of orders (bounded CPU-baseline sample): spin 0,

@@ -53,15 +53,20 @@ def test_seed_table_reproduces_first_row(m):
     """sign * 2^(log2N + pc log2 cos + ps log2 sin) is lambda_{l0,m} of the oracle."""
     L = 200
     seeds = sht.seed_table(L)
-    for var, sp in ((0, 0), (1, -2), (2, 2)):
+    rows = [(0, 0, 1.0)]
+    for spin in range(1, sht.MAX_SPIN + 1):
+        v = sht.seed_variant(spin)
+        # the +s variant carries (-1)^s
+        rows += [(v, -spin, 1.0), (v + 1, spin, -1.0 if spin & 1 else 1.0)]
+    for var, sp, extra in rows:
         l0 = max(m, abs(sp))
         for th in (0.3, 1.1, np.pi / 2):
             lg, sign, pc, ps = seeds[var, m]
             f = lg + pc * math.log2(math.cos(th / 2)) + ps * math.log2(math.sin(th / 2))
             val = sign * 2.0 ** f
-            want = oracle.lambda_row(L - 1, m, sp, th)[l0]
+            want = extra * oracle.lambda_row(L - 1, m, sp, th)[l0]
             if abs(want) > 1e-250:
-                assert abs(val - want) <= 1e-12 * abs(want)
+                assert abs(val - want) <= 1e-12 * abs(want), (var, sp, th)
 
 
 def test_nmtbin_linear_matches_reference_bands():
@@ -145,8 +150,9 @@ def test_legendre_tile_list():
     assert (1, 1) in t0 and len(t0) == len(set(t0))
     assert all(32 % (2 * nc) == 0 for nc, _ in t0)
     assert all(nc == 2 for nc, _ in t2)
+    assert autotune.tiles(1) == t2 and autotune.tiles(sht.MAX_SPIN) == t2   # polarised kernels
     with pytest.raises(ValueError):
-        autotune.tiles(1)
+        autotune.tiles(sht.MAX_SPIN + 1)
     import os
 
     assert autotune.autotune_enabled() == (os.environ.get("GMASTER_B200_AUTOTUNE", "1") != "0")
@@ -276,3 +282,15 @@ def test_covariance_term_table_matches_oracle_assembly(spins):
     xis = [{k: (None if v is None else v.numpy()) for k, v in d.items()} for d in cw.xiSS]
     want = oracle.nka_assemble(spins, xis, *cls, L).reshape(cw.nclsa * cw.nclsb, L, L)
     np.testing.assert_allclose(got, want, rtol=0, atol=1e-12)
+
+
+def test_oracle_general_spin_form_equals_pinned_spin2():
+    """The oracle's literal spin-s analysis (plus at +-m, healpix.py:800-814) reproduces its
+    spin-2 form, which the golden vectors pin, so the spin-1 and spin-3 checks rest on it."""
+    rng = np.random.default_rng(5)
+    nside, lmax = 8, 23
+    qu = rng.normal(size=(2, 12 * nside ** 2))
+    for n_iter in (0, 2):
+        a = oracle.map2alm(qu, 2, nside, lmax, n_iter)
+        b = oracle.map2alm(qu, 2, nside, lmax, n_iter, general=True)
+        assert np.max(np.abs(a - b)) <= 1e-13 * np.max(np.abs(a))
