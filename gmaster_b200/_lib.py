@@ -93,6 +93,10 @@ SIGNATURES = {
     "gm_cov_binned": ([_c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_i64, _c_vp, _c_vp, _c_vp,
                        _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
     "gm_cov_coupled": ([_c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
+    "gm_gl_nodes": ([_c_i64, _c_vp, _c_vp, _c_vp], _c_int),
+    "gm_wigner_table": ([_c_i64, _c_vp, _c_i64, _c_int, _c_int, _c_vp, _c_vp, _c_vp], _c_int),
+    "gm_wigner_corr": ([_c_i64, _c_vp, _c_i64, _c_int, _c_int, _c_vp, _c_i64, _c_vp, _c_vp, _c_vp],
+                       _c_int),
     "gm_mask_apodize": ([_c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_dbl, _c_int, _c_vp, _c_vp],
                         _c_int),
 }

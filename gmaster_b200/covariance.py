@@ -234,7 +234,7 @@ class NmtCovarianceWorkspace:
         na, nb, nc, nd = self.nmaps
         if wa.ncls != na * nb or wb.ncls != nc * nd:
             raise ValueError("Field spins do not match input workspaces")
-        dev = wa.mcm_blocks.device if wa.mcm_blocks is not None else torch.device("cuda")
+        dev = wa.mcm_binned.device if wa.mcm_binned is not None else torch.device("cuda")
         cls = [as_device(c, torch.float64, dev) for c in (cla1b1, cla1b2, cla2b1, cla2b2)]
         expected = (na * nc, na * nd, nb * nc, nb * nd)
         if any(c.ndim != 2 or c.shape[0] != n for c, n in zip(cls, expected)):

@@ -1,9 +1,9 @@
 """Curved-sky fields (`NmtField`), the counterpart of gmaster/field.py:20-499.
 
 Supported: HEALPix spin-0 and spin-2 fields with a beam, ``n_iter`` / ``n_iter_mask``,
-``lmax`` / ``lmax_mask``, ``masked_on_input`` and ``lite``.  Contaminant templates,
-purification and anisotropic masks are outside this build and raise
-``NotImplementedError``.
+``lmax`` / ``lmax_mask``, ``masked_on_input``, ``lite`` and E/B purification
+(``purify_e`` / ``purify_b``, `pure.purify_alms`).  Contaminant templates and anisotropic
+masks are outside this build and raise ``NotImplementedError``.
 """
 
 import weakref
@@ -59,15 +59,13 @@ class NmtField:
                  mask_12=None, precision=None):
         if templates is not None:
             raise NotImplementedError("contaminant deprojection is not part of this build")
-        if purify_e or purify_b:
-            raise NotImplementedError("E/B purification is not part of this build")
         if mask_22 is not None or mask_12 is not None:
             raise NotImplementedError("anisotropic masks are not part of this build")
         self.lite = bool(lite)
         self.precision = precision or get_precision()
         self.n_iter = nmt_params.n_iter_default if n_iter is None else int(n_iter)
         self.n_iter_mask = nmt_params.n_iter_mask_default if n_iter_mask is None else int(n_iter_mask)
-        self.pure_e = self.pure_b = False
+        self.pure_e, self.pure_b = bool(purify_e), bool(purify_b)
         self.is_catalog = False
         self.anisotropic_mask = False
         self.alm = self.alm_mask = self.maps = self.temp = None
@@ -115,8 +113,30 @@ class NmtField:
             raise NotImplementedError("only spin-0 and spin-2 fields are implemented")
         self.spin = int(spin)
         self.nmaps = 1 if self.spin == 0 else 2
+        pure_any = self.pure_e or self.pure_b
+        if pure_any and self.spin != 2:
+            raise ValueError("Purification only implemented for spin-2 fields")
+        if pure_any and self.ainfo != self.ainfo_mask:
+            raise ValueError("Pure fields require lmax == lmax_mask")
+        maps_unmasked = None
+        if pure_any:
+            # field.py:196-206: the purification needs the maps before masking
+            maps_unmasked = maps_t
+            if masked_on_input:
+                good = self.mask > 0
+                den = torch.where(good, self.mask, torch.ones_like(self.mask))
+                maps_unmasked = torch.where(good[None, :], maps_t / den[None, :], maps_t)
         if not masked_on_input:
             maps_t = maps_t * self.mask[None, :]
+        if pure_any:
+            from .pure import purify_alms
+
+            self.alm = purify_alms(self, self.get_mask_alms(), maps_unmasked,
+                                   (self.pure_e, self.pure_b))
+            if not self.lite:
+                self.maps = sht.alm2map_device(self.alm, 2, self.minfo.nside, self.ainfo.lmax,
+                                               self.precision)
+            return
         nside = self.minfo.nside
         cached = _cached_mask_alms(self)
         if cached is not None and not self.lite:

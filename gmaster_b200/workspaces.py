@@ -158,6 +158,26 @@ def _blocks_from_dense(dense, lmax, ncls, device):
     return torch.from_numpy(blocks).to(device)
 
 
+def _slot_blocks_from_dense(dense, lmax, ncls, device):
+    """A block per standard slot of a dense (ncls L)^2 coupling matrix (purified workspaces,
+    whose slots hold different blocks); raises if the matrix has entries off the slots."""
+    n = lmax + 1
+    d = np.asarray(dense, dtype=np.float64)
+    if d.shape != (ncls * n, ncls * n):
+        raise ValueError(f"coupling matrix of shape {d.shape}, expected {(ncls * n, ncls * n)}")
+    q = d.reshape(n, ncls, n, ncls)
+    rebuilt = np.zeros_like(q)
+    out = []
+    for _, r, c, sign in _slots(ncls):
+        blk = sign * q[:, r, :, c]
+        rebuilt[:, r, :, c] += sign * blk
+        out.append((torch.from_numpy(np.ascontiguousarray(blk)).to(device), r, c, sign))
+    if not np.array_equal(rebuilt.reshape(d.shape), d):
+        raise NotImplementedError("the coupling matrix is not that of a spin 0x2, 2x2 or joint "
+                                  "TEB workspace")
+    return out
+
+
 def _which(ncls):
     return {1: 1, 2: 2, 4: 12, 7: 15}[ncls]
 
@@ -236,6 +256,8 @@ class NmtWorkspace:
     def __init__(self, fl1=None, fl2=None, bins=None, is_teb=False, l_toeplitz=-1, l_exact=-1,
                  dl_band=-1, fname=None, normalization="MASTER"):
         self.mcm_blocks = self.mcm_binned = self._lu = None
+        self._slot_blocks = None
+        self.pure_e1 = self.pure_b1 = self.pure_e2 = self.pure_b2 = False
         if fname is not None:
             self.read_from(fname)
             return
@@ -257,14 +279,15 @@ class NmtWorkspace:
         """Write the workspace to a NaMaster-compatible FITS file (workspaces.py:2211-2255):
         the dense coupling matrix with the workspace keywords in the primary HDU, then the
         BEAMS, PCL_MASKS and BANDPOWERS tables.  An existing file is overwritten."""
-        if self.mcm_blocks is None:
+        if self._lu is None:
             raise RuntimeError("the workspace holds no coupling matrix")
         header = {
             "LMAX": self.lmax, "LMAX_MASK": self.lmax_mask, "IS_TEB": bool(getattr(self, "is_teb", False)),
             "NCLS": self.ncls,
             "NORM_TYPE": 0 if self.normalization == "MASTER" else 1, "WAWB": float(self.wawb),
             "SPIN1": self.spin1, "SPIN2": self.spin2, "ANISO1": False, "ANISO2": False,
-            "PURE_E1": False, "PURE_B1": False, "PURE_E2": False, "PURE_B2": False,
+            "PURE_E1": bool(self.pure_e1), "PURE_B1": bool(self.pure_b1),
+            "PURE_E2": bool(self.pure_e2), "PURE_B2": bool(self.pure_b2),
             "L_TOEPLITZ": self.l_toeplitz, "L_EXACT": self.l_exact, "DL_BAND": self.dl_band,
         }
         ell = np.arange(self.lmax + 1, dtype=np.int32)
@@ -286,9 +309,11 @@ class NmtWorkspace:
         hdus = {h["name"]: h for h in fits.read(fname)}
         prim = hdus.get("WSP_PRIMARY") or fits.read(fname)[0]
         h = prim["header"]
-        if any(bool(h.get(k, False)) for k in ("PURE_E1", "PURE_B1", "PURE_E2", "PURE_B2",
-                                               "ANISO1", "ANISO2")):
-            raise NotImplementedError("purified or anisotropic workspaces are not part of this build")
+        if any(bool(h.get(k, False)) for k in ("ANISO1", "ANISO2")):
+            raise NotImplementedError("anisotropic workspaces are not part of this build")
+        self.pure_e1, self.pure_b1 = bool(h.get("PURE_E1", False)), bool(h.get("PURE_B1", False))
+        self.pure_e2, self.pure_b2 = bool(h.get("PURE_E2", False)), bool(h.get("PURE_B2", False))
+        self._slot_blocks = None
         dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
         self.lmax = int(h["LMAX"])
         self.lmax_mask = int(h["LMAX_MASK"])
@@ -303,7 +328,12 @@ class NmtWorkspace:
         self.l_toeplitz = int(h.get("L_TOEPLITZ", -1))
         self.l_exact = int(h.get("L_EXACT", -1))
         self.dl_band = int(h.get("DL_BAND", -1))
-        self.mcm_blocks = _blocks_from_dense(prim["data"], self.lmax, self.ncls, dev)
+        if self.pure_e1 or self.pure_b1 or self.pure_e2 or self.pure_b2:
+            # purified channels take different blocks per slot: keep each slot's block
+            self.mcm_blocks = None
+            self._slot_blocks = _slot_blocks_from_dense(prim["data"], self.lmax, self.ncls, dev)
+        else:
+            self.mcm_blocks = _blocks_from_dense(prim["data"], self.lmax, self.ncls, dev)
         beams = hdus["BEAMS"]["data"]
         if "BEAMS" in beams:
             b1 = b2 = np.sqrt(beams["BEAMS"].astype(np.float64))
@@ -337,6 +367,11 @@ class NmtWorkspace:
             raise ValueError("If is_teb=True, fl1 must be spin-0 and fl2 non-zero spin")
         if is_teb and fl2.spin != 2:
             raise NotImplementedError("only spin 0 and spin 2 fields are implemented")
+        self.pure_e1, self.pure_b1 = bool(fl1.pure_e), bool(fl1.pure_b)
+        self.pure_e2, self.pure_b2 = bool(fl2.pure_e), bool(fl2.pure_b)
+        self._pure_any = self.pure_e1 or self.pure_b1 or self.pure_e2 or self.pure_b2
+        if self._pure_any and l_toeplitz > 0:
+            raise ValueError("Can't use Toeplitz approximation with purification.")
         toeplitz_sanity(l_toeplitz, l_exact, dl_band, fl1.ainfo.lmax)
         if normalization not in ("MASTER", "FKP"):
             raise ValueError(f"Unknown normalization type {normalization}. "
@@ -369,6 +404,10 @@ class NmtWorkspace:
         """Coupling blocks, or the exact ``blocks`` given (from a multi-workspace launch),
         then the Toeplitz fill when it is enabled."""
         l_toeplitz, l_exact, dl_band = self.l_toeplitz, self.l_exact, self.dl_band
+        self._slot_blocks = None
+        if getattr(self, "_pure_any", False):
+            self._compute_pure_blocks()
+            return
         if blocks is not None:
             self.mcm_blocks = blocks
         elif l_toeplitz > 0 and self.ncls == 1:
@@ -389,13 +428,65 @@ class NmtWorkspace:
                 self.mcm_blocks[x] = toeplitz_fill((self.mcm_blocks[x] / col).contiguous(),
                                                    self.lmax, l_toeplitz, l_exact, dl_band)
 
+    def _compute_pure_blocks(self):
+        """Blocks of a workspace with purified fields (workspaces.py:1782-1897): all spin-2
+        blocks from the Gauss-Legendre quadrature, each slot taking the standard block or
+        the one with one or two purified fields according to how many of its two channels
+        are purified."""
+        from .pure import coupling_blocks_pure
+
+        std_te, std_e, std_o, pure_te, e1, o1, e2, o2 = coupling_blocks_pure(self.window, self.lmax)
+        te_levels, even_levels, odd_levels = (std_te, pure_te), (std_e, e1, e2), (std_o, o1, o2)
+        slots = []
+        if self.ncls == 2:
+            pe, pb = int(self.pure_e1) + int(self.pure_e2), int(self.pure_b1) + int(self.pure_b2)
+            for index, level in enumerate((pe, pb)):
+                slots.append((te_levels[level], index, index, 1.0))
+        else:
+            offset = 3 if self.ncls == 7 else 0
+            if self.ncls == 7:
+                tt = coupling_blocks(self.window, self.lmax, 1)[_BLOCK_TT]
+                slots.append((tt, 0, 0, 1.0))
+                for index, level in enumerate((int(self.pure_e2), int(self.pure_b2))):
+                    slots.append((te_levels[level], 1 + index, 1 + index, 1.0))
+                pe1 = pe2 = int(self.pure_e2)
+                pb1 = pb2 = int(self.pure_b2)
+            else:
+                pe1, pb1 = int(self.pure_e1), int(self.pure_b1)
+                pe2, pb2 = int(self.pure_e2), int(self.pure_b2)
+            levels = (pe1 + pe2, pe1 + pb2, pb1 + pe2, pb1 + pb2)
+            for index, level in enumerate(levels):
+                slots.append((even_levels[level], offset + index, offset + index, 1.0))
+            for index, level in enumerate(levels):
+                slots.append((odd_levels[level], offset + index, offset + 3 - index,
+                              _MM_SIGNS[index]))
+        self._slot_blocks = [(b.contiguous(), r, c, sg) for b, r, c, sg in slots]
+        self.mcm_blocks = None
+
     def _postprocess(self):
-        dev = self.mcm_blocks.device
+        dev = (self.mcm_blocks if self.mcm_blocks is not None else self._slot_blocks[0][0]).device
         ops = self.bins.device_operators(dev)
         beam = (self.beam1 * self.beam2).contiguous()
         N = self.ncls * self.nbands
         if self.normalization == "FKP":
             self.mcm_binned = self.wawb * torch.eye(N, dtype=torch.float64, device=dev)
+        elif self._slot_blocks is not None:
+            # a block per slot: each distinct block binned once, then placed with its sign
+            nb = self.nbands
+            binned = {}
+            full = torch.zeros((nb, self.ncls, nb, self.ncls), dtype=torch.float64, device=dev)
+            for blk, r, c, sign in self._slot_blocks:
+                key = id(blk)
+                if key not in binned:
+                    scratch = torch.empty(2 * nb * nb, dtype=torch.float64, device=dev)
+                    out = torch.empty((nb, nb), dtype=torch.float64, device=dev)
+                    _lib.call("gm_bin_coupling_csr", self.lmax, nb, 1, _lib.ptr(blk),
+                              _lib.ptr(ops["ptr"]), _lib.ptr(ops["ells"]), _lib.ptr(ops["wfl"]),
+                              _lib.ptr(ops["inv_fl"]), _lib.ptr(beam), _lib.ptr(scratch),
+                              _lib.ptr(out), _lib.stream_handle(dev))
+                    binned[key] = out
+                full[:, r, :, c] += sign * binned[key]
+            self.mcm_binned = full.reshape(N, N)
         elif self.ncls == 7:
             # joint TEB: each distinct block binned on its own, then placed with its sign
             nb = self.nbands
@@ -424,6 +515,12 @@ class NmtWorkspace:
     def get_coupling_matrix(self):
         """Dense (ncls (lmax+1))^2 MCM in ``l * ncls + c`` order (workspaces.py:2005-2025)."""
         n = self.lmax + 1
+        if self._slot_blocks is not None:
+            dev = self._slot_blocks[0][0].device
+            out = torch.zeros((n, self.ncls, n, self.ncls), dtype=torch.float64, device=dev)
+            for blk, r, c, sign in self._slot_blocks:
+                out[:, r, :, c] += sign * blk
+            return out.reshape(self.ncls * n, self.ncls * n)
         b = self.mcm_blocks
         if self.ncls == 1:
             return b[_BLOCK_TT].clone()
@@ -479,7 +576,7 @@ class NmtWorkspace:
     def get_bandpower_windows(self):
         """(ncls, nbands, ncls, lmax+1) windows W with <C_b> = sum W C_l (workspaces.py:2149-2160)."""
         n = self.lmax + 1
-        ops = self.bins.device_operators(self.mcm_blocks.device)
+        ops = self.bins.device_operators(self.mcm_binned.device)
         M = self.get_coupling_matrix() * (self.beam1 * self.beam2).repeat_interleave(self.ncls)[None]
         B = torch.zeros((self.nbands, n), dtype=torch.float64, device=M.device)
         ells = torch.from_numpy(self.bins._ells_np.astype(np.int64)).to(M.device)

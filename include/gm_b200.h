@@ -387,6 +387,24 @@ int gm_cov_coupled(int64_t lmax, int64_t nblocks, const double *xi, const double
                    const int32_t *terms, const double *signs, const int32_t *block_ptr,
                    double *out, void *stream);
 
+/* ---------------------------------------------------------- purified coupling (quadrature) */
+
+/* Gauss-Legendre quadrature for the coupling blocks of purified E/B fields (replaces
+ * workspaces.py:593-605 `_gauss_legendre` and :608-679 `_wigner_d_table`, used by
+ * :927-1061 `_coupling_matrices_pure_quadrature`).
+ * gm_gl_nodes: the n nodes x (ascending) and weights w of the n-point rule on [-1, 1].
+ * gm_wigner_table: out (lmax + 1, nnodes) = d^l_mn(arccos x[i]) (zero for l < max(|m|,|n|));
+ * norm[k] = sqrt(k! (k+mu+nu)! / ((k+mu)! (k+nu)!)), mu = |m-n|, nu = |m+n|, for
+ * k <= lmax - max(|m|,|n|) (at least 2 entries).  |m|, |n| <= 16.
+ * gm_wigner_corr: out (nvec, nnodes) = sum_l d^l_mn(arccos x[i]) vec[v][l] for nvec <= 2
+ * vectors of lmax + 1 doubles (the rows are not stored). */
+int gm_gl_nodes(int64_t n, double *x, double *w, void *stream);
+int gm_wigner_table(int64_t nnodes, const double *x, int64_t lmax, int m, int n,
+                    const double *norm, double *out, void *stream);
+int gm_wigner_corr(int64_t nnodes, const double *x, int64_t lmax, int m, int n,
+                   const double *norm, int64_t nvec, const double *vec, double *out,
+                   void *stream);
+
 /* ---------------------------------------------------------- tensor-core check */
 
 /* One-CTA tcgen05 check: D[128 x N] (float32, row-major) = A[128 x K] * B[N x K]^T where

@@ -294,3 +294,34 @@ def test_oracle_general_spin_form_equals_pinned_spin2():
         a = oracle.map2alm(qu, 2, nside, lmax, n_iter)
         b = oracle.map2alm(qu, 2, nside, lmax, n_iter, general=True)
         assert np.max(np.abs(a - b)) <= 1e-13 * np.max(np.abs(a))
+
+
+def test_oracle_purification_quadrature_is_pinned():
+    """The oracle's restatement of the purified quadrature (gmaster/workspaces.py:608-679,
+    927-1061): its Wigner rows are the oracle's own rows transposed (d_mn = d_nm(-beta)),
+    its standard blocks equal the 3j blocks, and on the full sky (no mask derivatives)
+    every purified block equals its standard one."""
+    import oracle
+
+    beta = np.array([0.2, 1.3, 2.8])
+    ell = np.arange(31)
+    norm = np.sqrt((2 * ell + 1) / (4 * np.pi))
+    for m, n in ((0, 1), (1, 2), (0, 2), (2, 2), (0, -2), (-2, -2), (1, 1)):
+        got = oracle.wigner_d_table(beta, m, n, 30)
+        want = np.stack([oracle.lambda_row(30, n, m, b) for b in beta]) / norm[None]
+        np.testing.assert_allclose(got, want, rtol=0, atol=1e-13)
+    nside, lmax = 8, 23
+    vec = oracle.pix2vec(nside)
+    mask = (vec[:, 2] < 0.5) * (0.5 + 0.5 * vec[:, 0] ** 2)
+    am = oracle.map2alm(mask[None], 0, nside, lmax, 3)
+    window = oracle.pcl(am, am, lmax)[0]
+    b = oracle.coupling_blocks_pure(window, lmax)
+    te = oracle.coupling_blocks(window, lmax, 0, 2)["te"]
+    pm = oracle.coupling_blocks(window, lmax, 2, 2)
+    for got, want in ((b[0], te), (b[1], pm["pp"]), (b[2], pm["mm"])):
+        assert np.max(np.abs(got - want)) < 1e-13 * np.max(np.abs(want))
+    full = np.zeros(lmax + 1)
+    full[0] = 4 * np.pi
+    f = oracle.coupling_blocks_pure(full, lmax)
+    for p, q in ((3, 0), (4, 1), (6, 1), (5, 2), (7, 2)):
+        assert np.max(np.abs(f[p] - f[q])) < 1e-13
