@@ -56,17 +56,23 @@ def wigner_corr(x, lmax, m, n, vecs):
     return out
 
 
-def coupling_blocks_pure(window, lmax):
+# Wigner rows of one chunk of quadrature nodes stay below this many bytes (nine row tables
+# of (lmax + 1) x chunk doubles); the integrals accumulate over the chunks.
+PURE_TABLE_BYTES = 4 << 30
+
+
+def coupling_blocks_pure(window, lmax, table_bytes=None):
     """The eight (lmax+1)^2 spin-2 coupling blocks (standard TE, standard M+, standard M-,
     purified TE, M+ and M- with one purified field, M+ and M- with two) of a mask
     pseudo-spectrum `window` (zero-padded to 2 lmax + 1), following
-    workspaces.py:927-1061 step by step."""
+    workspaces.py:927-1061 step by step.  The quadrature nodes are processed in chunks
+    whose Wigner rows fit `table_bytes` (default `PURE_TABLE_BYTES`)."""
     dev = window.device
     L, L2 = lmax + 1, 2 * lmax + 1
     w2 = torch.zeros(L2, dtype=torch.float64, device=dev)
     nw = min(window.shape[0], L2)
     w2[:nw] = window[:nw]
-    x, wt = gl_nodes(L2, dev)
+    x_all, wt_all = gl_nodes(L2, dev)
     ell = torch.arange(L2, dtype=torch.float64, device=dev)
     first = torch.sqrt(ell * (ell + 1))
     second = torch.sqrt(torch.clamp((ell + 2) * (ell + 1) * ell * (ell - 1), min=0))
@@ -78,49 +84,58 @@ def coupling_blocks_pure(window, lmax):
                                                              min=1)), torch.zeros_like(row))
     coef = (2 * ell + 1) * w2 / (4 * np.pi)
     sign = 1.0 - 2.0 * (torch.arange(L2, device=dev) % 2).to(torch.float64)
-
-    def corr(m, n, factor=None):
-        c = coef if factor is None else coef * factor
-        return wigner_corr(x, L2 - 1, m, n, torch.stack([c, c * sign]))
-
-    c00, s00 = corr(0, 0)
-    c10, s10 = corr(1, 0, first)
-    c20, s20 = corr(2, 0, second)
-    c11, s11 = corr(1, 1, first ** 2)
-    c12, s12 = corr(1, 2, first * second)
-    c22, s22 = corr(2, 2, second ** 2)
-    c01 = corr(0, 1, first)[0]
-    c02 = corr(0, 2, second)[0]
-    d = {(m, n): wigner_table(x, lmax, m, n)
-         for m, n in ((0, 0), (0, 1), (0, 2), (1, 0), (1, 1), (1, 2), (2, 2))}
-    right_t = wigner_table(x, lmax, 0, -2)
-    right_s = wigner_table(x, lmax, -2, -2)
-    cols = (2 * row + 1)[None, :]
     rf, rs = row_first[:, None], row_second[:, None]
+    budget = PURE_TABLE_BYTES if table_bytes is None else int(table_bytes)
+    chunk = max(1, min(L2, budget // (9 * 8 * L)))
+    names = ("t", "std_t", "std", "std_s", "one", "one_s", "two", "two_s")
+    acc = {k: torch.zeros((L, L), dtype=torch.float64, device=dev) for k in names}
+    for a in range(0, L2, chunk):
+        x, wt = x_all[a:a + chunk].contiguous(), wt_all[a:a + chunk]
 
-    def integrate(left_t, right):
-        # sum_i left(x_i, l1) w_i right(x_i, l2) (2 l2 + 1) / 2, with (l, node) tables
-        return ((left_t * wt[None, :]) @ right.T) * cols / 2
+        def corr(m, n, factor=None):
+            c = coef if factor is None else coef * factor
+            return wigner_corr(x, L2 - 1, m, n, torch.stack([c, c * sign]))
 
+        c00, s00 = corr(0, 0)
+        c10, s10 = corr(1, 0, first)
+        c20, s20 = corr(2, 0, second)
+        c11, s11 = corr(1, 1, first ** 2)
+        c12, s12 = corr(1, 2, first * second)
+        c22, s22 = corr(2, 2, second ** 2)
+        c01 = corr(0, 1, first)[0]
+        c02 = corr(0, 2, second)[0]
+        d = {(m, n): wigner_table(x, lmax, m, n)
+             for m, n in ((0, 0), (0, 1), (0, 2), (1, 0), (1, 1), (1, 2), (2, 2))}
+        right_t = wigner_table(x, lmax, 0, -2)
+        right_s = wigner_table(x, lmax, -2, -2)
+
+        def add(key, left_t, right):
+            # sum over this chunk's nodes of left(x_i, l1) w_i right(x_i, l2)
+            acc[key] += (left_t * wt[None, :]) @ right.T
+
+        add("t", d[0, 2] * c00 + d[0, 1] * c01 * rf + d[0, 0] * c02 * rs, right_t)
+        add("std_t", d[0, 2] * c00, right_t)
+        add("std", d[2, 2] * c00, right_s)
+        add("std_s", d[2, 2] * s00, right_s)
+        add("one", d[2, 2] * c00 + d[1, 2] * c10 * rf + d[0, 2] * c20 * rs, right_s)
+        add("one_s", d[2, 2] * s00 + d[1, 2] * s10 * rf + d[0, 2] * s20 * rs, right_s)
+        add("two", d[2, 2] * c00 + 2 * d[1, 2] * c10 * rf + 2 * d[0, 2] * c20 * rs
+            + d[1, 1] * c11 * rf ** 2 + 2 * d[1, 0] * c12 * rf * rs + d[0, 0] * c22 * rs ** 2, right_s)
+        add("two_s", d[2, 2] * s00 + 2 * d[1, 2] * s10 * rf + 2 * d[0, 2] * s20 * rs
+            + d[1, 1] * s11 * rf ** 2 + 2 * d[1, 0] * s12 * rf * rs + d[0, 0] * s22 * rs ** 2, right_s)
+        del d, right_t, right_s
+    cols = (2 * row + 1)[None, :] / 2
     pair_sign = 1.0 - 2.0 * ((row[:, None] + row[None, :]) % 2)
 
-    def parity(left_t, signed_t):
-        total = integrate(left_t, right_s)
-        signed = integrate(signed_t, right_s) * pair_sign
+    def parity(total_key, signed_key):
+        total = acc[total_key] * cols
+        signed = acc[signed_key] * cols * pair_sign
         return (total + signed) / 2, (total - signed) / 2
 
-    temperature = integrate(d[0, 2] * c00 + d[0, 1] * c01 * rf + d[0, 0] * c02 * rs, right_t)
-    one = d[2, 2] * c00 + d[1, 2] * c10 * rf + d[0, 2] * c20 * rs
-    one_s = d[2, 2] * s00 + d[1, 2] * s10 * rf + d[0, 2] * s20 * rs
-    two = (d[2, 2] * c00 + 2 * d[1, 2] * c10 * rf + 2 * d[0, 2] * c20 * rs + d[1, 1] * c11 * rf ** 2
-           + 2 * d[1, 0] * c12 * rf * rs + d[0, 0] * c22 * rs ** 2)
-    two_s = (d[2, 2] * s00 + 2 * d[1, 2] * s10 * rf + 2 * d[0, 2] * s20 * rs + d[1, 1] * s11 * rf ** 2
-             + 2 * d[1, 0] * s12 * rf * rs + d[0, 0] * s22 * rs ** 2)
-    standard_t = integrate(d[0, 2] * c00, right_t)
-    standard_e, standard_o = parity(d[2, 2] * c00, d[2, 2] * s00)
-    one_e, one_o = parity(one, one_s)
-    two_e, two_o = parity(two, two_s)
-    return (standard_t, standard_e, standard_o, temperature, one_e, one_o, two_e, two_o)
+    standard_e, standard_o = parity("std", "std_s")
+    one_e, one_o = parity("one", "one_s")
+    two_e, two_o = parity("two", "two_s")
+    return (acc["std_t"] * cols, standard_e, standard_o, acc["t"] * cols, one_e, one_o, two_e, two_o)
 
 
 def purify_alms(field, alm_mask, maps_unmasked, task, n_iter=None):

@@ -73,6 +73,11 @@ def test_pure_coupling_blocks_match_oracle(cuda, nside):
     for g, w_ in zip(got, want):
         assert float(np.max(np.abs(g.cpu().numpy() - w_))) < 1e-11 * scale
     assert float(np.max(np.abs(want[5]))) < 1e-12 * scale   # one purified field: M- = 0
+    # node chunks small enough to need several passes give the same blocks
+    few = pure.coupling_blocks_pure(torch.from_numpy(window).cuda(), lmax,
+                                    table_bytes=9 * 8 * (lmax + 1) * 7)
+    for g, w_ in zip(few, want):
+        assert float(np.max(np.abs(g.cpu().numpy() - w_))) < 1e-11 * scale
 
 
 @pytest.mark.parametrize("task", [(True, False), (False, True), (True, True)])
