@@ -16,11 +16,16 @@ from .covariance import NmtCovarianceWorkspace, gaussian_covariance, get_iNKA_ce
 from .field import NmtField
 from .utils import (NmtAlmInfo, NmtMapInfo, alm2map, map2alm, map2alm_pair, mask_apodization,
                     synfast_spherical)
-from .workspaces import NmtWorkspace, compute_coupled_cell
+from .workspaces import (NmtWorkspace, compute_coupled_cell, compute_full_master,
+                         coupling_precision, deprojection_bias, get_general_coupling_matrix,
+                         get_master_coefficients, set_coupling_precision,
+                         uncorr_noise_deprojection_bias)
 
 __all__ = [
     "NmtAlmInfo", "NmtBin", "NmtCovarianceWorkspace", "NmtField", "NmtMapInfo", "NmtWorkspace",
-    "alm2map", "gaussian_covariance", "get_iNKA_cell",
+    "alm2map", "gaussian_covariance", "get_iNKA_cell", "compute_full_master",
+    "coupling_precision", "deprojection_bias", "get_general_coupling_matrix",
+    "get_master_coefficients", "set_coupling_precision", "uncorr_noise_deprojection_bias",
     "compute_coupled_cell", "compute_coupled_cells", "decouple_cells", "fields_from_maps",
     "mc_bandpowers", "workspaces_from_fields", "SimulationGraph",
     "get_default_params", "get_precision", "map2alm", "map2alm_pair",

@@ -586,3 +586,237 @@ class NmtWorkspace:
         one_sided = Bk @ M
         win = self._lu.solve(one_sided)
         return win.reshape(self.nbands, self.ncls, n, self.ncls).permute(1, 0, 3, 2)
+
+
+# ----------------------------------------------------------------------------- general couplings
+
+# Coupling operands are FP64 in this build at every size; the reference's switch between
+# FP32 and FP64 operands (workspaces.py:40-84) is kept as a recorded setting.
+_COUPLING_PRECISION = {"name": "auto"}
+
+
+def set_coupling_precision(name):
+    """Record the coupling operand precision ("fp64", "fp32" or "auto";
+    workspaces.py:56-78).  This build computes every coupling block in FP64 (the 3j
+    recursion and the quadrature alike), which is at least as accurate as either choice."""
+    if name not in ("fp64", "fp32", "auto"):
+        raise KeyError("GMaster coupling precision must be 'fp64', 'fp32' or 'auto'")
+    _COUPLING_PRECISION["name"] = name
+
+
+def coupling_precision():
+    """The recorded coupling-precision setting (workspaces.py:81-84)."""
+    return _COUPLING_PRECISION["name"]
+
+
+def general_coupling_matrix(mask_cl, s1, s2, n1, n2, lmax, lmax_mask, table_bytes=None):
+    """Even and odd general coupling matrices ``(2, lmax+1, lmax+1)`` by Gauss-Legendre
+    quadrature (workspaces.py:683-747, 878-905): with the mask correlation
+    xi(x) = sum_L (2L+1)/(4 pi) C_L d^L_{s1-n1, s2-n2}(x) (and its (-1)^L-signed twin),
+    M[l1, l2] = (2 l2 + 1)/2 sum_i w_i d^l1_{n1 n2}(x_i) xi(x_i) d^l2_{-s1,-s2}(x_i), split
+    by the parity of l1 + l2 + L.  Nodes are processed in chunks whose rows fit
+    `table_bytes` (4 GB by default)."""
+    from .pure import PURE_TABLE_BYTES, gl_nodes, wigner_corr, wigner_table
+
+    c = as_device(mask_cl, torch.float64)
+    dev = c.device
+    L, Lm = lmax + 1, lmax_mask + 1
+    cm = torch.zeros(Lm, dtype=torch.float64, device=dev)
+    k = min(c.shape[0], Lm)
+    cm[:k] = c[:k]
+    ell = torch.arange(Lm, dtype=torch.float64, device=dev)
+    coef = (2 * ell + 1) * cm / (4 * np.pi)
+    sign = 1.0 - 2.0 * (torch.arange(Lm, device=dev) % 2).to(torch.float64)
+    order = (2 * lmax + lmax_mask) // 2 + 1
+    x_all, w_all = gl_nodes(order, dev)
+    budget = PURE_TABLE_BYTES if table_bytes is None else int(table_bytes)
+    chunk = max(1, min(order, budget // (2 * 8 * L)))
+    tot = torch.zeros((L, L), dtype=torch.float64, device=dev)
+    sig = torch.zeros((L, L), dtype=torch.float64, device=dev)
+    vecs = torch.stack([coef, coef * sign])
+    for a in range(0, order, chunk):
+        x, w = x_all[a:a + chunk].contiguous(), w_all[a:a + chunk]
+        xi = wigner_corr(x, lmax_mask, s1 - n1, s2 - n2, vecs)
+        first = wigner_table(x, lmax, n1, n2)
+        second = wigner_table(x, lmax, -s1, -s2)
+        tot += (first * (w * xi[0])[None, :]) @ second.T
+        sig += (first * (w * xi[1])[None, :]) @ second.T
+    row = torch.arange(L, dtype=torch.float64, device=dev)
+    cols = ((2 * row + 1) / 2)[None, :]
+    pair_sign = 1.0 - 2.0 * ((row[:, None] + row[None, :]) % 2)
+    tot = tot * cols
+    sig = sig * cols * pair_sign
+    return torch.stack([(tot + sig) / 2, (tot - sig) / 2])
+
+
+def get_general_coupling_matrix(pcl_mask, s1, s2, n1, n2, parity="all"):
+    """General mode-coupling matrix as in pymaster (workspaces.py:1069-1122):
+    M[l, l'] = sum_l'' (2l'+1)(2l''+1)/(4 pi) C_l'' P (l l' l''; n1 -s1 s1-n1)
+    (l l' l''; n2 -s2 s2-n2) with P = 1 ("all"), the even or odd parity of l + l' + l''
+    ("even" / "odd"), or both stacked ("both").  Rows and columns below
+    max(s1, s2, n1, n2) are zero."""
+    if parity not in ("all", "even", "odd", "both"):
+        raise ValueError('`parity` must be "all", "even", "odd", or "both".')
+    c = as_device(pcl_mask, torch.float64)
+    if c.ndim != 1:
+        raise ValueError("pcl_mask must be one-dimensional")
+    lmax = c.shape[0] - 1
+    mats = general_coupling_matrix(c, int(s1), int(s2), int(n1), int(n2), lmax, lmax)
+    lstart = max(int(s1), int(s2), int(n1), int(n2))
+    keep = torch.arange(lmax + 1, device=c.device) >= lstart
+    mats = torch.where(keep[None, :, None] & keep[None, None, :], mats, torch.zeros_like(mats))
+    if parity == "both":
+        return mats
+    if parity == "even":
+        return mats[0]
+    if parity == "odd":
+        return mats[1]
+    return mats.sum(dim=0)
+
+
+def get_master_coefficients(pcl_mask, lmax, spin1, spin2, is_teb=False, pure_any=False,
+                            l_toeplitz=-1, l_exact=-1, dl_band=-1):
+    """The distinct MASTER coupling blocks of a spin pair, divided by 2 l' + 1
+    (workspaces.py:1197-1352): "00", "0s", "pp", "mm" (None when not applicable); "0s",
+    "pp", "mm" carry a leading purification-level axis (1 without purification, 2 or 3
+    with it) and a mask axis before the last two when `pcl_mask` is 2-D.  Spin-0/2
+    blocks come from the 3j recursion (the quadrature with purification), other spins
+    from `general_coupling_matrix`."""
+    from .pure import coupling_blocks_pure
+
+    spin1, spin2, lmax = int(spin1), int(spin2), int(lmax)
+    if is_teb and not (spin1 == 0 and spin2 != 0):
+        raise ValueError("is_teb is only valid for spin1=0 and spin2!=0")
+    if pure_any and spin1 != 2 and spin2 != 2:
+        raise ValueError("pure_any is only valid for spin 2")
+    if pure_any and (spin1 not in (0, 2) or spin2 not in (0, 2)):
+        raise ValueError("Purification is only implemented for spin 2")
+    toeplitz_sanity(l_toeplitz, l_exact, dl_band, lmax)
+    masks = as_device(pcl_mask, torch.float64)
+    one_d = masks.ndim == 1
+    if one_d:
+        masks = masks[None]
+    if masks.ndim != 2:
+        raise ValueError("pcl_mask must be one- or two-dimensional")
+    lmax_mask = masks.shape[1] - 1
+    dev = masks.device
+    cols = (2 * torch.arange(lmax + 1, dtype=torch.float64, device=dev) + 1)[None, :]
+    has_00 = (spin1 == spin2 == 0) or is_teb
+    has_0s = ((spin1 != spin2) and (spin1 == 0 or spin2 == 0)) or is_teb
+    has_ss = (spin1 != 0 and spin2 != 0) or is_teb
+
+    def toeplitz(S):
+        return toeplitz_fill(S.contiguous(), lmax, l_toeplitz, l_exact, dl_band) / cols
+
+    def standard(mask):
+        nw = min(mask.shape[0], 2 * lmax + 1)
+        window = mask[:nw].contiguous()
+        pure8 = coupling_blocks_pure(window, lmax) if pure_any else None
+        res = {}
+        if has_00:
+            if l_toeplitz > 0:
+                res["00"] = coupling_tt_toeplitz(window, lmax, l_toeplitz, l_exact, dl_band) / cols
+            else:
+                res["00"] = coupling_blocks(window, lmax, 1)[_BLOCK_TT] / cols
+        if has_0s:
+            if spin1 in (0, 2) and spin2 in (0, 2):
+                te = pure8[0] if pure8 is not None else coupling_blocks(window, lmax, 2)[_BLOCK_TE]
+                res["0s"] = te / cols
+            else:
+                p0, p1 = (0, spin2) if spin1 == 0 else (spin1, 0)
+                res["0s"] = general_coupling_matrix(mask, p0, p1, p0, p1, lmax, lmax_mask).sum(0) / cols
+        if has_ss:
+            a, b = (spin2, spin2) if is_teb else (spin1, spin2)
+            if a == b == 2:
+                if pure8 is not None:
+                    ev, od = pure8[1], pure8[2]
+                else:
+                    blk = coupling_blocks(window, lmax, 12)
+                    ev, od = blk[_BLOCK_PP], blk[_BLOCK_MM]
+                res["pp"], res["mm"] = ev / cols, od / cols
+            else:
+                mats = general_coupling_matrix(mask, a, b, a, b, lmax, lmax_mask) / cols
+                res["pp"], res["mm"] = mats[0], mats[1]
+        if l_toeplitz > 0:
+            for name in ("0s", "pp", "mm"):
+                if name in res:
+                    res[name] = toeplitz(res[name])
+        if pure_any:
+            p = [mtx / cols for mtx in pure8[3:]]
+            if has_0s:
+                res["0s"] = torch.stack([res["0s"], p[0]])
+            if has_ss:
+                res["pp"] = torch.stack([res["pp"], p[1], p[3]])
+                res["mm"] = torch.stack([res["mm"], p[2], p[4]])
+        else:
+            for name in ("0s", "pp", "mm"):
+                if name in res:
+                    res[name] = res[name][None]
+        return res
+
+    values = [standard(m) for m in masks]
+    out = {}
+    for name, present in (("00", has_00), ("0s", has_0s), ("pp", has_ss), ("mm", has_ss)):
+        if not present:
+            out[name] = None
+            continue
+        arrs = [v[name] for v in values]
+        out[name] = arrs[0] if one_d else torch.stack(arrs, dim=-3)
+    out.update(pure_any=bool(pure_any),
+               toeplitz={"l_toeplitz": l_toeplitz, "l_exact": l_exact, "dl_band": dl_band},
+               spins=(spin1, spin2), lmax=lmax, lmax_mask=lmax_mask)
+    return out
+
+
+def deprojection_bias(f1, f2, cl_guess, n_iter=None):
+    """Coupled bias from contaminant-template deprojection (workspaces.py:2268-2386).  Fields
+    of this build carry no templates (deprojection is outside it), so after the
+    reference's checks the bias is zero."""
+    if not f1.is_compatible(f2):
+        raise ValueError("Fields have incompatible pixelizations")
+    shape = (f1.nmaps * f2.nmaps, f1.ainfo.lmax + 1)
+    guess = as_device(cl_guess, torch.float64)
+    if tuple(guess.shape) != shape:
+        raise ValueError(f"Guess Cl should have shape {shape}")
+    if f1.lite or f2.lite:
+        raise ValueError("Can't compute deprojection bias for lightweight fields")
+    return torch.zeros(shape, dtype=torch.float64, device=guess.device)
+
+
+def uncorr_noise_deprojection_bias(f1, map_var, n_iter=None):
+    """Deprojection bias for uncorrelated noise (workspaces.py:2389-2454): zero for fields
+    without templates, which are all the fields of this build."""
+    if f1.lite:
+        raise ValueError("Can't compute deprojection bias for lightweight fields")
+    var = as_device(map_var, torch.float64).reshape(-1)
+    if var.shape[0] != f1.minfo.npix:
+        raise ValueError("Variance map doesn't match map resolution")
+    return torch.zeros((f1.nmaps * f1.nmaps, f1.ainfo.lmax + 1), dtype=torch.float64,
+                       device=var.device)
+
+
+def compute_full_master(f1, f2, b=None, cl_noise=None, cl_guess=None, workspace=None,
+                        l_toeplitz=-1, l_exact=-1, dl_band=-1, normalization="MASTER"):
+    """The full MASTER estimator for two fields (workspaces.py:2457-2517): coupled
+    pseudo-C_ell minus the deprojection and noise biases, decoupled into bandpowers with
+    `workspace` (built from `b` if not given)."""
+    if b is None and workspace is None:
+        raise SyntaxError("Must supply either workspace or bins")
+    if not f1.is_compatible(f2, strict=False):
+        raise ValueError("Fields have incompatible pixelizations")
+    coupled = compute_coupled_cell(f1, f2)
+    shape = (f1.nmaps * f2.nmaps, f1.ainfo.lmax + 1)
+    dev = coupled.device
+    noise = (torch.zeros(shape, dtype=torch.float64, device=dev) if cl_noise is None
+             else as_device(cl_noise, torch.float64, dev))
+    guess = (torch.zeros(shape, dtype=torch.float64, device=dev) if cl_guess is None
+             else as_device(cl_guess, torch.float64, dev))
+    if tuple(noise.shape) != shape:
+        raise ValueError(f"Noise Cl should have shape {shape}")
+    if tuple(guess.shape) != shape:
+        raise ValueError(f"Guess Cl should have shape {shape}")
+    bias = deprojection_bias(f1, f2, guess)
+    if workspace is None:
+        workspace = NmtWorkspace.from_fields(f1, f2, b, l_toeplitz=l_toeplitz, l_exact=l_exact,
+                                             dl_band=dl_band, normalization=normalization)
+    return workspace.decouple_cell(coupled - bias - noise)

@@ -1,7 +1,6 @@
 """Every compiled tile shape of the SIMT Legendre kernels gives the result of the built-in
 choice (only the summation order differs), and the autotuner picks one of them."""
 
-import numpy as np
 import pytest
 import torch
 

@@ -1,0 +1,108 @@
+"""General coupling matrices, MASTER coefficients and the full-MASTER helpers on the GPU.
+
+`get_general_coupling_matrix` is checked against the oracle's restatement of the
+reference's quadrature (workspaces.py:683-747, oracle.c orc_coupling_quadrature, whose
+spin 0/2 cases equal the 3j closed forms), and `get_master_coefficients` against the
+oracle's blocks divided by 2 l' + 1.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+import gmaster_b200 as nmt
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _window(nside, lmax):
+    vec = oracle.pix2vec(nside)
+    mask = (vec[:, 2] < 0.45) * (0.6 + 0.4 * vec[:, 0] ** 2)
+    am = oracle.map2alm(mask[None], 0, nside, lmax, 3)
+    return mask, oracle.pcl(am, am, lmax)[0]
+
+
+def _rel(got, want):
+    return float(np.max(np.abs(got - want)) / np.max(np.abs(want)))
+
+
+@pytest.mark.parametrize("spins", [(0, 2, 0, 2), (2, 2, 2, 2), (1, 1, 1, 1), (0, 1, 0, 1),
+                                   (2, 1, 2, 1), (0, 0, 0, 0)])
+def test_general_coupling_matrix_matches_oracle(cuda, spins):
+    nside = 8
+    lmax = 3 * nside - 1
+    _, w = _window(nside, lmax)
+    s1, s2, n1, n2 = spins
+    got = nmt.get_general_coupling_matrix(w, s1, s2, n1, n2, parity="both").cpu().numpy()
+    even, odd = oracle.coupling_quadrature(w, lmax, s1, s2, n1, n2, lmax_mask=lmax)
+    lo = max(spins)
+    for g, o in zip(got, (even, odd)):
+        o = o.copy()
+        o[:lo, :] = 0
+        o[:, :lo] = 0
+        if np.max(np.abs(o)) > 0:
+            assert np.max(np.abs(g - o)) < 1e-11 * np.max(np.abs(even) + np.abs(odd))
+    allp = nmt.get_general_coupling_matrix(w, s1, s2, n1, n2).cpu().numpy()
+    np.testing.assert_allclose(allp, got[0] + got[1], rtol=0, atol=1e-14)
+    with pytest.raises(ValueError):
+        nmt.get_general_coupling_matrix(w, s1, s2, n1, n2, parity="bad")
+
+
+def test_master_coefficients_match_oracle_blocks(cuda):
+    nside = 8
+    lmax = 3 * nside - 1
+    _, w = _window(nside, lmax)
+    cols = (2.0 * np.arange(lmax + 1) + 1.0)[None, :]
+    tt = oracle.coupling_tt_closed(w, lmax) / cols
+    te = oracle.coupling_blocks(w, lmax, 0, 2)["te"] / cols
+    pm = oracle.coupling_blocks(w, lmax, 2, 2)
+    c = nmt.get_master_coefficients(w, lmax, 0, 0)
+    assert _rel(c["00"].cpu().numpy(), tt) < 1e-11 and c["0s"] is None and c["pp"] is None
+    c = nmt.get_master_coefficients(w, lmax, 0, 2, is_teb=True)
+    assert _rel(c["00"].cpu().numpy(), tt) < 1e-11
+    assert c["0s"].shape == (1, lmax + 1, lmax + 1) and _rel(c["0s"][0].cpu().numpy(), te) < 1e-11
+    assert _rel(c["pp"][0].cpu().numpy(), pm["pp"] / cols) < 1e-11
+    assert _rel(c["mm"][0].cpu().numpy(), pm["mm"] / cols) < 1e-11
+    c = nmt.get_master_coefficients(np.stack([w, 2 * w]), lmax, 2, 2, pure_any=True)
+    assert c["pp"].shape == (3, 2, lmax + 1, lmax + 1) and c["pure_any"]
+    pure = oracle.coupling_blocks_pure(w, lmax)
+    assert _rel(c["pp"][2, 0].cpu().numpy(), pure[6] / cols) < 1e-10
+    assert _rel(c["pp"][0, 1].cpu().numpy(), 2 * pure[1] / cols) < 1e-10
+    c = nmt.get_master_coefficients(w, lmax, 0, 1)
+    gen = oracle.coupling_quadrature(w, lmax, 0, 1, 0, 1, lmax_mask=lmax)
+    want = (gen[0] + gen[1]) / cols
+    want[:1, :] = 0
+    want[:, :1] = 0
+    got = c["0s"][0].cpu().numpy()
+    got[:1, :] = 0
+    got[:, :1] = 0
+    assert _rel(got, want) < 1e-10
+    with pytest.raises(ValueError):
+        nmt.get_master_coefficients(w, lmax, 2, 0, is_teb=True)
+
+
+def test_compute_full_master_and_biases(cuda):
+    nside, nlb = 16, 4
+    lmax = 3 * nside - 1
+    mask, _ = _window(nside, lmax)
+    rng = np.random.default_rng(2)
+    f = nmt.NmtField(mask, rng.normal(size=(2, len(mask))), spin=2, n_iter=0, precision="fp64")
+    b = nmt.NmtBin.from_nside_linear(nside, nlb)
+    w = nmt.NmtWorkspace.from_fields(f, f, b)
+    noise = rng.random((4, lmax + 1)) * 1e-3
+    want = w.decouple_cell(nmt.compute_coupled_cell(f, f) - torch.from_numpy(noise).cuda())
+    got = nmt.compute_full_master(f, f, b, cl_noise=noise)
+    np.testing.assert_allclose(got.cpu().numpy(), want.cpu().numpy(), rtol=1e-12, atol=0)
+    got_w = nmt.compute_full_master(f, f, workspace=w, cl_noise=noise)
+    np.testing.assert_array_equal(got_w.cpu().numpy(), want.cpu().numpy())
+    z = nmt.deprojection_bias(f, f, np.zeros((4, lmax + 1)))
+    assert float(z.abs().max()) == 0.0 and tuple(z.shape) == (4, lmax + 1)
+    z = nmt.uncorr_noise_deprojection_bias(f, np.ones(len(mask)))
+    assert tuple(z.shape) == (4, lmax + 1)
+    with pytest.raises(SyntaxError):
+        nmt.compute_full_master(f, f)
+    with pytest.raises(ValueError, match="Noise"):
+        nmt.compute_full_master(f, f, b, cl_noise=np.zeros((3, lmax + 1)))
+    with pytest.raises(ValueError, match="Guess"):
+        nmt.deprojection_bias(f, f, np.zeros((4, lmax)))

@@ -325,3 +325,17 @@ def test_oracle_purification_quadrature_is_pinned():
     f = oracle.coupling_blocks_pure(full, lmax)
     for p, q in ((3, 0), (4, 1), (6, 1), (5, 2), (7, 2)):
         assert np.max(np.abs(f[p] - f[q])) < 1e-13
+
+
+def test_coupling_precision_setting():
+    import gmaster_b200 as nmt
+
+    old = nmt.coupling_precision()
+    try:
+        for name in ("fp64", "fp32", "auto"):
+            nmt.set_coupling_precision(name)
+            assert nmt.coupling_precision() == name
+        with pytest.raises(KeyError):
+            nmt.set_coupling_precision("fp16")
+    finally:
+        nmt.set_coupling_precision(old)
