@@ -15,7 +15,7 @@ from .bins import NmtBin
 from .covariance import NmtCovarianceWorkspace, gaussian_covariance, get_iNKA_cell
 from .field import NmtField
 from .utils import (NmtAlmInfo, NmtMapInfo, alm2map, map2alm, map2alm_pair, mask_apodization,
-                    synfast_spherical)
+                    moore_penrose_pinvh, synfast_spherical)
 from .workspaces import (NmtWorkspace, compute_coupled_cell, compute_full_master,
                          coupling_precision, deprojection_bias, get_general_coupling_matrix,
                          get_master_coefficients, set_coupling_precision,
@@ -29,7 +29,7 @@ __all__ = [
     "compute_coupled_cell", "compute_coupled_cells", "decouple_cells", "fields_from_maps",
     "mc_bandpowers", "workspaces_from_fields", "SimulationGraph",
     "get_default_params", "get_precision", "map2alm", "map2alm_pair",
-    "mask_apodization", "nmt_params", "set_n_iter_default", "set_precision",
+    "mask_apodization", "moore_penrose_pinvh", "nmt_params", "set_n_iter_default", "set_precision",
     "set_sht_calculator", "set_tol_pinv_default", "synfast_spherical",
 ]
 

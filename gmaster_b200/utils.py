@@ -19,7 +19,7 @@ __all__ = [
     "NmtAlmInfo", "NmtMapInfo", "alm2map", "map2alm", "map2alm_pair", "mask_apodization",
     "synfast_spherical", "pix2vec_ring", "nmt_params", "get_default_params",
     "set_n_iter_default", "set_tol_pinv_default", "set_precision", "get_precision",
-    "set_sht_calculator", "as_device", "max_pixel_radius",
+    "set_sht_calculator", "as_device", "max_pixel_radius", "moore_penrose_pinvh",
 ]
 
 
@@ -262,6 +262,19 @@ def mask_apodization(mask_in, aposize, apotype="C1"):
               _lib.ptr(nxt), float(2 * threshold), float(threshold),
               0 if apotype == "C1" else 1, _lib.ptr(out), stream)
     return result(out)
+
+
+def moore_penrose_pinvh(mat, tol_pinv):
+    """Pseudo-inverse of a Hermitian matrix on the GPU (gmaster/utils.py:527-556): the
+    eigenvalues below ``tol_pinv`` times the largest have their inverse set to zero; with
+    ``tol_pinv`` None or <= 0 the ordinary inverse is returned."""
+    t = mat if isinstance(mat, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(mat))
+    m = as_device(t, torch.complex128 if t.is_complex() else torch.float64)
+    if tol_pinv is None or tol_pinv <= 0:
+        return torch.linalg.inv(m)
+    vals, vecs = torch.linalg.eigh(m)
+    inv = torch.where(vals >= tol_pinv * vals.max(), 1.0 / vals, torch.zeros_like(vals))
+    return (vecs * inv[None, :]) @ vecs.conj().T
 
 
 def gaussian_alm(cls, lmax, rng):

@@ -256,7 +256,7 @@ class NmtWorkspace:
     def __init__(self, fl1=None, fl2=None, bins=None, is_teb=False, l_toeplitz=-1, l_exact=-1,
                  dl_band=-1, fname=None, normalization="MASTER"):
         self.mcm_blocks = self.mcm_binned = self._lu = None
-        self._slot_blocks = None
+        self._slot_blocks = self._dense = self._bpws = None
         self.pure_e1 = self.pure_b1 = self.pure_e2 = self.pure_b2 = False
         if fname is not None:
             self.read_from(fname)
@@ -328,12 +328,19 @@ class NmtWorkspace:
         self.l_toeplitz = int(h.get("L_TOEPLITZ", -1))
         self.l_exact = int(h.get("L_EXACT", -1))
         self.dl_band = int(h.get("DL_BAND", -1))
-        if self.pure_e1 or self.pure_b1 or self.pure_e2 or self.pure_b2:
-            # purified channels take different blocks per slot: keep each slot's block
-            self.mcm_blocks = None
-            self._slot_blocks = _slot_blocks_from_dense(prim["data"], self.lmax, self.ncls, dev)
-        else:
-            self.mcm_blocks = _blocks_from_dense(prim["data"], self.lmax, self.ncls, dev)
+        self._dense = None
+        try:
+            if self.pure_e1 or self.pure_b1 or self.pure_e2 or self.pure_b2:
+                # purified channels take different blocks per slot: keep each slot's block
+                self.mcm_blocks = None
+                self._slot_blocks = _slot_blocks_from_dense(prim["data"], self.lmax, self.ncls, dev)
+            else:
+                self.mcm_blocks = _blocks_from_dense(prim["data"], self.lmax, self.ncls, dev)
+        except NotImplementedError:
+            # a matrix without the slot structure (e.g. one set by update_coupling_matrix):
+            # keep it dense
+            self.mcm_blocks = self._slot_blocks = None
+            self._dense = torch.from_numpy(np.ascontiguousarray(prim["data"], dtype=np.float64)).to(dev)
         beams = hdus["BEAMS"]["data"]
         if "BEAMS" in beams:
             b1 = b2 = np.sqrt(beams["BEAMS"].astype(np.float64))
@@ -404,7 +411,7 @@ class NmtWorkspace:
         """Coupling blocks, or the exact ``blocks`` given (from a multi-workspace launch),
         then the Toeplitz fill when it is enabled."""
         l_toeplitz, l_exact, dl_band = self.l_toeplitz, self.l_exact, self.dl_band
-        self._slot_blocks = None
+        self._slot_blocks = self._dense = None
         if getattr(self, "_pure_any", False):
             self._compute_pure_blocks()
             return
@@ -464,12 +471,23 @@ class NmtWorkspace:
         self.mcm_blocks = None
 
     def _postprocess(self):
-        dev = (self.mcm_blocks if self.mcm_blocks is not None else self._slot_blocks[0][0]).device
+        self._bpws = None
+        if self._dense is not None:
+            dev = self._dense.device
+        elif self.mcm_blocks is not None:
+            dev = self.mcm_blocks.device
+        else:
+            dev = self._slot_blocks[0][0].device
         ops = self.bins.device_operators(dev)
         beam = (self.beam1 * self.beam2).contiguous()
         N = self.ncls * self.nbands
         if self.normalization == "FKP":
             self.mcm_binned = self.wawb * torch.eye(N, dtype=torch.float64, device=dev)
+        elif self._dense is not None:
+            # B M diag(beam) T with kron(., I_ncls) operators, as FP64 GEMMs
+            B, T = self._dense_operators(dev)
+            rep = beam.repeat_interleave(self.ncls)[None, :]
+            self.mcm_binned = (B @ (self._dense * rep)) @ T
         elif self._slot_blocks is not None:
             # a block per slot: each distinct block binned once, then placed with its sign
             nb = self.nbands
@@ -515,6 +533,8 @@ class NmtWorkspace:
     def get_coupling_matrix(self):
         """Dense (ncls (lmax+1))^2 MCM in ``l * ncls + c`` order (workspaces.py:2005-2025)."""
         n = self.lmax + 1
+        if self._dense is not None:
+            return self._dense.clone()
         if self._slot_blocks is not None:
             dev = self._slot_blocks[0][0].device
             out = torch.zeros((n, self.ncls, n, self.ncls), dtype=torch.float64, device=dev)
@@ -573,19 +593,50 @@ class NmtWorkspace:
         sol = self._lu.solve(vec)
         return sol.reshape(self.nbands, self.ncls).T
 
+    def _dense_operators(self, dev):
+        """kron(B, I_ncls) (nbands ncls, L ncls) and kron(T, I_ncls) (L ncls, nbands ncls):
+        B averages a spectrum into bands with weight x f_ell, T spreads a bandpower over its
+        multipoles divided by f_ell (workspaces.py:1452-1470)."""
+        n = self.lmax + 1
+        ops = self.bins.device_operators(dev)
+        ells = torch.from_numpy(self.bins._ells_np.astype(np.int64)).to(dev)
+        bp = torch.from_numpy(self.bins._bpws_np.astype(np.int64)).to(dev)
+        B = torch.zeros((self.nbands, n), dtype=torch.float64, device=dev)
+        B[bp, ells] = ops["wfl"][ells]
+        T = torch.zeros((n, self.nbands), dtype=torch.float64, device=dev)
+        T[ells, bp] = ops["inv_fl"][ells]
+        eye = torch.eye(self.ncls, dtype=torch.float64, device=dev)
+        return torch.kron(B, eye), torch.kron(T, eye)
+
+    @property
+    def bpws(self):
+        """Bandpower windows solve(mcm_binned, B M diag(beam)), (nbands ncls, (lmax+1) ncls),
+        computed on first access (workspaces.py:1629-1638)."""
+        if self._bpws is None and self._lu is not None:
+            dev = self.mcm_binned.device
+            M = self.get_coupling_matrix() * (self.beam1 * self.beam2).repeat_interleave(self.ncls)[None]
+            B, _ = self._dense_operators(dev)
+            self._lu.check()
+            self._bpws = self._lu.solve((B @ M).contiguous())
+        return self._bpws
+
     def get_bandpower_windows(self):
         """(ncls, nbands, ncls, lmax+1) windows W with <C_b> = sum W C_l (workspaces.py:2149-2160)."""
         n = self.lmax + 1
-        ops = self.bins.device_operators(self.mcm_binned.device)
-        M = self.get_coupling_matrix() * (self.beam1 * self.beam2).repeat_interleave(self.ncls)[None]
-        B = torch.zeros((self.nbands, n), dtype=torch.float64, device=M.device)
-        ells = torch.from_numpy(self.bins._ells_np.astype(np.int64)).to(M.device)
-        bp = torch.from_numpy(self.bins._bpws_np.astype(np.int64)).to(M.device)
-        B[bp, ells] = ops["wfl"][ells]
-        Bk = torch.kron(B, torch.eye(self.ncls, dtype=torch.float64, device=M.device))
-        one_sided = Bk @ M
-        win = self._lu.solve(one_sided)
-        return win.reshape(self.nbands, self.ncls, n, self.ncls).permute(1, 0, 3, 2)
+        return self.bpws.reshape(self.nbands, self.ncls, n, self.ncls).permute(1, 0, 3, 2)
+
+    def update_coupling_matrix(self, new_matrix):
+        """Replace the unbinned coupling matrix ((ncls (lmax+1))^2, the ordering of
+        `get_coupling_matrix`) and recompute the binned matrix and its LU factors
+        (workspaces.py:2023-2040).  The matrix is kept dense."""
+        size = self.ncls * (self.lmax + 1)
+        if tuple(np.shape(new_matrix)) != (size, size):
+            raise ValueError(f"Input matrix has an inconsistent shape. Expected {(size, size)}, "
+                             f"but got {tuple(np.shape(new_matrix))}")
+        dev = self.mcm_binned.device if self.mcm_binned is not None else None
+        self._dense = as_device(new_matrix, torch.float64, dev).clone()
+        self.mcm_blocks = self._slot_blocks = None
+        self._postprocess()
 
 
 # ----------------------------------------------------------------------------- general couplings

@@ -106,3 +106,50 @@ def test_compute_full_master_and_biases(cuda):
         nmt.compute_full_master(f, f, b, cl_noise=np.zeros((3, lmax + 1)))
     with pytest.raises(ValueError, match="Guess"):
         nmt.deprojection_bias(f, f, np.zeros((4, lmax)))
+
+
+def test_update_coupling_matrix_bpws_and_dense_files(cuda, tmp_path):
+    """update_coupling_matrix keeps an arbitrary dense matrix (workspaces.py:2023-2040): the
+    same matrix reproduces the bandpowers, a perturbed one matches the oracle's binning,
+    bandpower windows map theory to bandpowers, and a dense matrix survives a file."""
+    nside, nlb = 16, 4
+    lmax = 3 * nside - 1
+    mask, _ = _window(nside, lmax)
+    rng = np.random.default_rng(3)
+    f = nmt.NmtField(mask, rng.normal(size=(2, len(mask))), spin=2, n_iter=0, precision="fp64")
+    b = nmt.NmtBin.from_nside_linear(nside, nlb)
+    w = nmt.NmtWorkspace.from_fields(f, f, b)
+    cl = rng.random((4, lmax + 1))
+    ref = w.decouple_cell(cl).cpu().numpy()
+    bp = w.bpws
+    assert tuple(bp.shape) == (4 * w.nbands, 4 * (lmax + 1))
+    theory = w.decouple_cell(w.couple_cell(cl)).cpu().numpy()
+    via_w = np.einsum("cbdl,dl->cb", w.get_bandpower_windows().cpu().numpy(), cl)
+    np.testing.assert_allclose(via_w, theory, rtol=1e-10, atol=1e-14)
+    M = w.get_coupling_matrix().cpu().numpy()
+    w.update_coupling_matrix(M)
+    np.testing.assert_allclose(w.decouple_cell(cl).cpu().numpy(), ref, rtol=1e-10, atol=0)
+    M2 = M + 1e-3 * rng.normal(size=M.shape) * np.abs(M).max()
+    w.update_coupling_matrix(M2)
+    want = oracle.decouple(oracle.binned_mcm(M2, lmax, nlb, 4), cl, lmax, nlb)
+    got = w.decouple_cell(cl).cpu().numpy()
+    assert _rel(got, want) < 1e-9
+    path = str(tmp_path / "dense.fits")
+    w.write_to(path)
+    back = nmt.NmtWorkspace.from_file(path)
+    np.testing.assert_array_equal(back.get_coupling_matrix().cpu().numpy(), M2)
+    np.testing.assert_allclose(back.decouple_cell(cl).cpu().numpy(), got, rtol=1e-12, atol=0)
+    with pytest.raises(ValueError, match="inconsistent shape"):
+        w.update_coupling_matrix(M2[:-1])
+
+
+def test_moore_penrose_pinvh(cuda):
+    rng = np.random.default_rng(4)
+    a = rng.normal(size=(6, 6))
+    spd = a @ a.T + 6 * np.eye(6)
+    np.testing.assert_allclose(nmt.moore_penrose_pinvh(spd, None).cpu().numpy(), np.linalg.inv(spd),
+                               rtol=1e-12, atol=1e-14)
+    v = rng.normal(size=(6, 3))
+    low = v @ v.T
+    got = nmt.moore_penrose_pinvh(low, 1e-10).cpu().numpy()
+    np.testing.assert_allclose(got, np.linalg.pinv(low, hermitian=True), rtol=1e-9, atol=1e-11)
