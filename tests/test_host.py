@@ -339,3 +339,43 @@ def test_coupling_precision_setting():
             nmt.set_coupling_precision("fp16")
     finally:
         nmt.set_coupling_precision(old)
+
+
+@pytest.mark.parametrize("ncls,flags", [(2, (False, False, False, True)), (2, (False, False, True, True)),
+                                        (4, (False, True, False, True)), (4, (True, True, False, False)),
+                                        (4, (True, False, False, True)), (7, (False, False, False, True)),
+                                        (7, (False, False, True, True))])
+def test_purified_slot_levels_match_the_reference_rule(monkeypatch, ncls, flags):
+    """The slot -> block choice of purified workspaces (gmaster/workspaces.py:1852-1897), on
+    the CPU with random stand-in blocks: the dense matrix equals the oracle's restatement,
+    and rebuilding per-slot blocks from it (what a file read does) gives it back."""
+    import oracle
+    import torch
+
+    from gmaster_b200 import pure
+    from gmaster_b200 import workspaces as wsm
+
+    rng = np.random.default_rng(ncls + 10 * sum(flags))
+    lmax = 6
+    n = lmax + 1
+    fake8 = tuple(torch.from_numpy(rng.normal(size=(n, n))) for _ in range(8))
+    tt = torch.from_numpy(rng.normal(size=(n, n)))
+    monkeypatch.setattr(pure, "coupling_blocks_pure", lambda window, lm: fake8)
+
+    def fake_blocks(window, lm, which):
+        out = torch.zeros((4, n, n), dtype=torch.float64)
+        out[wsm._BLOCK_TT] = tt
+        return out
+
+    monkeypatch.setattr(wsm, "coupling_blocks", fake_blocks)
+    w = wsm.NmtWorkspace()
+    w.lmax, w.ncls = lmax, ncls
+    w.window = torch.zeros(2 * lmax + 1, dtype=torch.float64)
+    w.pure_e1, w.pure_b1, w.pure_e2, w.pure_b2 = flags
+    w._compute_pure_blocks()
+    got = w.get_coupling_matrix().numpy()
+    want = oracle.assemble_pure_mcm(tuple(b.numpy() for b in fake8), tt.numpy(), lmax, ncls, flags)
+    np.testing.assert_array_equal(got, want)
+    slots = wsm._slot_blocks_from_dense(got, lmax, ncls, "cpu")
+    w._slot_blocks = slots
+    np.testing.assert_array_equal(w.get_coupling_matrix().numpy(), want)
