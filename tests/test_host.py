@@ -379,3 +379,51 @@ def test_purified_slot_levels_match_the_reference_rule(monkeypatch, ncls, flags)
     slots = wsm._slot_blocks_from_dense(got, lmax, ncls, "cpu")
     w._slot_blocks = slots
     np.testing.assert_array_equal(w.get_coupling_matrix().numpy(), want)
+
+
+def test_integration_document_lists_every_entry_point():
+    text = open("INTEGRATION.md").read()
+    missing = [s for s in _header_symbols() if s not in text]
+    assert not missing, missing
+
+
+def test_covariance_kernel_spin_rule_equals_the_reference_table():
+    """The rule choosing the kernels of each Wick contraction equals the table of
+    gmaster/covariance.py:266-283 (restated in the oracle) for all 16 spin combinations."""
+    import oracle
+    from gmaster_b200.covariance import _kernel_spins
+
+    for (a1, a2, b1, b2), (p0, p1) in oracle._COV_PAIRS.items():
+        assert _kernel_spins(a1, a2, b1, b2) == p0
+        assert _kernel_spins(a1, a2, b2, b1) == p1
+
+
+def test_covariance_workspace_file_layout_on_the_host(tmp_path):
+    """write_to / read_from of a covariance workspace in the reference's FITS layout
+    (gmaster/covariance.py:578-658), with host tensors."""
+    import torch
+
+    from gmaster_b200 import fits
+    from gmaster_b200.covariance import NmtCovarianceWorkspace
+
+    rng = np.random.default_rng(1)
+    n = 9
+    cw = NmtCovarianceWorkspace()
+    cw.spins = (0, 2, 0, 2)
+    cw.spin_a1, cw.spin_a2, cw.spin_b1, cw.spin_b2 = cw.spins
+    cw.lmax, cw.lmax_mask = n - 1, n - 1
+    cw.l_toeplitz, cw.l_exact, cw.dl_band = -1, -1, -1
+    cw._post_init()
+    xi0 = {"00": None, "0s": torch.from_numpy(rng.normal(size=(n, n))), "pp": None, "mm": None}
+    xi1 = {"00": torch.from_numpy(rng.normal(size=(n, n))), "0s": None, "pp": None, "mm": None}
+    cw.xiSS = [xi0, xi1]
+    path = str(tmp_path / "cw.fits")
+    cw.write_to(path)
+    names = [h["name"] for h in fits.read(path)]
+    assert names == ["CWSP_PRIMARY", "XI02_1122", "XI00_1221"]
+    back = NmtCovarianceWorkspace()
+    back.read_from(path, device="cpu")
+    assert back.spins == (0, 2, 0, 2) and back.nclsa == 2 and back.nclsb == 2
+    np.testing.assert_array_equal(back.xiSS[0]["0s"].numpy(), xi0["0s"].numpy())
+    np.testing.assert_array_equal(back.xiSS[1]["00"].numpy(), xi1["00"].numpy())
+    assert back.xiSS[0]["00"] is None and back.xiSS[1]["0s"] is None
