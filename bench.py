@@ -62,7 +62,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", default="mc",
                    choices=["mc", "uneven_workspaces", "nside4096", "mc1024", "nside8192", "apodize",
-                            "covariance"],
+                            "covariance", "purify"],
                    help="mc: the Monte-Carlo estimator (default); uneven_workspaces: TT "
                         "coupling matrices of 32 masks of mixed Nside in one launch; nside4096: "
                         "batched map2alm (n_iter=0) and alm2map at Nside 4096; mc1024: 512 TQU "
@@ -70,7 +70,8 @@ def parse():
                         "nside8192: one spin-2 spectrum at Nside 8192 with the exact and the "
                         "Toeplitz coupling matrix; apodize: C1 apodisation of the binary "
                         "Nside 2048 and 8192 config masks on the GPU; covariance: Gaussian "
-                        "(NKA) covariance workspaces and bandpower covariances at Nside 2048")
+                        "(NKA) covariance workspaces and bandpower covariances at Nside 2048; "
+                        "purify: a purified-B spin-2 field and its 2x2 workspace at Nside 2048")
     p.add_argument("--apo-nsides", default="2048,8192",
                    help="apodize workload: the Nside values to run (the first is the headline)")
     p.add_argument("--nmasks", type=int, default=32)
@@ -1000,6 +1001,67 @@ def run_covariance(args):
     print(json.dumps(line), flush=True)
 
 
+def run_purify(args):
+    """E/B purification at Nside 2048 (lmax 6143) on the config mask: a plain and a
+    purified-B spin-2 field (mixed precision, n_iter 3), their 2x2 workspaces (bands of 16;
+    the purified one by Gauss-Legendre quadrature) and the purified bandpowers.  Wall
+    times around synchronised steps (each stage is seconds long)."""
+    import torch
+
+    import gmaster_b200 as nmt
+    from gmaster_b200 import _lib, autotune
+
+    autotune.set_autotune(False)
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    nside, nlb = args.nside, args.nlb
+    mask = make_mask(nside, dev)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1)
+    qu = torch.randn((2, 12 * nside * nside), generator=gen, device=dev, dtype=torch.float64)
+    nmt.NmtField(mask, qu, spin=2, n_iter=3, precision="mixed")   # warm-up (plans, mask alms)
+    torch.cuda.synchronize()
+    calls0 = dict(_lib.CALLS)
+    sampler = ClockSampler(0)
+    sampler.start()
+    marks = [time.perf_counter()]
+
+    def mark():
+        torch.cuda.synchronize()
+        marks.append(time.perf_counter())
+
+    f_plain = nmt.NmtField(mask, qu, spin=2, n_iter=3, precision="mixed")
+    mark()
+    f_pure = nmt.NmtField(mask, qu, spin=2, purify_b=True, n_iter=3, precision="mixed")
+    mark()
+    b = nmt.NmtBin.from_nside_linear(nside, nlb)
+    nmt.NmtWorkspace.from_fields(f_plain, f_plain, b)
+    mark()
+    w_pure = nmt.NmtWorkspace.from_fields(f_pure, f_pure, b)
+    mark()
+    w_pure.decouple_cell(nmt.compute_coupled_cell(f_pure, f_pure))
+    mark()
+    clocks = sampler.stop()
+    launches = sum(_lib.CALLS.get(k, 0) - calls0.get(k, 0) for k in _lib.CALLS)
+    d = [b_ - a for a, b_ in zip(marks[:-1], marks[1:])]
+    total = d[1] + d[3] + d[4]
+    line = {
+        "metric": "purified-B spectrum s (purified field, purified 2x2 workspace, bandpowers), Nside 2048",
+        "value": total, "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 1,
+        "ms_per_step": total * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 transforms (f64 recurrence), f64 quadrature and LU",
+        "data": "synthetic (config mask recipe; Gaussian (Q, U) maps)",
+        "config": {"workload": f"purified-B spin-2 field and 2x2 workspace at Nside {nside}, "
+                               f"lmax {3 * nside - 1}, n_iter 3, bands of {nlb}",
+                   "nside": nside, "nlb": nlb},
+        "stages_s": {"plain field": d[0], "purified field": d[1], "plain 2x2 workspace": d[2],
+                     "purified 2x2 workspace": d[3], "spectra": d[4]},
+        "peak_device_gb": torch.cuda.max_memory_allocated(dev) / 1e9,
+        "clocks": clocks, "gpu_launches": int(launches),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -1022,6 +1084,9 @@ def main():
         return
     if args.workload == "covariance":
         run_covariance(args)
+        return
+    if args.workload == "purify":
+        run_purify(args)
         return
     import torch
     import torch.distributed as dist
