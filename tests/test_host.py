@@ -427,3 +427,45 @@ def test_covariance_workspace_file_layout_on_the_host(tmp_path):
     np.testing.assert_array_equal(back.xiSS[0]["0s"].numpy(), xi0["0s"].numpy())
     np.testing.assert_array_equal(back.xiSS[1]["00"].numpy(), xi1["00"].numpy())
     assert back.xiSS[0]["00"] is None and back.xiSS[1]["0s"] is None
+
+
+def _emulate_cov_binned(cov, ops_a, ops_b):
+    """The band-pair reduction of gm_cov_binned restated in numpy: for bands p, q the sum
+    over l1 in p and l2 in q of w_a[l1] w_b[l2] cov[x, l1, l2], from the CSR operators."""
+    pa, ea, wa = (ops_a[k].numpy() for k in ("ptr", "ells", "wfl"))
+    pb, eb, wb = (ops_b[k].numpy() for k in ("ptr", "ells", "wfl"))
+    out = np.zeros((cov.shape[0], len(pa) - 1, len(pb) - 1))
+    for p in range(len(pa) - 1):
+        l1 = ea[pa[p]:pa[p + 1]]
+        for q in range(len(pb) - 1):
+            l2 = eb[pb[q]:pb[q + 1]]
+            blk = cov[:, l1][:, :, l2]
+            out[:, p, q] = np.einsum("xij,i,j->x", blk, wa[l1], wb[l2])
+    return out
+
+
+def test_covariance_band_reduction_matches_the_reference_binning():
+    """gm_cov_binned's reduction over the bins' CSR lists equals the reference's binning
+    einsum (gmaster/covariance.py:533-538) with its output operator, for linear bands, ragged
+    bands with f_ell (D_l) and two different binnings."""
+    import oracle
+
+    rng = np.random.default_rng(9)
+    lmax = 30
+    cov = rng.normal(size=(3, lmax + 1, lmax + 1))
+    lin = NmtBin.from_lmax_linear(lmax, 4)
+    rag = NmtBin.from_edges([2, 5, 13, 20], [5, 13, 20, 31], is_Dell=True)
+    for ba, bb in ((lin, lin), (rag, lin), (lin, rag)):
+        got = _emulate_cov_binned(cov, ba.device_operators("cpu"), bb.device_operators("cpu"))
+
+        def output_op(b):
+            op = np.zeros((b.get_n_bands(), lmax + 1))
+            op[b._bpws_np, b._ells_np] = b._weights_np * b._f_ell_np
+            return op
+
+        want = np.einsum("pl,xlm,qm->xpq", output_op(ba), cov, output_op(bb))
+        np.testing.assert_allclose(got, want, rtol=1e-13, atol=1e-13)
+    out, _ = oracle.binning_operators(lmax, 4)
+    want = np.einsum("pl,xlm,qm->xpq", out, cov, out)
+    got = _emulate_cov_binned(cov, lin.device_operators("cpu"), lin.device_operators("cpu"))
+    np.testing.assert_allclose(got, want, rtol=1e-13, atol=1e-13)
