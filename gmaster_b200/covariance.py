@@ -12,6 +12,8 @@ Map-based spin-0 and spin-2 fields only: the catalog shot-noise terms and the fl
 variant of the reference are outside this build.
 """
 
+import itertools
+
 import numpy as np
 import torch
 
@@ -194,36 +196,28 @@ class NmtCovarianceWorkspace:
         off = (0, na * nc, na * nc + na * nd, na * nc + na * nd + nb * nc)
         kernels, kindex = [], {}
         rows, signs, bptr = [], [], [0]
-        for ia in range(na):
-            for ib in range(nb):
-                for ic in range(nc):
-                    for id_ in range(nd):
-                        for iap in range(na):
-                            for ibp in range(nb):
-                                for icp in range(nc):
-                                    for idp in range(nd):
-                                        for wick in range(2):
-                                            if wick == 0:
-                                                fa = _family(na, nc, ia, ic, iap, icp)
-                                                fb = _family(nb, nd, ib, id_, ibp, idp)
-                                                ra = off[0] + icp + nc * iap
-                                                rb = off[3] + idp + nd * ibp
-                                            else:
-                                                fa = _family(na, nd, ia, id_, iap, idp)
-                                                fb = _family(nb, nc, ib, ic, ibp, icp)
-                                                ra = off[1] + idp + nd * iap
-                                                rb = off[2] + icp + nc * ibp
-                                            sign, name = _paired(fa, fb)
-                                            xi = None if name is None else self.xiSS[wick][name]
-                                            if xi is None:
-                                                continue
-                                            key = (wick, name)
-                                            if key not in kindex:
-                                                kindex[key] = len(kernels)
-                                                kernels.append(xi)
-                                            rows.append((kindex[key], ra, rb))
-                                            signs.append(sign)
-                        bptr.append(len(rows))
+        outputs = itertools.product(range(na), range(nb), range(nc), range(nd))
+        for ia, ib, ic, id_ in outputs:
+            inputs = itertools.product(range(na), range(nb), range(nc), range(nd), range(2))
+            for iap, ibp, icp, idp, wick in inputs:
+                if wick == 0:   # <a1 b1><a2 b2>
+                    fa = _family(na, nc, ia, ic, iap, icp)
+                    fb = _family(nb, nd, ib, id_, ibp, idp)
+                    ra, rb = off[0] + icp + nc * iap, off[3] + idp + nd * ibp
+                else:           # <a1 b2><a2 b1>
+                    fa = _family(na, nd, ia, id_, iap, idp)
+                    fb = _family(nb, nc, ib, ic, ibp, icp)
+                    ra, rb = off[1] + idp + nd * iap, off[2] + icp + nc * ibp
+                sign, name = _paired(fa, fb)
+                xi = None if name is None else self.xiSS[wick][name]
+                if xi is None:
+                    continue
+                if (wick, name) not in kindex:
+                    kindex[wick, name] = len(kernels)
+                    kernels.append(xi)
+                rows.append((kindex[wick, name], ra, rb))
+                signs.append(sign)
+            bptr.append(len(rows))
         return kernels, rows, signs, bptr
 
     def gaussian_covariance(self, cla1b1, cla1b2, cla2b1, cla2b2, wa, wb=None, coupled=False):
