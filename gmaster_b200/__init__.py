@@ -7,8 +7,16 @@ sm_100a CUDA kernels (``libgm_b200.so``, C ABI in ``include/gm_b200.h``) on one 
 there is no CPU fallback.  Arrays are CUDA ``torch.Tensor``s.
 """
 
-from ._config import (get_default_params, get_precision, nmt_params, set_n_iter_default,
-                      set_precision, set_sht_calculator, set_tol_pinv_default)
+from . import utils
+from ._config import (get_default_params, get_precision, latitudinal_method, nmt_params,
+                      ring_dtype, set_latitudinal_method, set_n_iter_default, set_precision,
+                      set_ring_precision, set_sht_calculator, set_table_precision,
+                      set_tol_pinv_default, table_dtype)
+from .unsupported import (NmtBinFlat, NmtCovarianceWorkspaceFlat, NmtFieldCatalog,
+                          NmtFieldCatalogClustering, NmtFieldCatalogMomentum, NmtFieldFlat,
+                          NmtWorkspaceFlat, alm2catalog, catalog2alm, compute_coupled_cell_flat,
+                          compute_full_master_flat, deprojection_bias_flat,
+                          gaussian_covariance_flat, mask_apodization_flat, synfast_flat)
 from .batch import (SimulationGraph, compute_coupled_cells, decouple_cells, fields_from_maps,
                     mc_bandpowers, workspaces_from_fields)
 from .bins import NmtBin
@@ -22,6 +30,12 @@ from .workspaces import (NmtWorkspace, compute_coupled_cell, compute_full_master
                          uncorr_noise_deprojection_bias)
 
 __all__ = [
+    "utils", "latitudinal_method", "ring_dtype", "set_latitudinal_method", "set_ring_precision",
+    "set_table_precision", "table_dtype", "NmtBinFlat", "NmtCovarianceWorkspaceFlat",
+    "NmtFieldCatalog", "NmtFieldCatalogClustering", "NmtFieldCatalogMomentum", "NmtFieldFlat",
+    "NmtWorkspaceFlat", "alm2catalog", "catalog2alm", "compute_coupled_cell_flat",
+    "compute_full_master_flat", "deprojection_bias_flat", "gaussian_covariance_flat",
+    "mask_apodization_flat", "synfast_flat",
     "NmtAlmInfo", "NmtBin", "NmtCovarianceWorkspace", "NmtField", "NmtMapInfo", "NmtWorkspace",
     "alm2map", "gaussian_covariance", "get_iNKA_cell", "compute_full_master",
     "coupling_precision", "deprojection_bias", "get_general_coupling_matrix",

@@ -11,8 +11,8 @@ class NmtParams:
     tol_pinv_default : float
         Relative eigenvalue threshold of pseudo-inverses (kept for API parity).
     precision : str
-        ``"mixed"`` (default): single-precision ring stage and BF16-split / FP32
-        contraction with FP64 recurrence, accumulation and refinement.
+        ``"mixed"`` (default): single-precision ring stage and f16-split (tensor cores) /
+        FP32 (SIMT) contraction with FP64 recurrence, accumulation and refinement.
         ``"fp64"``: every stage in double precision.
     """
 
@@ -22,6 +22,9 @@ class NmtParams:
         self.tol_pinv_default = 1e-10
         self.precision = "mixed"
         self.sht_calculator = "gmaster_b200"
+        self.ring_precision = "auto"
+        self.table_dtype = "fp64"
+        self.latitudinal_method = "auto"
 
 
 nmt_params = NmtParams()
@@ -61,3 +64,63 @@ def get_precision():
 def set_sht_calculator(name):
     if name not in ("gmaster_b200", "ducc", "healpy", "jax"):
         raise KeyError(f"unknown SHT calculator {name}")
+
+
+# ----------------------------------------------------------------------------- engine knobs
+# The reference's transform-engine settings (gmaster/_config.py:57-268).  This build has
+# one latitudinal engine (the FP64-recurrence march, on SIMT or tensor-core kernels), no
+# stored transform tables (rows are generated on the fly) and a ring stage whose precision
+# follows `set_precision`; the settings are validated and recorded as in the reference.
+
+_RING_NAMES = ("auto", "follow", "fp64", "fp32")
+_TABLE_NAMES = ("fp64", "fp32")
+_LATITUDINAL = ("auto", "march", "dc")
+
+
+def set_ring_precision(name):
+    """Record the ring-FFT precision setting (gmaster/_config.py:113-133).  The ring
+    stage here runs in complex64 under the "mixed" precision and complex128 under "fp64"
+    (`set_precision`); `ring_dtype` reports which."""
+    if name not in _RING_NAMES:
+        raise KeyError("GMaster ring precision must be 'auto', 'follow', 'fp64' or 'fp32'")
+    nmt_params.ring_precision = name
+
+
+def ring_dtype(L=None):
+    """The element type of the ring FFTs the transforms use (gmaster/_config.py:74-110)."""
+    import torch
+
+    return torch.complex64 if nmt_params.precision == "mixed" else torch.complex128
+
+
+def set_table_precision(name):
+    """Record the table storage precision (gmaster/_config.py:202-226).  No transform
+    tables are stored here (the Legendre rows are generated in FP64 as they are used)."""
+    if name not in _TABLE_NAMES:
+        raise KeyError("GMaster table precision must be 'fp64' or 'fp32'")
+    nmt_params.table_dtype = name
+
+
+def table_dtype():
+    """The recorded table precision as a torch dtype (gmaster/_config.py:63-71)."""
+    import torch
+
+    return torch.float64 if nmt_params.table_dtype == "fp64" else torch.float32
+
+
+def latitudinal_method():
+    """The latitudinal engine setting (gmaster/_config.py:237-245)."""
+    return nmt_params.latitudinal_method
+
+
+def set_latitudinal_method(name):
+    """Choose the latitudinal engine (gmaster/_config.py:248-268): "auto" and "march" both
+    select this build's FP64-recurrence march; the divide-and-conquer engine ("dc") is
+    outside this build."""
+    if name not in _LATITUDINAL:
+        raise KeyError("latitudinal method must be 'auto', 'march' (fp32 v2 difference form), "
+                       "or 'dc' (divide-and-conquer)")
+    if name == "dc":
+        raise NotImplementedError("the divide-and-conquer latitudinal engine is not part of "
+                                  "this build")
+    nmt_params.latitudinal_method = name
