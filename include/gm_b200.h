@@ -8,9 +8,9 @@
  * synchronises the stream except where stated.
  *
  * Each declaration names the reference (licongxu/GMaster) interface it replaces.
- * The reference binds its kernels as XLA FFI handlers (gmaster/_native/cuda/*.cu)
- * or lowers the step to XLA library calls (cuFFT, cuBLAS, cuSOLVER, segment_sum);
- * INTEGRATION.md shows the jax.ffi / ctypes binding a maintainer adds.
+ * The reference binds its kernels as XLA FFI handlers (the .cu files under
+ * gmaster/_native/cuda) or lowers the step to XLA library calls (cuFFT, cuBLAS, cuSOLVER,
+ * segment_sum); a jax.ffi handler or a ctypes binding calls these entry points directly.
  *
  * Data layouts (all row-major, complex values interleaved re/im):
  *   maps      (ncomp, npix)                  float64 or float32, HEALPix RING order
