@@ -148,7 +148,8 @@ def workspaces_from_fields(field_pairs, bins, **kwargs):
     ``field_pairs`` is a list of (fl1, fl2); ``bins`` one NmtBin for every pair or a list
     of them.  The workspaces may differ in lmax and spins.  Scalar workspaces with the
     Toeplitz approximation keep their own launch (they compute only the entries the fill
-    reads); every other workspace takes its exact blocks from the shared launch.
+    reads), workspaces of purified fields their quadrature; every other workspace takes its
+    exact blocks from the shared launch.
     """
     pairs = list(field_pairs)
     if not isinstance(bins, (list, tuple)):
@@ -160,7 +161,9 @@ def workspaces_from_fields(field_pairs, bins, **kwargs):
         w = NmtWorkspace()
         w._prepare(f1, f2, b, **kwargs)
         wss.append(w)
-    shared = [w for w in wss if not (w.l_toeplitz > 0 and w.ncls == 1)]
+    # scalar Toeplitz workspaces compute only the entries their fill reads, and purified
+    # ones take all their blocks from the quadrature: neither needs the shared launch
+    shared = [w for w in wss if not (w.l_toeplitz > 0 and w.ncls == 1) and not w._pure_any]
     blocks = coupling_blocks_multi([w.window for w in shared], [w.lmax for w in shared],
                                    [_which(w.ncls) for w in shared])
     given = {id(w): bl for w, bl in zip(shared, blocks)}
