@@ -163,7 +163,8 @@ def workspaces_from_fields(field_pairs, bins, **kwargs):
         wss.append(w)
     # scalar Toeplitz workspaces compute only the entries their fill reads, and purified
     # ones take all their blocks from the quadrature: neither needs the shared launch
-    shared = [w for w in wss if not (w.l_toeplitz > 0 and w.ncls == 1) and not w._pure_any]
+    shared = [w for w in wss if not (w.l_toeplitz > 0 and w.ncls == 1) and not w._pure_any
+              and w.spin1 in (0, 2) and w.spin2 in (0, 2)]
     blocks = coupling_blocks_multi([w.window for w in shared], [w.lmax for w in shared],
                                    [_which(w.ncls) for w in shared])
     given = {id(w): bl for w, bl in zip(shared, blocks)}

@@ -109,8 +109,8 @@ class NmtField:
             spin = 0 if maps_t.shape[0] == 1 else 2
         if (spin == 0) != (maps_t.shape[0] == 1):
             raise ValueError("Spin-zero fields are associated with a single map")
-        if spin not in (0, 2):
-            raise NotImplementedError("only spin-0 and spin-2 fields are implemented")
+        if spin < 0 or spin > sht.MAX_SPIN:
+            raise NotImplementedError(f"fields of spin 0..{sht.MAX_SPIN} are implemented")
         self.spin = int(spin)
         self.nmaps = 1 if self.spin == 0 else 2
         pure_any = self.pure_e or self.pure_b

@@ -372,8 +372,6 @@ class NmtWorkspace:
                              f"({fl1.ainfo.lmax}) are not the same")
         if is_teb and (fl1.spin != 0 or fl2.spin == 0):
             raise ValueError("If is_teb=True, fl1 must be spin-0 and fl2 non-zero spin")
-        if is_teb and fl2.spin != 2:
-            raise NotImplementedError("only spin 0 and spin 2 fields are implemented")
         self.pure_e1, self.pure_b1 = bool(fl1.pure_e), bool(fl1.pure_b)
         self.pure_e2, self.pure_b2 = bool(fl2.pure_e), bool(fl2.pure_b)
         self._pure_any = self.pure_e1 or self.pure_b1 or self.pure_e2 or self.pure_b2
@@ -415,6 +413,9 @@ class NmtWorkspace:
         if getattr(self, "_pure_any", False):
             self._compute_pure_blocks()
             return
+        if self.spin1 not in (0, 2) or self.spin2 not in (0, 2):
+            self._compute_general_spin_blocks()
+            return
         if blocks is not None:
             self.mcm_blocks = blocks
         elif l_toeplitz > 0 and self.ncls == 1:
@@ -434,6 +435,53 @@ class NmtWorkspace:
             for x in slots:
                 self.mcm_blocks[x] = toeplitz_fill((self.mcm_blocks[x] / col).contiguous(),
                                                    self.lmax, l_toeplitz, l_exact, dl_band)
+
+    def _compute_general_spin_blocks(self):
+        """Blocks of workspaces with fields of spins other than 0 and 2 (workspaces.py:
+        1811-1831, 1856-1897): the spin-0 x spin-s block and the spin-s1 x spin-s2 M+ / M-
+        from the Gauss-Legendre quadrature of the general coupling matrix, the scalar block
+        of a TEB workspace from the 3j kernel; the slot signs depend on the spins."""
+        s1, s2, L = self.spin1, self.spin2, self.lmax
+        lm = self.lmax_mask
+        te = even = odd = None
+        if s1 == 0 or s2 == 0:
+            te = general_coupling_matrix(self.pcl_mask, s1, s2, s1, s2, L, lm).sum(0)
+        else:
+            even, odd = general_coupling_matrix(self.pcl_mask, s1, s2, s1, s2, L, lm)
+        if self.is_teb:
+            even, odd = general_coupling_matrix(self.pcl_mask, s2, s2, s2, s2, L, lm)
+        col = (2.0 * torch.arange(L + 1, dtype=torch.float64, device=self.window.device)
+               + 1.0)[None, :]
+        if self.l_toeplitz > 0:
+            def approx(x):
+                return None if x is None else toeplitz_fill((x / col).contiguous(), L,
+                                                             self.l_toeplitz, self.l_exact,
+                                                             self.dl_band)
+            te, even, odd = approx(te), approx(even), approx(odd)
+        slots = []
+        if self.ncls == 2:
+            sign = -1.0 if (s1 + s2) % 2 else 1.0
+            slots += [(te, 0, 0, sign), (te, 1, 1, sign)]
+        else:
+            offset = 3 if self.ncls == 7 else 0
+            if self.ncls == 7:
+                if self.l_toeplitz > 0:
+                    tt = coupling_tt_toeplitz(self.window, L, self.l_toeplitz, self.l_exact,
+                                              self.dl_band)
+                else:
+                    tt = coupling_blocks(self.window, L, 1)[_BLOCK_TT]
+                mixed = -1.0 if s2 % 2 else 1.0
+                slots += [(tt, 0, 0, 1.0), (te, 1, 1, mixed), (te, 2, 2, mixed)]
+                spin_sign = 1.0
+            else:
+                spin_sign = -1.0 if (s1 + s2) % 2 else 1.0
+            for index in range(4):
+                slots.append((even, offset + index, offset + index, spin_sign))
+            for index in range(4):
+                slots.append((odd, offset + index, offset + 3 - index,
+                              -spin_sign if index in (1, 2) else spin_sign))
+        self._slot_blocks = [(b.contiguous(), r, c, sg) for b, r, c, sg in slots]
+        self.mcm_blocks = None
 
     def _compute_pure_blocks(self):
         """Blocks of a workspace with purified fields (workspaces.py:1782-1897): all spin-2

@@ -153,3 +153,41 @@ def test_moore_penrose_pinvh(cuda):
     low = v @ v.T
     got = nmt.moore_penrose_pinvh(low, 1e-10).cpu().numpy()
     np.testing.assert_allclose(got, np.linalg.pinv(low, hermitian=True), rtol=1e-9, atol=1e-11)
+
+
+@pytest.mark.parametrize("spins,is_teb", [((0, 1), False), ((1, 0), False), ((1, 3), False),
+                                          ((3, 3), False), ((0, 3), True)])
+def test_arbitrary_spin_workspaces_match_oracle(cuda, spins, is_teb):
+    """Workspaces of spin-1 and spin-3 fields (the cases of the reference's
+    test_workspaces.py:429-458): coupling matrix and bandpowers against the oracle's
+    general quadrature and the reference's slot signs."""
+    nside, nlb = 8, 2
+    lmax = 3 * nside - 1
+    rng = np.random.default_rng(17)
+    masks = [rng.uniform(0.2, 1, 12 * nside ** 2), rng.uniform(0.2, 1, 12 * nside ** 2)]
+    fields = []
+    for mask, spin in zip(masks, spins):
+        maps = rng.normal(size=(1 if spin == 0 else 2, len(mask)))
+        fields.append(nmt.NmtField(mask, maps, spin=spin, lmax=lmax, lmax_mask=lmax, n_iter=0,
+                                   n_iter_mask=0, precision="fp64"))
+    b = nmt.NmtBin.from_lmax_linear(lmax, nlb)
+    w = nmt.NmtWorkspace.from_fields(*fields, b, is_teb=is_teb)
+    a1 = oracle.map2alm(masks[0][None], 0, nside, lmax, 0)
+    a2 = oracle.map2alm(masks[1][None], 0, nside, lmax, 0)
+    window = oracle.pcl(a1, a2, lmax)[0]
+    s1, s2 = spins
+    te = even = odd = None
+    if s1 == 0 or s2 == 0:
+        e, o = oracle.coupling_quadrature(window, lmax, s1, s2, s1, s2, lmax_mask=lmax)
+        te = e + o
+    else:
+        even, odd = oracle.coupling_quadrature(window, lmax, s1, s2, s1, s2, lmax_mask=lmax)
+    if is_teb:
+        even, odd = oracle.coupling_quadrature(window, lmax, s2, s2, s2, s2, lmax_mask=lmax)
+    tt = oracle.coupling_tt_closed(window, lmax)
+    want = oracle.assemble_general_mcm(te, even, odd, tt, lmax, s1, s2, is_teb)
+    assert _rel(w.get_coupling_matrix().cpu().numpy(), want) < 1e-10
+    ncls = w.ncls
+    cl = rng.random((ncls, lmax + 1))
+    ref = oracle.decouple(oracle.binned_mcm(want, lmax, nlb, ncls), cl, lmax, nlb)
+    assert _rel(w.decouple_cell(cl).cpu().numpy(), ref) < 1e-9

@@ -517,3 +517,74 @@ def test_public_names_cover_the_reference_api():
         nmt.set_ring_precision(old[0])
         nmt.set_table_precision(old[1])
         nmt.set_latitudinal_method(old[2])
+
+
+@pytest.mark.parametrize("spins,is_teb", [((0, 1), False), ((1, 0), False), ((1, 3), False),
+                                          ((3, 3), False), ((0, 3), True), ((1, 2), False),
+                                          ((0, 5), False)])
+def test_general_spin_slot_signs_match_the_reference_rule(monkeypatch, spins, is_teb):
+    """Slots and signs of workspaces with spins other than 0/2 (gmaster/workspaces.py:
+    1811-1831, 1856-1897), on the CPU with stand-in blocks for the quadrature (the
+    quadrature itself is GPU-tested against the oracle): the dense matrix equals the
+    oracle's restatement, and a file-style rebuild from it gives it back."""
+    import oracle
+    import torch
+
+    from gmaster_b200 import workspaces as wsm
+
+    rng = np.random.default_rng(sum(spins) + 7 * is_teb)
+    lmax = 5
+    n = lmax + 1
+    calls = {}
+
+    def fake_general(mask_cl, s1, s2, n1, n2, lm, lmm, table_bytes=None):
+        key = (s1, s2, n1, n2)
+        if key not in calls:
+            calls[key] = torch.from_numpy(rng.normal(size=(2, n, n)))
+        return calls[key]
+
+    tt = torch.from_numpy(rng.normal(size=(n, n)))
+
+    def fake_blocks(window, lm, which):
+        out = torch.zeros((4, n, n), dtype=torch.float64)
+        out[wsm._BLOCK_TT] = tt
+        return out
+
+    monkeypatch.setattr(wsm, "general_coupling_matrix", fake_general)
+    monkeypatch.setattr(wsm, "coupling_blocks", fake_blocks)
+    w = wsm.NmtWorkspace()
+    w.spin1, w.spin2 = spins
+    w.is_teb = is_teb
+    w.ncls = 7 if is_teb else (2 if 0 in spins else 4)
+    w.lmax = w.lmax_mask = lmax
+    w.pcl_mask = torch.zeros(n, dtype=torch.float64)
+    w.window = w.pcl_mask
+    w.l_toeplitz = w.l_exact = w.dl_band = -1
+    w._pure_any = False
+    w._compute_blocks()
+    got = w.get_coupling_matrix().numpy()
+    s1, s2 = spins
+    te = even = odd = None
+    if s1 == 0 or s2 == 0:
+        te = calls[(s1, s2, s1, s2)].sum(0).numpy()
+    else:
+        even, odd = (x.numpy() for x in calls[(s1, s2, s1, s2)])
+    if is_teb:
+        even, odd = (x.numpy() for x in calls[(s2, s2, s2, s2)])
+    want = oracle.assemble_general_mcm(te, even, odd, tt.numpy(), lmax, s1, s2, is_teb)
+    np.testing.assert_allclose(got, want, rtol=0, atol=1e-15)
+    slots = wsm._slot_blocks_from_dense(got, lmax, w.ncls, "cpu")
+    w._slot_blocks = slots
+    np.testing.assert_allclose(w.get_coupling_matrix().numpy(), want, rtol=0, atol=1e-15)
+
+
+def test_oracle_general_assembly_reduces_to_the_spin2_assembly():
+    import oracle
+
+    rng = np.random.default_rng(3)
+    n = 5
+    te, even, odd, tt = (rng.normal(size=(n, n)) for _ in range(4))
+    for s1, s2 in ((0, 2), (2, 0), (2, 2), (0, 0)):
+        blocks = {"tt": tt, "te": te, "pp": even, "mm": odd}
+        np.testing.assert_array_equal(oracle.assemble_general_mcm(te, even, odd, tt, n - 1, s1, s2),
+                                      oracle.assemble_mcm(blocks, n - 1, s1, s2))
