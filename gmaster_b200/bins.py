@@ -24,31 +24,45 @@ class NmtBin:
     """
 
     def __init__(self, *, bpws, ells, lmax=None, weights=None, f_ell=None):
-        ells = np.asarray(ells, dtype=np.int32)
-        bpws = np.asarray(bpws, dtype=np.int32)
-        if ells.ndim != 1 or bpws.shape != ells.shape or not len(ells):
-            raise ValueError("ells and bpws must be non-empty 1-D arrays of equal size")
-        self.lmax = int(np.max(ells) if lmax is None else lmax)
-        weights = np.ones(len(ells)) if weights is None else np.asarray(weights)
-        f_ell = np.ones(len(ells)) if f_ell is None else np.asarray(f_ell)
-        if weights.shape != ells.shape or f_ell.shape != ells.shape:
-            raise ValueError("weights and f_ell must have the same shape as ells")
-        keep = (ells <= self.lmax) & (bpws >= 0)
-        ells, bpws = ells[keep], bpws[keep]
-        weights = np.asarray(weights[keep], dtype=np.float64)
-        f_ell = np.asarray(f_ell[keep], dtype=np.float64)
-        n_bands = int(np.max(bpws, initial=0)) + 1
-        totals = np.bincount(bpws, weights=weights, minlength=n_bands)
-        if np.any(totals <= 0):
-            bad = int(np.flatnonzero(totals <= 0)[0])
-            raise RuntimeError(f"Weights in band {bad} are wrong")
-        weights /= totals[bpws]
-        f_ell = np.where(f_ell > 0, f_ell, 1.0)
-        self.n_bands = n_bands
-        self.ell_max = self.lmax
-        self._ells_np, self._bpws_np = ells, bpws
-        self._weights_np, self._f_ell_np = weights, f_ell
+        # The definition: entries (l, b, w, f) with b >= 0 and l <= lmax take part; within a
+        # band the weights are divided by their sum; f <= 0 means "no factor" (f = 1).
+        table = self._entry_table(ells, bpws, weights, f_ell)
+        if lmax is None:
+            lmax = table["l"].max()
+        self.lmax = self.ell_max = int(lmax)
+        table = table[(table["b"] >= 0) & (table["l"] <= self.lmax)]
+        self.n_bands = int(table["b"].max()) + 1 if len(table) else 1
+        band_sum = np.zeros(self.n_bands)
+        np.add.at(band_sum, table["b"], table["w"])
+        empty = np.nonzero(~(band_sum > 0))[0]
+        if len(empty):
+            raise RuntimeError(f"Weights in band {int(empty[0])} are wrong")
+        self._ells_np = np.ascontiguousarray(table["l"])
+        self._bpws_np = np.ascontiguousarray(table["b"])
+        self._weights_np = table["w"] / band_sum[table["b"]]
+        self._f_ell_np = np.where(table["f"] > 0, table["f"], 1.0)
         self._dev = {}
+
+    @staticmethod
+    def _entry_table(ells, bpws, weights, f_ell):
+        """The constructor's inputs as one structured array (l, b, w, f), checked for
+        shape: ells and bpws non-empty 1-D of one length, weights and f_ell (default 1)
+        of that length too."""
+        l_arr = np.asarray(ells, dtype=np.int32)
+        b_arr = np.asarray(bpws, dtype=np.int32)
+        n = l_arr.shape[0] if l_arr.ndim == 1 else -1
+        if n <= 0 or b_arr.shape != (n,):
+            raise ValueError("ells and bpws must be non-empty 1-D arrays of equal size")
+        cols = []
+        for extra in (weights, f_ell):
+            col = np.ones(n) if extra is None else np.asarray(extra)
+            if col.shape != (n,):
+                raise ValueError("weights and f_ell must have the same shape as ells")
+            cols.append(col.astype(np.float64))
+        table = np.empty(n, dtype=[("l", np.int32), ("b", np.int32), ("w", np.float64),
+                                   ("f", np.float64)])
+        table["l"], table["b"], table["w"], table["f"] = l_arr, b_arr, cols[0], cols[1]
+        return table
 
     def _fits_table(self, extname="BANDPOWERS"):
         """The bandpower table of workspace files (gmaster/bins.py:288-302): one row per l

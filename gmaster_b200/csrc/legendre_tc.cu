@@ -1287,7 +1287,10 @@ namespace ltc {
 constexpr int64_t kNoAllocLaneSlots = 148 * 4096;
 static __device__ __align__(256) double g_ana_state[kNoAllocLaneSlots * 3];
 
-// Device address of g_ana_state, looked up once per device with that device current.
+// Device address of g_ana_state, looked up once per device with that device current and
+// kept for the life of the process.  The cached address belongs to the device's context at
+// the time of the lookup: it does not survive cudaDeviceReset (or any teardown of that
+// context), after which this entry point must not be called again in the same process.
 static double *noalloc_state_ptr(int dev, cudaError_t &err)
 {
     static std::mutex mu;
@@ -1315,7 +1318,9 @@ extern "C" int gm_tc_analysis_noalloc(int64_t nside, int64_t lmax, int spin, int
                                       const void *img, double *alm_i, double scale, int64_t nctas,
                                       int32_t *err, void *stream)
 {
-    if (nside < 1 || nctas < 1 || nctas * 2 * nside > gm::ltc::kNoAllocLaneSlots) {
+    // compared by division so that no product of caller values can wrap around
+    if (nside < 1 || nctas < 1 || nctas > gm::ltc::kNoAllocLaneSlots ||
+        nside > gm::ltc::kNoAllocLaneSlots / (2 * nctas)) {
         gm::set_error_msg("gm_tc_analysis_noalloc: nctas * 2 * nside exceeds the 606208 lane slots "
                           "of the static scratch (e.g. at most 148 CTAs at Nside 2048)");
         return GM_ERR_BAD_SHAPE;

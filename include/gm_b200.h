@@ -288,7 +288,9 @@ int gm_tc_analysis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
  * Nside 2048), held by every GPU that loads the library until the process exits; calls with
  * nctas * 2 * nside above 606208 return GM_ERR_BAD_SHAPE.  The first call on a device looks
  * up the array's device address with that device current; make that first call before any
- * stream capture.  The array keeps the last call's contents (nothing in it needs clearing)
+ * stream capture.  That address is kept for the life of the process and does not survive a
+ * cudaDeviceReset of the device (or any other teardown of its context): do not call this
+ * entry point again after one.  The array keeps the last call's contents (nothing in it needs clearing)
  * and calls that overlap on the GPU race on it.  Inputs and outputs as gm_tc_analysis: the
  * caller zeroes alm_i before the first accumulation and *err before the call. */
 int gm_tc_analysis_noalloc(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,

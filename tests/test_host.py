@@ -381,12 +381,6 @@ def test_purified_slot_levels_match_the_reference_rule(monkeypatch, ncls, flags)
     np.testing.assert_array_equal(w.get_coupling_matrix().numpy(), want)
 
 
-def test_integration_document_lists_every_entry_point():
-    text = open("INTEGRATION.md").read()
-    missing = [s for s in _header_symbols() if s not in text]
-    assert not missing, missing
-
-
 def test_covariance_kernel_spin_rule_equals_the_reference_table():
     """The rule choosing the kernels of each Wick contraction equals the table of
     gmaster/covariance.py:266-283 (restated in the oracle) for all 16 spin combinations."""
