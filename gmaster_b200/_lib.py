@@ -99,6 +99,16 @@ SIGNATURES = {
                        _c_int),
     "gm_mask_apodize": ([_c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_dbl, _c_int, _c_vp, _c_vp],
                         _c_int),
+    "gm_ck_offsets": ([_c_i64, _c_int, _c_vp, _c_vp], _c_int),
+    "gm_ck_table_entries": ([_c_i64, _c_i64, _c_int], _c_i64),
+    "gm_ck_build": ([_c_i64, _c_i64, _c_int, _c_int, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],
+                    _c_int),
+    "gm_ck_analysis": ([_c_i64, _c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
+                        _c_vp, _c_vp, _c_dbl, _c_i64, _c_vp, _c_vp], _c_int),
+    "gm_ck_syn_chunk_offsets": ([_c_i64, _c_int, _c_vp], _c_int),
+    "gm_ck_prep_syn": ([_c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_i64, _c_dbl, _c_vp], _c_int),
+    "gm_ck_synthesis": ([_c_i64, _c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
+                         _c_vp, _c_vp, _c_dbl, _c_vp, _c_vp], _c_int),
 }
 
 STATUS = {0: "GM_OK", 1: "GM_ERR_BAD_SHAPE", 2: "GM_ERR_BAD_PTR", 3: "GM_ERR_LAUNCH",
@@ -114,7 +124,8 @@ LAUNCHES = {"gm_last_error": 0, "gm_version": 0, "gm_ring_twiddle_count": 0,
             "gm_seed_table_len": 0, "gm_bin_coupling_csr": 3, "gm_tc_lane_groups": 0,
             "gm_tc_ana_image_bytes": 0, "gm_tc_ana_scratch_bytes": 0,
             "gm_tc_syn_chunk_offsets": 0, "gm_tc_syn_image_bytes": 0, "gm_legendre_tiles": 0,
-            "gm_coupling_units": 0, "gm_ring_big_scratch_bytes": 0}
+            "gm_coupling_units": 0, "gm_ring_big_scratch_bytes": 0, "gm_ck_offsets": 0,
+            "gm_ck_table_entries": 0, "gm_ck_syn_chunk_offsets": 0}
 CALLS = {}
 
 

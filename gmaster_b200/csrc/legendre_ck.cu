@@ -1,0 +1,820 @@
+// Checkpointed Legendre / Wigner-d contraction on the tcgen05 tensor cores (sm_100a).
+//
+// The rows lambda^{s'}_lm(theta) are generated in single precision by the three-term
+// recurrence in its difference form
+//     C_l = c1_l (x - 1) + E_l,   D_l = b_l D_{l-1} + C_l v_{l-1},   v_l = v_{l-1} + D_l
+// (c1 = alpha, b = beta, E = alpha - beta - 1 - alpha s'c0/|s'|; algebraically the same as
+// v_l = alpha (x - c) v_{l-1} - beta v_{l-2}), restarted every kSeg = 128 rows from a
+// state computed once per geometry by the FP64 recurrence (the checkpoint table).  The
+// difference form keeps each rounding unamplified near the poles and turning points, where
+// the plain form multiplies it by 1/sin(phi) (phi the local oscillation phase); over 128 rows
+// from an exact start the FP32 rows stay within ~2e-6 of the row scale sqrt((2l+1)/4pi).
+// FP64 is kept for the checkpoint states, the seeds and the alm accumulation.
+//
+// Because every 128-row segment starts from the table, segments are independent:
+//   * the analysis splits each 256-row superblock between two sets of 4 generator warps
+//     (8 warps, twice the latency hiding of a single carried recurrence), and its work units
+//     (order m, superblock) are independent, so the CTAs that run the superblocks of one
+//     order at the same time share that order's right-hand-side images through L2 and each
+//     alm element is written by exactly one unit (no atomics);
+//   * the synthesis runs two sets of 8 generator warps on alternate segments.
+// A checkpoint stores the pre-state (v_{l_s - 1}, D_{l_s}) of the segment's first row l_s,
+// so that row is the uniform step with coefficients (c1, E, b) = (0, 0, 1).  The state is
+// kept in FP32 with a shift n in {0..5}: actual = stored * 2^(-64 n).  Lanes whose rows are
+// still far below 2^-16 (the seed region of high orders, where a segment can grow by 2^230)
+// carry n > 0, emit v * 2^(-64 n) and renormalise every 8 rows; a warp in which every lane
+// has n = 0 takes the plain path.  Segments whose state is below 2^-336 are stored as
+// zeros: they cannot reach 2^-40 within 128 rows.
+//
+// Operands and accumulation as legendre_tc.cu: f16 hi/lo operands, three products
+// (hi*hi + hi*lo + lo*hi) into separate hi*hi and cross-product TMEM accumulators, FP64
+// alm accumulation in the epilogue.
+//
+// Replaces gmaster/_native/cuda/march_v2.cu:155-407 (FP32 SIMT march with a two-word
+// difference form over all rows) for batched maps.
+#include <math.h>
+
+#include "gm_common.cuh"
+#include "ltc_common.cuh"
+#include "tc_common.cuh"
+
+namespace gm {
+namespace lck {
+
+using ltc::alm_idx;
+using ltc::Coef;
+using ltc::load_coef;
+using ltc::pack8;
+using ltc::sgn_of;
+using ltc::sts128;
+using ltc::wait_or_abort;
+
+constexpr int kSeg = 128;                           // rows per checkpoint segment
+constexpr int kMaxShift = 5;                        // largest stored shift n (2^-320)
+// analysis
+constexpr int kSB = 2 * kSeg;                       // superblock rows (one unit)
+constexpr int kHalf = 64;                           // rows per half-tile
+constexpr int kKC = 128;                            // lanes per group (MMA K per group)
+constexpr int kGenA = 256;                          // generator threads (8 warps, 2 sets)
+constexpr int kThrA = kGenA + 32;                   // + the producer / MMA warp
+constexpr int kMmaWarpA = kGenA / 32;
+constexpr uint32_t kAImg = 128u * kKC * 2u;         // one plane of a right-hand-side image (32 KB)
+constexpr uint32_t kHalfBytes = 2u * kHalf * kKC * 2u;   // half-tile: 64 hi + 64 lo rows (32 KB)
+constexpr int kStageLd = kSB + 1;                   // epilogue staging row stride (floats)
+// the epilogue stages 128 rows x kStageLd floats in the half-tiles and coefficient rows
+static_assert(128 * kStageLd * 4 <= 4 * kHalfBytes + kSB * 16, "epilogue staging does not fit");
+// synthesis
+constexpr int kLT = 256;                            // lanes per CTA (MMA N)
+constexpr int kKL = 64;                             // rows per chunk (MMA K)
+constexpr int kGenS = 2 * kLT;                      // generator threads (16 warps, 2 sets)
+constexpr int kThrS = kGenS + 32;
+constexpr int kMmaWarpS = kGenS / 32;
+constexpr uint32_t kSImg = 128u * kKL * 2u;         // one plane of an alm image (16 KB)
+constexpr uint32_t kBTileS = kLT * kKL * 2u;        // one plane of a generated tile (32 KB)
+
+struct CkParams {
+    int64_t nside, lmax, nlanes;
+    int sp;            // s' of the rows: 0, -2 or +2
+    int H;             // rows per half (maps x re/im); valid rows 2H <= 128
+    int NR;            // rows of the interleaved alm
+    int o0, o1;        // output row base of the first / second half (analysis)
+    double scale;      // analysis: alm += scale * result; synthesis: output scale
+    const double *geom;      // (3, nlanes): cos(theta), log2 sin(theta/2), log2 cos(theta/2)
+    const double *coef;      // (nelem, 4): alpha, beta, c0, 0
+    const int64_t *segoff;   // (L + 1): first checkpoint segment of each order
+    const int64_t *uoff;     // (L + 1): first analysis unit of each order
+    const float2 *ck;        // (segments, nlanes): pre-state (v_{l_s - 1}, D_{l_s}), scaled
+    const uint8_t *cn;       // (segments, nlanes): shift n
+};
+
+__host__ __device__ __forceinline__ int64_t first_row(int64_t m, int sp)
+{
+    const int64_t a = sp < 0 ? -sp : sp;
+    return m > a ? m : a;
+}
+
+// Difference-form coefficients of the step to row l of order m (coefficient base mb).
+__device__ __forceinline__ float4 diff_coef(const double *__restrict__ coef, int64_t mb, int64_t l,
+                                            int64_t L, double sgn_c, bool restart)
+{
+    if (restart) return make_float4(0.f, 0.f, 1.f, 0.f);   // D = D, v = v + D
+    if (l >= L) return make_float4(0.f, -1.f, 0.f, 0.f);   // v = 0 from here on
+    const Coef c = load_coef(coef, mb + l);
+    return make_float4((float)c.alpha, (float)(c.alpha - c.beta - 1.0 - sgn_c * c.alpha * c.c0),
+                       (float)c.beta, 0.f);
+}
+
+// A warp-uniform bounded wait: every lane waits, and the warp goes on only if all did.
+__device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity, volatile int *abort, int *err)
+{
+    const bool ok = wait_or_abort(bar, parity, abort, err);
+    return __all_sync(0xffffffffu, ok);
+}
+
+// One step of the FP32 difference form with coefficients q = (c1, E, b):
+//   C = c1 (x - 1) + E,  D <- C v + b D,  v <- v + D.
+// b D is formed off the dependent chain, so a row costs two dependent operations.
+__device__ __forceinline__ void diff_step(const float4 &q, float y, float &v, float &D)
+{
+    const float C = fmaf(q.x, y, q.y);
+    const float bD = q.z * D;
+    D = fmaf(C, v, bD);
+    v = v + D;
+}
+
+// Sixty-four rows of one lane (eight chunks of eight), split into f16 hi/lo and stored as
+// 16-byte chunks: chunk cc at base + ((cc ^ sw) << 4), its lo plane lo_delta bytes further.
+// SCALED: some lane of the warp still carries a shift n > 0 (decided once per 64 rows; a
+// lane's shift only decreases): such lanes emit v * 2^(-64 n) and renormalise every 8 rows.
+template <bool SCALED>
+__device__ __forceinline__ void gen64(const float4 *__restrict__ cw, float y, float &v, float &D, int &n,
+                                      uint32_t base, uint32_t lo_delta, uint32_t sw)
+{
+#pragma unroll 2
+    for (int cc = 0; cc < 8; ++cc) {
+        float vals[8];
+        if (SCALED) {
+            const float sc = n == 0 ? 1.0f : (n == 1 ? 0x1p-64f : 0.0f);
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                diff_step(cw[8 * cc + e], y, v, D);
+                vals[e] = v * sc;
+            }
+            // 8 rows grow a value by at most 2^63 (alpha <= sqrt(2m) + 1 at Nside <= 8192),
+            // so a renormalisation at 2^48 keeps every shifted value below 2^111
+            if (n != 0 && fabsf(v) > 0x1p48f) {
+                v *= 0x1p-64f;
+                D *= 0x1p-64f;
+                --n;
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                diff_step(cw[8 * cc + e], y, v, D);
+                vals[e] = v;
+            }
+        }
+        uint4 hi, lo;
+        pack8(vals, hi, lo);
+        const uint32_t off = ((uint32_t)cc ^ sw) << 4;
+        sts128(base + off, hi);
+        sts128(base + lo_delta + off, lo);
+    }
+}
+
+__device__ __forceinline__ void gen_rows64(const float4 *__restrict__ cw, float y, float &v, float &D,
+                                           int &n, uint32_t base, uint32_t lo_delta, uint32_t sw)
+{
+    if (__any_sync(0xffffffffu, n != 0)) gen64<true>(cw, y, v, D, n, base, lo_delta, sw);
+    else gen64<false>(cw, y, v, D, n, base, lo_delta, sw);
+}
+
+// ----------------------------------------------------------------------- checkpoint table
+
+// Stored checkpoint of an FP64 state: (vpre, d) * 2^(600 k) actual.
+__device__ __forceinline__ void ck_put(float2 *__restrict__ ck, uint8_t *__restrict__ cn, int64_t idx,
+                                       double vpre, double d, int k)
+{
+    const double mx = fmax(fabs(vpre), fabs(d));
+    float2 out = make_float2(0.f, 0.f);
+    int n = 0;
+    if (mx > 0.0) {
+        const int e = ilogb(mx) + 600 * k;   // floor(log2) of the actual largest entry
+        const int sh = e < -16 ? (-16 - e + 63) / 64 : 0;
+        if (sh <= kMaxShift) {
+            const int p = 600 * k + 64 * sh;
+            out = make_float2((float)ldexp(vpre, p), (float)ldexp(d, p));
+            n = sh;
+        }
+    }
+    ck[idx] = out;
+    cn[idx] = (uint8_t)n;
+}
+
+// One thread per (order m, lane): the FP64 recurrence with binary-exponent carry (the
+// recurrence of legendre_tc.cu), writing the pre-state of every segment's first row.
+__global__ void __launch_bounds__(128) k_ck_build(int64_t nside, int64_t lmax, int sp, int var,
+                                                  const double *__restrict__ geom,
+                                                  const double *__restrict__ seeds,
+                                                  const double *__restrict__ coef,
+                                                  const int64_t *__restrict__ segoff,
+                                                  float2 *__restrict__ ck, uint8_t *__restrict__ cn)
+{
+    const int64_t nlanes = 2 * nside, L = lmax + 1;
+    const int64_t m = blockIdx.y;
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t l0 = first_row(m, sp);
+    if (l0 > lmax || j >= nlanes) return;
+    const double sgn_c = sgn_of(sp);
+    const int64_t mb = alm_idx(lmax, 0, m);
+    const double x = geom[j];
+    double v, vp = 0.0;
+    int k;
+    ltc::seed_lane(seeds + ((int64_t)var * L + m) * 4, geom[nlanes + j], geom[2 * nlanes + j], v, k);
+    int64_t row = segoff[m] * nlanes + j;
+    ck_put(ck, cn, row, 0.0, v, k);   // the seed row: v_{l0 - 1} = 0
+    for (int64_t l = l0 + 1; l < L; ++l) {
+        const Coef c = load_coef(coef, mb + l);
+        const double a = c.alpha * (x - sgn_c * c.c0);
+        const double nv = fma(a, v, -c.beta * vp);
+        vp = v;
+        v = nv;
+        if (((l - l0) & (kSeg - 1)) == 0) {
+            row += nlanes;
+            ck_put(ck, cn, row, vp, v - vp, k);
+        }
+        if (((l - l0) & 7) == 0) ltc::rescale(v, vp, k);
+    }
+}
+
+// ------------------------------------------------------------------------------- analysis
+
+struct __align__(8) AnaShared {
+    uint64_t a_full, a_free, b_full[4], b_free[4], d_full, d_free, drain;
+    uint32_t tmem;
+    int abort;
+};
+
+// Order of analysis unit u: the last m with uoff[m] <= u.
+__device__ __forceinline__ int64_t unit_order(const int64_t *__restrict__ uoff, int64_t L, int64_t u)
+{
+    int64_t lo = 0, hi = L;   // uoff[lo] <= u < uoff[hi]
+    while (hi - lo > 1) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (__ldg(uoff + mid) <= u) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void gen_barrier_a() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+
+// Units (m, s): superblock s of order m covers rows l0 + 256 s + [0, 256).  CTA c takes
+// units c, c + G, ...; within a unit the lane groups g = 0..NG-1 stream their images
+// (one image buffer; set 0 generates rows [0, 128), set 1 rows [128, 256) into two
+// half-tiles each, each half-tile consumed by two MMAs per K step as in legendre_tc.cu).
+template <int SPIN>
+__global__ void __launch_bounds__(kThrA, 1) k_ana_ck(CkParams p, const uint8_t *__restrict__ aimg,
+                                                     double *__restrict__ alm_i, int *__restrict__ err)
+{
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ AnaShared sh;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t base = (tc::smem_u32(smem_raw) + 1023u) & ~1023u;
+    uint8_t *smem = smem_raw + (base - tc::smem_u32(smem_raw));
+    uint8_t *sA = smem;                                              // image: hi, lo planes
+    uint8_t *sB = smem + 2 * kAImg;                                  // 4 half-tiles
+    float4 *sCf = reinterpret_cast<float4 *>(sB + 4 * kHalfBytes);  // kSB coefficient rows
+    const int64_t L = p.lmax + 1, NG = (p.nlanes + kKC - 1) / kKC;
+    const int64_t U = p.uoff[L];
+    const int64_t G = gridDim.x, c = blockIdx.x;
+
+    if (tid == 0) {
+        tc::mbar_init(&sh.a_full, 1);
+        tc::mbar_init(&sh.a_free, 1);
+        for (int h = 0; h < 4; ++h) {
+            tc::mbar_init(&sh.b_full[h], 4);
+            tc::mbar_init(&sh.b_free[h], 1);
+        }
+        tc::mbar_init(&sh.d_full, 1);
+        tc::mbar_init(&sh.d_free, kGenA / 32);
+        tc::mbar_init(&sh.drain, 1);
+        sh.abort = 0;
+        tc::fence_mbar_init();
+    }
+    if (warp == kMmaWarpA) {
+        tc::tmem_alloc(&sh.tmem, 512);
+        tc::tmem_relinquish();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = sh.tmem;
+    volatile int *abort = &sh.abort;
+
+    if (warp == kMmaWarpA) {
+        // ------------------------------------------------ producer + MMA issuer
+        if (lane == 0) {
+            // concatenated MMA: hi image x [hi | lo] rows of a half-tile (N = 128) writes the
+            // hi*hi and hi*lo halves of the half-tile's 128 accumulator columns; the second
+            // adds lo image x hi rows (N = 64) into the cross half.  One image buffer: it is
+            // refilled when a group's MMAs are done, from L2, where the image was prefetched a
+            // group earlier (the CTAs running the superblocks of one order read the same
+            // images, so most of them find it there anyway).
+            const uint32_t idesc_cat = tc::idesc_f16(128, 2 * kHalf, 0, 1, 1);
+            const uint32_t idesc_hi = tc::idesc_f16(128, kHalf, 0, 1, 1);
+            uint32_t ja = 0, q = 0;
+            bool inflight = false, ok = true;
+            auto image = [&](int64_t m, int64_t g) { return aimg + ((m * NG + g) * 2) * (int64_t)kAImg; };
+            auto load_image = [&](int64_t m, int64_t g) {
+                tc::mbar_arrive_expect_tx(&sh.a_full, 2 * kAImg);
+                tc::bulk_g2s(sA, image(m, g), 2 * kAImg, &sh.a_full);
+                inflight = true;
+            };
+            if (c < U) load_image(unit_order(p.uoff, L, c), 0);
+            for (int64_t u = c; u < U && ok; u += G, ++q) {
+                const int64_t m = unit_order(p.uoff, L, u);
+                const int64_t mnext = u + G < U ? unit_order(p.uoff, L, u + G) : -1;
+                for (int64_t g = 0; g < NG && ok; ++g, ++ja) {
+                    // the group after this one: (m, g + 1) or group 0 of the next unit
+                    const bool more = g + 1 < NG || mnext >= 0;
+                    const int64_t mn = g + 1 < NG ? m : mnext, gn = g + 1 < NG ? g + 1 : 0;
+                    if (more) tc::prefetch_l2(image(mn, gn), 2 * kAImg);
+                    if (!(ok = wait_or_abort(&sh.a_full, ja & 1, abort, err))) break;
+                    inflight = false;
+                    if (g == 0 && !(ok = wait_or_abort(&sh.d_free, (q & 1) ^ 1, abort, err))) break;
+                    tc::tc_fence_after();
+                    const uint32_t a0 = tc::smem_u32(sA);
+                    for (int h = 0; h < 4; ++h) {
+                        if (!(ok = wait_or_abort(&sh.b_full[h], ja & 1, abort, err))) break;
+                        tc::tc_fence_after();
+                        const uint32_t b0 = tc::smem_u32(sB + h * kHalfBytes);
+                        const uint32_t dh = tmem + 128u * h, dx = dh + kHalf;
+#pragma unroll
+                        for (int ks = 0; ks < kKC / 16; ++ks) {
+                            const uint64_t ah = tc::desc_sw128_mn(a0 + ks * 4096, 1024, 2048);
+                            const uint64_t al = tc::desc_sw128_mn(a0 + kAImg + ks * 4096, 1024, 2048);
+                            const uint64_t bt = tc::desc_sw128_mn(b0 + ks * 4096, 1024, 2048);
+                            tc::mma_f16(dh, ah, bt, idesc_cat, (g > 0 || ks > 0) ? 1u : 0u);
+                            tc::mma_f16(dx, al, bt, idesc_hi, 1u);
+                        }
+                        tc::mma_commit(&sh.b_free[h]);
+                    }
+                    if (!ok) break;
+                    tc::mma_commit(&sh.a_free);
+                    if (g == NG - 1) tc::mma_commit(&sh.d_full);
+                    if (more) {
+                        // refill the image buffer once this group's MMAs have read it (the
+                        // generators run ahead into the freed half-tiles meanwhile)
+                        if (!(ok = wait_or_abort(&sh.a_free, ja & 1, abort, err))) break;
+                        load_image(mn, gn);
+                    }
+                }
+            }
+            // every issued MMA completes before TMEM is released, and an image copy still in
+            // flight lands before the CTA exits (both waits bounded)
+            tc::mma_commit(&sh.drain);
+            tc::mbar_wait(&sh.drain, 0);
+            if (inflight) tc::mbar_wait(&sh.a_full, ja & 1);
+        }
+    } else {
+        // ------------------------------------------------ generators + epilogue
+        const int S = warp >> 2;          // set: rows [128 S, 128 S + 128) of the superblock
+        const int t = tid & (kKC - 1);    // lane within the group (the MMA K index)
+        const double sgn_c = sgn_of(p.sp);
+        const uint32_t rowbase0 = tc::smem_u32(sB) + (t >> 3) * 2048 + (t & 7) * 128;
+        uint32_t jb = 0;
+        bool dead = false;
+        // this thread's coefficient row of a unit, loaded one unit ahead
+        auto unit_coef = [&](int64_t uu) {
+            const int64_t mm = unit_order(p.uoff, L, uu);
+            const int64_t lbb = first_row(mm, p.sp) + (uu - p.uoff[mm]) * kSB;
+            return diff_coef(p.coef, alm_idx(p.lmax, 0, mm), lbb + tid, L, sgn_c, (tid & (kSeg - 1)) == 0);
+        };
+        float4 ncoef = c < U ? unit_coef(c) : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int64_t u = c; u < U; u += G) {
+            const int64_t m = unit_order(p.uoff, L, u);
+            const int64_t s = u - p.uoff[m];
+            const int64_t lb = first_row(m, p.sp) + s * kSB;
+            const int64_t mb = alm_idx(p.lmax, 0, m);
+            // coefficient rows of the unit (the previous unit's rows are no longer read: every
+            // generator has passed its epilogue)
+            gen_barrier_a();
+            if (!dead) sCf[tid] = ncoef;
+            gen_barrier_a();
+            if (!dead && u + G < U) ncoef = unit_coef(u + G);
+            // the set's segment; the second half of an order's last superblock may lie past
+            // the order's last segment (all its rows are >= L): it then starts from zero
+            const int64_t seg = p.segoff[m] + 2 * s + S;
+            const bool has_seg = seg < p.segoff[m + 1];
+            const int64_t segrow = seg * p.nlanes;
+            // lane state of group g + 1 is loaded while group g is generated (converted only
+            // when used, so the loads do not stall the generation)
+            float2 nst = make_float2(0.f, 0.f);
+            int nn = 0;
+            double nx = 1.0;
+            auto fetch = [&](int64_t g) {
+                const int64_t j = g * kKC + t;
+                nst = make_float2(0.f, 0.f);
+                nn = 0;
+                nx = 1.0;
+                if (has_seg && j < p.nlanes) {   // padding lanes stay exactly zero
+                    nst = __ldg(p.ck + segrow + j);
+                    nn = __ldg(p.cn + segrow + j);
+                    nx = __ldg(p.geom + j);
+                }
+            };
+            if (!dead) fetch(0);
+            for (int64_t g = 0; g < NG; ++g, ++jb) {
+                if (dead) continue;
+                float v = nst.x, D = nst.y;
+                const float y = (float)(nx - 1.0);
+                int n = nn;
+                if (g + 1 < NG) fetch(g + 1);
+                for (int hh = 0; hh < 2; ++hh) {
+                    const int h = 2 * S + hh;
+                    if (!warp_wait(&sh.b_free[h], (jb & 1) ^ 1, abort, err)) {
+                        dead = true;
+                        break;
+                    }
+                    // half-tile: MN-major SW128 with 128 MN rows (64 hi rows, then 64 lo rows) and
+                    // 128 K lanes; a thread stores 8 consecutive rows of its lane as 16 bytes
+                    gen_rows64(sCf + kSeg * S + kHalf * hh, y, v, D, n, rowbase0 + h * kHalfBytes, 1024,
+                               (uint32_t)(t & 7));
+                    tc::fence_async_smem();
+                    __syncwarp();
+                    if (lane == 0) tc::mbar_arrive(&sh.b_full[h]);
+                }
+            }
+            // epilogue of the unit.  The two hemisphere halves of the image rows may add into
+            // the same alm row (spin 0), so the accumulators are staged in shared memory (the
+            // half-tiles and coefficient rows, free now) and each alm element then receives
+            // exactly one addition per launch, from one thread: the result does not depend
+            // on the order of the units.
+            const uint32_t q = (uint32_t)((u - c) / G);
+            if (!dead && !warp_wait(&sh.d_full, q & 1, abort, err)) dead = true;
+            float *stage = reinterpret_cast<float *>(sB);   // [128 rows][kStageLd] floats
+            if (!dead) {
+                tc::tc_fence_after();
+                const int row = 32 * (warp & 3) + lane;
+                for (int hh = 0; hh < 2; ++hh) {
+                    const int h = 2 * S + hh;
+                    for (int cb = 0; cb < kHalf; cb += 16) {
+                        uint32_t r[16], rx[16];
+                        const uint32_t ta = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + 128u * h + cb;
+                        tc::tmem_ld16(ta, r);
+                        tc::tmem_ld16(ta + kHalf, rx);
+                        tc::tmem_ld_wait();
+#pragma unroll
+                        for (int e = 0; e < 16; ++e)
+                            stage[row * kStageLd + kHalf * h + cb + e] =
+                                __uint_as_float(r[e]) + __uint_as_float(rx[e]);
+                    }
+                }
+                tc::tc_fence_before();
+            }
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(&sh.d_free);   // TMEM may be overwritten
+            gen_barrier_a();                               // every row staged
+            if (!dead) {
+                // output (row orow of the interleaved alm, row l = lb + i): the north image row
+                // orow - o0 and the south image row H + orow - o1 (with the hemisphere parity
+                // (-1)^(l + m)) where they exist; consecutive threads take consecutive orow
+                const int nout = p.NR * kSB;
+                for (int f = tid; f < nout; f += kGenA) {
+                    const int orow = f % p.NR, i = f / p.NR;
+                    const int64_t l = lb + i;
+                    if (l >= L) continue;
+                    const int rn = orow - p.o0, rs = orow - p.o1;
+                    double val = 0.0;
+                    if (rn >= 0 && rn < p.H) val += (double)stage[rn * kStageLd + i];
+                    if (rs >= 0 && rs < p.H) {
+                        const double sv = (double)stage[(p.H + rs) * kStageLd + i];
+                        val += ((l + m) & 1) ? -sv : sv;
+                    }
+                    // one reduction per element and launch (no return value: it does not wait)
+                    atomicAdd(alm_i + (mb + l) * p.NR + orow, val * p.scale);
+                }
+            }
+        }
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == kMmaWarpA) tc::tmem_dealloc(tmem, 512);
+}
+
+// ------------------------------------------------------------------------------ synthesis
+
+struct __align__(8) SynShared {
+    uint64_t a_full[2], a_free[2], b_full[2], b_free[2], d_full, drain;
+    uint32_t tmem;
+    int abort;
+};
+
+__device__ __forceinline__ void set_barrier_s(int set)
+{
+    asm volatile("bar.sync %0, 256;" ::"r"(2 + set) : "memory");
+}
+
+// One CTA per (order m, tile of 256 lanes).  Chunk cc of order m covers rows
+// l0 + 64 cc + [0, 64) (image index choff[m] + cc); segment k = chunks 2k, 2k + 1 is
+// generated by set k & 1 from its checkpoint.  D[row, lane] = sum_l almT[row, l] lambda_l(lane).
+template <int SPIN>
+__global__ void __launch_bounds__(kThrS, 1) k_syn_ck(CkParams p, const uint8_t *__restrict__ simg,
+                                                     const int64_t *__restrict__ choff,
+                                                     float *__restrict__ synd, int R2,
+                                                     int *__restrict__ err)
+{
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ SynShared sh;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t base = (tc::smem_u32(smem_raw) + 1023u) & ~1023u;
+    uint8_t *smem = smem_raw + (base - tc::smem_u32(smem_raw));
+    uint8_t *sA = smem;                                              // 2 x (hi, lo) alm images
+    uint8_t *sB = smem + 4 * kSImg;                                  // 2 sets x (hi, lo) tiles
+    float4 *sCf = reinterpret_cast<float4 *>(sB + 4 * kBTileS);     // 2 sets x kSeg rows
+    const int64_t L = p.lmax + 1;
+    const int64_t m = blockIdx.y, tile = blockIdx.x;
+    const int64_t l0 = first_row(m, p.sp);
+    if (l0 > p.lmax) return;
+    const int64_t nch = (L - l0 + kKL - 1) / kKL;
+
+    if (tid == 0) {
+        for (int i = 0; i < 2; ++i) {
+            tc::mbar_init(&sh.a_full[i], 1);
+            tc::mbar_init(&sh.a_free[i], 1);
+            tc::mbar_init(&sh.b_full[i], kLT / 32);
+            tc::mbar_init(&sh.b_free[i], 1);
+        }
+        tc::mbar_init(&sh.d_full, 1);
+        tc::mbar_init(&sh.drain, 1);
+        sh.abort = 0;
+        tc::fence_mbar_init();
+    }
+    if (warp == kMmaWarpS) {
+        tc::tmem_alloc(&sh.tmem, 512);
+        tc::tmem_relinquish();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = sh.tmem;
+    volatile int *abort = &sh.abort;
+    const uint8_t *img = simg + (choff[m] - choff[0]) * 2 * (int64_t)kSImg;
+
+    if (warp == kMmaWarpS) {
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_f16(128, kLT, 0, 1, 0);
+            bool ok = true;
+            int inflight = -1;          // buffer of an image copy not yet waited for
+            uint32_t inflight_ph = 0;   // and the phase it completes
+            tc::mbar_arrive_expect_tx(&sh.a_full[0], 2 * kSImg);
+            tc::bulk_g2s(sA, img, 2 * kSImg, &sh.a_full[0]);
+            inflight = 0;
+            for (int64_t cc = 0; cc < nch && ok; ++cc) {
+                const uint32_t a = (uint32_t)cc & 1, pha = (uint32_t)(cc >> 1) & 1;
+                const int S = (int)((cc >> 1) & 1);
+                const uint32_t phb = (uint32_t)(((cc >> 2) * 2 + (cc & 1)) & 1);
+                if (!(ok = wait_or_abort(&sh.a_full[a], pha, abort, err))) break;
+                inflight = -1;
+                if (!(ok = wait_or_abort(&sh.b_full[S], phb, abort, err))) break;
+                tc::tc_fence_after();
+                const uint32_t a0 = tc::smem_u32(sA + a * 2 * kSImg);
+                const uint32_t b0 = tc::smem_u32(sB + S * 2 * kBTileS);
+#pragma unroll
+                for (int ks = 0; ks < kKL / 16; ++ks) {
+                    const uint64_t ah = tc::desc_sw128_mn(a0 + ks * 4096, 1024, 2048);
+                    const uint64_t al = tc::desc_sw128_mn(a0 + kSImg + ks * 4096, 1024, 2048);
+                    const uint64_t bh = tc::desc_sw128(b0 + ks * 32);
+                    const uint64_t bl = tc::desc_sw128(b0 + kBTileS + ks * 32);
+                    const uint32_t acc = (cc > 0 || ks > 0) ? 1u : 0u;
+                    tc::mma_f16(tmem, ah, bh, idesc, acc);
+                    tc::mma_f16(tmem + kLT, ah, bl, idesc, acc);
+                    tc::mma_f16(tmem + kLT, al, bh, idesc, 1u);
+                }
+                tc::mma_commit(&sh.b_free[S]);
+                tc::mma_commit(&sh.a_free[a]);
+                if (cc + 1 < nch) {
+                    // the next chunk's image goes into the buffer of chunk cc - 1 once its MMAs are done
+                    const uint32_t nb = (uint32_t)(cc + 1) & 1;
+                    if (!(ok = wait_or_abort(&sh.a_free[nb], ((uint32_t)((cc + 1) >> 1) & 1) ^ 1, abort, err)))
+                        break;
+                    tc::mbar_arrive_expect_tx(&sh.a_full[nb], 2 * kSImg);
+                    tc::bulk_g2s(sA + nb * 2 * kSImg, img + (cc + 1) * 2 * (int64_t)kSImg, 2 * kSImg,
+                                 &sh.a_full[nb]);
+                    inflight = (int)nb;
+                    inflight_ph = (uint32_t)((cc + 1) >> 1) & 1;
+                }
+            }
+            if (ok) tc::mma_commit(&sh.d_full);
+            tc::mma_commit(&sh.drain);
+            tc::mbar_wait(&sh.drain, 0);
+            if (inflight >= 0) tc::mbar_wait(&sh.a_full[inflight], inflight_ph);
+        }
+    } else {
+        const int S = warp >> 3;              // set: segments k with k % 2 == S
+        const int t = tid & (kLT - 1);        // lane within the tile (the MMA N row)
+        const int64_t jl = tile * kLT + t;
+        const bool valid = jl < p.nlanes;
+        const double sgn_c = sgn_of(p.sp);
+        const int64_t mb = alm_idx(p.lmax, 0, m);
+        const float y = valid ? (float)(p.geom[jl] - 1.0) : 0.f;
+        float4 *cwin = sCf + kSeg * S;
+        const uint32_t b0 = tc::smem_u32(sB + S * 2 * kBTileS);
+        const uint32_t rowoff = (uint32_t)((t >> 3) * 1024 + (t & 7) * 128);
+        uint32_t js = 0;   // chunks generated by this set
+        bool dead = false;
+        // state and coefficient row of the set's next segment, loaded one segment ahead
+        float2 nst = make_float2(0.f, 0.f);
+        int nn = 0;
+        float4 ncoef = make_float4(0.f, 0.f, 0.f, 0.f);
+        auto fetch = [&](int64_t k) {
+            nst = make_float2(0.f, 0.f);
+            nn = 0;
+            if (2 * k >= nch) return;
+            if (valid) {
+                const int64_t idx = (p.segoff[m] + k) * p.nlanes + jl;
+                nst = __ldg(p.ck + idx);
+                nn = __ldg(p.cn + idx);
+            }
+            if (t < kSeg) ncoef = diff_coef(p.coef, mb, l0 + kSeg * k + t, L, sgn_c, t == 0);
+        };
+        fetch(S);
+        for (int64_t k = S; 2 * k < nch; k += 2) {
+            set_barrier_s(S);   // the set's previous segment is generated: its rows are free
+            if (!dead && t < kSeg) cwin[t] = ncoef;
+            set_barrier_s(S);
+            if (dead) continue;
+            float v = nst.x, D = nst.y;
+            int n = nn;
+            fetch(k + 2);
+            for (int half = 0; half < 2 && 2 * k + half < nch; ++half, ++js) {
+                if (!warp_wait(&sh.b_free[S], (js & 1) ^ 1, abort, err)) {
+                    dead = true;
+                    break;
+                }
+                // tile: K-major SW128, 256 N rows (lanes) of 64 K values (rows l)
+                gen_rows64(cwin + kKL * half, y, v, D, n, b0 + rowoff, kBTileS, (uint32_t)(t & 7));
+                tc::fence_async_smem();
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(&sh.b_full[S]);
+            }
+        }
+        // epilogue: D[row, lane] -> synd[m][lane][row]; warp w reads TMEM lanes 32 (w % 4)
+        // (rows) and the column quarter w / 4 (lanes)
+        if (!dead && warp_wait(&sh.d_full, 0, abort, err)) {
+            tc::tc_fence_after();
+            const int wq = warp & 3, row = wq * 32 + lane;
+            const int cbeg = (warp >> 2) * (kLT / 4);
+            for (int cb = cbeg; cb < cbeg + kLT / 4; cb += 16) {
+                uint32_t r[16], rx[16];
+                const uint32_t trow = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)cb;
+                tc::tmem_ld16(trow, r);
+                tc::tmem_ld16(trow + kLT, rx);
+                tc::tmem_ld_wait();
+                if (row < R2) {
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        const int64_t j2 = tile * kLT + cb + e;
+                        if (j2 < p.nlanes)
+                            synd[(m * p.nlanes + j2) * R2 + row] =
+                                (__uint_as_float(r[e]) + __uint_as_float(rx[e])) * (float)p.scale;
+                    }
+                }
+            }
+            tc::tc_fence_before();
+        }
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == kMmaWarpS) tc::tmem_dealloc(tmem, 512);
+}
+
+}  // namespace lck
+}  // namespace gm
+
+using namespace gm;
+using namespace gm::lck;
+
+static bool ck_spin_ok(int spin, int sp)
+{
+    return (spin == 0 && sp == 0) || (spin == 2 && (sp == 2 || sp == -2));
+}
+
+static int64_t ck_nseg(int64_t lmax, int spin, int64_t m)
+{
+    const int64_t l0 = first_row(m, spin);
+    return l0 <= lmax ? (lmax + 1 - l0 + kSeg - 1) / kSeg : 0;
+}
+
+extern "C" int gm_ck_offsets(int64_t lmax, int spin, int64_t *segoff_host, int64_t *uoff_host)
+{
+    if (lmax < 2 || lmax > 65535 || (spin != 0 && spin != 2)) return GM_ERR_BAD_SHAPE;
+    if (!segoff_host || !uoff_host) return GM_ERR_BAD_PTR;
+    int64_t s = 0, u = 0;
+    for (int64_t m = 0; m <= lmax; ++m) {
+        segoff_host[m] = s;
+        uoff_host[m] = u;
+        const int64_t n = ck_nseg(lmax, spin, m);
+        s += n;
+        u += (n + 1) / 2;
+    }
+    segoff_host[lmax + 1] = s;
+    uoff_host[lmax + 1] = u;
+    return GM_OK;
+}
+
+extern "C" int64_t gm_ck_table_entries(int64_t nside, int64_t lmax, int spin)
+{
+    if (nside < 1 || lmax < 2 || (spin != 0 && spin != 2)) return -1;
+    int64_t s = 0;
+    for (int64_t m = 0; m <= lmax; ++m) s += ck_nseg(lmax, spin, m);
+    return s * 2 * nside;
+}
+
+extern "C" int gm_ck_build(int64_t nside, int64_t lmax, int spin, int sp, const double *geom,
+                           const double *seeds, const double *coef, const int64_t *segoff,
+                           void *ck_state, uint8_t *ck_shift, void *stream)
+{
+    if (nside < 1 || lmax < 2 || lmax > 65535 || !ck_spin_ok(spin, sp)) return GM_ERR_BAD_SHAPE;
+    if (!geom || !seeds || !coef || !segoff || !ck_state || !ck_shift) return GM_ERR_BAD_PTR;
+    const int var = sp == 0 ? 0 : (sp < 0 ? 1 : 2);
+    dim3 grid((unsigned)((2 * nside + 127) / 128), (unsigned)(lmax + 1));
+    k_ck_build<<<grid, 128, 0, as_stream(stream)>>>(nside, lmax, sp, var, geom, seeds, coef, segoff,
+                                                    (float2 *)ck_state, ck_shift);
+    return check_launch("gm_ck_build");
+}
+
+static CkParams ck_params(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp, const double *geom,
+                          const double *coef, const int64_t *segoff, const int64_t *uoff,
+                          const void *ck_state, const uint8_t *ck_shift, double scale)
+{
+    CkParams p;
+    p.nside = nside;
+    p.lmax = lmax;
+    p.nlanes = 2 * nside;
+    p.sp = sp;
+    p.H = spin == 0 ? (int)(2 * ncomp) : (int)ncomp;
+    p.NR = spin == 0 ? p.H : 2 * p.H;
+    if (spin == 0) { p.o0 = 0; p.o1 = 0; }
+    else if (sp < 0) { p.o0 = 0; p.o1 = p.H; }
+    else { p.o0 = p.H; p.o1 = 0; }
+    p.scale = scale;
+    p.geom = geom;
+    p.coef = coef;
+    p.segoff = segoff;
+    p.uoff = uoff;
+    p.ck = (const float2 *)ck_state;
+    p.cn = ck_shift;
+    return p;
+}
+
+static bool ck_shape_ok(int spin, int64_t ncomp)
+{
+    if (spin == 0) return ncomp >= 1 && ncomp <= 32;
+    if (spin == 2) return ncomp >= 2 && ncomp <= 64 && ncomp % 2 == 0;
+    return false;
+}
+
+extern "C" int gm_ck_analysis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                              const double *geom, const double *coef, const int64_t *segoff,
+                              const int64_t *uoff, const void *ck_state, const uint8_t *ck_shift,
+                              const void *img, double *alm_i, double scale, int64_t nctas, int32_t *err,
+                              void *stream)
+{
+    if (nside < 1 || lmax < 2 || lmax > 65535 || !ck_shape_ok(spin, ncomp) || !ck_spin_ok(spin, sp) ||
+        nctas < 1 || nctas > 4096)
+        return GM_ERR_BAD_SHAPE;
+    if (!geom || !coef || !segoff || !uoff || !ck_state || !ck_shift || !img || !alm_i || !err)
+        return GM_ERR_BAD_PTR;
+    const size_t smem = 2 * kAImg + 4 * kHalfBytes + kSB * sizeof(float4) + 1024;
+    auto kern = spin == 0 ? k_ana_ck<0> : k_ana_ck<2>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) {
+        set_error("gm_ck_analysis attr", e);
+        return GM_ERR_LAUNCH;
+    }
+    CkParams p = ck_params(nside, lmax, spin, sp, ncomp, geom, coef, segoff, uoff, ck_state, ck_shift, scale);
+    kern<<<(unsigned)nctas, kThrA, smem, as_stream(stream)>>>(p, (const uint8_t *)img, alm_i, (int *)err);
+    return check_launch("gm_ck_analysis");
+}
+
+extern "C" int gm_ck_syn_chunk_offsets(int64_t lmax, int spin, int64_t *choff_host)
+{
+    if (lmax < 0 || (spin != 0 && spin != 2)) return GM_ERR_BAD_SHAPE;
+    if (!choff_host) return GM_ERR_BAD_PTR;
+    int64_t acc = 0;
+    for (int64_t m = 0; m <= lmax; ++m) {
+        choff_host[m] = acc;
+        const int64_t l0 = first_row(m, spin);
+        if (l0 <= lmax) acc += (lmax + 1 - l0 + kKL - 1) / kKL;
+    }
+    choff_host[lmax + 1] = acc;
+    return GM_OK;
+}
+
+extern "C" int gm_ck_synthesis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                               const double *geom, const double *coef, const int64_t *segoff,
+                               const void *ck_state, const uint8_t *ck_shift, const void *simg,
+                               const int64_t *choff, float *synd, double out_scale, int32_t *err,
+                               void *stream)
+{
+    if (nside < 1 || lmax < 2 || lmax > 65535 || !ck_shape_ok(spin, ncomp) || !ck_spin_ok(spin, sp) ||
+        !(out_scale > 0.0))
+        return GM_ERR_BAD_SHAPE;
+    if (!geom || !coef || !segoff || !ck_state || !ck_shift || !simg || !choff || !synd || !err)
+        return GM_ERR_BAD_PTR;
+    const size_t smem = 4 * kSImg + 4 * kBTileS + 2 * kSeg * sizeof(float4) + 1024;
+    auto kern = spin == 0 ? k_syn_ck<0> : k_syn_ck<2>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) {
+        set_error("gm_ck_synthesis attr", e);
+        return GM_ERR_LAUNCH;
+    }
+    CkParams p = ck_params(nside, lmax, spin, sp, ncomp, geom, coef, segoff, nullptr, ck_state, ck_shift,
+                           out_scale);
+    const int R2 = 2 * p.H;
+    dim3 grid((unsigned)((p.nlanes + kLT - 1) / kLT), (unsigned)(lmax + 1));
+    kern<<<grid, kThrS, smem, as_stream(stream)>>>(p, (const uint8_t *)simg, choff, synd, R2, (int *)err);
+    return check_launch("gm_ck_synthesis");
+}

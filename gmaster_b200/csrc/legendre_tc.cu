@@ -27,6 +27,7 @@
 
 #include "gm_common.cuh"
 #include "tc_common.cuh"
+#include "ltc_common.cuh"
 
 namespace gm {
 namespace ltc {
@@ -46,90 +47,6 @@ constexpr uint32_t kAImg = 128u * kKC * 2u;        // one plane of an analysis A
 constexpr uint32_t kBTileA = kNB * kKC * 2u;       // one plane of an analysis B tile (32 KB)
 constexpr uint32_t kSImg = 128u * kKL * 2u;        // one plane of a synthesis A image (16 KB)
 constexpr uint32_t kBTileS = kLT * kKL * 2u;       // one plane of a synthesis B tile (32 KB)
-constexpr double kBig = 2.037035976334486e90;      // 2^300
-constexpr double kShrink = 2.409919865102884e-181; // 2^-600
-
-struct Coef {
-    double alpha, beta, c0;
-};
-
-__device__ __forceinline__ int64_t alm_idx(int64_t lmax, int64_t l, int64_t m)
-{
-    return m * (2 * lmax + 1 - m) / 2 + l;
-}
-
-__device__ __forceinline__ void seed_lane(const double *__restrict__ sd, double lsin, double lcos,
-                                          double &v, int &k)
-{
-    double f = sd[0];
-    if (sd[2] != 0.0) f += sd[2] * lcos;
-    if (sd[3] != 0.0) f += sd[3] * lsin;
-    if (!(f > -1.0e300)) {
-        v = 0.0;
-        k = 0;
-        return;
-    }
-    int kk = 0;
-    if (f < -300.0) kk = (int)floor((f + 300.0) / 600.0);
-    v = sd[1] * exp2(f - 600.0 * (double)kk);
-    k = kk;
-}
-
-// One recurrence step to degree l (> l0) using coefficients for (l, m); sgn_c selects
-// x - c0 (s' = +2), x + c0 (s' = -2) or x (s' = 0, c0 = 0).  Written so that a single
-// FMA sits on the dependent chain: a = alpha (x - c) and b = beta v_{l-2} do not depend on
-// v_{l-1}.
-__device__ __forceinline__ void step(double x, const Coef &c, double sgn_c, double &v, double &vp)
-{
-    const double a = c.alpha * (x - sgn_c * c.c0);
-    const double b = c.beta * vp;
-    const double nv = fma(a, v, -b);
-    vp = v;
-    v = nv;
-}
-
-// Binary-exponent carry, applied once per 8 steps: a lane still below 2^-300 (k < 0) is
-// renormalised when it passes 2^300 (growth over 8 steps stays far below 2^700).
-__device__ __forceinline__ void rescale(double &v, double &vp, int &k)
-{
-    if (k < 0 && fabs(v) > kBig) {
-        v *= kShrink;
-        vp *= kShrink;
-        ++k;
-    }
-}
-
-// Coefficient table entries are 32 bytes: (alpha, beta) then (c0, 0), so one 16-byte load
-// fetches (alpha, beta).
-__device__ __forceinline__ Coef load_coef(const double *__restrict__ tab, int64_t idx)
-{
-    const double2 ab = __ldg(reinterpret_cast<const double2 *>(tab) + 2 * idx);
-    Coef c;
-    c.alpha = ab.x;
-    c.beta = ab.y;
-    c.c0 = __ldg(tab + 4 * idx + 2);
-    return c;
-}
-
-// Operands are f16 hi/lo pairs (22 significant bits; the products hi*hi + hi*lo + lo*hi
-// run as three kind::f16 MMAs).  The generated rows are bounded by sqrt((2l+1)/4pi); the
-// right-hand-side and alm images are scaled by a power of two so their largest entry sits
-// near 2^13.
-__device__ __forceinline__ void pack8(const float (&v)[8], uint4 &hi, uint4 &lo)
-{
-    tc::split_f16x2(v[0], v[1], hi.x, lo.x);
-    tc::split_f16x2(v[2], v[3], hi.y, lo.y);
-    tc::split_f16x2(v[4], v[5], hi.z, lo.z);
-    tc::split_f16x2(v[6], v[7], hi.w, lo.w);
-}
-
-__device__ __forceinline__ void sts128(uint32_t addr, const uint4 &v)
-{
-    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(v.x), "r"(v.y), "r"(v.z),
-                 "r"(v.w)
-                 : "memory");
-}
-
 struct Params {
     int64_t nside, lmax, nlanes;
     int sp;          // s' of the rows: 0, -2 or +2
@@ -147,8 +64,6 @@ struct Params {
 __device__ __forceinline__ void gen_barrier() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 __device__ __forceinline__ void gen_barrier_s() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 
-__device__ __forceinline__ double sgn_of(int sp) { return sp > 0 ? 1.0 : (sp < 0 ? -1.0 : 0.0); }
-
 // ------------------------------------------------------------------------------- analysis
 
 struct __align__(8) AnaShared {
@@ -156,16 +71,6 @@ struct __align__(8) AnaShared {
     uint32_t tmem;
     int abort;
 };
-
-__device__ __forceinline__ bool wait_or_abort(uint64_t *bar, uint32_t parity, volatile int *abort,
-                                              int *err)
-{
-    if (*abort) return false;
-    if (tc::mbar_wait(bar, parity)) return true;
-    *abort = 1;
-    atomicExch(err, 1);
-    return false;
-}
 
 // The m handled in slot i of CTA c (snake order over gridDim.x CTAs).
 __device__ __forceinline__ int64_t snake_m(int64_t i, int64_t c, int64_t G)
@@ -771,15 +676,18 @@ __global__ void __launch_bounds__(128) k_pack_tc(int64_t nside, int64_t L, int n
 // Synthesis operand images from the interleaved alm (nelem, NR) float64.
 // Rows: spin 0 [a | s a] (src row r mod H); spin 2 variant -2 (lambda+): [2a | s -2a]
 // (src row r); variant +2 (lambda-): [-2a | s 2a] (src r < H ? H + r : r - H); s = (-1)^(l+m).
+// With `rel` set the chunks start at the order's first row instead: chunk cc covers
+// l0 + 64 cc + [0, 64) (the layout of the checkpointed synthesis, legendre_ck.cu).
 __global__ void k_prep_syn(int64_t lmax, int spin, int sp, int H, int NR,
                            const double *__restrict__ alm_i, const int64_t *__restrict__ choff,
-                           uint8_t *__restrict__ simg, double scale, int64_t mbeg)
+                           uint8_t *__restrict__ simg, double scale, int64_t mbeg, int rel)
 {
     const int64_t m = mbeg + blockIdx.y, L = lmax + 1;
     const int l0min = abs(sp);
     const int64_t l0 = m > l0min ? m : l0min;
     if (l0 > lmax) return;
-    const int64_t c0 = l0 / kKL, nch = (L + kKL - 1) / kKL - c0;
+    const int64_t lfirst = rel ? l0 : (l0 / kKL) * kKL;   // first row of chunk 0
+    const int64_t nch = (L - lfirst + kKL - 1) / kKL;
     const int64_t mb = alm_idx(lmax, 0, m);
     // thread -> (chunk cc, l within chunk, 8-row group)
     const int64_t per = (int64_t)kKL * 16;
@@ -787,7 +695,7 @@ __global__ void k_prep_syn(int64_t lmax, int spin, int sp, int H, int NR,
          t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t cc = t / per;
         const int kl = (int)((t % per) / 16), r0 = (int)(t % 16) * 8;
-        const int64_t l = (c0 + cc) * kKL + kl;
+        const int64_t l = lfirst + cc * kKL + kl;
         float v[8];
         const bool lok = l >= l0 && l < L;
         const double sgn = ((l + m) & 1) ? -1.0 : 1.0;
@@ -1177,8 +1085,28 @@ extern "C" int gm_tc_prep_syn_window(int64_t lmax, int spin, int sp, int64_t nco
         return GM_ERR_LAUNCH;
     }
     k_prep_syn<<<dim3(16, (unsigned)(mend - mbeg)), 256, 0, s>>>(lmax, spin, sp, H, NR, alm_i, choff,
-                                                                (uint8_t *)simg, alm_scale, mbeg);
+                                                                (uint8_t *)simg, alm_scale, mbeg, 0);
     return check_launch("gm_tc_prep_syn");
+}
+
+extern "C" int gm_ck_prep_syn(int64_t lmax, int spin, int sp, int64_t ncomp, const double *alm_i,
+                              const int64_t *choff, void *simg, int64_t simg_bytes, double alm_scale,
+                              void *stream)
+{
+    if (lmax < 2 || !tc_shape_ok(spin, ncomp) || !(alm_scale > 0.0)) return GM_ERR_BAD_SHAPE;
+    if ((spin == 0) != (sp == 0) || (spin == 2 && sp != 2 && sp != -2)) return GM_ERR_BAD_SHAPE;
+    if (!alm_i || !choff || !simg) return GM_ERR_BAD_PTR;
+    const int H = spin == 0 ? (int)(2 * ncomp) : (int)ncomp;
+    const int NR = spin == 0 ? H : 2 * H;
+    cudaStream_t s = as_stream(stream);
+    cudaError_t e = cudaMemsetAsync(simg, 0, (size_t)simg_bytes, s);
+    if (e != cudaSuccess) {
+        set_error("gm_ck_prep_syn memset", e);
+        return GM_ERR_LAUNCH;
+    }
+    k_prep_syn<<<dim3(16, (unsigned)(lmax + 1)), 256, 0, s>>>(lmax, spin, sp, H, NR, alm_i, choff,
+                                                              (uint8_t *)simg, alm_scale, 0, 1);
+    return check_launch("gm_ck_prep_syn");
 }
 
 extern "C" int gm_tc_prep_syn(int64_t lmax, int spin, int sp, int64_t ncomp, const double *alm_i,

@@ -87,6 +87,12 @@ __device__ __forceinline__ void bulk_g2s(void *smem_dst, const void *gmem_src, u
         : "memory");
 }
 
+// Prefetch `bytes` of global memory into L2 (16-byte aligned address, size a multiple of 16).
+__device__ __forceinline__ void prefetch_l2(const void *gmem_src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(gmem_src), "r"(bytes) : "memory");
+}
+
 // Make generic-proxy shared-memory writes visible to the async proxy (tcgen05.mma reads).
 __device__ __forceinline__ void fence_async_smem()
 {

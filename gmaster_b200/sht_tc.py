@@ -18,6 +18,12 @@ from . import _lib, sht
 MAX_MAPS_SPIN0 = 32
 MAX_FIELDS_SPIN2 = 32
 
+# The checkpointed kernels (legendre_ck.cu) restart the single-precision recurrence from a
+# per-geometry table every 128 rows; the tables of one geometry (all row variants) may take
+# at most this share of the device memory, else the carried-state kernels run.
+USE_CHECKPOINTS = True
+CK_MEMORY_SHARE = 0.2
+
 _TC_PLANS = {}
 _LOCK = threading.Lock()
 
@@ -42,6 +48,23 @@ class TCPlan:
             self.choff[spin] = torch.from_numpy(host).to(dev)
             self.choff_host[spin] = host
             self.nchunks[spin] = int(host[-1])
+        # checkpoint tables: segment / unit offsets and relative synthesis chunks per spin;
+        # the tables themselves are built on first use (`ck_tables`)
+        self.ck_segoff, self.ck_uoff, self.ck_choff, self.ck_nchunks = {}, {}, {}, {}
+        self.ck = {}
+        self.ck_entries = {}
+        for spin in (0, 2):
+            seg = np.zeros(plan.L + 1, dtype=np.int64)
+            uo = np.zeros(plan.L + 1, dtype=np.int64)
+            _lib.call("gm_ck_offsets", lmax, spin, seg.ctypes.data_as(ctypes.c_void_p),
+                      uo.ctypes.data_as(ctypes.c_void_p))
+            self.ck_segoff[spin] = torch.from_numpy(seg).to(dev)
+            self.ck_uoff[spin] = torch.from_numpy(uo).to(dev)
+            self.ck_entries[spin] = int(seg[-1]) * plan.nlanes
+            ch = np.zeros(plan.L + 1, dtype=np.int64)
+            _lib.call("gm_ck_syn_chunk_offsets", lmax, spin, ch.ctypes.data_as(ctypes.c_void_p))
+            self.ck_choff[spin] = torch.from_numpy(ch).to(dev)
+            self.ck_nchunks[spin] = int(ch[-1])
         self.nctas = torch.cuda.get_device_properties(dev).multi_processor_count
         self.img_bytes = lib.gm_tc_ana_image_bytes(plan.nside, lmax)
         self.img_bytes_per_order = lib.gm_tc_ana_image_bytes(plan.nside, 0)
@@ -63,6 +86,38 @@ def get_tc_plan(nside, lmax, device=None):
 
 def _variants(spin):
     return (0,) if spin == 0 else (-2, 2)
+
+
+def ck_table_bytes(tp, spin):
+    """Bytes of the checkpoint tables of both row variants of `spin` (state float2 + shift)."""
+    return len(_variants(spin)) * tp.ck_entries[spin] * 9
+
+
+def ck_tables(tp, spin):
+    """{s': (state, shift)} checkpoint tables of the row variants of `spin`, built on the
+    first call and kept with the plan; None when checkpoints are switched off or the
+    tables of the geometry would take more than CK_MEMORY_SHARE of the device memory."""
+    if not USE_CHECKPOINTS:
+        return None
+    p = tp.plan
+    with _LOCK:
+        have = tp.ck.get(spin)
+        if have is not None:
+            return have
+        total = torch.cuda.get_device_properties(p.device).total_memory
+        built = sum(ck_table_bytes(tp, s) for s in tp.ck)
+        if built + ck_table_bytes(tp, spin) > CK_MEMORY_SHARE * total:
+            return None
+        out = {}
+        for sp in _variants(spin):
+            state = torch.empty((tp.ck_entries[spin], 2), dtype=torch.float32, device=p.device)
+            shift = torch.empty(tp.ck_entries[spin], dtype=torch.uint8, device=p.device)
+            _lib.call("gm_ck_build", p.nside, p.lmax, spin, sp, _lib.ptr(p.geom), _lib.ptr(p.seeds),
+                      _lib.ptr(tp.coef[spin]), _lib.ptr(tp.ck_segoff[spin]), _lib.ptr(state),
+                      _lib.ptr(shift), _lib.stream_handle(p.device))
+            out[sp] = (state, shift)
+        tp.ck[spin] = out
+        return out
 
 
 def _rows(spin, ncomp):
@@ -110,7 +165,15 @@ class _Batch:
     def analysis(self, scale):
         """alm_i += scale * analysis of the images (which carry img_scale)."""
         p, tp = self.tp.plan, self.tp
+        ck = ck_tables(tp, self.spin)
         for sp, img in zip(_variants(self.spin), self.img):
+            if ck is not None:
+                _lib.call("gm_ck_analysis", p.nside, p.lmax, self.spin, sp, self.ncomp, _lib.ptr(p.geom),
+                          _lib.ptr(tp.coef[self.spin]), _lib.ptr(tp.ck_segoff[self.spin]),
+                          _lib.ptr(tp.ck_uoff[self.spin]), _lib.ptr(ck[sp][0]), _lib.ptr(ck[sp][1]),
+                          _lib.ptr(img), _lib.ptr(self.alm_i), float(scale) / self.img_scale, tp.nctas,
+                          _lib.ptr(tp.err), _lib.stream_handle(p.device))
+                continue
             _lib.call("gm_tc_analysis", p.nside, p.lmax, self.spin, sp, self.ncomp, _lib.ptr(p.geom),
                       _lib.ptr(p.seeds), _lib.ptr(tp.coef[self.spin]), _lib.ptr(img),
                       _lib.ptr(self.alm_i), float(scale) / self.img_scale, _lib.ptr(tp.scratch),
@@ -119,7 +182,8 @@ class _Batch:
     def synthesis(self, synd=None):
         """-> list of synd tensors (L, nlanes, 2H) float32, one per row variant."""
         p, tp = self.tp.plan, self.tp
-        nch = tp.nchunks[self.spin]
+        ck = ck_tables(tp, self.spin)
+        nch = tp.nchunks[self.spin] if ck is None else tp.ck_nchunks[self.spin]
         simg_bytes = _lib.load().gm_tc_syn_image_bytes(nch)
         simg = torch.empty(simg_bytes, dtype=torch.uint8, device=p.device)
         outs = synd if synd is not None else [
@@ -127,6 +191,16 @@ class _Batch:
             for _ in _variants(self.spin)]
         alm_scale = pow2_scale(self.alm_i)
         for sp, out in zip(_variants(self.spin), outs):
+            if ck is not None:
+                _lib.call("gm_ck_prep_syn", p.lmax, self.spin, sp, self.ncomp, _lib.ptr(self.alm_i),
+                          _lib.ptr(tp.ck_choff[self.spin]), _lib.ptr(simg), simg_bytes, alm_scale,
+                          _lib.stream_handle(p.device))
+                _lib.call("gm_ck_synthesis", p.nside, p.lmax, self.spin, sp, self.ncomp, _lib.ptr(p.geom),
+                          _lib.ptr(tp.coef[self.spin]), _lib.ptr(tp.ck_segoff[self.spin]),
+                          _lib.ptr(ck[sp][0]), _lib.ptr(ck[sp][1]), _lib.ptr(simg),
+                          _lib.ptr(tp.ck_choff[self.spin]), _lib.ptr(out), 1.0 / alm_scale,
+                          _lib.ptr(tp.err), _lib.stream_handle(p.device))
+                continue
             _lib.call("gm_tc_prep_syn", p.lmax, self.spin, sp, self.ncomp, _lib.ptr(self.alm_i),
                       _lib.ptr(tp.choff[self.spin]), _lib.ptr(simg), simg_bytes, alm_scale,
                       _lib.stream_handle(p.device))

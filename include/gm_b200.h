@@ -316,6 +316,47 @@ int gm_tc_fold(int64_t nside, int64_t lmax, int spin, int64_t ncomp, const float
 /* Batched synthesis output -> syn layout of gm_ring_synthesis. */
 int gm_tc_synd_to_syn(int64_t nside, int64_t lmax, int spin, int64_t ncomp, const float *synd_a,
                       const float *synd_b, float *syn, void *stream);
+
+/* ---- checkpointed batched Legendre contraction (replaces march_v2.cu:155-407 for batched
+ * maps; the reference's window tables march_v2.py:388-450 are its per-geometry constants).
+ * The rows are generated in single precision by the difference form of the recurrence,
+ * restarted every 128 rows (segment) from a checkpoint table built once per geometry and
+ * row variant by the FP64 recurrence.  Order m has ceil((lmax + 1 - l0)/128) segments
+ * (l0 = max(m, |s'|)); the table holds, per (segment, lane), the pre-state float2
+ * (v_{l_s - 1}, D_{l_s}) scaled by 2^(64 n) and the shift n (uint8).  Analysis units are
+ * superblocks of 256 rows (two segments).
+ *
+ * Host-side offsets: segoff[m] (first segment of order m) and uoff[m] (first analysis unit),
+ * lmax + 2 entries each. */
+int gm_ck_offsets(int64_t lmax, int spin, int64_t *segoff_host, int64_t *uoff_host);
+/* Entries (segments x 2 nside) of one row variant's table, or -1 on bad arguments. */
+int64_t gm_ck_table_entries(int64_t nside, int64_t lmax, int spin);
+/* Build the checkpoint table of row variant sp (0; -2, +2) from the FP64 recurrence.
+ * segoff: device copy of gm_ck_offsets' segoff. */
+int gm_ck_build(int64_t nside, int64_t lmax, int spin, int sp, const double *geom,
+                const double *seeds, const double *coef, const int64_t *segoff, void *ck_state,
+                uint8_t *ck_shift, void *stream);
+/* alm_i += scale * analysis of the rows of `img` (gm_tc_pack / gm_tc_fold images) for row
+ * variant sp; nctas persistent CTAs.  No scratch: each alm element belongs to one unit.
+ * err (int32) set non-zero if a bounded wait timed out. */
+int gm_ck_analysis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                   const double *geom, const double *coef, const int64_t *segoff,
+                   const int64_t *uoff, const void *ck_state, const uint8_t *ck_shift,
+                   const void *img, double *alm_i, double scale, int64_t nctas, int32_t *err,
+                   void *stream);
+/* Synthesis chunk offsets of the checkpointed layout: chunk cc of order m covers rows
+ * l0 + 64 cc + [0, 64); choff_host has lmax + 2 entries. */
+int gm_ck_syn_chunk_offsets(int64_t lmax, int spin, int64_t *choff_host);
+/* Synthesis operand images (checkpointed layout) from alm_scale * alm_i, row variant sp. */
+int gm_ck_prep_syn(int64_t lmax, int spin, int sp, int64_t ncomp, const double *alm_i,
+                   const int64_t *choff, void *simg, int64_t simg_bytes, double alm_scale,
+                   void *stream);
+/* synd (L, nlanes, 2H) float32 = out_scale * rows of the synthesis for row variant sp. */
+int gm_ck_synthesis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                    const double *geom, const double *coef, const int64_t *segoff,
+                    const void *ck_state, const uint8_t *ck_shift, const void *simg,
+                    const int64_t *choff, float *synd, double out_scale, int32_t *err,
+                    void *stream);
 /* Order windows of the batched transforms, for geometries whose full-size buffers do not
  * fit (Nside 4096 batches, Nside 8192): each entry handles the orders m in [mbeg, mend)
  * only, and its per-order buffers hold just those orders, indexed by m - mbeg (analysis
