@@ -69,18 +69,9 @@ def _save():
             json.dump(_CACHE, fh, indent=1, sort_keys=True)
 
 
-def _key(plan, spin, ncomp, prec, kind):
+def _key(plan, spin, ncomp, prec, kind, ck=False):
     name = torch.cuda.get_device_name(plan.device).replace(" ", "_").replace(":", "_")
-    return f"{name}:{kind}:p{prec}:s{spin}:n{plan.nside}:l{plan.lmax}:c{ncomp}"
-
-
-def _run(plan, spin, ncomp, prec, kind, tile, a, b, st):
-    if kind == "ana":
-        _lib.call("gm_legendre_analysis_tile", prec, spin, plan.nside, plan.lmax, ncomp,
-                  _lib.ptr(plan.geom), _lib.ptr(plan.seeds), _lib.ptr(a), _lib.ptr(b), 1.0, tile, st)
-    else:
-        _lib.call("gm_legendre_synthesis_tile", prec, spin, plan.nside, plan.lmax, ncomp,
-                  _lib.ptr(plan.geom), _lib.ptr(plan.seeds), _lib.ptr(a), _lib.ptr(b), tile, st)
+    return f"{name}:{kind}:p{prec}:s{spin}:n{plan.nside}:l{plan.lmax}:c{ncomp}" + (":ck" if ck else "")
 
 
 def tune(plan, spin, ncomp, prec, kind, reps=2):
@@ -97,14 +88,16 @@ def tune(plan, spin, ncomp, prec, kind, reps=2):
     else:
         alm.real.normal_(generator=gen)
         a, b = alm, rhs
-    st = _lib.stream_handle(dev)
+    from . import sht
+
+    ck = sht.ck_args(plan, spin, prec)
     times = {}
     for t in range(len(tiles(spin))):
-        _run(plan, spin, ncomp, prec, kind, t, a, b, st)
+        sht.run_legendre(plan, spin, ncomp, prec, kind, t, a, b, ck=ck)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(reps):
-            _run(plan, spin, ncomp, prec, kind, t, a, b, st)
+            sht.run_legendre(plan, spin, ncomp, prec, kind, t, a, b, ck=ck)
         e1.record()
         e1.synchronize()
         times[t] = e0.elapsed_time(e1) / reps
@@ -117,7 +110,9 @@ def tile_for(plan, spin, ncomp, prec, kind):
     """Tile index for this transform (-1: the built-in choice when tuning is off)."""
     if not _STATE["enabled"]:
         return -1
-    key = _key(plan, spin, ncomp, prec, kind)
+    from . import sht
+
+    key = _key(plan, spin, ncomp, prec, kind, sht.ck_args(plan, spin, prec) is not None)
     with _LOCK:
         _load()
         if key not in _CACHE:
@@ -132,7 +127,7 @@ def choices():
     """{key: (chosen tile (NC, R), timings in ms per tile)} of this process."""
     out = {}
     for k, v in _CACHE.items():
-        spin = int(k.split(":")[-4][1:])
+        spin = int(next(f for f in k.split(":") if f.startswith("s") and f[1:].isdigit())[1:])
         out[k] = (tiles(spin)[v], _TIMINGS.get(k))
     return out
 

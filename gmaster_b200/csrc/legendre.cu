@@ -88,6 +88,45 @@ __device__ __forceinline__ Coef make_coef(int l, int m, int s, int l0)
     return c;
 }
 
+// Checkpoint tables of the single-precision rows (legendre_ck.cu): segment k of order m
+// starts at row l0 + 128 k; per (segment, lane) the scaled pre-state (v_{l-1}, D_l) and its
+// shift n (actual = stored * 2^(-64 n)).  Variant q = 0: s' = 0 (spin 0) or -2; q = 1: +2.
+struct CkTab {
+    const int64_t *segoff;
+    const float2 *ck[2];
+    const uint8_t *cn[2];
+};
+constexpr int kCkSeg = 128;
+
+// Single-precision difference-form coefficients of row l (legendre_ck.cu): (c1, E for
+// s' = -s, E for s' = +s, b); a segment's first row is the restart step (0, 0, 0, 1).
+__device__ __forceinline__ float4 ck_coef(int l, int m, int s, int l0)
+{
+    if ((l - l0) % kCkSeg == 0) return make_float4(0.f, 0.f, 0.f, 1.f);
+    const Coef c = make_coef(l, m, s, l0);
+    const double e = c.alpha - c.beta - 1.0;
+    return make_float4((float)c.alpha, (float)(e + c.c0), (float)(e - c.c0), (float)c.beta);
+}
+
+// One FP32 difference-form step, then the emitted value (scaled lanes: n > 0).
+__device__ __forceinline__ float ck_step(float c1, float E, float b, float y, float &v, float &D, int &n,
+                                         bool scaled)
+{
+    const float C = fmaf(c1, y, E);
+    const float bD = b * D;
+    D = fmaf(C, v, bD);
+    v = v + D;
+    if (!scaled) return v;
+    const float out = v * (n == 0 ? 1.0f : (n == 1 ? 0x1p-64f : 0.0f));
+    // a row grows a value by at most 2^8 (alpha <= sqrt(2m) + 1 at Nside <= 8192)
+    if (n != 0 && fabsf(v) > 0x1p48f) {
+        v *= 0x1p-64f;
+        D *= 0x1p-64f;
+        --n;
+    }
+    return out;
+}
+
 template <typename T, int V>
 __device__ __forceinline__ T warp_reduce_scatter(T (&v)[V], int lane)
 {
@@ -116,11 +155,14 @@ __device__ __forceinline__ int64_t alm_index(int64_t lmax, int64_t l, int64_t m)
 
 // NC components per CTA (spin 0: NC maps; spin 2: NC = 2, one (Q, U) pair).
 // NV values per degree: spin 0: 2 NC; spin 2: 8.  LB degrees per reduce-scatter block.
-template <typename T, int SPIN, int NC, int R>
+//
+// CK: the rows come from the single-precision difference form restarted from the checkpoint
+// tables every 128 rows (mixed precision, spin 0 and 2) instead of the FP64 recurrence.
+template <typename T, int SPIN, int NC, int R, bool CK>
 __global__ void __launch_bounds__(kThreads) k_legendre_ana(
     int64_t nside, int64_t lmax, int64_t ncomp, const double *__restrict__ geom,
     const double *__restrict__ seeds, const T *__restrict__ rhs, double *__restrict__ alm,
-    double scale, int spin)
+    double scale, int spin, CkTab tab)
 {
     constexpr int NV = SPIN == 0 ? 2 * NC : 8;
     constexpr int LB = 32 / NV;
@@ -128,6 +170,7 @@ __global__ void __launch_bounds__(kThreads) k_legendre_ana(
     static_assert(LB * NV == 32, "reduce-scatter width");
     static_assert(LB % 2 == 0 && kWindow % 2 == 0, "row parity is fixed by the row index");
     __shared__ Coef coef[kWindow];
+    __shared__ float4 fcoef[kWindow];
     __shared__ double red[kWarps][kWindow * NV];
 
     const int64_t L = lmax + 1, nlanes = 2 * nside, nelem = L * (L + 1) / 2;
@@ -140,24 +183,29 @@ __global__ void __launch_bounds__(kThreads) k_legendre_ana(
 
     double x[R], v[NVAR][R], vp[NVAR][R];
     int kx[NVAR][R];
+    float fy[R], fv[NVAR][R], fD[NVAR][R];
+    int fn[NVAR][R];
     T rh[R][NC][4];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int64_t j = (int64_t)blockIdx.x * kThreads * R + r * kThreads + threadIdx.x;
         const bool ok = j < nlanes;
         x[r] = ok ? geom[j] : 0.0;
+        fy[r] = ok ? (float)(geom[j] - 1.0) : 0.0f;
         const double ls = ok ? geom[nlanes + j] : 0.0, lc = ok ? geom[2 * nlanes + j] : 0.0;
 #pragma unroll
         for (int q = 0; q < NVAR; ++q) {
             // seed variants: s' = -s (lambda+), then s' = +s (lambda-, times (-1)^s)
             const int var = SPIN == 0 ? 0 : seed_variant(sv) + q;
-            if (ok) {
+            if (!CK && ok) {
                 seed_lane(seeds + ((int64_t)var * L + m) * 4, ls, lc, v[q][r], kx[q][r]);
             } else {
                 v[q][r] = 0.0;
                 kx[q][r] = 0;
             }
             vp[q][r] = 0.0;
+            fv[q][r] = fD[q][r] = 0.0f;
+            fn[q][r] = 0;
         }
 #pragma unroll
         for (int c = 0; c < NC; ++c)
@@ -189,7 +237,37 @@ __global__ void __launch_bounds__(kThreads) k_legendre_ana(
     for (int lb = l0; lb < L; lb += kWindow) {
         if (threadIdx.x < kWindow) {
             const int l = lb + threadIdx.x;
-            coef[threadIdx.x] = make_coef(l, m, sv, l0);
+            if (CK) fcoef[threadIdx.x] = ck_coef(l, m, sv, l0);
+            else coef[threadIdx.x] = make_coef(l, m, sv, l0);
+        }
+        bool scaled = false;
+        if (CK) {
+            if ((lb - l0) % kCkSeg == 0) {
+                // a new segment: the lane states restart from the checkpoint table
+                const int64_t seg = tab.segoff[m] + (lb - l0) / kCkSeg;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int64_t j = (int64_t)blockIdx.x * kThreads * R + r * kThreads + threadIdx.x;
+#pragma unroll
+                    for (int q = 0; q < NVAR; ++q) {
+                        float2 st = make_float2(0.f, 0.f);
+                        int n = 0;
+                        if (j < nlanes) {
+                            st = __ldg(tab.ck[q] + seg * nlanes + j);
+                            n = __ldg(tab.cn[q] + seg * nlanes + j);
+                        }
+                        fv[q][r] = st.x;
+                        fD[q][r] = st.y;
+                        fn[q][r] = n;
+                    }
+                }
+            }
+            int any = 0;
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+#pragma unroll
+                for (int q = 0; q < NVAR; ++q) any |= fn[q][r];
+            scaled = __any_sync(0xffffffffu, any != 0);
         }
         __syncthreads();
 #pragma unroll 1
@@ -201,7 +279,16 @@ __global__ void __launch_bounds__(kThreads) k_legendre_ana(
             for (int s = 0; s < LB; ++s) {
                 const int l = lb + i + s;
                 if (l < L) {
-                    if (l > l0) {
+                    float fval[NVAR][R];
+                    if (CK) {
+                        const float4 cq = fcoef[i + s];
+#pragma unroll
+                        for (int r = 0; r < R; ++r)
+#pragma unroll
+                            for (int q = 0; q < NVAR; ++q)
+                                fval[q][r] = ck_step(cq.x, q == 0 ? cq.y : cq.z, cq.w, fy[r], fv[q][r],
+                                                     fD[q][r], fn[q][r], scaled);
+                    } else if (l > l0) {
                         const Coef cf = coef[i + s];
 #pragma unroll
                         for (int r = 0; r < R; ++r) {
@@ -228,7 +315,7 @@ __global__ void __launch_bounds__(kThreads) k_legendre_ana(
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         if (SPIN == 0) {
-                            const T val = kx[0][r] == 0 ? (T)v[0][r] : (T)0;
+                            const T val = CK ? (T)fval[0][r] : (kx[0][r] == 0 ? (T)v[0][r] : (T)0);
 #pragma unroll
                             for (int c = 0; c < NC; ++c) {
                                 const T hr = par ? rh[r][c][2] : rh[r][c][0];
@@ -237,9 +324,16 @@ __global__ void __launch_bounds__(kThreads) k_legendre_ana(
                                 acc[s * NV + 2 * c + 1] += val * hi;
                             }
                         } else {
-                            const double lp = kx[0][r] == 0 ? v[0][r] : 0.0;
-                            const double lm = kx[1][r] == 0 ? v[1][r] : 0.0;
-                            const T f1 = (T)(0.5 * (lp + lm)), f2 = (T)(0.5 * (lp - lm));
+                            T f1, f2;
+                            if (CK) {
+                                f1 = (T)(0.5f * (fval[0][r] + fval[NVAR - 1][r]));
+                                f2 = (T)(0.5f * (fval[0][r] - fval[NVAR - 1][r]));
+                            } else {
+                                const double lp = kx[0][r] == 0 ? v[0][r] : 0.0;
+                                const double lm = kx[NVAR - 1][r] == 0 ? v[NVAR - 1][r] : 0.0;
+                                f1 = (T)(0.5 * (lp + lm));
+                                f2 = (T)(0.5 * (lp - lm));
+                            }
                             // same-parity side P = Sum (even) / Diff (odd); other side D
                             const T qpr = par ? rh[r][0][2] : rh[r][0][0];
                             const T qpi = par ? rh[r][0][3] : rh[r][0][1];
@@ -303,16 +397,17 @@ __global__ void __launch_bounds__(kThreads) k_legendre_ana(
 
 // ---------------------------------------------------------------- synthesis
 
-template <typename T, int SPIN, int NC, int R>
+template <typename T, int SPIN, int NC, int R, bool CK>
 __global__ void __launch_bounds__(kThreads) k_legendre_syn(
     int64_t nside, int64_t lmax, int64_t ncomp, const double *__restrict__ geom,
     const double *__restrict__ seeds, const double *__restrict__ alm, T *__restrict__ syn,
-    int spin)
+    int spin, CkTab tab)
 {
     constexpr int NVAR = SPIN == 0 ? 1 : 2;
     constexpr int NA = SPIN == 0 ? NC : 2;  // complex alm rows per degree (maps, or E and B)
     constexpr int NACC = SPIN == 0 ? 4 * NC : 16;
     __shared__ Coef coef[2][kWindow];
+    __shared__ float4 fcoef[2][kWindow];
     __shared__ T aw[2][kWindow][NA][2];
 
     const int64_t L = lmax + 1, nlanes = 2 * nside, nelem = L * (L + 1) / 2;
@@ -323,23 +418,28 @@ __global__ void __launch_bounds__(kThreads) k_legendre_syn(
 
     double x[R], v[NVAR][R], vp[NVAR][R];
     int kx[NVAR][R];
+    float fy[R], fv[NVAR][R], fD[NVAR][R];
+    int fn[NVAR][R];
     T acc[R][NACC];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int64_t j = (int64_t)blockIdx.x * kThreads * R + r * kThreads + threadIdx.x;
         const bool ok = j < nlanes && l0 <= lmax;
         x[r] = ok ? geom[j] : 0.0;
+        fy[r] = ok ? (float)(geom[j] - 1.0) : 0.0f;
         const double ls = ok ? geom[nlanes + j] : 0.0, lc = ok ? geom[2 * nlanes + j] : 0.0;
 #pragma unroll
         for (int q = 0; q < NVAR; ++q) {
             const int var = SPIN == 0 ? 0 : seed_variant(sv) + q;
-            if (ok) {
+            if (!CK && ok) {
                 seed_lane(seeds + ((int64_t)var * L + m) * 4, ls, lc, v[q][r], kx[q][r]);
             } else {
                 v[q][r] = 0.0;
                 kx[q][r] = 0;
             }
             vp[q][r] = 0.0;
+            fv[q][r] = fD[q][r] = 0.0f;
+            fn[q][r] = 0;
         }
 #pragma unroll
         for (int q = 0; q < NACC; ++q) acc[r][q] = (T)0;
@@ -347,9 +447,39 @@ __global__ void __launch_bounds__(kThreads) k_legendre_syn(
 
     int buf = 0;
     for (int lb = l0; lb < L; lb += kWindow, buf ^= 1) {
+        bool scaled = false;
+        if (CK) {
+            if ((lb - l0) % kCkSeg == 0) {
+                // a new segment: the lane states restart from the checkpoint table
+                const int64_t seg = tab.segoff[m] + (lb - l0) / kCkSeg;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int64_t j = (int64_t)blockIdx.x * kThreads * R + r * kThreads + threadIdx.x;
+#pragma unroll
+                    for (int q = 0; q < NVAR; ++q) {
+                        float2 st = make_float2(0.f, 0.f);
+                        int n = 0;
+                        if (j < nlanes) {
+                            st = __ldg(tab.ck[q] + seg * nlanes + j);
+                            n = __ldg(tab.cn[q] + seg * nlanes + j);
+                        }
+                        fv[q][r] = st.x;
+                        fD[q][r] = st.y;
+                        fn[q][r] = n;
+                    }
+                }
+            }
+            int any = 0;
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+#pragma unroll
+                for (int q = 0; q < NVAR; ++q) any |= fn[q][r];
+            scaled = __any_sync(0xffffffffu, any != 0);
+        }
         if (threadIdx.x < kWindow) {
             const int l = lb + threadIdx.x;
-            coef[buf][threadIdx.x] = make_coef(l, m, sv, l0);
+            if (CK) fcoef[buf][threadIdx.x] = ck_coef(l, m, sv, l0);
+            else coef[buf][threadIdx.x] = make_coef(l, m, sv, l0);
 #pragma unroll
             for (int a = 0; a < NA; ++a) {
                 T re = 0, im = 0;
@@ -378,7 +508,16 @@ __global__ void __launch_bounds__(kThreads) k_legendre_syn(
                 const int s = s0 + hh;
                 if (s >= lend) break;
                 const int l = lb + s;
-                if (l > l0) {
+                float fval[NVAR][R];
+                if (CK) {
+                    const float4 cq = fcoef[buf][s];
+#pragma unroll
+                    for (int r = 0; r < R; ++r)
+#pragma unroll
+                        for (int q = 0; q < NVAR; ++q)
+                            fval[q][r] = ck_step(cq.x, q == 0 ? cq.y : cq.z, cq.w, fy[r], fv[q][r], fD[q][r],
+                                                 fn[q][r], scaled);
+                } else if (l > l0) {
                     const Coef cf = coef[buf][s];
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
@@ -402,16 +541,23 @@ __global__ void __launch_bounds__(kThreads) k_legendre_syn(
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     if (SPIN == 0) {
-                        const T val = kx[0][r] == 0 ? (T)v[0][r] : (T)0;
+                        const T val = CK ? (T)fval[0][r] : (kx[0][r] == 0 ? (T)v[0][r] : (T)0);
 #pragma unroll
                         for (int c = 0; c < NC; ++c) {
                             acc[r][4 * c + 2 * hh] += val * aw[buf][s][c][0];
                             acc[r][4 * c + 2 * hh + 1] += val * aw[buf][s][c][1];
                         }
                     } else {
-                        const double lp = kx[0][r] == 0 ? v[0][r] : 0.0;
-                        const double lm = kx[1][r] == 0 ? v[1][r] : 0.0;
-                        const T f1 = (T)(0.5 * (lp + lm)), f2 = (T)(0.5 * (lp - lm));
+                        T f1, f2;
+                        if (CK) {
+                            f1 = (T)(0.5f * (fval[0][r] + fval[NVAR - 1][r]));
+                            f2 = (T)(0.5f * (fval[0][r] - fval[NVAR - 1][r]));
+                        } else {
+                            const double lp = kx[0][r] == 0 ? v[0][r] : 0.0;
+                            const double lm = kx[NVAR - 1][r] == 0 ? v[NVAR - 1][r] : 0.0;
+                            f1 = (T)(0.5 * (lp + lm));
+                            f2 = (T)(0.5 * (lp - lm));
+                        }
                         const T er = aw[buf][s][0][0], ei = aw[buf][s][0][1];
                         const T br = aw[buf][s][1][0], bi = aw[buf][s][1][1];
                         // per parity: [S1E re, im, S1B re, im, S2E re, im, S2B re, im]
@@ -502,53 +648,63 @@ extern "C" int64_t gm_seed_table_len(int64_t L) { return (2 * kMaxSpin + 1) * 4 
 template <typename T, int SPIN, int NC, int R>
 static int launch_ana(int spin, int64_t nside, int64_t lmax, int64_t ncomp, const double *geom,
                       const double *seeds, const void *rhs, double *alm, double scale,
-                      cudaStream_t s)
+                      cudaStream_t s, const CkTab *tab = nullptr)
 {
     const int64_t nlanes = 2 * nside;
     dim3 grid((unsigned)((nlanes + kThreads * R - 1) / (kThreads * R)), (unsigned)(lmax + 1),
               (unsigned)((ncomp + NC - 1) / NC));
-    k_legendre_ana<T, SPIN, NC, R><<<grid, kThreads, 0, s>>>(nside, lmax, ncomp, geom, seeds,
-                                                             (const T *)rhs, alm, scale, spin);
+    if (tab)
+        k_legendre_ana<float, SPIN, NC, R, true><<<grid, kThreads, 0, s>>>(
+            nside, lmax, ncomp, geom, seeds, (const float *)rhs, alm, scale, spin, *tab);
+    else
+        k_legendre_ana<T, SPIN, NC, R, false><<<grid, kThreads, 0, s>>>(
+            nside, lmax, ncomp, geom, seeds, (const T *)rhs, alm, scale, spin, CkTab{});
     return check_launch("gm_legendre_analysis");
 }
 
 template <typename T, int SPIN, int NC, int R>
 static int launch_syn(int spin, int64_t nside, int64_t lmax, int64_t ncomp, const double *geom,
-                      const double *seeds, const double *alm, void *syn, cudaStream_t s)
+                      const double *seeds, const double *alm, void *syn, cudaStream_t s,
+                      const CkTab *tab = nullptr)
 {
     const int64_t nlanes = 2 * nside;
     dim3 grid((unsigned)((nlanes + kThreads * R - 1) / (kThreads * R)), (unsigned)(lmax + 1),
               (unsigned)((ncomp + NC - 1) / NC));
-    k_legendre_syn<T, SPIN, NC, R><<<grid, kThreads, 0, s>>>(nside, lmax, ncomp, geom, seeds, alm,
-                                                             (T *)syn, spin);
+    if (tab)
+        k_legendre_syn<float, SPIN, NC, R, true><<<grid, kThreads, 0, s>>>(
+            nside, lmax, ncomp, geom, seeds, alm, (float *)syn, spin, *tab);
+    else
+        k_legendre_syn<T, SPIN, NC, R, false><<<grid, kThreads, 0, s>>>(
+            nside, lmax, ncomp, geom, seeds, alm, (T *)syn, spin, CkTab{});
     return check_launch("gm_legendre_synthesis");
 }
 
 template <typename T>
 static int dispatch_ana(int spin, int64_t nside, int64_t lmax, int64_t ncomp, const double *geom,
                         const double *seeds, const void *rhs, double *alm, double scale,
-                        cudaStream_t s)
+                        cudaStream_t s, const CkTab *tab = nullptr)
 {
     if (spin == 0) {
         if (ncomp == 1)
-            return launch_ana<T, 0, 1, 4>(spin, nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s);
+            return launch_ana<T, 0, 1, 4>(spin, nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s, tab);
         if (ncomp == 2)
-            return launch_ana<T, 0, 2, 4>(spin, nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s);
-        return launch_ana<T, 0, 4, 2>(spin, nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s);
+            return launch_ana<T, 0, 2, 4>(spin, nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s, tab);
+        return launch_ana<T, 0, 4, 2>(spin, nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s, tab);
     }
-    return launch_ana<T, 2, 2, 2>(spin, nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s);
+    return launch_ana<T, 2, 2, 2>(spin, nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s, tab);
 }
 
 template <typename T>
 static int dispatch_syn(int spin, int64_t nside, int64_t lmax, int64_t ncomp, const double *geom,
-                        const double *seeds, const double *alm, void *syn, cudaStream_t s)
+                        const double *seeds, const double *alm, void *syn, cudaStream_t s,
+                        const CkTab *tab = nullptr)
 {
     if (spin == 0) {
-        if (ncomp == 1) return launch_syn<T, 0, 1, 2>(spin, nside, lmax, ncomp, geom, seeds, alm, syn, s);
-        if (ncomp == 2) return launch_syn<T, 0, 2, 2>(spin, nside, lmax, ncomp, geom, seeds, alm, syn, s);
-        return launch_syn<T, 0, 4, 1>(spin, nside, lmax, ncomp, geom, seeds, alm, syn, s);
+        if (ncomp == 1) return launch_syn<T, 0, 1, 2>(spin, nside, lmax, ncomp, geom, seeds, alm, syn, s, tab);
+        if (ncomp == 2) return launch_syn<T, 0, 2, 2>(spin, nside, lmax, ncomp, geom, seeds, alm, syn, s, tab);
+        return launch_syn<T, 0, 4, 1>(spin, nside, lmax, ncomp, geom, seeds, alm, syn, s, tab);
     }
-    return launch_syn<T, 2, 2, 2>(spin, nside, lmax, ncomp, geom, seeds, alm, syn, s);
+    return launch_syn<T, 2, 2, 2>(spin, nside, lmax, ncomp, geom, seeds, alm, syn, s, tab);
 }
 
 // Tile shapes the autotuner chooses from: (NC, R) = (components per CTA, lanes per thread).
@@ -562,9 +718,9 @@ constexpr int kNTiles2 = sizeof(kTiles2) / sizeof(kTiles2[0]);
 template <typename T>
 static int tile_ana(int spin, int tile, int64_t nside, int64_t lmax, int64_t ncomp,
                     const double *geom, const double *seeds, const void *rhs, double *alm,
-                    double scale, cudaStream_t s)
+                    double scale, cudaStream_t s, const CkTab *tab = nullptr)
 {
-#define GM_ANA(SP, NC, R) return launch_ana<T, SP, NC, R>(spin, nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s)
+#define GM_ANA(SP, NC, R) return launch_ana<T, SP, NC, R>(spin, nside, lmax, ncomp, geom, seeds, rhs, alm, scale, s, tab)
     if (spin == 0) {
         switch (tile) {
         case 0: GM_ANA(0, 1, 1);
@@ -591,9 +747,9 @@ static int tile_ana(int spin, int tile, int64_t nside, int64_t lmax, int64_t nco
 template <typename T>
 static int tile_syn(int spin, int tile, int64_t nside, int64_t lmax, int64_t ncomp,
                     const double *geom, const double *seeds, const double *alm, void *syn,
-                    cudaStream_t s)
+                    cudaStream_t s, const CkTab *tab = nullptr)
 {
-#define GM_SYN(SP, NC, R) return launch_syn<T, SP, NC, R>(spin, nside, lmax, ncomp, geom, seeds, alm, syn, s)
+#define GM_SYN(SP, NC, R) return launch_syn<T, SP, NC, R>(spin, nside, lmax, ncomp, geom, seeds, alm, syn, s, tab)
     if (spin == 0) {
         switch (tile) {
         case 0: GM_SYN(0, 1, 1);
@@ -701,4 +857,57 @@ extern "C" int gm_legendre_synthesis(int precision, int spin, int64_t nside, int
     if (precision == GM_MIXED)
         return dispatch_syn<float>(spin, nside, lmax, ncomp, lane_geom, seeds, alm, syn, s);
     return GM_ERR_UNSUPPORTED;
+}
+
+// Mixed-precision spin-0 / spin-2 transforms with the checkpointed single-precision rows.
+static int ck_args_ok(int spin, int64_t nside, int64_t lmax, int64_t ncomp, int tile)
+{
+    if (nside < 1 || lmax < 2 || lmax + 1 > 65535 || ncomp < 1 || ncomp > 65535) return GM_ERR_BAD_SHAPE;
+    if (spin != 0 && spin != 2) return GM_ERR_UNSUPPORTED;
+    if (spin == 2 && (ncomp % 2)) return GM_ERR_BAD_SHAPE;
+    if (tile < -1 || tile >= (spin == 0 ? kNTiles0 : kNTiles2)) return GM_ERR_BAD_SHAPE;
+    return GM_OK;
+}
+
+static CkTab ck_tab(const int64_t *segoff, const void *ck_a, const uint8_t *cn_a, const void *ck_b,
+                    const uint8_t *cn_b)
+{
+    CkTab t;
+    t.segoff = segoff;
+    t.ck[0] = (const float2 *)ck_a;
+    t.cn[0] = cn_a;
+    t.ck[1] = (const float2 *)ck_b;
+    t.cn[1] = cn_b;
+    return t;
+}
+
+extern "C" int gm_legendre_analysis_ck(int spin, int64_t nside, int64_t lmax, int64_t ncomp,
+                                       const double *lane_geom, const void *rhs, double *alm,
+                                       double scale, const int64_t *segoff, const void *ck_a,
+                                       const uint8_t *cn_a, const void *ck_b, const uint8_t *cn_b,
+                                       int tile, void *stream)
+{
+    const int st = ck_args_ok(spin, nside, lmax, ncomp, tile);
+    if (st != GM_OK) return st;
+    if (!lane_geom || !rhs || !alm || !segoff || !ck_a || !cn_a || (spin == 2 && (!ck_b || !cn_b)))
+        return GM_ERR_BAD_PTR;
+    const CkTab tab = ck_tab(segoff, ck_a, cn_a, ck_b, cn_b);
+    cudaStream_t s = as_stream(stream);
+    return tile < 0 ? dispatch_ana<float>(spin, nside, lmax, ncomp, lane_geom, nullptr, rhs, alm, scale, s, &tab)
+                    : tile_ana<float>(spin, tile, nside, lmax, ncomp, lane_geom, nullptr, rhs, alm, scale, s, &tab);
+}
+
+extern "C" int gm_legendre_synthesis_ck(int spin, int64_t nside, int64_t lmax, int64_t ncomp,
+                                        const double *lane_geom, const double *alm, void *syn,
+                                        const int64_t *segoff, const void *ck_a, const uint8_t *cn_a,
+                                        const void *ck_b, const uint8_t *cn_b, int tile, void *stream)
+{
+    const int st = ck_args_ok(spin, nside, lmax, ncomp, tile);
+    if (st != GM_OK) return st;
+    if (!lane_geom || !alm || !syn || !segoff || !ck_a || !cn_a || (spin == 2 && (!ck_b || !cn_b)))
+        return GM_ERR_BAD_PTR;
+    const CkTab tab = ck_tab(segoff, ck_a, cn_a, ck_b, cn_b);
+    cudaStream_t s = as_stream(stream);
+    return tile < 0 ? dispatch_syn<float>(spin, nside, lmax, ncomp, lane_geom, nullptr, alm, syn, s, &tab)
+                    : tile_syn<float>(spin, tile, nside, lmax, ncomp, lane_geom, nullptr, alm, syn, s, &tab);
 }

@@ -266,23 +266,64 @@ def pack_rhs(plan, spec, prec):
     return rhs
 
 
+def ck_args(plan, spin, prec):
+    """Checkpoint-table arguments (segoff, state and shift of the s' = -s and +s variants)
+    of the mixed-precision spin-0 / spin-2 Legendre kernels, whose rows then come from the
+    single-precision difference form restarted every 128 rows (legendre_ck.cu); None for
+    FP64, other spins, checkpoints switched off, or tables larger than their memory share
+    (the rows then come from the FP64 recurrence)."""
+    from . import sht_tc
+
+    if prec != _lib.MIXED or spin not in (0, 2) or plan.lmax < 2 or not sht_tc.USE_CHECKPOINTS:
+        return None
+    nvar = 1 if spin == 0 else 2
+    need = nvar * 9 * _lib.load().gm_ck_table_entries(plan.nside, plan.lmax, spin)
+    if need > sht_tc.CK_MEMORY_SHARE * torch.cuda.get_device_properties(plan.device).total_memory:
+        return None
+    tp = sht_tc.get_tc_plan(plan.nside, plan.lmax, plan.device)
+    tabs = sht_tc.ck_tables(tp, spin)
+    if tabs is None:
+        return None
+    a = tabs[0] if spin == 0 else tabs[-2]
+    b = tabs[0] if spin == 0 else tabs[2]
+    return (_lib.ptr(tp.ck_segoff[spin]), _lib.ptr(a[0]), _lib.ptr(a[1]), _lib.ptr(b[0]), _lib.ptr(b[1]))
+
+
+def run_legendre(plan, spin, ncomp, prec, kind, tile, src, dst, scale=1.0, ck=None):
+    """One Legendre pass (kind "ana": src = rhs, dst = alm; "syn": src = alm, dst = syn) with
+    the given tile shape, through the checkpointed entries when `ck` (ck_args) is given."""
+    st = _lib.stream_handle(plan.device)
+    if kind == "ana":
+        if ck is not None:
+            _lib.call("gm_legendre_analysis_ck", spin, plan.nside, plan.lmax, ncomp, _lib.ptr(plan.geom),
+                      _lib.ptr(src), _lib.ptr(dst), float(scale), *ck, tile, st)
+        else:
+            _lib.call("gm_legendre_analysis_tile", prec, spin, plan.nside, plan.lmax, ncomp,
+                      _lib.ptr(plan.geom), _lib.ptr(plan.seeds), _lib.ptr(src), _lib.ptr(dst),
+                      float(scale), tile, st)
+    elif ck is not None:
+        _lib.call("gm_legendre_synthesis_ck", spin, plan.nside, plan.lmax, ncomp, _lib.ptr(plan.geom),
+                  _lib.ptr(src), _lib.ptr(dst), *ck, tile, st)
+    else:
+        _lib.call("gm_legendre_synthesis_tile", prec, spin, plan.nside, plan.lmax, ncomp,
+                  _lib.ptr(plan.geom), _lib.ptr(plan.seeds), _lib.ptr(src), _lib.ptr(dst), tile, st)
+
+
 def legendre_analysis(plan, spin, rhs, alm, scale, prec):
     ncomp = rhs.shape[2]
     tile = autotune.tile_for(plan, spin, ncomp, prec, "ana")
-    _timed(f"legendre_analysis_s{spin}", plan, spin, ncomp, lambda: _lib.call(
-        "gm_legendre_analysis_tile", prec, spin, plan.nside, plan.lmax, ncomp,
-        _lib.ptr(plan.geom), _lib.ptr(plan.seeds), _lib.ptr(rhs), _lib.ptr(alm),
-        float(scale), tile, _lib.stream_handle(plan.device)))
+    ck = ck_args(plan, spin, prec)
+    _timed(f"legendre_analysis_s{spin}", plan, spin, ncomp,
+           lambda: run_legendre(plan, spin, ncomp, prec, "ana", tile, rhs, alm, scale, ck))
 
 
 def legendre_synthesis(plan, spin, alm, ncomp, prec, out=None):
     syn = out if out is not None else torch.empty(
         (plan.L, plan.nlanes, ncomp, 4), dtype=_real_dtype(prec), device=plan.device)
     tile = autotune.tile_for(plan, spin, ncomp, prec, "syn")
-    _timed(f"legendre_synthesis_s{spin}", plan, spin, ncomp, lambda: _lib.call(
-        "gm_legendre_synthesis_tile", prec, spin, plan.nside, plan.lmax, ncomp,
-        _lib.ptr(plan.geom), _lib.ptr(plan.seeds), _lib.ptr(alm), _lib.ptr(syn), tile,
-        _lib.stream_handle(plan.device)))
+    ck = ck_args(plan, spin, prec)
+    _timed(f"legendre_synthesis_s{spin}", plan, spin, ncomp,
+           lambda: run_legendre(plan, spin, ncomp, prec, "syn", tile, alm, syn, ck=ck))
     return syn
 
 

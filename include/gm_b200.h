@@ -317,6 +317,20 @@ int gm_tc_fold(int64_t nside, int64_t lmax, int spin, int64_t ncomp, const float
 int gm_tc_synd_to_syn(int64_t nside, int64_t lmax, int spin, int64_t ncomp, const float *synd_a,
                       const float *synd_b, float *syn, void *stream);
 
+/* gm_legendre_analysis_tile / gm_legendre_synthesis_tile in mixed precision (spin 0 or 2)
+ * with the rows of the checkpoint tables below instead of the FP64 recurrence: the
+ * single-precision difference form restarted every 128 rows (same reference interface,
+ * march_v2.cu:155-407).  ck_a/cn_a: table of s' = 0 (spin 0) or -2; ck_b/cn_b: s' = +2
+ * (ignored for spin 0); segoff: device offsets of gm_ck_offsets. */
+int gm_legendre_analysis_ck(int spin, int64_t nside, int64_t lmax, int64_t ncomp,
+                            const double *lane_geom, const void *rhs, double *alm, double scale,
+                            const int64_t *segoff, const void *ck_a, const uint8_t *cn_a,
+                            const void *ck_b, const uint8_t *cn_b, int tile, void *stream);
+int gm_legendre_synthesis_ck(int spin, int64_t nside, int64_t lmax, int64_t ncomp,
+                             const double *lane_geom, const double *alm, void *syn,
+                             const int64_t *segoff, const void *ck_a, const uint8_t *cn_a,
+                             const void *ck_b, const uint8_t *cn_b, int tile, void *stream);
+
 /* ---- checkpointed batched Legendre contraction (replaces march_v2.cu:155-407 for batched
  * maps; the reference's window tables march_v2.py:388-450 are its per-geometry constants).
  * The rows are generated in single precision by the difference form of the recurrence,
