@@ -89,6 +89,7 @@ SIGNATURES = {
                                   _c_vp], _c_int),
     "gm_tc_alm_layout": ([_c_i64, _c_int, _c_i64, _c_vp, _c_vp, _c_int, _c_vp], _c_int),
     "gm_tc_selftest": ([_c_i64, _c_i64, _c_int, _c_int, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
+    "gm_tc_selftest_timeout": ([_c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_i64, _c_vp], _c_int),
     "gm_mask_ring_runs": ([_c_i64, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
     "gm_cov_binned": ([_c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_i64, _c_vp, _c_vp, _c_vp,
                        _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),

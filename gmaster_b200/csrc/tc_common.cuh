@@ -53,9 +53,9 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t by
 // warps sharing its scheduler need.
 constexpr uint32_t kSuspendNs = 200000u;
 
-// Wait for the phase with parity `parity` to complete.  Returns false once kWaitNs of
-// global time have passed without completion.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+// Wait for the phase with parity `parity` to complete.  Returns false once `limit_ns` of
+// global time (kWaitNs by default) have passed without completion.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64_t limit_ns = kWaitNs)
 {
     const uint32_t addr = smem_u32(bar);
     uint64_t start = 0;
@@ -71,7 +71,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
         if (done) return true;
         const uint64_t now = global_ns();
         if (it == 0) start = now;
-        else if (now - start > kWaitNs) return false;
+        else if (now - start > limit_ns) return false;
     }
 }
 

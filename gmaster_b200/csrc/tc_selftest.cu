@@ -2,6 +2,11 @@
 // from K-major, 128-byte-swizzled bf16 operand images, exercising the bulk copy engine,
 // mbarriers, TMEM allocation, tcgen05.mma / commit and tcgen05.ld exactly as the
 // Legendre tensor-core kernels do.  Used by the GPU tests and as a device health check.
+//
+// With `skip_copies` the issuer arms the load barrier for both operand images but issues
+// no copy, so the bounded wait of every thread runs out after `wait_ns`: the kernel then
+// records the timeout in *err, skips the MMAs and the TMEM reads, releases its TMEM and
+// returns (the error path of the Legendre kernels, exercised without a fault or hang).
 #include "gm_common.cuh"
 #include "tc_common.cuh"
 
@@ -10,7 +15,8 @@ namespace gm {
 __global__ void __launch_bounds__(128) k_tc_selftest(int N, int K, int a_mn, int b_mn,
                                                      const uint8_t *__restrict__ aimg,
                                                      const uint8_t *__restrict__ bimg,
-                                                     float *__restrict__ D, int *__restrict__ err)
+                                                     float *__restrict__ D, int *__restrict__ err,
+                                                     uint64_t wait_ns, int skip_copies)
 {
     extern __shared__ uint8_t smem_raw[];
     __shared__ uint64_t bar_load, bar_mma;
@@ -37,10 +43,12 @@ __global__ void __launch_bounds__(128) k_tc_selftest(int N, int K, int a_mn, int
     const uint32_t taddr = tmem_base;
     if (tid == 0) {
         tc::mbar_arrive_expect_tx(&bar_load, a_bytes + b_bytes);
-        tc::bulk_g2s(sA, aimg, a_bytes, &bar_load);
-        tc::bulk_g2s(sB, bimg, b_bytes, &bar_load);
+        if (!skip_copies) {
+            tc::bulk_g2s(sA, aimg, a_bytes, &bar_load);
+            tc::bulk_g2s(sB, bimg, b_bytes, &bar_load);
+        }
     }
-    const bool loaded = tc::mbar_wait(&bar_load, 0);
+    const bool loaded = tc::mbar_wait(&bar_load, 0, wait_ns);
     if (tid == 0) {
         if (loaded) {
             const uint32_t idesc = tc::idesc_f16(128, N, 1, a_mn, b_mn);
@@ -63,7 +71,7 @@ __global__ void __launch_bounds__(128) k_tc_selftest(int N, int K, int a_mn, int
         }
     }
     bool done = true;
-    if (loaded) done = tc::mbar_wait(&bar_mma, 0);
+    if (loaded) done = tc::mbar_wait(&bar_mma, 0, wait_ns);
     if (!done && lane == 0) atomicExch(err, 2);
     tc::tc_fence_after();
     if (loaded && done) {
@@ -85,8 +93,24 @@ __global__ void __launch_bounds__(128) k_tc_selftest(int N, int K, int a_mn, int
 
 using namespace gm;
 
+static int launch_selftest(int64_t N, int64_t K, int a_mn, int b_mn, const void *aimg, const void *bimg,
+                           float *D, int32_t *err, uint64_t wait_ns, int skip_copies, void *stream);
+
 extern "C" int gm_tc_selftest(int64_t N, int64_t K, int a_mn, int b_mn, const void *aimg,
                               const void *bimg, float *D, int32_t *err, void *stream)
+{
+    return launch_selftest(N, K, a_mn, b_mn, aimg, bimg, D, err, tc::kWaitNs, 0, stream);
+}
+
+extern "C" int gm_tc_selftest_timeout(int64_t N, int64_t K, const void *aimg, const void *bimg,
+                                      float *D, int32_t *err, int64_t wait_ns, void *stream)
+{
+    if (wait_ns < 1000 || wait_ns > (int64_t)tc::kWaitNs) return GM_ERR_BAD_SHAPE;
+    return launch_selftest(N, K, 0, 0, aimg, bimg, D, err, (uint64_t)wait_ns, 1, stream);
+}
+
+static int launch_selftest(int64_t N, int64_t K, int a_mn, int b_mn, const void *aimg, const void *bimg,
+                           float *D, int32_t *err, uint64_t wait_ns, int skip_copies, void *stream)
 {
     if (N < 16 || N > 256 || (N % 16) || K < 64 || (K % 64) || 128 * K * 2 + N * K * 2 > 200 * 1024)
         return GM_ERR_BAD_SHAPE;
@@ -99,6 +123,7 @@ extern "C" int gm_tc_selftest(int64_t N, int64_t K, int a_mn, int b_mn, const vo
         return GM_ERR_LAUNCH;
     }
     k_tc_selftest<<<1, 128, smem, as_stream(stream)>>>((int)N, (int)K, a_mn, b_mn, (const uint8_t *)aimg,
-                                                      (const uint8_t *)bimg, D, (int *)err);
+                                                      (const uint8_t *)bimg, D, (int *)err, wait_ns,
+                                                      skip_copies);
     return check_launch("gm_tc_selftest");
 }

@@ -48,3 +48,17 @@ def selftest(N=128, K=128, seed=0, device="cuda", a_mn=False, b_mn=False):
     torch.cuda.synchronize()
     got = d.cpu()
     return float((got - want).abs().max()), float(want.abs().max()), int(err.item())
+
+
+def selftest_timeout(wait_ns=1_000_000, N=64, K=64, device="cuda"):
+    """Run the self-test with its operand copies withheld: returns (err flag, output
+    untouched), the flag 1 once every bounded wait has run out after `wait_ns`."""
+    dev = torch.device(device)
+    ai = torch.zeros(128 * K * 2, dtype=torch.uint8, device=dev)
+    bi = torch.zeros(N * K * 2, dtype=torch.uint8, device=dev)
+    d = torch.full((128, N), 7.0, dtype=torch.float32, device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    _lib.call("gm_tc_selftest_timeout", N, K, _lib.ptr(ai), _lib.ptr(bi), _lib.ptr(d), _lib.ptr(err),
+              int(wait_ns), _lib.stream_handle(dev))
+    torch.cuda.synchronize()
+    return int(err.item()), bool(torch.all(d == 7.0).item())

@@ -476,6 +476,14 @@ int gm_wigner_corr(int64_t nnodes, const double *x, int64_t lmax, int m, int n,
  * tensor-core machinery used by gm_legendre_*_tc. */
 int gm_tc_selftest(int64_t N, int64_t K, int a_mn, int b_mn, const void *aimg,
                    const void *bimg, float *D, int32_t *err, void *stream);
+/* gm_tc_selftest (K-major operands) whose issuer arms the load barrier but issues no copy:
+ * every bounded wait runs out after wait_ns (1 us .. 2 s) and *err is set to 1; the kernel
+ * skips its MMAs, releases its tensor memory and returns.  Exercises the timeout path of
+ * the tensor-core kernels (GM_ERR_TIMEOUT on the host) without a fault or a hang.  No
+ * counterpart in the reference (its FFI handlers map launch errors to XLA errors,
+ * march_v2.cu:509-518). */
+int gm_tc_selftest_timeout(int64_t N, int64_t K, const void *aimg, const void *bimg, float *D,
+                           int32_t *err, int64_t wait_ns, void *stream);
 
 #ifdef __cplusplus
 }
