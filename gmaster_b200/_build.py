@@ -73,6 +73,38 @@ def build(force=False, verbose=False, jobs=None):
     return LIB
 
 
+FFI_LIB = os.path.join(HERE, "libgm_b200_ffi.so")
+
+
+def ffi_include_dir():
+    """jaxlib's XLA FFI header directory, or None where JAX is not installed."""
+    try:
+        import jax.ffi
+
+        path = jax.ffi.include_dir()
+    except Exception:  # JAX absent or too old: no FFI headers
+        return None
+    return path if os.path.exists(os.path.join(path, "xla", "ffi", "api", "ffi.h")) else None
+
+
+def build_ffi():
+    """Compile csrc/ffi/gm_ffi.cc (the jax.ffi handlers) where jaxlib's headers exist;
+    returns the library path, or None when they do not."""
+    inc = ffi_include_dir()
+    if inc is None:
+        return None
+    lib = build()
+    src = os.path.join(HERE, "csrc", "ffi", "gm_ffi.cc")
+    cuda_inc = os.path.join(os.path.dirname(os.path.dirname(nvcc())) if os.path.sep in nvcc() else "/usr/local/cuda",
+                            "include")
+    subprocess.check_call(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-I" + inc, "-I" + cuda_inc,
+                           "-I" + os.path.join(ROOT, "include"), src, "-o", FFI_LIB, lib,
+                           "-Wl,-rpath," + HERE])
+    return FFI_LIB
+
+
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose="-v" in sys.argv)
     print(LIB)
+    if build_ffi():
+        print(FFI_LIB)

@@ -72,6 +72,7 @@ SIGNATURES = {
                                     _c_int, _c_vp], _c_int),
     "gm_lu_panel": ([_c_i64, _c_vp, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp], _c_int),
     "gm_lu_trsm": ([_c_i64, _c_vp, _c_i64, _c_i64, _c_vp], _c_int),
+    "gm_lu_update": ([_c_i64, _c_vp, _c_i64, _c_i64, _c_vp], _c_int),
     "gm_ring_big_scratch_bytes": ([_c_i64, _c_i64], _c_i64),
     "gm_ring_analysis_ws": ([_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_int, _c_vp, _c_vp, _c_vp, _c_vp,
                              _c_vp, _c_i64, _c_i64, _c_i64, _c_vp], _c_int),

@@ -11,7 +11,7 @@ that loop for a whole batch at once:
   generated Legendre row.  In FP64 each field goes through the FP64 transform.
 * ``compute_coupled_cells`` returns the coupled spectra of field pairs.
 * ``decouple_cells`` bins and decouples many spectra at once (one FP64 product with the
-  inverse of the binned coupling matrix, formed once per workspace from its LU factors).
+  LU factors of the binned coupling matrix, one right-hand side per simulation).
 * ``workspaces_from_fields`` builds many workspaces -- of uneven lmax too -- whose
   coupling blocks come from one persistent FP64 Wigner-3j launch sharing a device work
   queue, instead of one launch per workspace.
@@ -107,8 +107,8 @@ def compute_coupled_cells(fields1, fields2):
 
 
 def decouple_cells(workspace, cls, cl_bias=None, cl_noise=None):
-    """Bandpowers of many coupled spectra (each (ncls, lmax+1)) with one product by the
-    inverse of the binned coupling matrix.
+    """Bandpowers of many coupled spectra (each (ncls, lmax+1)) with one LU solve of the
+    binned coupling matrix for all of them (one right-hand side per spectrum).
 
     Equivalent to ``[workspace.decouple_cell(c, cl_bias, cl_noise) for c in cls]``.
     """
@@ -134,9 +134,9 @@ def decouple_cells(workspace, cls, cl_bias=None, cl_noise=None):
     nb = binned.shape[1]
     rhs = binned.reshape(len(cls), w.ncls, nb).permute(2, 1, 0).reshape(nb * w.ncls, len(cls))
     w._lu.check()
-    # one FP64 product with the inverse of the binned coupling matrix (computed once per
-    # workspace from its LU factors) instead of row-sequential triangular solves
-    sol = w._lu.inverse() @ rhs                                # (nb ncls, nsims)
+    # every simulation is one right-hand side of the LU solve (the factors of the binned
+    # coupling matrix, as decouple_cell uses them), all in one launch
+    sol = w._lu.solve(rhs)                                     # (nb ncls, nsims)
     out = sol.reshape(nb, w.ncls, len(cls)).permute(2, 1, 0)
     return [out[i] for i in range(len(cls))]
 

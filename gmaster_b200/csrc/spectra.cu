@@ -540,6 +540,61 @@ __global__ void k_lu_trsm(int64_t n, int64_t k0, int64_t k1, double *__restrict_
     }
 }
 
+// Blocked LU, trailing update: A[i][j] -= sum_{k in [k0, k1)} A[i][k] A[k][j] for i, j >= k1
+// (the Schur complement of the panel).  One CTA per 64 x 64 tile of the trailing matrix;
+// the panel width (<= 64) is taken in chunks of 32: the tile's rows of the left factor and
+// columns of the U rows are staged in shared memory and each of the 256 threads
+// accumulates a 4 x 4 block in FP64.
+constexpr int kLuTile = 64;
+constexpr int kLuK = 32;
+__global__ void __launch_bounds__(256) k_lu_update(int64_t n, int64_t k0, int64_t k1,
+                                                   double *__restrict__ a)
+{
+    __shared__ double sl[kLuTile][kLuK + 1];   // [row][k]
+    __shared__ double su[kLuTile][kLuK + 1];   // [col][k]
+    const int kw = (int)(k1 - k0);
+    const int64_t r0 = k1 + (int64_t)blockIdx.y * kLuTile, c0 = k1 + (int64_t)blockIdx.x * kLuTile;
+    const int tid = threadIdx.x;
+    const int ty = tid / 16, tx = tid % 16;   // rows 4 ty + i, columns tx + 16 j
+    double acc[4][4] = {};
+    for (int kc = 0; kc < kw; kc += kLuK) {
+        for (int e = tid; e < kLuTile * kLuK; e += 256) {
+            // left factor: consecutive threads take consecutive k of a row
+            const int r = e / kLuK, k = e % kLuK;
+            const int64_t gr = r0 + r;
+            sl[r][k] = (gr < n && kc + k < kw) ? a[gr * n + k0 + kc + k] : 0.0;
+            // U rows: consecutive threads take consecutive columns of a row
+            const int kk = e / kLuTile, c = e % kLuTile;
+            const int64_t gc = c0 + c;
+            su[c][kk] = (gc < n && kc + kk < kw) ? a[(k0 + kc + kk) * n + gc] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int k = 0; k < kLuK; ++k) {
+            double l[4], u[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) l[i] = sl[4 * ty + i][k];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) u[j] = su[tx + 16 * j][k];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fma(l[i], u[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int64_t gr = r0 + 4 * ty + i;
+        if (gr >= n) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int64_t gc = c0 + tx + 16 * j;
+            if (gc < n) a[gr * n + gc] -= acc[i][j];
+        }
+    }
+}
+
 // One warp per right-hand-side column: P, then L (unit) forward, then U backward.
 // b is (n, nrhs) row-major.
 __global__ void k_lu_solve(int64_t n, const double *__restrict__ lu, const int32_t *__restrict__ piv,
@@ -731,6 +786,16 @@ extern "C" int gm_lu_trsm(int64_t n, double *a, int64_t k0, int64_t k1, void *st
     if (k1 == n) return GM_OK;
     k_lu_trsm<<<(unsigned)((n - k1 + 127) / 128), 128, 0, as_stream(stream)>>>(n, k0, k1, a);
     return check_launch("gm_lu_trsm");
+}
+
+extern "C" int gm_lu_update(int64_t n, double *a, int64_t k0, int64_t k1, void *stream)
+{
+    if (n < 1 || k0 < 0 || k1 <= k0 || k1 - k0 > kLuTile || k1 > n) return GM_ERR_BAD_SHAPE;
+    if (!a) return GM_ERR_BAD_PTR;
+    if (k1 == n) return GM_OK;
+    const unsigned t = (unsigned)((n - k1 + kLuTile - 1) / kLuTile);
+    k_lu_update<<<dim3(t, t), 256, 0, as_stream(stream)>>>(n, k0, k1, a);
+    return check_launch("gm_lu_update");
 }
 
 extern "C" int gm_lu_solve(int64_t n, const double *lu, const int32_t *piv, int64_t nrhs,

@@ -204,8 +204,8 @@ def _slots(ncls):
 class LUFactor:
     """FP64 LU factorisation with partial pivoting of a square device matrix."""
 
-    # matrices above this order are factored in panels of _PANEL columns, the trailing
-    # updates as FP64 GEMMs; smaller ones in one single-CTA kernel
+    # matrices above this order are factored in panels of _PANEL columns (the trailing
+    # updates by the FP64 tile kernel gm_lu_update); smaller ones in one single-CTA kernel
     _BLOCKED_FROM = 256
     _PANEL = 64
 
@@ -225,21 +225,12 @@ class LUFactor:
             _lib.call("gm_lu_panel", n, _lib.ptr(A), k0, k1, _lib.ptr(self.piv), _lib.ptr(self.status), st)
             if k1 < n:
                 _lib.call("gm_lu_trsm", n, _lib.ptr(A), k0, k1, st)
-                A[k1:, k1:].addmm_(A[k1:, k0:k1], A[k0:k1, k1:], alpha=-1.0)
+                _lib.call("gm_lu_update", n, _lib.ptr(A), k0, k1, st)
 
     def check(self):
         st = int(self.status.item())
         if st:
             raise np.linalg.LinAlgError(f"binned coupling matrix is singular (pivot {st - 1})")
-
-    def inverse(self):
-        """A^-1 (computed once from the factors, one right-hand side per column).  Many
-        right-hand sides at once are cheaper as one FP64 matrix product with it than as
-        triangular solves, which walk the rows one after another."""
-        if getattr(self, "_inv", None) is None:
-            eye = torch.eye(self.n, dtype=torch.float64, device=self.lu.device)
-            self._inv = self.solve(eye)
-        return self._inv
 
     def solve(self, b):
         """Solve A x = b for b of shape (n,) or (n, nrhs)."""

@@ -231,12 +231,15 @@ int gm_bin_cells_csr(int64_t lmax, int64_t nbands, int64_t ncls, const double *c
 int gm_lu_factor(int64_t n, double *a, int32_t *piv, int32_t *status, void *stream);
 /* Blocked form of gm_lu_factor (same factors, pivots and status; the caller zeroes
  * `status`): for each panel [k0, k1): gm_lu_panel (pivoting and factoring the panel's
- * columns, whole-row swaps), gm_lu_trsm (the U rows right of the panel), then the caller's
- * GEMM A[k1:, k1:] -= A[k1:, k0:k1] A[k0:k1, k1:].  Replaces the reference's
+ * columns, whole-row swaps), gm_lu_trsm (the U rows right of the panel), then
+ * gm_lu_update (A[k1:, k1:] -= A[k1:, k0:k1] A[k0:k1, k1:]).  Replaces the reference's
  * jnp.linalg.solve factorisation (workspaces.py:2146) for large binned matrices. */
 int gm_lu_panel(int64_t n, double *a, int64_t k0, int64_t k1, int32_t *piv, int32_t *status,
                 void *stream);
 int gm_lu_trsm(int64_t n, double *a, int64_t k0, int64_t k1, void *stream);
+/* Blocked LU trailing update after panel [k0, k1) (k1 - k0 <= 64): a[i][j] -= sum_k
+ * a[i][k] a[k][j] over k in [k0, k1), for i, j >= k1, in FP64 (64 x 64 tiles). */
+int gm_lu_update(int64_t n, double *a, int64_t k0, int64_t k1, void *stream);
 int gm_lu_solve(int64_t n, const double *lu, const int32_t *piv, int64_t nrhs,
                 double *b, void *stream);
 

@@ -582,3 +582,79 @@ def test_oracle_general_assembly_reduces_to_the_spin2_assembly():
         blocks = {"tt": tt, "te": te, "pp": even, "mm": odd}
         np.testing.assert_array_equal(oracle.assemble_general_mcm(te, even, odd, tt, n - 1, s1, s2),
                                       oracle.assemble_mcm(blocks, n - 1, s1, s2))
+
+
+def _split_args(text):
+    """Top-level comma-separated arguments of a call's parenthesised text."""
+    depth, cur, out = 0, [], []
+    for ch in text.replace("->", "."):
+        if ch in "(<[{":
+            depth += 1
+        elif ch in ")>]}":
+            depth -= 1
+        if ch == "," and depth == 0:
+            out.append("".join(cur).strip())
+            cur = []
+        else:
+            cur.append(ch)
+    if "".join(cur).strip():
+        out.append("".join(cur).strip())
+    return out
+
+
+def _balanced(src, start):
+    """Text between the parenthesis at src[start] and its match."""
+    depth = 0
+    for i in range(start, len(src)):
+        if src[i] == "(":
+            depth += 1
+        elif src[i] == ")":
+            depth -= 1
+            if depth == 0:
+                return src[start + 1:i]
+    raise ValueError("unbalanced")
+
+
+def test_ffi_handlers_bind_header_entry_points():
+    """gmaster_b200/csrc/ffi/gm_ffi.cc (the jax.ffi handlers, compiled where jaxlib's XLA FFI
+    headers exist): every gmb_* symbol is bound to a handler defined in the file whose
+    parameters follow its binding (stream, Arg buffers, Ret buffers, then attributes of the
+    bound types), and every gm_* call passes as many arguments as include/gm_b200.h declares."""
+    import os
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = open(os.path.join(root, "gmaster_b200", "csrc", "ffi", "gm_ffi.cc")).read()
+    header = open(os.path.join(root, "include", "gm_b200.h")).read()
+    decl = {m.group(2): len(_split_args(m.group(3))) for m in
+            re.finditer(r"\b(int|int64_t|const char \*)\s+(gm_\w+)\s*\(([^;]*?)\);", header, re.S)}
+    impls = {}
+    for m in re.finditer(r"ffi::Error\s+(\w+)\s*\(", src):
+        params = _split_args(_balanced(src, m.end() - 1))
+        impls[m.group(1)] = params
+    symbols = re.findall(r"XLA_FFI_DEFINE_HANDLER_SYMBOL\((gmb_\w+),\s*(\w+),", src)
+    assert len(symbols) >= 20
+    for sym, impl in symbols:
+        assert impl in impls, (sym, impl)
+        start = src.index(f"XLA_FFI_DEFINE_HANDLER_SYMBOL({sym},")
+        binding = _balanced(src, src.index("(", start))
+        kinds = re.findall(r"\.(Arg|Ret|Attr)<([^>]+)>", binding)
+        params = impls[impl]
+        assert params[0].startswith("cudaStream_t"), sym
+        assert len(params) == 1 + len(kinds), (sym, len(params), len(kinds))
+        for (kind, typ), param in zip(kinds, params[1:]):
+            if kind == "Arg":
+                assert param.startswith("ffi::AnyBuffer"), (sym, param)
+            elif kind == "Ret":
+                assert param.startswith("ffi::Result<ffi::AnyBuffer>"), (sym, param)
+            else:
+                assert param.split()[0] == typ, (sym, param, typ)
+    calls = 0
+    for m in re.finditer(r"\b(gm_\w+)\(", src):
+        name = m.group(1)
+        if name == "gm_last_error":
+            continue
+        assert name in decl, name
+        args = _split_args(_balanced(src, m.end() - 1))
+        assert len(args) == decl[name], (name, len(args), decl[name])
+        calls += 1
+    assert calls >= 20
