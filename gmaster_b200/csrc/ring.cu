@@ -13,6 +13,8 @@
 // (gmaster/_native/cuda/march_v2.cu:426-493).
 #include <math.h>
 
+#include <type_traits>
+
 #include "gm_common.cuh"
 
 namespace gm {
@@ -653,67 +655,91 @@ __device__ float2 *bs_apply(float2 *X, float2 *Y, const float2 *FB, int h, int n
     return Z;
 }
 
-template <typename Tin>
+// T = float: three buffers of Mmax complex floats per slot (Bluestein rings included).
+// T = double: no Bluestein path (the mixed-radix FFT takes every ring, as in the FP64
+// shared-memory kernel); two buffers of 2 nside complex doubles per slot, which fit the
+// same slot bytes (64 nside <= 96 nside).
+template <typename T, typename Tin>
 __global__ void __launch_bounds__(512) k_ring_analysis_big(int64_t nside, int64_t L, int64_t ncomp,
                                                            const Tin *__restrict__ maps,
                                                            const double *__restrict__ mask,
                                                            const void *__restrict__ twall,
                                                            int64_t twcnt,
                                                            const uint8_t *__restrict__ shifted,
-                                                           float2 *__restrict__ out, int hcap,
-                                                           int bsmin, float2 *__restrict__ gbuf,
-                                                           int64_t Mmax)
+                                                           typename vec2<T>::type *__restrict__ out,
+                                                           int hcap, int bsmin, void *__restrict__ gscratch,
+                                                           int64_t slot_bytes)
 {
+    using T2 = typename vec2<T>::type;
+    constexpr bool kSingle = std::is_same<T, float>::value;
     const int64_t nring = 4 * nside - 1, npix = 12 * nside * nside;
-    float2 *b0 = gbuf + (int64_t)blockIdx.x * 3 * Mmax, *b1 = b0 + Mmax, *b2 = b1 + Mmax;
-    const float2 *tw32 = TwTable<float2>::get(twall, twcnt);
-    const float w = (float)(4.0 * M_PI / (double)npix);
+    T2 *b0 = reinterpret_cast<T2 *>(static_cast<unsigned char *>(gscratch) + blockIdx.x * slot_bytes);
+    const int64_t bstride = kSingle ? 4 * nside : 2 * nside;
+    T2 *b1 = b0 + bstride, *b2 = b1 + bstride;
+    const T2 *twT = TwTable<T2>::get(twall, twcnt);
+    const T w = (T)(4.0 * M_PI / (double)npix);
     for (int64_t r = blockIdx.x; r < nring; r += gridDim.x) {
         const int n = (int)ring_nphi(nside, r), h = n / 2;
         if (!ring_big(h, hcap, (int)nside, bsmin)) continue;
         const int64_t off = ring_offset(nside, r);
-        const float2 *tw = tw32 + twiddle_offset(n);
+        const T2 *tw = twT + twiddle_offset(n);
         const bool sh = shifted[r] != 0;
-        const bool bs = bluestein_big(h, (int)nside, bsmin);
-        const int M = bs ? next_pow2(2 * h - 1) : 0;
-        const float2 *twM = bs ? tw32 + twiddle_offset(M) : nullptr;
-        float2 *FB = nullptr, *X = b0, *Y = b1;
-        if (bs) {
-            FB = bs_filter(h, n, M, tw, twM, -1, b0, b1);
-            X = (FB == b0) ? b1 : b0;
-            Y = b2;
-        }
-        for (int64_t c = 0; c < ncomp; ++c) {
-            float2 *Z;
+        if constexpr (kSingle) {
+            const bool bs = bluestein_big(h, (int)nside, bsmin);
+            const int M = bs ? next_pow2(2 * h - 1) : 0;
+            const float2 *twM = bs ? twT + twiddle_offset(M) : nullptr;
+            float2 *FB = nullptr, *X = b0, *Y = b1;
             if (bs) {
-                load_ring<float>(maps + c * npix + off, mask ? mask + off : nullptr, h, X,
-                                 [&](int t, float2 z) { return cmul(z, bs_chirp(tw, h, n, t, -1)); });
-                __syncthreads();
-                Z = bs_apply(X, Y, FB, h, n, M, tw, twM, -1);
-            } else {
-                load_ring<float>(maps + c * npix + off, mask ? mask + off : nullptr, h, X,
-                                 [](int, float2 z) { return z; });
-                __syncthreads();
-                Z = fft_shared(X, Y, h, tw, -1);
+                FB = bs_filter(h, n, M, tw, twM, -1, b0, b1);
+                X = (FB == b0) ? b1 : b0;
+                Y = b2;
             }
-            ring_outputs<float>(Z, n, L, tw, sh, w, out + (c * nring + r) * L);
-            __syncthreads();
+            for (int64_t c = 0; c < ncomp; ++c) {
+                float2 *Z;
+                if (bs) {
+                    load_ring<float>(maps + c * npix + off, mask ? mask + off : nullptr, h, X,
+                                     [&](int t, float2 z) { return cmul(z, bs_chirp(tw, h, n, t, -1)); });
+                    __syncthreads();
+                    Z = bs_apply(X, Y, FB, h, n, M, tw, twM, -1);
+                } else {
+                    load_ring<float>(maps + c * npix + off, mask ? mask + off : nullptr, h, X,
+                                     [](int, float2 z) { return z; });
+                    __syncthreads();
+                    Z = fft_shared(X, Y, h, tw, -1);
+                }
+                ring_outputs<float>(Z, n, L, tw, sh, w, out + (c * nring + r) * L);
+                __syncthreads();
+            }
+        } else {
+            for (int64_t c = 0; c < ncomp; ++c) {
+                load_ring<T>(maps + c * npix + off, mask ? mask + off : nullptr, h, b0,
+                             [](int, T2 z) { return z; });
+                __syncthreads();
+                T2 *Z = fft_shared(b0, b1, h, tw, -1);
+                ring_outputs<T>(Z, n, L, tw, sh, w, out + (c * nring + r) * L);
+                __syncthreads();
+            }
         }
     }
 }
 
+template <typename T>
 __global__ void __launch_bounds__(512) k_ring_synthesis_big(int64_t nside, int64_t L, int64_t ncomp,
-                                                            const float *__restrict__ syn,
+                                                            const T *__restrict__ syn,
                                                             const void *__restrict__ twall,
                                                             int64_t twcnt,
                                                             const uint8_t *__restrict__ shifted,
                                                             double *__restrict__ maps, int hcap,
-                                                            int bsmin, float2 *__restrict__ gbuf,
-                                                            int64_t Mmax)
+                                                            int bsmin, void *__restrict__ gscratch,
+                                                            int64_t slot_bytes)
 {
+    using T2 = typename vec2<T>::type;
+    constexpr bool kSingle = std::is_same<T, float>::value;
     const int64_t nring = 4 * nside - 1, npix = 12 * nside * nside, nlanes = 2 * nside;
-    float2 *b0 = gbuf + (int64_t)blockIdx.x * 3 * Mmax, *b1 = b0 + Mmax, *b2 = b1 + Mmax;
-    const float2 *tw32 = TwTable<float2>::get(twall, twcnt);
+    T2 *b0 = reinterpret_cast<T2 *>(static_cast<unsigned char *>(gscratch) + blockIdx.x * slot_bytes);
+    const int64_t bstride = kSingle ? 4 * nside : 2 * nside;
+    T2 *b1 = b0 + bstride, *b2 = b1 + bstride;
+    const T2 *twT = TwTable<T2>::get(twall, twcnt);
     for (int64_t r = blockIdx.x; r < nring; r += gridDim.x) {
         const int n = (int)ring_nphi(nside, r), h = n / 2;
         if (!ring_big(h, hcap, (int)nside, bsmin)) continue;
@@ -721,45 +747,54 @@ __global__ void __launch_bounds__(512) k_ring_synthesis_big(int64_t nside, int64
         const bool south = r >= nlanes;
         const int64_t j = south ? 4 * nside - 2 - r : r;
         const bool sh = shifted[r] != 0;
-        const float2 *tw = tw32 + twiddle_offset(n);
-        float2 cpi;
+        const T2 *tw = twT + twiddle_offset(n);
+        T2 cpi;
         {
             double s1, c1d;
             sincospi(-1.0 / (double)n, &s1, &c1d);
-            cpi = make_float2((float)c1d, (float)s1);
+            cpi = make2<T2, T>((T)c1d, (T)s1);
         }
-        const bool bs = bluestein_big(h, (int)nside, bsmin);
-        const int M = bs ? next_pow2(2 * h - 1) : 0;
-        const float2 *twM = bs ? tw32 + twiddle_offset(M) : nullptr;
-        float2 *FB = nullptr, *X = b0, *Y = b1;
-        if (bs) {
-            FB = bs_filter(h, n, M, tw, twM, +1, b0, b1);
-            X = (FB == b0) ? b1 : b0;
-            Y = b2;
+        bool bs = false;
+        int M = 0;
+        const T2 *twM = nullptr;
+        T2 *FB = nullptr, *X = b0, *Y = b1;
+        if constexpr (kSingle) {
+            bs = bluestein_big(h, (int)nside, bsmin);
+            M = bs ? next_pow2(2 * h - 1) : 0;
+            twM = bs ? twT + twiddle_offset(M) : nullptr;
+            if (bs) {
+                FB = bs_filter(h, n, M, tw, twM, +1, b0, b1);
+                X = (FB == b0) ? b1 : b0;
+                Y = b2;
+            }
         }
-        const float *base = syn + (south ? 2 : 0);
+        const T *base = syn + (south ? 2 : 0);
         for (int64_t c = 0; c < ncomp; ++c) {
             for (int k = threadIdx.x; k < h; k += blockDim.x) {
-                float c0[2], c1[2], dummy[2];
+                T c0[2], c1[2], dummy[2];
                 residue_sums(base, L, nlanes, ncomp, j, c, k, n, sh, false, c0, dummy);
                 residue_sums(base, L, nlanes, ncomp, j, c, k + h, n, sh, false, c1, dummy);
-                float2 ck = make_float2(c0[0], c0[1]);
-                float2 ckh = make_float2(c1[0], c1[1]);
+                T2 ck = make2<T2, T>(c0[0], c0[1]);
+                T2 ckh = make2<T2, T>(c1[0], c1[1]);
                 if (sh) {
                     ck = cmul(ck, phase_pi(tw, h, k, cpi, +1));
                     ckh = cmul(ckh, phase_pi(tw, h, k + h, cpi, +1));
                 }
-                const float2 sum = cadd(ck, ckh);
-                const float2 dif = cmul(csub(ck, ckh), twiddle_n(tw, h, k, +1));
-                float2 z = make_float2(sum.x - dif.y, sum.y + dif.x);
-                if (bs) z = cmul(z, bs_chirp(tw, h, n, k, +1));
+                const T2 sum = cadd(ck, ckh);
+                const T2 dif = cmul(csub(ck, ckh), twiddle_n(tw, h, k, +1));
+                T2 z = make2<T2, T>(sum.x - dif.y, sum.y + dif.x);
+                if constexpr (kSingle) {
+                    if (bs) z = cmul(z, bs_chirp(tw, h, n, k, +1));
+                }
                 X[k] = z;
             }
             __syncthreads();
-            float2 *Z = bs ? bs_apply(X, Y, FB, h, n, M, tw, twM, +1) : fft_shared(X, Y, h, tw, +1);
+            T2 *Z;
+            if constexpr (kSingle) Z = bs ? bs_apply(X, Y, FB, h, n, M, tw, twM, +1) : fft_shared(X, Y, h, tw, +1);
+            else Z = fft_shared(X, Y, h, tw, +1);
             double *dst = maps + c * npix + off;
             for (int t = threadIdx.x; t < h; t += blockDim.x) {
-                const float2 z = Z[t];
+                const T2 z = Z[t];
                 dst[2 * t] = (double)z.x;
                 dst[2 * t + 1] = (double)z.y;
             }
@@ -833,7 +868,7 @@ extern "C" int gm_ring_analysis_ws(int precision, int64_t nside, int64_t L, int6
                                    void *scratch, int64_t scratch_bytes, int64_t hcap_max,
                                    int64_t bs_min, void *stream)
 {
-    const bool big = precision == GM_MIXED && scratch != nullptr;
+    const bool big = scratch != nullptr;
     if (nside < 1 || nside > 8192 || L < 1 || ncomp < 1 || ncomp > 65535) return GM_ERR_BAD_SHAPE;
     if (!big && !ring_shape_ok(precision, nside, L, ncomp)) return GM_ERR_BAD_SHAPE;
     if (!maps || !tw || !shifted || !ringspec) return GM_ERR_BAD_PTR;
@@ -843,21 +878,32 @@ extern "C" int gm_ring_analysis_ws(int precision, int64_t nside, int64_t L, int6
     const int64_t nring = 4 * nside - 1, cnt = gm_ring_twiddle_count(nside);
     int hcap = ring_hcap(precision, nside, big);
     if (big && hcap_max > 0 && hcap_max < hcap) hcap = (int)hcap_max;
-    const int bsmin = big ? (bs_min > 0 ? (int)bs_min : 8192) : 0;
+    // single precision only: FP64 has no Bluestein path
+    const int bsmin = big && precision == GM_MIXED ? (bs_min > 0 ? (int)bs_min : 8192) : 0;
     const size_t smem = 2 * (size_t)hcap * (precision == GM_FP64 ? sizeof(double2) : sizeof(float2));
+    const int64_t slot = gm_ring_big_scratch_bytes(nside, 1);
     int threads = nside >= 256 ? 512 : 128;
     dim3 grid((unsigned)nring, (unsigned)ncomp);
     cudaStream_t s = as_stream(stream);
     int st;
     if (precision == GM_FP64) {
+        const unsigned gbig = (unsigned)(nslots < nring ? nslots : nring);
         if (map_dtype_bytes == 8) {
             if ((st = set_smem(k_ring_analysis<double, double>, smem))) return st;
             k_ring_analysis<double, double><<<grid, threads, smem, s>>>(
                 nside, L, (const double *)maps, mask, tw, cnt, shifted, (double2 *)ringspec, 0, hcap, 0);
+            if (big)
+                k_ring_analysis_big<double, double><<<gbig, 512, 0, s>>>(
+                    nside, L, ncomp, (const double *)maps, mask, tw, cnt, shifted, (double2 *)ringspec,
+                    hcap, 0, scratch, slot);
         } else {
             if ((st = set_smem(k_ring_analysis<double, float>, smem))) return st;
             k_ring_analysis<double, float><<<grid, threads, smem, s>>>(
                 nside, L, (const float *)maps, mask, tw, cnt, shifted, (double2 *)ringspec, 0, hcap, 0);
+            if (big)
+                k_ring_analysis_big<double, float><<<gbig, 512, 0, s>>>(
+                    nside, L, ncomp, (const float *)maps, mask, tw, cnt, shifted, (double2 *)ringspec,
+                    hcap, 0, scratch, slot);
         }
     } else if (precision == GM_MIXED) {
         const int mcap = bluestein_mcap(nside);
@@ -874,9 +920,9 @@ extern "C" int gm_ring_analysis_ws(int precision, int64_t nside, int64_t L, int6
                 nside, L, ncomp, cpc, mcap, hcap, bsmin, (const double *)maps, mask, tw, cnt, shifted,
                 (float2 *)ringspec);
             if (big)
-                k_ring_analysis_big<double><<<gbig, 512, 0, s>>>(
+                k_ring_analysis_big<float, double><<<gbig, 512, 0, s>>>(
                     nside, L, ncomp, (const double *)maps, mask, tw, cnt, shifted, (float2 *)ringspec,
-                    hcap, bsmin, (float2 *)scratch, 4 * nside);
+                    hcap, bsmin, scratch, slot);
         } else {
             if ((st = set_smem(k_ring_analysis<float, float>, smem))) return st;
             k_ring_analysis<float, float><<<grid, threads, smem, s>>>(
@@ -886,9 +932,9 @@ extern "C" int gm_ring_analysis_ws(int precision, int64_t nside, int64_t L, int6
                 nside, L, ncomp, cpc, mcap, hcap, bsmin, (const float *)maps, mask, tw, cnt, shifted,
                 (float2 *)ringspec);
             if (big)
-                k_ring_analysis_big<float><<<gbig, 512, 0, s>>>(
+                k_ring_analysis_big<float, float><<<gbig, 512, 0, s>>>(
                     nside, L, ncomp, (const float *)maps, mask, tw, cnt, shifted, (float2 *)ringspec,
-                    hcap, bsmin, (float2 *)scratch, 4 * nside);
+                    hcap, bsmin, scratch, slot);
         }
     } else {
         return GM_ERR_UNSUPPORTED;
@@ -951,7 +997,7 @@ extern "C" int gm_ring_synthesis_ws(int precision, int64_t nside, int64_t L, int
                                     double *maps, void *scratch, int64_t scratch_bytes,
                                     int64_t hcap_max, int64_t bs_min, void *stream)
 {
-    const bool big = precision == GM_MIXED && scratch != nullptr;
+    const bool big = scratch != nullptr;
     if (nside < 1 || nside > 8192 || L < 1 || ncomp < 1 || ncomp > 65535) return GM_ERR_BAD_SHAPE;
     if (!big && !ring_shape_ok(precision, nside, L, ncomp)) return GM_ERR_BAD_SHAPE;
     if (!syn || !tw || !shifted || !maps) return GM_ERR_BAD_PTR;
@@ -960,8 +1006,10 @@ extern "C" int gm_ring_synthesis_ws(int precision, int64_t nside, int64_t L, int
     const int64_t nring = 4 * nside - 1, cnt = gm_ring_twiddle_count(nside);
     int hcap = ring_hcap(precision, nside, big);
     if (big && hcap_max > 0 && hcap_max < hcap) hcap = (int)hcap_max;
-    const int bsmin = big ? (bs_min > 0 ? (int)bs_min : 8192) : 0;
+    const int bsmin = big && precision == GM_MIXED ? (bs_min > 0 ? (int)bs_min : 8192) : 0;
     const size_t smem = 2 * (size_t)hcap * (precision == GM_FP64 ? sizeof(double2) : sizeof(float2));
+    const int64_t slot = gm_ring_big_scratch_bytes(nside, 1);
+    const unsigned gbig = (unsigned)(nslots < nring ? nslots : nring);
     int threads = nside >= 256 ? 512 : 128;
     dim3 grid((unsigned)nring, (unsigned)ncomp);
     cudaStream_t s = as_stream(stream);
@@ -970,14 +1018,16 @@ extern "C" int gm_ring_synthesis_ws(int precision, int64_t nside, int64_t L, int
         if ((st = set_smem(k_ring_synthesis<double>, smem))) return st;
         k_ring_synthesis<double><<<grid, threads, smem, s>>>(nside, L, ncomp, (const double *)syn,
                                                              tw, cnt, shifted, maps, hcap, 0);
+        if (big)
+            k_ring_synthesis_big<double><<<gbig, 512, 0, s>>>(nside, L, ncomp, (const double *)syn, tw, cnt,
+                                                              shifted, maps, hcap, 0, scratch, slot);
     } else if (precision == GM_MIXED) {
         if ((st = set_smem(k_ring_synthesis<float>, smem))) return st;
         k_ring_synthesis<float><<<grid, threads, smem, s>>>(nside, L, ncomp, (const float *)syn,
                                                             tw, cnt, shifted, maps, hcap, bsmin);
         if (big)
-            k_ring_synthesis_big<<<(unsigned)(nslots < nring ? nslots : nring), 512, 0, s>>>(
-                nside, L, ncomp, (const float *)syn, tw, cnt, shifted, maps, hcap, bsmin,
-                (float2 *)scratch, 4 * nside);
+            k_ring_synthesis_big<float><<<gbig, 512, 0, s>>>(nside, L, ncomp, (const float *)syn, tw, cnt,
+                                                             shifted, maps, hcap, bsmin, scratch, slot);
     } else {
         return GM_ERR_UNSUPPORTED;
     }

@@ -240,15 +240,14 @@ def ring_analysis(plan, maps, prec, mask=None, out=None):
     return spec
 
 
-# Global-memory ring path (single precision): a scratch of two slots per SM for the rings
-# that do not fit the shared-memory kernels (Nside above 4096).  The knobs lower the
-# thresholds that send a ring there (0: the defaults); they exist for tests.
+# Global-memory ring path: a scratch of two slots per SM for the rings that do not fit the
+# shared-memory kernels (single precision above Nside 4096, double precision above Nside
+# 2048).  The knobs lower the thresholds that send a ring there (0: the defaults); they
+# exist for tests.
 RING_TUNING = {"hcap_max": 0, "bs_min": 0}
 
 
 def _ring_scratch(plan, prec):
-    if prec != _lib.MIXED:
-        return None, 0
     sc = getattr(plan, "_ring_scratch_buf", None)
     if sc is None:
         nslots = 2 * torch.cuda.get_device_properties(plan.device).multi_processor_count
