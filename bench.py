@@ -40,13 +40,17 @@ METRIC = "MASTER sims/s, Nside 2048 TQU (shared workspace, n_iter=3), mixed prec
 os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "expandable_segments:True")
 
 
-# Kernel behind each timed Legendre pass, and the DRAM traffic of one launch of it at the
-# Nside 2048, 32-simulation workload (dram__bytes_read.sum + dram__bytes_write.sum from one
-# ncu capture of that launch; None where not captured).
-KERNEL_OF = {"tc_analysis_s2": "k_ana_tc<2>", "tc_analysis_s0": "k_ana_tc<0>",
-             "tc_synthesis_s2": "k_syn_tc<2>", "tc_synthesis_s0": "k_syn_tc<0>"}
-TRAFFIC_PER_LAUNCH = {"tc_analysis_s2": 214.29e9, "tc_analysis_s0": 194.95e9,
-                      "tc_synthesis_s2": 23.21e9, "tc_synthesis_s0": 23.22e9}
+# Kernel behind each timed Legendre pass (the checkpointed kernels of legendre_ck.cu when
+# the geometry's checkpoint tables are in use, else the carried-state ones of
+# legendre_tc.cu), and the DRAM traffic of one launch of it at the Nside 2048,
+# 32-simulation workload (dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of
+# the kernel on the Nside 512 case, scaled to Nside 2048 by the launch's units of work;
+# None where not captured).
+KERNEL_OF = {"tc_analysis_s2": "k_ana_ck<2>", "tc_analysis_s0": "k_ana_ck<0>",
+             "tc_synthesis_s2": "k_syn_ck<2>", "tc_synthesis_s0": "k_syn_ck<0>"}
+KERNEL_OF_CARRIED = {"tc_analysis_s2": "k_ana_tc<2>", "tc_analysis_s0": "k_ana_tc<0>",
+                     "tc_synthesis_s2": "k_syn_tc<2>", "tc_synthesis_s0": "k_syn_tc<0>"}
+TRAFFIC_PER_LAUNCH = {}
 
 
 def parse():
@@ -693,8 +697,8 @@ def run_mc1024(args):
         "value": nsims * 1e3 / ms_batched, "unit": "sims/s", "n_gpus": 1, "steps": nsims // S,
         "warmup": args.warmup, "ms_per_step": ms_batched / (nsims // S), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
-        "dtype": "f16x3 tensor-core products (f32 accumulate), f64 recurrence and alm accumulation, "
-                 "f32 ring FFTs",
+        "dtype": "f16x3 tensor-core products (f32 accumulate), f32 difference-form rows restarted "
+                 "from f64 checkpoints every 128 rows, f64 alm accumulation, f32 ring FFTs",
         "data": "synthetic (seeded Gaussian TQU sims, config mask recipe at Nside 1024)",
         "config": {"workload": "512 Nside 1024 TQU simulations in batches of 32 through "
                                "mc_bandpowers; per-simulation CUDA graph and eager timings on 32",
@@ -1156,6 +1160,19 @@ def main():
     t_all, qu_all = make_sims(nside, S, 1000 + 7919 * rank, dev)
     torch.cuda.synchronize()
 
+    # per-geometry constants of the tensor-core and one-field mixed paths (the checkpoint
+    # tables of the spin-0 and spin-2 rows), built once and kept, as the reference keeps its
+    # window tables (march_v2.py:388-450): their build time is reported on its own
+    from gmaster_b200 import sht_tc
+
+    tp = sht_tc.get_tc_plan(nside, lmax, dev)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ck_built = [sht_tc.ck_tables(tp, sp) is not None for sp in (0, 2)]
+    torch.cuda.synchronize()
+    table_ms = 1e3 * (time.perf_counter() - t0)
+    kernel_of = KERNEL_OF if all(ck_built) else KERNEL_OF_CARRIED
+
     # full estimator from scratch for one simulation (seconds per spectrum)
     s_per_spec = {}
     spec_stages = {}
@@ -1287,8 +1304,8 @@ def main():
         "metric": METRIC, "value": value, "unit": "sims/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f16x3 tensor-core products (f32 accumulate), f64 recurrence and alm accumulation, "
-                 "f32 ring FFTs",
+        "dtype": "f16x3 tensor-core products (f32 accumulate), f32 difference-form rows restarted "
+                 "from f64 checkpoints every 128 rows, f64 alm accumulation, f32 ring FFTs",
         "data": "synthetic (seeded Gaussian TQU sims and analytic mask of the Nside 2048 recipe)",
         "config": {
             "workload": f"batch of {S} Nside {nside} TQU simulations through fields_from_maps x2, "
@@ -1300,7 +1317,7 @@ def main():
         "e2e": {"value": value_e2e, "unit": "sims/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h[0]), "pinned": pinned},
         "roofline": {
-            "bound": "tensor", "kernel": KERNEL_OF.get(dominant, dominant),
+            "bound": "tensor", "kernel": kernel_of.get(dominant, dominant),
             "achieved": dom_tflops, "peak": peak, "unit": "TFLOP/s",
             "frac": dom_tflops / peak, "traffic": TRAFFIC_PER_LAUNCH.get(dominant),
             "note": "algorithmic flops per launch (one complex MAC = 4 flops per (l, m, lane) and "
@@ -1318,6 +1335,11 @@ def main():
         "speedup_mixed_vs_fp64": value / value64,
         "s_per_spectrum": s_per_spec,
         "s_per_spectrum_stages_ms": spec_stages,
+        "geometry_tables": {"checkpoint_tables_built": all(ck_built), "build_ms": table_ms,
+                            "gb": sum(sht_tc.ck_table_bytes(tp, sp) for sp in (0, 2)) / 1e9,
+                            "note": "checkpoint tables of the spin-0 and spin-2 rows at this Nside, "
+                                    "built once per geometry before the timed regions and kept"},
+        "peak_device_gb": torch.cuda.max_memory_allocated(dev) / 1e9,
         "bandpower_err_mixed_vs_fp64": {"max_abs_over_scale": errs, "max_rel_auto": rel_auto,
                                         "max_in_sigma_cv": sig_cv, "fsky": fsky},
         "clocks": clocks,
