@@ -191,3 +191,44 @@ def test_arbitrary_spin_workspaces_match_oracle(cuda, spins, is_teb):
     cl = rng.random((ncls, lmax + 1))
     ref = oracle.decouple(oracle.binned_mcm(want, lmax, nlb, ncls), cl, lmax, nlb)
     assert _rel(w.decouple_cell(cl).cpu().numpy(), ref) < 1e-9
+
+
+@pytest.mark.parametrize("spins,is_teb", [((1, 3), False), ((0, 1), False), ((0, 3), True)])
+def test_arbitrary_spin_workspaces_with_toeplitz_match_oracle(cuda, spins, is_teb):
+    """The Toeplitz branch of the general-spin workspaces (workspaces.py:1832-1843): every
+    quadrature block is approximated as (M / (2 l' + 1)) -> Toeplitz -> x (2 l' + 1), and the
+    scalar block of a TEB workspace is the Toeplitz TT block; against the oracle's quadrature
+    blocks through its restatement of the reference's _apply_toeplitz (golden-pinned)."""
+    nside, nlb = 8, 2
+    lmax = 3 * nside - 1
+    lt, le, db = 14, 4, 3
+    rng = np.random.default_rng(19)
+    masks = [rng.uniform(0.2, 1, 12 * nside ** 2), rng.uniform(0.2, 1, 12 * nside ** 2)]
+    fields = []
+    for mask, spin in zip(masks, spins):
+        maps = rng.normal(size=(1 if spin == 0 else 2, len(mask)))
+        fields.append(nmt.NmtField(mask, maps, spin=spin, lmax=lmax, lmax_mask=lmax, n_iter=0,
+                                   n_iter_mask=0, precision="fp64"))
+    b = nmt.NmtBin.from_lmax_linear(lmax, nlb)
+    w = nmt.NmtWorkspace.from_fields(*fields, b, is_teb=is_teb, l_toeplitz=lt, l_exact=le, dl_band=db)
+    a1 = oracle.map2alm(masks[0][None], 0, nside, lmax, 0)
+    a2 = oracle.map2alm(masks[1][None], 0, nside, lmax, 0)
+    window = oracle.pcl(a1, a2, lmax)[0]
+    cols = (2.0 * np.arange(lmax + 1) + 1.0)[None, :]
+
+    def approx(x):
+        return None if x is None else oracle.apply_toeplitz(x / cols, lt, le, db) * cols
+
+    s1, s2 = spins
+    te = even = odd = None
+    if s1 == 0 or s2 == 0:
+        e, o = oracle.coupling_quadrature(window, lmax, s1, s2, s1, s2, lmax_mask=lmax)
+        te = e + o
+    else:
+        even, odd = oracle.coupling_quadrature(window, lmax, s1, s2, s1, s2, lmax_mask=lmax)
+    if is_teb:
+        even, odd = oracle.coupling_quadrature(window, lmax, s2, s2, s2, s2, lmax_mask=lmax)
+    te, even, odd = approx(te), approx(even), approx(odd)
+    tt = oracle.coupling_tt_toeplitz(window, lmax, lt, le, db)
+    want = oracle.assemble_general_mcm(te, even, odd, tt, lmax, s1, s2, is_teb)
+    assert _rel(w.get_coupling_matrix().cpu().numpy(), want) < 1e-10
