@@ -42,15 +42,34 @@ os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "expandable_segments:True")
 
 # Kernel behind each timed Legendre pass (the checkpointed kernels of legendre_ck.cu when
 # the geometry's checkpoint tables are in use, else the carried-state ones of
-# legendre_tc.cu), and the DRAM traffic of one launch of it at the Nside 2048,
-# 32-simulation workload (dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of
-# the kernel on the Nside 512 case, scaled to Nside 2048 by the launch's units of work;
-# None where not captured).
+# legendre_tc.cu).
 KERNEL_OF = {"tc_analysis_s2": "k_ana_ck<2>", "tc_analysis_s0": "k_ana_ck<0>",
              "tc_synthesis_s2": "k_syn_ck<2>", "tc_synthesis_s0": "k_syn_ck<0>"}
 KERNEL_OF_CARRIED = {"tc_analysis_s2": "k_ana_tc<2>", "tc_analysis_s0": "k_ana_tc<0>",
                      "tc_synthesis_s2": "k_syn_tc<2>", "tc_synthesis_s0": "k_syn_tc<0>"}
-TRAFFIC_PER_LAUNCH = {}
+
+# DRAM traffic of one checkpointed analysis launch: ncu measured 1.539 GB (dram__bytes_read.sum
+# + dram__bytes_write.sum) for the spin-2 launch of 8 fields at Nside 512, 1.025 x the byte
+# model below (operand images read once, alm accumulator read and written once, checkpoint
+# states read once); the launch at the benchmark size is given as that model x 1.025.
+CK_TRAFFIC_RATIO = 1.539 / 1.501
+
+
+def ck_analysis_bytes(nside, lmax, nrows):
+    """Byte model of one checkpointed analysis launch (one row variant): 64 KB operand image
+    per (order, 128-lane group), nrows FP64 alm rows read and written, 9 B checkpoint state
+    per (128-row segment, lane)."""
+    L, nlanes = lmax + 1, 2 * nside
+    groups = (nlanes + 127) // 128
+    nelem = L * (L + 1) // 2
+    segs = sum((L - max(m, 2) + 127) // 128 for m in range(L))
+    return L * groups * 65536 + 2 * nelem * nrows * 8 + segs * nlanes * 9
+
+
+def traffic_per_launch(kernel, nside, lmax, sims):
+    if kernel == "k_ana_ck<2>":
+        return CK_TRAFFIC_RATIO * ck_analysis_bytes(nside, lmax, 4 * sims)
+    return None
 
 
 def parse():
@@ -1319,11 +1338,13 @@ def main():
         "roofline": {
             "bound": "tensor", "kernel": kernel_of.get(dominant, dominant),
             "achieved": dom_tflops, "peak": peak, "unit": "TFLOP/s",
-            "frac": dom_tflops / peak, "traffic": TRAFFIC_PER_LAUNCH.get(dominant),
+            "frac": dom_tflops / peak,
+            "traffic": traffic_per_launch(kernel_of.get(dominant, dominant), nside, lmax, S),
             "note": "algorithmic flops per launch (one complex MAC = 4 flops per (l, m, lane) and "
                     "map; the f16x3 split issues 3x these on the tensor pipe) / CUDA-event time "
                     "of the launch; peak = measured sustained bf16 dense (MEASURED_PEAKS.json); traffic = "
-                    "DRAM bytes read + written per launch, ncu at this workload",
+                    "DRAM bytes read + written per launch: ncu measured 1.025x the launch's byte "
+                    "model at Nside 512 (8 fields); the model scaled to this workload x 1.025",
             "launches": dom_launches, "avg_ms": dom_avg_ms,
             "tensor_pipe_tflops_issued": 3 * dom_tflops,
         },
