@@ -89,7 +89,8 @@ def fields_from_maps(mask, maps, *, spin=None, n_iter=None, beam=None, lmax=None
             del spec
         del flat, chunk
         alms.append(a.reshape(-1, nmaps, a.shape[1]))
-    alms = torch.cat(alms)
+    # one launch's alms are used as they are (a concatenation would hold a second copy)
+    alms = alms[0] if len(alms) == 1 else torch.cat(alms)
     fields = []
     for i in range(nsims):
         f = NmtField(mask_t, None, spin=spin, n_iter=n_iter, beam=beam, lmax=lmax, lite=True,

@@ -710,8 +710,11 @@ static int dispatch_syn(int spin, int64_t nside, int64_t lmax, int64_t ncomp, co
 // Tile shapes the autotuner chooses from: (NC, R) = (components per CTA, lanes per thread).
 // Spin 0 takes NC in {1, 2, 4, 8} (the reduce-scatter needs 2 NC to divide 32); spin 2
 // handles one (Q, U) pair per CTA (NC = 2).  Index -1 selects the built-in heuristic.
-static const int kTiles0[][2] = {{1, 1}, {1, 2}, {1, 4}, {2, 1}, {2, 2}, {2, 4}, {4, 1}, {4, 2}, {8, 1}};
-static const int kTiles2[][2] = {{2, 1}, {2, 2}, {2, 4}};
+// The last tile of each list (8 lanes per thread: a reduce-scatter tree per 8 rows shared by
+// 64 elements of a thread instead of 32) is compiled for single precision only; the FP64
+// kernels run it as the tile with 4 lanes per thread.
+static const int kTiles0[][2] = {{1, 1}, {1, 2}, {1, 4}, {2, 1}, {2, 2}, {2, 4}, {4, 1}, {4, 2}, {8, 1}, {2, 8}};
+static const int kTiles2[][2] = {{2, 1}, {2, 2}, {2, 4}, {2, 8}};
 constexpr int kNTiles0 = sizeof(kTiles0) / sizeof(kTiles0[0]);
 constexpr int kNTiles2 = sizeof(kTiles2) / sizeof(kTiles2[0]);
 
@@ -732,6 +735,8 @@ static int tile_ana(int spin, int tile, int64_t nside, int64_t lmax, int64_t nco
         case 6: GM_ANA(0, 4, 1);
         case 7: GM_ANA(0, 4, 2);
         case 8: GM_ANA(0, 8, 1);
+        case 9:
+            if constexpr (sizeof(T) == 8) { GM_ANA(0, 2, 4); } else { GM_ANA(0, 2, 8); }
         default: return GM_ERR_BAD_SHAPE;
         }
     }
@@ -739,6 +744,8 @@ static int tile_ana(int spin, int tile, int64_t nside, int64_t lmax, int64_t nco
     case 0: GM_ANA(2, 2, 1);
     case 1: GM_ANA(2, 2, 2);
     case 2: GM_ANA(2, 2, 4);
+    case 3:
+        if constexpr (sizeof(T) == 8) { GM_ANA(2, 2, 4); } else { GM_ANA(2, 2, 8); }
     default: return GM_ERR_BAD_SHAPE;
     }
 #undef GM_ANA
@@ -761,6 +768,8 @@ static int tile_syn(int spin, int tile, int64_t nside, int64_t lmax, int64_t nco
         case 6: GM_SYN(0, 4, 1);
         case 7: GM_SYN(0, 4, 2);
         case 8: GM_SYN(0, 8, 1);
+        case 9:
+            if constexpr (sizeof(T) == 8) { GM_SYN(0, 2, 4); } else { GM_SYN(0, 2, 8); }
         default: return GM_ERR_BAD_SHAPE;
         }
     }
@@ -768,6 +777,8 @@ static int tile_syn(int spin, int tile, int64_t nside, int64_t lmax, int64_t nco
     case 0: GM_SYN(2, 2, 1);
     case 1: GM_SYN(2, 2, 2);
     case 2: GM_SYN(2, 2, 4);
+    case 3:
+        if constexpr (sizeof(T) == 8) { GM_SYN(2, 2, 4); } else { GM_SYN(2, 2, 8); }
     default: return GM_ERR_BAD_SHAPE;
     }
 #undef GM_SYN

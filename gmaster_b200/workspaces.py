@@ -57,15 +57,28 @@ def coupling_blocks_multi(windows, lmaxs, whiches):
     if len(windows) == 0:
         return []
     dev = windows[0].device
-    order = sorted(range(len(windows)), key=lambda i: -int(lmaxs[i]))
-    rows, wparts, woff, boff, first = [], [], 0, 0, 0
-    offsets = [None] * len(windows)
-    for i in order:
-        w = as_device(windows[i], torch.float64).contiguous()
+    wins = [as_device(w, torch.float64).contiguous() for w in windows]
+    # workspaces with equal windows and lmax (the 0x0, 0x2 and 2x2 workspaces of one mask)
+    # share one job computing the union of their blocks: each (l1, l2) recursion then runs
+    # once, and every block equals the one of a separate job bit for bit
+    groups = []   # [lmax, window, which, members]
+    for i, w in enumerate(wins):
         lmax = int(lmaxs[i])
+        for g in groups:
+            if g[0] == lmax and g[1].shape == w.shape and torch.equal(g[1], w):
+                g[2] |= int(whiches[i])
+                g[3].append(i)
+                break
+        else:
+            groups.append([lmax, w, int(whiches[i]), [i]])
+    order = sorted(range(len(groups)), key=lambda k: -groups[k][0])
+    rows, wparts, woff, boff, first = [], [], 0, 0, 0
+    offsets = [None] * len(groups)
+    for k in order:
+        lmax, w, which, _ = groups[k]
         n = lmax + 1
-        rows.append([lmax, woff, w.shape[0], int(whiches[i]), boff, first])
-        offsets[i] = boff
+        rows.append([lmax, woff, w.shape[0], which, boff, first])
+        offsets[k] = boff
         wparts.append(w)
         woff += w.shape[0]
         boff += 4 * n * n
@@ -76,10 +89,22 @@ def coupling_blocks_multi(windows, lmaxs, whiches):
     queue = torch.zeros(1, dtype=torch.int64, device=dev)
     _lib.call("gm_coupling_blocks_multi", len(rows), _lib.ptr(jobs), first, _lib.ptr(allw),
               _lib.ptr(blocks), _lib.ptr(queue), _lib.stream_handle(dev))
-    out = []
-    for i in range(len(windows)):
-        n = int(lmaxs[i]) + 1
-        out.append(blocks[offsets[i]:offsets[i] + 4 * n * n].view(4, n, n))
+    out = [None] * len(windows)
+    for k, (lmax, _, _, members) in enumerate(groups):
+        n = lmax + 1
+        shared = blocks[offsets[k]:offsets[k] + 4 * n * n].view(4, n, n)
+        # every workspace gets its own blocks (a Toeplitz fill edits them in place), with
+        # the blocks it did not ask for zero
+        for i in members[1:]:
+            own = torch.zeros_like(shared)
+            for x in range(4):
+                if int(whiches[i]) & (1 << x):
+                    own[x] = shared[x]
+            out[i] = own
+        for x in range(4):
+            if not int(whiches[members[0]]) & (1 << x):
+                shared[x].zero_()
+        out[members[0]] = shared
     return out
 
 
