@@ -52,17 +52,20 @@ using ltc::wait_or_abort;
 constexpr int kSeg = 128;                           // rows per checkpoint segment
 constexpr int kMaxShift = 5;                        // largest stored shift n (2^-320)
 // analysis
-constexpr int kSB = 2 * kSeg;                       // superblock rows (one unit)
-constexpr int kHalf = 64;                           // rows per half-tile
-constexpr int kKC = 128;                            // lanes per group (MMA K per group)
-constexpr int kGenA = 256;                          // generator threads (8 warps, 2 sets)
-constexpr int kThrA = kGenA + 32;                   // + the producer / MMA warp
+constexpr int kSB = 2 * kSeg;                       // superblock rows (one unit; MMA N)
+constexpr int kHalf = 64;                           // rows per generation step
+constexpr int kKC = 128;                            // lanes per operand image (global layout)
+constexpr int kKG = 64;                             // lanes per analysis group (MMA K per group)
+constexpr int kGenA = 256;                          // generator threads (8 warps, 2 sets of 4)
 constexpr int kMmaWarpA = kGenA / 32;
+constexpr int kLoadWarpA = kMmaWarpA + 1;
+constexpr int kThrA = kGenA + 64;                   // + the MMA warp and the image loader warp
 constexpr uint32_t kAImg = 128u * kKC * 2u;         // one plane of a right-hand-side image (32 KB)
-constexpr uint32_t kHalfBytes = 2u * kHalf * kKC * 2u;   // half-tile: 64 hi + 64 lo rows (32 KB)
+constexpr uint32_t kAImgG = 2u * 128u * kKG * 2u;   // a group's hi and lo image planes (32 KB)
+constexpr uint32_t kTileA = 2u * kSB * kKG * 2u;    // tile: 256 rows x 64 lanes, hi + lo (64 KB)
 constexpr int kStageLd = kSB + 1;                   // epilogue staging row stride (floats)
-// the epilogue stages 128 rows x kStageLd floats in the half-tiles and coefficient rows
-static_assert(128 * kStageLd * 4 <= 4 * kHalfBytes + kSB * 16, "epilogue staging does not fit");
+// the epilogue stages 128 rows x kStageLd floats in the tiles and coefficient rows
+static_assert(128 * kStageLd * 4 <= 2 * kTileA + kSB * 16, "epilogue staging does not fit");
 // synthesis
 constexpr int kLT = 256;                            // lanes per CTA (MMA N)
 constexpr int kKL = 64;                             // rows per chunk (MMA K)
@@ -230,7 +233,7 @@ __global__ void __launch_bounds__(128) k_ck_build(int64_t nside, int64_t lmax, i
 // ------------------------------------------------------------------------------- analysis
 
 struct __align__(8) AnaShared {
-    uint64_t a_full, a_free, b_full[4], b_free[4], d_full, d_free, drain;
+    uint64_t a_full[2], a_free[2], b_full[2], b_free[2], d_full, d_free, drain;
     uint32_t tmem;
     int abort;
 };
@@ -250,9 +253,14 @@ __device__ __forceinline__ int64_t unit_order(const int64_t *__restrict__ uoff, 
 __device__ __forceinline__ void gen_barrier_a() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 
 // Units (m, s): superblock s of order m covers rows l0 + 256 s + [0, 256).  CTA c takes
-// units c, c + G, ...; within a unit the lane groups g = 0..NG-1 stream their images
-// (one image buffer; set 0 generates rows [0, 128), set 1 rows [128, 256) into two
-// half-tiles each, each half-tile consumed by two MMAs per K step as in legendre_tc.cu).
+// units c, c + G, ...  Within a unit the lanes run in groups g of 64 (half of a 128-lane
+// operand image); a group's image (hi and lo planes, 32 KB) goes into one of two buffers
+// that a loader warp refills while the other group's MMAs run.  Set S (four warps) fills
+// the tile of the groups with g % 2 == S: all 256 rows of the superblock for the group's
+// 64 lanes, each thread one segment (128 rows) of one lane, f16 hi and lo planes.  Per K
+// step the tile is consumed by three MMAs of N = 256 (hi image x hi rows into the hi*hi
+// accumulator; hi image x lo rows and lo image x hi rows into the cross accumulator), so
+// the image is read from shared memory once per 256 rows and product.
 template <int SPIN>
 __global__ void __launch_bounds__(kThrA, 1) k_ana_ck(CkParams p, const uint8_t *__restrict__ aimg,
                                                      double *__restrict__ alm_i, int *__restrict__ err)
@@ -262,19 +270,19 @@ __global__ void __launch_bounds__(kThrA, 1) k_ana_ck(CkParams p, const uint8_t *
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t base = (tc::smem_u32(smem_raw) + 1023u) & ~1023u;
     uint8_t *smem = smem_raw + (base - tc::smem_u32(smem_raw));
-    uint8_t *sA = smem;                                              // image: hi, lo planes
-    uint8_t *sB = smem + 2 * kAImg;                                  // 4 half-tiles
-    float4 *sCf = reinterpret_cast<float4 *>(sB + 4 * kHalfBytes);  // kSB coefficient rows
-    const int64_t L = p.lmax + 1, NG = (p.nlanes + kKC - 1) / kKC;
+    uint8_t *sA = smem;                                              // 2 image buffers
+    uint8_t *sB = smem + 2 * kAImgG;                                 // 2 tiles
+    float4 *sCf = reinterpret_cast<float4 *>(sB + 2 * kTileA);      // kSB coefficient rows
+    const int64_t L = p.lmax + 1, NG = (p.nlanes + kKC - 1) / kKC, NGK = (p.nlanes + kKG - 1) / kKG;
     const int64_t U = p.uoff[L];
     const int64_t G = gridDim.x, c = blockIdx.x;
 
     if (tid == 0) {
-        tc::mbar_init(&sh.a_full, 1);
-        tc::mbar_init(&sh.a_free, 1);
-        for (int h = 0; h < 4; ++h) {
-            tc::mbar_init(&sh.b_full[h], 4);
-            tc::mbar_init(&sh.b_free[h], 1);
+        for (int i = 0; i < 2; ++i) {
+            tc::mbar_init(&sh.a_full[i], 1);
+            tc::mbar_init(&sh.a_free[i], 1);
+            tc::mbar_init(&sh.b_full[i], 4);
+            tc::mbar_init(&sh.b_free[i], 1);
         }
         tc::mbar_init(&sh.d_full, 1);
         tc::mbar_init(&sh.d_free, kGenA / 32);
@@ -293,77 +301,85 @@ __global__ void __launch_bounds__(kThrA, 1) k_ana_ck(CkParams p, const uint8_t *
     volatile int *abort = &sh.abort;
 
     if (warp == kMmaWarpA) {
-        // ------------------------------------------------ producer + MMA issuer
+        // ------------------------------------------------ MMA issuer
         if (lane == 0) {
-            // concatenated MMA: hi image x [hi | lo] rows of a half-tile (N = 128) writes the
-            // hi*hi and hi*lo halves of the half-tile's 128 accumulator columns; the second
-            // adds lo image x hi rows (N = 64) into the cross half.  One image buffer: it is
-            // refilled when a group's MMAs are done, from L2, where the image was prefetched a
-            // group earlier (the CTAs running the superblocks of one order read the same
-            // images, so most of them find it there anyway).
-            const uint32_t idesc_cat = tc::idesc_f16(128, 2 * kHalf, 0, 1, 1);
-            const uint32_t idesc_hi = tc::idesc_f16(128, kHalf, 0, 1, 1);
-            uint32_t ja = 0, q = 0;
-            bool inflight = false, ok = true;
-            auto image = [&](int64_t m, int64_t g) { return aimg + ((m * NG + g) * 2) * (int64_t)kAImg; };
-            auto load_image = [&](int64_t m, int64_t g) {
-                tc::mbar_arrive_expect_tx(&sh.a_full, 2 * kAImg);
-                tc::bulk_g2s(sA, image(m, g), 2 * kAImg, &sh.a_full);
-                inflight = true;
-            };
-            if (c < U) load_image(unit_order(p.uoff, L, c), 0);
+            const uint32_t idesc = tc::idesc_f16(128, kSB, 0, 1, 1);
+            uint32_t cnt0 = 0, cnt1 = 0;   // groups consumed from each tile
+            uint32_t q = 0;
+            int64_t jg = 0;
+            bool ok = true;
             for (int64_t u = c; u < U && ok; u += G, ++q) {
-                const int64_t m = unit_order(p.uoff, L, u);
-                const int64_t mnext = u + G < U ? unit_order(p.uoff, L, u + G) : -1;
-                for (int64_t g = 0; g < NG && ok; ++g, ++ja) {
-                    // the group after this one: (m, g + 1) or group 0 of the next unit
-                    const bool more = g + 1 < NG || mnext >= 0;
-                    const int64_t mn = g + 1 < NG ? m : mnext, gn = g + 1 < NG ? g + 1 : 0;
-                    if (more) tc::prefetch_l2(image(mn, gn), 2 * kAImg);
-                    if (!(ok = wait_or_abort(&sh.a_full, ja & 1, abort, err))) break;
-                    inflight = false;
+                for (int64_t g = 0; g < NGK && ok; ++g, ++jg) {
+                    const uint32_t b = (uint32_t)(jg & 1);
+                    const int S = (int)(g & 1);
+                    const uint32_t ph = S ? cnt1 : cnt0;
+                    if (!(ok = wait_or_abort(&sh.a_full[b], (uint32_t)(jg >> 1) & 1, abort, err))) break;
                     if (g == 0 && !(ok = wait_or_abort(&sh.d_free, (q & 1) ^ 1, abort, err))) break;
+                    if (!(ok = wait_or_abort(&sh.b_full[S], ph & 1, abort, err))) break;
                     tc::tc_fence_after();
-                    const uint32_t a0 = tc::smem_u32(sA);
-                    for (int h = 0; h < 4; ++h) {
-                        if (!(ok = wait_or_abort(&sh.b_full[h], ja & 1, abort, err))) break;
-                        tc::tc_fence_after();
-                        const uint32_t b0 = tc::smem_u32(sB + h * kHalfBytes);
-                        const uint32_t dh = tmem + 128u * h, dx = dh + kHalf;
+                    const uint32_t a0 = tc::smem_u32(sA + b * kAImgG);
+                    const uint32_t b0 = tc::smem_u32(sB + S * kTileA);
 #pragma unroll
-                        for (int ks = 0; ks < kKC / 16; ++ks) {
-                            const uint64_t ah = tc::desc_sw128_mn(a0 + ks * 4096, 1024, 2048);
-                            const uint64_t al = tc::desc_sw128_mn(a0 + kAImg + ks * 4096, 1024, 2048);
-                            const uint64_t bt = tc::desc_sw128_mn(b0 + ks * 4096, 1024, 2048);
-                            tc::mma_f16(dh, ah, bt, idesc_cat, (g > 0 || ks > 0) ? 1u : 0u);
-                            tc::mma_f16(dx, al, bt, idesc_hi, 1u);
-                        }
-                        tc::mma_commit(&sh.b_free[h]);
+                    for (int ks = 0; ks < kKG / 16; ++ks) {
+                        const uint64_t ah = tc::desc_sw128_mn(a0 + ks * 4096, 1024, 2048);
+                        const uint64_t al = tc::desc_sw128_mn(a0 + kAImgG / 2 + ks * 4096, 1024, 2048);
+                        const uint64_t bh = tc::desc_sw128_mn(b0 + ks * 8192, 1024, 4096);
+                        const uint64_t bl = tc::desc_sw128_mn(b0 + kTileA / 2 + ks * 8192, 1024, 4096);
+                        const uint32_t acc = (g > 0 || ks > 0) ? 1u : 0u;
+                        tc::mma_f16(tmem, ah, bh, idesc, acc);
+                        tc::mma_f16(tmem + kSB, ah, bl, idesc, acc);
+                        tc::mma_f16(tmem + kSB, al, bh, idesc, 1u);
                     }
-                    if (!ok) break;
-                    tc::mma_commit(&sh.a_free);
-                    if (g == NG - 1) tc::mma_commit(&sh.d_full);
-                    if (more) {
-                        // refill the image buffer once this group's MMAs have read it (the
-                        // generators run ahead into the freed half-tiles meanwhile)
-                        if (!(ok = wait_or_abort(&sh.a_free, ja & 1, abort, err))) break;
-                        load_image(mn, gn);
-                    }
+                    tc::mma_commit(&sh.b_free[S]);
+                    tc::mma_commit(&sh.a_free[b]);
+                    if (g == NGK - 1) tc::mma_commit(&sh.d_full);
+                    if (S) ++cnt1;
+                    else ++cnt0;
                 }
             }
-            // every issued MMA completes before TMEM is released, and an image copy still in
-            // flight lands before the CTA exits (both waits bounded)
+            // every issued MMA completes before TMEM is released (bounded wait)
             tc::mma_commit(&sh.drain);
             tc::mbar_wait(&sh.drain, 0);
-            if (inflight) tc::mbar_wait(&sh.a_full, ja & 1);
+        }
+    } else if (warp == kLoadWarpA) {
+        // ------------------------------------------------ image loader
+        // group g of order m: lanes 64 g + [0, 64) are the first or second half (g % 2) of
+        // the 128-lane image g / 2, i.e. 16 KB of its hi plane and 16 KB of its lo plane
+        if (lane == 0) {
+            int64_t jg = 0;
+            bool issued[2] = {false, false};
+            uint32_t last_ph[2] = {0u, 0u};
+            bool ok = true;
+            for (int64_t u = c; u < U && ok; u += G) {
+                const int64_t m = unit_order(p.uoff, L, u);
+                for (int64_t g = 0; g < NGK; ++g, ++jg) {
+                    const uint32_t b = (uint32_t)(jg & 1);
+                    const uint8_t *src = aimg + ((m * NG + (g >> 1)) * 2) * (int64_t)kAImg + (g & 1) * (kAImgG / 2);
+                    tc::prefetch_l2(src, kAImgG / 2);
+                    tc::prefetch_l2(src + kAImg, kAImgG / 2);
+                    if (!(ok = wait_or_abort(&sh.a_free[b], ((uint32_t)(jg >> 1) & 1) ^ 1, abort, err))) break;
+                    tc::mbar_arrive_expect_tx(&sh.a_full[b], kAImgG);
+                    tc::bulk_g2s(sA + b * kAImgG, src, kAImgG / 2, &sh.a_full[b]);
+                    tc::bulk_g2s(sA + b * kAImgG + kAImgG / 2, src + kAImg, kAImgG / 2, &sh.a_full[b]);
+                    issued[b] = true;
+                    last_ph[b] = (uint32_t)(jg >> 1) & 1;
+                }
+            }
+            // copies still in flight land before the CTA exits (bounded waits)
+            for (int b = 0; b < 2; ++b)
+                if (issued[b]) tc::mbar_wait(&sh.a_full[b], last_ph[b]);
         }
     } else {
         // ------------------------------------------------ generators + epilogue
-        const int S = warp >> 2;          // set: rows [128 S, 128 S + 128) of the superblock
-        const int t = tid & (kKC - 1);    // lane within the group (the MMA K index)
+        const int S = warp >> 2;                  // tile of the groups g % 2 == S
+        const int sseg = (warp >> 1) & 1;         // segment of the superblock
+        const int t = tid & (kKG - 1);            // lane within the group (the MMA K index)
         const double sgn_c = sgn_of(p.sp);
-        const uint32_t rowbase0 = tc::smem_u32(sB) + (t >> 3) * 2048 + (t & 7) * 128;
-        uint32_t jb = 0;
+        // tile: MN-major SW128 planes (hi, then lo) of 256 MN rows (the superblock) and 64 K
+        // lanes; per 8 lanes 4 blocks of 64 rows; this thread writes blocks 2 sseg, 2 sseg + 1
+        const uint32_t rowbase = tc::smem_u32(sB) + (uint32_t)S * kTileA + (t >> 3) * 4096 +
+                                 (uint32_t)(2 * sseg) * 1024 + (t & 7) * 128;
+        uint32_t js = 0;   // groups generated into this set's tile
         bool dead = false;
         // this thread's coefficient row of a unit, loaded one unit ahead
         auto unit_coef = [&](int64_t uu) {
@@ -383,18 +399,17 @@ __global__ void __launch_bounds__(kThrA, 1) k_ana_ck(CkParams p, const uint8_t *
             if (!dead) sCf[tid] = ncoef;
             gen_barrier_a();
             if (!dead && u + G < U) ncoef = unit_coef(u + G);
-            // the set's segment; the second half of an order's last superblock may lie past
-            // the order's last segment (all its rows are >= L): it then starts from zero
-            const int64_t seg = p.segoff[m] + 2 * s + S;
+            // this thread's segment; the second half of an order's last superblock may lie
+            // past the order's last segment (all its rows are >= L): it then starts from zero
+            const int64_t seg = p.segoff[m] + 2 * s + sseg;
             const bool has_seg = seg < p.segoff[m + 1];
             const int64_t segrow = seg * p.nlanes;
-            // lane state of group g + 1 is loaded while group g is generated (converted only
-            // when used, so the loads do not stall the generation)
+            // lane state of the set's next group is loaded while this one is generated
             float2 nst = make_float2(0.f, 0.f);
             int nn = 0;
             double nx = 1.0;
             auto fetch = [&](int64_t g) {
-                const int64_t j = g * kKC + t;
+                const int64_t j = g * kKG + t;
                 nst = make_float2(0.f, 0.f);
                 nn = 0;
                 nx = 1.0;
@@ -404,52 +419,46 @@ __global__ void __launch_bounds__(kThrA, 1) k_ana_ck(CkParams p, const uint8_t *
                     nx = __ldg(p.geom + j);
                 }
             };
-            if (!dead) fetch(0);
-            for (int64_t g = 0; g < NG; ++g, ++jb) {
+            if (!dead) fetch(S);
+            for (int64_t g = S; g < NGK; g += 2, ++js) {
                 if (dead) continue;
                 float v = nst.x, D = nst.y;
                 const float y = (float)(nx - 1.0);
                 int n = nn;
-                if (g + 1 < NG) fetch(g + 1);
-                for (int hh = 0; hh < 2; ++hh) {
-                    const int h = 2 * S + hh;
-                    if (!warp_wait(&sh.b_free[h], (jb & 1) ^ 1, abort, err)) {
-                        dead = true;
-                        break;
-                    }
-                    // half-tile: MN-major SW128 with 128 MN rows (64 hi rows, then 64 lo rows) and
-                    // 128 K lanes; a thread stores 8 consecutive rows of its lane as 16 bytes
-                    gen_rows64(sCf + kSeg * S + kHalf * hh, y, v, D, n, rowbase0 + h * kHalfBytes, 1024,
-                               (uint32_t)(t & 7));
-                    tc::fence_async_smem();
-                    __syncwarp();
-                    if (lane == 0) tc::mbar_arrive(&sh.b_full[h]);
+                if (g + 2 < NGK) fetch(g + 2);
+                if (!warp_wait(&sh.b_free[S], (js & 1) ^ 1, abort, err)) {
+                    dead = true;
+                    continue;
                 }
+                // 128 rows of the lane: MN blocks 2 sseg (rows 0-63) and 2 sseg + 1; a thread
+                // stores 8 consecutive rows as 16 bytes, the lo plane kTileA / 2 bytes further
+                gen_rows64(sCf + kSeg * sseg, y, v, D, n, rowbase, kTileA / 2, (uint32_t)(t & 7));
+                gen_rows64(sCf + kSeg * sseg + kHalf, y, v, D, n, rowbase + 1024, kTileA / 2, (uint32_t)(t & 7));
+                tc::fence_async_smem();
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(&sh.b_full[S]);
             }
             // epilogue of the unit.  The two hemisphere halves of the image rows may add into
             // the same alm row (spin 0), so the accumulators are staged in shared memory (the
-            // half-tiles and coefficient rows, free now) and each alm element then receives
+            // tiles and coefficient rows, free now) and each alm element then receives
             // exactly one addition per launch, from one thread: the result does not depend
-            // on the order of the units.
+            // on the order of the units.  Warp w reads TMEM lanes 32 (w % 4), superblock
+            // rows 128 (w / 4) + [0, 128).
             const uint32_t q = (uint32_t)((u - c) / G);
             if (!dead && !warp_wait(&sh.d_full, q & 1, abort, err)) dead = true;
             float *stage = reinterpret_cast<float *>(sB);   // [128 rows][kStageLd] floats
             if (!dead) {
                 tc::tc_fence_after();
-                const int row = 32 * (warp & 3) + lane;
-                for (int hh = 0; hh < 2; ++hh) {
-                    const int h = 2 * S + hh;
-                    for (int cb = 0; cb < kHalf; cb += 16) {
-                        uint32_t r[16], rx[16];
-                        const uint32_t ta = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + 128u * h + cb;
-                        tc::tmem_ld16(ta, r);
-                        tc::tmem_ld16(ta + kHalf, rx);
-                        tc::tmem_ld_wait();
+                const int row = 32 * (warp & 3) + lane, c0 = 128 * (warp >> 2);
+                for (int cb = c0; cb < c0 + 128; cb += 16) {
+                    uint32_t r[16], rx[16];
+                    const uint32_t ta = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)cb;
+                    tc::tmem_ld16(ta, r);
+                    tc::tmem_ld16(ta + kSB, rx);
+                    tc::tmem_ld_wait();
 #pragma unroll
-                        for (int e = 0; e < 16; ++e)
-                            stage[row * kStageLd + kHalf * h + cb + e] =
-                                __uint_as_float(r[e]) + __uint_as_float(rx[e]);
-                    }
+                    for (int e = 0; e < 16; ++e)
+                        stage[row * kStageLd + cb + e] = __uint_as_float(r[e]) + __uint_as_float(rx[e]);
                 }
                 tc::tc_fence_before();
             }
@@ -767,7 +776,7 @@ extern "C" int gm_ck_analysis(int64_t nside, int64_t lmax, int spin, int sp, int
         return GM_ERR_BAD_SHAPE;
     if (!geom || !coef || !segoff || !uoff || !ck_state || !ck_shift || !img || !alm_i || !err)
         return GM_ERR_BAD_PTR;
-    const size_t smem = 2 * kAImg + 4 * kHalfBytes + kSB * sizeof(float4) + 1024;
+    const size_t smem = 2 * kAImgG + 2 * kTileA + kSB * sizeof(float4) + 1024;
     auto kern = spin == 0 ? k_ana_ck<0> : k_ana_ck<2>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) {
