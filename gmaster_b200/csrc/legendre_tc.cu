@@ -804,6 +804,33 @@ __global__ void __launch_bounds__(128) k_fold_tc(int64_t nside, int64_t L, int n
     const float neg = sh ? -1.0f : 1.0f;   // sign of an order read as a negative alias, relative
                                            // to its sign as a positive alias
 
+    if (n >= L) {
+        // rings at least as long as lmax + 1 (the belt): order k is its residue's only
+        // positive alias and n - k (when below L) its only negative one, so the residue
+        // pairs are independent and the loop keeps several loads in flight.  The same
+        // sums as the general loop below, in the same order of operations.
+        emit(0, pa[0], pb[0]);
+#pragma unroll 4
+        for (int k = 1; k <= n / 2 && k < L; ++k) {
+            const int k2 = n - k;
+            const float ak = pa[(int64_t)k * stride], bk = SPIN ? pb[(int64_t)k * stride] : ak;
+            if (k2 == k) {
+                put(ia, k, wn * (ak + neg * cs * bk) - rhs(k, 0));
+                if (SPIN) put(ib, k, wn * (bk + neg * cs * ak) - rhs(k, 1));
+            } else if (k2 < L) {
+                const float a2 = pa[(int64_t)k2 * stride], b2 = SPIN ? pb[(int64_t)k2 * stride] : a2;
+                put(ia, k, wn * (ak + neg * cs * b2) - rhs(k, 0));
+                if (SPIN) put(ib, k, wn * (bk + neg * cs * a2) - rhs(k, 1));
+                put(ia, k2, wn * (neg * cs * bk + a2) - rhs(k2, 0));
+                if (SPIN) put(ib, k2, wn * (neg * cs * ak + b2) - rhs(k2, 1));
+            } else {
+                put(ia, k, wn * ak - rhs(k, 0));
+                if (SPIN) put(ib, k, wn * bk - rhs(k, 1));
+            }
+        }
+        return;
+    }
+
     // residue 0: orders t n (t >= 0), and t n (t >= 1) as negative aliases
     {
         float s0a = 0.f, s0b = 0.f;

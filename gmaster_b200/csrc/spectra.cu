@@ -20,29 +20,41 @@ __device__ __forceinline__ int64_t alm_idx(int64_t lmax, int64_t l, int64_t m)
 
 // ---------------------------------------------------------------- pseudo-C_ell
 
-constexpr int kPclMChunk = 64;
+constexpr int kPclLanes = 32;   // degrees per CTA (one per lane: coalesced over l)
+constexpr int kPclWarps = 8;    // orders interleaved over the warps of a CTA
 
-// grid (l-blocks, m-chunks, pairs); thread l sums its orders of the chunk and adds.
-__global__ void k_pseudo_cl(int64_t lmax, int64_t n1, const double2 *__restrict__ a,
-                            int64_t n2, const double2 *__restrict__ b, double *__restrict__ cls)
+// grid (l-blocks of 32, pairs), 256 threads: lane = degree l, warp w sums the orders
+// m = w, w + 8, ... <= l; the eight partial sums are then added in a fixed order, so the
+// result does not depend on scheduling (equal inputs give bit-equal spectra).
+__global__ void __launch_bounds__(kPclLanes * kPclWarps) k_pseudo_cl(int64_t lmax, int64_t n1,
+                                                                     const double2 *__restrict__ a, int64_t n2,
+                                                                     const double2 *__restrict__ b,
+                                                                     double *__restrict__ cls)
 {
+    __shared__ double part[kPclWarps][kPclLanes];
     const int64_t L = lmax + 1, nelem = L * (L + 1) / 2;
-    const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t m0 = (int64_t)blockIdx.y * kPclMChunk;
-    const int64_t pair = blockIdx.z, i = pair / n2, j = pair % n2;
-    if (l >= L || m0 > l) return;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t l = (int64_t)blockIdx.x * kPclLanes + lane;
+    const int64_t pair = blockIdx.y, i = pair / n2, j = pair % n2;
     const double2 *ai = a + i * nelem;
     const double2 *bj = b + j * nelem;
     double s = 0.0;
-    int64_t mend = m0 + kPclMChunk - 1;
-    if (mend > l) mend = l;
-    for (int64_t m = m0; m <= mend; ++m) {
-        const int64_t k = alm_idx(lmax, l, m);
-        const double2 x = ai[k], y = bj[k];
-        const double re = x.x * y.x + x.y * y.y;
-        s += m == 0 ? re : 2.0 * re;
+    if (l < L) {
+        for (int64_t m = w; m <= l; m += kPclWarps) {
+            const int64_t k = alm_idx(lmax, l, m);
+            const double2 x = ai[k], y = bj[k];
+            const double re = x.x * y.x + x.y * y.y;
+            s += m == 0 ? re : 2.0 * re;
+        }
     }
-    atomicAdd(cls + pair * L + l, s / (2.0 * (double)l + 1.0));
+    part[w][lane] = s;
+    __syncthreads();
+    if (w == 0 && l < L) {
+        double t = 0.0;
+#pragma unroll
+        for (int q = 0; q < kPclWarps; ++q) t += part[q][lane];
+        cls[pair * L + l] = t / (2.0 * (double)l + 1.0);
+    }
 }
 
 // ---------------------------------------------------------------- Wigner-3j coupling
@@ -629,6 +641,115 @@ __global__ void k_lu_solve(int64_t n, const double *__restrict__ lu, const int32
     }
 }
 
+// Blocked solve for many right-hand sides: one CTA per kLuCB columns of b, held in shared
+// memory.  Rows go in blocks of 32: the contributions of the rows solved so far are summed
+// by all 256 threads (thread = (row, one eighth of the columns j), partials added in a fixed
+// order), then the 32 x 32 diagonal block is solved by one warp per column with shuffles.
+// The same arithmetic as k_lu_solve up to the order of the sums.
+constexpr int kLuCB = 4;      // right-hand sides per CTA
+constexpr int kLuRB = 32;     // rows per block
+
+__device__ __forceinline__ void lu_block_sums(int64_t n, const double *__restrict__ lu, const double *x,
+                                              int64_t r0, int rows, int64_t jbeg, int64_t jend,
+                                              double (*part)[kLuCB])
+{
+    const int tid = threadIdx.x, r = tid >> 3, pt = tid & 7;
+    double acc[kLuCB];
+#pragma unroll
+    for (int c = 0; c < kLuCB; ++c) acc[c] = 0.0;
+    if (r < rows) {
+        const double *row = lu + (r0 + r) * n;
+        for (int64_t j = jbeg + pt; j < jend; j += 8) {
+            const double l = __ldg(row + j);
+#pragma unroll
+            for (int c = 0; c < kLuCB; ++c) acc[c] = fma(l, x[j * kLuCB + c], acc[c]);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < kLuCB; ++c)
+        for (int o = 1; o < 8; o <<= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+    if (pt == 0 && r < rows)
+#pragma unroll
+        for (int c = 0; c < kLuCB; ++c) part[r][c] = acc[c];
+}
+
+__global__ void __launch_bounds__(256) k_lu_solve_blk(int64_t n, const double *__restrict__ lu,
+                                                      const int32_t *__restrict__ piv, int64_t nrhs,
+                                                      double *__restrict__ b)
+{
+    extern __shared__ double xs[];                   // [n][kLuCB]
+    __shared__ double part[kLuRB][kLuCB];
+    __shared__ double dg[kLuRB][kLuRB + 1];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int64_t c0 = (int64_t)blockIdx.x * kLuCB;
+    const int ncol = (int)(nrhs - c0 < kLuCB ? nrhs - c0 : kLuCB);
+    for (int64_t i = tid; i < n * kLuCB; i += blockDim.x) {
+        const int64_t r = i / kLuCB;
+        const int c = (int)(i % kLuCB);
+        xs[i] = c < ncol ? b[r * nrhs + c0 + c] : 0.0;
+    }
+    __syncthreads();
+    if (tid < kLuCB)   // row interchanges, in order
+        for (int64_t k = 0; k < n; ++k) {
+            const int64_t p = piv[k];
+            if (p != k) {
+                const double t = xs[k * kLuCB + tid];
+                xs[k * kLuCB + tid] = xs[p * kLuCB + tid];
+                xs[p * kLuCB + tid] = t;
+            }
+        }
+    const int64_t nblk = (n + kLuRB - 1) / kLuRB;
+    // forward: L with unit diagonal
+    for (int64_t I = 0; I < nblk; ++I) {
+        const int64_t r0 = I * kLuRB;
+        const int rows = (int)(n - r0 < kLuRB ? n - r0 : kLuRB);
+        __syncthreads();
+        lu_block_sums(n, lu, xs, r0, rows, 0, r0, part);
+        for (int i = tid; i < kLuRB * kLuRB; i += blockDim.x) {
+            const int rr = i / kLuRB, kk = i % kLuRB;
+            dg[rr][kk] = (rr < rows && kk < rows) ? lu[(r0 + rr) * n + r0 + kk] : 0.0;
+        }
+        __syncthreads();
+        if (warp < kLuCB) {
+            const int c = warp;
+            double v = lane < rows ? xs[(r0 + lane) * kLuCB + c] - part[lane][c] : 0.0;
+            for (int k = 0; k < rows; ++k) {
+                const double xk = __shfl_sync(0xffffffffu, v, k);
+                if (lane > k) v = fma(-dg[lane][k], xk, v);
+            }
+            if (lane < rows) xs[(r0 + lane) * kLuCB + c] = v;
+        }
+    }
+    // backward: U
+    for (int64_t I = nblk - 1; I >= 0; --I) {
+        const int64_t r0 = I * kLuRB;
+        const int rows = (int)(n - r0 < kLuRB ? n - r0 : kLuRB);
+        __syncthreads();
+        lu_block_sums(n, lu, xs, r0, rows, r0 + rows, n, part);
+        for (int i = tid; i < kLuRB * kLuRB; i += blockDim.x) {
+            const int rr = i / kLuRB, kk = i % kLuRB;
+            dg[rr][kk] = (rr < rows && kk < rows) ? lu[(r0 + rr) * n + r0 + kk] : 1.0;
+        }
+        __syncthreads();
+        if (warp < kLuCB) {
+            const int c = warp;
+            double v = lane < rows ? xs[(r0 + lane) * kLuCB + c] - part[lane][c] : 0.0;
+            for (int k = rows - 1; k >= 0; --k) {
+                if (lane == k) v = v / dg[k][k];
+                const double xk = __shfl_sync(0xffffffffu, v, k);
+                if (lane < k) v = fma(-dg[lane][k], xk, v);
+            }
+            if (lane < rows) xs[(r0 + lane) * kLuCB + c] = v;
+        }
+    }
+    __syncthreads();
+    for (int64_t i = tid; i < n * kLuCB; i += blockDim.x) {
+        const int64_t r = i / kLuCB;
+        const int c = (int)(i % kLuCB);
+        if (c < ncol) b[r * nrhs + c0 + c] = xs[i];
+    }
+}
+
 }  // namespace gm
 
 using namespace gm;
@@ -640,14 +761,9 @@ extern "C" int gm_pseudo_cl(int64_t lmax, int64_t n1, const double *alm1, int64_
     if (!alm1 || !alm2 || !cls) return GM_ERR_BAD_PTR;
     const int64_t L = lmax + 1;
     cudaStream_t s = as_stream(stream);
-    cudaError_t e = cudaMemsetAsync(cls, 0, sizeof(double) * n1 * n2 * L, s);
-    if (e != cudaSuccess) {
-        set_error("gm_pseudo_cl memset", e);
-        return GM_ERR_LAUNCH;
-    }
-    dim3 grid((unsigned)((L + 255) / 256), (unsigned)((L + kPclMChunk - 1) / kPclMChunk),
-              (unsigned)(n1 * n2));
-    k_pseudo_cl<<<grid, 256, 0, s>>>(lmax, n1, (const double2 *)alm1, n2, (const double2 *)alm2, cls);
+    dim3 grid((unsigned)((L + kPclLanes - 1) / kPclLanes), (unsigned)(n1 * n2));
+    k_pseudo_cl<<<grid, kPclLanes * kPclWarps, 0, s>>>(lmax, n1, (const double2 *)alm1, n2,
+                                                       (const double2 *)alm2, cls);
     return check_launch("gm_pseudo_cl");
 }
 
@@ -803,6 +919,19 @@ extern "C" int gm_lu_solve(int64_t n, const double *lu, const int32_t *piv, int6
 {
     if (n < 1 || nrhs < 1) return GM_ERR_BAD_SHAPE;
     if (!lu || !piv || !b) return GM_ERR_BAD_PTR;
+    const size_t smem = (size_t)n * kLuCB * sizeof(double);
+    if (smem <= 200 * 1024) {
+        // the columns of b fit in shared memory: the blocked solve
+        cudaError_t e = cudaFuncSetAttribute(k_lu_solve_blk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) {
+            set_error("gm_lu_solve attr", e);
+            return GM_ERR_LAUNCH;
+        }
+        k_lu_solve_blk<<<(unsigned)((nrhs + kLuCB - 1) / kLuCB), 256, smem, as_stream(stream)>>>(n, lu, piv,
+                                                                                                nrhs, b);
+        return check_launch("gm_lu_solve");
+    }
     const int64_t threads = 256, warps_per = threads / 32;
     k_lu_solve<<<(unsigned)((nrhs + warps_per - 1) / warps_per), (unsigned)threads, 0,
                  as_stream(stream)>>>(n, lu, piv, nrhs, b);

@@ -157,7 +157,8 @@ int gm_legendre_synthesis_tile(int precision, int spin, int64_t nside, int64_t l
 /* ------------------------------------------------------------- spectra */
 
 /* Coupled pseudo-C_ell of all component pairs (replaces workspaces.py:86-95
- * `_compute_coupled_cell`): cls[(i n2 + j) (lmax+1) + l]. */
+ * `_compute_coupled_cell`): cls[(i n2 + j) (lmax+1) + l].  The sum over orders runs in a
+ * fixed order: equal inputs give bit-equal spectra. */
 int gm_pseudo_cl(int64_t lmax, int64_t n1, const double *alm1, int64_t n2,
                  const double *alm2, double *cls, void *stream);
 
