@@ -48,11 +48,11 @@ KERNEL_OF = {"tc_analysis_s2": "k_ana_ck<2>", "tc_analysis_s0": "k_ana_ck<0>",
 KERNEL_OF_CARRIED = {"tc_analysis_s2": "k_ana_tc<2>", "tc_analysis_s0": "k_ana_tc<0>",
                      "tc_synthesis_s2": "k_syn_tc<2>", "tc_synthesis_s0": "k_syn_tc<0>"}
 
-# DRAM traffic of one checkpointed analysis launch: ncu measured 1.539 GB (dram__bytes_read.sum
-# + dram__bytes_write.sum) for the spin-2 launch of 8 fields at Nside 512, 1.025 x the byte
+# DRAM traffic of one checkpointed analysis launch: ncu measured 1.545 GB (dram__bytes_read.sum
+# + dram__bytes_write.sum) for the spin-2 launch of 8 fields at Nside 512, 1.029 x the byte
 # model below (operand images read once, alm accumulator read and written once, checkpoint
-# states read once); the launch at the benchmark size is given as that model x 1.025.
-CK_TRAFFIC_RATIO = 1.539 / 1.501
+# states read once); the launch at the benchmark size is given as that model x 1.029.
+CK_TRAFFIC_RATIO = 1.545 / 1.501
 
 
 def ck_analysis_bytes(nside, lmax, nrows):
@@ -1349,8 +1349,8 @@ def main():
             "note": "algorithmic flops per launch (one complex MAC = 4 flops per (l, m, lane) and "
                     "map; the f16x3 split issues 3x these on the tensor pipe) / CUDA-event time "
                     "of the launch; peak = measured sustained bf16 dense (MEASURED_PEAKS.json); traffic = "
-                    "DRAM bytes read + written per launch: ncu measured 1.025x the launch's byte "
-                    "model at Nside 512 (8 fields); the model scaled to this workload x 1.025",
+                    "DRAM bytes read + written per launch: ncu measured 1.029x the launch's byte "
+                    "model at Nside 512 (8 fields); the model scaled to this workload x 1.029",
             "launches": dom_launches, "avg_ms": dom_avg_ms,
             "tensor_pipe_tflops_issued": 3 * dom_tflops,
         },

@@ -115,6 +115,12 @@ SIGNATURES = {
     "gm_ck_prep_syn": ([_c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_i64, _c_dbl, _c_vp], _c_int),
     "gm_ck_synthesis": ([_c_i64, _c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
                          _c_vp, _c_vp, _c_dbl, _c_vp, _c_vp], _c_int),
+    "gm_ck_segments": ([_c_i64, _c_int], _c_i64),
+    "gm_ck_masks": ([_c_i64, _c_i64, _c_int, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp], _c_int),
+    "gm_ck_analysis_masked": ([_c_i64, _c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
+                               _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_i64, _c_vp, _c_vp], _c_int),
+    "gm_ck_synthesis_masked": ([_c_i64, _c_i64, _c_int, _c_int, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
+                                _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_vp, _c_vp], _c_int),
 }
 
 STATUS = {0: "GM_OK", 1: "GM_ERR_BAD_SHAPE", 2: "GM_ERR_BAD_PTR", 3: "GM_ERR_LAUNCH",
@@ -131,7 +137,8 @@ LAUNCHES = {"gm_last_error": 0, "gm_version": 0, "gm_ring_twiddle_count": 0,
             "gm_tc_ana_image_bytes": 0, "gm_tc_ana_scratch_bytes": 0,
             "gm_tc_syn_chunk_offsets": 0, "gm_tc_syn_image_bytes": 0, "gm_legendre_tiles": 0,
             "gm_coupling_units": 0, "gm_ring_big_scratch_bytes": 0, "gm_ck_offsets": 0,
-            "gm_ck_table_entries": 0, "gm_ck_syn_chunk_offsets": 0}
+            "gm_ck_table_entries": 0, "gm_ck_syn_chunk_offsets": 0, "gm_ck_segments": 0,
+            "gm_ck_masks": 2}
 CALLS = {}
 
 

@@ -162,6 +162,29 @@ ffi::Error CkAnalysis(cudaStream_t s, ffi::AnyBuffer geom, ffi::AnyBuffer coef, 
                                        scale, nctas, rptr<int32_t>(err), s));
 }
 
+ffi::Error CkMasks(cudaStream_t s, ffi::AnyBuffer ck_state, ffi::AnyBuffer ck_shift, ffi::AnyBuffer segoff,
+                   ffi::AnyBuffer uoff, ffi::Result<ffi::AnyBuffer> seg_mask, ffi::Result<ffi::AnyBuffer> unit_mask,
+                   int64_t nside, int64_t lmax, int32_t spin)
+{
+    return status_error(gm_ck_masks(nside, lmax, spin, ck_state.untyped_data(), ptr<const uint8_t>(ck_shift),
+                                    ptr<const int64_t>(segoff), ptr<const int64_t>(uoff), rptr<uint64_t>(seg_mask),
+                                    rptr<uint64_t>(unit_mask), s));
+}
+
+ffi::Error CkAnalysisMasked(cudaStream_t s, ffi::AnyBuffer geom, ffi::AnyBuffer coef, ffi::AnyBuffer segoff,
+                            ffi::AnyBuffer uoff, ffi::AnyBuffer ck_state, ffi::AnyBuffer ck_shift,
+                            ffi::AnyBuffer unit_mask, ffi::AnyBuffer img, ffi::AnyBuffer alm_in,
+                            ffi::Result<ffi::AnyBuffer> alm_i, ffi::Result<ffi::AnyBuffer> err, int64_t nside,
+                            int64_t lmax, int32_t spin, int32_t sp, int64_t ncomp, double scale, int64_t nctas)
+{
+    return status_error(gm_ck_analysis_masked(nside, lmax, spin, sp, ncomp, ptr<const double>(geom),
+                                              ptr<const double>(coef), ptr<const int64_t>(segoff),
+                                              ptr<const int64_t>(uoff), ck_state.untyped_data(),
+                                              ptr<const uint8_t>(ck_shift), ptr<const uint64_t>(unit_mask),
+                                              img.untyped_data(), rptr<double>(alm_i), scale, nctas,
+                                              rptr<int32_t>(err), s));
+}
+
 ffi::Error CkPrepSyn(cudaStream_t s, ffi::AnyBuffer alm_i, ffi::AnyBuffer choff, ffi::Result<ffi::AnyBuffer> simg,
                      int64_t lmax, int32_t spin, int32_t sp, int64_t ncomp, double alm_scale)
 {
@@ -180,6 +203,20 @@ ffi::Error CkSynthesis(cudaStream_t s, ffi::AnyBuffer geom, ffi::AnyBuffer coef,
                                         ck_state.untyped_data(), ptr<const uint8_t>(ck_shift),
                                         simg.untyped_data(), ptr<const int64_t>(choff), rptr<float>(synd),
                                         out_scale, rptr<int32_t>(err), s));
+}
+
+ffi::Error CkSynthesisMasked(cudaStream_t s, ffi::AnyBuffer geom, ffi::AnyBuffer coef, ffi::AnyBuffer segoff,
+                             ffi::AnyBuffer ck_state, ffi::AnyBuffer ck_shift, ffi::AnyBuffer seg_mask,
+                             ffi::AnyBuffer simg, ffi::AnyBuffer choff, ffi::Result<ffi::AnyBuffer> synd,
+                             ffi::Result<ffi::AnyBuffer> err, int64_t nside, int64_t lmax, int32_t spin, int32_t sp,
+                             int64_t ncomp, double out_scale)
+{
+    return status_error(gm_ck_synthesis_masked(nside, lmax, spin, sp, ncomp, ptr<const double>(geom),
+                                               ptr<const double>(coef), ptr<const int64_t>(segoff),
+                                               ck_state.untyped_data(), ptr<const uint8_t>(ck_shift),
+                                               ptr<const uint64_t>(seg_mask), simg.untyped_data(),
+                                               ptr<const int64_t>(choff), rptr<float>(synd), out_scale,
+                                               rptr<int32_t>(err), s));
 }
 
 ffi::Error TcFold(cudaStream_t s, ffi::AnyBuffer synd_a, ffi::AnyBuffer synd_b, ffi::AnyBuffer rhs_map,
@@ -316,6 +353,25 @@ XLA_FFI_DEFINE_HANDLER_SYMBOL(gmb_ck_analysis, CkAnalysis,
                                   .Attr<int64_t>("nside").Attr<int64_t>("lmax").Attr<int32_t>("spin")
                                   .Attr<int32_t>("sp").Attr<int64_t>("ncomp").Attr<double>("scale")
                                   .Attr<int64_t>("nctas"));
+XLA_FFI_DEFINE_HANDLER_SYMBOL(gmb_ck_masks, CkMasks,
+                              GMB_STREAM.Arg<ffi::AnyBuffer>().Arg<ffi::AnyBuffer>().Arg<ffi::AnyBuffer>()
+                                  .Arg<ffi::AnyBuffer>().Ret<ffi::AnyBuffer>().Ret<ffi::AnyBuffer>()
+                                  .Attr<int64_t>("nside").Attr<int64_t>("lmax").Attr<int32_t>("spin"));
+XLA_FFI_DEFINE_HANDLER_SYMBOL(gmb_ck_analysis_masked, CkAnalysisMasked,
+                              GMB_STREAM.Arg<ffi::AnyBuffer>().Arg<ffi::AnyBuffer>().Arg<ffi::AnyBuffer>()
+                                  .Arg<ffi::AnyBuffer>().Arg<ffi::AnyBuffer>().Arg<ffi::AnyBuffer>()
+                                  .Arg<ffi::AnyBuffer>().Arg<ffi::AnyBuffer>().Arg<ffi::AnyBuffer>()
+                                  .Ret<ffi::AnyBuffer>().Ret<ffi::AnyBuffer>()
+                                  .Attr<int64_t>("nside").Attr<int64_t>("lmax").Attr<int32_t>("spin")
+                                  .Attr<int32_t>("sp").Attr<int64_t>("ncomp").Attr<double>("scale")
+                                  .Attr<int64_t>("nctas"));
+XLA_FFI_DEFINE_HANDLER_SYMBOL(gmb_ck_synthesis_masked, CkSynthesisMasked,
+                              GMB_STREAM.Arg<ffi::AnyBuffer>().Arg<ffi::AnyBuffer>().Arg<ffi::AnyBuffer>()
+                                  .Arg<ffi::AnyBuffer>().Arg<ffi::AnyBuffer>().Arg<ffi::AnyBuffer>()
+                                  .Arg<ffi::AnyBuffer>().Arg<ffi::AnyBuffer>().Ret<ffi::AnyBuffer>()
+                                  .Ret<ffi::AnyBuffer>()
+                                  .Attr<int64_t>("nside").Attr<int64_t>("lmax").Attr<int32_t>("spin")
+                                  .Attr<int32_t>("sp").Attr<int64_t>("ncomp").Attr<double>("out_scale"));
 XLA_FFI_DEFINE_HANDLER_SYMBOL(gmb_ck_prep_syn, CkPrepSyn,
                               GMB_STREAM.Arg<ffi::AnyBuffer>().Arg<ffi::AnyBuffer>().Ret<ffi::AnyBuffer>()
                                   .Attr<int64_t>("lmax").Attr<int32_t>("spin").Attr<int32_t>("sp")

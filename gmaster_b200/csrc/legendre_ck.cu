@@ -88,7 +88,26 @@ struct CkParams {
     const int64_t *uoff;     // (L + 1): first analysis unit of each order
     const float2 *ck;        // (segments, nlanes): pre-state (v_{l_s - 1}, D_{l_s}), scaled
     const uint8_t *cn;       // (segments, nlanes): shift n
+    // optional (NULL: every lane group active): bit g set when a lane of the 64-lane group g
+    // has a non-zero stored state, per segment (synthesis) or per analysis unit (the union of
+    // its two segments).  A segment that starts from a zero state stays exactly zero.
+    const unsigned long long *seg_mask;   // (segments)
+    const unsigned long long *unit_mask;  // (analysis units)
 };
+
+__device__ __forceinline__ unsigned long long all_groups(int64_t ngroups)
+{
+    return ngroups >= 64 ? ~0ull : ((1ull << ngroups) - 1ull);
+}
+
+// Pops the lowest set bit of r and returns its index, or -1 when r is empty.
+__device__ __forceinline__ int pop_group(unsigned long long &r)
+{
+    if (!r) return -1;
+    const int g = __ffsll((long long)r) - 1;
+    r &= r - 1ull;
+    return g;
+}
 
 __host__ __device__ __forceinline__ int64_t first_row(int64_t m, int sp)
 {
@@ -230,6 +249,30 @@ __global__ void __launch_bounds__(128) k_ck_build(int64_t nside, int64_t lmax, i
     }
 }
 
+// Non-zero 64-lane groups of every checkpoint segment (nlanes <= 4096): bit g of
+// seg_mask[seg] is set when a lane of group g has a non-zero stored state or shift.
+__global__ void __launch_bounds__(256) k_ck_seg_mask(int64_t nlanes, int64_t nseg, const float2 *__restrict__ ck,
+                                                     const uint8_t *__restrict__ cn,
+                                                     unsigned long long *__restrict__ seg_mask)
+{
+    __shared__ unsigned long long acc;
+    for (int64_t seg = blockIdx.x; seg < nseg; seg += gridDim.x) {
+        if (threadIdx.x == 0) acc = 0ull;
+        __syncthreads();
+        unsigned long long bits = 0ull;
+        for (int64_t j = threadIdx.x; j < nlanes; j += blockDim.x) {
+            const float2 st = __ldg(ck + seg * nlanes + j);
+            const uint8_t n = __ldg(cn + seg * nlanes + j);
+            if (st.x != 0.f || st.y != 0.f || n != 0) bits |= 1ull << (j >> 6);
+        }
+        for (int o = 16; o >= 1; o >>= 1) bits |= __shfl_xor_sync(0xffffffffu, bits, o);
+        if ((threadIdx.x & 31) == 0 && bits) atomicOr(&acc, bits);
+        __syncthreads();
+        if (threadIdx.x == 0) seg_mask[seg] = acc;
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------------------------- analysis
 
 struct __align__(8) AnaShared {
@@ -248,6 +291,22 @@ __device__ __forceinline__ int64_t unit_order(const int64_t *__restrict__ uoff, 
         else hi = mid;
     }
     return lo;
+}
+
+// Analysis unit masks: unit u = (order m, superblock s) takes the union of the masks of
+// its segments 2 s and 2 s + 1 (when the order has it).
+__global__ void k_ck_unit_mask(int64_t L, const int64_t *__restrict__ segoff, const int64_t *__restrict__ uoff,
+                               const unsigned long long *__restrict__ seg_mask,
+                               unsigned long long *__restrict__ unit_mask)
+{
+    const int64_t U = uoff[L];
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < U; u += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t m = unit_order(uoff, L, u);
+        const int64_t s0 = segoff[m] + 2 * (u - uoff[m]);
+        unsigned long long mk = seg_mask[s0];
+        if (s0 + 1 < segoff[m + 1]) mk |= seg_mask[s0 + 1];
+        unit_mask[u] = mk;
+    }
 }
 
 __device__ __forceinline__ void gen_barrier_a() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
@@ -309,12 +368,16 @@ __global__ void __launch_bounds__(kThrA, 1) k_ana_ck(CkParams p, const uint8_t *
             int64_t jg = 0;
             bool ok = true;
             for (int64_t u = c; u < U && ok; u += G, ++q) {
-                for (int64_t g = 0; g < NGK && ok; ++g, ++jg) {
+                // the previous unit's epilogue has read TMEM (waited for every unit, so the
+                // phases stay in step); a unit without active groups only signals d_full
+                if (!(ok = wait_or_abort(&sh.d_free, (q & 1) ^ 1, abort, err))) break;
+                unsigned long long rest = p.unit_mask ? (__ldg(p.unit_mask + u) & all_groups(NGK)) : all_groups(NGK);
+                int k = 0;
+                for (int g = pop_group(rest); g >= 0 && ok; g = pop_group(rest), ++jg, ++k) {
                     const uint32_t b = (uint32_t)(jg & 1);
-                    const int S = (int)(g & 1);
+                    const int S = k & 1;
                     const uint32_t ph = S ? cnt1 : cnt0;
                     if (!(ok = wait_or_abort(&sh.a_full[b], (uint32_t)(jg >> 1) & 1, abort, err))) break;
-                    if (g == 0 && !(ok = wait_or_abort(&sh.d_free, (q & 1) ^ 1, abort, err))) break;
                     if (!(ok = wait_or_abort(&sh.b_full[S], ph & 1, abort, err))) break;
                     tc::tc_fence_after();
                     const uint32_t a0 = tc::smem_u32(sA + b * kAImgG);
@@ -325,17 +388,18 @@ __global__ void __launch_bounds__(kThrA, 1) k_ana_ck(CkParams p, const uint8_t *
                         const uint64_t al = tc::desc_sw128_mn(a0 + kAImgG / 2 + ks * 4096, 1024, 2048);
                         const uint64_t bh = tc::desc_sw128_mn(b0 + ks * 8192, 1024, 4096);
                         const uint64_t bl = tc::desc_sw128_mn(b0 + kTileA / 2 + ks * 8192, 1024, 4096);
-                        const uint32_t acc = (g > 0 || ks > 0) ? 1u : 0u;
+                        const uint32_t acc = (k > 0 || ks > 0) ? 1u : 0u;
                         tc::mma_f16(tmem, ah, bh, idesc, acc);
                         tc::mma_f16(tmem + kSB, ah, bl, idesc, acc);
                         tc::mma_f16(tmem + kSB, al, bh, idesc, 1u);
                     }
                     tc::mma_commit(&sh.b_free[S]);
                     tc::mma_commit(&sh.a_free[b]);
-                    if (g == NGK - 1) tc::mma_commit(&sh.d_full);
                     if (S) ++cnt1;
                     else ++cnt0;
                 }
+                if (!ok) break;
+                tc::mma_commit(&sh.d_full);
             }
             // every issued MMA completes before TMEM is released (bounded wait)
             tc::mma_commit(&sh.drain);
@@ -352,7 +416,8 @@ __global__ void __launch_bounds__(kThrA, 1) k_ana_ck(CkParams p, const uint8_t *
             bool ok = true;
             for (int64_t u = c; u < U && ok; u += G) {
                 const int64_t m = unit_order(p.uoff, L, u);
-                for (int64_t g = 0; g < NGK; ++g, ++jg) {
+                unsigned long long rest = p.unit_mask ? (__ldg(p.unit_mask + u) & all_groups(NGK)) : all_groups(NGK);
+                for (int g = pop_group(rest); g >= 0; g = pop_group(rest), ++jg) {
                     const uint32_t b = (uint32_t)(jg & 1);
                     const uint8_t *src = aimg + ((m * NG + (g >> 1)) * 2) * (int64_t)kAImg + (g & 1) * (kAImgG / 2);
                     tc::prefetch_l2(src, kAImgG / 2);
@@ -419,13 +484,25 @@ __global__ void __launch_bounds__(kThrA, 1) k_ana_ck(CkParams p, const uint8_t *
                     nx = __ldg(p.geom + j);
                 }
             };
-            if (!dead) fetch(S);
-            for (int64_t g = S; g < NGK; g += 2, ++js) {
-                if (dead) continue;
+            // this set's groups: the active groups at positions S, S + 2, ... of the unit
+            const unsigned long long umask =
+                p.unit_mask ? (__ldg(p.unit_mask + u) & all_groups(NGK)) : all_groups(NGK);
+            unsigned long long rest = umask;
+            if (S) pop_group(rest);
+            int g = pop_group(rest);
+            if (!dead && g >= 0) fetch(g);
+            for (; g >= 0; ++js) {
+                pop_group(rest);                      // the other set's group
+                const int gnext = pop_group(rest);
+                if (dead) {
+                    g = gnext;
+                    continue;
+                }
                 float v = nst.x, D = nst.y;
                 const float y = (float)(nx - 1.0);
                 int n = nn;
-                if (g + 2 < NGK) fetch(g + 2);
+                if (gnext >= 0) fetch(gnext);
+                g = gnext;
                 if (!warp_wait(&sh.b_free[S], (js & 1) ^ 1, abort, err)) {
                     dead = true;
                     continue;
@@ -447,7 +524,9 @@ __global__ void __launch_bounds__(kThrA, 1) k_ana_ck(CkParams p, const uint8_t *
             const uint32_t q = (uint32_t)((u - c) / G);
             if (!dead && !warp_wait(&sh.d_full, q & 1, abort, err)) dead = true;
             float *stage = reinterpret_cast<float *>(sB);   // [128 rows][kStageLd] floats
-            if (!dead) {
+            // a unit without active groups adds nothing (its accumulator was never written)
+            const bool out = !dead && umask != 0ull;
+            if (out) {
                 tc::tc_fence_after();
                 const int row = 32 * (warp & 3) + lane, c0 = 128 * (warp >> 2);
                 for (int cb = c0; cb < c0 + 128; cb += 16) {
@@ -465,7 +544,7 @@ __global__ void __launch_bounds__(kThrA, 1) k_ana_ck(CkParams p, const uint8_t *
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(&sh.d_free);   // TMEM may be overwritten
             gen_barrier_a();                               // every row staged
-            if (!dead) {
+            if (out) {
                 // output (row orow of the interleaved alm, row l = lb + i): the north image row
                 // orow - o0 and the south image row H + orow - o1 (with the hemisphere parity
                 // (-1)^(l + m)) where they exist; consecutive threads take consecutive orow
@@ -506,8 +585,11 @@ __device__ __forceinline__ void set_barrier_s(int set)
 }
 
 // One CTA per (order m, tile of 256 lanes).  Chunk cc of order m covers rows
-// l0 + 64 cc + [0, 64) (image index choff[m] + cc); segment k = chunks 2k, 2k + 1 is
-// generated by set k & 1 from its checkpoint.  D[row, lane] = sum_l almT[row, l] lambda_l(lane).
+// l0 + 64 cc + [0, 64) (image index choff[m] + cc); segment k = chunks 2k, 2k + 1.  Only the
+// segments in which some lane of the tile has a non-zero state are generated and
+// contracted (the others are exactly zero); the i-th of them is generated by set i % 2
+// from its checkpoint.  D[row, lane] = sum_l almT[row, l] lambda_l(lane).
+constexpr int kMaxSegS = 512;   // segments of an order at lmax <= 65535
 template <int SPIN>
 __global__ void __launch_bounds__(kThrS, 1) k_syn_ck(CkParams p, const uint8_t *__restrict__ simg,
                                                      const int64_t *__restrict__ choff,
@@ -516,6 +598,8 @@ __global__ void __launch_bounds__(kThrS, 1) k_syn_ck(CkParams p, const uint8_t *
 {
     extern __shared__ uint8_t smem_raw[];
     __shared__ SynShared sh;
+    __shared__ short slist[kMaxSegS];   // active segments of the order, ascending
+    __shared__ int snact;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t base = (tc::smem_u32(smem_raw) + 1023u) & ~1023u;
     uint8_t *smem = smem_raw + (base - tc::smem_u32(smem_raw));
@@ -527,7 +611,26 @@ __global__ void __launch_bounds__(kThrS, 1) k_syn_ck(CkParams p, const uint8_t *
     const int64_t l0 = first_row(m, p.sp);
     if (l0 > p.lmax) return;
     const int64_t nch = (L - l0 + kKL - 1) / kKL;
+    const int nseg = (int)((nch + 1) / 2);
 
+    if (warp == 0) {
+        // active segments: some 64-lane group of this tile's 256 lanes has a non-zero state
+        const int64_t s0 = p.segoff[m];
+        int cnt = 0;
+        for (int b0 = 0; b0 < nseg; b0 += 32) {
+            const int k = b0 + lane;
+            bool act = false;
+            if (k < nseg) {
+                act = true;
+                if (p.seg_mask && p.nlanes <= 4096)
+                    act = ((__ldg(p.seg_mask + s0 + k) >> (4 * tile)) & 0xFull) != 0ull;
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, act);
+            if (act) slist[cnt + __popc(bal & ((1u << lane) - 1u))] = (short)k;
+            cnt += __popc(bal);
+        }
+        if (lane == 0) snact = cnt;
+    }
     if (tid == 0) {
         for (int i = 0; i < 2; ++i) {
             tc::mbar_init(&sh.a_full[i], 1);
@@ -549,59 +652,71 @@ __global__ void __launch_bounds__(kThrS, 1) k_syn_ck(CkParams p, const uint8_t *
     tc::tc_fence_after();
     const uint32_t tmem = sh.tmem;
     volatile int *abort = &sh.abort;
+    const int nact = snact;
     const uint8_t *img = simg + (choff[m] - choff[0]) * 2 * (int64_t)kSImg;
+    // absolute chunk of the c-th active chunk walk: segment slist[i], half h
+    auto chunk_of = [&](int i, int h) { return 2 * (int64_t)slist[i] + h; };
+    auto chunks_in = [&](int i) { return 2 * (int64_t)slist[i] + 1 < nch ? 2 : 1; };
 
     if (warp == kMmaWarpS) {
         if (lane == 0) {
             const uint32_t idesc = tc::idesc_f16(128, kLT, 0, 1, 0);
             bool ok = true;
-            int inflight = -1;          // buffer of an image copy not yet waited for
-            uint32_t inflight_ph = 0;   // and the phase it completes
-            tc::mbar_arrive_expect_tx(&sh.a_full[0], 2 * kSImg);
-            tc::bulk_g2s(sA, img, 2 * kSImg, &sh.a_full[0]);
-            inflight = 0;
-            for (int64_t cc = 0; cc < nch && ok; ++cc) {
-                const uint32_t a = (uint32_t)cc & 1, pha = (uint32_t)(cc >> 1) & 1;
-                const int S = (int)((cc >> 1) & 1);
-                const uint32_t phb = (uint32_t)(((cc >> 2) * 2 + (cc & 1)) & 1);
-                if (!(ok = wait_or_abort(&sh.a_full[a], pha, abort, err))) break;
-                inflight = -1;
-                if (!(ok = wait_or_abort(&sh.b_full[S], phb, abort, err))) break;
-                tc::tc_fence_after();
-                const uint32_t a0 = tc::smem_u32(sA + a * 2 * kSImg);
-                const uint32_t b0 = tc::smem_u32(sB + S * 2 * kBTileS);
+            int issued = -1;            // buffer of an image copy not yet waited for
+            uint32_t issued_ph = 0;     // and the phase it completes
+            uint32_t cs[2] = {0u, 0u};  // chunks consumed from each set's tile
+            int64_t c = 0;              // active chunks so far (image ring position)
+            if (nact > 0) {
+                tc::mbar_arrive_expect_tx(&sh.a_full[0], 2 * kSImg);
+                tc::bulk_g2s(sA, img + chunk_of(0, 0) * 2 * (int64_t)kSImg, 2 * kSImg, &sh.a_full[0]);
+                issued = 0;
+            }
+            for (int i = 0; i < nact && ok; ++i) {
+                const int S = i & 1, nh = chunks_in(i);
+                for (int h = 0; h < nh && ok; ++h, ++c) {
+                    const uint32_t a = (uint32_t)c & 1, pha = (uint32_t)(c >> 1) & 1;
+                    if (!(ok = wait_or_abort(&sh.a_full[a], pha, abort, err))) break;
+                    issued = -1;
+                    if (!(ok = wait_or_abort(&sh.b_full[S], cs[S] & 1, abort, err))) break;
+                    tc::tc_fence_after();
+                    const uint32_t a0 = tc::smem_u32(sA + a * 2 * kSImg);
+                    const uint32_t b0 = tc::smem_u32(sB + S * 2 * kBTileS);
 #pragma unroll
-                for (int ks = 0; ks < kKL / 16; ++ks) {
-                    const uint64_t ah = tc::desc_sw128_mn(a0 + ks * 4096, 1024, 2048);
-                    const uint64_t al = tc::desc_sw128_mn(a0 + kSImg + ks * 4096, 1024, 2048);
-                    const uint64_t bh = tc::desc_sw128(b0 + ks * 32);
-                    const uint64_t bl = tc::desc_sw128(b0 + kBTileS + ks * 32);
-                    const uint32_t acc = (cc > 0 || ks > 0) ? 1u : 0u;
-                    tc::mma_f16(tmem, ah, bh, idesc, acc);
-                    tc::mma_f16(tmem + kLT, ah, bl, idesc, acc);
-                    tc::mma_f16(tmem + kLT, al, bh, idesc, 1u);
-                }
-                tc::mma_commit(&sh.b_free[S]);
-                tc::mma_commit(&sh.a_free[a]);
-                if (cc + 1 < nch) {
-                    // the next chunk's image goes into the buffer of chunk cc - 1 once its MMAs are done
-                    const uint32_t nb = (uint32_t)(cc + 1) & 1;
-                    if (!(ok = wait_or_abort(&sh.a_free[nb], ((uint32_t)((cc + 1) >> 1) & 1) ^ 1, abort, err)))
-                        break;
-                    tc::mbar_arrive_expect_tx(&sh.a_full[nb], 2 * kSImg);
-                    tc::bulk_g2s(sA + nb * 2 * kSImg, img + (cc + 1) * 2 * (int64_t)kSImg, 2 * kSImg,
-                                 &sh.a_full[nb]);
-                    inflight = (int)nb;
-                    inflight_ph = (uint32_t)((cc + 1) >> 1) & 1;
+                    for (int ks = 0; ks < kKL / 16; ++ks) {
+                        const uint64_t ah = tc::desc_sw128_mn(a0 + ks * 4096, 1024, 2048);
+                        const uint64_t al = tc::desc_sw128_mn(a0 + kSImg + ks * 4096, 1024, 2048);
+                        const uint64_t bh = tc::desc_sw128(b0 + ks * 32);
+                        const uint64_t bl = tc::desc_sw128(b0 + kBTileS + ks * 32);
+                        const uint32_t acc = (c > 0 || ks > 0) ? 1u : 0u;
+                        tc::mma_f16(tmem, ah, bh, idesc, acc);
+                        tc::mma_f16(tmem + kLT, ah, bl, idesc, acc);
+                        tc::mma_f16(tmem + kLT, al, bh, idesc, 1u);
+                    }
+                    tc::mma_commit(&sh.b_free[S]);
+                    tc::mma_commit(&sh.a_free[a]);
+                    ++cs[S];
+                    // the next active chunk's image goes into the buffer of chunk c - 1 once
+                    // its MMAs are done
+                    const bool more = h + 1 < nh || i + 1 < nact;
+                    if (more) {
+                        const int64_t cn = h + 1 < nh ? chunk_of(i, h + 1) : chunk_of(i + 1, 0);
+                        const uint32_t nb = (uint32_t)(c + 1) & 1;
+                        if (!(ok = wait_or_abort(&sh.a_free[nb], ((uint32_t)((c + 1) >> 1) & 1) ^ 1, abort, err)))
+                            break;
+                        tc::mbar_arrive_expect_tx(&sh.a_full[nb], 2 * kSImg);
+                        tc::bulk_g2s(sA + nb * 2 * kSImg, img + cn * 2 * (int64_t)kSImg, 2 * kSImg, &sh.a_full[nb]);
+                        issued = (int)nb;
+                        issued_ph = (uint32_t)((c + 1) >> 1) & 1;
+                    }
                 }
             }
             if (ok) tc::mma_commit(&sh.d_full);
             tc::mma_commit(&sh.drain);
             tc::mbar_wait(&sh.drain, 0);
-            if (inflight >= 0) tc::mbar_wait(&sh.a_full[inflight], inflight_ph);
+            if (issued >= 0) tc::mbar_wait(&sh.a_full[issued], issued_ph);
         }
     } else {
-        const int S = warp >> 3;              // set: segments k with k % 2 == S
+        const int S = warp >> 3;              // set: active segments i with i % 2 == S
         const int t = tid & (kLT - 1);        // lane within the tile (the MMA N row)
         const int64_t jl = tile * kLT + t;
         const bool valid = jl < p.nlanes;
@@ -617,10 +732,11 @@ __global__ void __launch_bounds__(kThrS, 1) k_syn_ck(CkParams p, const uint8_t *
         float2 nst = make_float2(0.f, 0.f);
         int nn = 0;
         float4 ncoef = make_float4(0.f, 0.f, 0.f, 0.f);
-        auto fetch = [&](int64_t k) {
+        auto fetch = [&](int i) {
             nst = make_float2(0.f, 0.f);
             nn = 0;
-            if (2 * k >= nch) return;
+            if (i >= nact) return;
+            const int64_t k = slist[i];
             if (valid) {
                 const int64_t idx = (p.segoff[m] + k) * p.nlanes + jl;
                 nst = __ldg(p.ck + idx);
@@ -629,15 +745,16 @@ __global__ void __launch_bounds__(kThrS, 1) k_syn_ck(CkParams p, const uint8_t *
             if (t < kSeg) ncoef = diff_coef(p.coef, mb, l0 + kSeg * k + t, L, sgn_c, t == 0);
         };
         fetch(S);
-        for (int64_t k = S; 2 * k < nch; k += 2) {
+        for (int i = S; i < nact; i += 2) {
             set_barrier_s(S);   // the set's previous segment is generated: its rows are free
             if (!dead && t < kSeg) cwin[t] = ncoef;
             set_barrier_s(S);
             if (dead) continue;
             float v = nst.x, D = nst.y;
             int n = nn;
-            fetch(k + 2);
-            for (int half = 0; half < 2 && 2 * k + half < nch; ++half, ++js) {
+            fetch(i + 2);
+            const int nh = chunks_in(i);
+            for (int half = 0; half < nh; ++half, ++js) {
                 if (!warp_wait(&sh.b_free[S], (js & 1) ^ 1, abort, err)) {
                     dead = true;
                     break;
@@ -650,17 +767,23 @@ __global__ void __launch_bounds__(kThrS, 1) k_syn_ck(CkParams p, const uint8_t *
             }
         }
         // epilogue: D[row, lane] -> synd[m][lane][row]; warp w reads TMEM lanes 32 (w % 4)
-        // (rows) and the column quarter w / 4 (lanes)
+        // (rows) and the column quarter w / 4 (lanes).  Without active segments the
+        // output is zero (the accumulator was never written).
         if (!dead && warp_wait(&sh.d_full, 0, abort, err)) {
             tc::tc_fence_after();
             const int wq = warp & 3, row = wq * 32 + lane;
             const int cbeg = (warp >> 2) * (kLT / 4);
             for (int cb = cbeg; cb < cbeg + kLT / 4; cb += 16) {
                 uint32_t r[16], rx[16];
-                const uint32_t trow = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)cb;
-                tc::tmem_ld16(trow, r);
-                tc::tmem_ld16(trow + kLT, rx);
-                tc::tmem_ld_wait();
+                if (nact > 0) {
+                    const uint32_t trow = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)cb;
+                    tc::tmem_ld16(trow, r);
+                    tc::tmem_ld16(trow + kLT, rx);
+                    tc::tmem_ld_wait();
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) r[e] = rx[e] = 0u;
+                }
                 if (row < R2) {
 #pragma unroll
                     for (int e = 0; e < 16; ++e) {
@@ -755,6 +878,8 @@ static CkParams ck_params(int64_t nside, int64_t lmax, int spin, int sp, int64_t
     p.uoff = uoff;
     p.ck = (const float2 *)ck_state;
     p.cn = ck_shift;
+    p.seg_mask = nullptr;
+    p.unit_mask = nullptr;
     return p;
 }
 
@@ -765,11 +890,10 @@ static bool ck_shape_ok(int spin, int64_t ncomp)
     return false;
 }
 
-extern "C" int gm_ck_analysis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
-                              const double *geom, const double *coef, const int64_t *segoff,
-                              const int64_t *uoff, const void *ck_state, const uint8_t *ck_shift,
-                              const void *img, double *alm_i, double scale, int64_t nctas, int32_t *err,
-                              void *stream)
+static int ck_analysis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp, const double *geom,
+                       const double *coef, const int64_t *segoff, const int64_t *uoff, const void *ck_state,
+                       const uint8_t *ck_shift, const uint64_t *unit_mask, const void *img, double *alm_i,
+                       double scale, int64_t nctas, int32_t *err, void *stream)
 {
     if (nside < 1 || lmax < 2 || lmax > 65535 || !ck_shape_ok(spin, ncomp) || !ck_spin_ok(spin, sp) ||
         nctas < 1 || nctas > 4096)
@@ -784,8 +908,57 @@ extern "C" int gm_ck_analysis(int64_t nside, int64_t lmax, int spin, int sp, int
         return GM_ERR_LAUNCH;
     }
     CkParams p = ck_params(nside, lmax, spin, sp, ncomp, geom, coef, segoff, uoff, ck_state, ck_shift, scale);
+    p.unit_mask = (const unsigned long long *)unit_mask;
     kern<<<(unsigned)nctas, kThrA, smem, as_stream(stream)>>>(p, (const uint8_t *)img, alm_i, (int *)err);
     return check_launch("gm_ck_analysis");
+}
+
+extern "C" int gm_ck_analysis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                              const double *geom, const double *coef, const int64_t *segoff,
+                              const int64_t *uoff, const void *ck_state, const uint8_t *ck_shift,
+                              const void *img, double *alm_i, double scale, int64_t nctas, int32_t *err,
+                              void *stream)
+{
+    return ck_analysis(nside, lmax, spin, sp, ncomp, geom, coef, segoff, uoff, ck_state, ck_shift, nullptr, img,
+                       alm_i, scale, nctas, err, stream);
+}
+
+extern "C" int gm_ck_analysis_masked(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                                     const double *geom, const double *coef, const int64_t *segoff,
+                                     const int64_t *uoff, const void *ck_state, const uint8_t *ck_shift,
+                                     const uint64_t *unit_mask, const void *img, double *alm_i, double scale,
+                                     int64_t nctas, int32_t *err, void *stream)
+{
+    if (!unit_mask) return GM_ERR_BAD_PTR;
+    return ck_analysis(nside, lmax, spin, sp, ncomp, geom, coef, segoff, uoff, ck_state, ck_shift, unit_mask,
+                       img, alm_i, scale, nctas, err, stream);
+}
+
+extern "C" int64_t gm_ck_segments(int64_t lmax, int spin)
+{
+    if (lmax < 2 || lmax > 65535 || (spin != 0 && spin != 2)) return -1;
+    int64_t s = 0;
+    for (int64_t m = 0; m <= lmax; ++m) s += ck_nseg(lmax, spin, m);
+    return s;
+}
+
+extern "C" int gm_ck_masks(int64_t nside, int64_t lmax, int spin, const void *ck_state, const uint8_t *ck_shift,
+                           const int64_t *segoff, const int64_t *uoff, uint64_t *seg_mask, uint64_t *unit_mask,
+                           void *stream)
+{
+    if (nside < 1 || 2 * nside > 4096 || lmax < 2 || lmax > 65535 || (spin != 0 && spin != 2))
+        return GM_ERR_BAD_SHAPE;
+    if (!ck_state || !ck_shift || !segoff || !uoff || !seg_mask || !unit_mask) return GM_ERR_BAD_PTR;
+    const int64_t nseg = gm_ck_segments(lmax, spin);
+    cudaStream_t s = as_stream(stream);
+    const unsigned blocks = (unsigned)(nseg < 148 * 16 ? nseg : 148 * 16);
+    k_ck_seg_mask<<<blocks, 256, 0, s>>>(2 * nside, nseg, (const float2 *)ck_state, ck_shift,
+                                         (unsigned long long *)seg_mask);
+    int st = check_launch("gm_ck_masks segments");
+    if (st != GM_OK) return st;
+    k_ck_unit_mask<<<148 * 4, 256, 0, s>>>(lmax + 1, segoff, uoff, (const unsigned long long *)seg_mask,
+                                          (unsigned long long *)unit_mask);
+    return check_launch("gm_ck_masks units");
 }
 
 extern "C" int gm_ck_syn_chunk_offsets(int64_t lmax, int spin, int64_t *choff_host)
@@ -802,11 +975,10 @@ extern "C" int gm_ck_syn_chunk_offsets(int64_t lmax, int spin, int64_t *choff_ho
     return GM_OK;
 }
 
-extern "C" int gm_ck_synthesis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
-                               const double *geom, const double *coef, const int64_t *segoff,
-                               const void *ck_state, const uint8_t *ck_shift, const void *simg,
-                               const int64_t *choff, float *synd, double out_scale, int32_t *err,
-                               void *stream)
+static int ck_synthesis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp, const double *geom,
+                        const double *coef, const int64_t *segoff, const void *ck_state, const uint8_t *ck_shift,
+                        const uint64_t *seg_mask, const void *simg, const int64_t *choff, float *synd,
+                        double out_scale, int32_t *err, void *stream)
 {
     if (nside < 1 || lmax < 2 || lmax > 65535 || !ck_shape_ok(spin, ncomp) || !ck_spin_ok(spin, sp) ||
         !(out_scale > 0.0))
@@ -822,8 +994,30 @@ extern "C" int gm_ck_synthesis(int64_t nside, int64_t lmax, int spin, int sp, in
     }
     CkParams p = ck_params(nside, lmax, spin, sp, ncomp, geom, coef, segoff, nullptr, ck_state, ck_shift,
                            out_scale);
+    p.seg_mask = (const unsigned long long *)seg_mask;
     const int R2 = 2 * p.H;
     dim3 grid((unsigned)((p.nlanes + kLT - 1) / kLT), (unsigned)(lmax + 1));
     kern<<<grid, kThrS, smem, as_stream(stream)>>>(p, (const uint8_t *)simg, choff, synd, R2, (int *)err);
     return check_launch("gm_ck_synthesis");
+}
+
+extern "C" int gm_ck_synthesis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                               const double *geom, const double *coef, const int64_t *segoff,
+                               const void *ck_state, const uint8_t *ck_shift, const void *simg,
+                               const int64_t *choff, float *synd, double out_scale, int32_t *err,
+                               void *stream)
+{
+    return ck_synthesis(nside, lmax, spin, sp, ncomp, geom, coef, segoff, ck_state, ck_shift, nullptr, simg, choff,
+                        synd, out_scale, err, stream);
+}
+
+extern "C" int gm_ck_synthesis_masked(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                                      const double *geom, const double *coef, const int64_t *segoff,
+                                      const void *ck_state, const uint8_t *ck_shift, const uint64_t *seg_mask,
+                                      const void *simg, const int64_t *choff, float *synd, double out_scale,
+                                      int32_t *err, void *stream)
+{
+    if (!seg_mask) return GM_ERR_BAD_PTR;
+    return ck_synthesis(nside, lmax, spin, sp, ncomp, geom, coef, segoff, ck_state, ck_shift, seg_mask, simg,
+                        choff, synd, out_scale, err, stream);
 }

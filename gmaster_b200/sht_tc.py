@@ -23,6 +23,9 @@ MAX_FIELDS_SPIN2 = 32
 # at most this share of the device memory, else the carried-state kernels run.
 USE_CHECKPOINTS = True
 CK_MEMORY_SHARE = 0.2
+# Skip the 64-lane groups whose checkpoint states are all zero (exact: their rows are zero);
+# False runs every group, for comparisons.
+USE_TILE_SKIP = True
 
 _TC_PLANS = {}
 _LOCK = threading.Lock()
@@ -52,6 +55,7 @@ class TCPlan:
         # the tables themselves are built on first use (`ck_tables`)
         self.ck_segoff, self.ck_uoff, self.ck_choff, self.ck_nchunks = {}, {}, {}, {}
         self.ck = {}
+        self.ck_masks = {}
         self.ck_entries = {}
         for spin in (0, 2):
             seg = np.zeros(plan.L + 1, dtype=np.int64)
@@ -117,7 +121,26 @@ def ck_tables(tp, spin):
                       _lib.ptr(shift), _lib.stream_handle(p.device))
             out[sp] = (state, shift)
         tp.ck[spin] = out
+        masks = {}
+        if p.nlanes <= 4096:
+            for sp, (state, shift) in out.items():
+                seg_mask = torch.empty(int(_lib.load().gm_ck_segments(p.lmax, spin)), dtype=torch.int64,
+                                       device=p.device)
+                unit_mask = torch.empty(int(tp.ck_uoff[spin][-1].item()), dtype=torch.int64, device=p.device)
+                _lib.call("gm_ck_masks", p.nside, p.lmax, spin, _lib.ptr(state), _lib.ptr(shift),
+                          _lib.ptr(tp.ck_segoff[spin]), _lib.ptr(tp.ck_uoff[spin]), _lib.ptr(seg_mask),
+                          _lib.ptr(unit_mask), _lib.stream_handle(p.device))
+                masks[sp] = (seg_mask, unit_mask)
+        tp.ck_masks[spin] = masks
         return out
+
+
+def ck_masks(tp, spin, sp):
+    """(seg_mask, unit_mask) of the row variant's checkpoint table, or None (tile skipping
+    off, or a geometry above Nside 2048)."""
+    if not USE_TILE_SKIP:
+        return None
+    return getattr(tp, "ck_masks", {}).get(spin, {}).get(sp)
 
 
 def _rows(spin, ncomp):
@@ -168,11 +191,16 @@ class _Batch:
         ck = ck_tables(tp, self.spin)
         for sp, img in zip(_variants(self.spin), self.img):
             if ck is not None:
-                _lib.call("gm_ck_analysis", p.nside, p.lmax, self.spin, sp, self.ncomp, _lib.ptr(p.geom),
+                mk = ck_masks(tp, self.spin, sp)
+                common = (p.nside, p.lmax, self.spin, sp, self.ncomp, _lib.ptr(p.geom),
                           _lib.ptr(tp.coef[self.spin]), _lib.ptr(tp.ck_segoff[self.spin]),
-                          _lib.ptr(tp.ck_uoff[self.spin]), _lib.ptr(ck[sp][0]), _lib.ptr(ck[sp][1]),
-                          _lib.ptr(img), _lib.ptr(self.alm_i), float(scale) / self.img_scale, tp.nctas,
-                          _lib.ptr(tp.err), _lib.stream_handle(p.device))
+                          _lib.ptr(tp.ck_uoff[self.spin]), _lib.ptr(ck[sp][0]), _lib.ptr(ck[sp][1]))
+                rest = (_lib.ptr(img), _lib.ptr(self.alm_i), float(scale) / self.img_scale, tp.nctas,
+                        _lib.ptr(tp.err), _lib.stream_handle(p.device))
+                if mk is not None:
+                    _lib.call("gm_ck_analysis_masked", *common, _lib.ptr(mk[1]), *rest)
+                else:
+                    _lib.call("gm_ck_analysis", *common, *rest)
                 continue
             _lib.call("gm_tc_analysis", p.nside, p.lmax, self.spin, sp, self.ncomp, _lib.ptr(p.geom),
                       _lib.ptr(p.seeds), _lib.ptr(tp.coef[self.spin]), _lib.ptr(img),
@@ -195,11 +223,16 @@ class _Batch:
                 _lib.call("gm_ck_prep_syn", p.lmax, self.spin, sp, self.ncomp, _lib.ptr(self.alm_i),
                           _lib.ptr(tp.ck_choff[self.spin]), _lib.ptr(simg), simg_bytes, alm_scale,
                           _lib.stream_handle(p.device))
-                _lib.call("gm_ck_synthesis", p.nside, p.lmax, self.spin, sp, self.ncomp, _lib.ptr(p.geom),
+                mk = ck_masks(tp, self.spin, sp)
+                common = (p.nside, p.lmax, self.spin, sp, self.ncomp, _lib.ptr(p.geom),
                           _lib.ptr(tp.coef[self.spin]), _lib.ptr(tp.ck_segoff[self.spin]),
-                          _lib.ptr(ck[sp][0]), _lib.ptr(ck[sp][1]), _lib.ptr(simg),
-                          _lib.ptr(tp.ck_choff[self.spin]), _lib.ptr(out), 1.0 / alm_scale,
-                          _lib.ptr(tp.err), _lib.stream_handle(p.device))
+                          _lib.ptr(ck[sp][0]), _lib.ptr(ck[sp][1]))
+                rest = (_lib.ptr(simg), _lib.ptr(tp.ck_choff[self.spin]), _lib.ptr(out), 1.0 / alm_scale,
+                        _lib.ptr(tp.err), _lib.stream_handle(p.device))
+                if mk is not None:
+                    _lib.call("gm_ck_synthesis_masked", *common, _lib.ptr(mk[0]), *rest)
+                else:
+                    _lib.call("gm_ck_synthesis", *common, *rest)
                 continue
             _lib.call("gm_tc_prep_syn", p.lmax, self.spin, sp, self.ncomp, _lib.ptr(self.alm_i),
                       _lib.ptr(tp.choff[self.spin]), _lib.ptr(simg), simg_bytes, alm_scale,

@@ -375,6 +375,30 @@ int gm_ck_synthesis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp
                     const void *ck_state, const uint8_t *ck_shift, const void *simg,
                     const int64_t *choff, float *synd, double out_scale, int32_t *err,
                     void *stream);
+/* Lane-group masks of the checkpoint tables (nside <= 2048): bit g of seg_mask[seg] is set
+ * when some lane of the 64-lane group g has a non-zero stored state or shift at segment seg
+ * (a segment that starts from a zero state stays exactly zero); unit_mask[u] is the union
+ * over analysis unit u's two segments.  seg_mask has gm_ck_segments(lmax, spin) entries,
+ * unit_mask uoff[lmax + 1]; segoff and uoff are device copies of gm_ck_offsets' tables.
+ * Built once per geometry and row variant, beside the tables (the reference's march skips
+ * polar lanes whose rows stay below its emission threshold, march_v2.py:290-332, mlim). */
+int64_t gm_ck_segments(int64_t lmax, int spin);
+int gm_ck_masks(int64_t nside, int64_t lmax, int spin, const void *ck_state, const uint8_t *ck_shift,
+                const int64_t *segoff, const int64_t *uoff, uint64_t *seg_mask, uint64_t *unit_mask,
+                void *stream);
+/* gm_ck_analysis skipping the 64-lane groups of a unit whose rows are all zero, and
+ * gm_ck_synthesis skipping the segments in which all 256 lanes of a CTA's tile are zero:
+ * bit-identical results (the skipped products are exact zeros). */
+int gm_ck_analysis_masked(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                          const double *geom, const double *coef, const int64_t *segoff,
+                          const int64_t *uoff, const void *ck_state, const uint8_t *ck_shift,
+                          const uint64_t *unit_mask, const void *img, double *alm_i, double scale,
+                          int64_t nctas, int32_t *err, void *stream);
+int gm_ck_synthesis_masked(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
+                           const double *geom, const double *coef, const int64_t *segoff,
+                           const void *ck_state, const uint8_t *ck_shift, const uint64_t *seg_mask,
+                           const void *simg, const int64_t *choff, float *synd, double out_scale,
+                           int32_t *err, void *stream);
 /* Order windows of the batched transforms, for geometries whose full-size buffers do not
  * fit (Nside 4096 batches, Nside 8192): each entry handles the orders m in [mbeg, mend)
  * only, and its per-order buffers hold just those orders, indexed by m - mbeg (analysis

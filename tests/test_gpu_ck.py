@@ -129,3 +129,38 @@ def test_ck_matches_fp64_path_nside256(cuda, spin):
         sht_tc.USE_CHECKPOINTS = old
     assert _rel(got, ref) < TOL
     assert _rel(got, carried) < TOL
+
+
+@pytest.mark.parametrize("spin", [0, 2])
+def test_tile_skip_is_exact(cuda, spin):
+    """Skipping the 64-lane groups whose checkpoint states are all zero (the rows of such a
+    segment are exactly zero) leaves the batched transforms bit-identical; at Nside 512 about
+    a sixth of the analysis groups are skipped."""
+    nside, lmax = 512, 1535
+    rng = np.random.default_rng(31 + spin)
+    maps = torch.from_numpy(rng.normal(size=(8, 12 * nside ** 2))).cuda()
+    old = sht_tc.USE_TILE_SKIP
+    try:
+        sht_tc.USE_TILE_SKIP = False
+        full = sht_tc.map2alm_tc(maps, spin, nside, lmax, 3)
+        syn_full = sht_tc.alm2map_tc(full, spin, nside, lmax)
+        sht_tc.USE_TILE_SKIP = True
+        skip = sht_tc.map2alm_tc(maps, spin, nside, lmax, 3)
+        syn_skip = sht_tc.alm2map_tc(full, spin, nside, lmax)
+    finally:
+        sht_tc.USE_TILE_SKIP = old
+    assert torch.equal(full, skip)
+    assert torch.equal(syn_full, syn_skip)
+    tp = sht_tc.get_tc_plan(nside, lmax)
+    for sp, (seg_mask, unit_mask) in tp.ck_masks[spin].items():
+        ngroups = tp.plan.nlanes // 64
+        bits = (unit_mask.cpu().numpy().astype(np.uint64)[:, None] >> np.arange(ngroups, dtype=np.uint64)) & 1
+        zero = 1.0 - bits.mean()
+        assert 0.1 < zero < 0.3, (sp, zero)
+        # a group is marked active exactly when one of its lanes has a non-zero state
+        state, shift = sht_tc.ck_tables(tp, spin)[sp]
+        nseg = seg_mask.shape[0]
+        nz = ((state.view(nseg, -1, 2) != 0).any(dim=2) | (shift.view(nseg, -1) != 0))
+        want = nz.view(nseg, ngroups, 64).any(dim=2).cpu().numpy()
+        got = (seg_mask.cpu().numpy()[:, None].astype(np.uint64) >> np.arange(ngroups, dtype=np.uint64)) & 1
+        assert np.array_equal(got.astype(bool), want)
