@@ -102,9 +102,9 @@ SIGNATURES = {
     "gm_mask_apodize": ([_c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_dbl, _c_dbl, _c_int, _c_vp, _c_vp],
                         _c_int),
     "gm_legendre_analysis_ck": ([_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_dbl, _c_vp, _c_vp,
-                                 _c_vp, _c_vp, _c_vp, _c_int, _c_vp], _c_int),
+                                 _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_int, _c_vp], _c_int),
     "gm_legendre_synthesis_ck": ([_c_int, _c_i64, _c_i64, _c_i64, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
-                                  _c_vp, _c_vp, _c_int, _c_vp], _c_int),
+                                  _c_vp, _c_vp, _c_vp, _c_vp, _c_int, _c_vp], _c_int),
     "gm_ck_offsets": ([_c_i64, _c_int, _c_vp, _c_vp], _c_int),
     "gm_ck_table_entries": ([_c_i64, _c_i64, _c_int], _c_i64),
     "gm_ck_build": ([_c_i64, _c_i64, _c_int, _c_int, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp],

@@ -109,7 +109,7 @@ ffi::Error LegendreAnalysisCk(cudaStream_t s, ffi::AnyBuffer geom, ffi::AnyBuffe
                                                 rhs.untyped_data(), rptr<double>(alm), scale,
                                                 ptr<const int64_t>(segoff), ck_a.untyped_data(),
                                                 ptr<const uint8_t>(cn_a), ck_b.untyped_data(),
-                                                ptr<const uint8_t>(cn_b), tile, s));
+                                                ptr<const uint8_t>(cn_b), nullptr, nullptr, tile, s));
 }
 
 ffi::Error LegendreSynthesisCk(cudaStream_t s, ffi::AnyBuffer geom, ffi::AnyBuffer alm, ffi::AnyBuffer segoff,
@@ -121,7 +121,7 @@ ffi::Error LegendreSynthesisCk(cudaStream_t s, ffi::AnyBuffer geom, ffi::AnyBuff
                                                  ptr<const double>(alm), syn->untyped_data(),
                                                  ptr<const int64_t>(segoff), ck_a.untyped_data(),
                                                  ptr<const uint8_t>(cn_a), ck_b.untyped_data(),
-                                                 ptr<const uint8_t>(cn_b), tile, s));
+                                                 ptr<const uint8_t>(cn_b), nullptr, nullptr, tile, s));
 }
 
 // ------------------------------------------------------- Legendre stage (tensor cores)

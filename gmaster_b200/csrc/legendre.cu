@@ -95,8 +95,27 @@ struct CkTab {
     const int64_t *segoff;
     const float2 *ck[2];
     const uint8_t *cn[2];
+    // optional (NULL: every segment generated): per segment, bit g set when a lane of the
+    // 64-lane group g has a non-zero stored state (legendre_ck.cu:gm_ck_masks)
+    const unsigned long long *mask[2];
 };
 constexpr int kCkSeg = 128;
+
+// Whether some lane of this CTA (lanes [j0, j0 + nl)) has a non-zero state at segment seg
+// of either row variant: a CTA whose lanes all start the segment from zero gives exactly
+// zero rows for its 128 rows and skips them (the decision is uniform over the CTA).
+__device__ __forceinline__ bool ck_segment_active(const CkTab &tab, int nvar, int64_t seg, int64_t j0, int64_t nl,
+                                                  int64_t nlanes)
+{
+    if (!tab.mask[0] || nlanes > 4096) return true;
+    const int64_t j1 = (j0 + nl < nlanes ? j0 + nl : nlanes) - 1;
+    const int g0 = (int)(j0 >> 6), g1 = (int)(j1 >> 6);
+    const unsigned long long hi = g1 >= 63 ? ~0ull : ((1ull << (g1 + 1)) - 1ull);
+    const unsigned long long bits = hi & ~((1ull << g0) - 1ull);
+    unsigned long long mk = __ldg(tab.mask[0] + seg);
+    if (nvar > 1 && tab.mask[1]) mk |= __ldg(tab.mask[1] + seg);
+    return (mk & bits) != 0ull;
+}
 
 // Single-precision difference-form coefficients of row l (legendre_ck.cu): (c1, E for
 // s' = -s, E for s' = +s, b); a segment's first row is the restart step (0, 0, 0, 1).
@@ -235,6 +254,12 @@ __global__ void __launch_bounds__(kThreads) k_legendre_ana(
             }
     }
     for (int lb = l0; lb < L; lb += kWindow) {
+        if (CK && (lb - l0) % kCkSeg == 0 &&
+            !ck_segment_active(tab, NVAR, tab.segoff[m] + (lb - l0) / kCkSeg,
+                               (int64_t)blockIdx.x * kThreads * R, (int64_t)kThreads * R, nlanes)) {
+            lb += kCkSeg - kWindow;   // the segment's rows are zero on all lanes of this CTA
+            continue;
+        }
         if (threadIdx.x < kWindow) {
             const int l = lb + threadIdx.x;
             if (CK) fcoef[threadIdx.x] = ck_coef(l, m, sv, l0);
@@ -447,6 +472,15 @@ __global__ void __launch_bounds__(kThreads) k_legendre_syn(
 
     int buf = 0;
     for (int lb = l0; lb < L; lb += kWindow, buf ^= 1) {
+        if (CK && (lb - l0) % kCkSeg == 0 &&
+            !ck_segment_active(tab, NVAR, tab.segoff[m] + (lb - l0) / kCkSeg,
+                               (int64_t)blockIdx.x * kThreads * R, (int64_t)kThreads * R, nlanes)) {
+            // the segment's rows are zero on all lanes of this CTA; the next window that runs
+            // takes the other buffer, as it would have after this one
+            lb += kCkSeg - kWindow;
+            buf ^= 1;
+            continue;
+        }
         bool scaled = false;
         if (CK) {
             if ((lb - l0) % kCkSeg == 0) {
@@ -881,7 +915,7 @@ static int ck_args_ok(int spin, int64_t nside, int64_t lmax, int64_t ncomp, int 
 }
 
 static CkTab ck_tab(const int64_t *segoff, const void *ck_a, const uint8_t *cn_a, const void *ck_b,
-                    const uint8_t *cn_b)
+                    const uint8_t *cn_b, const uint64_t *mask_a, const uint64_t *mask_b)
 {
     CkTab t;
     t.segoff = segoff;
@@ -889,6 +923,10 @@ static CkTab ck_tab(const int64_t *segoff, const void *ck_a, const uint8_t *cn_a
     t.cn[0] = cn_a;
     t.ck[1] = (const float2 *)ck_b;
     t.cn[1] = cn_b;
+    // both variants' masks or neither
+    const bool masked = mask_a && (mask_b || ck_b == nullptr);
+    t.mask[0] = masked ? (const unsigned long long *)mask_a : nullptr;
+    t.mask[1] = masked ? (const unsigned long long *)mask_b : nullptr;
     return t;
 }
 
@@ -896,13 +934,13 @@ extern "C" int gm_legendre_analysis_ck(int spin, int64_t nside, int64_t lmax, in
                                        const double *lane_geom, const void *rhs, double *alm,
                                        double scale, const int64_t *segoff, const void *ck_a,
                                        const uint8_t *cn_a, const void *ck_b, const uint8_t *cn_b,
-                                       int tile, void *stream)
+                                       const uint64_t *mask_a, const uint64_t *mask_b, int tile, void *stream)
 {
     const int st = ck_args_ok(spin, nside, lmax, ncomp, tile);
     if (st != GM_OK) return st;
     if (!lane_geom || !rhs || !alm || !segoff || !ck_a || !cn_a || (spin == 2 && (!ck_b || !cn_b)))
         return GM_ERR_BAD_PTR;
-    const CkTab tab = ck_tab(segoff, ck_a, cn_a, ck_b, cn_b);
+    const CkTab tab = ck_tab(segoff, ck_a, cn_a, spin == 2 ? ck_b : nullptr, cn_b, mask_a, spin == 2 ? mask_b : nullptr);
     cudaStream_t s = as_stream(stream);
     return tile < 0 ? dispatch_ana<float>(spin, nside, lmax, ncomp, lane_geom, nullptr, rhs, alm, scale, s, &tab)
                     : tile_ana<float>(spin, tile, nside, lmax, ncomp, lane_geom, nullptr, rhs, alm, scale, s, &tab);
@@ -911,13 +949,14 @@ extern "C" int gm_legendre_analysis_ck(int spin, int64_t nside, int64_t lmax, in
 extern "C" int gm_legendre_synthesis_ck(int spin, int64_t nside, int64_t lmax, int64_t ncomp,
                                         const double *lane_geom, const double *alm, void *syn,
                                         const int64_t *segoff, const void *ck_a, const uint8_t *cn_a,
-                                        const void *ck_b, const uint8_t *cn_b, int tile, void *stream)
+                                        const void *ck_b, const uint8_t *cn_b, const uint64_t *mask_a,
+                                        const uint64_t *mask_b, int tile, void *stream)
 {
     const int st = ck_args_ok(spin, nside, lmax, ncomp, tile);
     if (st != GM_OK) return st;
     if (!lane_geom || !alm || !syn || !segoff || !ck_a || !cn_a || (spin == 2 && (!ck_b || !cn_b)))
         return GM_ERR_BAD_PTR;
-    const CkTab tab = ck_tab(segoff, ck_a, cn_a, ck_b, cn_b);
+    const CkTab tab = ck_tab(segoff, ck_a, cn_a, spin == 2 ? ck_b : nullptr, cn_b, mask_a, spin == 2 ? mask_b : nullptr);
     cudaStream_t s = as_stream(stream);
     return tile < 0 ? dispatch_syn<float>(spin, nside, lmax, ncomp, lane_geom, nullptr, alm, syn, s, &tab)
                     : tile_syn<float>(spin, tile, nside, lmax, ncomp, lane_geom, nullptr, alm, syn, s, &tab);

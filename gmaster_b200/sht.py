@@ -266,7 +266,8 @@ def pack_rhs(plan, spec, prec):
 
 
 def ck_args(plan, spin, prec):
-    """Checkpoint-table arguments (segoff, state and shift of the s' = -s and +s variants)
+    """Checkpoint-table arguments (segoff, state and shift of the s' = -s and +s variants,
+    their lane-group masks or None)
     of the mixed-precision spin-0 / spin-2 Legendre kernels, whose rows then come from the
     single-precision difference form restarted every 128 rows (legendre_ck.cu); None for
     FP64, other spins, checkpoints switched off, or tables larger than their memory share
@@ -283,9 +284,11 @@ def ck_args(plan, spin, prec):
     tabs = sht_tc.ck_tables(tp, spin)
     if tabs is None:
         return None
-    a = tabs[0] if spin == 0 else tabs[-2]
-    b = tabs[0] if spin == 0 else tabs[2]
-    return (_lib.ptr(tp.ck_segoff[spin]), _lib.ptr(a[0]), _lib.ptr(a[1]), _lib.ptr(b[0]), _lib.ptr(b[1]))
+    sa, sb = (0, 0) if spin == 0 else (-2, 2)
+    a, b = tabs[sa], tabs[sb]
+    ma, mb = sht_tc.ck_masks(tp, spin, sa), sht_tc.ck_masks(tp, spin, sb)
+    masks = (_lib.ptr(ma[0]), _lib.ptr(mb[0])) if ma is not None and mb is not None else (None, None)
+    return (_lib.ptr(tp.ck_segoff[spin]), _lib.ptr(a[0]), _lib.ptr(a[1]), _lib.ptr(b[0]), _lib.ptr(b[1])) + masks
 
 
 def run_legendre(plan, spin, ncomp, prec, kind, tile, src, dst, scale=1.0, ck=None):

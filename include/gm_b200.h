@@ -325,15 +325,19 @@ int gm_tc_synd_to_syn(int64_t nside, int64_t lmax, int spin, int64_t ncomp, cons
  * with the rows of the checkpoint tables below instead of the FP64 recurrence: the
  * single-precision difference form restarted every 128 rows (same reference interface,
  * march_v2.cu:155-407).  ck_a/cn_a: table of s' = 0 (spin 0) or -2; ck_b/cn_b: s' = +2
- * (ignored for spin 0); segoff: device offsets of gm_ck_offsets. */
+ * (ignored for spin 0); segoff: device offsets of gm_ck_offsets.  mask_a / mask_b: NULL, or
+ * the per-segment lane-group masks of the two tables (gm_ck_masks' seg_mask; mask_b ignored
+ * for spin 0): a CTA whose lanes all start a segment from zero skips its 128 rows (exact). */
 int gm_legendre_analysis_ck(int spin, int64_t nside, int64_t lmax, int64_t ncomp,
                             const double *lane_geom, const void *rhs, double *alm, double scale,
                             const int64_t *segoff, const void *ck_a, const uint8_t *cn_a,
-                            const void *ck_b, const uint8_t *cn_b, int tile, void *stream);
+                            const void *ck_b, const uint8_t *cn_b, const uint64_t *mask_a,
+                            const uint64_t *mask_b, int tile, void *stream);
 int gm_legendre_synthesis_ck(int spin, int64_t nside, int64_t lmax, int64_t ncomp,
                              const double *lane_geom, const double *alm, void *syn,
                              const int64_t *segoff, const void *ck_a, const uint8_t *cn_a,
-                             const void *ck_b, const uint8_t *cn_b, int tile, void *stream);
+                             const void *ck_b, const uint8_t *cn_b, const uint64_t *mask_a,
+                             const uint64_t *mask_b, int tile, void *stream);
 
 /* ---- checkpointed batched Legendre contraction (replaces march_v2.cu:155-407 for batched
  * maps; the reference's window tables march_v2.py:388-450 are its per-geometry constants).

@@ -164,3 +164,27 @@ def test_tile_skip_is_exact(cuda, spin):
         want = nz.view(nseg, ngroups, 64).any(dim=2).cpu().numpy()
         got = (seg_mask.cpu().numpy()[:, None].astype(np.uint64) >> np.arange(ngroups, dtype=np.uint64)) & 1
         assert np.array_equal(got.astype(bool), want)
+
+
+@pytest.mark.parametrize("spin", [0, 2])
+def test_simt_segment_skip_is_exact(cuda, spin):
+    """The one-field SIMT passes skip the 128-row segments in which every lane of a CTA
+    starts from a zero state.  The synthesis stays bit-identical; the analysis adds the same
+    values, but its lane blocks add into each alm element with FP64 atomics in no fixed
+    order, so it agrees to the rounding of those sums."""
+    nside, lmax = 512, 1535
+    rng = np.random.default_rng(41 + spin)
+    maps = torch.from_numpy(rng.normal(size=(2, 12 * nside ** 2))).cuda()
+    old = sht_tc.USE_TILE_SKIP
+    try:
+        sht_tc.USE_TILE_SKIP = False
+        a_full = sht.map2alm_device(maps, spin, nside, lmax, 3, "mixed")
+        m_full = sht.alm2map_device(a_full, spin, nside, lmax, "mixed")
+        sht_tc.USE_TILE_SKIP = True
+        assert sht.ck_args(sht.get_plan(nside, lmax), spin, 1)[-1] is not None
+        a_skip = sht.map2alm_device(maps, spin, nside, lmax, 3, "mixed")
+        m_skip = sht.alm2map_device(a_full, spin, nside, lmax, "mixed")
+    finally:
+        sht_tc.USE_TILE_SKIP = old
+    assert float((a_full - a_skip).abs().max() / a_full.abs().max()) < 1e-13
+    assert torch.equal(m_full, m_skip)
