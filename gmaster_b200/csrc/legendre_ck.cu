@@ -16,7 +16,7 @@
 //     (8 warps, twice the latency hiding of a single carried recurrence), and its work units
 //     (order m, superblock) are independent, so the CTAs that run the superblocks of one
 //     order at the same time share that order's right-hand-side images through L2 and each
-//     alm element is written by exactly one unit (no atomics);
+//     alm element receives exactly one addition per launch, from one unit;
 //   * the synthesis runs two sets of 8 generator warps on alternate segments.
 // A checkpoint stores the pre-state (v_{l_s - 1}, D_{l_s}) of the segment's first row l_s,
 // so that row is the uniform step with coefficients (c1, E, b) = (0, 0, 1).  The state is
@@ -515,17 +515,51 @@ __global__ void __launch_bounds__(kThrA, 1) k_ana_ck(CkParams p, const uint8_t *
                 __syncwarp();
                 if (lane == 0) tc::mbar_arrive(&sh.b_full[S]);
             }
-            // epilogue of the unit.  The two hemisphere halves of the image rows may add into
-            // the same alm row (spin 0), so the accumulators are staged in shared memory (the
-            // tiles and coefficient rows, free now) and each alm element then receives
-            // exactly one addition per launch, from one thread: the result does not depend
-            // on the order of the units.  Warp w reads TMEM lanes 32 (w % 4), superblock
-            // rows 128 (w / 4) + [0, 128).
+            // epilogue of the unit: each alm element receives exactly one addition per launch,
+            // from one thread, so the result does not depend on the order of the units.  Warp
+            // w reads TMEM lanes 32 (w % 4), superblock rows 128 (w / 4) + [0, 128).
             const uint32_t q = (uint32_t)((u - c) / G);
             if (!dead && !warp_wait(&sh.d_full, q & 1, abort, err)) dead = true;
-            float *stage = reinterpret_cast<float *>(sB);   // [128 rows][kStageLd] floats
             // a unit without active groups adds nothing (its accumulator was never written)
             const bool out = !dead && umask != 0ull;
+            if (SPIN == 2 && 2 * p.H >= 64) {
+                // spin 2: the north image rows r < H feed alm rows o0 + r and the south rows
+                // H + r' feed rows o1 + r' (o0 != o1, so no row receives both): each thread adds
+                // its TMEM lane straight into the alm rows, one 256-byte row segment per warp
+                // (with fewer than 64 image rows the staged path below spreads the additions
+                // over all the worker threads instead)
+                if (out) {
+                    tc::tc_fence_after();
+                    const int r = 32 * (warp & 3) + lane, c0 = 128 * (warp >> 2);
+                    const bool north = r < p.H, valid = r < 2 * p.H;
+                    const int orow = north ? p.o0 + r : p.o1 + (r - p.H);
+                    double *dst = alm_i + (mb + lb) * p.NR + orow;
+                    for (int cb = c0; cb < c0 + 128; cb += 16) {
+                        uint32_t rh[16], rx[16];
+                        const uint32_t ta = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)cb;
+                        tc::tmem_ld16(ta, rh);
+                        tc::tmem_ld16(ta + kSB, rx);
+                        tc::tmem_ld_wait();
+#pragma unroll
+                        for (int e = 0; e < 16; ++e) {
+                            const int i = cb + e;
+                            if (valid && lb + i < L) {
+                                double val = (double)(__uint_as_float(rh[e]) + __uint_as_float(rx[e]));
+                                if (!north && ((lb + i + m) & 1)) val = -val;
+                                atomicAdd(dst + (int64_t)i * p.NR, val * p.scale);
+                            }
+                        }
+                    }
+                    tc::tc_fence_before();
+                }
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(&sh.d_free);   // TMEM may be overwritten
+                continue;
+            }
+            // spin 0: the two hemisphere halves of the image rows add into the same alm rows,
+            // so the accumulators are staged in shared memory (the tiles and coefficient rows,
+            // free now) and each element is then summed by one thread
+            float *stage = reinterpret_cast<float *>(sB);   // [128 rows][kStageLd] floats
             if (out) {
                 tc::tc_fence_after();
                 const int row = 32 * (warp & 3) + lane, c0 = 128 * (warp >> 2);
