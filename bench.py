@@ -52,24 +52,64 @@ KERNEL_OF_CARRIED = {"tc_analysis_s2": "k_ana_tc<2>", "tc_analysis_s0": "k_ana_t
 # + dram__bytes_write.sum) for the spin-2 launch of 8 fields at Nside 512, 1.029 x the byte
 # model below (operand images read once, alm accumulator read and written once, checkpoint
 # states read once); the launch at the benchmark size is given as that model x 1.029.
-CK_TRAFFIC_RATIO = 1.545 / 1.501
+# DRAM bytes ncu measured for one k_ana_ck<2> launch (row variant s' = -2) at Nside 512 with
+# 8 fields (1.061 GB read + 0.293 GB written), over the byte model below evaluated on the
+# same launch's unit masks (1.3298 GB)
+CK_TRAFFIC_RATIO = 1.354e9 / 1.3298e9
 
 
-def ck_analysis_bytes(nside, lmax, nrows):
-    """Byte model of one checkpointed analysis launch (one row variant): 64 KB operand image
-    per (order, 128-lane group), nrows FP64 alm rows read and written, 9 B checkpoint state
-    per (128-row segment, lane)."""
+def ck_unit_activity(nside, lmax, spin=2, sp=-2):
+    """(active 64-lane groups per analysis unit, unit offsets per order) of the row variant,
+    from the zero-group masks the geometry's checkpoint tables were built with; None when
+    the masks do not exist."""
+    from gmaster_b200 import sht_tc
+    tp = sht_tc.get_tc_plan(nside, lmax)
+    mk = sht_tc.ck_masks(tp, spin, sp)
+    if mk is None:
+        return None
+    um = mk[1].cpu().numpy().view(np.uint64)
+    return um, tp.ck_uoff[spin].cpu().numpy()
+
+
+def ck_analysis_bytes(nside, lmax, nrows, activity=None):
+    """Byte model of one checkpointed analysis launch (one row variant).  Without masks: a 64 KB
+    operand image per (order, 128-lane group), nrows FP64 alm rows read and written, 9 B
+    checkpoint state per (128-row segment, lane).  With the unit masks (`ck_unit_activity`):
+    32 KB per (order, 64-lane group) active in some unit of the order, the alm rows of the
+    units with an active group, and the states of the active (unit, group) pairs."""
     L, nlanes = lmax + 1, 2 * nside
     groups = (nlanes + 127) // 128
-    nelem = L * (L + 1) // 2
-    segs = sum((L - max(m, 2) + 127) // 128 for m in range(L))
-    return L * groups * 65536 + 2 * nelem * nrows * 8 + segs * nlanes * 9
+    if activity is None:
+        nelem = L * (L + 1) // 2
+        segs = sum((L - max(m, 2) + 127) // 128 for m in range(L))
+        return L * groups * 65536 + 2 * nelem * nrows * 8 + segs * nlanes * 9
+    um, uoff = activity
+    per_order = np.bitwise_or.reduceat(um, uoff[:-1].astype(np.int64))
+    img = int(np.bitwise_count(per_order).sum()) * 32768
+    first = np.maximum(np.arange(L), 2)
+    rows = 0
+    for m in range(L):
+        n_m = int(uoff[m + 1] - uoff[m])
+        live = um[uoff[m]:uoff[m + 1]] != 0
+        full = np.minimum(256, L - first[m] - 256 * np.arange(n_m))
+        rows += int(full[live].sum())
+    states = int(np.bitwise_count(um).sum()) * 64 * 2 * 9
+    return img + 2 * rows * nrows * 8 + states
 
 
-def traffic_per_launch(kernel, nside, lmax, sims):
+def ck_issued_flops(activity, nrows_mma=128):
+    """Tensor-pipe flops one k_ana_ck launch issues: three f16 products of M = 128, N = 256,
+    K = 64 per active (unit, 64-lane group)."""
+    um, _ = activity
+    return 3 * 2 * nrows_mma * 256 * 64 * int(np.bitwise_count(um).sum())
+
+
+def traffic_per_launch(kernel, nside, lmax, sims, activity=None):
+    """(model bytes, DRAM bytes scaled by the measured ratio) of one launch, or (None, None)."""
     if kernel == "k_ana_ck<2>":
-        return CK_TRAFFIC_RATIO * ck_analysis_bytes(nside, lmax, 4 * sims)
-    return None
+        model = ck_analysis_bytes(nside, lmax, 4 * sims, activity)
+        return model, CK_TRAFFIC_RATIO * model
+    return None, None
 
 
 def parse():
@@ -1325,6 +1365,14 @@ def main():
     dom_launches = kcount[dominant] * per_pass
     dom_avg_ms = ktime[dominant] / dom_launches
     dom_tflops = kflops[dominant] / (ktime[dominant] / 1e3) / 1e12
+    dom_kernel = kernel_of.get(dominant, dominant)
+    activity = ck_unit_activity(nside, lmax) if dom_kernel == "k_ana_ck<2>" else None
+    traffic = traffic_per_launch(dom_kernel, nside, lmax, S, activity)
+    if activity is not None:
+        issued_tflops = ck_issued_flops(activity) / (dom_avg_ms / 1e3) / 1e12
+        active_frac = float(np.bitwise_count(activity[0]).sum()) / (len(activity[0]) * ((2 * nside + 63) // 64))
+    else:
+        issued_tflops, active_frac = 3 * dom_tflops, 1.0
     line = {
         "metric": METRIC, "value": value, "unit": "sims/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -1342,17 +1390,22 @@ def main():
         "e2e": {"value": value_e2e, "unit": "sims/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h[0]), "pinned": pinned},
         "roofline": {
-            "bound": "tensor", "kernel": kernel_of.get(dominant, dominant),
+            "bound": "tensor", "kernel": dom_kernel,
             "achieved": dom_tflops, "peak": peak, "unit": "TFLOP/s",
             "frac": dom_tflops / peak,
-            "traffic": traffic_per_launch(kernel_of.get(dominant, dominant), nside, lmax, S),
+            "traffic": traffic[1],
+            "traffic_model_bytes": traffic[0],
             "note": "algorithmic flops per launch (one complex MAC = 4 flops per (l, m, lane) and "
-                    "map; the f16x3 split issues 3x these on the tensor pipe) / CUDA-event time "
-                    "of the launch; peak = measured sustained bf16 dense (MEASURED_PEAKS.json); traffic = "
-                    "DRAM bytes read + written per launch: ncu measured 1.029x the launch's byte "
-                    "model at Nside 512 (8 fields); the model scaled to this workload x 1.029",
+                    "map, every (l, m, lane) counted) / CUDA-event time of the launch; the kernel "
+                    "skips the 64-lane groups whose rows are exactly zero and issues three f16 "
+                    "products per active group (tensor_pipe_tflops_issued); peak = measured "
+                    "sustained bf16 dense (MEASURED_PEAKS.json); traffic = DRAM bytes read + "
+                    f"written per launch: ncu measured {CK_TRAFFIC_RATIO:.3f}x the launch's "
+                    "mask-aware byte model at Nside 512 (8 fields); the model of this workload "
+                    f"x {CK_TRAFFIC_RATIO:.3f}",
             "launches": dom_launches, "avg_ms": dom_avg_ms,
-            "tensor_pipe_tflops_issued": 3 * dom_tflops,
+            "tensor_pipe_tflops_issued": issued_tflops,
+            "active_group_fraction": active_frac,
         },
         "legendre_share_of_step": leg_ms / ms,
         "legendre_tflops": leg_flops / (leg_ms / 1e3) / 1e12,
