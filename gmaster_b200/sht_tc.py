@@ -23,6 +23,8 @@ MAX_FIELDS_SPIN2 = 32
 # at most this share of the device memory, else the carried-state kernels run.
 USE_CHECKPOINTS = True
 CK_MEMORY_SHARE = 0.2
+# lanes (2 Nside) of the largest geometry with checkpoint tables: 64 groups of 64 lanes
+CK_MAX_LANES = 4096
 # Skip the 64-lane groups whose checkpoint states are all zero (exact: their rows are zero);
 # False runs every group, for comparisons.
 USE_TILE_SKIP = True
@@ -99,11 +101,15 @@ def ck_table_bytes(tp, spin):
 
 def ck_tables(tp, spin):
     """{s': (state, shift)} checkpoint tables of the row variants of `spin`, built on the
-    first call and kept with the plan; None when checkpoints are switched off or the
-    tables of the geometry would take more than CK_MEMORY_SHARE of the device memory."""
+    first call and kept with the plan; None when checkpoints are switched off, the geometry
+    has more than CK_MAX_LANES lanes (the checkpointed analysis walks a unit's lane groups as
+    one 64-bit word) or its tables would take more than CK_MEMORY_SHARE of the device
+    memory.  Without tables the transforms take the carried-recurrence kernels."""
     if not USE_CHECKPOINTS:
         return None
     p = tp.plan
+    if p.nlanes > CK_MAX_LANES:
+        return None
     with _LOCK:
         have = tp.ck.get(spin)
         if have is not None:

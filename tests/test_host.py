@@ -142,6 +142,24 @@ def test_compute_without_gpu_fails_loudly():
         _lib.require_cuda()
 
 
+def test_checkpointed_analysis_lane_limit():
+    """The checkpointed analysis walks a unit's 64-lane groups as one 64-bit word: above 4096
+    lanes the entry point refuses the shape (before any device work) and the transforms keep
+    to the carried-recurrence kernels (no checkpoint tables)."""
+    from types import SimpleNamespace
+
+    from gmaster_b200 import _lib, sht_tc
+
+    lib = _lib.load()
+    bad_shape = [k for k, v in _lib.STATUS.items() if v == "GM_ERR_BAD_SHAPE"][0]
+    null = [None] * 6
+    for nside, want_shape in ((2048, False), (2049, True), (3000, True)):
+        st = lib.gm_ck_analysis(nside, 3 * nside - 1, 2, -2, 4, *null, None, None, 1.0, 148, None, None)
+        assert (st == bad_shape) == want_shape, (nside, st)
+    tp = SimpleNamespace(plan=SimpleNamespace(nlanes=sht_tc.CK_MAX_LANES + 2), ck={})
+    assert sht_tc.CK_MAX_LANES == 4096 and sht_tc.ck_tables(tp, 2) is None
+
+
 def test_legendre_tile_list():
     """The autotuner's tile shapes are listed by the library without a GPU."""
     from gmaster_b200 import autotune
