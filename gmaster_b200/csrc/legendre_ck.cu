@@ -929,8 +929,9 @@ static int ck_analysis(int64_t nside, int64_t lmax, int spin, int sp, int64_t nc
                        const uint8_t *ck_shift, const uint64_t *unit_mask, const void *img, double *alm_i,
                        double scale, int64_t nctas, int32_t *err, void *stream)
 {
-    if (nside < 1 || lmax < 2 || lmax > 65535 || !ck_shape_ok(spin, ncomp) || !ck_spin_ok(spin, sp) ||
-        nctas < 1 || nctas > 4096)
+    // the lane groups of a unit are walked as the bits of one 64-bit word: 64 x kKG lanes
+    if (nside < 1 || 2 * nside > 64 * kKG || lmax < 2 || lmax > 65535 || !ck_shape_ok(spin, ncomp) ||
+        !ck_spin_ok(spin, sp) || nctas < 1 || nctas > 4096)
         return GM_ERR_BAD_SHAPE;
     if (!geom || !coef || !segoff || !uoff || !ck_state || !ck_shift || !img || !alm_i || !err)
         return GM_ERR_BAD_PTR;
