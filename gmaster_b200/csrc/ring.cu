@@ -322,9 +322,10 @@ __device__ __forceinline__ void ring_outputs(const T2 *__restrict__ Z, int n, in
     }
 }
 
-// One CTA per (ring, map component): mixed-radix Stockham FFT in shared memory.  In single
-// precision the rings of the Bluestein path (use_bluestein with `mcap` > 0) are left to
-// k_ring_analysis_bluestein.
+// One CTA per (map component, ring), the component the fast grid index so that the CTAs of
+// one ring run together and read its mask once from DRAM: mixed-radix Stockham FFT in
+// shared memory.  In single precision the rings of the Bluestein path (use_bluestein with
+// `mcap` > 0) are left to k_ring_analysis_bluestein.
 template <typename T, typename Tin>
 __global__ void __launch_bounds__(512) k_ring_analysis(int64_t nside, int64_t L,
                                                        const Tin *__restrict__ maps,
@@ -337,7 +338,7 @@ __global__ void __launch_bounds__(512) k_ring_analysis(int64_t nside, int64_t L,
 {
     using T2 = typename vec2<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int64_t r = blockIdx.x, c = blockIdx.y;
+    const int64_t r = blockIdx.y, c = blockIdx.x;
     const int64_t nring = 4 * nside - 1, npix = 12 * nside * nside;
     const int n = (int)ring_nphi(nside, r), h = n / 2;
     if (mcap > 0 && use_bluestein(h, mcap)) return;
@@ -354,7 +355,8 @@ __global__ void __launch_bounds__(512) k_ring_analysis(int64_t nside, int64_t L,
                     out + (c * nring + r) * L);
 }
 
-// Bluestein path, single precision: one CTA per (ring, block of `cpc` components).
+// Bluestein path, single precision: one CTA per (block of `cpc` components, ring), the
+// component block the fast grid index.
 //   X_k = sum_j z_j omega_h^{jk} = c_k sum_j (z_j c_j) conj(c_{k-j}),  c_j = e^{-i pi j^2 / h}
 // evaluated as a circular convolution of length M: the transform of the wrapped conjugate
 // chirp once per CTA, then per component one forward and one inverse FFT.  The chirp is
@@ -372,7 +374,7 @@ __global__ void __launch_bounds__(512) k_ring_analysis_bluestein(int64_t nside, 
 {
     using T2 = float2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int64_t r = blockIdx.x;
+    const int64_t r = blockIdx.y;
     const int n = (int)ring_nphi(nside, r), h = n / 2;
     if (!use_bluestein(h, mcap) || ring_big(h, hcap, (int)nside, bsmin)) return;
     const int M = next_pow2(2 * h - 1);
@@ -401,8 +403,8 @@ __global__ void __launch_bounds__(512) k_ring_analysis_bluestein(int64_t nside, 
     const float invM = 1.0f / (float)M;
     const bool sh = shifted[r] != 0;
     const float w = (float)(4.0 * M_PI / (double)npix);
-    const int64_t c1 = (int64_t)(blockIdx.y + 1) * cpc < ncomp ? (int64_t)(blockIdx.y + 1) * cpc : ncomp;
-    for (int64_t c = (int64_t)blockIdx.y * cpc; c < c1; ++c) {
+    const int64_t c1 = (int64_t)(blockIdx.x + 1) * cpc < ncomp ? (int64_t)(blockIdx.x + 1) * cpc : ncomp;
+    for (int64_t c = (int64_t)blockIdx.x * cpc; c < c1; ++c) {
         for (int j = h + threadIdx.x; j < M; j += blockDim.x) X[j] = make_float2(0.f, 0.f);
         load_ring<float>(maps + c * npix + off, mask ? mask + off : nullptr, h, X,
                          [&](int t, T2 z) { return cmul(z, chirp(t)); });
@@ -883,7 +885,7 @@ extern "C" int gm_ring_analysis_ws(int precision, int64_t nside, int64_t L, int6
     const size_t smem = 2 * (size_t)hcap * (precision == GM_FP64 ? sizeof(double2) : sizeof(float2));
     const int64_t slot = gm_ring_big_scratch_bytes(nside, 1);
     int threads = nside >= 256 ? 512 : 128;
-    dim3 grid((unsigned)nring, (unsigned)ncomp);
+    dim3 grid((unsigned)ncomp, (unsigned)nring);
     cudaStream_t s = as_stream(stream);
     int st;
     if (precision == GM_FP64) {
@@ -909,7 +911,7 @@ extern "C" int gm_ring_analysis_ws(int precision, int64_t nside, int64_t L, int6
         const int mcap = bluestein_mcap(nside);
         const size_t bs_smem = 3 * (size_t)mcap * sizeof(float2);
         const int cpc = 8;
-        dim3 bs_grid((unsigned)nring, (unsigned)((ncomp + cpc - 1) / cpc));
+        dim3 bs_grid((unsigned)((ncomp + cpc - 1) / cpc), (unsigned)nring);
         const unsigned gbig = (unsigned)(nslots < nring ? nslots : nring);
         if (map_dtype_bytes == 8) {
             if ((st = set_smem(k_ring_analysis<float, double>, smem))) return st;
