@@ -12,8 +12,8 @@
 // FP64 is kept for the checkpoint states, the seeds and the alm accumulation.
 //
 // Because every 128-row segment starts from the table, segments are independent:
-//   * the analysis splits each 256-row superblock between two sets of 4 generator warps
-//     (8 warps, twice the latency hiding of a single carried recurrence), and its work units
+//   * the analysis generates each 256-row superblock with one warp per 128-row segment and
+//     32-lane group, four such warp pairs taking the groups in turn, and its work units
 //     (order m, superblock) are independent, so the CTAs that run the superblocks of one
 //     order at the same time share that order's right-hand-side images through L2 and each
 //     alm element receives exactly one addition per launch, from one unit;
@@ -55,17 +55,20 @@ constexpr int kMaxShift = 5;                        // largest stored shift n (2
 constexpr int kSB = 2 * kSeg;                       // superblock rows (one unit; MMA N)
 constexpr int kHalf = 64;                           // rows per generation step
 constexpr int kKC = 128;                            // lanes per operand image (global layout)
-constexpr int kKG = 64;                             // lanes per analysis group (MMA K per group)
-constexpr int kGenA = 256;                          // generator threads (8 warps, 2 sets of 4)
+constexpr int kKG = 32;                             // lanes per analysis group (MMA K per group)
+constexpr int kSetsA = 4;                           // generator sets (2 warps each, one tile each)
+constexpr int kImgBufA = 4;                         // image buffers
+constexpr int kMaxGroupsA = 128;                    // lane groups of a unit (two 64-bit words)
+constexpr int kGenA = 256;                          // generator threads (8 warps)
 constexpr int kMmaWarpA = kGenA / 32;
 constexpr int kLoadWarpA = kMmaWarpA + 1;
 constexpr int kThrA = kGenA + 64;                   // + the MMA warp and the image loader warp
 constexpr uint32_t kAImg = 128u * kKC * 2u;         // one plane of a right-hand-side image (32 KB)
-constexpr uint32_t kAImgG = 2u * 128u * kKG * 2u;   // a group's hi and lo image planes (32 KB)
-constexpr uint32_t kTileA = 2u * kSB * kKG * 2u;    // tile: 256 rows x 64 lanes, hi + lo (64 KB)
+constexpr uint32_t kAImgG = 2u * 128u * kKG * 2u;   // a group's hi and lo image planes (16 KB)
+constexpr uint32_t kTileA = 2u * kSB * kKG * 2u;    // tile: 256 rows x 32 lanes, hi + lo (32 KB)
 constexpr int kStageLd = kSB + 1;                   // epilogue staging row stride (floats)
 // the epilogue stages 128 rows x kStageLd floats in the tiles and coefficient rows
-static_assert(128 * kStageLd * 4 <= 2 * kTileA + kSB * 16, "epilogue staging does not fit");
+static_assert(128 * kStageLd * 4 <= kSetsA * kTileA + kSB * 16, "epilogue staging does not fit");
 // synthesis
 constexpr int kLT = 256;                            // lanes per CTA (MMA N)
 constexpr int kKL = 64;                             // rows per chunk (MMA K)
@@ -107,6 +110,47 @@ __device__ __forceinline__ int pop_group(unsigned long long &r)
     const int g = __ffsll((long long)r) - 1;
     r &= r - 1ull;
     return g;
+}
+
+// A set of up to 128 lane groups (bit g of word g / 64).
+struct GroupSet {
+    unsigned long long w0, w1;
+};
+
+__device__ __forceinline__ int pop_group(GroupSet &r)
+{
+    const int g = pop_group(r.w0);
+    if (g >= 0) return g;
+    const int h = pop_group(r.w1);
+    return h >= 0 ? 64 + h : -1;
+}
+
+// Bit i of the low 32 bits of x to bits 2i and 2i + 1.
+__device__ __forceinline__ unsigned long long spread_pairs(unsigned long long x)
+{
+    x &= 0xffffffffull;
+    x = (x | (x << 16)) & 0x0000ffff0000ffffull;
+    x = (x | (x << 8)) & 0x00ff00ff00ff00ffull;
+    x = (x | (x << 4)) & 0x0f0f0f0f0f0f0f0full;
+    x = (x | (x << 2)) & 0x3333333333333333ull;
+    x = (x | (x << 1)) & 0x5555555555555555ull;
+    return x | (x << 1);
+}
+
+// Active 32-lane groups of analysis unit u: both halves of every 64-lane group whose mask
+// bit is set (all `ngroups` groups without masks).
+__device__ __forceinline__ GroupSet unit_groups(const unsigned long long *__restrict__ unit_mask, int64_t u,
+                                                int64_t ngroups)
+{
+    GroupSet r;
+    r.w0 = all_groups(ngroups);
+    r.w1 = ngroups > 64 ? all_groups(ngroups - 64) : 0ull;
+    if (unit_mask) {
+        const unsigned long long mk = __ldg(unit_mask + u);
+        r.w0 &= spread_pairs(mk);
+        r.w1 &= spread_pairs(mk >> 32);
+    }
+    return r;
 }
 
 __host__ __device__ __forceinline__ int64_t first_row(int64_t m, int sp)
@@ -276,7 +320,7 @@ __global__ void __launch_bounds__(256) k_ck_seg_mask(int64_t nlanes, int64_t nse
 // ------------------------------------------------------------------------------- analysis
 
 struct __align__(8) AnaShared {
-    uint64_t a_full[2], a_free[2], b_full[2], b_free[2], d_full, d_free, drain;
+    uint64_t a_full[kImgBufA], a_free[kImgBufA], b_full[kSetsA], b_free[kSetsA], d_full, d_free, drain;
     uint32_t tmem;
     int abort;
 };
@@ -312,11 +356,14 @@ __global__ void k_ck_unit_mask(int64_t L, const int64_t *__restrict__ segoff, co
 __device__ __forceinline__ void gen_barrier_a() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 
 // Units (m, s): superblock s of order m covers rows l0 + 256 s + [0, 256).  CTA c takes
-// units c, c + G, ...  Within a unit the lanes run in groups g of 64 (half of a 128-lane
-// operand image); a group's image (hi and lo planes, 32 KB) goes into one of two buffers
-// that a loader warp refills while the other group's MMAs run.  Set S (four warps) fills
-// the tile of the groups with g % 2 == S: all 256 rows of the superblock for the group's
-// 64 lanes, each thread one segment (128 rows) of one lane, f16 hi and lo planes.  Per K
+// units c, c + G, ...  Within a unit the lanes run in groups of 32 (a quarter of a 128-lane
+// operand image); a group's image (hi and lo planes, 16 KB) goes into one of four buffers
+// that a loader warp refills while the other groups' MMAs run.  Four sets of two warps
+// take the active groups in turn (set S the ones at positions S, S + 4, ...), each into
+// its own tile: all 256 rows of the superblock for the group's 32 lanes, each warp one
+// segment (128 rows) of each lane, f16 hi and lo planes.  A set regenerates its tile once
+// the MMAs of its previous group are done, so with four sets a set waits for a quarter of
+// the MMA stream instead of half of it (two sets of 64-lane tiles, same shared memory).  Per K
 // step the tile is consumed by three MMAs of N = 256 (hi image x hi rows into the hi*hi
 // accumulator; hi image x lo rows and lo image x hi rows into the cross accumulator), so
 // the image is read from shared memory once per 256 rows and product.
@@ -329,18 +376,20 @@ __global__ void __launch_bounds__(kThrA, 1) k_ana_ck(CkParams p, const uint8_t *
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t base = (tc::smem_u32(smem_raw) + 1023u) & ~1023u;
     uint8_t *smem = smem_raw + (base - tc::smem_u32(smem_raw));
-    uint8_t *sA = smem;                                              // 2 image buffers
-    uint8_t *sB = smem + 2 * kAImgG;                                 // 2 tiles
-    float4 *sCf = reinterpret_cast<float4 *>(sB + 2 * kTileA);      // kSB coefficient rows
+    uint8_t *sA = smem;                                              // kImgBufA image buffers
+    uint8_t *sB = smem + kImgBufA * kAImgG;                          // kSetsA tiles
+    float4 *sCf = reinterpret_cast<float4 *>(sB + kSetsA * kTileA); // kSB coefficient rows
     const int64_t L = p.lmax + 1, NG = (p.nlanes + kKC - 1) / kKC, NGK = (p.nlanes + kKG - 1) / kKG;
     const int64_t U = p.uoff[L];
     const int64_t G = gridDim.x, c = blockIdx.x;
 
     if (tid == 0) {
-        for (int i = 0; i < 2; ++i) {
+        for (int i = 0; i < kImgBufA; ++i) {
             tc::mbar_init(&sh.a_full[i], 1);
             tc::mbar_init(&sh.a_free[i], 1);
-            tc::mbar_init(&sh.b_full[i], 4);
+        }
+        for (int i = 0; i < kSetsA; ++i) {
+            tc::mbar_init(&sh.b_full[i], kGenA / 32 / kSetsA);
             tc::mbar_init(&sh.b_free[i], 1);
         }
         tc::mbar_init(&sh.d_full, 1);
@@ -363,7 +412,7 @@ __global__ void __launch_bounds__(kThrA, 1) k_ana_ck(CkParams p, const uint8_t *
         // ------------------------------------------------ MMA issuer
         if (lane == 0) {
             const uint32_t idesc = tc::idesc_f16(128, kSB, 0, 1, 1);
-            uint32_t cnt0 = 0, cnt1 = 0;   // groups consumed from each tile
+            uint32_t par = 0;              // bit S: parity of the groups consumed from tile S
             uint32_t q = 0;
             int64_t jg = 0;
             bool ok = true;
@@ -371,14 +420,13 @@ __global__ void __launch_bounds__(kThrA, 1) k_ana_ck(CkParams p, const uint8_t *
                 // the previous unit's epilogue has read TMEM (waited for every unit, so the
                 // phases stay in step); a unit without active groups only signals d_full
                 if (!(ok = wait_or_abort(&sh.d_free, (q & 1) ^ 1, abort, err))) break;
-                unsigned long long rest = p.unit_mask ? (__ldg(p.unit_mask + u) & all_groups(NGK)) : all_groups(NGK);
+                GroupSet rest = unit_groups(p.unit_mask, u, NGK);
                 int k = 0;
                 for (int g = pop_group(rest); g >= 0 && ok; g = pop_group(rest), ++jg, ++k) {
-                    const uint32_t b = (uint32_t)(jg & 1);
-                    const int S = k & 1;
-                    const uint32_t ph = S ? cnt1 : cnt0;
-                    if (!(ok = wait_or_abort(&sh.a_full[b], (uint32_t)(jg >> 1) & 1, abort, err))) break;
-                    if (!(ok = wait_or_abort(&sh.b_full[S], ph & 1, abort, err))) break;
+                    const uint32_t b = (uint32_t)(jg % kImgBufA);
+                    const int S = k % kSetsA;
+                    if (!(ok = wait_or_abort(&sh.a_full[b], (uint32_t)(jg / kImgBufA) & 1, abort, err))) break;
+                    if (!(ok = wait_or_abort(&sh.b_full[S], (par >> S) & 1u, abort, err))) break;
                     tc::tc_fence_after();
                     const uint32_t a0 = tc::smem_u32(sA + b * kAImgG);
                     const uint32_t b0 = tc::smem_u32(sB + S * kTileA);
@@ -395,8 +443,7 @@ __global__ void __launch_bounds__(kThrA, 1) k_ana_ck(CkParams p, const uint8_t *
                     }
                     tc::mma_commit(&sh.b_free[S]);
                     tc::mma_commit(&sh.a_free[b]);
-                    if (S) ++cnt1;
-                    else ++cnt0;
+                    par ^= 1u << S;
                 }
                 if (!ok) break;
                 tc::mma_commit(&sh.d_full);
@@ -407,40 +454,39 @@ __global__ void __launch_bounds__(kThrA, 1) k_ana_ck(CkParams p, const uint8_t *
         }
     } else if (warp == kLoadWarpA) {
         // ------------------------------------------------ image loader
-        // group g of order m: lanes 64 g + [0, 64) are the first or second half (g % 2) of
-        // the 128-lane image g / 2, i.e. 16 KB of its hi plane and 16 KB of its lo plane
+        // group g of order m: lanes 32 g + [0, 32) are quarter g % 4 of the 128-lane image
+        // g / 4, i.e. 8 KB of its hi plane and 8 KB of its lo plane
         if (lane == 0) {
             int64_t jg = 0;
-            bool issued[2] = {false, false};
-            uint32_t last_ph[2] = {0u, 0u};
+            uint32_t issued = 0u, last_ph = 0u;   // bit b: buffer b was filled / its last phase
             bool ok = true;
             for (int64_t u = c; u < U && ok; u += G) {
                 const int64_t m = unit_order(p.uoff, L, u);
-                unsigned long long rest = p.unit_mask ? (__ldg(p.unit_mask + u) & all_groups(NGK)) : all_groups(NGK);
+                GroupSet rest = unit_groups(p.unit_mask, u, NGK);
                 for (int g = pop_group(rest); g >= 0; g = pop_group(rest), ++jg) {
-                    const uint32_t b = (uint32_t)(jg & 1);
-                    const uint8_t *src = aimg + ((m * NG + (g >> 1)) * 2) * (int64_t)kAImg + (g & 1) * (kAImgG / 2);
+                    const uint32_t b = (uint32_t)(jg % kImgBufA), ph = (uint32_t)(jg / kImgBufA) & 1;
+                    const uint8_t *src = aimg + ((m * NG + (g >> 2)) * 2) * (int64_t)kAImg + (g & 3) * (kAImgG / 2);
                     tc::prefetch_l2(src, kAImgG / 2);
                     tc::prefetch_l2(src + kAImg, kAImgG / 2);
-                    if (!(ok = wait_or_abort(&sh.a_free[b], ((uint32_t)(jg >> 1) & 1) ^ 1, abort, err))) break;
+                    if (!(ok = wait_or_abort(&sh.a_free[b], ph ^ 1, abort, err))) break;
                     tc::mbar_arrive_expect_tx(&sh.a_full[b], kAImgG);
                     tc::bulk_g2s(sA + b * kAImgG, src, kAImgG / 2, &sh.a_full[b]);
                     tc::bulk_g2s(sA + b * kAImgG + kAImgG / 2, src + kAImg, kAImgG / 2, &sh.a_full[b]);
-                    issued[b] = true;
-                    last_ph[b] = (uint32_t)(jg >> 1) & 1;
+                    issued |= 1u << b;
+                    last_ph = (last_ph & ~(1u << b)) | (ph << b);
                 }
             }
             // copies still in flight land before the CTA exits (bounded waits)
-            for (int b = 0; b < 2; ++b)
-                if (issued[b]) tc::mbar_wait(&sh.a_full[b], last_ph[b]);
+            for (int b = 0; b < kImgBufA; ++b)
+                if ((issued >> b) & 1u) tc::mbar_wait(&sh.a_full[b], (last_ph >> b) & 1u);
         }
     } else {
         // ------------------------------------------------ generators + epilogue
-        const int S = warp >> 2;                  // tile of the groups g % 2 == S
-        const int sseg = (warp >> 1) & 1;         // segment of the superblock
+        const int S = warp >> 1;                  // set: active groups at positions S, S + 4, ...
+        const int sseg = warp & 1;                // segment of the superblock
         const int t = tid & (kKG - 1);            // lane within the group (the MMA K index)
         const double sgn_c = sgn_of(p.sp);
-        // tile: MN-major SW128 planes (hi, then lo) of 256 MN rows (the superblock) and 64 K
+        // tile: MN-major SW128 planes (hi, then lo) of 256 MN rows (the superblock) and 32 K
         // lanes; per 8 lanes 4 blocks of 64 rows; this thread writes blocks 2 sseg, 2 sseg + 1
         const uint32_t rowbase = tc::smem_u32(sB) + (uint32_t)S * kTileA + (t >> 3) * 4096 +
                                  (uint32_t)(2 * sseg) * 1024 + (t & 7) * 128;
@@ -484,15 +530,14 @@ __global__ void __launch_bounds__(kThrA, 1) k_ana_ck(CkParams p, const uint8_t *
                     nx = __ldg(p.geom + j);
                 }
             };
-            // this set's groups: the active groups at positions S, S + 2, ... of the unit
-            const unsigned long long umask =
-                p.unit_mask ? (__ldg(p.unit_mask + u) & all_groups(NGK)) : all_groups(NGK);
-            unsigned long long rest = umask;
-            if (S) pop_group(rest);
+            // this set's groups: the active groups at positions S, S + 4, ... of the unit
+            const GroupSet umask = unit_groups(p.unit_mask, u, NGK);
+            GroupSet rest = umask;
+            for (int q = 0; q < S; ++q) pop_group(rest);
             int g = pop_group(rest);
             if (!dead && g >= 0) fetch(g);
             for (; g >= 0; ++js) {
-                pop_group(rest);                      // the other set's group
+                for (int q = 1; q < kSetsA; ++q) pop_group(rest);   // the other sets' groups
                 const int gnext = pop_group(rest);
                 if (dead) {
                     g = gnext;
@@ -521,7 +566,7 @@ __global__ void __launch_bounds__(kThrA, 1) k_ana_ck(CkParams p, const uint8_t *
             const uint32_t q = (uint32_t)((u - c) / G);
             if (!dead && !warp_wait(&sh.d_full, q & 1, abort, err)) dead = true;
             // a unit without active groups adds nothing (its accumulator was never written)
-            const bool out = !dead && umask != 0ull;
+            const bool out = !dead && (umask.w0 | umask.w1) != 0ull;
             if (SPIN == 2 && 2 * p.H >= 64) {
                 // spin 2: the north image rows r < H feed alm rows o0 + r and the south rows
                 // H + r' feed rows o1 + r' (o0 != o1, so no row receives both): each thread adds
@@ -929,13 +974,13 @@ static int ck_analysis(int64_t nside, int64_t lmax, int spin, int sp, int64_t nc
                        const uint8_t *ck_shift, const uint64_t *unit_mask, const void *img, double *alm_i,
                        double scale, int64_t nctas, int32_t *err, void *stream)
 {
-    // the lane groups of a unit are walked as the bits of one 64-bit word: 64 x kKG lanes
-    if (nside < 1 || 2 * nside > 64 * kKG || lmax < 2 || lmax > 65535 || !ck_shape_ok(spin, ncomp) ||
+    // the lane groups of a unit are walked as the bits of two 64-bit words: 128 x kKG lanes
+    if (nside < 1 || 2 * nside > kMaxGroupsA * kKG || lmax < 2 || lmax > 65535 || !ck_shape_ok(spin, ncomp) ||
         !ck_spin_ok(spin, sp) || nctas < 1 || nctas > 4096)
         return GM_ERR_BAD_SHAPE;
     if (!geom || !coef || !segoff || !uoff || !ck_state || !ck_shift || !img || !alm_i || !err)
         return GM_ERR_BAD_PTR;
-    const size_t smem = 2 * kAImgG + 2 * kTileA + kSB * sizeof(float4) + 1024;
+    const size_t smem = kImgBufA * kAImgG + kSetsA * kTileA + kSB * sizeof(float4) + 1024;
     auto kern = spin == 0 ? k_ana_ck<0> : k_ana_ck<2>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) {
