@@ -360,6 +360,7 @@ int gm_ck_build(int64_t nside, int64_t lmax, int spin, int sp, const double *geo
                 uint8_t *ck_shift, void *stream);
 /* alm_i += scale * analysis of the rows of `img` (gm_tc_pack / gm_tc_fold images) for row
  * variant sp; nctas persistent CTAs.  No scratch: each alm element belongs to one unit.
+ * At most 4096 lanes (nside <= 2048; GM_ERR_BAD_SHAPE above).
  * err (int32) set non-zero if a bounded wait timed out. */
 int gm_ck_analysis(int64_t nside, int64_t lmax, int spin, int sp, int64_t ncomp,
                    const double *geom, const double *coef, const int64_t *segoff,
