@@ -740,8 +740,10 @@ __global__ void k_prep_syn(int64_t lmax, int spin, int sp, int H, int NR,
 // Reads the synthesis and rhs_map once, writes each image row once (coalesced across the
 // row threads); rows beyond 2H and the absent south ring of the equator lane keep the
 // zeros the pack wrote.
+// Occupancy bound per spin (measured at Nside 2048: spin 0 without spills at 16 CTAs per SM,
+// 15.0 -> 11.6 ms; spin 2 at 10, 23.9 -> 21.7 ms, where 16 would spill).
 template <int SPIN>
-__global__ void __launch_bounds__(128) k_fold_tc(int64_t nside, int64_t L, int ncomp,
+__global__ void __launch_bounds__(128, SPIN == 0 ? 16 : 10) k_fold_tc(int64_t nside, int64_t L, int ncomp,
                                                  const float *__restrict__ synd_a,
                                                  const float *__restrict__ synd_b, int R2,
                                                  const float4 *__restrict__ rhs_map,
