@@ -363,7 +363,7 @@ __device__ __forceinline__ void gen_barrier_a() { asm volatile("bar.sync 1, 256;
 // its own tile: all 256 rows of the superblock for the group's 32 lanes, each warp one
 // segment (128 rows) of each lane, f16 hi and lo planes.  A set regenerates its tile once
 // the MMAs of its previous group are done, so with four sets a set waits for a quarter of
-// the MMA stream instead of half of it (two sets of 64-lane tiles, same shared memory).  Per K
+// the MMA stream (two sets of 64-lane tiles in the same shared memory would wait for half).  Per K
 // step the tile is consumed by three MMAs of N = 256 (hi image x hi rows into the hi*hi
 // accumulator; hi image x lo rows and lo image x hi rows into the cross accumulator), so
 // the image is read from shared memory once per 256 rows and product.
