@@ -62,3 +62,28 @@ def test_single_process_is_identity():
     bench = _bench()
     assert bench.max_over_ranks(7.5, "cpu") == 7.5
     assert bench.throughput(1, 4, 32, 2000.0) == pytest.approx(64.0)
+
+
+def test_ck_byte_model_with_unit_masks():
+    """The mask-aware byte model of the checkpointed analysis launch equals the unmasked
+    model (up to the per-unit rounding of its segment count) when every lane group is
+    active, and drops the images, alm rows and states of inactive units."""
+    import numpy as np
+
+    bench = _bench()
+    nside, lmax, nrows = 64, 191, 32
+    L = lmax + 1
+    uoff = np.zeros(L + 1, dtype=np.int64)
+    for m in range(L):
+        uoff[m + 1] = uoff[m] + (L - max(m, 2) + 255) // 256
+    ngk = (2 * nside + 63) // 64
+    full = np.full(uoff[-1], (1 << ngk) - 1, dtype=np.uint64)
+    plain = bench.ck_analysis_bytes(nside, lmax, nrows)
+    masked = bench.ck_analysis_bytes(nside, lmax, nrows, (full, uoff))
+    assert abs(masked / plain - 1.0) < 0.01
+    none = np.zeros_like(full)
+    assert bench.ck_analysis_bytes(nside, lmax, nrows, (none, uoff)) == 0
+    half = full.copy()
+    half[::2] = 0
+    assert 0 < bench.ck_analysis_bytes(nside, lmax, nrows, (half, uoff)) < masked
+    assert bench.ck_issued_flops((full, uoff)) == 3 * 2 * 128 * 256 * 64 * int(uoff[-1]) * ngk
